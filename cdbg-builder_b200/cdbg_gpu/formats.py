@@ -1,0 +1,239 @@
+"""Readers for the on-disk artifacts of phases 1 and 2 (inspection and parity).
+
+* bucket files   ``bucket_<b>.bin``: LZ4 frames ``[u32 unc][u32 comp][bytes]``,
+                 ``[u32 0]`` end marker (bucket_io.hpp:19-40); records
+                 ``varint ncolors, varint color deltas, varint (len<<4|flags),
+                 packed bases`` (super_kmer.hpp:1-29, 105-143).
+* frag spill     ``frag_unitigs.bin``: ``[u8 open][u32 nruns][nruns x (u64 cid,
+                 u32 num_kmers)][u32 seq_len][seq]`` (unitig_spill.hpp:642-665).
+* .color_sets    ``[u32 C][u32 sparse][u32 dense][u64 bits][u64 words][words]``
+                 then Elias-Fano of the class offsets
+                 (streaming_color_set_dict.hpp:29-37, 221-294); classes are
+                 hybrid-encoded (hybrid_color_sets.hpp:48-95) with
+                 delta(x) = Elias delta of x + 1, LSB-first.
+"""
+import ctypes
+import struct
+
+import numpy as np
+
+FOREIGN = (1 << 64) - 1
+
+_lz4 = None
+
+
+def _lz4lib():
+    global _lz4
+    if _lz4 is None:
+        _lz4 = ctypes.CDLL("liblz4.so.1")
+        _lz4.LZ4_decompress_safe.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        _lz4.LZ4_decompress_safe.restype = ctypes.c_int
+    return _lz4
+
+
+def read_bucket_raw(path):
+    """Decompressed record bytes of one bucket file."""
+    out = bytearray()
+    with open(path, "rb") as f:
+        data = f.read()
+    p = 0
+    while p + 4 <= len(data):
+        (u,) = struct.unpack_from("<I", data, p)
+        p += 4
+        if u == 0:
+            break
+        (c,) = struct.unpack_from("<I", data, p)
+        p += 4
+        dst = ctypes.create_string_buffer(u)
+        d = _lz4lib().LZ4_decompress_safe(bytes(data[p:p + c]), dst, c, u)
+        if d != u:
+            raise RuntimeError("LZ4_decompress_safe failed on " + path)
+        out += dst.raw
+        p += c
+    return bytes(out)
+
+
+def _varint(b, p):
+    v = 0
+    s = 0
+    while True:
+        c = b[p]
+        p += 1
+        v |= (c & 0x7F) << s
+        if not c & 0x80:
+            return v, p
+        s += 7
+
+
+def parse_records(raw):
+    """[(flags, colors tuple, bases 'ACGT' string)] of a decompressed bucket."""
+    out = []
+    p = 0
+    while p < len(raw):
+        n, p = _varint(raw, p)
+        cols = []
+        prev = 0
+        for _ in range(n):
+            d, p = _varint(raw, p)
+            prev += d
+            cols.append(prev)
+        lf, p = _varint(raw, p)
+        ln, fl = lf >> 4, lf & 15
+        nb = (ln + 3) // 4
+        chunk = raw[p:p + nb]
+        p += nb
+        bases = "".join("ACGT"[(chunk[i >> 2] >> (2 * (i & 3))) & 3] for i in range(ln))
+        out.append((fl, tuple(cols), bases))
+    return out
+
+
+def read_frags(data):
+    """[(open_flags, [(cid, num_kmers)], seq)] from frag spill bytes or a path."""
+    if isinstance(data, str):
+        with open(data, "rb") as f:
+            data = f.read()
+    out = []
+    p = 0
+    n = len(data)
+    while p < n:
+        fl = data[p]
+        (nr,) = struct.unpack_from("<I", data, p + 1)
+        p += 5
+        runs = []
+        for _ in range(nr):
+            cid, nk = struct.unpack_from("<QI", data, p)
+            runs.append((cid, nk))
+            p += 12
+        (sl,) = struct.unpack_from("<I", data, p)
+        p += 4
+        out.append((fl, runs, data[p:p + sl].decode()))
+        p += sl
+    return out
+
+
+class _Bits:
+    def __init__(self, words, pos):
+        self.w = words
+        self.p = pos
+
+    def take(self, n):
+        v = 0
+        for i in range(n):
+            q = self.p + i
+            v |= ((int(self.w[q >> 6]) >> (q & 63)) & 1) << i
+        self.p += n
+        return v
+
+    def zeros(self):
+        z = 0
+        while not (int(self.w[self.p >> 6]) >> (self.p & 63)) & 1:
+            z += 1
+            self.p += 1
+        return z
+
+
+def read_gamma(b):
+    l = b.zeros()
+    b.take(1)
+    return (1 << l) | b.take(l)
+
+
+def read_delta(b):
+    l = read_gamma(b) - 1
+    return ((1 << l) | b.take(l)) - 1
+
+
+def decode_class(words, pos, C):
+    """Inverse of the hybrid encoder at bit `pos` (compact_color_set_dict.hpp:176-222)."""
+    sparse_t, dense_t = int(0.25 * C), int(0.75 * C)
+    b = _Bits(words, pos)
+    N = read_delta(b)
+    if N == 0:
+        return []
+    if N < sparse_t:
+        prev = read_delta(b)
+        out = [prev]
+        for _ in range(1, N):
+            prev = prev + read_delta(b) + 1
+            out.append(prev)
+        return out
+    if N < dense_t:
+        return [i for i in range(C) if b.take(1)]
+    comp = C - N
+    absent = set()
+    if comp:
+        prev = read_delta(b)
+        absent.add(prev)
+        for _ in range(1, comp):
+            prev = prev + read_delta(b) + 1
+            absent.add(prev)
+    return [v for v in range(C) if v not in absent]
+
+
+def read_color_sets(path):
+    """(C, words ndarray, class offsets list, decoded classes list)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    C, st, dt, nbits, nwords = struct.unpack_from("<IIIQQ", data, 0)
+    p = 28
+    words = np.frombuffer(data, dtype=np.uint64, count=nwords, offset=p).copy() if nwords else \
+        np.zeros(1, dtype=np.uint64)
+    p += 8 * nwords
+    U, n, l = struct.unpack_from("<QQQ", data, p)
+    p += 24
+    lb, lw = struct.unpack_from("<QQ", data, p)
+    p += 16
+    low = np.frombuffer(data, dtype=np.uint64, count=lw, offset=p) if lw else np.zeros(0, np.uint64)
+    p += 8 * lw
+    hb, hw = struct.unpack_from("<QQ", data, p)
+    p += 16
+    high = np.frombuffer(data, dtype=np.uint64, count=hw, offset=p) if hw else np.zeros(0, np.uint64)
+    offs = []
+    i = 0
+    for wi in range(hw):
+        w = int(high[wi])
+        while w:
+            bit = (w & -w).bit_length() - 1
+            pos = wi * 64 + bit
+            hi = pos - i
+            lo = 0
+            if l:
+                q = i * l
+                lo = 0
+                for j in range(l):
+                    qq = q + j
+                    lo |= ((int(low[qq >> 6]) >> (qq & 63)) & 1) << j
+            offs.append((hi << l) | lo)
+            i += 1
+            w &= w - 1
+    offsets = offs[:-1]
+    if nwords == 0:
+        words = np.zeros(1, dtype=np.uint64)
+    classes = [decode_class(np.append(words, np.uint64(0)), o, C) for o in offsets]
+    return C, words[:nwords], offsets, classes
+
+
+def decode_classes(words, offsets, C):
+    w = np.append(np.asarray(words, dtype=np.uint64), np.uint64(0))
+    return [decode_class(w, int(o), C) for o in offsets]
+
+
+_RC = str.maketrans("ACGT", "TGCA")
+
+
+def revcomp(s):
+    return s.translate(_RC)[::-1]
+
+
+def canonical_frag(fl, runs, seq, classes):
+    """Orientation-free form of a fragment: (seq, per-k-mer color sets, open bits)
+    taken in whichever orientation has the smaller sequence; cids are replaced
+    by their decoded color sets so different id orders compare equal."""
+    per = []
+    for cid, nk in runs:
+        cs = None if cid == FOREIGN else tuple(classes[cid])
+        per.extend([cs] * nk)
+    rs = revcomp(seq)
+    if rs < seq:
+        return (rs, tuple(reversed(per)), ((fl & 1) << 1) | ((fl >> 1) & 1))
+    return (seq, tuple(per), fl)

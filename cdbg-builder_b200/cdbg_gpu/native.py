@@ -1,0 +1,275 @@
+"""ctypes binding of libcdbg_gpu.so (include/cdbg_gpu.h).
+
+Mirrors the reference's phase entry points:
+
+* ``Engine.phase1``  <- ``cdbg::ingest_bucketed`` + ``bucket_writer::close``
+  (phase1_bucket_write/bucket_ingester.hpp:183, bucket_io.hpp:389)
+* ``Engine.phase2``  <- ``cdbg::process_buckets``
+  (phase2_bucket_process/bucket_walker.hpp:608)
+* ``Engine.build``   <- both, in memory (builder.hpp:180 + :269)
+
+Errors raise ``RuntimeError`` with the library's message, as the reference
+throws ``std::runtime_error``.  There is no fallback: if the library is
+missing or no CUDA device is present the calls fail.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "libcdbg_gpu.so")
+
+c_u8p = ctypes.POINTER(ctypes.c_uint8)
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+class SeqBatch(ctypes.Structure):
+    _fields_ = [("seq", ctypes.c_void_p), ("seq_bytes", ctypes.c_uint64),
+                ("seq_off", ctypes.c_void_p), ("seq_color", ctypes.c_void_p),
+                ("num_seqs", ctypes.c_uint32), ("on_device", ctypes.c_int32)]
+
+
+class Phase1Args(ctypes.Structure):
+    _fields_ = [("files", ctypes.POINTER(ctypes.c_char_p)), ("num_files", ctypes.c_uint32),
+                ("k", ctypes.c_uint32), ("m", ctypes.c_uint32), ("num_buckets", ctypes.c_uint32),
+                ("tmp_dir", ctypes.c_char_p), ("host_threads", ctypes.c_uint32),
+                ("chunk_bytes", ctypes.c_uint64), ("bucket_unc_bytes", c_u64p)]
+
+
+class Phase1Stats(ctypes.Structure):
+    _fields_ = [("input_bytes", ctypes.c_uint64), ("seq_bytes", ctypes.c_uint64),
+                ("n_kmers", ctypes.c_uint64), ("n_supers", ctypes.c_uint64),
+                ("n_records", ctypes.c_uint64), ("unc_bytes", ctypes.c_uint64),
+                ("comp_bytes", ctypes.c_uint64), ("seconds_total", ctypes.c_double),
+                ("seconds_device", ctypes.c_double)]
+
+
+CLASS_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, c_u32p, ctypes.c_uint64)
+
+
+class Phase2Args(ctypes.Structure):
+    _fields_ = [("tmp_dir", ctypes.c_char_p), ("num_buckets", ctypes.c_uint32),
+                ("k", ctypes.c_uint32), ("num_colors", ctypes.c_uint32),
+                ("frag_path", ctypes.c_char_p), ("color_sets_path", ctypes.c_char_p),
+                ("on_class", CLASS_CB), ("ctx", ctypes.c_void_p),
+                ("delete_consumed", ctypes.c_int32), ("host_threads", ctypes.c_uint32),
+                ("batch_occ", ctypes.c_uint64)]
+
+
+class Phase2Stats(ctypes.Structure):
+    _fields_ = [("n_records", ctypes.c_uint64), ("n_kmers", ctypes.c_uint64),
+                ("n_distinct", ctypes.c_uint64), ("n_fragments", ctypes.c_uint64),
+                ("total_seq_bytes", ctypes.c_uint64), ("n_color_sets", ctypes.c_uint64),
+                ("total_integers", ctypes.c_uint64), ("color_bits", ctypes.c_uint64),
+                ("seconds_total", ctypes.c_double), ("seconds_device", ctypes.c_double)]
+
+
+class BuildParams(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_uint32), ("m", ctypes.c_uint32), ("num_buckets", ctypes.c_uint32),
+                ("num_colors", ctypes.c_uint32), ("batch_occ", ctypes.c_uint64),
+                ("outputs_to_host", ctypes.c_int32)]
+
+
+class BuildResult(ctypes.Structure):
+    _fields_ = [("frag_bytes", ctypes.c_void_p), ("frag_nbytes", ctypes.c_uint64),
+                ("class_words", ctypes.c_void_p), ("class_bits", ctypes.c_uint64),
+                ("class_offsets", ctypes.c_void_p), ("n_color_sets", ctypes.c_uint64),
+                ("total_integers", ctypes.c_uint64), ("n_kmers", ctypes.c_uint64),
+                ("n_supers", ctypes.c_uint64), ("n_records", ctypes.c_uint64),
+                ("n_occ", ctypes.c_uint64), ("n_distinct", ctypes.c_uint64),
+                ("n_fragments", ctypes.c_uint64), ("total_seq_bytes", ctypes.c_uint64),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+                ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
+                ("ms_total", ctypes.c_double)]
+
+
+# symbol -> (restype, argtypes); the header's complete list
+SIGNATURES = {
+    "cdbg_engine_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "cdbg_engine_destroy": (None, [ctypes.c_void_p]),
+    "cdbg_last_error": (ctypes.c_char_p, []),
+    "cdbg_gpu_version": (ctypes.c_int, []),
+    "cdbg_read_sequences": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32,
+                                           ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(SeqBatch)]),
+    "cdbg_free_sequences": (None, [ctypes.POINTER(SeqBatch)]),
+    "cdbg_gpu_phase1": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Phase1Args),
+                                       ctypes.POINTER(Phase1Stats)]),
+    "cdbg_gpu_dump_supers": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
+                                            ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.c_char_p, c_u64p]),
+    "cdbg_gpu_phase2": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Phase2Args),
+                                       ctypes.POINTER(Phase2Stats)]),
+    "cdbg_gpu_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
+                                      ctypes.POINTER(BuildParams), ctypes.POINTER(BuildResult)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libcdbg_gpu.so (raises OSError when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libcdbg_gpu.so not built: run cdbg-builder_b200/build.py (%s)" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(lib().cdbg_last_error().decode(errors="replace"))
+
+
+def best_m(k):
+    """compute_best_m (phase1_bucket_write/minimizer.hpp:65-73)."""
+    if k <= 13:
+        return (k // 2) if (k // 2 > k - 4) else (k - 4 if k > 4 else 1)
+    for lim, m in ((15, 9), (21, 10), (30, 11), (37, 12), (42, 13), (64, 14)):
+        if k <= lim:
+            return m
+    return (k + 2) // 4
+
+
+def host_batch(seqs, colors):
+    """SeqBatch over host arrays built from Python byte strings (keeps refs alive)."""
+    data = b"".join(seqs)
+    off = np.zeros(len(seqs) + 1, dtype=np.uint64)
+    if seqs:
+        off[1:] = np.cumsum([len(s) for s in seqs])
+    col = np.asarray(colors, dtype=np.uint32)
+    buf = np.frombuffer(data, dtype=np.uint8) if data else np.zeros(1, dtype=np.uint8)
+    b = SeqBatch(buf.ctypes.data, len(data), off.ctypes.data, col.ctypes.data, len(seqs), 0)
+    b._keep = (buf, off, col)
+    return b
+
+
+def array_batch(seq_u8, seq_off_u64, colors_u32, on_device=False):
+    """SeqBatch over numpy arrays (host) or raw device pointers (on_device=True)."""
+    if on_device:
+        b = SeqBatch(seq_u8[0], seq_u8[1], seq_off_u64, colors_u32[0], colors_u32[1], 1)
+        return b
+    b = SeqBatch(seq_u8.ctypes.data, seq_u8.nbytes, seq_off_u64.ctypes.data,
+                 colors_u32.ctypes.data, len(colors_u32), 0)
+    b._keep = (seq_u8, seq_off_u64, colors_u32)
+    return b
+
+
+class HostSequences:
+    """Sequences of FASTA/FASTQ(.gz) files read by the library's host reader
+    (kseq record rules); `.batch` is the SeqBatch to pass to Engine calls."""
+
+    def __init__(self, files, first_color=0, host_threads=0):
+        arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
+        self.batch = SeqBatch()
+        _check(lib().cdbg_read_sequences(arr, len(files), first_color, host_threads,
+                                         ctypes.byref(self.batch)))
+
+    def close(self):
+        if self.batch.seq_off:
+            lib().cdbg_free_sequences(ctypes.byref(self.batch))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def seq_bytes(self):
+        return ctypes.string_at(self.batch.seq, self.batch.seq_bytes)
+
+    def offsets(self):
+        return np.ctypeslib.as_array(ctypes.cast(self.batch.seq_off, c_u64p),
+                                     shape=(self.batch.num_seqs + 1,)).copy()
+
+    def colors(self):
+        if self.batch.num_seqs == 0:
+            return np.zeros(0, dtype=np.uint32)
+        return np.ctypeslib.as_array(ctypes.cast(self.batch.seq_color, c_u32p),
+                                     shape=(self.batch.num_seqs,)).copy()
+
+
+class Engine:
+    """One CUDA device, one stream, a cached device arena."""
+
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        _check(lib().cdbg_engine_create(device, ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().cdbg_engine_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def dump_supers(self, batch, k, m, num_buckets, path):
+        n = ctypes.c_uint64()
+        _check(lib().cdbg_gpu_dump_supers(self._h, ctypes.byref(batch), k, m, num_buckets,
+                                          path.encode(), ctypes.byref(n)))
+        return n.value
+
+    def phase1(self, files, k, num_buckets, tmp_dir, m=0, host_threads=0, chunk_bytes=0):
+        arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
+        unc = np.zeros(num_buckets, dtype=np.uint64)
+        a = Phase1Args(arr, len(files), k, m, num_buckets, tmp_dir.encode(), host_threads,
+                       chunk_bytes, unc.ctypes.data_as(c_u64p))
+        s = Phase1Stats()
+        _check(lib().cdbg_gpu_phase1(self._h, ctypes.byref(a), ctypes.byref(s)))
+        return s, unc
+
+    def phase2(self, tmp_dir, num_buckets, k, num_colors, frag_path, color_sets_path=None,
+               on_class=None, delete_consumed=False, host_threads=0, batch_occ=0):
+        cb = CLASS_CB(0)
+        if on_class is not None:
+            def _cb(ctx, p, n):
+                on_class(np.ctypeslib.as_array(p, shape=(n,)).copy() if n else
+                         np.zeros(0, dtype=np.uint32))
+            cb = CLASS_CB(_cb)
+        a = Phase2Args(tmp_dir.encode(), num_buckets, k, num_colors, frag_path.encode(),
+                       color_sets_path.encode() if color_sets_path else None, cb, None,
+                       1 if delete_consumed else 0, host_threads, batch_occ)
+        s = Phase2Stats()
+        _check(lib().cdbg_gpu_phase2(self._h, ctypes.byref(a), ctypes.byref(s)))
+        return s
+
+    def build(self, batch, k, num_buckets, num_colors, m=0, batch_occ=0, outputs_to_host=True):
+        p = BuildParams(k, m, num_buckets, num_colors, batch_occ, 1 if outputs_to_host else 0)
+        r = BuildResult()
+        _check(lib().cdbg_gpu_build(self._h, ctypes.byref(batch), ctypes.byref(p), ctypes.byref(r)))
+        return r
+
+
+def result_frag_bytes(r):
+    """Host copy of a BuildResult's frag bytes (outputs_to_host=True)."""
+    return ctypes.string_at(r.frag_bytes, r.frag_nbytes) if r.frag_nbytes else b""
+
+
+def result_class_words(r):
+    n = (r.class_bits + 63) // 64
+    if n == 0:
+        return np.zeros(0, dtype=np.uint64)
+    return np.ctypeslib.as_array(ctypes.cast(r.class_words, c_u64p), shape=(n,)).copy()
+
+
+def result_class_offsets(r):
+    if r.n_color_sets == 0:
+        return np.zeros(0, dtype=np.uint64)
+    return np.ctypeslib.as_array(ctypes.cast(r.class_offsets, c_u64p), shape=(r.n_color_sets,)).copy()

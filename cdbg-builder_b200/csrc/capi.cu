@@ -1,0 +1,459 @@
+// C-ABI entry points (include/cdbg_gpu.h): engine lifetime, the two
+// drop-in phases over files, and the in-memory whole path.
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <map>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../host/io.hpp"
+#include "cdbg_gpu.h"
+#include "engine.cuh"
+#include "phase1.cuh"
+#include "phase2.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::map<const uint64_t*, cdbg::io::seq_batch*> g_owned_batches;  // cdbg_read_sequences buffers
+
+int fail(std::exception const& e) {
+    g_last_error = e.what();
+    return -1;
+}
+
+uint32_t best_m(uint32_t k) {  // minimizer.hpp:65-73
+    if (k <= 13) return (k / 2 > k - 4) ? (k / 2) : (k > 4 ? (k - 4) : 1);
+    if (k <= 15) return 9;
+    if (k <= 21) return 10;
+    if (k <= 30) return 11;
+    if (k <= 37) return 12;
+    if (k <= 42) return 13;
+    if (k <= 64) return 14;
+    return (k + 2) / 4;
+}
+
+uint32_t host_threads(uint32_t t) {
+    if (t) return t;
+    unsigned h = std::thread::hardware_concurrency();
+    return h ? h : 8;
+}
+
+void validate(uint32_t k, uint32_t m, uint32_t B) {
+    if (k < 2 || k > 63) throw std::runtime_error("k must be in [2, 63]");
+    if (m == 0 || m >= k || m > 32 || k - m > 62) throw std::runtime_error("invalid minimizer length m");
+    if (B == 0) throw std::runtime_error("num_buckets must be > 0");
+}
+
+struct dev_batch {
+    cdbg::seq_input in;
+};
+
+// Upload (or wrap) a sequence batch.
+cdbg::seq_input stage_batch(cdbg_engine* e, cdbg_seq_batch const* b, uint64_t* h2d) {
+    cdbg::seq_input in;
+    in.nbytes = b->seq_bytes;
+    in.num_seqs = b->num_seqs;
+    if (b->on_device) {
+        in.ascii = reinterpret_cast<uint8_t const*>(b->seq);
+        in.seq_off = b->seq_off;
+        in.seq_color = b->seq_color;
+        return in;
+    }
+    uint8_t* a = e->A.alloc<uint8_t>(b->seq_bytes + 16);
+    uint64_t* so = e->A.alloc<uint64_t>((uint64_t)b->num_seqs + 1);
+    uint32_t* sc = e->A.alloc<uint32_t>((uint64_t)b->num_seqs + 1);
+    if (b->seq_bytes) CDBG_CUDA(cudaMemcpyAsync(a, b->seq, b->seq_bytes, cudaMemcpyHostToDevice, e->st));
+    CDBG_CUDA(cudaMemcpyAsync(so, b->seq_off, 8ull * (b->num_seqs + 1), cudaMemcpyHostToDevice, e->st));
+    if (b->num_seqs)
+        CDBG_CUDA(cudaMemcpyAsync(sc, b->seq_color, 4ull * b->num_seqs, cudaMemcpyHostToDevice, e->st));
+    if (h2d) *h2d += b->seq_bytes + 8ull * (b->num_seqs + 1) + 4ull * b->num_seqs;
+    in.ascii = a;
+    in.seq_off = so;
+    in.seq_color = sc;
+    return in;
+}
+
+inline uint64_t host_bits64(std::vector<uint64_t> const& w, uint64_t pos) {
+    const uint64_t i = pos >> 5;
+    const uint32_t s = (uint32_t)(pos & 31) * 2;
+    uint64_t lo = w[i] >> s;
+    if (s && i + 1 < w.size()) lo |= w[i + 1] << (64 - s);
+    return lo;
+}
+
+}  // namespace
+
+namespace cdbg {
+void check_device_error(cdbg_engine* e, char const* stage) {
+    uint32_t v = 0;
+    CDBG_CUDA(cudaMemcpyAsync(&v, e->d_err, 4, cudaMemcpyDeviceToHost, e->st));
+    CDBG_CUDA(cudaStreamSynchronize(e->st));
+    if (v) {
+        CDBG_CUDA(cudaMemsetAsync(e->d_err, 0, 4, e->st));
+        throw std::runtime_error(std::string("device error ") + std::to_string(v) + " in " + stage);
+    }
+}
+}  // namespace cdbg
+
+extern "C" {
+
+const char* cdbg_last_error(void) { return g_last_error.c_str(); }
+int cdbg_gpu_version(void) { return CDBG_GPU_VERSION; }
+
+int cdbg_read_sequences(const char* const* files, uint32_t num_files, uint32_t first_color,
+                        uint32_t threads, cdbg_seq_batch* out) {
+    try {
+        std::vector<std::string> f(files, files + num_files);
+        auto* hb = new cdbg::io::seq_batch();
+        try {
+            cdbg::io::read_files(f, 0, f.size(), first_color, host_threads(threads), *hb);
+        } catch (...) {
+            delete hb;
+            throw;
+        }
+        out->seq = hb->seq.data();
+        out->seq_bytes = hb->seq.size();
+        out->seq_off = hb->off.data();
+        out->seq_color = hb->color.data();
+        out->num_seqs = (uint32_t)hb->color.size();
+        out->on_device = 0;
+        g_owned_batches[out->seq_off] = hb;
+        return 0;
+    } catch (std::exception const& ex) {
+        return fail(ex);
+    }
+}
+
+void cdbg_free_sequences(cdbg_seq_batch* b) {
+    if (!b) return;
+    auto it = g_owned_batches.find(b->seq_off);
+    if (it != g_owned_batches.end()) {
+        delete it->second;
+        g_owned_batches.erase(it);
+    }
+    b->seq = nullptr;
+    b->seq_off = nullptr;
+    b->seq_color = nullptr;
+    b->seq_bytes = 0;
+    b->num_seqs = 0;
+}
+
+int cdbg_engine_create(int device, cdbg_engine** out) {
+    try {
+        if (!out) throw std::runtime_error("null engine pointer");
+        int n = 0;
+        CDBG_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) throw std::runtime_error("no such CUDA device");
+        CDBG_CUDA(cudaSetDevice(device));
+        auto* e = new cdbg_engine();
+        e->device = device;
+        CDBG_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        CDBG_CUDA(cudaMalloc(&e->d_err, 16));
+        CDBG_CUDA(cudaMemset(e->d_err, 0, 16));
+        *out = e;
+        return 0;
+    } catch (std::exception const& ex) {
+        return fail(ex);
+    }
+}
+
+void cdbg_engine_destroy(cdbg_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    e->A.free_all();
+    if (e->d_err) cudaFree(e->d_err);
+    if (e->st) cudaStreamDestroy(e->st);
+    delete e;
+}
+
+int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, uint32_t m,
+                         uint32_t num_buckets, const char* dump_path, uint64_t* n_supers) {
+    try {
+        if (m == 0) m = best_m(k);
+        validate(k, m, num_buckets);
+        CDBG_CUDA(cudaSetDevice(e->device));
+        e->A.reset();
+        cdbg::seq_input in = stage_batch(e, b, nullptr);
+        cdbg::run_table rt;
+        cdbg::build_runs(in, k, e->A, e->st, rt);
+        cdbg::super_list sl;
+        cdbg::find_supers(rt, k, m, num_buckets, e->A, e->st, sl, e->d_err);
+        cdbg::check_device_error(e, "super-k-mers");
+        const uint64_t n = sl.n;
+        std::vector<uint64_t> start(n), words(rt.nwords);
+        std::vector<uint32_t> len(n), color(n), flags(n), bucket(n);
+        if (n) {
+            CDBG_CUDA(cudaMemcpyAsync(start.data(), sl.start, 8 * n, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(len.data(), sl.len, 4 * n, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(color.data(), sl.color, 4 * n, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(flags.data(), sl.flags, 4 * n, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(bucket.data(), sl.bucket, 4 * n, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(words.data(), rt.words, 8 * rt.nwords, cudaMemcpyDeviceToHost, e->st));
+        }
+        CDBG_CUDA(cudaStreamSynchronize(e->st));
+        std::FILE* f = std::fopen(dump_path, "wb");
+        if (!f) throw std::runtime_error(std::string("cannot open ") + dump_path);
+        std::fwrite(&n, 8, 1, f);
+        std::vector<uint8_t> pk;
+        for (uint64_t i = 0; i < n; ++i) {
+            const uint8_t fl = (uint8_t)flags[i];
+            std::fwrite(&bucket[i], 4, 1, f);
+            std::fwrite(&fl, 1, 1, f);
+            std::fwrite(&color[i], 4, 1, f);
+            std::fwrite(&len[i], 4, 1, f);
+            pk.assign((len[i] + 3) / 4, 0);
+            for (uint32_t j = 0; j < len[i]; j += 32) {
+                uint64_t w = host_bits64(words, start[i] + j);
+                const uint32_t nb = std::min<uint32_t>(32, len[i] - j);
+                for (uint32_t q = 0; q < (nb + 3) / 4; ++q) {
+                    uint8_t byte = (uint8_t)(w >> (8 * q));
+                    const uint32_t valid = std::min<uint32_t>(4, nb - 4 * q);
+                    if (valid < 4) byte &= (uint8_t)((1u << (2 * valid)) - 1);
+                    pk[j / 4 + q] = byte;
+                }
+            }
+            std::fwrite(pk.data(), 1, pk.size(), f);
+        }
+        std::fclose(f);
+        if (n_supers) *n_supers = n;
+        e->A.reset();
+        return 0;
+    } catch (std::exception const& ex) {
+        if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
+int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats* s) {
+    try {
+        auto t0 = std::chrono::steady_clock::now();
+        const uint32_t k = a->k;
+        const uint32_t m = a->m ? a->m : best_m(k);
+        validate(k, m, a->num_buckets);
+        CDBG_CUDA(cudaSetDevice(e->device));
+        const uint32_t T = host_threads(a->host_threads);
+        std::vector<std::string> files(a->files, a->files + a->num_files);
+        cdbg::io::bucket_file_set out(a->tmp_dir, a->num_buckets);
+        cdbg_phase1_stats st{};
+        const uint64_t chunk = a->chunk_bytes ? a->chunk_bytes : (8ull << 30);
+        double dev_s = 0;
+        size_t f0 = 0;
+        while (f0 < files.size()) {
+            // files [f0, f1): whole files until the byte budget is reached
+            size_t f1 = f0;
+            uint64_t acc = 0;
+            while (f1 < files.size()) {
+                std::error_code ec;
+                uint64_t sz = std::filesystem::file_size(files[f1], ec);
+                if (ec) sz = 0;
+                const bool gz = files[f1].size() > 3 && files[f1].compare(files[f1].size() - 3, 3, ".gz") == 0;
+                if (gz) sz *= 4;  // inflated size estimate
+                if (f1 > f0 && acc + sz > chunk) break;
+                acc += sz;
+                ++f1;
+            }
+            cdbg::io::seq_batch hb;
+            cdbg::io::read_files(files, f0, f1 - f0, (uint32_t)f0, T, hb);
+            st.input_bytes += hb.input_bytes;
+            st.seq_bytes += hb.seq.size();
+            auto td = std::chrono::steady_clock::now();
+            e->A.reset();
+            cdbg_seq_batch b{hb.seq.data(), hb.seq.size(), hb.off.data(), hb.color.data(),
+                             (uint32_t)hb.color.size(), 0};
+            cdbg::seq_input in = stage_batch(e, &b, nullptr);
+            cdbg::run_table rt;
+            cdbg::build_runs(in, k, e->A, e->st, rt);
+            cdbg::super_list sl;
+            cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err);
+            cdbg::record_set rs;
+            cdbg::build_records(rt, sl, k, a->num_buckets, e->A, e->st, rs, e->d_err);
+            cdbg::serialized_buckets sb;
+            cdbg::serialize_records(rs, e->A, e->st, sb);
+            cdbg::check_device_error(e, "phase 1");
+            std::vector<uint8_t> raw(sb.nbytes);
+            std::vector<uint64_t> boff(a->num_buckets + 1);
+            if (sb.nbytes)
+                CDBG_CUDA(cudaMemcpyAsync(raw.data(), sb.bytes, sb.nbytes, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(boff.data(), sb.bucket_off, 8ull * (a->num_buckets + 1),
+                                      cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaStreamSynchronize(e->st));
+            dev_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - td).count();
+            st.n_kmers += rt.n_kmers;
+            st.n_supers += sl.n;
+            st.n_records += rs.n;
+            out.append_frames(raw.data(), boff.data(), T);
+            e->A.reset();
+            f0 = f1;
+        }
+        out.close();
+        for (uint64_t u : out.unc_bytes()) st.unc_bytes += u;
+        st.comp_bytes = out.comp_bytes();
+        if (a->bucket_unc_bytes)
+            std::memcpy(a->bucket_unc_bytes, out.unc_bytes().data(), 8ull * a->num_buckets);
+        st.seconds_device = dev_s;
+        st.seconds_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (s) *s = st;
+        return 0;
+    } catch (std::exception const& ex) {
+        if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
+int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats* s) {
+    try {
+        auto t0 = std::chrono::steady_clock::now();
+        CDBG_CUDA(cudaSetDevice(e->device));
+        const uint32_t T = host_threads(a->host_threads);
+        const uint32_t B = a->num_buckets;
+        if (a->k < 2 || a->k > 63) throw std::runtime_error("k must be in [2, 63]");
+        e->A.reset();
+        // bucket bytes: decompress straight into pinned host memory
+        uint8_t* pinned = nullptr;
+        cdbg::io::bucket_bytes bb;
+        cdbg::io::read_bucket_files(
+            a->tmp_dir, B, T,
+            [&](uint64_t n) -> uint8_t* {
+                CDBG_CUDA(cudaMallocHost(&pinned, n));
+                return pinned;
+            },
+            bb, a->delete_consumed != 0);
+        auto td = std::chrono::steady_clock::now();
+        uint8_t* dbytes = e->A.alloc<uint8_t>(bb.nbytes + 64);
+        CDBG_CUDA(cudaMemcpyAsync(dbytes, bb.data, bb.nbytes + 64, cudaMemcpyHostToDevice, e->st));
+        const uint32_t nch = (uint32_t)bb.chunk_bucket.size();
+        uint64_t* dco = e->A.alloc<uint64_t>(nch + 1);
+        uint32_t* dcb = e->A.alloc<uint32_t>(nch + 1);
+        CDBG_CUDA(cudaMemcpyAsync(dco, bb.chunk_off.data(), 8ull * (nch + 1), cudaMemcpyHostToDevice, e->st));
+        if (nch)
+            CDBG_CUDA(cudaMemcpyAsync(dcb, bb.chunk_bucket.data(), 4ull * nch, cudaMemcpyHostToDevice, e->st));
+        CDBG_CUDA(cudaStreamSynchronize(e->st));
+        cudaFreeHost(pinned);
+        pinned = nullptr;
+        cdbg::record_set rs;
+        cdbg::parse_records(dbytes, bb.nbytes, dco, dcb, nch, B, e->A, e->st, rs, e->d_err);
+        cdbg::check_device_error(e, "bucket record parse");
+        cdbg::phase2_params pp;
+        pp.k = a->k;
+        pp.num_colors = a->num_colors;
+        pp.batch_occ = a->batch_occ;
+        pp.to_host = true;
+        pp.keep_lists = a->on_class != nullptr;
+        cdbg::phase2_result res;
+        cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, res);
+        const double dev_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - td).count();
+        // frag spill
+        {
+            std::FILE* f = std::fopen(a->frag_path, "wb");
+            if (!f) throw std::runtime_error(std::string("cannot open frag spill: ") + a->frag_path);
+            if (!res.frag.empty() && std::fwrite(res.frag.data(), 1, res.frag.size(), f) != res.frag.size()) {
+                std::fclose(f);
+                throw std::runtime_error(std::string("short write to ") + a->frag_path);
+            }
+            std::fclose(f);
+        }
+        if (a->color_sets_path)
+            cdbg::io::write_color_sets(a->color_sets_path, a->num_colors, res.words.data(), res.nbits,
+                                       res.offsets.data(), res.n_classes);
+        if (a->on_class)
+            for (uint64_t c = 0; c < res.n_classes; ++c)
+                a->on_class(a->ctx, res.lists.data() + res.list_off[c], res.list_off[c + 1] - res.list_off[c]);
+        if (s) {
+            cdbg_phase2_stats st{};
+            st.n_records = rs.n;
+            st.n_kmers = res.n_occ;
+            st.n_distinct = res.n_distinct;
+            st.n_fragments = res.n_fragments;
+            st.total_seq_bytes = res.total_seq_bytes;
+            st.n_color_sets = res.n_classes;
+            st.total_integers = res.total_integers;
+            st.color_bits = res.nbits;
+            st.seconds_device = dev_s;
+            st.seconds_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            *s = st;
+        }
+        e->A.reset();
+        return 0;
+    } catch (std::exception const& ex) {
+        if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
+int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p, cdbg_build_result* r) {
+    try {
+        const uint32_t k = p->k;
+        const uint32_t m = p->m ? p->m : best_m(k);
+        validate(k, m, p->num_buckets);
+        CDBG_CUDA(cudaSetDevice(e->device));
+        e->A.reset();
+        cdbg_build_result res{};
+        cudaEvent_t ev[4];
+        for (auto& x : ev) CDBG_CUDA(cudaEventCreate(&x));
+        CDBG_CUDA(cudaEventRecord(ev[0], e->st));
+        cdbg::seq_input in = stage_batch(e, b, &res.h2d_bytes);
+        cdbg::run_table rt;
+        cdbg::build_runs(in, k, e->A, e->st, rt);
+        cdbg::super_list sl;
+        cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err);
+        cdbg::record_set rs;
+        cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err);
+        cdbg::check_device_error(e, "phase 1");
+        CDBG_CUDA(cudaEventRecord(ev[1], e->st));
+        cdbg::phase2_params pp;
+        pp.k = k;
+        pp.num_colors = p->num_colors;
+        pp.batch_occ = p->batch_occ;
+        pp.to_host = p->outputs_to_host != 0;
+        cdbg::phase2_result out;
+        cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, out);
+        CDBG_CUDA(cudaEventRecord(ev[2], e->st));
+        CDBG_CUDA(cudaEventSynchronize(ev[2]));
+        float ms1 = 0, ms2 = 0;
+        CDBG_CUDA(cudaEventElapsedTime(&ms1, ev[0], ev[1]));
+        CDBG_CUDA(cudaEventElapsedTime(&ms2, ev[1], ev[2]));
+        for (auto& x : ev) cudaEventDestroy(x);
+        res.ms_phase1 = ms1;
+        res.ms_phase2 = ms2;
+        res.ms_total = ms1 + ms2;
+        res.n_kmers = rt.n_kmers;
+        res.n_supers = sl.n;
+        res.n_records = rs.n;
+        res.n_occ = out.n_occ;
+        res.n_distinct = out.n_distinct;
+        res.n_fragments = out.n_fragments;
+        res.total_seq_bytes = out.total_seq_bytes;
+        res.n_color_sets = out.n_classes;
+        res.total_integers = out.total_integers;
+        res.class_bits = out.nbits;
+        res.frag_nbytes = out.frag_nbytes;
+        if (pp.to_host) {
+            e->h_frag.swap(out.frag);
+            e->h_words.swap(out.words);
+            e->h_offsets.swap(out.offsets);
+            res.frag_bytes = e->h_frag.data();
+            res.class_words = e->h_words.data();
+            res.class_offsets = e->h_offsets.data();
+            res.d2h_bytes = e->h_frag.size() + 8 * e->h_words.size() + 8 * e->h_offsets.size();
+        } else {
+            res.frag_bytes = out.d_frag;
+            res.class_words = out.d_words;
+            res.class_offsets = out.d_offsets;
+        }
+        *r = res;
+        return 0;
+    } catch (std::exception const& ex) {
+        if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
+}  // extern "C"

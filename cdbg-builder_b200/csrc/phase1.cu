@@ -1,0 +1,844 @@
+// Phase 1 (bucket-write) kernels for sm_100a.
+//
+// Restates on the device what the reference does per input file in
+// phase1_bucket_write/bucket_ingester.hpp:36-177 and the compaction of
+// bucket_io.hpp:127-277:
+//   1. ACGT runs >= k of every sequence (bucket_ingester.hpp:152-171),
+//      packed into a 2-bit stream (one 64-bit word = 32 bases).
+//   2. Per run tile (2048 (k-1)-mers, staged into shared memory with a TMA
+//      bulk copy): canonical ntHash of each m-mer (minimizer.hpp:40-62),
+//      sliding minimum over W = k - m m-mers = the (k-1)-mer minimizer
+//      (minimizer.hpp:94-157), and the super-k-mer cut points where the
+//      minimizer changes (bucket_ingester.hpp:106-126).
+//   3. Super-k-mers with flags, bucket (h >> 1) % B and a 64-bit key hash.
+//   4. Full per-bucket dedup: stable radix sort by (bucket, key hash), equal
+//      neighbours merged (flags AND, colors sorted-unique) -- the merge rule of
+//      bucket_io.hpp:137-166, applied to the whole bucket instead of a spill
+//      window (phase-2 results do not depend on the window).
+//   5. Record serialization in the bucket-file record layout
+//      (super_kmer.hpp:105-117) and the inverse parse (super_kmer.hpp:121-143).
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "device_kmer.cuh"
+#include "phase1.cuh"
+#include "primitives.cuh"
+
+namespace cdbg {
+
+namespace {
+
+constexpr int EV_THREADS = 256;
+constexpr int EV_PER_THREAD = 32;
+constexpr int EV_TILE = EV_THREADS * EV_PER_THREAD;
+
+__device__ __forceinline__ uint32_t nuc_code(uint8_t c) {
+    // A/a=0 C/c=1 G/g=2 T/t=3 else 0xff (kmer.hpp:35-52)
+    switch (c | 0x20) {
+        case 'a': return 0;
+        case 'c': return 1;
+        case 'g': return 2;
+        case 't': return 3;
+        default: return 0xffu;
+    }
+}
+
+__device__ __forceinline__ uint32_t upper_bound_u64(uint64_t const* a, uint32_t n, uint64_t x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] <= x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Run boundary events over positions [0, nbytes]: (pos << 1) | 1 for a run
+// start, (pos << 1) for a run end.  Sequence starts (and nbytes) split runs.
+template <bool WRITE>
+__global__ void __launch_bounds__(EV_THREADS)
+    k_run_events(uint8_t const* __restrict__ ascii, uint64_t nbytes,
+                 uint64_t const* __restrict__ seq_off, uint32_t num_seqs,
+                 uint32_t* __restrict__ tile_count, uint64_t const* __restrict__ tile_off,
+                 uint64_t* __restrict__ events) {
+    __shared__ uint32_t sw[EV_THREADS / 32 + 1];
+    const uint64_t p0 = (uint64_t)blockIdx.x * EV_TILE + (uint64_t)threadIdx.x * EV_PER_THREAD;
+    uint32_t cnt = 0;
+    uint64_t ev[2 * EV_PER_THREAD];
+    if (p0 <= nbytes) {
+        const uint64_t pend = (p0 + EV_PER_THREAD < nbytes + 1) ? p0 + EV_PER_THREAD : nbytes + 1;
+        // first sequence boundary strictly after p0; is p0 itself a sequence start?
+        uint32_t s = upper_bound_u64(seq_off, num_seqs + 1, p0);
+        uint64_t next_start = (s <= num_seqs) ? seq_off[s] : ~0ull;
+        bool start_here = (s > 0 && seq_off[s - 1] == p0);
+        bool pvalid = (p0 > 0 && !start_here) ? (nuc_code(ascii[p0 - 1]) != 0xffu) : false;
+        for (uint64_t p = p0; p < pend; ++p) {
+            bool is_seq_start = (p == p0) ? start_here : false;
+            while (p == next_start) {
+                is_seq_start = true;
+                ++s;
+                next_start = (s <= num_seqs) ? seq_off[s] : ~0ull;
+            }
+            if (p == nbytes) is_seq_start = true;
+            const bool valid = (p < nbytes) && nuc_code(ascii[p]) != 0xffu;
+            if (pvalid && (!valid || is_seq_start)) ev[cnt++] = p << 1;          // run end
+            if (valid && (is_seq_start || !pvalid)) ev[cnt++] = (p << 1) | 1u;  // run start
+            pvalid = valid;
+        }
+    }
+    if (!WRITE) {
+        uint32_t tot;
+        prim::block_exclusive_scan<uint32_t, EV_THREADS>(cnt, sw, tot);
+        if (threadIdx.x == 0) tile_count[blockIdx.x] = tot;
+    } else {
+        uint32_t tot;
+        uint32_t ex = prim::block_exclusive_scan<uint32_t, EV_THREADS>(cnt, sw, tot);
+        uint64_t o = tile_off[blockIdx.x] + ex;
+        for (uint32_t i = 0; i < cnt; ++i) events[o + i] = ev[i];
+    }
+}
+
+// Pair events into runs; keep[i] = len >= k.
+__global__ void k_runs_from_events(uint64_t const* __restrict__ ev, uint64_t nruns,
+                                   uint64_t const* __restrict__ seq_off, uint32_t num_seqs,
+                                   uint32_t const* __restrict__ seq_color, uint32_t k,
+                                   uint64_t* __restrict__ src, uint32_t* __restrict__ len,
+                                   uint32_t* __restrict__ color, uint32_t* __restrict__ keep,
+                                   uint32_t* err) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nruns) return;
+    const uint64_t a = ev[2 * i] >> 1, b = ev[2 * i + 1] >> 1;
+    const uint64_t l = b - a;
+    if (l >= 0xffffffffull) set_error(err, ERR_FIELD_OVERFLOW);
+    src[i] = a;
+    len[i] = (uint32_t)l;
+    uint32_t s = upper_bound_u64(seq_off, num_seqs + 1, a) - 1;
+    color[i] = seq_color[s];
+    keep[i] = l >= k ? 1u : 0u;
+}
+
+__global__ void k_runs_compact(uint64_t nruns, uint32_t const* __restrict__ keep,
+                               uint64_t const* __restrict__ kpos, uint64_t const* __restrict__ src,
+                               uint32_t const* __restrict__ len, uint32_t const* __restrict__ color,
+                               uint64_t* __restrict__ osrc, uint32_t* __restrict__ olen,
+                               uint32_t* __restrict__ ocolor, uint64_t* __restrict__ padded) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nruns || !keep[i]) return;
+    const uint64_t o = kpos[i];
+    osrc[o] = src[i];
+    olen[o] = len[i];
+    ocolor[o] = color[i];
+    padded[o] = ((uint64_t)len[i] + 31) & ~uint64_t(31);
+}
+
+// One 64-bit stream word per thread.
+__global__ void k_pack(uint8_t const* __restrict__ ascii, uint32_t nruns,
+                       uint64_t const* __restrict__ soff, uint64_t const* __restrict__ src,
+                       uint32_t const* __restrict__ len, uint64_t nwords_data,
+                       uint64_t* __restrict__ words) {
+    uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nwords_data) return;
+    const uint64_t pos = w * 32;
+    const uint32_t r = upper_bound_u64(soff, nruns, pos) - 1;
+    const uint64_t j = pos - soff[r];
+    const uint32_t L = len[r];
+    uint64_t out = 0;
+    if (j < L) {
+        const uint32_t n = (L - j) < 32 ? (uint32_t)(L - j) : 32u;
+        uint8_t const* p = ascii + src[r] + j;
+        for (uint32_t i = 0; i < n; ++i) out |= (uint64_t)(nuc_code(p[i]) & 3u) << (2 * i);
+    }
+    words[w] = out;
+}
+
+// ------------------------------------------------------------ minimizer tile
+constexpr int MZ_THREADS = 256;
+constexpr int MZ_TT = 2048;                 // (k-1)-mers per tile
+constexpr int MZ_PER = MZ_TT / MZ_THREADS;  // 8
+constexpr int MZ_HMAX = MZ_TT + 1 + 64;     // m-mer hashes (W <= 62)
+constexpr int MZ_WMAX = (MZ_TT + 256) / 32 + 4;
+
+__device__ __forceinline__ uint32_t smem_u32(void const* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// TMA bulk copy global -> shared (cp.async.bulk), completion on an mbarrier.
+// The wait is bounded; on a timeout the whole block gets false and the error
+// word is set (the block then exits without touching the staged tile).
+__device__ __forceinline__ bool tma_load_1d(void* smem_dst, void const* gsrc, uint32_t bytes,
+                                            uint64_t* bar, uint32_t* err) {
+    const uint32_t b = smem_u32(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(smem_dst)),
+            "l"(gsrc), "r"(bytes), "r"(b)
+            : "memory");
+    }
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(b)
+            : "memory");
+        if (done) break;
+    }
+    const int ok = __syncthreads_and((int)done);
+    if (!ok && threadIdx.x == 0) set_error(err, ERR_CHAIN_LIMIT);
+    return ok != 0;
+}
+
+template <bool EMIT>
+__global__ void __launch_bounds__(MZ_THREADS)
+    k_minimizers(uint32_t nruns, uint64_t const* __restrict__ tile_start,
+                 uint64_t const* __restrict__ soff, uint32_t const* __restrict__ len,
+                 uint64_t const* __restrict__ words, uint32_t k, uint32_t m,
+                 uint32_t* __restrict__ tile_count, uint64_t const* __restrict__ tile_off,
+                 uint64_t* __restrict__ out_min, uint32_t* __restrict__ out_run,
+                 uint32_t* __restrict__ out_a, uint32_t* err) {
+    __shared__ __align__(16) uint64_t sw[MZ_WMAX];
+    __shared__ uint64_t sh[MZ_HMAX];
+    __shared__ uint64_t smin[MZ_TT + 1];
+    __shared__ uint32_t sred[MZ_THREADS / 32 + 1];
+    __shared__ __align__(8) uint64_t bar;
+
+    const uint64_t tile = blockIdx.x;
+    const uint32_t r = upper_bound_u64(tile_start, nruns + 1, tile) - 1;
+    const uint64_t t_local = tile - tile_start[r];
+    const uint32_t L = len[r];
+    const uint32_t W = k - m;
+    const uint64_t nk1 = (uint64_t)L - k + 2;  // (k-1)-mers 0..K
+    const uint64_t j0 = t_local * MZ_TT;
+    const uint64_t j1 = (j0 + MZ_TT < nk1) ? j0 + MZ_TT : nk1;
+    const uint64_t e0 = j0 ? j0 - 1 : 0;
+    const uint32_t nmin = (uint32_t)(j1 - e0);
+    const uint32_t nh = nmin + W - 1;
+    // bases [e0, j1 + k - 2) of the run
+    const uint64_t pa = soff[r] + e0;
+    const uint64_t pb = soff[r] + j1 + k - 2;
+    const uint64_t wa = (pa >> 5) & ~uint64_t(1);
+    const uint64_t wb = ((pb + 31) >> 5) + 1;
+    const uint32_t nw = (uint32_t)(((wb - wa) + 1) & ~uint64_t(1));
+    if (!tma_load_1d(sw, words + wa, nw * 8u, &bar, err)) return;  // uniform across the block
+    const uint32_t rel0 = (uint32_t)(pa - wa * 32);  // stream offset of base e0 in sw
+    auto base_at = [&](uint32_t q) -> uint32_t {     // q relative to e0
+        const uint32_t x = rel0 + q;
+        return (uint32_t)(sw[x >> 5] >> (2 * (x & 31))) & 3u;
+    };
+    // canonical m-mer hashes h[0..nh) (h[q] = m-mer at base e0 + q)
+    const uint32_t per_h = (nh + MZ_THREADS - 1) / MZ_THREADS;
+    {
+        const uint32_t q0 = threadIdx.x * per_h;
+        const uint32_t q1 = min(q0 + per_h, nh);
+        if (q0 < q1) {
+            uint64_t f = 0, rc = 0;
+            for (uint32_t i = 0; i < m; ++i) {
+                const uint32_t b = base_at(q0 + i);
+                f ^= rol64(nt_seed(b), m - 1 - i);
+                rc ^= rol64(nt_seed(b ^ 3u), i);
+            }
+            sh[q0] = f <= rc ? f : rc;
+            for (uint32_t q = q0 + 1; q < q1; ++q) {
+                const uint32_t out = base_at(q - 1), in = base_at(q + m - 1);
+                f = rol64(f, 1) ^ rol64(nt_seed(out), m) ^ nt_seed(in);
+                rc = ror64(rc, 1) ^ ror64(nt_seed(out ^ 3u), 1) ^ rol64(nt_seed(in ^ 3u), m - 1);
+                sh[q] = f <= rc ? f : rc;
+            }
+        }
+    }
+    __syncthreads();
+    // sliding minimum: smin[q] = min h[q .. q + W - 1]
+    const uint32_t per_m = (nmin + MZ_THREADS - 1) / MZ_THREADS;
+    {
+        const uint32_t q0 = threadIdx.x * per_m;
+        const uint32_t q1 = min(q0 + per_m, nmin);
+        if (q0 < q1) {
+            uint64_t cur = ~0ull;
+            uint32_t cp = 0;
+            for (uint32_t i = 0; i < W; ++i) {
+                const uint64_t v = sh[q0 + i];
+                if (v <= cur) {
+                    cur = v;
+                    cp = q0 + i;
+                }
+            }
+            smin[q0] = cur;
+            for (uint32_t q = q0 + 1; q < q1; ++q) {
+                const uint64_t v = sh[q + W - 1];
+                if (cp < q) {
+                    cur = ~0ull;
+                    for (uint32_t i = q; i < q + W; ++i) {
+                        const uint64_t x = sh[i];
+                        if (x <= cur) {
+                            cur = x;
+                            cp = i;
+                        }
+                    }
+                } else if (v <= cur) {
+                    cur = v;
+                    cp = q + W - 1;
+                }
+                smin[q] = cur;
+            }
+        }
+    }
+    __syncthreads();
+    // cut points j in [j0, j1): j == 0 or min(j) != min(j - 1)
+    const uint32_t off = (uint32_t)(j0 - e0);  // 0 or 1
+    const uint32_t ncut = (uint32_t)(j1 - j0);
+    const uint32_t c0 = threadIdx.x * MZ_PER;
+    uint32_t cnt = 0;
+    for (uint32_t c = c0; c < c0 + MZ_PER && c < ncut; ++c) {
+        const uint64_t j = j0 + c;
+        const uint32_t q = c + off;
+        if (j == 0 || smin[q] != smin[q - 1]) ++cnt;
+    }
+    uint32_t tot;
+    const uint32_t ex = prim::block_exclusive_scan<uint32_t, MZ_THREADS>(cnt, sred, tot);
+    if (!EMIT) {
+        if (threadIdx.x == 0) tile_count[tile] = tot;
+        return;
+    }
+    uint64_t o = tile_off[tile] + ex;
+    for (uint32_t c = c0; c < c0 + MZ_PER && c < ncut; ++c) {
+        const uint64_t j = j0 + c;
+        const uint32_t q = c + off;
+        if (j == 0 || smin[q] != smin[q - 1]) {
+            out_min[o] = smin[q];
+            out_run[o] = r;
+            out_a[o] = (uint32_t)j;
+            ++o;
+        }
+    }
+}
+
+__global__ void k_run_tiles(uint32_t nruns, uint32_t const* __restrict__ len, uint32_t k,
+                            uint64_t* __restrict__ ntiles) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns) return;
+    const uint64_t nk1 = (uint64_t)len[r] - k + 2;
+    ntiles[r] = (nk1 + MZ_TT - 1) / MZ_TT;
+}
+
+__global__ void k_run_kmers(uint32_t nruns, uint32_t const* __restrict__ len, uint32_t k,
+                            unsigned long long* __restrict__ acc) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = 0, b = 0;
+    if (r < nruns) {
+        v = (unsigned long long)len[r] - k + 1;
+        b = len[r];
+    }
+    for (int o = 16; o; o >>= 1) {
+        v += __shfl_down_sync(0xffffffffu, v, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(acc, v);
+        atomicAdd(acc + 1, b);
+    }
+}
+
+// Super-k-mer fields from the cut list (bucket_ingester.hpp:80-126).
+__global__ void k_super_finalize(uint64_t n, uint64_t const* __restrict__ minv,
+                                 uint32_t const* __restrict__ run, uint32_t const* __restrict__ a_arr,
+                                 uint64_t const* __restrict__ soff, uint32_t const* __restrict__ rlen,
+                                 uint32_t const* __restrict__ rcolor, uint64_t const* __restrict__ words,
+                                 uint32_t k, uint32_t B, uint32_t bb, uint64_t* __restrict__ start,
+                                 uint32_t* __restrict__ len, uint32_t* __restrict__ color,
+                                 uint32_t* __restrict__ flags, uint32_t* __restrict__ bucket,
+                                 uint64_t* __restrict__ key) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t r = run[i];
+    const uint32_t a = a_arr[i];
+    const uint64_t K = (uint64_t)rlen[r] - k + 1;
+    const bool next_same = (i + 1 < n) && run[i + 1] == r;
+    const uint64_t b = next_same ? (uint64_t)a_arr[i + 1] - 1 : K;
+    const uint64_t fk = a ? a - 1 : 0;
+    const uint64_t lk = b < K - 1 ? b : K - 1;
+    const uint32_t l = (uint32_t)(lk - fk + k);
+    const uint64_t mv = minv[i];
+    uint32_t f = 0;
+    if (a == 0) f |= 1u;                             // IS_ACGT_BEGIN
+    if (!next_same) f |= 2u;                         // IS_ACGT_END
+    if (a == 0 || mv < minv[i - 1]) f |= 4u;         // OWNS_FIRST
+    if (!next_same || mv < minv[i + 1]) f |= 8u;     // OWNS_LAST
+    const uint32_t bk = (uint32_t)((mv >> 1) % B);
+    const uint64_t st = soff[r] + fk;
+    start[i] = st;
+    len[i] = l;
+    color[i] = rcolor[r];
+    flags[i] = f;
+    bucket[i] = bk;
+    const uint64_t h = super_hash_dev(words, st, l);
+    key[i] = bb ? (((uint64_t)bk << (64 - bb)) | (h >> bb)) : h;
+}
+
+__device__ __forceinline__ bool same_bases(uint64_t const* __restrict__ words, uint64_t pa,
+                                           uint64_t pb, uint32_t len) {
+    for (uint32_t i = 0; i < len; i += 32) {
+        uint64_t x = stream_bits64(words, pa + i) ^ stream_bits64(words, pb + i);
+        const uint32_t n = len - i;
+        if (n < 32) x &= (uint64_t(1) << (2 * n)) - 1;
+        if (x) return false;
+    }
+    return true;
+}
+
+__global__ void k_group_heads(uint64_t n, uint64_t const* __restrict__ key,
+                              uint32_t const* __restrict__ idx, uint64_t const* __restrict__ start,
+                              uint32_t const* __restrict__ len, uint32_t const* __restrict__ color,
+                              uint64_t const* __restrict__ words, uint32_t* __restrict__ head,
+                              uint32_t* __restrict__ ckeep) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t i = idx[p];
+    bool h = true;
+    if (p > 0) {
+        const uint32_t j = idx[p - 1];
+        h = !(key[p] == key[p - 1] && len[i] == len[j] && same_bases(words, start[i], start[j], len[i]));
+        ckeep[p] = (h || color[i] != color[j]) ? 1u : 0u;
+    } else {
+        ckeep[p] = 1u;
+    }
+    head[p] = h ? 1u : 0u;
+}
+
+__global__ void k_records_fill(uint64_t n, uint32_t const* __restrict__ idx,
+                               uint32_t const* __restrict__ head, uint64_t const* __restrict__ rid_ex,
+                               uint32_t const* __restrict__ ckeep, uint64_t const* __restrict__ cpos,
+                               uint64_t const* __restrict__ start, uint32_t const* __restrict__ len,
+                               uint32_t const* __restrict__ color, uint32_t const* __restrict__ flags,
+                               uint32_t const* __restrict__ bucket, uint64_t* __restrict__ r_start,
+                               uint32_t* __restrict__ r_len, uint32_t* __restrict__ r_flags,
+                               uint64_t* __restrict__ r_coloff, uint32_t* __restrict__ colors,
+                               uint32_t* __restrict__ r_bucket) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t i = idx[p];
+    const uint64_t rid = rid_ex[p] + head[p] - 1;  // inclusive count - 1
+    if (head[p]) {
+        r_start[rid] = start[i];
+        r_len[rid] = len[i];
+        r_coloff[rid] = cpos[p];
+        r_bucket[rid] = bucket[i];
+    }
+    atomicAnd(&r_flags[rid], flags[i]);
+    if (ckeep[p]) colors[cpos[p]] = color[i];
+}
+
+__global__ void k_bucket_hist(uint64_t n, uint32_t const* __restrict__ rb,
+                              unsigned long long* __restrict__ cnt) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&cnt[rb[i]], 1ull);
+}
+
+__global__ void k_fill_u32(uint32_t* p, uint64_t n, uint32_t v) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+__global__ void k_iota_u32(uint32_t* p, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = (uint32_t)i;
+}
+__global__ void k_set_last_u64(uint64_t* p, uint64_t idx, uint64_t const* v) { p[idx] = *v; }
+
+// ------------------------------------------------------------ serialization
+__device__ __forceinline__ uint32_t varint_len(uint64_t v) {
+    uint32_t n = 1;
+    while (v >= 0x80) {
+        v >>= 7;
+        ++n;
+    }
+    return n;
+}
+__device__ __forceinline__ uint8_t* varint_put(uint8_t* o, uint64_t v) {
+    while (v >= 0x80) {
+        *o++ = (uint8_t)((v & 0x7f) | 0x80);
+        v >>= 7;
+    }
+    *o++ = (uint8_t)v;
+    return o;
+}
+
+__global__ void k_rec_sizes(uint64_t n, uint64_t const* __restrict__ coloff,
+                            uint32_t const* __restrict__ colors, uint32_t const* __restrict__ len,
+                            uint32_t const* __restrict__ flags, uint64_t* __restrict__ sz) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint64_t c0 = coloff[r], c1 = coloff[r + 1];
+    uint64_t s = varint_len(c1 - c0);
+    uint32_t prev = 0;
+    for (uint64_t c = c0; c < c1; ++c) {
+        s += varint_len(colors[c] - prev);
+        prev = colors[c];
+    }
+    s += varint_len(((uint64_t)len[r] << 4) | (flags[r] & 0xfu));
+    s += (len[r] + 3) / 4;
+    sz[r] = s;
+}
+
+__global__ void k_rec_write(uint64_t n, uint64_t const* __restrict__ coloff,
+                            uint32_t const* __restrict__ colors, uint64_t const* __restrict__ start,
+                            uint32_t const* __restrict__ len, uint32_t const* __restrict__ flags,
+                            uint64_t const* __restrict__ words, uint64_t const* __restrict__ off,
+                            uint8_t* __restrict__ out) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    uint8_t* o = out + off[r];
+    const uint64_t c0 = coloff[r], c1 = coloff[r + 1];
+    o = varint_put(o, c1 - c0);
+    uint32_t prev = 0;
+    for (uint64_t c = c0; c < c1; ++c) {
+        o = varint_put(o, colors[c] - prev);
+        prev = colors[c];
+    }
+    const uint32_t l = len[r];
+    o = varint_put(o, ((uint64_t)l << 4) | (flags[r] & 0xfu));
+    const uint64_t st = start[r];
+    for (uint32_t i = 0; i < l; i += 32) {
+        uint64_t w = stream_bits64(words, st + i);
+        const uint32_t nb = (l - i) < 32 ? (l - i) : 32u;
+        if (nb < 32) w &= (uint64_t(1) << (2 * nb)) - 1;
+        const uint32_t bytes = (nb + 3) / 4;
+        for (uint32_t b = 0; b < bytes; ++b) o[b] = (uint8_t)(w >> (8 * b));
+        o += bytes;
+    }
+}
+
+// ------------------------------------------------------------ parsing
+__device__ __forceinline__ uint64_t varint_get(uint8_t const* b, uint64_t end, uint64_t& p, bool& ok) {
+    uint64_t v = 0;
+    uint32_t sh = 0;
+    while (p < end) {
+        const uint8_t c = b[p++];
+        v |= (uint64_t)(c & 0x7f) << sh;
+        if (!(c & 0x80)) return v;
+        sh += 7;
+        if (sh >= 64) break;
+    }
+    ok = false;
+    return v;
+}
+
+// One thread per chunk: count records and colors (pass 0) or fill (pass 1).
+template <bool FILL>
+__global__ void k_parse_chunks(uint8_t const* __restrict__ bytes, uint64_t const* __restrict__ chunk_off,
+                               uint32_t nchunks, uint64_t* __restrict__ nrec, uint64_t* __restrict__ ncol,
+                               uint64_t const* __restrict__ rec_base, uint64_t const* __restrict__ col_base,
+                               uint64_t* __restrict__ r_start, uint32_t* __restrict__ r_len,
+                               uint32_t* __restrict__ r_flags, uint64_t* __restrict__ r_coloff,
+                               uint32_t* __restrict__ colors, uint32_t* err) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    uint64_t p = chunk_off[c];
+    const uint64_t end = chunk_off[c + 1];
+    uint64_t nr = 0, nc = 0;
+    uint64_t ro = FILL ? rec_base[c] : 0, co = FILL ? col_base[c] : 0;
+    while (p < end) {
+        bool ok = true;
+        const uint64_t k = varint_get(bytes, end, p, ok);
+        if (FILL) r_coloff[ro + nr] = co + nc;
+        uint32_t prev = 0;
+        for (uint64_t i = 0; i < k && ok; ++i) {
+            prev += (uint32_t)varint_get(bytes, end, p, ok);
+            if (FILL) colors[co + nc + i] = prev;
+        }
+        const uint64_t lf = varint_get(bytes, end, p, ok);
+        const uint64_t l = lf >> 4;
+        const uint64_t nb = (l + 3) / 4;
+        if (!ok || p + nb > end || l >= (1ull << 32)) {
+            set_error(err, ERR_BAD_RECORD);
+            return;
+        }
+        if (FILL) {
+            r_start[ro + nr] = p * 4;  // byte offset -> 2-bit stream position
+            r_len[ro + nr] = (uint32_t)l;
+            r_flags[ro + nr] = (uint32_t)(lf & 0xf);
+        }
+        p += nb;
+        nc += k;
+        ++nr;
+    }
+    if (!FILL) {
+        nrec[c] = nr;
+        ncol[c] = nc;
+    }
+}
+
+__global__ void k_bucket_bytes(uint32_t B, uint64_t const* __restrict__ bstart,
+                               uint64_t const* __restrict__ rec_off, uint64_t* __restrict__ boff) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b <= B) boff[b] = rec_off[bstart[b]];
+}
+
+__global__ void k_chunk_bucket_counts(uint32_t nchunks, uint32_t const* __restrict__ chunk_bucket,
+                                      uint64_t const* __restrict__ nrec,
+                                      unsigned long long* __restrict__ bcnt) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nchunks) atomicAdd(&bcnt[chunk_bucket[c]], (unsigned long long)nrec[c]);
+}
+
+inline unsigned grid(uint64_t n, unsigned t) { return (unsigned)ceil_div(n, t); }
+
+template <typename T>
+T read_dev(T const* p, cudaStream_t st) {
+    T v;
+    CDBG_CUDA(cudaMemcpyAsync(&v, p, sizeof(T), cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    return v;
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- host side
+void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt) {
+    rt = run_table();
+    const uint64_t npos = in.nbytes + 1;
+    const uint64_t tiles = ceil_div(npos, EV_TILE);
+    uint32_t* tcount = A.alloc<uint32_t>(tiles);
+    uint64_t* toff = A.alloc<uint64_t>(tiles + 1);
+    k_run_events<false><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
+                                                                 in.num_seqs, tcount, nullptr, nullptr);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, tiles, A, st, toff + tiles);
+    const uint64_t nev = read_dev(toff + tiles, st);
+    const uint64_t nraw = nev / 2;
+    if (nraw == 0) return;
+    uint64_t* ev = A.alloc<uint64_t>(nev);
+    k_run_events<true><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
+                                                                in.num_seqs, tcount, toff, ev);
+    CDBG_CHECK_LAUNCH();
+    uint64_t* src = A.alloc<uint64_t>(nraw);
+    uint32_t* len = A.alloc<uint32_t>(nraw);
+    uint32_t* color = A.alloc<uint32_t>(nraw);
+    uint32_t* keep = A.alloc<uint32_t>(nraw);
+    uint64_t* kpos = A.alloc<uint64_t>(nraw + 1);
+    uint32_t* err = A.alloc<uint32_t>(1);
+    CDBG_CUDA(cudaMemsetAsync(err, 0, 4, st));
+    k_runs_from_events<<<grid(nraw, 256), 256, 0, st>>>(ev, nraw, in.seq_off, in.num_seqs,
+                                                         in.seq_color, k, src, len, color, keep, err);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(keep, kpos, nraw, A, st, kpos + nraw);
+    const uint64_t nruns = read_dev(kpos + nraw, st);
+    if (read_dev(err, st) != 0) throw std::runtime_error("run length exceeds 2^32 bases");
+    if (nruns == 0) return;
+    if (nruns >= 0xffffffffull) throw std::runtime_error("too many ACGT runs");
+    rt.n = (uint32_t)nruns;
+    rt.src = A.alloc<uint64_t>(nruns);
+    rt.len = A.alloc<uint32_t>(nruns);
+    rt.color = A.alloc<uint32_t>(nruns);
+    uint64_t* padded = A.alloc<uint64_t>(nruns);
+    rt.soff = A.alloc<uint64_t>(nruns + 1);
+    k_runs_compact<<<grid(nraw, 256), 256, 0, st>>>(nraw, keep, kpos, src, len, color, rt.src, rt.len,
+                                                     rt.color, padded);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint64_t, uint64_t>(padded, rt.soff, nruns, A, st, rt.soff + nruns);
+    const uint64_t total = read_dev(rt.soff + nruns, st);
+    const uint64_t nwd = total / 32;
+    rt.nwords = nwd + 8;
+    rt.words = A.alloc<uint64_t>(rt.nwords);
+    CDBG_CUDA(cudaMemsetAsync(rt.words + nwd, 0, 8 * 8, st));
+    if (nwd) {
+        k_pack<<<grid(nwd, 256), 256, 0, st>>>(in.ascii, rt.n, rt.soff, rt.src, rt.len, nwd, rt.words);
+        CDBG_CHECK_LAUNCH();
+    }
+    unsigned long long* acc = A.alloc<unsigned long long>(2);
+    CDBG_CUDA(cudaMemsetAsync(acc, 0, 16, st));
+    k_run_kmers<<<grid(nruns, 256), 256, 0, st>>>(rt.n, rt.len, k, acc);
+    CDBG_CHECK_LAUNCH();
+    unsigned long long h[2];
+    CDBG_CUDA(cudaMemcpyAsync(h, acc, 16, cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    rt.n_kmers = h[0];
+    rt.n_bases = h[1];
+}
+
+void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
+                 cudaStream_t st, super_list& out, uint32_t* d_err) {
+    out = super_list();
+    if (rt.n == 0) return;
+    if (k < 2 || m >= k || k - m > 62 || m > 32)
+        throw std::runtime_error("unsupported k/m combination");
+    uint64_t* ntl = A.alloc<uint64_t>(rt.n);
+    uint64_t* tstart = A.alloc<uint64_t>(rt.n + 1);
+    k_run_tiles<<<grid(rt.n, 256), 256, 0, st>>>(rt.n, rt.len, k, ntl);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint64_t, uint64_t>(ntl, tstart, rt.n, A, st, tstart + rt.n);
+    const uint64_t ntiles = read_dev(tstart + rt.n, st);
+    uint32_t* tcount = A.alloc<uint32_t>(ntiles);
+    uint64_t* toff = A.alloc<uint64_t>(ntiles + 1);
+    k_minimizers<false><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+        rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, nullptr, nullptr, nullptr, nullptr, d_err);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, ntiles, A, st, toff + ntiles);
+    const uint64_t n = read_dev(toff + ntiles, st);
+    if (n >= 0xffffffffull) throw std::runtime_error("more than 2^32 super-k-mers in one call");
+    uint64_t* minv = A.alloc<uint64_t>(n);
+    uint32_t* run = A.alloc<uint32_t>(n);
+    uint32_t* aa = A.alloc<uint32_t>(n);
+    k_minimizers<true><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+        rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, toff, minv, run, aa, d_err);
+    CDBG_CHECK_LAUNCH();
+    out.n = n;
+    out.start = A.alloc<uint64_t>(n);
+    out.len = A.alloc<uint32_t>(n);
+    out.color = A.alloc<uint32_t>(n);
+    out.flags = A.alloc<uint32_t>(n);
+    out.bucket = A.alloc<uint32_t>(n);
+    out.key = A.alloc<uint64_t>(n);
+    uint32_t bb = 0;
+    while ((1ull << bb) < B) ++bb;
+    k_super_finalize<<<grid(n, 256), 256, 0, st>>>(n, minv, run, aa, rt.soff, rt.len, rt.color, rt.words,
+                                                    k, B, bb, out.start, out.len, out.color, out.flags,
+                                                    out.bucket, out.key);
+    CDBG_CHECK_LAUNCH();
+}
+
+void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, dev_arena& A,
+                   cudaStream_t st, record_set& rs, uint32_t* d_err) {
+    (void)k;
+    (void)d_err;
+    rs = record_set();
+    rs.B = B;
+    rs.words = rt.words;
+    rs.nwords = rt.nwords;
+    rs.n_occ_supers = sl.n;
+    rs.bucket_start = A.alloc<uint64_t>(B + 1);
+    const uint64_t n = sl.n;
+    if (n == 0) {
+        CDBG_CUDA(cudaMemsetAsync(rs.bucket_start, 0, 8 * (B + 1), st));
+        rs.col_off = A.alloc<uint64_t>(1);
+        CDBG_CUDA(cudaMemsetAsync(rs.col_off, 0, 8, st));
+        return;
+    }
+    uint32_t* idx = A.alloc<uint32_t>(n);
+    k_iota_u32<<<grid(n, 256), 256, 0, st>>>(idx, n);
+    CDBG_CHECK_LAUNCH();
+    // sort a copy of the keys (the super list keeps its input order)
+    uint64_t* skey = A.alloc<uint64_t>(n);
+    CDBG_CUDA(cudaMemcpyAsync(skey, sl.key, n * 8, cudaMemcpyDeviceToDevice, st));
+    prim::radix_sort_pairs<uint32_t>(skey, idx, n, 0, 64, A, st);
+    uint32_t* head = A.alloc<uint32_t>(n);
+    uint32_t* ckeep = A.alloc<uint32_t>(n);
+    k_group_heads<<<grid(n, 256), 256, 0, st>>>(n, skey, idx, sl.start, sl.len, sl.color, rt.words,
+                                                 head, ckeep);
+    CDBG_CHECK_LAUNCH();
+    uint64_t* rid = A.alloc<uint64_t>(n + 1);
+    uint64_t* cpos = A.alloc<uint64_t>(n + 1);
+    prim::exclusive_scan<uint32_t, uint64_t>(head, rid, n, A, st, rid + n);
+    prim::exclusive_scan<uint32_t, uint64_t>(ckeep, cpos, n, A, st, cpos + n);
+    uint64_t tot[2];
+    CDBG_CUDA(cudaMemcpyAsync(&tot[0], rid + n, 8, cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaMemcpyAsync(&tot[1], cpos + n, 8, cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    const uint64_t nr = tot[0], nc = tot[1];
+    rs.n = nr;
+    rs.ncolors = nc;
+    rs.start = A.alloc<uint64_t>(nr);
+    rs.len = A.alloc<uint32_t>(nr);
+    rs.flags = A.alloc<uint32_t>(nr);
+    rs.col_off = A.alloc<uint64_t>(nr + 1);
+    rs.colors = A.alloc<uint32_t>(nc);
+    uint32_t* rb = A.alloc<uint32_t>(nr);
+    k_fill_u32<<<grid(nr, 256), 256, 0, st>>>(rs.flags, nr, 0xfu);
+    CDBG_CHECK_LAUNCH();
+    k_records_fill<<<grid(n, 256), 256, 0, st>>>(n, idx, head, rid, ckeep, cpos, sl.start, sl.len,
+                                                  sl.color, sl.flags, sl.bucket, rs.start, rs.len,
+                                                  rs.flags, rs.col_off, rs.colors, rb);
+    CDBG_CHECK_LAUNCH();
+    k_set_last_u64<<<1, 1, 0, st>>>(rs.col_off, nr, cpos + n);
+    CDBG_CHECK_LAUNCH();
+    unsigned long long* bc = A.alloc<unsigned long long>(B);
+    CDBG_CUDA(cudaMemsetAsync(bc, 0, 8ull * B, st));
+    k_bucket_hist<<<grid(nr, 256), 256, 0, st>>>(nr, rb, bc);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<unsigned long long, uint64_t>(bc, rs.bucket_start, B, A, st, rs.bucket_start + B);
+}
+
+void serialize_records(record_set const& rs, dev_arena& A, cudaStream_t st, serialized_buckets& out) {
+    out = serialized_buckets();
+    out.rec_off = A.alloc<uint64_t>(rs.n + 1);
+    out.bucket_off = A.alloc<uint64_t>(rs.B + 1);
+    if (rs.n == 0) {
+        CDBG_CUDA(cudaMemsetAsync(out.rec_off, 0, 8, st));
+        CDBG_CUDA(cudaMemsetAsync(out.bucket_off, 0, 8ull * (rs.B + 1), st));
+        out.bytes = A.alloc<uint8_t>(16);
+        return;
+    }
+    uint64_t* sz = A.alloc<uint64_t>(rs.n);
+    k_rec_sizes<<<grid(rs.n, 256), 256, 0, st>>>(rs.n, rs.col_off, rs.colors, rs.len, rs.flags, sz);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint64_t, uint64_t>(sz, out.rec_off, rs.n, A, st, out.rec_off + rs.n);
+    out.nbytes = read_dev(out.rec_off + rs.n, st);
+    out.bytes = A.alloc<uint8_t>(out.nbytes + 16);
+    k_rec_write<<<grid(rs.n, 256), 256, 0, st>>>(rs.n, rs.col_off, rs.colors, rs.start, rs.len, rs.flags,
+                                                  rs.words, out.rec_off, out.bytes);
+    CDBG_CHECK_LAUNCH();
+    k_bucket_bytes<<<grid(rs.B + 1, 256), 256, 0, st>>>(rs.B, rs.bucket_start, out.rec_off, out.bucket_off);
+    CDBG_CHECK_LAUNCH();
+}
+
+void parse_records(uint8_t const* bytes, uint64_t nbytes, uint64_t const* chunk_off,
+                   uint32_t const* chunk_bucket, uint32_t nchunks, uint32_t B, dev_arena& A,
+                   cudaStream_t st, record_set& rs, uint32_t* d_err) {
+    (void)nbytes;
+    rs = record_set();
+    rs.B = B;
+    rs.words = reinterpret_cast<uint64_t const*>(bytes);
+    rs.nwords = (nbytes + 7) / 8;
+    rs.bucket_start = A.alloc<uint64_t>(B + 1);
+    uint64_t* nrec = A.alloc<uint64_t>(nchunks + 1);
+    uint64_t* ncol = A.alloc<uint64_t>(nchunks + 1);
+    uint64_t* rbase = A.alloc<uint64_t>(nchunks + 1);
+    uint64_t* cbase = A.alloc<uint64_t>(nchunks + 1);
+    if (nchunks) {
+        k_parse_chunks<false><<<grid(nchunks, 64), 64, 0, st>>>(bytes, chunk_off, nchunks, nrec, ncol,
+                                                                 nullptr, nullptr, nullptr, nullptr,
+                                                                 nullptr, nullptr, nullptr, d_err);
+        CDBG_CHECK_LAUNCH();
+    }
+    prim::exclusive_scan<uint64_t, uint64_t>(nrec, rbase, nchunks, A, st, rbase + nchunks);
+    prim::exclusive_scan<uint64_t, uint64_t>(ncol, cbase, nchunks, A, st, cbase + nchunks);
+    uint64_t t[2];
+    CDBG_CUDA(cudaMemcpyAsync(&t[0], rbase + nchunks, 8, cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaMemcpyAsync(&t[1], cbase + nchunks, 8, cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    rs.n = t[0];
+    rs.ncolors = t[1];
+    rs.start = A.alloc<uint64_t>(rs.n);
+    rs.len = A.alloc<uint32_t>(rs.n);
+    rs.flags = A.alloc<uint32_t>(rs.n);
+    rs.col_off = A.alloc<uint64_t>(rs.n + 1);
+    rs.colors = A.alloc<uint32_t>(rs.ncolors);
+    if (nchunks) {
+        k_parse_chunks<true><<<grid(nchunks, 64), 64, 0, st>>>(bytes, chunk_off, nchunks, nrec, ncol, rbase,
+                                                                cbase, rs.start, rs.len, rs.flags,
+                                                                rs.col_off, rs.colors, d_err);
+        CDBG_CHECK_LAUNCH();
+    }
+    k_set_last_u64<<<1, 1, 0, st>>>(rs.col_off, rs.n, cbase + nchunks);
+    CDBG_CHECK_LAUNCH();
+    unsigned long long* bc = A.alloc<unsigned long long>(B);
+    CDBG_CUDA(cudaMemsetAsync(bc, 0, 8ull * B, st));
+    if (nchunks) {
+        k_chunk_bucket_counts<<<grid(nchunks, 256), 256, 0, st>>>(nchunks, chunk_bucket, nrec, bc);
+        CDBG_CHECK_LAUNCH();
+    }
+    prim::exclusive_scan<unsigned long long, uint64_t>(bc, rs.bucket_start, B, A, st, rs.bucket_start + B);
+}
+
+}  // namespace cdbg

@@ -1,0 +1,1697 @@
+// Phase 2 (bucket-process) kernels for sm_100a.
+//
+// Restates phase2_bucket_process/bucket_walker.hpp:166-779 on the device.
+// Buckets are processed in batches (consecutive buckets whose k-mer
+// occurrences fit a budget); every batch runs the same stages:
+//
+//  load     one thread per k-mer occurrence rolls its canonical k-mer straight
+//           from the 2-bit record stream and aggregates it into its bucket's
+//           open-addressing table (load_bucket, bucket_walker.hpp:166-255):
+//           boundary side bits OR-ed, `primary` OR-ed, owned records' min/max
+//           record id, and the first-insertion rank (record, index) by atomicMin.
+//  nodes    distinct k-mers are numbered in first-insertion order -- the
+//           iteration order of the reference's insertion-ordered map, which is
+//           its seed and class order -- by marking each k-mer's first
+//           occurrence in a bitmap over the batch's occurrences and scanning it.
+//  resolve  a primary k-mer owned by one record has that record's color set;
+//           one owned by several records gets the union of their sets
+//           (bucket_walker.hpp:360-428), built in a per-warp shared-memory
+//           bitmap.  Sets are hashed (order-independent 64-bit set hash) and
+//           interned in a global device dictionary with full list equality;
+//           new classes get global ids in order of first appearance (bucket,
+//           then insertion rank), which is the id order of the reference's
+//           streaming_color_set_dict when buckets are merged in order
+//           (bucket_walker.hpp:713-757, streaming_color_set_dict.hpp:148-182).
+//           New classes are hybrid-encoded (hybrid_color_sets.hpp:48-95) into
+//           the .color_sets bit vector.
+//  walk     8-neighbour extension masks (local_ext_mask, :260-271) and the
+//           clean-step links of walk_step (:317-336).  Clean links pair the
+//           ports of k-mers into disjoint chains (paths and cycles); one thread
+//           per chain replays the reference's sequential seed loop restricted
+//           to that chain (emit_from_seed, :451-566): seeds in insertion order,
+//           a shared visited set, contig-break stops and the seed shortcuts.
+//           Chains never interact, so this equals the whole-bucket loop.
+//  emit     fragments in seed order, serialized in the frag_unitig_writer
+//           record layout (unitig_spill.hpp:491-522) with global class ids.
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "device_kmer.cuh"
+#include "phase2.cuh"
+#include "primitives.cuh"
+
+namespace cdbg {
+
+namespace {
+
+constexpr uint32_t NONE32 = 0xffffffffu;
+constexpr uint32_t MULTI_TAG = 0x80000000u;
+constexpr uint32_t M_LEFT = 1, M_RIGHT = 2, M_PRIMARY = 4;
+constexpr uint32_t SK_BEGIN = 1, SK_END = 2, SK_OWNS_FIRST = 4, SK_OWNS_LAST = 8;
+constexpr uint64_t HASH_EMPTY = ~0ull;
+
+inline unsigned grid(uint64_t n, unsigned t) { return (unsigned)ceil_div(n, t); }
+
+template <typename T>
+T read_dev(T const* p, cudaStream_t st) {
+    T v;
+    CDBG_CUDA(cudaMemcpyAsync(&v, p, sizeof(T), cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    return v;
+}
+
+// Growable device array (class dictionary storage that outlives batches).
+template <typename T>
+struct dvec {
+    T* p = nullptr;
+    size_t n = 0, cap = 0;
+    dvec() = default;
+    dvec(dvec const&) = delete;
+    ~dvec() {
+        if (p) cudaFree(p);
+    }
+    void reserve(size_t c, cudaStream_t st, bool zero_new = false) {
+        if (c <= cap) return;
+        size_t nc = std::max<size_t>(c, std::max<size_t>(cap * 2, 1024));
+        T* q = nullptr;
+        CDBG_CUDA(cudaMalloc(&q, nc * sizeof(T)));
+        if (n) CDBG_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        if (zero_new) CDBG_CUDA(cudaMemsetAsync(q + n, 0, (nc - n) * sizeof(T), st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        if (p) cudaFree(p);
+        p = q;
+        cap = nc;
+    }
+};
+
+__device__ __forceinline__ uint32_t upper_bound_u64(uint64_t const* a, uint64_t n, uint64_t x) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return (uint32_t)lo;
+}
+
+// ------------------------------------------------------------------ set hash
+__host__ __device__ __forceinline__ uint64_t elem_mix(uint32_t c) {
+    return mix64((uint64_t)c * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL);
+}
+__host__ __device__ __forceinline__ uint64_t set_hash_final(uint64_t acc, uint64_t n) {
+    uint64_t h = mix64(acc ^ (n * 0xD6E8FEB86659FD93ULL));
+    return h == HASH_EMPTY ? HASH_EMPTY - 1 : h;
+}
+
+// ------------------------------------------------------------------ tables
+__device__ __forceinline__ uint64_t key_cas(uint64_t* a, uint64_t cmp, uint64_t val) {
+    return (uint64_t)atomicCAS((unsigned long long*)a, (unsigned long long)cmp, (unsigned long long)val);
+}
+__device__ __forceinline__ u128 key_cas(u128* a, u128 cmp, u128 val) {
+    uint64_t olo, ohi;
+    const uint64_t clo = (uint64_t)cmp, chi = (uint64_t)(cmp >> 64);
+    const uint64_t vlo = (uint64_t)val, vhi = (uint64_t)(val >> 64);
+    asm volatile(
+        "{\n\t.reg .b128 d, c, v;\n\t"
+        "mov.b128 c, {%2, %3};\n\t"
+        "mov.b128 v, {%4, %5};\n\t"
+        "atom.global.cas.b128 d, [%6], c, v;\n\t"
+        "mov.b128 {%0, %1}, d;\n\t}"
+        : "=l"(olo), "=l"(ohi)
+        : "l"(clo), "l"(chi), "l"(vlo), "l"(vhi), "l"(a)
+        : "memory");
+    return ((u128)ohi << 64) | (u128)olo;
+}
+__device__ __forceinline__ uint64_t key_load(uint64_t const* a) { return *(volatile uint64_t const*)a; }
+__device__ __forceinline__ u128 key_load(u128 const* a) {
+    const ulonglong2 v = *reinterpret_cast<ulonglong2 const*>(a);
+    return ((u128)v.y << 64) | (u128)v.x;
+}
+
+// Insert-or-find; returns the slot (absolute) or NONE64 when the region is full.
+template <typename K>
+__device__ __forceinline__ uint64_t table_upsert(K* keys, uint64_t off, uint64_t cap, K x) {
+    const K EMPTY = kmer_ops<K>::empty();
+    uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
+    for (uint64_t i = 0; i < cap; ++i) {
+        K* a = keys + off + s;
+        if (sizeof(K) == 8) {
+            const K cur = key_load(a);
+            if (cur == x) return off + s;
+            if (cur == EMPTY) {
+                const K old = key_cas(a, EMPTY, x);
+                if (old == EMPTY || old == x) return off + s;
+            }
+        } else {
+            const K old = key_cas(a, EMPTY, x);  // atomic 128-bit read-or-claim
+            if (old == EMPTY || old == x) return off + s;
+        }
+        if (++s == cap) s = 0;
+    }
+    return ~0ull;
+}
+
+template <typename K>
+__device__ __forceinline__ uint64_t table_find(K const* keys, uint64_t off, uint64_t cap, K x) {
+    const K EMPTY = kmer_ops<K>::empty();
+    uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
+    for (uint64_t i = 0; i < cap; ++i) {
+        const K cur = key_load(keys + off + s);
+        if (cur == x) return off + s;
+        if (cur == EMPTY) return ~0ull;
+        if (++s == cap) s = 0;
+    }
+    return ~0ull;
+}
+
+struct rec_view {
+    uint64_t const* start;
+    uint32_t const* len;
+    uint32_t const* flags;
+    uint64_t const* col_off;
+    uint32_t const* colors;
+    uint32_t const* bucket;   // per record
+    uint64_t const* occ;      // n + 1 exclusive prefix of k-mers per record
+    uint64_t const* words;
+};
+
+template <typename K>
+struct tables {
+    K* key;
+    uint32_t* meta;
+    unsigned long long* rank;
+    uint32_t* rmin;
+    uint32_t* rmax;
+    uint32_t* node;
+    uint64_t const* tab_off;  // per batch bucket
+    uint64_t const* tab_cap;
+    uint32_t b0;
+};
+
+// Occurrence o of the batch -> (record, index, canonical k-mer, contrib, owned).
+template <typename K>
+struct occ_info {
+    uint32_t r;
+    uint32_t idx;
+    K can;
+    uint32_t contrib;
+    bool owned;
+};
+
+template <typename K>
+__device__ __forceinline__ occ_info<K> decode_occ(rec_view const& R, uint64_t R0, uint64_t nrec,
+                                                  uint64_t o, uint32_t k) {
+    occ_info<K> oi;
+    const uint32_t rr = upper_bound_u64(R.occ + R0, nrec + 1, o) - 1;
+    const uint64_t r = R0 + rr;
+    oi.r = (uint32_t)r;
+    oi.idx = (uint32_t)(o - R.occ[r]);
+    const uint32_t nk = R.len[r] - k + 1;
+    const uint32_t f = R.flags[r];
+    K fwd, rc;
+    kmer_ops<K>::load(R.words, R.start[r] + oi.idx, k, fwd, rc);
+    const bool isf = fwd <= rc;
+    oi.can = isf ? fwd : rc;
+    uint32_t contrib = 0;
+    if (!(f & SK_BEGIN) && oi.idx == 0) contrib |= isf ? M_LEFT : M_RIGHT;
+    if (!(f & SK_END) && oi.idx == nk - 1) contrib |= isf ? M_RIGHT : M_LEFT;
+    oi.contrib = contrib;
+    oi.owned = !((oi.idx == 0 && !(f & SK_OWNS_FIRST)) || (oi.idx == nk - 1 && !(f & SK_OWNS_LAST)));
+    return oi;
+}
+
+// ------------------------------------------------------------------ kernels
+__global__ void k_rec_prep(uint64_t n, uint32_t const* __restrict__ len, uint32_t k,
+                           uint64_t const* __restrict__ bstart, uint32_t B,
+                           uint64_t* __restrict__ nk, uint32_t* __restrict__ rbucket,
+                           uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors,
+                           uint64_t* __restrict__ rhash) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t l = len[r];
+    nk[r] = l >= k ? (uint64_t)(l - k + 1) : 0;
+    rbucket[r] = upper_bound_u64(bstart, (uint64_t)B + 1, r) - 1;
+    uint64_t acc = 0;
+    const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
+    for (uint64_t c = c0; c < c1; ++c) acc += elem_mix(colors[c]);
+    rhash[r] = set_hash_final(acc, c1 - c0);
+}
+
+__global__ void k_gather_u64(uint64_t n, uint64_t const* __restrict__ src,
+                             uint64_t const* __restrict__ idx, uint64_t* __restrict__ out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = src[idx[i]];
+}
+
+template <typename K>
+__global__ void k_init_tables(uint64_t T, K* key, uint32_t* meta, unsigned long long* rank,
+                              uint32_t* rmin, uint32_t* rmax) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T) return;
+    key[i] = kmer_ops<K>::empty();
+    meta[i] = 0;
+    rank[i] = ~0ull;
+    rmin[i] = NONE32;
+    rmax[i] = 0;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_t R0, uint64_t nrec,
+                                                uint64_t O0, uint64_t nocc, uint32_t k, uint32_t* err) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nocc) return;
+    const occ_info<K> oi = decode_occ<K>(R, R0, nrec, O0 + t, k);
+    const uint32_t tb = R.bucket[oi.r] - T.b0;
+    const uint64_t s = table_upsert<K>(T.key, T.tab_off[tb], T.tab_cap[tb], oi.can);
+    if (s == ~0ull) {
+        set_error(err, ERR_TABLE_FULL);
+        return;
+    }
+    const uint32_t mo = oi.contrib | (oi.owned ? M_PRIMARY : 0u);
+    if (mo && (T.meta[s] & mo) != mo) atomicOr(&T.meta[s], mo);
+    const unsigned long long rk = ((unsigned long long)oi.r << 32) | oi.idx;
+    if (rk < T.rank[s]) atomicMin(&T.rank[s], rk);
+    if (oi.owned) {
+        if (oi.r < T.rmin[s]) atomicMin(&T.rmin[s], oi.r);
+        if (oi.r > T.rmax[s]) atomicMax(&T.rmax[s], oi.r);
+    }
+}
+
+// Bit q of `bits` <- first occurrence of each distinct k-mer.
+template <typename K>
+__global__ void k_firstbits(uint64_t T, K const* __restrict__ key, unsigned long long const* __restrict__ rank,
+                            uint64_t const* __restrict__ occ, uint64_t O0, uint32_t* __restrict__ bits) {
+    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= T || key[s] == kmer_ops<K>::empty()) return;
+    const unsigned long long rk = rank[s];
+    const uint64_t q = occ[rk >> 32] + (rk & 0xffffffffull) - O0;
+    atomicOr(&bits[q >> 5], 1u << (q & 31));
+}
+
+__global__ void k_popc(uint64_t n, uint32_t const* __restrict__ bits, uint32_t* __restrict__ cnt) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cnt[i] = __popc(bits[i]);
+}
+
+template <typename K>
+__global__ void k_make_nodes(uint64_t T, K const* __restrict__ key, uint32_t const* __restrict__ meta,
+                             unsigned long long const* __restrict__ rank, uint32_t const* __restrict__ rmin,
+                             uint32_t const* __restrict__ rmax, uint64_t const* __restrict__ occ, uint64_t O0,
+                             uint32_t const* __restrict__ bits, uint64_t const* __restrict__ wpre,
+                             uint32_t const* __restrict__ rbucket, uint32_t* __restrict__ node_of_slot,
+                             K* __restrict__ n_key, uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
+                             uint32_t* __restrict__ n_bucket) {
+    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= T || key[s] == kmer_ops<K>::empty()) return;
+    const unsigned long long rk = rank[s];
+    const uint64_t q = occ[rk >> 32] + (rk & 0xffffffffull) - O0;
+    const uint32_t w = bits[q >> 5];
+    const uint64_t n = wpre[q >> 5] + __popc(w & ((1u << (q & 31)) - 1u));
+    node_of_slot[s] = (uint32_t)n;
+    n_key[n] = key[s];
+    const uint32_t m = meta[s];
+    n_meta[n] = (uint8_t)m;
+    uint32_t rec = NONE32;
+    if (m & M_PRIMARY) rec = (rmin[s] == rmax[s]) ? rmin[s] : MULTI_TAG;
+    n_rec[n] = rec;
+    n_bucket[n] = rbucket[rk >> 32];
+}
+
+// (node << 32 | record) for owned occurrences of multi-record k-mers.
+template <typename K, bool WRITE>
+__global__ void __launch_bounds__(256)
+    k_multi_pairs(rec_view R, tables<K> T, uint64_t R0, uint64_t nrec, uint64_t O0, uint64_t nocc,
+                  uint32_t k, uint32_t const* __restrict__ n_rec, unsigned long long* __restrict__ cnt,
+                  uint64_t* __restrict__ pairs) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool emit = false;
+    uint64_t val = 0;
+    if (t < nocc) {
+        const occ_info<K> oi = decode_occ<K>(R, R0, nrec, O0 + t, k);
+        if (oi.owned) {
+            const uint32_t tb = R.bucket[oi.r] - T.b0;
+            const uint64_t s = table_find<K>(T.key, T.tab_off[tb], T.tab_cap[tb], oi.can);
+            if (s != ~0ull) {
+                const uint32_t n = T.node[s];
+                if (n_rec[n] == MULTI_TAG) {
+                    emit = true;
+                    val = ((uint64_t)n << 32) | oi.r;
+                }
+            }
+        }
+    }
+    // warp-aggregated counter reservation
+    const uint32_t b = __ballot_sync(0xffffffffu, emit);
+    if (!b) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(b) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(cnt, (unsigned long long)__popc(b));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (WRITE && emit) pairs[base + __popc(b & lanemask_lt())] = val;
+}
+
+__global__ void k_unique_heads(uint64_t n, uint64_t const* __restrict__ a, uint32_t* __restrict__ keep) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keep[i] = (i == 0 || a[i] != a[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_compact_u64(uint64_t n, uint64_t const* __restrict__ a, uint32_t const* __restrict__ keep,
+                              uint64_t const* __restrict__ pos, uint64_t* __restrict__ out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && keep[i]) out[pos[i]] = a[i];
+}
+
+__global__ void k_node_heads(uint64_t n, uint64_t const* __restrict__ a, uint32_t* __restrict__ head) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) head[i] = (i == 0 || (a[i] >> 32) != (a[i - 1] >> 32)) ? 1u : 0u;
+}
+
+// Multi-record nodes: m-th head -> node id, record range [moff[m], moff[m+1]).
+__global__ void k_multi_index(uint64_t n, uint64_t const* __restrict__ a, uint32_t const* __restrict__ head,
+                              uint64_t const* __restrict__ hpos, uint32_t* __restrict__ mnode,
+                              uint64_t* __restrict__ moff, uint32_t* __restrict__ n_rec) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !head[i]) return;
+    const uint64_t m = hpos[i];
+    const uint32_t node = (uint32_t)(a[i] >> 32);
+    mnode[m] = node;
+    moff[m] = i;
+    n_rec[node] = MULTI_TAG | (uint32_t)m;
+}
+
+// Warp-level helpers over a per-warp shared-memory bitmap of C bits.
+__device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ uint32_t warp_excl_scan32(uint32_t v, uint32_t& total) {
+    const int lane = threadIdx.x & 31;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+__device__ __forceinline__ uint64_t warp_excl_scan64(uint64_t v, uint64_t& total) {
+    const int lane = threadIdx.x & 31;
+    uint64_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+// Union of the color lists of a multi-record node.  Pass 0: size and hash;
+// pass 1: write the ascending list at pool[poff[m]].
+template <bool WRITE>
+__global__ void k_union(uint64_t M, uint64_t const* __restrict__ moff, uint64_t const* __restrict__ upairs,
+                        uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors,
+                        uint32_t C, uint32_t* __restrict__ msize, uint64_t* __restrict__ mhash,
+                        uint64_t const* __restrict__ poff, uint32_t* __restrict__ pool) {
+    extern __shared__ uint32_t smem_bm[];
+    const uint32_t nw = (C + 31) / 32;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* bm = smem_bm + (size_t)wib * nw;
+    const uint64_t m = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (m >= M) return;
+    for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
+    __syncwarp();
+    for (uint64_t p = moff[m]; p < moff[m + 1]; ++p) {
+        const uint32_t r = (uint32_t)(upairs[p] & 0xffffffffu);
+        const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
+        for (uint64_t c = c0 + lane; c < c1; c += 32) {
+            const uint32_t v = colors[c];
+            atomicOr(&bm[v >> 5], 1u << (v & 31));
+        }
+    }
+    __syncwarp();
+    const uint32_t per = (nw + 31) / 32;
+    const uint32_t w0 = lane * per, w1 = min(w0 + per, nw);
+    uint32_t cnt = 0;
+    uint64_t acc = 0;
+    for (uint32_t w = w0; w < w1; ++w) {
+        uint32_t x = bm[w];
+        cnt += __popc(x);
+        if (!WRITE)
+            while (x) {
+                const uint32_t b = __ffs(x) - 1;
+                x &= x - 1;
+                acc += elem_mix(w * 32 + b);
+            }
+    }
+    uint32_t total;
+    const uint32_t ex = warp_excl_scan32(cnt, total);
+    if (!WRITE) {
+        acc = warp_sum64(acc);
+        if (lane == 0) {
+            msize[m] = total;
+            mhash[m] = set_hash_final(acc, total);
+        }
+    } else {
+        uint32_t* out = pool + poff[m] + ex;
+        for (uint32_t w = w0; w < w1; ++w) {
+            uint32_t x = bm[w];
+            while (x) {
+                const uint32_t b = __ffs(x) - 1;
+                x &= x - 1;
+                *out++ = w * 32 + b;
+            }
+        }
+    }
+}
+
+// rec_first[r] = smallest node index whose color set is record r's list.
+__global__ void k_rec_first(uint64_t D, uint32_t const* __restrict__ n_rec, uint32_t R0,
+                            uint32_t* __restrict__ rec_first) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D) return;
+    const uint32_t r = n_rec[n];
+    if (r == NONE32 || (r & MULTI_TAG)) return;
+    atomicMin(&rec_first[r - R0], (uint32_t)n);
+}
+
+// Candidate class sources: used records then multi nodes.
+struct cand_view {
+    uint32_t* kind_id;   // record id (global) or MULTI_TAG | m
+    uint32_t* first;     // node of first appearance
+    uint64_t* hash;
+};
+
+__global__ void k_cand_records(uint64_t nrec, uint32_t R0, uint32_t const* __restrict__ rec_first,
+                               uint32_t const* __restrict__ keep, uint64_t const* __restrict__ pos,
+                               uint64_t const* __restrict__ rhash, cand_view cv, uint32_t* __restrict__ rec_cand) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrec || !keep[i]) return;
+    const uint64_t c = pos[i];
+    cv.kind_id[c] = R0 + (uint32_t)i;
+    cv.first[c] = rec_first[i];
+    cv.hash[c] = rhash[R0 + i];
+    rec_cand[i] = (uint32_t)c;
+}
+
+__global__ void k_cand_multi(uint64_t M, uint64_t base, uint32_t const* __restrict__ mnode,
+                             uint64_t const* __restrict__ mhash, cand_view cv) {
+    uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    cv.kind_id[base + m] = MULTI_TAG | (uint32_t)m;
+    cv.first[base + m] = mnode[m];
+    cv.hash[base + m] = mhash[m];
+}
+
+struct list_src {
+    uint64_t const* col_off;
+    uint32_t const* colors;
+    uint64_t const* poff;
+    uint32_t const* pool;
+    uint32_t const* msize;
+};
+__device__ __forceinline__ void cand_list(list_src const& L, uint32_t kind_id, uint32_t const*& p, uint64_t& n) {
+    if (kind_id & MULTI_TAG) {
+        const uint32_t m = kind_id & ~MULTI_TAG;
+        p = L.pool + L.poff[m];
+        n = L.msize[m];
+    } else {
+        p = L.colors + L.col_off[kind_id];
+        n = L.col_off[kind_id + 1] - L.col_off[kind_id];
+    }
+}
+__device__ __forceinline__ bool lists_equal(uint32_t const* a, uint64_t na, uint32_t const* b, uint64_t nb) {
+    if (na != nb) return false;
+    for (uint64_t i = 0; i < na; ++i)
+        if (a[i] != b[i]) return false;
+    return true;
+}
+
+struct dict_view {
+    uint64_t* slot_hash;
+    uint32_t* slot_cid;
+    uint64_t mask;
+    uint64_t const* cls_off;  // list offsets into cls_pool
+    uint32_t const* cls_pool;
+};
+
+__global__ void k_dict_lookup(uint64_t nc, cand_view cv, list_src L, dict_view D, uint32_t* __restrict__ cid) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const uint64_t h = cv.hash[c];
+    uint32_t const* lp;
+    uint64_t ln;
+    cand_list(L, cv.kind_id[c], lp, ln);
+    uint32_t res = NONE32;
+    if (D.slot_hash) {
+        uint64_t s = h & D.mask;
+        for (uint64_t i = 0; i <= D.mask; ++i) {
+            const uint64_t sh = D.slot_hash[s];
+            if (sh == HASH_EMPTY) break;
+            if (sh == h) {
+                const uint32_t k = D.slot_cid[s];
+                const uint64_t a = D.cls_off[k], b = D.cls_off[k + 1];
+                if (lists_equal(lp, ln, D.cls_pool + a, b - a)) {
+                    res = k;
+                    break;
+                }
+            }
+            s = (s + 1) & D.mask;
+        }
+    }
+    cid[c] = res;
+}
+
+__global__ void k_new_flags(uint64_t nc, uint32_t const* __restrict__ cid, uint32_t* __restrict__ flag) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) flag[c] = cid[c] == NONE32 ? 1u : 0u;
+}
+
+__global__ void k_new_gather(uint64_t nc, uint32_t const* __restrict__ flag, uint64_t const* __restrict__ pos,
+                             cand_view cv, uint64_t* __restrict__ nkey, uint32_t* __restrict__ nidx) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc || !flag[c]) return;
+    nkey[pos[c]] = cv.hash[c];
+    nidx[pos[c]] = (uint32_t)c;
+}
+
+__global__ void k_run_heads(uint64_t n, uint64_t const* __restrict__ key, uint32_t* __restrict__ head) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) head[i] = (i == 0 || key[i] != key[i - 1]) ? 1u : 0u;
+}
+
+// One thread per equal-hash run of new candidates: group members by list
+// equality (normally one group per run); rep[i] = representative candidate.
+__global__ void k_group_runs(uint64_t n, uint64_t const* __restrict__ key, uint32_t const* __restrict__ head,
+                             uint32_t const* __restrict__ nidx, cand_view cv, list_src L,
+                             uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !head[i]) return;
+    uint64_t e = i + 1;
+    while (e < n && !head[e]) ++e;
+    // members [i, e); reps are members whose rep is themselves
+    for (uint64_t j = i; j < e; ++j) {
+        const uint32_t cj = nidx[j];
+        uint32_t const* pj;
+        uint64_t lj;
+        cand_list(L, cv.kind_id[cj], pj, lj);
+        uint32_t r = cj;
+        for (uint64_t q = i; q < j; ++q) {
+            const uint32_t cq = nidx[q];
+            if (rep[cq] != cq) continue;
+            uint32_t const* pq;
+            uint64_t lq;
+            cand_list(L, cv.kind_id[cq], pq, lq);
+            if (lists_equal(pj, lj, pq, lq)) {
+                r = cq;
+                break;
+            }
+        }
+        rep[cj] = r;
+        const uint32_t f = cv.first[cj];
+        if (r == cj)
+            rep_first[cj] = f;
+        else if (f < rep_first[r])
+            rep_first[r] = f;
+    }
+}
+
+__global__ void k_rep_keys(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
+                           uint32_t const* __restrict__ rep_first, uint32_t* __restrict__ is_rep) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = nidx[i];
+    is_rep[i] = rep[c] == c ? 1u : 0u;
+    (void)rep_first;
+}
+
+__global__ void k_rep_gather(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ is_rep,
+                             uint64_t const* __restrict__ pos, uint32_t const* __restrict__ rep_first,
+                             uint64_t* __restrict__ rkey, uint32_t* __restrict__ rcand) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !is_rep[i]) return;
+    const uint32_t c = nidx[i];
+    rkey[pos[i]] = rep_first[c];
+    rcand[pos[i]] = c;
+}
+
+// New class j (in first-appearance order) = candidate rcand[j]; cid base+j.
+__global__ void k_assign_new(uint64_t nnew, uint32_t const* __restrict__ rcand, uint64_t base,
+                             uint32_t* __restrict__ cid) {
+    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < nnew) cid[rcand[j]] = (uint32_t)(base + j);
+}
+
+__global__ void k_assign_members(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
+                                 uint32_t* __restrict__ cid) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = nidx[i];
+    if (rep[c] != c) cid[c] = cid[rep[c]];
+}
+
+__global__ void k_new_sizes(uint64_t nnew, uint32_t const* __restrict__ rcand, cand_view cv, list_src L,
+                            uint64_t* __restrict__ sz, uint64_t* __restrict__ hashes) {
+    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nnew) return;
+    uint32_t const* p;
+    uint64_t n;
+    cand_list(L, cv.kind_id[rcand[j]], p, n);
+    sz[j] = n;
+    hashes[j] = cv.hash[rcand[j]];
+}
+
+// Copy new class lists into the dictionary pool (warp per class).
+__global__ void k_new_copy(uint64_t nnew, uint32_t const* __restrict__ rcand, cand_view cv, list_src L,
+                           uint64_t const* __restrict__ dst_off, uint32_t* __restrict__ pool) {
+    const uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (j >= nnew) return;
+    uint32_t const* p;
+    uint64_t n;
+    cand_list(L, cv.kind_id[rcand[j]], p, n);
+    uint32_t* d = pool + dst_off[j];
+    for (uint64_t i = threadIdx.x & 31; i < n; i += 32) d[i] = p[i];
+}
+
+__global__ void k_dict_insert(uint64_t c0, uint64_t c1, uint64_t const* __restrict__ cls_hash,
+                              uint64_t* __restrict__ slot_hash, uint32_t* __restrict__ slot_cid, uint64_t mask,
+                              uint32_t* err) {
+    uint64_t c = c0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c1) return;
+    const uint64_t h = cls_hash[c];
+    uint64_t s = h & mask;
+    for (uint64_t i = 0; i <= mask; ++i) {
+        const uint64_t old = atomicCAS((unsigned long long*)&slot_hash[s], (unsigned long long)HASH_EMPTY,
+                                       (unsigned long long)h);
+        if (old == HASH_EMPTY) {
+            slot_cid[s] = (uint32_t)c;
+            return;
+        }
+        s = (s + 1) & mask;
+    }
+    set_error(err, ERR_TABLE_FULL);
+}
+
+// ---- hybrid encoding (hybrid_color_sets.hpp:48-95) with the delta code of
+// this project's `bits` stand-in: delta(x) = Elias delta of x + 1, LSB-first.
+__device__ __forceinline__ uint32_t msb64(uint64_t y) { return 63u - (uint32_t)__clzll((long long)y); }
+__device__ __forceinline__ uint32_t delta_bits(uint64_t x) {
+    const uint64_t y = x + 1;
+    const uint32_t l = msb64(y);
+    const uint32_t ll = msb64(l + 1);
+    return 2 * ll + 1 + l;
+}
+__device__ __forceinline__ void or_bits(uint64_t* w, uint64_t pos, uint64_t val, uint32_t len) {
+    if (len == 0) return;
+    if (len < 64) val &= (1ull << len) - 1;
+    const uint64_t i = pos >> 6;
+    const uint32_t s = (uint32_t)(pos & 63);
+    atomicOr((unsigned long long*)&w[i], (unsigned long long)(val << s));
+    if (s && s + len > 64) atomicOr((unsigned long long*)&w[i + 1], (unsigned long long)(val >> (64 - s)));
+}
+__device__ __forceinline__ uint64_t put_delta(uint64_t* w, uint64_t pos, uint64_t x) {
+    const uint64_t y = x + 1;
+    const uint32_t l = msb64(y);
+    const uint64_t L1 = l + 1;
+    const uint32_t ll = msb64(L1);
+    // gamma(L1): ll zeros, a one, the low ll bits of L1
+    const uint64_t g = (1ull << ll) | ((L1 & ((1ull << ll) - 1)) << (ll + 1));
+    or_bits(w, pos, g, 2 * ll + 1);
+    pos += 2 * ll + 1;
+    if (l) or_bits(w, pos, y, l);
+    return pos + l;
+}
+
+// Warp per new class.  Pass 0 (ENC = false): encoded size -> bits[j].
+// Pass 1: write at bit offset boff[j] of `words`.
+template <bool ENC>
+__global__ void k_encode(uint64_t nnew, uint64_t const* __restrict__ off, uint32_t const* __restrict__ pool,
+                         uint32_t C, uint64_t* __restrict__ nbits, uint64_t const* __restrict__ boff,
+                         uint64_t* __restrict__ words) {
+    extern __shared__ uint32_t smem_bm[];
+    const uint32_t nw = (C + 31) / 32;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* bm = smem_bm + (size_t)wib * nw;
+    const uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (j >= nnew) return;
+    const uint64_t a = off[j], N = off[j + 1] - off[j];
+    for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
+    __syncwarp();
+    for (uint64_t i = lane; i < N; i += 32) {
+        const uint32_t v = pool[a + i];
+        atomicOr(&bm[v >> 5], 1u << (v & 31));
+    }
+    __syncwarp();
+    const uint64_t sparse_t = (uint64_t)(0.25 * (double)C);
+    const uint64_t dense_t = (uint64_t)(0.75 * (double)C);
+    uint64_t pos = ENC ? boff[j] : 0;
+    const uint32_t hdr = delta_bits(N);
+    if (ENC && lane == 0) put_delta(words, pos, N);
+    pos += hdr;
+    if (N >= sparse_t && N < dense_t) {
+        // plain C-bit bitmap
+        if (ENC)
+            for (uint32_t w = lane; w < nw; w += 32) {
+                const uint32_t len = min(32u, C - w * 32);
+                or_bits(words, pos + (uint64_t)w * 32, bm[w], len);
+            }
+        if (!ENC && lane == 0) nbits[j] = hdr + C;
+        return;
+    }
+    const bool want_ones = N < sparse_t;  // else complement: values not in the set
+    const uint32_t per = (nw + 31) / 32;
+    const uint32_t w0 = lane * per, w1 = min(w0 + per, nw);
+    auto word_bits = [&](uint32_t w) -> uint32_t {
+        uint32_t x = want_ones ? bm[w] : ~bm[w];
+        const uint32_t valid = C - w * 32;
+        if (valid < 32) x &= (1u << valid) - 1u;
+        return x;
+    };
+    // last element of this lane's range
+    int32_t last = -1;
+    for (uint32_t w = w0; w < w1; ++w) {
+        const uint32_t x = word_bits(w);
+        if (x) last = (int32_t)(w * 32 + 31 - __clz(x));
+    }
+    // previous element before this lane's range = max of `last` over lower lanes
+    int32_t prev = -1;
+    {
+        int32_t x = last;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x = max(x, y);
+        }
+        prev = __shfl_up_sync(0xffffffffu, x, 1);
+        if (lane == 0) prev = -1;
+    }
+    // code lengths of this lane's elements
+    uint64_t mybits = 0;
+    {
+        int32_t pv = prev;
+        for (uint32_t w = w0; w < w1; ++w) {
+            uint32_t x = word_bits(w);
+            while (x) {
+                const uint32_t b = __ffs(x) - 1;
+                x &= x - 1;
+                const int32_t v = (int32_t)(w * 32 + b);
+                mybits += delta_bits(pv < 0 ? (uint64_t)v : (uint64_t)(v - pv - 1));
+                pv = v;
+            }
+        }
+    }
+    uint64_t total;
+    const uint64_t ex = warp_excl_scan64(mybits, total);
+    if (!ENC) {
+        if (lane == 0) nbits[j] = hdr + total;
+        return;
+    }
+    uint64_t p = pos + ex;
+    int32_t pv = prev;
+    for (uint32_t w = w0; w < w1; ++w) {
+        uint32_t x = word_bits(w);
+        while (x) {
+            const uint32_t b = __ffs(x) - 1;
+            x &= x - 1;
+            const int32_t v = (int32_t)(w * 32 + b);
+            p = put_delta(words, p, pv < 0 ? (uint64_t)v : (uint64_t)(v - pv - 1));
+            pv = v;
+        }
+    }
+}
+
+__global__ void k_node_cid(uint64_t D, uint32_t const* __restrict__ n_rec, uint32_t R0,
+                           uint32_t const* __restrict__ rec_cand, uint64_t mbase,
+                           uint32_t const* __restrict__ cid, uint32_t* __restrict__ n_cid) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D) return;
+    const uint32_t r = n_rec[n];
+    uint32_t c = NONE32;
+    if (r != NONE32) c = (r & MULTI_TAG) ? cid[mbase + (r & ~MULTI_TAG)] : cid[rec_cand[r - R0]];
+    n_cid[n] = c;
+}
+
+// ---- extension masks and clean links -------------------------------------
+template <typename K>
+__device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb, K x) {
+    const uint64_t s = table_find<K>(T.key, T.tab_off[tb], T.tab_cap[tb], x);
+    return s == ~0ull ? NONE32 : T.node[s];
+}
+
+template <typename K>
+__global__ void k_ext_mask(uint64_t D, tables<K> T, K const* __restrict__ n_key,
+                           uint32_t const* __restrict__ n_bucket, uint32_t k, uint8_t* __restrict__ n_mask) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D) return;
+    typedef kmer_ops<K> ops;
+    const K can = n_key[n];
+    const K msk = ops::mask(k);
+    const K rev = ops::revcomp(can, k);
+    const uint32_t tb = n_bucket[n] - T.b0;
+    uint32_t out = 0;
+#pragma unroll
+    for (uint32_t nt = 0; nt < 4; ++nt) {
+        K f = ((can << 2) | (K)nt) & msk;
+        K fr = ops::revcomp(f, k);
+        if (node_lookup<K>(T, tb, f <= fr ? f : fr) != NONE32) out |= 1u << nt;
+        K r = ((rev << 2) | (K)nt) & msk;
+        K rr = ops::revcomp(r, k);
+        if (node_lookup<K>(T, tb, r <= rr ? r : rr) != NONE32) out |= 1u << (4 + nt);
+    }
+    n_mask[n] = (uint8_t)out;
+}
+
+__device__ __forceinline__ uint32_t fwd_nib(uint32_t m, bool rc) { return (rc ? (m >> 4) : m) & 0xfu; }
+__device__ __forceinline__ uint32_t back_nib(uint32_t m, bool rc) { return (rc ? m : (m >> 4)) & 0xfu; }
+
+// link[2n] = L port, link[2n+1] = R port: (node << 1) | rc of the state
+// reached, NONE32 when the step is not clean.
+template <typename K>
+__global__ void k_links(uint64_t D, tables<K> T, K const* __restrict__ n_key, uint32_t const* __restrict__ n_bucket,
+                        uint8_t const* __restrict__ n_mask, uint32_t k, uint32_t* __restrict__ link) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D) return;
+    typedef kmer_ops<K> ops;
+    const K can = n_key[n];
+    const uint32_t m = n_mask[n];
+    const uint32_t tb = n_bucket[n] - T.b0;
+    const K msk = ops::mask(k);
+    // R: forward from (can, rc = false)
+    uint32_t lr = NONE32, ll = NONE32;
+    {
+        const uint32_t nib = fwd_nib(m, false);
+        if (__popc(nib) == 1) {
+            const uint32_t nt = __ffs(nib) - 1;
+            const K nf = ((can << 2) | (K)nt) & msk;
+            const K nr = ops::revcomp(nf, k);
+            const bool nrc = !(nf <= nr);
+            const uint32_t nn = node_lookup<K>(T, tb, nrc ? nr : nf);
+            if (nn != NONE32 && __popc(back_nib(n_mask[nn], nrc)) == 1) lr = (nn << 1) | (nrc ? 1u : 0u);
+        }
+    }
+    // L: backward from (can, rc = false) = bstep(can, rc = true) then flip
+    {
+        const uint32_t nib = back_nib(m, false);
+        if (__popc(nib) == 1) {
+            const uint32_t nt = __ffs(nib) - 1;
+            const K cur = ops::revcomp(can, k);
+            const K nf = ((cur << 2) | (K)nt) & msk;
+            const K nr = ops::revcomp(nf, k);
+            const bool srcc = !(nf <= nr);
+            const bool nrc = !srcc;
+            const uint32_t nn = node_lookup<K>(T, tb, srcc ? nr : nf);
+            if (nn != NONE32 && __popc(fwd_nib(n_mask[nn], nrc)) == 1) ll = (nn << 1) | (nrc ? 1u : 0u);
+        }
+    }
+    // a port linked to the node itself ends the chain (the reference's walk
+    // meets its own visited k-mer there)
+    if (lr != NONE32 && (lr >> 1) == (uint32_t)n) lr = NONE32;
+    if (ll != NONE32 && (ll >> 1) == (uint32_t)n) ll = NONE32;
+    link[2 * n] = ll;
+    link[2 * n + 1] = lr;
+}
+
+// ---- chains ---------------------------------------------------------------
+struct chain_ws {
+    uint32_t const* link;
+    uint8_t const* meta;
+    uint8_t const* mask;
+    uint32_t* ch_node;
+    uint8_t* ch_rc;
+    unsigned long long* ch_ord;
+    uint8_t* ch_vis;
+    uint32_t* fe;            // fragment elements (node << 1 | walk rc)
+    uint32_t* seed_start;    // per seed node: offset into fe
+    uint32_t* seed_len;      // per seed node: elements (0 = not a seed)
+    uint8_t* seed_open;
+    uint8_t* covered;
+    unsigned long long* cursor;
+    uint64_t D;
+};
+
+// Step forward from state (c, rc): use the R port when rc is false.
+__device__ __forceinline__ bool chain_step(uint32_t const* link, uint32_t& c, bool& rc) {
+    const uint32_t l = link[2 * (uint64_t)c + (rc ? 0 : 1)];
+    if (l == NONE32) return false;
+    c = l >> 1;
+    rc = ((l & 1u) != 0) != rc;
+    return true;
+}
+
+__device__ void heap_sort(unsigned long long* a, uint32_t n) {
+    auto sift = [&](uint32_t i, uint32_t len) {
+        for (;;) {
+            uint32_t l = 2 * i + 1, m = i;
+            if (l < len && a[l] > a[m]) m = l;
+            if (l + 1 < len && a[l + 1] > a[m]) m = l + 1;
+            if (m == i) return;
+            unsigned long long t = a[i];
+            a[i] = a[m];
+            a[m] = t;
+            i = m;
+        }
+    };
+    if (n < 2) return;
+    for (uint32_t i = n / 2; i-- > 0;) sift(i, n);
+    for (uint32_t e = n - 1; e > 0; --e) {
+        unsigned long long t = a[0];
+        a[0] = a[e];
+        a[e] = t;
+        sift(0, e);
+    }
+}
+
+// Replay the reference's seed loop on one chain stored at [c0, c0 + L).
+__device__ void simulate_chain(chain_ws const& W, uint64_t c0, uint32_t L, bool cyclic) {
+    uint32_t const* cn = W.ch_node + c0;
+    uint8_t const* crc = W.ch_rc + c0;
+    unsigned long long* ord = W.ch_ord + c0;
+    uint8_t* vis = W.ch_vis + c0;
+    for (uint32_t i = 0; i < L; ++i) {
+        ord[i] = ((unsigned long long)cn[i] << 32) | i;
+        vis[i] = 0;
+        W.covered[cn[i]] = 1;
+    }
+    heap_sort(ord, L);
+    uint64_t fcur = c0;
+    for (uint32_t t = 0; t < L; ++t) {
+        const uint32_t p = (uint32_t)(ord[t] & 0xffffffffu);
+        if (vis[p]) continue;
+        vis[p] = 1;
+        const uint32_t s = cn[p];
+        const int df = crc[p] ? -1 : 1;  // chain direction of the seed's canonical forward
+        const uint32_t sflags = W.meta[s] & 3u;
+        uint32_t nb = 0, nf = 0;
+        bool open_l = false, open_r = false;
+        for (int dir = 0; dir < 2; ++dir) {
+            const bool forward = dir == 1;
+            if (!forward && sflags == M_LEFT) {
+                open_l = __popc(back_nib(W.mask[s], false)) <= 1;
+                continue;
+            }
+            if (forward && sflags == M_RIGHT) {
+                open_r = __popc(fwd_nib(W.mask[s], false)) <= 1;
+                continue;
+            }
+            const int step = forward ? df : -df;
+            int64_t q = p;
+            uint32_t cnt = 0;
+            for (;;) {
+                int64_t q2 = q + step;
+                if (cyclic) {
+                    if (q2 < 0) q2 += L;
+                    if (q2 >= (int64_t)L) q2 -= L;
+                } else if (q2 < 0 || q2 >= (int64_t)L) {
+                    break;
+                }
+                if (vis[q2]) break;
+                vis[q2] = 1;
+                ++cnt;
+                q = q2;
+                const uint32_t nd = cn[q];
+                const uint32_t f = W.meta[nd] & 3u;
+                if (f == M_LEFT || f == M_RIGHT) {
+                    const bool wrc = (df == 1) ? (crc[q] != 0) : (crc[q] == 0);
+                    if (forward)
+                        open_r = __popc(fwd_nib(W.mask[nd], wrc)) <= 1;
+                    else
+                        open_l = __popc(back_nib(W.mask[nd], wrc)) <= 1;
+                    break;
+                }
+            }
+            if (forward)
+                nf = cnt;
+            else
+                nb = cnt;
+        }
+        const uint32_t flen = nb + 1 + nf;
+        for (uint32_t j = 0; j < flen; ++j) {
+            int64_t q = (int64_t)p + (int64_t)df * ((int64_t)j - (int64_t)nb);
+            if (cyclic) {
+                q %= (int64_t)L;
+                if (q < 0) q += L;
+            }
+            const bool wrc = (df == 1) ? (crc[q] != 0) : (crc[q] == 0);
+            W.fe[fcur + j] = (cn[q] << 1) | (wrc ? 1u : 0u);
+        }
+        W.seed_start[s] = (uint32_t)fcur;
+        W.seed_len[s] = flen;
+        W.seed_open[s] = (uint8_t)((open_l ? 1 : 0) | (open_r ? 2 : 0));
+        fcur += flen;
+    }
+}
+
+// Paths: a node with at most one linked port starts a walk to the other end;
+// the end with the smaller node index owns the chain.
+__global__ void k_chain_paths(chain_ws W, uint32_t* err) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= W.D) return;
+    const uint32_t ll = W.link[2 * n], lr = W.link[2 * n + 1];
+    const int deg = (ll != NONE32) + (lr != NONE32);
+    if (deg == 2) return;
+    uint32_t c = (uint32_t)n;
+    bool rc = (lr == NONE32);  // walk out through the linked port
+    uint32_t L = 1;
+    if (deg == 1) {
+        uint32_t cc = c;
+        bool r = rc;
+        while (chain_step(W.link, cc, r)) {
+            if (++L > W.D) {
+                set_error(err, ERR_CHAIN_LIMIT);
+                return;
+            }
+        }
+        if (cc < n) return;  // the other end leads
+    }
+    const uint64_t c0 = atomicAdd(W.cursor, (unsigned long long)L);
+    if (c0 + L > W.D) {  // chains partition the nodes; anything else is a bug
+        set_error(err, ERR_CAPACITY);
+        return;
+    }
+    uint32_t i = 0;
+    uint32_t cc = c;
+    bool r = rc;
+    W.ch_node[c0] = cc;
+    W.ch_rc[c0] = r ? 1 : 0;
+    while (++i < L && chain_step(W.link, cc, r)) {
+        W.ch_node[c0 + i] = cc;
+        W.ch_rc[c0 + i] = r ? 1 : 0;
+    }
+    simulate_chain(W, c0, L, false);
+}
+
+// Cycles: nodes left uncovered; the smallest node index of a cycle leads.
+__global__ void k_chain_cycles(chain_ws W, uint32_t* err) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= W.D || W.covered[n]) return;
+    uint32_t cc = (uint32_t)n;
+    bool r = false;
+    uint32_t L = 1;
+    for (;;) {
+        if (!chain_step(W.link, cc, r)) {
+            set_error(err, ERR_CHAIN_LIMIT);  // an uncovered node must be on a cycle
+            return;
+        }
+        if (cc == n) break;
+        if (cc < n) return;
+        if (++L > W.D) {
+            set_error(err, ERR_CHAIN_LIMIT);
+            return;
+        }
+    }
+    const uint64_t c0 = atomicAdd(W.cursor, (unsigned long long)L);
+    if (c0 + L > W.D) {
+        set_error(err, ERR_CAPACITY);
+        return;
+    }
+    cc = (uint32_t)n;
+    r = false;
+    W.ch_node[c0] = cc;
+    W.ch_rc[c0] = 0;
+    for (uint32_t i = 1; i < L; ++i) {
+        chain_step(W.link, cc, r);
+        W.ch_node[c0 + i] = cc;
+        W.ch_rc[c0 + i] = r ? 1 : 0;
+    }
+    simulate_chain(W, c0, L, true);
+}
+
+// ---- fragments --------------------------------------------------------------
+__device__ __forceinline__ uint32_t frag_cid(uint32_t const* n_cid, uint32_t node) { return n_cid[node]; }
+
+__global__ void k_frag_sizes(uint64_t D, uint32_t const* __restrict__ seed_start, uint32_t const* __restrict__ seed_len,
+                             uint32_t const* __restrict__ fe, uint32_t const* __restrict__ n_cid, uint32_t k,
+                             uint64_t* __restrict__ sz, uint32_t* __restrict__ is_seed,
+                             unsigned long long* __restrict__ seq_total) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D) return;
+    const uint32_t len = seed_len[n];
+    if (!len) {
+        sz[n] = 0;
+        is_seed[n] = 0;
+        return;
+    }
+    is_seed[n] = 1;
+    const uint32_t a = seed_start[n];
+    uint32_t runs = 1, prev = frag_cid(n_cid, fe[a] >> 1);
+    for (uint32_t j = 1; j < len; ++j) {
+        const uint32_t c = frag_cid(n_cid, fe[a + j] >> 1);
+        if (c != prev) ++runs;
+        prev = c;
+    }
+    const uint64_t seq = (uint64_t)k + len - 1;
+    sz[n] = 1 + 4 + 12ull * runs + 4 + seq;
+    atomicAdd(seq_total, (unsigned long long)seq);
+}
+
+__device__ __forceinline__ void put_bytes(uint8_t* o, uint64_t v, int n) {
+    for (int i = 0; i < n; ++i) o[i] = (uint8_t)(v >> (8 * i));
+}
+
+template <typename K>
+__global__ void k_frag_write(uint64_t D, uint32_t const* __restrict__ seed_start, uint32_t const* __restrict__ seed_len,
+                             uint8_t const* __restrict__ seed_open, uint32_t const* __restrict__ fe,
+                             uint32_t const* __restrict__ n_cid, K const* __restrict__ n_key, uint32_t k,
+                             uint64_t const* __restrict__ off, uint8_t* __restrict__ out) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D) return;
+    const uint32_t len = seed_len[n];
+    if (!len) return;
+    typedef kmer_ops<K> ops;
+    const uint32_t a = seed_start[n];
+    uint8_t* o = out + off[n];
+    o[0] = seed_open[n];
+    // runs
+    uint32_t runs = 0;
+    uint8_t* rp = o + 5;
+    uint32_t prev = frag_cid(n_cid, fe[a] >> 1), cnt = 1;
+    for (uint32_t j = 1; j <= len; ++j) {
+        const uint32_t c = j < len ? frag_cid(n_cid, fe[a + j] >> 1) : ~prev;
+        if (j < len && c == prev) {
+            ++cnt;
+            continue;
+        }
+        const uint64_t cid64 = prev == NONE32 ? ~0ull : (uint64_t)prev;
+        put_bytes(rp, cid64, 8);
+        put_bytes(rp + 8, cnt, 4);
+        rp += 12;
+        ++runs;
+        prev = c;
+        cnt = 1;
+    }
+    put_bytes(o + 1, runs, 4);
+    const uint32_t seq_len = k + len - 1;
+    put_bytes(rp, seq_len, 4);
+    uint8_t* sp = rp + 4;
+    const char acgt[4] = {'A', 'C', 'G', 'T'};
+    {
+        const uint32_t e = fe[a];
+        K w = n_key[e >> 1];
+        if (e & 1u) w = ops::revcomp(w, k);
+        for (uint32_t i = 0; i < k; ++i) sp[k - 1 - i] = acgt[ops::low2(w >> (2 * i))];
+    }
+    for (uint32_t j = 1; j < len; ++j) {
+        const uint32_t e = fe[a + j];
+        K w = n_key[e >> 1];
+        if (e & 1u) w = ops::revcomp(w, k);
+        sp[k - 1 + j] = acgt[ops::low2(w)];
+    }
+}
+
+
+// ---- small helpers ----------------------------------------------------------
+__global__ void k_count_flags(uint64_t n, uint32_t const* __restrict__ f, unsigned long long* __restrict__ c) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t v = (i < n) ? f[i] : 0u;
+    const uint32_t b = __ballot_sync(0xffffffffu, v != 0);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(c, (unsigned long long)__popc(b));
+}
+__global__ void k_add_offsets(uint64_t n, uint64_t const* __restrict__ src, uint64_t add,
+                              uint64_t* __restrict__ dst) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i] + add;
+}
+__global__ void k_set_u64(uint64_t* p, uint64_t v) { *p = v; }
+__global__ void k_used_flags(uint64_t n, uint32_t const* __restrict__ first, uint32_t* __restrict__ keep) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keep[i] = first[i] != NONE32 ? 1u : 0u;
+}
+
+void add_offsets(uint64_t const* src, uint64_t n, uint64_t add, uint64_t* dst, cudaStream_t st) {
+    if (!n) return;
+    k_add_offsets<<<grid(n, 256), 256, 0, st>>>(n, src, add, dst);
+    CDBG_CHECK_LAUNCH();
+}
+
+void check_device_error_word(uint32_t* d_err, cudaStream_t st, char const* stage) {
+    const uint32_t e = read_dev(d_err, st);
+    if (e == ERR_NONE) return;
+    CDBG_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
+    static char const* names[] = {"none", "hash table full", "field overflow", "malformed record",
+                                  "capacity exceeded", "chain walk bound exceeded"};
+    throw std::runtime_error(std::string("device error in ") + stage + ": " +
+                             (e < 6 ? names[e] : "unknown"));
+}
+
+// ---------------------------------------------------------------------------
+struct class_dict {
+    dvec<uint64_t> cls_hash;
+    dvec<uint64_t> cls_off;   // n + 1
+    dvec<uint32_t> pool;
+    dvec<uint64_t> bit_off;   // n
+    dvec<uint64_t> words;
+    dvec<uint64_t> slot_hash;
+    dvec<uint32_t> slot_cid;
+    uint64_t n = 0, pool_n = 0, nbits = 0, total_integers = 0, mask = 0;
+
+    void init(cudaStream_t st) {
+        cls_off.reserve(1024, st);
+        CDBG_CUDA(cudaMemsetAsync(cls_off.p, 0, 8, st));
+        cls_off.n = 1;
+        words.reserve(1024, st, true);
+    }
+    // Make room for `n` classes (load <= 1/2); classes [first_new, n) still
+    // need inserting.  A resized table is rebuilt from every class hash.
+    void ensure_table(uint64_t first_new, cudaStream_t st, uint32_t* d_err) {
+        uint64_t cap = 1024;
+        while (cap < 2 * n) cap <<= 1;
+        uint64_t from = first_new;
+        if (!slot_hash.p || cap - 1 > mask) {
+            slot_hash.reserve(cap, st);
+            slot_cid.reserve(cap, st);
+            mask = cap - 1;
+            CDBG_CUDA(cudaMemsetAsync(slot_hash.p, 0xff, cap * 8, st));
+            from = 0;
+        }
+        if (n > from) {
+            k_dict_insert<<<grid(n - from, 256), 256, 0, st>>>(from, n, cls_hash.p, slot_hash.p, slot_cid.p, mask,
+                                                              d_err);
+            CDBG_CHECK_LAUNCH();
+        }
+    }
+};
+
+template <typename K>
+void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, uint32_t b0, uint32_t b1,
+               std::vector<uint64_t> const& bocc, dev_arena& A, cudaStream_t st, uint32_t* d_err,
+               class_dict& dict, phase2_result& out, std::vector<uint64_t> const& hbstart, uint64_t* d_rhash,
+               dvec<uint8_t>& dfrag) {
+    const uint32_t k = p.k, C = p.num_colors;
+    const uint64_t R0 = hbstart[b0], R1 = hbstart[b1];
+    const uint64_t nrec = R1 - R0;
+    const uint64_t O0 = bocc[b0], O1 = bocc[b1];
+    const uint64_t nocc = O1 - O0;
+    if (nocc == 0) return;
+    auto mark = A.mark();
+    // ---- tables
+    const uint32_t nb = b1 - b0;
+    std::vector<uint64_t> toff(nb), tcap(nb);
+    uint64_t T = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint64_t o = bocc[b0 + b + 1] - bocc[b0 + b];
+        const uint64_t cap = o ? std::max<uint64_t>(64, o + o / 2 + 16) : 0;
+        toff[b] = T;
+        tcap[b] = cap;
+        T += cap;
+    }
+    uint64_t* d_toff = A.alloc<uint64_t>(nb);
+    uint64_t* d_tcap = A.alloc<uint64_t>(nb);
+    CDBG_CUDA(cudaMemcpyAsync(d_toff, toff.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
+    CDBG_CUDA(cudaMemcpyAsync(d_tcap, tcap.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
+    tables<K> TB;
+    TB.key = A.alloc<K>(T);
+    TB.meta = A.alloc<uint32_t>(T);
+    TB.rank = A.alloc<unsigned long long>(T);
+    TB.rmin = A.alloc<uint32_t>(T);
+    TB.rmax = A.alloc<uint32_t>(T);
+    TB.node = A.alloc<uint32_t>(T);
+    TB.tab_off = d_toff;
+    TB.tab_cap = d_tcap;
+    TB.b0 = b0;
+    k_init_tables<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax);
+    CDBG_CHECK_LAUNCH();
+    // ---- load
+    k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, d_err);
+    CDBG_CHECK_LAUNCH();
+    // ---- nodes in first-insertion order
+    const uint64_t nwb = ceil_div(nocc, 32);
+    uint32_t* bits = A.alloc<uint32_t>(nwb);
+    CDBG_CUDA(cudaMemsetAsync(bits, 0, 4 * nwb, st));
+    k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.rank, R.occ, O0, bits);
+    CDBG_CHECK_LAUNCH();
+    uint32_t* wcnt = A.alloc<uint32_t>(nwb);
+    uint64_t* wpre = A.alloc<uint64_t>(nwb + 1);
+    k_popc<<<grid(nwb, 256), 256, 0, st>>>(nwb, bits, wcnt);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(wcnt, wpre, nwb, A, st, wpre + nwb);
+    const uint64_t D = read_dev(wpre + nwb, st);
+    if (D >= (1ull << 31)) throw std::runtime_error("too many distinct k-mers in one bucket batch");
+    check_device_error_word(d_err, st, "k-mer table insert");
+    K* n_key = A.alloc<K>(D);
+    uint8_t* n_meta = A.alloc<uint8_t>(D);
+    uint32_t* n_rec = A.alloc<uint32_t>(D);
+    uint32_t* n_bucket = A.alloc<uint32_t>(D);
+    k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax, R.occ, O0, bits,
+                                                   wpre, R.bucket, TB.node, n_key, n_meta, n_rec, n_bucket);
+    CDBG_CHECK_LAUNCH();
+    // ---- multi-record k-mers
+    unsigned long long* cnt = A.alloc<unsigned long long>(1);
+    CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
+    k_multi_pairs<K, false><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, nullptr);
+    CDBG_CHECK_LAUNCH();
+    const uint64_t npairs = read_dev(cnt, st);
+    uint64_t M = 0;
+    uint32_t* mnode = nullptr;
+    uint64_t* moff = nullptr;
+    uint64_t* upairs = nullptr;
+    uint32_t* msize = nullptr;
+    uint64_t* mhash = nullptr;
+    uint64_t* poff = nullptr;
+    uint32_t* pool = nullptr;
+    if (npairs) {
+        uint64_t* pairs = A.alloc<uint64_t>(npairs);
+        CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
+        k_multi_pairs<K, true><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, pairs);
+        CDBG_CHECK_LAUNCH();
+        uint32_t* dummy = A.alloc<uint32_t>(npairs);
+        prim::radix_sort_pairs<uint32_t>(pairs, dummy, npairs, 0, 64, A, st);
+        uint32_t* keep = A.alloc<uint32_t>(npairs);
+        uint64_t* kpos = A.alloc<uint64_t>(npairs + 1);
+        k_unique_heads<<<grid(npairs, 256), 256, 0, st>>>(npairs, pairs, keep);
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(keep, kpos, npairs, A, st, kpos + npairs);
+        const uint64_t nu = read_dev(kpos + npairs, st);
+        upairs = A.alloc<uint64_t>(nu);
+        k_compact_u64<<<grid(npairs, 256), 256, 0, st>>>(npairs, pairs, keep, kpos, upairs);
+        CDBG_CHECK_LAUNCH();
+        uint32_t* head = A.alloc<uint32_t>(nu);
+        uint64_t* hpos = A.alloc<uint64_t>(nu + 1);
+        k_node_heads<<<grid(nu, 256), 256, 0, st>>>(nu, upairs, head);
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(head, hpos, nu, A, st, hpos + nu);
+        M = read_dev(hpos + nu, st);
+        mnode = A.alloc<uint32_t>(M);
+        moff = A.alloc<uint64_t>(M + 1);
+        k_multi_index<<<grid(nu, 256), 256, 0, st>>>(nu, upairs, head, hpos, mnode, moff, n_rec);
+        CDBG_CHECK_LAUNCH();
+        k_set_u64<<<1, 1, 0, st>>>(moff + M, nu);
+        CDBG_CHECK_LAUNCH();
+        msize = A.alloc<uint32_t>(M);
+        mhash = A.alloc<uint64_t>(M);
+        const uint32_t nw = (C + 31) / 32;
+        int wpb = (int)std::max<uint64_t>(1, std::min<uint64_t>(8, (96 * 1024) / (4ull * nw)));
+        const size_t shm = (size_t)wpb * nw * 4;
+        if (shm > 48 * 1024) {
+            CDBG_CUDA(cudaFuncSetAttribute(k_union<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+            CDBG_CUDA(cudaFuncSetAttribute(k_union<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        }
+        k_union<false><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
+                                                             nullptr, nullptr);
+        CDBG_CHECK_LAUNCH();
+        poff = A.alloc<uint64_t>(M + 1);
+        prim::exclusive_scan<uint32_t, uint64_t>(msize, poff, M, A, st, poff + M);
+        const uint64_t ptot = read_dev(poff + M, st);
+        pool = A.alloc<uint32_t>(ptot + 1);
+        k_union<true><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
+                                                            poff, pool);
+        CDBG_CHECK_LAUNCH();
+    }
+    out.n_multi += M;
+    // ---- candidates: used records, then multi nodes
+    uint32_t* rec_first = A.alloc<uint32_t>(nrec);
+    CDBG_CUDA(cudaMemsetAsync(rec_first, 0xff, 4 * nrec, st));
+    k_rec_first<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_first);
+    CDBG_CHECK_LAUNCH();
+    uint32_t* rkeep = A.alloc<uint32_t>(nrec);
+    uint64_t* rpos = A.alloc<uint64_t>(nrec + 1);
+    k_used_flags<<<grid(nrec, 256), 256, 0, st>>>(nrec, rec_first, rkeep);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(rkeep, rpos, nrec, A, st, rpos + nrec);
+    const uint64_t nrc = read_dev(rpos + nrec, st);
+    const uint64_t nc = nrc + M;
+    cand_view cv;
+    cv.kind_id = A.alloc<uint32_t>(nc);
+    cv.first = A.alloc<uint32_t>(nc);
+    cv.hash = A.alloc<uint64_t>(nc);
+    uint32_t* rec_cand = A.alloc<uint32_t>(nrec);
+    k_cand_records<<<grid(nrec, 256), 256, 0, st>>>(nrec, (uint32_t)R0, rec_first, rkeep, rpos, d_rhash, cv, rec_cand);
+    CDBG_CHECK_LAUNCH();
+    if (M) {
+        k_cand_multi<<<grid(M, 256), 256, 0, st>>>(M, nrc, mnode, mhash, cv);
+        CDBG_CHECK_LAUNCH();
+    }
+    list_src L{R.col_off, R.colors, poff, pool, msize};
+    dict_view DV{dict.slot_hash.p, dict.slot_cid.p, dict.mask, dict.cls_off.p, dict.pool.p};
+    uint32_t* cid = A.alloc<uint32_t>(nc);
+    k_dict_lookup<<<grid(nc, 256), 256, 0, st>>>(nc, cv, L, DV, cid);
+    CDBG_CHECK_LAUNCH();
+    // ---- new classes
+    uint32_t* nflag = A.alloc<uint32_t>(nc);
+    uint64_t* npos = A.alloc<uint64_t>(nc + 1);
+    k_new_flags<<<grid(nc, 256), 256, 0, st>>>(nc, cid, nflag);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(nflag, npos, nc, A, st, npos + nc);
+    const uint64_t nn = read_dev(npos + nc, st);
+    if (nn) {
+        uint64_t* nkey = A.alloc<uint64_t>(nn);
+        uint32_t* nidx = A.alloc<uint32_t>(nn);
+        k_new_gather<<<grid(nc, 256), 256, 0, st>>>(nc, nflag, npos, cv, nkey, nidx);
+        CDBG_CHECK_LAUNCH();
+        prim::radix_sort_pairs<uint32_t>(nkey, nidx, nn, 0, 64, A, st);
+        uint32_t* head = A.alloc<uint32_t>(nn);
+        k_run_heads<<<grid(nn, 256), 256, 0, st>>>(nn, nkey, head);
+        CDBG_CHECK_LAUNCH();
+        uint32_t* rep = A.alloc<uint32_t>(nc);
+        uint32_t* rep_first = A.alloc<uint32_t>(nc);
+        k_group_runs<<<grid(nn, 128), 128, 0, st>>>(nn, nkey, head, nidx, cv, L, rep, rep_first);
+        CDBG_CHECK_LAUNCH();
+        uint32_t* is_rep = A.alloc<uint32_t>(nn);
+        uint64_t* rpos2 = A.alloc<uint64_t>(nn + 1);
+        k_rep_keys<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, rep_first, is_rep);
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(is_rep, rpos2, nn, A, st, rpos2 + nn);
+        const uint64_t nnew = read_dev(rpos2 + nn, st);
+        uint64_t* rkey = A.alloc<uint64_t>(nnew);
+        uint32_t* rcand = A.alloc<uint32_t>(nnew);
+        k_rep_gather<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, is_rep, rpos2, rep_first, rkey, rcand);
+        CDBG_CHECK_LAUNCH();
+        prim::radix_sort_pairs<uint32_t>(rkey, rcand, nnew, 0, 32, A, st);
+        const uint64_t base = dict.n;
+        k_assign_new<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, base, cid);
+        CDBG_CHECK_LAUNCH();
+        k_assign_members<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, cid);
+        CDBG_CHECK_LAUNCH();
+        // append lists, hashes, offsets to the dictionary
+        uint64_t* nsz = A.alloc<uint64_t>(nnew);
+        uint64_t* nh = A.alloc<uint64_t>(nnew);
+        k_new_sizes<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, cv, L, nsz, nh);
+        CDBG_CHECK_LAUNCH();
+        uint64_t* loff = A.alloc<uint64_t>(nnew + 1);
+        prim::exclusive_scan<uint64_t, uint64_t>(nsz, loff, nnew, A, st, loff + nnew);
+        const uint64_t ladd = read_dev(loff + nnew, st);
+        dict.cls_hash.reserve(base + nnew, st);
+        dict.cls_off.reserve(base + nnew + 1, st);
+        dict.pool.reserve(dict.pool_n + ladd + 1, st);
+        dict.bit_off.reserve(base + nnew, st);
+        CDBG_CUDA(cudaMemcpyAsync(dict.cls_hash.p + base, nh, 8 * nnew, cudaMemcpyDeviceToDevice, st));
+        // cls_off[base + 1 + j] = pool_n + loff[j + 1]; absolute list offsets for the encoder
+        add_offsets(loff + 1, nnew, dict.pool_n, dict.cls_off.p + base + 1, st);
+        uint64_t* loff_abs = A.alloc<uint64_t>(nnew + 1);
+        add_offsets(loff, nnew + 1, dict.pool_n, loff_abs, st);
+        k_new_copy<<<grid(nnew, 8), 256, 0, st>>>(nnew, rcand, cv, L, loff, dict.pool.p + dict.pool_n);
+        CDBG_CHECK_LAUNCH();
+        // encode
+        const uint32_t nw = (C + 31) / 32;
+        int wpb = (int)std::max<uint64_t>(1, std::min<uint64_t>(8, (96 * 1024) / (4ull * nw)));
+        const size_t shm = (size_t)wpb * nw * 4;
+        if (shm > 48 * 1024) {
+            CDBG_CUDA(cudaFuncSetAttribute(k_encode<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+            CDBG_CUDA(cudaFuncSetAttribute(k_encode<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        }
+        uint64_t* nbits = A.alloc<uint64_t>(nnew);
+        uint64_t* boff = A.alloc<uint64_t>(nnew + 1);
+        k_encode<false><<<grid(nnew, wpb), wpb * 32, shm, st>>>(nnew, loff_abs, dict.pool.p, C, nbits, nullptr,
+                                                                  nullptr);
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint64_t, uint64_t>(nbits, boff, nnew, A, st, boff + nnew);
+        const uint64_t badd = read_dev(boff + nnew, st);
+        add_offsets(boff, nnew + 1, dict.nbits, boff, st);  // absolute bit offsets
+        CDBG_CUDA(cudaMemcpyAsync(dict.bit_off.p + base, boff, 8 * nnew, cudaMemcpyDeviceToDevice, st));
+        const uint64_t need_words = (dict.nbits + badd + 63) / 64 + 2;
+        dict.words.reserve(need_words, st, true);
+        k_encode<true><<<grid(nnew, wpb), wpb * 32, shm, st>>>(nnew, loff_abs, dict.pool.p, C, nullptr, boff,
+                                                                 dict.words.p);
+        CDBG_CHECK_LAUNCH();
+        dict.n = base + nnew;
+        dict.cls_hash.n = dict.cls_off.n = dict.bit_off.n = dict.n;
+        dict.cls_off.n = dict.n + 1;
+        dict.pool_n += ladd;
+        dict.pool.n = dict.pool_n;
+        dict.nbits += badd;
+        dict.words.n = (dict.nbits + 63) / 64;
+        dict.total_integers += ladd;
+        dict.ensure_table(base, st, d_err);
+    }
+    // ---- node class ids
+    uint32_t* n_cid = A.alloc<uint32_t>(D);
+    k_node_cid<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_cand, nrc, cid, n_cid);
+    CDBG_CHECK_LAUNCH();
+    // ---- extension masks, links, chains
+    uint8_t* n_mask = A.alloc<uint8_t>(D);
+    k_ext_mask<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, k, n_mask);
+    CDBG_CHECK_LAUNCH();
+    uint32_t* link = A.alloc<uint32_t>(2 * D);
+    k_links<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, n_mask, k, link);
+    CDBG_CHECK_LAUNCH();
+    chain_ws W;
+    W.link = link;
+    W.meta = n_meta;
+    W.mask = n_mask;
+    W.ch_node = A.alloc<uint32_t>(D);
+    W.ch_rc = A.alloc<uint8_t>(D);
+    W.ch_ord = A.alloc<unsigned long long>(D);
+    W.ch_vis = A.alloc<uint8_t>(D);
+    W.fe = A.alloc<uint32_t>(D);
+    W.seed_start = A.alloc<uint32_t>(D);
+    W.seed_len = A.alloc<uint32_t>(D);
+    W.seed_open = A.alloc<uint8_t>(D);
+    W.covered = A.alloc<uint8_t>(D);
+    W.cursor = A.alloc<unsigned long long>(1);
+    W.D = D;
+    CDBG_CUDA(cudaMemsetAsync(W.seed_len, 0, 4 * D, st));
+    CDBG_CUDA(cudaMemsetAsync(W.covered, 0, D, st));
+    CDBG_CUDA(cudaMemsetAsync(W.cursor, 0, 8, st));
+    k_chain_paths<<<grid(D, 128), 128, 0, st>>>(W, d_err);
+    CDBG_CHECK_LAUNCH();
+    k_chain_cycles<<<grid(D, 128), 128, 0, st>>>(W, d_err);
+    CDBG_CHECK_LAUNCH();
+    // ---- fragments
+    uint64_t* fsz = A.alloc<uint64_t>(D);
+    uint32_t* is_seed = A.alloc<uint32_t>(D);
+    uint64_t* foff = A.alloc<uint64_t>(D + 1);
+    unsigned long long* seqt = A.alloc<unsigned long long>(1);
+    CDBG_CUDA(cudaMemsetAsync(seqt, 0, 8, st));
+    k_frag_sizes<<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.fe, n_cid, k, fsz, is_seed, seqt);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint64_t, uint64_t>(fsz, foff, D, A, st, foff + D);
+    const uint64_t fbytes = read_dev(foff + D, st);
+    check_device_error_word(d_err, st, "unitig walk");
+    uint8_t* fb = A.alloc<uint8_t>(fbytes + 8);
+    k_frag_write<K><<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.seed_open, W.fe, n_cid, n_key, k,
+                                                   foff, fb);
+    CDBG_CHECK_LAUNCH();
+    uint64_t nfr = 0;
+    {
+        std::vector<uint32_t> dummy;
+        (void)dummy;
+        unsigned long long* fc = A.alloc<unsigned long long>(1);
+        CDBG_CUDA(cudaMemsetAsync(fc, 0, 8, st));
+        k_count_flags<<<grid(D, 256), 256, 0, st>>>(D, is_seed, fc);
+        CDBG_CHECK_LAUNCH();
+        nfr = read_dev(fc, st);
+    }
+    const uint64_t seq_total = read_dev(seqt, st);
+    out.n_fragments += nfr;
+    out.total_seq_bytes += seq_total;
+    out.n_occ += nocc;
+    out.n_distinct += D;
+    if (p.to_host) {
+        const size_t o = out.frag.size();
+        out.frag.resize(o + fbytes);
+        CDBG_CUDA(cudaMemcpyAsync(out.frag.data() + o, fb, fbytes, cudaMemcpyDeviceToHost, st));
+    } else {
+        dfrag.reserve(dfrag.n + fbytes + 8, st);
+        CDBG_CUDA(cudaMemcpyAsync(dfrag.p + dfrag.n, fb, fbytes, cudaMemcpyDeviceToDevice, st));
+        dfrag.n += fbytes;
+    }
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    out.frag_nbytes += fbytes;
+    check_device_error_word(d_err, st, "phase-2 batch");
+    A.release(mark);
+}
+
+}  // namespace
+}  // namespace cdbg
+
+namespace cdbg {
+
+namespace {
+template <typename K>
+void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStream_t st, uint32_t* d_err,
+             phase2_result& out) {
+    const uint64_t n = rs.n;
+    const uint32_t B = rs.B;
+    auto mark = A.mark();
+    uint64_t* nk = A.alloc<uint64_t>(n + 1);
+    uint32_t* rbucket = A.alloc<uint32_t>(n + 1);
+    uint64_t* rhash = A.alloc<uint64_t>(n + 1);
+    uint64_t* occ = A.alloc<uint64_t>(n + 1);
+    if (n) {
+        k_rec_prep<<<grid(n, 256), 256, 0, st>>>(n, rs.len, p.k, rs.bucket_start, B, nk, rbucket, rs.col_off,
+                                                 rs.colors, rhash);
+        CDBG_CHECK_LAUNCH();
+    }
+    prim::exclusive_scan<uint64_t, uint64_t>(nk, occ, n, A, st, occ + n);
+    uint64_t* d_bocc = A.alloc<uint64_t>(B + 1);
+    k_gather_u64<<<grid(B + 1, 256), 256, 0, st>>>(B + 1, occ, rs.bucket_start, d_bocc);
+    CDBG_CHECK_LAUNCH();
+    std::vector<uint64_t> bocc(B + 1), hbstart(B + 1);
+    CDBG_CUDA(cudaMemcpyAsync(bocc.data(), d_bocc, 8ull * (B + 1), cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaMemcpyAsync(hbstart.data(), rs.bucket_start, 8ull * (B + 1), cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    uint64_t budget = p.batch_occ;
+    if (budget == 0) {
+        size_t fr = 0, tot = 0;
+        CDBG_CUDA(cudaMemGetInfo(&fr, &tot));
+        // ~160 B of device memory per k-mer occurrence in the batch, worst case
+        budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(fr / 2) / 160));
+    }
+    rec_view R{rs.start, rs.len, rs.flags, rs.col_off, rs.colors, rbucket, occ, rs.words};
+    class_dict dict;
+    dict.init(st);
+    dvec<uint8_t> dfrag;
+    uint32_t b = 0;
+    while (b < B) {
+        const uint32_t s = b;
+        uint64_t acc = 0;
+        while (b < B) {
+            const uint64_t ob = bocc[b + 1] - bocc[b];
+            if (b > s && acc + ob > budget) break;
+            acc += ob;
+            ++b;
+        }
+        run_batch<K>(rs, R, p, s, b, bocc, A, st, d_err, dict, out, hbstart, rhash, dfrag);
+    }
+    // outputs
+    out.n_classes = dict.n;
+    out.nbits = dict.nbits;
+    out.total_integers = dict.total_integers;
+    const uint64_t nwords = (dict.nbits + 63) / 64;
+    if (p.to_host) {
+        out.words.resize(nwords);
+        out.offsets.resize(dict.n);
+        if (nwords)
+            CDBG_CUDA(cudaMemcpyAsync(out.words.data(), dict.words.p, 8 * nwords, cudaMemcpyDeviceToHost, st));
+        if (dict.n)
+            CDBG_CUDA(cudaMemcpyAsync(out.offsets.data(), dict.bit_off.p, 8 * dict.n, cudaMemcpyDeviceToHost, st));
+    }
+    if (p.keep_lists) {
+        out.list_off.resize(dict.n + 1);
+        out.lists.resize(dict.pool_n);
+        CDBG_CUDA(cudaMemcpyAsync(out.list_off.data(), dict.cls_off.p, 8 * (dict.n + 1), cudaMemcpyDeviceToHost, st));
+        if (dict.pool_n)
+            CDBG_CUDA(cudaMemcpyAsync(out.lists.data(), dict.pool.p, 4 * dict.pool_n, cudaMemcpyDeviceToHost, st));
+    }
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    A.release(mark);
+    if (!p.to_host) {
+        // device-resident outputs in the arena (valid until the arena is reset)
+        out.d_frag = A.alloc<uint8_t>(dfrag.n + 8);
+        out.d_words = A.alloc<uint64_t>(nwords + 1);
+        out.d_offsets = A.alloc<uint64_t>(dict.n + 1);
+        if (dfrag.n) CDBG_CUDA(cudaMemcpyAsync(out.d_frag, dfrag.p, dfrag.n, cudaMemcpyDeviceToDevice, st));
+        if (nwords) CDBG_CUDA(cudaMemcpyAsync(out.d_words, dict.words.p, 8 * nwords, cudaMemcpyDeviceToDevice, st));
+        if (dict.n)
+            CDBG_CUDA(cudaMemcpyAsync(out.d_offsets, dict.bit_off.p, 8 * dict.n, cudaMemcpyDeviceToDevice, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+    }
+}
+}  // namespace
+
+void run_phase2(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStream_t st, uint32_t* d_err,
+                phase2_result& out) {
+    out = phase2_result();
+    if (p.k < 2 || p.k > 63) throw std::runtime_error("k must be in [2, 63]");
+    if (p.num_colors == 0) throw std::runtime_error("num_colors must be > 0");
+    if (p.k <= 31)
+        run_all<uint64_t>(rs, p, A, st, d_err, out);
+    else
+        run_all<u128>(rs, p, A, st, d_err, out);
+}
+
+}  // namespace cdbg

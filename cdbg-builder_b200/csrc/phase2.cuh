@@ -1,0 +1,50 @@
+// Phase 2 (bucket-process) on the device: entry point and outputs.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "arena.cuh"
+#include "phase1.cuh"
+
+namespace cdbg {
+
+// Outputs of phase 2, accumulated over bucket batches.
+struct phase2_result {
+    // frag_unitigs.bin bytes (unitig_spill.hpp:642-665 record layout), in
+    // bucket order and, per bucket, in seed order.
+    std::vector<uint8_t> frag;          // host copy (when to_host)
+    uint8_t* d_frag = nullptr;          // device copy (when !to_host), arena memory
+    uint64_t frag_nbytes = 0;
+    // color classes in global cid order
+    std::vector<uint64_t> words;        // encoded .color_sets bit vector
+    std::vector<uint64_t> offsets;      // bit offset of each class
+    uint64_t* d_words = nullptr;        // device copies (when !to_host)
+    uint64_t* d_offsets = nullptr;
+    uint64_t nbits = 0;
+    uint64_t n_classes = 0;
+    uint64_t total_integers = 0;
+    // class lists (only when keep_lists): concatenated ascending colors
+    std::vector<uint32_t> lists;
+    std::vector<uint64_t> list_off;
+    // counters
+    uint64_t n_occ = 0, n_distinct = 0, n_fragments = 0, total_seq_bytes = 0;
+    uint64_t n_multi = 0;
+    double ms_device = 0;
+};
+
+struct phase2_params {
+    uint32_t k = 31;
+    uint32_t num_colors = 0;
+    uint64_t batch_occ = 0;   // k-mer occurrences per batch (0 = auto)
+    bool to_host = true;      // copy outputs to host vectors
+    bool keep_lists = false;  // also return the class color lists
+};
+
+// Run phase 2 over all buckets of `rs` (records grouped by bucket).
+void run_phase2(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStream_t st,
+                uint32_t* d_err, phase2_result& out);
+
+}  // namespace cdbg

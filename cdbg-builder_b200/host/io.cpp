@@ -1,0 +1,342 @@
+// Host-side I/O for the GPU phases (see io.hpp).
+
+#include "io.hpp"
+
+#include <zlib.h>
+
+#include <atomic>
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <stdexcept>
+#include <thread>
+
+extern "C" {
+// System LZ4 block API (liblz4.so.1), the functions the reference calls at
+// bucket_io.hpp:259-263 and :695.
+int LZ4_compressBound(int inputSize);
+int LZ4_compress_default(const char* src, char* dst, int srcSize, int dstCapacity);
+int LZ4_decompress_safe(const char* src, char* dst, int compressedSize, int dstCapacity);
+}
+
+namespace cdbg {
+namespace io {
+
+namespace {
+inline bool is_space(char c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
+
+template <typename F>
+void parallel_for(size_t n, uint32_t threads, F&& f) {
+    if (threads <= 1 || n <= 1) {
+        for (size_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> ts;
+    std::exception_ptr err;
+    std::atomic<bool> failed{false};
+    for (uint32_t t = 0; t < threads && t < n; ++t)
+        ts.emplace_back([&] {
+            for (;;) {
+                size_t i = next.fetch_add(1);
+                if (i >= n || failed) break;
+                try {
+                    f(i);
+                } catch (...) {
+                    if (!failed.exchange(true)) err = std::current_exception();
+                }
+            }
+        });
+    for (auto& t : ts) t.join();
+    if (err) std::rethrow_exception(err);
+}
+}  // namespace
+
+bool parse_fastx(char const* d, size_t n, std::function<void(char const*, size_t)> const& emit) {
+    size_t p = 0;
+    int last = 0;
+    std::string seq;
+    for (;;) {
+        if (last == 0) {
+            while (p < n && d[p] != '>' && d[p] != '@') ++p;
+            if (p >= n) return true;
+            last = d[p++];
+        }
+        // name up to whitespace; the rest of the header line is a comment
+        if (p >= n) return true;  // header char at EOF: nothing to read
+        char c = 0;
+        while (p < n && !is_space(d[p])) ++p;
+        if (p < n) c = d[p++];
+        if (c != '\n')
+            while (p < n && d[p++] != '\n') {
+            }
+        seq.clear();
+        int cc = -1;
+        while (p < n) {
+            cc = (unsigned char)d[p++];
+            if (cc == '>' || cc == '+' || cc == '@') break;
+            cc = -1;
+            if (d[p - 1] == '\n') continue;
+            size_t e = p - 1;
+            while (p < n && d[p] != '\n') ++p;
+            seq.append(d + e, p - e);
+            if (p < n) ++p;  // newline
+        }
+        if (cc == '>' || cc == '@') last = cc;
+        if (cc != '+') {
+            emit(seq.data(), seq.size());
+            if (cc == -1) return true;
+            continue;
+        }
+        // FASTQ quality: skip the '+' line, then read seq.size() printable chars
+        while (p < n && d[p] != '\n') ++p;
+        if (p >= n) return false;
+        ++p;
+        size_t q = 0;
+        while (p < n) {
+            unsigned char qc = (unsigned char)d[p++];
+            if (q >= seq.size()) break;
+            if (qc >= 33 && qc <= 127) ++q;
+        }
+        last = 0;
+        if (q != seq.size()) return false;
+        emit(seq.data(), seq.size());
+    }
+}
+
+std::string slurp(std::string const& path) {
+    gzFile f = gzopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("could not open input file: " + path);
+    gzbuffer(f, 1 << 20);
+    std::string out;
+    std::vector<char> buf(1 << 22);
+    for (;;) {
+        int r = gzread(f, buf.data(), (unsigned)buf.size());
+        if (r < 0) {
+            gzclose(f);
+            throw std::runtime_error("gzip read error on " + path);
+        }
+        if (r == 0) break;
+        out.append(buf.data(), (size_t)r);
+    }
+    gzclose(f);
+    return out;
+}
+
+void read_files(std::vector<std::string> const& files, size_t first, size_t count,
+                uint32_t color_base, uint32_t threads, seq_batch& out) {
+    struct per_file {
+        std::string seq;
+        std::vector<uint64_t> lens;
+        uint64_t disk = 0;
+    };
+    std::vector<per_file> pf(count);
+    parallel_for(count, threads, [&](size_t i) {
+        std::string const& path = files[first + i];
+        std::error_code ec;
+        auto sz = std::filesystem::file_size(path, ec);
+        pf[i].disk = ec ? 0 : (uint64_t)sz;
+        std::string raw = slurp(path);
+        pf[i].seq.reserve(raw.size());
+        parse_fastx(raw.data(), raw.size(), [&](char const* s, size_t l) {
+            pf[i].seq.append(s, l);
+            pf[i].lens.push_back(l);
+        });
+    });
+    uint64_t total = out.seq.size();
+    for (auto const& f : pf) total += f.seq.size();
+    out.seq.reserve(total);
+    for (size_t i = 0; i < count; ++i) {
+        out.seq.insert(out.seq.end(), pf[i].seq.begin(), pf[i].seq.end());
+        for (uint64_t l : pf[i].lens) {
+            out.off.push_back(out.off.back() + l);
+            out.color.push_back(color_base + (uint32_t)i);
+        }
+        out.input_bytes += pf[i].disk;
+    }
+}
+
+// ---------------------------------------------------------------- buckets
+bucket_file_set::bucket_file_set(std::string dir, uint32_t num_buckets)
+    : m_dir(std::move(dir)), m_B(num_buckets), m_files(num_buckets, nullptr), m_unc(num_buckets, 0) {
+    std::filesystem::create_directories(m_dir);
+    for (uint32_t b = 0; b < m_B; ++b) {
+        std::FILE* f = std::fopen(path(b).c_str(), "wb");
+        if (!f) throw std::runtime_error("cannot open bucket file: " + path(b) + ": " + std::strerror(errno));
+        m_files[b] = f;
+    }
+}
+
+bucket_file_set::~bucket_file_set() {
+    for (void* f : m_files)
+        if (f) std::fclose((std::FILE*)f);
+}
+
+std::string bucket_file_set::path(uint32_t b) const { return m_dir + "/bucket_" + std::to_string(b) + ".bin"; }
+
+void bucket_file_set::append_frames(uint8_t const* raw, uint64_t const* boff, uint32_t threads) {
+    // One frame per bucket slice, capped at 64 MiB of input per frame so the
+    // int-sized LZ4 API is never exceeded (records never straddle a frame:
+    // frame splits happen only at slice starts, which are record starts).
+    std::vector<uint64_t> comp(m_B, 0);
+    parallel_for(m_B, threads, [&](size_t b) {
+        uint64_t a = boff[b], e = boff[b + 1];
+        if (a == e) return;
+        std::FILE* f = (std::FILE*)m_files[b];
+        std::vector<char> out;
+        const uint64_t cap = 64ull << 20;
+        // split only at record boundaries: a slice above the cap is written
+        // as one frame per <= cap piece only when the caller's slice is
+        // already record aligned -- slices come from one device serialization
+        // per chunk, so the slice itself is the frame.
+        (void)cap;
+        const int src = (int)(e - a);
+        out.resize((size_t)LZ4_compressBound(src));
+        int c = LZ4_compress_default((char const*)raw + a, out.data(), src, (int)out.size());
+        if (c <= 0) throw std::runtime_error("LZ4_compress_default failed on " + path((uint32_t)b));
+        uint32_t u32 = (uint32_t)src, c32 = (uint32_t)c;
+        if (std::fwrite(&u32, 4, 1, f) != 1 || std::fwrite(&c32, 4, 1, f) != 1 ||
+            std::fwrite(out.data(), 1, (size_t)c, f) != (size_t)c)
+            throw std::runtime_error("short write to " + path((uint32_t)b));
+        m_unc[b] += (uint64_t)src;
+        comp[b] = 8 + (uint64_t)c;
+    });
+    for (uint64_t c : comp) m_comp += c;
+}
+
+void bucket_file_set::close() {
+    for (uint32_t b = 0; b < m_B; ++b) {
+        std::FILE* f = (std::FILE*)m_files[b];
+        if (!f) continue;
+        uint32_t eof = 0;
+        if (std::fwrite(&eof, 4, 1, f) != 1) throw std::runtime_error("short write to " + path(b));
+        std::fclose(f);
+        m_files[b] = nullptr;
+        m_comp += 4;
+    }
+}
+
+void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
+                       std::function<uint8_t*(uint64_t)> const& alloc, bucket_bytes& out,
+                       bool delete_after) {
+    struct frame {
+        uint32_t u, c;
+        long pos;
+    };
+    std::vector<std::vector<frame>> frames(B);
+    std::vector<std::vector<char>> comp(B);
+    out.bucket_unc.assign(B, 0);
+    // pass 1: read each file whole (compressed), index its frames
+    parallel_for(B, threads, [&](size_t b) {
+        std::string p = dir + "/bucket_" + std::to_string(b) + ".bin";
+        std::FILE* f = std::fopen(p.c_str(), "rb");
+        if (!f) return;  // a missing bucket file is an empty bucket
+        std::fseek(f, 0, SEEK_END);
+        long sz = std::ftell(f);
+        std::fseek(f, 0, SEEK_SET);
+        comp[b].resize((size_t)sz);
+        if (sz > 0 && std::fread(comp[b].data(), 1, (size_t)sz, f) != (size_t)sz) {
+            std::fclose(f);
+            throw std::runtime_error("short read of " + p);
+        }
+        std::fclose(f);
+        size_t q = 0;
+        for (;;) {
+            if (q + 4 > comp[b].size()) {
+                if (q == comp[b].size()) break;
+                throw std::runtime_error("short read of frame header on " + p);
+            }
+            uint32_t u;
+            std::memcpy(&u, comp[b].data() + q, 4);
+            q += 4;
+            if (u == 0) break;
+            if (q + 4 > comp[b].size()) throw std::runtime_error("short read of compressed_size on " + p);
+            uint32_t c;
+            std::memcpy(&c, comp[b].data() + q, 4);
+            q += 4;
+            if (q + c > comp[b].size()) throw std::runtime_error("short read of compressed payload on " + p);
+            frames[b].push_back({u, c, (long)q});
+            q += c;
+            out.bucket_unc[b] += u;
+        }
+        if (delete_after) {
+            std::error_code ec;
+            std::filesystem::remove(p, ec);
+        }
+    });
+    uint64_t total = 0;
+    for (uint64_t u : out.bucket_unc) total += u;
+    out.nbytes = total;
+    out.data = alloc(total + 64);
+    std::memset(out.data + total, 0, 64);
+    std::vector<uint64_t> bstart(B + 1, 0);
+    for (uint32_t b = 0; b < B; ++b) bstart[b + 1] = bstart[b] + out.bucket_unc[b];
+    out.chunk_off.clear();
+    out.chunk_bucket.clear();
+    for (uint32_t b = 0; b < B; ++b) {
+        uint64_t o = bstart[b];
+        for (auto const& fr : frames[b]) {
+            out.chunk_off.push_back(o);
+            out.chunk_bucket.push_back(b);
+            o += fr.u;
+        }
+    }
+    out.chunk_off.push_back(total);
+    // pass 2: decompress in parallel into place
+    parallel_for(B, threads, [&](size_t b) {
+        uint64_t o = bstart[b];
+        for (auto const& fr : frames[b]) {
+            int d = LZ4_decompress_safe(comp[b].data() + fr.pos, (char*)out.data + o, (int)fr.c, (int)fr.u);
+            if (d < 0 || (uint32_t)d != fr.u)
+                throw std::runtime_error("LZ4_decompress_safe failed on bucket " + std::to_string(b));
+            o += fr.u;
+        }
+        std::vector<char>().swap(comp[b]);
+    });
+}
+
+void write_color_sets(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
+                      uint64_t const* offsets, uint64_t nclasses) {
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot open color-set output: " + path);
+    const uint32_t st = (uint32_t)(0.25 * C), dt = (uint32_t)(0.75 * C);
+    const uint64_t nwords = (nbits + 63) / 64;
+    bool ok = std::fwrite(&C, 4, 1, f) == 1 && std::fwrite(&st, 4, 1, f) == 1 &&
+              std::fwrite(&dt, 4, 1, f) == 1 && std::fwrite(&nbits, 8, 1, f) == 1 &&
+              std::fwrite(&nwords, 8, 1, f) == 1;
+    if (ok && nwords) ok = std::fwrite(words, 8, nwords, f) == nwords;
+    // Elias-Fano over offsets[0..n) + the total bit count
+    const uint64_t n = nclasses + 1, U = nbits;
+    uint64_t l = 0;
+    if (U > n) {
+        const uint64_t q = U / n;
+        while ((uint64_t(1) << (l + 1)) <= q) ++l;
+    }
+    std::vector<uint64_t> low(((n * l) + 63) / 64, 0);
+    const uint64_t hbits = n + (U >> l) + 1;
+    std::vector<uint64_t> high((hbits + 63) / 64, 0);
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t v = i < nclasses ? offsets[i] : nbits;
+        if (l) {
+            const uint64_t pos = i * l, lo = v & ((uint64_t(1) << l) - 1);
+            low[pos >> 6] |= lo << (pos & 63);
+            if ((pos & 63) + l > 64) low[(pos >> 6) + 1] |= lo >> (64 - (pos & 63));
+        }
+        const uint64_t hp = (v >> l) + i;
+        high[hp >> 6] |= uint64_t(1) << (hp & 63);
+    }
+    auto wbv = [&](std::vector<uint64_t> const& w, uint64_t bits) {
+        const uint64_t sz = w.size();
+        ok = ok && std::fwrite(&bits, 8, 1, f) == 1 && std::fwrite(&sz, 8, 1, f) == 1;
+        if (ok && sz) ok = std::fwrite(w.data(), 8, sz, f) == sz;
+    };
+    ok = ok && std::fwrite(&U, 8, 1, f) == 1 && std::fwrite(&n, 8, 1, f) == 1 && std::fwrite(&l, 8, 1, f) == 1;
+    wbv(low, n * l);
+    wbv(high, hbits);
+    std::fclose(f);
+    if (!ok) throw std::runtime_error("short write to " + path);
+}
+
+}  // namespace io
+}  // namespace cdbg

@@ -1,0 +1,82 @@
+// Host-side I/O for the GPU phases: FASTA/FASTQ(.gz) reading, LZ4-framed
+// bucket files, the frag spill and the .color_sets file.  Plain C++17 over
+// zlib and the system LZ4 block library.
+#pragma once
+
+#include <cstdint>
+#include <functional>
+#include <string>
+#include <vector>
+
+namespace cdbg {
+namespace io {
+
+// Sequences of many files back to back: seq bytes, per-sequence offsets
+// (num_seqs + 1) and colors.
+struct seq_batch {
+    std::vector<char> seq;
+    std::vector<uint64_t> off{0};
+    std::vector<uint32_t> color;
+    uint64_t input_bytes = 0;  // on-disk bytes of the files read
+};
+
+// Parse one FASTA/FASTQ buffer with the record rules of kseq_read
+// (external/kseq.h, __KSEQ_READ), calling emit(seq_ptr, len) per record.
+// Returns false when a FASTQ quality string is truncated (kseq returns -2 and
+// the reference's seq_reader::next stops reading the file there).
+bool parse_fastx(char const* d, size_t n, std::function<void(char const*, size_t)> const& emit);
+
+// Inflate a file (gzip or plain; gzread passes plain files through).
+std::string slurp(std::string const& path);
+
+// Read files [first, first + count) with `threads` threads; file i gets color
+// color_base + (i - first).  Throws on an unreadable file.
+void read_files(std::vector<std::string> const& files, size_t first, size_t count,
+                uint32_t color_base, uint32_t threads, seq_batch& out);
+
+// ---- bucket files (bucket_io.hpp:19-40) ------------------------------------
+// Append one LZ4 frame per non-empty bucket slice to open bucket files.
+class bucket_file_set {
+public:
+    bucket_file_set(std::string dir, uint32_t num_buckets);
+    ~bucket_file_set();
+    std::string path(uint32_t b) const;
+    // raw: serialized records of all buckets; boff: B + 1 byte offsets.
+    void append_frames(uint8_t const* raw, uint64_t const* boff, uint32_t threads);
+    // EOF markers, close; returns per-bucket uncompressed bytes.
+    void close();
+    std::vector<uint64_t> const& unc_bytes() const { return m_unc; }
+    uint64_t comp_bytes() const { return m_comp; }
+
+private:
+    std::string m_dir;
+    uint32_t m_B;
+    std::vector<void*> m_files;
+    std::vector<uint64_t> m_unc;
+    uint64_t m_comp = 0;
+};
+
+// Decompressed contents of bucket files 0..B-1 back to back (buffer from
+// `alloc`), with `chunk_off` = byte offsets of frame starts (records never
+// straddle a frame) and `chunk_bucket` = the bucket of each chunk.
+struct bucket_bytes {
+    uint8_t* data = nullptr;
+    uint64_t nbytes = 0;
+    std::vector<uint64_t> chunk_off;   // nchunks + 1
+    std::vector<uint32_t> chunk_bucket;
+    std::vector<uint64_t> bucket_unc;  // B
+};
+void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
+                       std::function<uint8_t*(uint64_t)> const& alloc, bucket_bytes& out,
+                       bool delete_after);
+
+// ---- .color_sets finalize layout (streaming_color_set_dict.hpp:221-294) ----
+// header [u32 C][u32 floor(.25C)][u32 floor(.75C)][u64 bits][u64 words],
+// the words, then Elias-Fano of the class bit offsets plus the total, in the
+// layout of this project's `bits` stand-in (u64 universe, u64 n, u64 l, then
+// the low and high bit vectors each as [u64 num_bits][u64 num_words][words]).
+void write_color_sets(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
+                      uint64_t const* offsets, uint64_t nclasses);
+
+}  // namespace io
+}  // namespace cdbg

@@ -1,0 +1,166 @@
+/* C-ABI of the B200 (sm_100a) implementation of cdbg-builder's phase 1
+ * (bucket-write) and phase 2 (bucket-process).
+ *
+ * Plain pointers and sizes only.  Every function returns 0 on success and a
+ * negative code on failure; cdbg_last_error() then describes the failure
+ * (thread-local).  The reference throws std::runtime_error in the same
+ * situations (bucket_io.hpp:255-272, 681-699; seq_reader.hpp:48); the C++
+ * adapter in INTEGRATION.md turns a non-zero return back into that exception.
+ *
+ * Reference interfaces replaced (paths relative to the reference repository):
+ *   cdbg_gpu_phase1  <- ingest_bucketed(files, k, m, B, bucket_writer&, T, ...)
+ *                       include/phase1_bucket_write/bucket_ingester.hpp:183-215,
+ *                       plus bucket_writer::close() (bucket_io.hpp:389-415) that
+ *                       builder.hpp:195 calls right after it.
+ *   cdbg_gpu_phase2  <- process_buckets(writer, k, num_colors, T, sink,
+ *                       global_dict, mu, done, mem_budget, delete_consumed)
+ *                       include/phase2_bucket_process/bucket_walker.hpp:607-779
+ *                       with frag_unitig_writer::write_batch as the sink
+ *                       (unitig_spill.hpp:491-522) and
+ *                       streaming_color_set_dict::intern_with_hashes as the
+ *                       color-set merge (streaming_color_set_dict.hpp:148-182).
+ *   cdbg_gpu_build   <- the two calls above back to back, in memory (no bucket
+ *                       files): builder.hpp:180 + :269.
+ */
+#ifndef CDBG_GPU_H
+#define CDBG_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CDBG_GPU_VERSION 1
+
+typedef struct cdbg_engine cdbg_engine;
+
+/* Engine: one CUDA device, one stream, a cached device arena.  Not
+ * thread-safe: one host thread drives one engine. */
+int cdbg_engine_create(int device, cdbg_engine** out);
+void cdbg_engine_destroy(cdbg_engine* e);
+const char* cdbg_last_error(void);
+int cdbg_gpu_version(void);
+
+/* Sequences of many inputs back to back: seq[seq_off[i] .. seq_off[i+1]) is
+ * sequence i (ASCII; A/C/G/T in either case are bases, anything else splits
+ * runs), of color seq_color[i].  With on_device = 1 all three pointers are
+ * device pointers (inputs already resident in HBM). */
+typedef struct cdbg_seq_batch {
+    const char* seq;
+    uint64_t seq_bytes;
+    const uint64_t* seq_off; /* num_seqs + 1 */
+    const uint32_t* seq_color;
+    uint32_t num_seqs;
+    int32_t on_device;
+} cdbg_seq_batch;
+
+/* Host reader: FASTA/FASTQ (optionally gzip) files -> one sequence batch,
+ * file i = color first_color + i, with the record rules of kseq_read
+ * (external/kseq.h) that the reference's seq_reader::next uses
+ * (phase1_bucket_write/seq_reader.hpp:66).  The buffers belong to the
+ * library until cdbg_free_sequences. */
+int cdbg_read_sequences(const char* const* files, uint32_t num_files, uint32_t first_color,
+                        uint32_t host_threads, cdbg_seq_batch* out);
+void cdbg_free_sequences(cdbg_seq_batch* b);
+
+/* ---- phase 1 ------------------------------------------------------------ */
+
+typedef struct cdbg_phase1_args {
+    const char* const* files; /* file i = color i (FASTA/FASTQ, optionally gzip) */
+    uint32_t num_files;
+    uint32_t k;               /* <= 63 */
+    uint32_t m;               /* 0 = compute_best_m(k) (minimizer.hpp:65) */
+    uint32_t num_buckets;
+    const char* tmp_dir;      /* bucket_<b>.bin written here */
+    uint32_t host_threads;    /* inflate / parse / LZ4 threads (0 = all cores) */
+    uint64_t chunk_bytes;     /* sequence bytes per device pass (0 = 8 GiB) */
+    uint64_t* bucket_unc_bytes; /* out, num_buckets entries, may be NULL */
+} cdbg_phase1_args;
+
+typedef struct cdbg_phase1_stats {
+    uint64_t input_bytes;     /* on-disk bytes of the inputs */
+    uint64_t seq_bytes;       /* sequence characters */
+    uint64_t n_kmers;         /* k-mers in ACGT runs >= k (the throughput unit) */
+    uint64_t n_supers;        /* super-k-mer occurrences */
+    uint64_t n_records;       /* records written after dedup */
+    uint64_t unc_bytes, comp_bytes;
+    double seconds_total, seconds_device;
+} cdbg_phase1_stats;
+
+int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats* s);
+
+/* Every super-k-mer occurrence of a batch in emission order, written to
+ * dump_path as: u64 count, then per occurrence [u32 bucket][u8 flags]
+ * [u32 color][u32 len][ceil(len/4) 2-bit packed bases].  Parity aid; the
+ * layout matches the recording harness used to dump the reference's own
+ * emit_super_kmers (bucket_ingester.hpp:36-127). */
+int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, uint32_t m,
+                         uint32_t num_buckets, const char* dump_path, uint64_t* n_supers);
+
+/* ---- phase 2 ------------------------------------------------------------ */
+
+/* Called once per new color class in global cid order (the order the
+ * reference's streaming_color_set_dict assigns ids when buckets are processed
+ * in order by one thread).  `colors` is ascending. */
+typedef void (*cdbg_class_cb)(void* ctx, const uint32_t* colors, uint64_t n);
+
+typedef struct cdbg_phase2_args {
+    const char* tmp_dir;         /* holds bucket_<b>.bin */
+    uint32_t num_buckets;
+    uint32_t k;
+    uint32_t num_colors;
+    const char* frag_path;       /* frag_unitigs.bin (unitig_spill.hpp:642-665 layout) */
+    const char* color_sets_path; /* finalized .color_sets, or NULL */
+    cdbg_class_cb on_class;      /* may be NULL */
+    void* ctx;
+    int32_t delete_consumed;     /* remove bucket files after reading */
+    uint32_t host_threads;
+    uint64_t batch_occ;          /* k-mer occurrences per device batch (0 = auto) */
+} cdbg_phase2_args;
+
+typedef struct cdbg_phase2_stats {
+    uint64_t n_records;
+    uint64_t n_kmers;            /* k-mer occurrences rolled (reference "k-mers rolled") */
+    uint64_t n_distinct;         /* distinct (bucket, canonical k-mer) nodes */
+    uint64_t n_fragments;        /* frag_unitig_writer::count() */
+    uint64_t total_seq_bytes;    /* frag_unitig_writer::total_seq_bytes() */
+    uint64_t n_color_sets;       /* streaming_color_set_dict::size() */
+    uint64_t total_integers;     /* sum of class sizes */
+    uint64_t color_bits;         /* encoded bits of all classes */
+    double seconds_total, seconds_device;
+} cdbg_phase2_stats;
+
+int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats* s);
+
+/* ---- whole path in memory ---------------------------------------------- */
+
+typedef struct cdbg_build_params {
+    uint32_t k, m, num_buckets, num_colors;
+    uint64_t batch_occ;          /* 0 = auto */
+    int32_t outputs_to_host;     /* 1 = copy frag bytes and color-set words to host */
+} cdbg_build_params;
+
+typedef struct cdbg_build_result {
+    /* Owned by the engine, valid until its next call.  Host pointers when
+     * outputs_to_host = 1, else device pointers. */
+    const uint8_t* frag_bytes;   /* frag_unitigs.bin contents */
+    uint64_t frag_nbytes;
+    const uint64_t* class_words; /* .color_sets bit-vector words */
+    uint64_t class_bits;
+    const uint64_t* class_offsets; /* bit offset of each class */
+    uint64_t n_color_sets;
+    uint64_t total_integers;
+    uint64_t n_kmers, n_supers, n_records, n_occ, n_distinct, n_fragments, total_seq_bytes;
+    uint64_t h2d_bytes, d2h_bytes;
+    double ms_phase1, ms_phase2, ms_total; /* device time (CUDA events) */
+} cdbg_build_result;
+
+int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
+                   cdbg_build_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

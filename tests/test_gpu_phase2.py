@@ -1,0 +1,95 @@
+"""GPU phase 2 vs the reference's own process_buckets (golden outputs and
+oracle/_ref runs): frag_unitigs.bin and .color_sets must be byte-identical."""
+import filecmp
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden_case, golden_filelist, ref_bin, run_ref
+from cdbg_gpu import formats, native, synth
+import make_golden
+
+pytestmark = pytest.mark.gpu
+CASES = ["tiny_k31", "tiny_k63", "tiny_skew_fq"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_phase2_on_reference_buckets(engine, case, tmp_path):
+    d, meta = golden_case(case)
+    bdir = str(tmp_path / "b")
+    make_golden.unpack_buckets(d, bdir)
+    frag = str(tmp_path / "frag_unitigs.bin")
+    cs = str(tmp_path / "out.color_sets")
+    st = engine.phase2(bdir, meta["num_buckets"], meta["k"], meta["num_colors"], frag, cs)
+    assert st.n_fragments == int(meta["phase2"]["fragments"])
+    assert st.n_color_sets == int(meta["phase2"]["num_color_sets"])
+    assert filecmp.cmp(frag, os.path.join(d, "frag_unitigs.bin"), shallow=False)
+    assert filecmp.cmp(cs, os.path.join(d, "out.color_sets"), shallow=False)
+
+
+def _fresh(tmp_path, seed, n, **kw):
+    base = dict(len_min=40000, len_max=90000, div_min=0.001, div_max=0.02, indels=10, mobile_pool=3,
+                mobile_min=1000, mobile_max=3000, contigs_min=1, contigs_max=20, contigs_log=1,
+                lowercase_runs=1, n_runs=1)
+    base.update(kw)
+    p = synth.make_params(seed=seed, **base)
+    return synth.write_fasta(p, n, str(tmp_path / "in"))
+
+
+@pytest.mark.parametrize("k,n,B,extra", [
+    (31, 8, 128, {}),
+    (63, 6, 128, dict(tandem_frac=0.02, repeat_pool=4, repeats_per_genome=6)),
+    (31, 10, 64, dict(lowcomp_frac=0.10)),
+    (31, 40, 256, dict(len_min=10000, len_max=30000)),
+])
+def test_phase2_vs_reference_fresh(engine, oracle, tmp_path, k, n, B, extra):
+    r2 = ref_bin("ref_phase2", k)
+    if not r2:
+        pytest.skip("oracle/_ref not built")
+    lst = _fresh(tmp_path, 1000 + k + n, n, **extra)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    bdir = tmp_path / "gb"
+    os.makedirs(bdir)
+    engine.phase1(files, k, B, str(bdir))
+    run_ref([r2, str(bdir), str(B), str(k), str(n), "1", str(tmp_path / "ref")])
+    frag = str(tmp_path / "frag_unitigs.bin")
+    cs = str(tmp_path / "out.color_sets")
+    engine.phase2(str(bdir), B, k, n, frag, cs)
+    assert filecmp.cmp(frag, str(tmp_path / "ref" / "frag_unitigs.bin"), shallow=False)
+    assert filecmp.cmp(cs, str(tmp_path / "ref" / "out.color_sets"), shallow=False)
+
+
+def test_batching_does_not_change_results(engine, tmp_path):
+    lst = _fresh(tmp_path, 77, 6)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    B = 128
+    bdir = tmp_path / "gb"
+    os.makedirs(bdir)
+    engine.phase1(files, 31, B, str(bdir))
+    outs = []
+    for occ in (0, 5000, 100000):
+        frag = str(tmp_path / ("f%d" % occ))
+        cs = str(tmp_path / ("c%d" % occ))
+        engine.phase2(str(bdir), B, 31, 6, frag, cs, batch_occ=occ)
+        outs.append((open(frag, "rb").read(), open(cs, "rb").read()))
+    assert outs[0] == outs[1] == outs[2]
+
+
+def test_in_memory_build_matches_file_path(engine, tmp_path):
+    lst = _fresh(tmp_path, 5, 5)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    B, k = 128, 31
+    bdir = tmp_path / "gb"
+    os.makedirs(bdir)
+    engine.phase1(files, k, B, str(bdir))
+    frag = str(tmp_path / "frag")
+    classes = []
+    engine.phase2(str(bdir), B, k, 5, frag, str(tmp_path / "cs"), on_class=lambda c: classes.append(list(c)))
+    hs = native.HostSequences(files)
+    r = engine.build(hs.batch, k, B, 5)
+    assert native.result_frag_bytes(r) == open(frag, "rb").read()
+    C, words, offsets, decoded = formats.read_color_sets(str(tmp_path / "cs"))
+    assert list(native.result_class_offsets(r)) == offsets
+    assert np.array_equal(native.result_class_words(r), words)
+    assert decoded == classes
