@@ -76,7 +76,9 @@ __global__ void __launch_bounds__(EV_THREADS)
         uint32_t s = upper_bound_u64(seq_off, num_seqs + 1, p0);
         uint64_t next_start = (s <= num_seqs) ? seq_off[s] : ~0ull;
         bool start_here = (s > 0 && seq_off[s - 1] == p0);
-        bool pvalid = (p0 > 0 && !start_here) ? (nuc_code(ascii[p0 - 1]) != 0xffu) : false;
+        // validity of the byte before p0, whatever sequence it belongs to: a
+        // run of the previous sequence that ends exactly at p0 is closed here
+        bool pvalid = (p0 > 0) ? (nuc_code(ascii[p0 - 1]) != 0xffu) : false;
         for (uint64_t p = p0; p < pend; ++p) {
             bool is_seq_start = (p == p0) ? start_here : false;
             while (p == next_start) {

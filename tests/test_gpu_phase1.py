@@ -80,3 +80,33 @@ def test_phase1_chunked_is_valid(engine, oracle, tmp_path):
                     out.add((bases, c, fl & 12))
             return out
         assert pairs(tmp_path / "a") == pairs(tmp_path / "b")
+
+
+def test_sequence_boundaries_on_chunk_edges(engine, oracle, tmp_path):
+    """Sequences whose starts fall on 32-byte multiples, runs that end exactly
+    at a sequence end, empty sequences, N runs at the edges, lower case."""
+    import random
+    rnd = random.Random(5)
+    seqs = []
+    for i in range(60):
+        n = rnd.choice([32, 64, 96, 33, 31, 128, 0, 256, 1000])
+        s = "".join(rnd.choice("ACGTacgt") for _ in range(n))
+        if n > 40 and i % 3 == 0:
+            s = "NN" + s[2:-3] + "NNN"
+        seqs.append(s)
+    d = tmp_path / "in"
+    os.makedirs(d)
+    files = []
+    for c in range(3):
+        p = d / ("c%d.fa" % c)
+        with open(p, "w") as f:
+            for j, s in enumerate(seqs[c::3]):
+                f.write(">s%d\n%s\n" % (j, s))
+        files.append(str(p))
+    lst = str(d / "list.txt")
+    open(lst, "w").write("".join(f + "\n" for f in files))
+    for k in (21, 31):
+        oracle.phase1(lst, k, 64, dump=str(tmp_path / "o.bin"))
+        hs = native.HostSequences(files)
+        engine.dump_supers(hs.batch, k, 0, 64, str(tmp_path / "g.bin"))
+        assert filecmp.cmp(str(tmp_path / "o.bin"), str(tmp_path / "g.bin"), shallow=False), k
