@@ -1,0 +1,355 @@
+"""Benchmark: phase 1 + phase 2 k-mers/s on one B200 (or N replicas).
+
+Workload (default): the pangenome configuration -- 1000 synthetic genomes of
+~4.8 Mbp derived from one seeded ancestor (0.1-2% SNPs, 20 indels, one mobile
+insert, 1-200 contigs), k = 31, m = 12, 4096 buckets.  A step is one full pass
+of phase 1 + phase 2 over the whole collection (all k-mers), producing the
+frag spill and the color classes.
+
+  value   k-mers/s with the sequences already resident in HBM and the outputs
+          left on the device (cdbg_gpu_build, on_device = 1).
+  e2e     the same call with pinned host input buffers and host outputs: the
+          H2D copy of the sequences and the D2H copy of the frag bytes and the
+          color-set words are inside every timed step.
+
+Time is measured with CUDA events on the stream the library launches on
+(the engine runs on a torch stream), max over ranks.  `--impl reference`
+times the reference's own CPU build (oracle/_ref/cdbg-build, built from its
+sources) on a bounded sample with all host cores.  With --gpus N each rank
+builds its own collection (independent replicas, weak scaling).
+"""
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cdbg-builder_b200"))
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "cdbg-build")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="pangenome")
+    ap.add_argument("--genomes", type=int, default=0, help="override genome count (0 = workload's)")
+    ap.add_argument("--cpu-sample-genomes", type=int, default=24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch-occ", type=int, default=0)
+    ap.add_argument("--out", default="")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), \
+        int(os.environ.get("WORLD_SIZE", "1"))
+
+
+def count_kmers(lens, k):
+    import numpy as np
+    l = lens.astype(np.int64)
+    return int(np.maximum(l - k + 1, 0).sum())
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                   "--format=csv,noheader,nounits", "-lms", "200"],
+                                  stdout=self.f, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        d = json.load(open(PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference_sample(genomes, k, blog2, threads, seed, workdir):
+    """One reference build of `genomes` genomes; returns (kmers, seconds p1+p2, detail)."""
+    from cdbg_gpu import synth
+    p, _, _, _ = synth.preset("pangenome", seed=seed)
+    ind = os.path.join(workdir, "in")
+    if not os.path.exists(os.path.join(ind, "filenames.txt")):
+        synth.write_fasta(p, genomes, ind, gzip_level=1)
+    _, lens, _ = synth.collection(p, genomes)
+    kmers = count_kmers(lens, k)
+    out = os.path.join(workdir, "o")
+    shutil.rmtree(out, ignore_errors=True)
+    os.makedirs(out)
+    r = subprocess.run([REF_BIN, "-i", os.path.join(ind, "filenames.txt"), "-k", str(k), "-o",
+                        os.path.join(out, "out"), "-t", str(threads), "-b", str(blog2), "-d",
+                        os.path.join(out, "tmp")], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference build failed: " + r.stderr[-500:])
+    t1 = float(re.search(r"\[bucket-write\] ([0-9.eE+-]+) s", r.stdout).group(1))
+    t2 = float(re.search(r"\[bucket-process\] ([0-9.eE+-]+) s", r.stdout).group(1))
+    return kmers, t1 + t2, {"bucket_write_s": t1, "bucket_process_s": t2}
+
+
+def reference_arm(a):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cdbg-build not built"}))
+        return 0
+    threads = os.cpu_count() or 1
+    k, blog2 = 31, 12
+    g = a.cpu_sample_genomes
+    work = tempfile.mkdtemp(prefix="cdbg_ref_")
+    try:
+        for _ in range(a.warmup):
+            run_reference_sample(g, k, blog2, threads, 1, work)
+        vals, secs = [], []
+        kmers = 0
+        for _ in range(a.steps):
+            kmers, s, det = run_reference_sample(g, k, blog2, threads, 1, work)
+            vals.append(kmers / s)
+            secs.append(s)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    v = statistics.median(vals)
+    sample = "%d of 1000 pangenome genomes (~4.8 Mbp, gzip FASTA), %d k-mers per step" % (g, kmers)
+    line = {"impl": "reference", "metric": "phase1+2 k-mers/s", "value": v, "unit": "k-mers/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1000 * statistics.median(secs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "pangenome: 1000 genomes x 4.8 Mbp, k=31, m=12, -b 12 (sampled)",
+                       "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "k-mers/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def main_gpu(a):
+    import numpy as np
+    import torch
+    from cdbg_gpu import native, synth
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    p, n_genomes, k, blog2 = synth.preset(a.workload, seed=1 + rank)
+    if a.genomes:
+        n_genomes = a.genomes
+    B = 1 << blog2
+    t0 = time.time()
+    seq, lens, per = synth.collection(p, n_genomes)
+    gen_s = time.time() - t0
+    off = np.zeros(len(lens) + 1, dtype=np.uint64)
+    off[1:] = np.cumsum(lens)
+    colors = np.repeat(np.arange(n_genomes, dtype=np.uint32), per)
+    kmers = count_kmers(lens, k)
+
+    # host (pinned) and device copies of the inputs
+    h_seq = torch.from_numpy(seq).pin_memory()
+    h_off = torch.from_numpy(off.view(np.int64)).pin_memory()
+    h_col = torch.from_numpy(colors.view(np.int32)).pin_memory()
+    d_seq = h_seq.to("cuda")
+    d_off = h_off.to("cuda")
+    d_col = h_col.to("cuda")
+    torch.cuda.synchronize()
+    dev_batch = native.SeqBatch(d_seq.data_ptr(), seq.nbytes, d_off.data_ptr(), d_col.data_ptr(),
+                                len(colors), 1)
+    host_batch = native.SeqBatch(h_seq.data_ptr(), seq.nbytes, h_off.data_ptr(), h_col.data_ptr(),
+                                 len(colors), 0)
+
+    stream = torch.cuda.Stream()
+    eng = native.Engine(local)
+    eng.set_stream(stream.cuda_stream)
+
+    def step(batch, to_host):
+        return eng.build(batch, k, B, n_genomes, batch_occ=a.batch_occ, outputs_to_host=to_host)
+
+    for _ in range(a.warmup):
+        r = step(dev_batch, False)
+    torch.cuda.synchronize()
+
+    # ---- value: device-resident inputs
+    clk = ClockSampler(local)
+    eng.profile(True)
+    barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    l0 = native.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    res = []
+    for _ in range(a.steps):
+        res.append(step(dev_batch, False))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = native.launch_count() - l0
+    clocks = clk.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / a.steps
+    kstats = eng.kernel_stats()
+    eng.profile(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    r = res[-1]
+    value = world * kmers / (ms / 1000.0)
+
+    # ---- e2e: pinned host buffers in, host outputs out
+    e2e = None
+    if not a.no_e2e:
+        step(host_batch, True)
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            re2 = step(host_batch, True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / a.steps
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
+               "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes)}
+
+    # ---- roofline for the dominant kernel
+    peak, peak_kind = peaks()
+    dom = max(kstats.items(), key=lambda kv: kv[1][0]) if kstats else None
+    roof = None
+    if dom:
+        name, (tot_ms, nl) = dom
+        w = 8 if k <= 31 else 16
+        per_launch_ms = tot_ms / nl
+        # algorithmic bytes per launch (DESIGN.md "roofline accounting")
+        alg = algorithmic_bytes(name, r, w, a.steps, nl)
+        ach = alg / (per_launch_ms / 1000.0) / 1e9 if alg else None
+        roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": (ach / peak) if ach else None, "traffic": None, "peak_kind": peak_kind,
+                "ms_per_launch": per_launch_ms, "launches_per_step": nl / a.steps,
+                "share_of_step": tot_ms / (ms * a.steps)}
+
+    # ---- CPU baseline (reference, bounded sample), rank 0 at N = 1
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(REF_BIN):
+        work = tempfile.mkdtemp(prefix="cdbg_cpu_")
+        try:
+            km, s, det = run_reference_sample(a.cpu_sample_genomes, k, blog2, os.cpu_count() or 1, 1, work)
+            cpu = {"value": km / s, "unit": "k-mers/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "%d of %d genomes, %d k-mers, reference cdbg-build -t %d -b %d (%s)" % (
+                       a.cpu_sample_genomes, n_genomes, km, os.cpu_count(), blog2, json.dumps(det))}
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+
+    if rank == 0:
+        top = sorted(kstats.items(), key=lambda kv: -kv[1][0])[:12]
+        line = {"metric": "phase1+2 k-mers/s", "value": value, "unit": "k-mers/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": "pangenome: %d genomes x 4.8 Mbp (0.1-2%% SNPs, 1-200 contigs), "
+                                       "k=%d, m=12, %d buckets, phase1+2 in HBM" % (n_genomes, k, B),
+                           "kmers_per_step": kmers, "bases": int(seq.nbytes),
+                           "l2": "inputs (%.1f GB) larger than L2" % (seq.nbytes / 1e9),
+                           "parallelism": "replicas%d" % world, "generate_s": gen_s},
+                "counts": {"supers": int(r.n_supers), "records": int(r.n_records), "occ": int(r.n_occ),
+                           "distinct": int(r.n_distinct), "fragments": int(r.n_fragments),
+                           "color_sets": int(r.n_color_sets), "frag_bytes": int(r.frag_nbytes)},
+                "phase_ms": {"phase1": r.ms_phase1, "phase2": r.ms_phase2},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks,
+                "kernels_ms_per_step": {kname: round(v[0] / a.steps, 3) for kname, v in top}}
+        s = json.dumps(line)
+        print(s)
+        if a.out:
+            with open(a.out, "w") as f:
+                f.write(s + "\n")
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def algorithmic_bytes(name, r, w, steps, launches):
+    """Algorithmic bytes of one launch of `name` (per-unit figures x units)."""
+    per_step = {
+        # phase 2 load: each k-mer occurrence read once (w + 4 B as a (k-mer, record) pair)
+        # and each distinct k-mer written once (w + 8 B: key + flags/rank/cid)
+        "k_insert": r.n_occ * (w + 4) + r.n_distinct * (w + 8),
+        "k_multi_pairs": r.n_occ * (w + 4),
+        "k_ext_mask": r.n_distinct * (w + 1),
+        "k_links": r.n_distinct * (w + 9),
+        "k_minimizers": r.n_kmers / 4.0 + r.n_supers * 16,
+        "k_rs_downsweep": 0,
+    }
+    v = per_step.get(name)
+    if v is None or v == 0:
+        return None
+    return v * steps / launches
+
+
+if __name__ == "__main__":
+    args = parse()
+    if args.impl == "reference":
+        sys.exit(reference_arm(args))
+    sys.exit(main_gpu(args))

@@ -91,6 +91,13 @@ SIGNATURES = {
     "cdbg_engine_destroy": (None, [ctypes.c_void_p]),
     "cdbg_last_error": (ctypes.c_char_p, []),
     "cdbg_gpu_version": (ctypes.c_int, []),
+    "cdbg_engine_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cdbg_launch_count": (ctypes.c_uint64, []),
+    "cdbg_engine_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "cdbg_engine_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64,
+                                                ctypes.POINTER(ctypes.c_double), c_u64p, ctypes.c_uint32]),
+    "cdbg_engine_copy_out": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_uint64]),
     "cdbg_read_sequences": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32,
                                            ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(SeqBatch)]),
     "cdbg_free_sequences": (None, [ctypes.POINTER(SeqBatch)]),
@@ -220,6 +227,26 @@ class Engine:
     def __exit__(self, *a):
         self.close()
 
+    def set_stream(self, stream_handle):
+        """Run on a caller-owned cudaStream_t (int handle, e.g. torch's
+        Stream.cuda_stream); None restores the engine's own stream."""
+        _check(lib().cdbg_engine_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    def profile(self, enable=True):
+        _check(lib().cdbg_engine_profile(self._h, 1 if enable else 0))
+
+    def kernel_stats(self):
+        """{kernel name: (total ms, launches)} collected while profiling."""
+        cap = 256
+        names = ctypes.create_string_buffer(64 * cap)
+        ms = (ctypes.c_double * cap)()
+        ln = (ctypes.c_uint64 * cap)()
+        n = lib().cdbg_engine_kernel_stats(self._h, names, len(names), ms, ln, cap)
+        if n < 0:
+            raise RuntimeError("kernel stats failed")
+        keys = names.raw.split(b"\0")[:min(n, cap)]
+        return {keys[i].decode(): (ms[i], ln[i]) for i in range(min(n, cap))}
+
     def dump_supers(self, batch, k, m, num_buckets, path):
         n = ctypes.c_uint64()
         _check(lib().cdbg_gpu_dump_supers(self._h, ctypes.byref(batch), k, m, num_buckets,
@@ -250,11 +277,22 @@ class Engine:
         _check(lib().cdbg_gpu_phase2(self._h, ctypes.byref(a), ctypes.byref(s)))
         return s
 
+    def copy_out(self, device_ptr, nbytes):
+        """Host bytes of a device-resident build output."""
+        buf = ctypes.create_string_buffer(max(1, nbytes))
+        _check(lib().cdbg_engine_copy_out(self._h, ctypes.c_void_p(device_ptr), buf, nbytes))
+        return buf.raw[:nbytes]
+
     def build(self, batch, k, num_buckets, num_colors, m=0, batch_occ=0, outputs_to_host=True):
         p = BuildParams(k, m, num_buckets, num_colors, batch_occ, 1 if outputs_to_host else 0)
         r = BuildResult()
         _check(lib().cdbg_gpu_build(self._h, ctypes.byref(batch), ctypes.byref(p), ctypes.byref(r)))
         return r
+
+
+def launch_count():
+    """Kernel launches issued by libcdbg_gpu.so in this process."""
+    return lib().cdbg_launch_count()
 
 
 def result_frag_bytes(r):

@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -78,6 +79,15 @@ public:
         return s;
     }
     size_t peak_bytes() const { return m_peak; }
+    // Bytes held in cached chunks but not handed out (reusable without cudaMalloc).
+    size_t cached_free() const {
+        size_t s = 0;
+        for (size_t i = 0; i < m_chunks.size(); ++i) {
+            if (i < m_cur) continue;
+            s += m_chunks[i].size - (i == m_cur ? m_chunks[i].used : 0);
+        }
+        return s;
+    }
     void set_chunk_bytes(size_t b) { m_chunk_bytes = b; }
 
 private:
@@ -96,6 +106,31 @@ private:
     size_t m_cur = 0;
     size_t m_chunk_bytes = size_t(1) << 30;
     size_t m_peak = 0;
+};
+
+// Growable device array (storage that outlives arena resets: the class
+// dictionary across bucket batches, device-resident outputs of a build).
+template <typename T>
+struct dvec {
+    T* p = nullptr;
+    size_t n = 0, cap = 0;
+    dvec() = default;
+    dvec(dvec const&) = delete;
+    ~dvec() {
+        if (p) cudaFree(p);
+    }
+    void reserve(size_t c, cudaStream_t st, bool zero_new = false) {
+        if (c <= cap) return;
+        size_t nc = std::max<size_t>(c, std::max<size_t>(cap * 2, 1024));
+        T* q = nullptr;
+        CDBG_CUDA(cudaMalloc(&q, nc * sizeof(T)));
+        if (n) CDBG_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        if (zero_new) CDBG_CUDA(cudaMemsetAsync(q + n, 0, (nc - n) * sizeof(T), st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        if (p) cudaFree(p);
+        p = q;
+        cap = nc;
+    }
 };
 
 }  // namespace cdbg

@@ -81,6 +81,77 @@ cdbg::seq_input stage_batch(cdbg_engine* e, cdbg_seq_batch const* b, uint64_t* h
     return in;
 }
 
+// Per-call scope: route kernel timing to this engine's profiler and fold the
+// recorded launches into its totals when the call returns.
+struct call_scope {
+    cdbg_engine* e;
+    explicit call_scope(cdbg_engine* en) : e(en) { cdbg::g_prof = &e->prof; }
+    ~call_scope() {
+        if (e->prof.on) e->prof.resolve();
+        cdbg::g_prof = nullptr;
+    }
+};
+
+// Host inverse of the hybrid encoder (compact_color_set_dict.hpp:176-222)
+// with delta(x) = Elias delta of x + 1, LSB-first.
+struct bit_reader {
+    std::vector<uint64_t> const& w;
+    uint64_t p;
+    uint64_t bit() {
+        const uint64_t i = p >> 6;
+        const uint64_t b = i < w.size() ? (w[i] >> (p & 63)) & 1 : 0;
+        ++p;
+        return b;
+    }
+    uint64_t take(uint32_t n) {
+        uint64_t v = 0;
+        for (uint32_t i = 0; i < n; ++i) v |= bit() << i;
+        return v;
+    }
+    uint64_t delta() {
+        uint32_t ll = 0;
+        while (!bit()) ++ll;
+        const uint64_t L1 = (1ull << ll) | take(ll);
+        const uint32_t l = (uint32_t)(L1 - 1);
+        return ((1ull << l) | take(l)) - 1;
+    }
+};
+void decode_class_host(std::vector<uint64_t> const& words, uint64_t pos, uint32_t C, std::vector<uint32_t>& out) {
+    out.clear();
+    bit_reader r{words, pos};
+    const uint64_t N = r.delta();
+    const uint64_t st = (uint64_t)(0.25 * C), dt = (uint64_t)(0.75 * C);
+    if (N == 0) return;
+    if (N < st) {
+        uint64_t v = r.delta();
+        out.push_back((uint32_t)v);
+        for (uint64_t i = 1; i < N; ++i) {
+            v += r.delta() + 1;
+            out.push_back((uint32_t)v);
+        }
+    } else if (N < dt) {
+        for (uint32_t i = 0; i < C; ++i)
+            if (r.bit()) out.push_back(i);
+    } else {
+        std::vector<uint32_t> absent;
+        if (C > N) {
+            uint64_t v = r.delta();
+            absent.push_back((uint32_t)v);
+            for (uint64_t i = 1; i < C - N; ++i) {
+                v += r.delta() + 1;
+                absent.push_back((uint32_t)v);
+            }
+        }
+        size_t a = 0;
+        for (uint32_t v = 0; v < C; ++v) {
+            if (a < absent.size() && absent[a] == v)
+                ++a;
+            else
+                out.push_back(v);
+        }
+    }
+}
+
 inline uint64_t host_bits64(std::vector<uint64_t> const& w, uint64_t pos) {
     const uint64_t i = pos >> 5;
     const uint32_t s = (uint32_t)(pos & 31) * 2;
@@ -92,6 +163,9 @@ inline uint64_t host_bits64(std::vector<uint64_t> const& w, uint64_t pos) {
 }  // namespace
 
 namespace cdbg {
+std::atomic<uint64_t> g_launches{0};
+thread_local kernel_profiler* g_prof = nullptr;
+
 void check_device_error(cdbg_engine* e, char const* stage) {
     uint32_t v = 0;
     CDBG_CUDA(cudaMemcpyAsync(&v, e->d_err, 4, cudaMemcpyDeviceToHost, e->st));
@@ -155,7 +229,8 @@ int cdbg_engine_create(int device, cdbg_engine** out) {
         CDBG_CUDA(cudaSetDevice(device));
         auto* e = new cdbg_engine();
         e->device = device;
-        CDBG_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        CDBG_CUDA(cudaStreamCreateWithFlags(&e->own_st, cudaStreamNonBlocking));
+        e->st = e->own_st;
         CDBG_CUDA(cudaMalloc(&e->d_err, 16));
         CDBG_CUDA(cudaMemset(e->d_err, 0, 16));
         *out = e;
@@ -170,12 +245,65 @@ void cdbg_engine_destroy(cdbg_engine* e) {
     cudaSetDevice(e->device);
     e->A.free_all();
     if (e->d_err) cudaFree(e->d_err);
-    if (e->st) cudaStreamDestroy(e->st);
+    e->prof.resolve();
+    if (e->own_st) cudaStreamDestroy(e->own_st);
     delete e;
+}
+
+int cdbg_engine_set_stream(cdbg_engine* e, void* stream) {
+    if (!e) return -1;
+    e->st = stream ? (cudaStream_t)stream : e->own_st;
+    return 0;
+}
+
+uint64_t cdbg_launch_count(void) { return cdbg::g_launches.load(); }
+
+int cdbg_engine_copy_out(cdbg_engine* e, const void* device_src, void* host_dst, uint64_t bytes) {
+    try {
+        if (!e) throw std::runtime_error("null engine");
+        if (bytes == 0) return 0;
+        CDBG_CUDA(cudaSetDevice(e->device));
+        CDBG_CUDA(cudaMemcpyAsync(host_dst, device_src, bytes, cudaMemcpyDeviceToHost, e->st));
+        CDBG_CUDA(cudaStreamSynchronize(e->st));
+        return 0;
+    } catch (std::exception const& ex) {
+        return fail(ex);
+    }
+}
+
+int cdbg_engine_profile(cdbg_engine* e, int32_t enable) {
+    if (!e) return -1;
+    e->prof.resolve();
+    if (enable) e->prof.totals.clear();
+    e->prof.on = enable != 0;
+    return 0;
+}
+
+int cdbg_engine_kernel_stats(cdbg_engine* e, char* names, uint64_t names_cap, double* ms,
+                             uint64_t* launches, uint32_t cap) {
+    if (!e) return -1;
+    e->prof.resolve();
+    uint32_t i = 0;
+    uint64_t used = 0;
+    for (auto const& kv : e->prof.totals) {
+        if (i >= cap) break;
+        const uint64_t len = kv.first.size() + 1;
+        if (names && used + len <= names_cap) std::memcpy(names + used, kv.first.c_str(), len);
+        used += len;
+        if (ms) ms[i] = kv.second.first;
+        if (launches) launches[i] = kv.second.second;
+        ++i;
+    }
+    return (int)e->prof.totals.size();
 }
 
 int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, uint32_t m,
                          uint32_t num_buckets, const char* dump_path, uint64_t* n_supers) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    call_scope scope_(e);
     try {
         if (m == 0) m = best_m(k);
         validate(k, m, num_buckets);
@@ -183,7 +311,7 @@ int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, ui
         e->A.reset();
         cdbg::seq_input in = stage_batch(e, b, nullptr);
         cdbg::run_table rt;
-        cdbg::build_runs(in, k, e->A, e->st, rt);
+        cdbg::build_runs(in, k, e->A, e->st, rt, e->A);
         cdbg::super_list sl;
         cdbg::find_supers(rt, k, m, num_buckets, e->A, e->st, sl, e->d_err);
         cdbg::check_device_error(e, "super-k-mers");
@@ -233,6 +361,11 @@ int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, ui
 }
 
 int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats* s) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    call_scope scope_(e);
     try {
         auto t0 = std::chrono::steady_clock::now();
         const uint32_t k = a->k;
@@ -270,11 +403,11 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
                              (uint32_t)hb.color.size(), 0};
             cdbg::seq_input in = stage_batch(e, &b, nullptr);
             cdbg::run_table rt;
-            cdbg::build_runs(in, k, e->A, e->st, rt);
+            cdbg::build_runs(in, k, e->A, e->st, rt, e->A);
             cdbg::super_list sl;
             cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err);
             cdbg::record_set rs;
-            cdbg::build_records(rt, sl, k, a->num_buckets, e->A, e->st, rs, e->d_err);
+            cdbg::build_records(rt, sl, k, a->num_buckets, e->A, e->st, rs, e->d_err, e->A);
             cdbg::serialized_buckets sb;
             cdbg::serialize_records(rs, e->A, e->st, sb);
             cdbg::check_device_error(e, "phase 1");
@@ -309,6 +442,11 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
 }
 
 int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats* s) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    call_scope scope_(e);
     try {
         auto t0 = std::chrono::steady_clock::now();
         CDBG_CUDA(cudaSetDevice(e->device));
@@ -346,7 +484,6 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         pp.num_colors = a->num_colors;
         pp.batch_occ = a->batch_occ;
         pp.to_host = true;
-        pp.keep_lists = a->on_class != nullptr;
         cdbg::phase2_result res;
         cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, res);
         const double dev_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - td).count();
@@ -363,9 +500,13 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         if (a->color_sets_path)
             cdbg::io::write_color_sets(a->color_sets_path, a->num_colors, res.words.data(), res.nbits,
                                        res.offsets.data(), res.n_classes);
-        if (a->on_class)
-            for (uint64_t c = 0; c < res.n_classes; ++c)
-                a->on_class(a->ctx, res.lists.data() + res.list_off[c], res.list_off[c + 1] - res.list_off[c]);
+        if (a->on_class) {
+            std::vector<uint32_t> cls;
+            for (uint64_t c = 0; c < res.n_classes; ++c) {
+                decode_class_host(res.words, res.offsets[c], a->num_colors, cls);
+                a->on_class(a->ctx, cls.data(), cls.size());
+            }
+        }
         if (s) {
             cdbg_phase2_stats st{};
             st.n_records = rs.n;
@@ -389,24 +530,32 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
 }
 
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p, cdbg_build_result* r) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    call_scope scope_(e);
     try {
         const uint32_t k = p->k;
         const uint32_t m = p->m ? p->m : best_m(k);
         validate(k, m, p->num_buckets);
         CDBG_CUDA(cudaSetDevice(e->device));
         e->A.reset();
+        e->P.reset();
         cdbg_build_result res{};
         cudaEvent_t ev[4];
         for (auto& x : ev) CDBG_CUDA(cudaEventCreate(&x));
         CDBG_CUDA(cudaEventRecord(ev[0], e->st));
         cdbg::seq_input in = stage_batch(e, b, &res.h2d_bytes);
         cdbg::run_table rt;
-        cdbg::build_runs(in, k, e->A, e->st, rt);
+        cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
         cdbg::super_list sl;
         cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err);
         cdbg::record_set rs;
-        cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err);
+        cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
         cdbg::check_device_error(e, "phase 1");
+        const uint64_t n_kmers = rt.n_kmers, n_supers = sl.n;
+        e->A.reset();  // phase-1 scratch (staged input, super-k-mers, sort buffers)
         CDBG_CUDA(cudaEventRecord(ev[1], e->st));
         cdbg::phase2_params pp;
         pp.k = k;
@@ -414,6 +563,9 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         pp.batch_occ = p->batch_occ;
         pp.to_host = p->outputs_to_host != 0;
         cdbg::phase2_result out;
+        out.d_frag_out = &e->out_frag;
+        out.d_words_out = &e->out_words;
+        out.d_offsets_out = &e->out_offsets;
         cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, out);
         CDBG_CUDA(cudaEventRecord(ev[2], e->st));
         CDBG_CUDA(cudaEventSynchronize(ev[2]));
@@ -424,8 +576,8 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         res.ms_phase1 = ms1;
         res.ms_phase2 = ms2;
         res.ms_total = ms1 + ms2;
-        res.n_kmers = rt.n_kmers;
-        res.n_supers = sl.n;
+        res.n_kmers = n_kmers;
+        res.n_supers = n_supers;
         res.n_records = rs.n;
         res.n_occ = out.n_occ;
         res.n_distinct = out.n_distinct;

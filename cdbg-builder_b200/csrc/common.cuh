@@ -4,12 +4,80 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <map>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace cdbg {
 
 typedef unsigned __int128 u128;
+
+extern std::atomic<uint64_t> g_launches;
+
+// Per-kernel device time with CUDA events on the launching stream.  Enabled
+// per engine call; a scope records an event before and after the launch it
+// encloses, and resolve() folds the finished pairs into per-name totals.
+struct kernel_profiler {
+    struct pending {
+        char const* name;
+        cudaEvent_t a, b;
+    };
+    bool on = false;
+    std::vector<pending> open;
+    std::vector<cudaEvent_t> pool;
+    std::map<std::string, std::pair<double, uint64_t>> totals;  // ms, launches
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void resolve() {
+        for (auto& p : open) {
+            float ms = 0;
+            cudaEventSynchronize(p.b);
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            auto& t = totals[p.name];
+            t.first += ms;
+            t.second += 1;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        open.clear();
+    }
+    ~kernel_profiler() {
+        resolve();
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+extern thread_local kernel_profiler* g_prof;
+
+struct prof_scope {
+    kernel_profiler* p;
+    cudaStream_t st;
+    char const* name;
+    cudaEvent_t a{};
+    prof_scope(char const* n, cudaStream_t s) : p(g_prof && g_prof->on ? g_prof : nullptr), st(s), name(n) {
+        if (p) {
+            a = p->get();
+            cudaEventRecord(a, st);
+        }
+    }
+    ~prof_scope() {
+        if (p) {
+            cudaEvent_t b = p->get();
+            cudaEventRecord(b, st);
+            p->open.push_back({name, a, b});
+        }
+    }
+};
+#define CDBG_PROF(name, st) ::cdbg::prof_scope cdbg_prof_scope_(name, st)
 
 #define CDBG_CUDA(call)                                                                        \
     do {                                                                                       \
@@ -19,7 +87,13 @@ typedef unsigned __int128 u128;
                                      " at " + __FILE__ + ":" + std::to_string(__LINE__));      \
     } while (0)
 
-#define CDBG_CHECK_LAUNCH() CDBG_CUDA(cudaGetLastError())
+// Every kernel launch is followed by this check, which also counts launches
+// (the count is exported through cdbg_launch_count()).
+#define CDBG_CHECK_LAUNCH()                 \
+    do {                                    \
+        ::cdbg::g_launches.fetch_add(1);    \
+        CDBG_CUDA(cudaGetLastError());      \
+    } while (0)
 
 // Device-side error words.  Kernels never trap: a bounded loop that runs out,
 // a table that fills up or a size that overflows a field sets a code here and

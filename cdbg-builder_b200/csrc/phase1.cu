@@ -607,22 +607,29 @@ T read_dev(T const* p, cudaStream_t st) {
 }  // namespace
 
 // ----------------------------------------------------------------- host side
-void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt) {
+void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt,
+                dev_arena& out) {
     rt = run_table();
     const uint64_t npos = in.nbytes + 1;
     const uint64_t tiles = ceil_div(npos, EV_TILE);
     uint32_t* tcount = A.alloc<uint32_t>(tiles);
     uint64_t* toff = A.alloc<uint64_t>(tiles + 1);
-    k_run_events<false><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
-                                                                 in.num_seqs, tcount, nullptr, nullptr);
+    {
+        CDBG_PROF("k_run_events", st);
+        k_run_events<false><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
+                                                                     in.num_seqs, tcount, nullptr, nullptr);
+    }
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, tiles, A, st, toff + tiles);
     const uint64_t nev = read_dev(toff + tiles, st);
     const uint64_t nraw = nev / 2;
     if (nraw == 0) return;
     uint64_t* ev = A.alloc<uint64_t>(nev);
-    k_run_events<true><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
-                                                                in.num_seqs, tcount, toff, ev);
+    {
+        CDBG_PROF("k_run_events", st);
+        k_run_events<true><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
+                                                                    in.num_seqs, tcount, toff, ev);
+    }
     CDBG_CHECK_LAUNCH();
     uint64_t* src = A.alloc<uint64_t>(nraw);
     uint32_t* len = A.alloc<uint32_t>(nraw);
@@ -652,10 +659,13 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
     const uint64_t total = read_dev(rt.soff + nruns, st);
     const uint64_t nwd = total / 32;
     rt.nwords = nwd + 8;
-    rt.words = A.alloc<uint64_t>(rt.nwords);
+    rt.words = out.alloc<uint64_t>(rt.nwords);
     CDBG_CUDA(cudaMemsetAsync(rt.words + nwd, 0, 8 * 8, st));
     if (nwd) {
-        k_pack<<<grid(nwd, 256), 256, 0, st>>>(in.ascii, rt.n, rt.soff, rt.src, rt.len, nwd, rt.words);
+        {
+            CDBG_PROF("k_pack", st);
+            k_pack<<<grid(nwd, 256), 256, 0, st>>>(in.ascii, rt.n, rt.soff, rt.src, rt.len, nwd, rt.words);
+        }
         CDBG_CHECK_LAUNCH();
     }
     unsigned long long* acc = A.alloc<unsigned long long>(2);
@@ -683,8 +693,11 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
     const uint64_t ntiles = read_dev(tstart + rt.n, st);
     uint32_t* tcount = A.alloc<uint32_t>(ntiles);
     uint64_t* toff = A.alloc<uint64_t>(ntiles + 1);
-    k_minimizers<false><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
-        rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, nullptr, nullptr, nullptr, nullptr, d_err);
+    {
+        CDBG_PROF("k_minimizers", st);
+        k_minimizers<false><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+            rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, nullptr, nullptr, nullptr, nullptr, d_err);
+    }
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, ntiles, A, st, toff + ntiles);
     const uint64_t n = read_dev(toff + ntiles, st);
@@ -692,8 +705,11 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
     uint64_t* minv = A.alloc<uint64_t>(n);
     uint32_t* run = A.alloc<uint32_t>(n);
     uint32_t* aa = A.alloc<uint32_t>(n);
-    k_minimizers<true><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
-        rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, toff, minv, run, aa, d_err);
+    {
+        CDBG_PROF("k_minimizers", st);
+        k_minimizers<true><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+            rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, toff, minv, run, aa, d_err);
+    }
     CDBG_CHECK_LAUNCH();
     out.n = n;
     out.start = A.alloc<uint64_t>(n);
@@ -704,14 +720,17 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
     out.key = A.alloc<uint64_t>(n);
     uint32_t bb = 0;
     while ((1ull << bb) < B) ++bb;
-    k_super_finalize<<<grid(n, 256), 256, 0, st>>>(n, minv, run, aa, rt.soff, rt.len, rt.color, rt.words,
-                                                    k, B, bb, out.start, out.len, out.color, out.flags,
-                                                    out.bucket, out.key);
+    {
+        CDBG_PROF("k_super_finalize", st);
+        k_super_finalize<<<grid(n, 256), 256, 0, st>>>(n, minv, run, aa, rt.soff, rt.len, rt.color, rt.words,
+                                                        k, B, bb, out.start, out.len, out.color, out.flags,
+                                                        out.bucket, out.key);
+    }
     CDBG_CHECK_LAUNCH();
 }
 
 void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, dev_arena& A,
-                   cudaStream_t st, record_set& rs, uint32_t* d_err) {
+                   cudaStream_t st, record_set& rs, uint32_t* d_err, dev_arena& out) {
     (void)k;
     (void)d_err;
     rs = record_set();
@@ -719,11 +738,11 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     rs.words = rt.words;
     rs.nwords = rt.nwords;
     rs.n_occ_supers = sl.n;
-    rs.bucket_start = A.alloc<uint64_t>(B + 1);
+    rs.bucket_start = out.alloc<uint64_t>(B + 1);
     const uint64_t n = sl.n;
     if (n == 0) {
         CDBG_CUDA(cudaMemsetAsync(rs.bucket_start, 0, 8 * (B + 1), st));
-        rs.col_off = A.alloc<uint64_t>(1);
+        rs.col_off = out.alloc<uint64_t>(1);
         CDBG_CUDA(cudaMemsetAsync(rs.col_off, 0, 8, st));
         return;
     }
@@ -736,8 +755,11 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     prim::radix_sort_pairs<uint32_t>(skey, idx, n, 0, 64, A, st);
     uint32_t* head = A.alloc<uint32_t>(n);
     uint32_t* ckeep = A.alloc<uint32_t>(n);
-    k_group_heads<<<grid(n, 256), 256, 0, st>>>(n, skey, idx, sl.start, sl.len, sl.color, rt.words,
-                                                 head, ckeep);
+    {
+        CDBG_PROF("k_group_heads", st);
+        k_group_heads<<<grid(n, 256), 256, 0, st>>>(n, skey, idx, sl.start, sl.len, sl.color, rt.words,
+                                                     head, ckeep);
+    }
     CDBG_CHECK_LAUNCH();
     uint64_t* rid = A.alloc<uint64_t>(n + 1);
     uint64_t* cpos = A.alloc<uint64_t>(n + 1);
@@ -750,17 +772,20 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     const uint64_t nr = tot[0], nc = tot[1];
     rs.n = nr;
     rs.ncolors = nc;
-    rs.start = A.alloc<uint64_t>(nr);
-    rs.len = A.alloc<uint32_t>(nr);
-    rs.flags = A.alloc<uint32_t>(nr);
-    rs.col_off = A.alloc<uint64_t>(nr + 1);
-    rs.colors = A.alloc<uint32_t>(nc);
+    rs.start = out.alloc<uint64_t>(nr);
+    rs.len = out.alloc<uint32_t>(nr);
+    rs.flags = out.alloc<uint32_t>(nr);
+    rs.col_off = out.alloc<uint64_t>(nr + 1);
+    rs.colors = out.alloc<uint32_t>(nc);
     uint32_t* rb = A.alloc<uint32_t>(nr);
     k_fill_u32<<<grid(nr, 256), 256, 0, st>>>(rs.flags, nr, 0xfu);
     CDBG_CHECK_LAUNCH();
-    k_records_fill<<<grid(n, 256), 256, 0, st>>>(n, idx, head, rid, ckeep, cpos, sl.start, sl.len,
-                                                  sl.color, sl.flags, sl.bucket, rs.start, rs.len,
-                                                  rs.flags, rs.col_off, rs.colors, rb);
+    {
+        CDBG_PROF("k_records_fill", st);
+        k_records_fill<<<grid(n, 256), 256, 0, st>>>(n, idx, head, rid, ckeep, cpos, sl.start, sl.len,
+                                                      sl.color, sl.flags, sl.bucket, rs.start, rs.len,
+                                                      rs.flags, rs.col_off, rs.colors, rb);
+    }
     CDBG_CHECK_LAUNCH();
     k_set_last_u64<<<1, 1, 0, st>>>(rs.col_off, nr, cpos + n);
     CDBG_CHECK_LAUNCH();
@@ -782,13 +807,19 @@ void serialize_records(record_set const& rs, dev_arena& A, cudaStream_t st, seri
         return;
     }
     uint64_t* sz = A.alloc<uint64_t>(rs.n);
-    k_rec_sizes<<<grid(rs.n, 256), 256, 0, st>>>(rs.n, rs.col_off, rs.colors, rs.len, rs.flags, sz);
+    {
+        CDBG_PROF("k_rec_sizes", st);
+        k_rec_sizes<<<grid(rs.n, 256), 256, 0, st>>>(rs.n, rs.col_off, rs.colors, rs.len, rs.flags, sz);
+    }
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint64_t, uint64_t>(sz, out.rec_off, rs.n, A, st, out.rec_off + rs.n);
     out.nbytes = read_dev(out.rec_off + rs.n, st);
     out.bytes = A.alloc<uint8_t>(out.nbytes + 16);
-    k_rec_write<<<grid(rs.n, 256), 256, 0, st>>>(rs.n, rs.col_off, rs.colors, rs.start, rs.len, rs.flags,
-                                                  rs.words, out.rec_off, out.bytes);
+    {
+        CDBG_PROF("k_rec_write", st);
+        k_rec_write<<<grid(rs.n, 256), 256, 0, st>>>(rs.n, rs.col_off, rs.colors, rs.start, rs.len, rs.flags,
+                                                      rs.words, out.rec_off, out.bytes);
+    }
     CDBG_CHECK_LAUNCH();
     k_bucket_bytes<<<grid(rs.B + 1, 256), 256, 0, st>>>(rs.B, rs.bucket_start, out.rec_off, out.bucket_off);
     CDBG_CHECK_LAUNCH();

@@ -53,7 +53,8 @@ struct phase1_stats {
 };
 
 // Runs + packing: ASCII -> 2-bit stream of ACGT runs >= k.
-void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt);
+// The 2-bit stream (rt.words) comes from `out`, everything else from A.
+void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt, dev_arena& out);
 
 // Super-k-mer occurrences of every run (for parity tests): arrays in input
 // order, allocated from the arena.  Returns the count.
@@ -70,8 +71,9 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
                  cudaStream_t st, super_list& out, uint32_t* d_err);
 
 // Dedup super-k-mers into canonical bucket records.
+// Record arrays come from `out`, temporaries from A.
 void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, dev_arena& A,
-                   cudaStream_t st, record_set& rs, uint32_t* d_err);
+                   cudaStream_t st, record_set& rs, uint32_t* d_err, dev_arena& out);
 
 // Serialized record bytes (reference record layout, super_kmer.hpp:105-117):
 // out bytes for all buckets back to back, bucket_bytes[B + 1] offsets (device).

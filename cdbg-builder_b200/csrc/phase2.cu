@@ -64,30 +64,6 @@ T read_dev(T const* p, cudaStream_t st) {
     return v;
 }
 
-// Growable device array (class dictionary storage that outlives batches).
-template <typename T>
-struct dvec {
-    T* p = nullptr;
-    size_t n = 0, cap = 0;
-    dvec() = default;
-    dvec(dvec const&) = delete;
-    ~dvec() {
-        if (p) cudaFree(p);
-    }
-    void reserve(size_t c, cudaStream_t st, bool zero_new = false) {
-        if (c <= cap) return;
-        size_t nc = std::max<size_t>(c, std::max<size_t>(cap * 2, 1024));
-        T* q = nullptr;
-        CDBG_CUDA(cudaMalloc(&q, nc * sizeof(T)));
-        if (n) CDBG_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        if (zero_new) CDBG_CUDA(cudaMemsetAsync(q + n, 0, (nc - n) * sizeof(T), st));
-        CDBG_CUDA(cudaStreamSynchronize(st));
-        if (p) cudaFree(p);
-        p = q;
-        cap = nc;
-    }
-};
-
 __device__ __forceinline__ uint32_t upper_bound_u64(uint64_t const* a, uint64_t n, uint64_t x) {
     uint64_t lo = 0, hi = n;
     while (lo < hi) {
@@ -526,176 +502,27 @@ __device__ __forceinline__ void cand_list(list_src const& L, uint32_t kind_id, u
         n = L.col_off[kind_id + 1] - L.col_off[kind_id];
     }
 }
-__device__ __forceinline__ bool lists_equal(uint32_t const* a, uint64_t na, uint32_t const* b, uint64_t nb) {
-    if (na != nb) return false;
-    for (uint64_t i = 0; i < na; ++i)
-        if (a[i] != b[i]) return false;
+
+// ---- bit ranges -------------------------------------------------------------
+__device__ __forceinline__ uint64_t bits_at(uint64_t const* w, uint64_t pos) {
+    const uint64_t i = pos >> 6;
+    const uint32_t s = (uint32_t)(pos & 63);
+    uint64_t v = w[i] >> s;
+    if (s) v |= w[i + 1] << (64 - s);
+    return v;
+}
+// Equal bit strings [pa, pa + la) of wa and [pb, pb + lb) of wb.  The hybrid
+// encoding is canonical, so equal encodings <=> equal color sets.
+__device__ __forceinline__ bool bits_equal(uint64_t const* wa, uint64_t pa, uint64_t la, uint64_t const* wb,
+                                           uint64_t pb, uint64_t lb) {
+    if (la != lb) return false;
+    for (uint64_t i = 0; i < la; i += 64) {
+        uint64_t x = bits_at(wa, pa + i) ^ bits_at(wb, pb + i);
+        const uint64_t n = la - i;
+        if (n < 64) x &= (1ull << n) - 1;
+        if (x) return false;
+    }
     return true;
-}
-
-struct dict_view {
-    uint64_t* slot_hash;
-    uint32_t* slot_cid;
-    uint64_t mask;
-    uint64_t const* cls_off;  // list offsets into cls_pool
-    uint32_t const* cls_pool;
-};
-
-__global__ void k_dict_lookup(uint64_t nc, cand_view cv, list_src L, dict_view D, uint32_t* __restrict__ cid) {
-    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    const uint64_t h = cv.hash[c];
-    uint32_t const* lp;
-    uint64_t ln;
-    cand_list(L, cv.kind_id[c], lp, ln);
-    uint32_t res = NONE32;
-    if (D.slot_hash) {
-        uint64_t s = h & D.mask;
-        for (uint64_t i = 0; i <= D.mask; ++i) {
-            const uint64_t sh = D.slot_hash[s];
-            if (sh == HASH_EMPTY) break;
-            if (sh == h) {
-                const uint32_t k = D.slot_cid[s];
-                const uint64_t a = D.cls_off[k], b = D.cls_off[k + 1];
-                if (lists_equal(lp, ln, D.cls_pool + a, b - a)) {
-                    res = k;
-                    break;
-                }
-            }
-            s = (s + 1) & D.mask;
-        }
-    }
-    cid[c] = res;
-}
-
-__global__ void k_new_flags(uint64_t nc, uint32_t const* __restrict__ cid, uint32_t* __restrict__ flag) {
-    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < nc) flag[c] = cid[c] == NONE32 ? 1u : 0u;
-}
-
-__global__ void k_new_gather(uint64_t nc, uint32_t const* __restrict__ flag, uint64_t const* __restrict__ pos,
-                             cand_view cv, uint64_t* __restrict__ nkey, uint32_t* __restrict__ nidx) {
-    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc || !flag[c]) return;
-    nkey[pos[c]] = cv.hash[c];
-    nidx[pos[c]] = (uint32_t)c;
-}
-
-__global__ void k_run_heads(uint64_t n, uint64_t const* __restrict__ key, uint32_t* __restrict__ head) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) head[i] = (i == 0 || key[i] != key[i - 1]) ? 1u : 0u;
-}
-
-// One thread per equal-hash run of new candidates: group members by list
-// equality (normally one group per run); rep[i] = representative candidate.
-__global__ void k_group_runs(uint64_t n, uint64_t const* __restrict__ key, uint32_t const* __restrict__ head,
-                             uint32_t const* __restrict__ nidx, cand_view cv, list_src L,
-                             uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !head[i]) return;
-    uint64_t e = i + 1;
-    while (e < n && !head[e]) ++e;
-    // members [i, e); reps are members whose rep is themselves
-    for (uint64_t j = i; j < e; ++j) {
-        const uint32_t cj = nidx[j];
-        uint32_t const* pj;
-        uint64_t lj;
-        cand_list(L, cv.kind_id[cj], pj, lj);
-        uint32_t r = cj;
-        for (uint64_t q = i; q < j; ++q) {
-            const uint32_t cq = nidx[q];
-            if (rep[cq] != cq) continue;
-            uint32_t const* pq;
-            uint64_t lq;
-            cand_list(L, cv.kind_id[cq], pq, lq);
-            if (lists_equal(pj, lj, pq, lq)) {
-                r = cq;
-                break;
-            }
-        }
-        rep[cj] = r;
-        const uint32_t f = cv.first[cj];
-        if (r == cj)
-            rep_first[cj] = f;
-        else if (f < rep_first[r])
-            rep_first[r] = f;
-    }
-}
-
-__global__ void k_rep_keys(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
-                           uint32_t const* __restrict__ rep_first, uint32_t* __restrict__ is_rep) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t c = nidx[i];
-    is_rep[i] = rep[c] == c ? 1u : 0u;
-    (void)rep_first;
-}
-
-__global__ void k_rep_gather(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ is_rep,
-                             uint64_t const* __restrict__ pos, uint32_t const* __restrict__ rep_first,
-                             uint64_t* __restrict__ rkey, uint32_t* __restrict__ rcand) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !is_rep[i]) return;
-    const uint32_t c = nidx[i];
-    rkey[pos[i]] = rep_first[c];
-    rcand[pos[i]] = c;
-}
-
-// New class j (in first-appearance order) = candidate rcand[j]; cid base+j.
-__global__ void k_assign_new(uint64_t nnew, uint32_t const* __restrict__ rcand, uint64_t base,
-                             uint32_t* __restrict__ cid) {
-    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < nnew) cid[rcand[j]] = (uint32_t)(base + j);
-}
-
-__global__ void k_assign_members(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
-                                 uint32_t* __restrict__ cid) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t c = nidx[i];
-    if (rep[c] != c) cid[c] = cid[rep[c]];
-}
-
-__global__ void k_new_sizes(uint64_t nnew, uint32_t const* __restrict__ rcand, cand_view cv, list_src L,
-                            uint64_t* __restrict__ sz, uint64_t* __restrict__ hashes) {
-    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nnew) return;
-    uint32_t const* p;
-    uint64_t n;
-    cand_list(L, cv.kind_id[rcand[j]], p, n);
-    sz[j] = n;
-    hashes[j] = cv.hash[rcand[j]];
-}
-
-// Copy new class lists into the dictionary pool (warp per class).
-__global__ void k_new_copy(uint64_t nnew, uint32_t const* __restrict__ rcand, cand_view cv, list_src L,
-                           uint64_t const* __restrict__ dst_off, uint32_t* __restrict__ pool) {
-    const uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (j >= nnew) return;
-    uint32_t const* p;
-    uint64_t n;
-    cand_list(L, cv.kind_id[rcand[j]], p, n);
-    uint32_t* d = pool + dst_off[j];
-    for (uint64_t i = threadIdx.x & 31; i < n; i += 32) d[i] = p[i];
-}
-
-__global__ void k_dict_insert(uint64_t c0, uint64_t c1, uint64_t const* __restrict__ cls_hash,
-                              uint64_t* __restrict__ slot_hash, uint32_t* __restrict__ slot_cid, uint64_t mask,
-                              uint32_t* err) {
-    uint64_t c = c0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= c1) return;
-    const uint64_t h = cls_hash[c];
-    uint64_t s = h & mask;
-    for (uint64_t i = 0; i <= mask; ++i) {
-        const uint64_t old = atomicCAS((unsigned long long*)&slot_hash[s], (unsigned long long)HASH_EMPTY,
-                                       (unsigned long long)h);
-        if (old == HASH_EMPTY) {
-            slot_cid[s] = (uint32_t)c;
-            return;
-        }
-        s = (s + 1) & mask;
-    }
-    set_error(err, ERR_TABLE_FULL);
 }
 
 // ---- hybrid encoding (hybrid_color_sets.hpp:48-95) with the delta code of
@@ -728,23 +555,24 @@ __device__ __forceinline__ uint64_t put_delta(uint64_t* w, uint64_t pos, uint64_
     return pos + l;
 }
 
-// Warp per new class.  Pass 0 (ENC = false): encoded size -> bits[j].
-// Pass 1: write at bit offset boff[j] of `words`.
+// Warp per candidate class.  Pass 0 (ENC = false): encoded size -> nbits[j].
+// Pass 1: write at bit offset boff[j] of `words` (zeroed).
 template <bool ENC>
-__global__ void k_encode(uint64_t nnew, uint64_t const* __restrict__ off, uint32_t const* __restrict__ pool,
-                         uint32_t C, uint64_t* __restrict__ nbits, uint64_t const* __restrict__ boff,
-                         uint64_t* __restrict__ words) {
+__global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint64_t* __restrict__ nbits,
+                         uint64_t const* __restrict__ boff, uint64_t* __restrict__ words) {
     extern __shared__ uint32_t smem_bm[];
     const uint32_t nw = (C + 31) / 32;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     uint32_t* bm = smem_bm + (size_t)wib * nw;
     const uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
-    if (j >= nnew) return;
-    const uint64_t a = off[j], N = off[j + 1] - off[j];
+    if (j >= nc) return;
+    uint32_t const* lp;
+    uint64_t N;
+    cand_list(L, cv.kind_id[j], lp, N);
     for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
     __syncwarp();
     for (uint64_t i = lane; i < N; i += 32) {
-        const uint32_t v = pool[a + i];
+        const uint32_t v = lp[i];
         atomicOr(&bm[v >> 5], 1u << (v & 31));
     }
     __syncwarp();
@@ -773,14 +601,13 @@ __global__ void k_encode(uint64_t nnew, uint64_t const* __restrict__ off, uint32
         if (valid < 32) x &= (1u << valid) - 1u;
         return x;
     };
-    // last element of this lane's range
     int32_t last = -1;
     for (uint32_t w = w0; w < w1; ++w) {
         const uint32_t x = word_bits(w);
         if (x) last = (int32_t)(w * 32 + 31 - __clz(x));
     }
     // previous element before this lane's range = max of `last` over lower lanes
-    int32_t prev = -1;
+    int32_t prev;
     {
         int32_t x = last;
         for (int o = 1; o < 32; o <<= 1) {
@@ -790,7 +617,6 @@ __global__ void k_encode(uint64_t nnew, uint64_t const* __restrict__ off, uint32
         prev = __shfl_up_sync(0xffffffffu, x, 1);
         if (lane == 0) prev = -1;
     }
-    // code lengths of this lane's elements
     uint64_t mybits = 0;
     {
         int32_t pv = prev;
@@ -822,6 +648,187 @@ __global__ void k_encode(uint64_t nnew, uint64_t const* __restrict__ off, uint32
             p = put_delta(words, p, pv < 0 ? (uint64_t)v : (uint64_t)(v - pv - 1));
             pv = v;
         }
+    }
+}
+
+// Global class dictionary as seen by kernels: hash slots -> class id, and the
+// classes' encodings (bit_off has n + 1 entries).
+struct dict_view {
+    uint64_t const* slot_hash;
+    uint32_t const* slot_cid;
+    uint64_t mask;
+    uint64_t const* bit_off;
+    uint64_t const* words;
+};
+
+// Candidate encodings: cw words, cb[c] .. cb[c + 1] bit range of candidate c.
+__global__ void k_dict_lookup(uint64_t nc, cand_view cv, uint64_t const* __restrict__ cw,
+                              uint64_t const* __restrict__ cb, dict_view D, uint32_t* __restrict__ cid) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const uint64_t h = cv.hash[c];
+    uint32_t res = NONE32;
+    if (D.slot_hash) {
+        uint64_t s = h & D.mask;
+        for (uint64_t i = 0; i <= D.mask; ++i) {
+            const uint64_t sh = D.slot_hash[s];
+            if (sh == HASH_EMPTY) break;
+            if (sh == h) {
+                const uint32_t k = D.slot_cid[s];
+                if (bits_equal(cw, cb[c], cb[c + 1] - cb[c], D.words, D.bit_off[k], D.bit_off[k + 1] - D.bit_off[k])) {
+                    res = k;
+                    break;
+                }
+            }
+            s = (s + 1) & D.mask;
+        }
+    }
+    cid[c] = res;
+}
+
+__global__ void k_new_flags(uint64_t nc, uint32_t const* __restrict__ cid, uint32_t* __restrict__ flag) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) flag[c] = cid[c] == NONE32 ? 1u : 0u;
+}
+
+__global__ void k_new_gather(uint64_t nc, uint32_t const* __restrict__ flag, uint64_t const* __restrict__ pos,
+                             cand_view cv, uint64_t* __restrict__ nkey, uint32_t* __restrict__ nidx) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc || !flag[c]) return;
+    nkey[pos[c]] = cv.hash[c];
+    nidx[pos[c]] = (uint32_t)c;
+}
+
+__global__ void k_run_heads(uint64_t n, uint64_t const* __restrict__ key, uint32_t* __restrict__ head) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) head[i] = (i == 0 || key[i] != key[i - 1]) ? 1u : 0u;
+}
+
+// run_start[run id] = position of the run's head
+__global__ void k_run_starts(uint64_t n, uint32_t const* __restrict__ head, uint64_t const* __restrict__ hpos,
+                             uint64_t* __restrict__ run_start) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && head[i]) run_start[hpos[i]] = i;
+}
+
+// Every member of an equal-hash run against the run's head (normally the
+// whole run is one color set).  rep[c] = the head when equal; a member that
+// differs marks its run for the exact fallback below.
+__global__ void k_member_match(uint64_t n, uint32_t const* __restrict__ head, uint64_t const* __restrict__ hpos,
+                               uint64_t const* __restrict__ run_start, uint32_t const* __restrict__ nidx,
+                               cand_view cv, uint64_t const* __restrict__ cw, uint64_t const* __restrict__ cb,
+                               uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first,
+                               uint32_t* __restrict__ collided) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t run = hpos[i] + head[i] - 1;  // inclusive count - 1
+    const uint32_t c = nidx[i];
+    const uint32_t h = nidx[run_start[run]];
+    if (c == h) {
+        rep[c] = c;
+        atomicMin(&rep_first[c], cv.first[c]);
+        return;
+    }
+    if (bits_equal(cw, cb[c], cb[c + 1] - cb[c], cw, cb[h], cb[h + 1] - cb[h])) {
+        rep[c] = h;
+        atomicMin(&rep_first[h], cv.first[c]);
+    } else {
+        rep[c] = c;
+        collided[run] = 1;
+    }
+}
+
+// Exact grouping of a run with a 64-bit hash collision (thread per run).
+__global__ void k_group_collided(uint64_t nruns, uint32_t const* __restrict__ collided,
+                                 uint64_t const* __restrict__ run_start, uint64_t n,
+                                 uint32_t const* __restrict__ nidx, cand_view cv,
+                                 uint64_t const* __restrict__ cw, uint64_t const* __restrict__ cb,
+                                 uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns || !collided[r]) return;
+    const uint64_t i = run_start[r];
+    const uint64_t e = (r + 1 < nruns) ? run_start[r + 1] : n;
+    for (uint64_t j = i; j < e; ++j) {
+        const uint32_t cj = nidx[j];
+        uint32_t rr = cj;
+        for (uint64_t q = i; q < j; ++q) {
+            const uint32_t cq = nidx[q];
+            if (rep[cq] != cq) continue;
+            if (bits_equal(cw, cb[cj], cb[cj + 1] - cb[cj], cw, cb[cq], cb[cq + 1] - cb[cq])) {
+                rr = cq;
+                break;
+            }
+        }
+        rep[cj] = rr;
+        rep_first[cj] = NONE32;
+        const uint32_t f = cv.first[cj];
+        if (rr == cj)
+            rep_first[cj] = f;
+        else if (f < rep_first[rr])
+            rep_first[rr] = f;
+    }
+}
+
+__global__ void k_rep_keys(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
+                           uint32_t* __restrict__ is_rep) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = nidx[i];
+    is_rep[i] = rep[c] == c ? 1u : 0u;
+}
+
+__global__ void k_rep_gather(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ is_rep,
+                             uint64_t const* __restrict__ pos, uint32_t const* __restrict__ rep_first,
+                             uint64_t* __restrict__ rkey, uint32_t* __restrict__ rcand) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !is_rep[i]) return;
+    const uint32_t c = nidx[i];
+    rkey[pos[i]] = rep_first[c];
+    rcand[pos[i]] = c;
+}
+
+// New class j (in first-appearance order) = candidate rcand[j]; cid base+j.
+__global__ void k_assign_new(uint64_t nnew, uint32_t const* __restrict__ rcand, uint64_t base,
+                             uint32_t* __restrict__ cid) {
+    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < nnew) cid[rcand[j]] = (uint32_t)(base + j);
+}
+
+__global__ void k_assign_members(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
+                                 uint32_t* __restrict__ cid) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = nidx[i];
+    if (rep[c] != c) cid[c] = cid[rep[c]];
+}
+
+// Per new class: encoded length, hash and color count.
+__global__ void k_new_sizes(uint64_t nnew, uint32_t const* __restrict__ rcand, cand_view cv, list_src L,
+                            uint64_t const* __restrict__ cb, uint64_t* __restrict__ nbits,
+                            uint64_t* __restrict__ hashes, unsigned long long* __restrict__ ints) {
+    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nnew) return;
+    const uint32_t c = rcand[j];
+    uint32_t const* p;
+    uint64_t n;
+    cand_list(L, cv.kind_id[c], p, n);
+    nbits[j] = cb[c + 1] - cb[c];
+    hashes[j] = cv.hash[c];
+    atomicAdd(ints, (unsigned long long)n);
+}
+
+// Append new classes' encodings to the dictionary's bit vector (warp per class;
+// words beyond the old end are zero, neighbours share boundary words).
+__global__ void k_append_bits(uint64_t nnew, uint32_t const* __restrict__ rcand, uint64_t const* __restrict__ cw,
+                              uint64_t const* __restrict__ cb, uint64_t const* __restrict__ dst_off,
+                              uint64_t* __restrict__ dw) {
+    const uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (j >= nnew) return;
+    const uint32_t c = rcand[j];
+    const uint64_t a = cb[c], len = cb[c + 1] - a, d = dst_off[j];
+    for (uint64_t i = (threadIdx.x & 31) * 64ull; i < len; i += 32 * 64ull) {
+        const uint64_t n = len - i < 64 ? len - i : 64;
+        or_bits(dw, d + i, bits_at(cw, a + i), (uint32_t)n);
     }
 }
 
@@ -1239,24 +1246,45 @@ void check_device_error_word(uint32_t* d_err, cudaStream_t st, char const* stage
 }
 
 // ---------------------------------------------------------------------------
+__global__ void k_dict_insert(uint64_t c0, uint64_t c1, uint64_t const* __restrict__ cls_hash,
+                              uint64_t* __restrict__ slot_hash, uint32_t* __restrict__ slot_cid, uint64_t mask,
+                              uint32_t* err) {
+    uint64_t c = c0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c1) return;
+    const uint64_t h = cls_hash[c];
+    uint64_t s = h & mask;
+    for (uint64_t i = 0; i <= mask; ++i) {
+        const uint64_t old = atomicCAS((unsigned long long*)&slot_hash[s], (unsigned long long)HASH_EMPTY,
+                                       (unsigned long long)h);
+        if (old == HASH_EMPTY) {
+            slot_cid[s] = (uint32_t)c;
+            return;
+        }
+        s = (s + 1) & mask;
+    }
+    set_error(err, ERR_TABLE_FULL);
+}
+
+// Global color-class dictionary (persists across bucket batches): per class
+// its 64-bit set hash and its bit range in the encoded .color_sets vector; an
+// open-addressing table hash -> class id.  Equality is tested on encodings.
 struct class_dict {
-    dvec<uint64_t> cls_hash;
-    dvec<uint64_t> cls_off;   // n + 1
-    dvec<uint32_t> pool;
-    dvec<uint64_t> bit_off;   // n
-    dvec<uint64_t> words;
+    dvec<uint64_t> cls_hash;  // n
+    dvec<uint64_t> bit_off;   // n + 1 (last = nbits)
+    dvec<uint64_t> words;     // encoded classes, zero beyond nbits
     dvec<uint64_t> slot_hash;
     dvec<uint32_t> slot_cid;
-    uint64_t n = 0, pool_n = 0, nbits = 0, total_integers = 0, mask = 0;
+    uint64_t n = 0, nbits = 0, total_integers = 0, mask = 0;
 
     void init(cudaStream_t st) {
-        cls_off.reserve(1024, st);
-        CDBG_CUDA(cudaMemsetAsync(cls_off.p, 0, 8, st));
-        cls_off.n = 1;
+        bit_off.reserve(1024, st);
+        CDBG_CUDA(cudaMemsetAsync(bit_off.p, 0, 8, st));
+        bit_off.n = 1;
         words.reserve(1024, st, true);
     }
-    // Make room for `n` classes (load <= 1/2); classes [first_new, n) still
-    // need inserting.  A resized table is rebuilt from every class hash.
+    dict_view view() const { return dict_view{slot_hash.p, slot_cid.p, mask, bit_off.p, words.p}; }
+    // Make room for n classes (load <= 1/2); classes [first_new, n) still need
+    // inserting.  A resized table is rebuilt from every class hash.
     void ensure_table(uint64_t first_new, cudaStream_t st, uint32_t* d_err) {
         uint64_t cap = 1024;
         while (cap < 2 * n) cap <<= 1;
@@ -1313,16 +1341,25 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     TB.tab_off = d_toff;
     TB.tab_cap = d_tcap;
     TB.b0 = b0;
-    k_init_tables<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax);
+    {
+        CDBG_PROF("k_init_tables", st);
+        k_init_tables<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax);
+    }
     CDBG_CHECK_LAUNCH();
     // ---- load
-    k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, d_err);
+    {
+        CDBG_PROF("k_insert", st);
+        k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, d_err);
+    }
     CDBG_CHECK_LAUNCH();
     // ---- nodes in first-insertion order
     const uint64_t nwb = ceil_div(nocc, 32);
     uint32_t* bits = A.alloc<uint32_t>(nwb);
     CDBG_CUDA(cudaMemsetAsync(bits, 0, 4 * nwb, st));
-    k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.rank, R.occ, O0, bits);
+    {
+        CDBG_PROF("k_firstbits", st);
+        k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.rank, R.occ, O0, bits);
+    }
     CDBG_CHECK_LAUNCH();
     uint32_t* wcnt = A.alloc<uint32_t>(nwb);
     uint64_t* wpre = A.alloc<uint64_t>(nwb + 1);
@@ -1336,13 +1373,19 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint8_t* n_meta = A.alloc<uint8_t>(D);
     uint32_t* n_rec = A.alloc<uint32_t>(D);
     uint32_t* n_bucket = A.alloc<uint32_t>(D);
-    k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax, R.occ, O0, bits,
-                                                   wpre, R.bucket, TB.node, n_key, n_meta, n_rec, n_bucket);
+    {
+        CDBG_PROF("k_make_nodes", st);
+        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax, R.occ, O0, bits,
+                                                       wpre, R.bucket, TB.node, n_key, n_meta, n_rec, n_bucket);
+    }
     CDBG_CHECK_LAUNCH();
     // ---- multi-record k-mers
     unsigned long long* cnt = A.alloc<unsigned long long>(1);
     CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
-    k_multi_pairs<K, false><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, nullptr);
+    {
+        CDBG_PROF("k_multi_pairs", st);
+        k_multi_pairs<K, false><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, nullptr);
+    }
     CDBG_CHECK_LAUNCH();
     const uint64_t npairs = read_dev(cnt, st);
     uint64_t M = 0;
@@ -1356,7 +1399,10 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     if (npairs) {
         uint64_t* pairs = A.alloc<uint64_t>(npairs);
         CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
-        k_multi_pairs<K, true><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, pairs);
+        {
+            CDBG_PROF("k_multi_pairs", st);
+            k_multi_pairs<K, true><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, pairs);
+        }
         CDBG_CHECK_LAUNCH();
         uint32_t* dummy = A.alloc<uint32_t>(npairs);
         prim::radix_sort_pairs<uint32_t>(pairs, dummy, npairs, 0, 64, A, st);
@@ -1390,22 +1436,31 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             CDBG_CUDA(cudaFuncSetAttribute(k_union<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
             CDBG_CUDA(cudaFuncSetAttribute(k_union<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         }
-        k_union<false><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
-                                                             nullptr, nullptr);
+        {
+            CDBG_PROF("k_union", st);
+            k_union<false><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
+                                                                 nullptr, nullptr);
+        }
         CDBG_CHECK_LAUNCH();
         poff = A.alloc<uint64_t>(M + 1);
         prim::exclusive_scan<uint32_t, uint64_t>(msize, poff, M, A, st, poff + M);
         const uint64_t ptot = read_dev(poff + M, st);
         pool = A.alloc<uint32_t>(ptot + 1);
-        k_union<true><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
-                                                            poff, pool);
+        {
+            CDBG_PROF("k_union", st);
+            k_union<true><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
+                                                                poff, pool);
+        }
         CDBG_CHECK_LAUNCH();
     }
     out.n_multi += M;
     // ---- candidates: used records, then multi nodes
     uint32_t* rec_first = A.alloc<uint32_t>(nrec);
     CDBG_CUDA(cudaMemsetAsync(rec_first, 0xff, 4 * nrec, st));
-    k_rec_first<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_first);
+    {
+        CDBG_PROF("k_rec_first", st);
+        k_rec_first<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_first);
+    }
     CDBG_CHECK_LAUNCH();
     uint32_t* rkeep = A.alloc<uint32_t>(nrec);
     uint64_t* rpos = A.alloc<uint64_t>(nrec + 1);
@@ -1415,9 +1470,9 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     const uint64_t nrc = read_dev(rpos + nrec, st);
     const uint64_t nc = nrc + M;
     cand_view cv;
-    cv.kind_id = A.alloc<uint32_t>(nc);
-    cv.first = A.alloc<uint32_t>(nc);
-    cv.hash = A.alloc<uint64_t>(nc);
+    cv.kind_id = A.alloc<uint32_t>(nc + 1);
+    cv.first = A.alloc<uint32_t>(nc + 1);
+    cv.hash = A.alloc<uint64_t>(nc + 1);
     uint32_t* rec_cand = A.alloc<uint32_t>(nrec);
     k_cand_records<<<grid(nrec, 256), 256, 0, st>>>(nrec, (uint32_t)R0, rec_first, rkeep, rpos, d_rhash, cv, rec_cand);
     CDBG_CHECK_LAUNCH();
@@ -1426,66 +1481,9 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         CDBG_CHECK_LAUNCH();
     }
     list_src L{R.col_off, R.colors, poff, pool, msize};
-    dict_view DV{dict.slot_hash.p, dict.slot_cid.p, dict.mask, dict.cls_off.p, dict.pool.p};
-    uint32_t* cid = A.alloc<uint32_t>(nc);
-    k_dict_lookup<<<grid(nc, 256), 256, 0, st>>>(nc, cv, L, DV, cid);
-    CDBG_CHECK_LAUNCH();
-    // ---- new classes
-    uint32_t* nflag = A.alloc<uint32_t>(nc);
-    uint64_t* npos = A.alloc<uint64_t>(nc + 1);
-    k_new_flags<<<grid(nc, 256), 256, 0, st>>>(nc, cid, nflag);
-    CDBG_CHECK_LAUNCH();
-    prim::exclusive_scan<uint32_t, uint64_t>(nflag, npos, nc, A, st, npos + nc);
-    const uint64_t nn = read_dev(npos + nc, st);
-    if (nn) {
-        uint64_t* nkey = A.alloc<uint64_t>(nn);
-        uint32_t* nidx = A.alloc<uint32_t>(nn);
-        k_new_gather<<<grid(nc, 256), 256, 0, st>>>(nc, nflag, npos, cv, nkey, nidx);
-        CDBG_CHECK_LAUNCH();
-        prim::radix_sort_pairs<uint32_t>(nkey, nidx, nn, 0, 64, A, st);
-        uint32_t* head = A.alloc<uint32_t>(nn);
-        k_run_heads<<<grid(nn, 256), 256, 0, st>>>(nn, nkey, head);
-        CDBG_CHECK_LAUNCH();
-        uint32_t* rep = A.alloc<uint32_t>(nc);
-        uint32_t* rep_first = A.alloc<uint32_t>(nc);
-        k_group_runs<<<grid(nn, 128), 128, 0, st>>>(nn, nkey, head, nidx, cv, L, rep, rep_first);
-        CDBG_CHECK_LAUNCH();
-        uint32_t* is_rep = A.alloc<uint32_t>(nn);
-        uint64_t* rpos2 = A.alloc<uint64_t>(nn + 1);
-        k_rep_keys<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, rep_first, is_rep);
-        CDBG_CHECK_LAUNCH();
-        prim::exclusive_scan<uint32_t, uint64_t>(is_rep, rpos2, nn, A, st, rpos2 + nn);
-        const uint64_t nnew = read_dev(rpos2 + nn, st);
-        uint64_t* rkey = A.alloc<uint64_t>(nnew);
-        uint32_t* rcand = A.alloc<uint32_t>(nnew);
-        k_rep_gather<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, is_rep, rpos2, rep_first, rkey, rcand);
-        CDBG_CHECK_LAUNCH();
-        prim::radix_sort_pairs<uint32_t>(rkey, rcand, nnew, 0, 32, A, st);
-        const uint64_t base = dict.n;
-        k_assign_new<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, base, cid);
-        CDBG_CHECK_LAUNCH();
-        k_assign_members<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, cid);
-        CDBG_CHECK_LAUNCH();
-        // append lists, hashes, offsets to the dictionary
-        uint64_t* nsz = A.alloc<uint64_t>(nnew);
-        uint64_t* nh = A.alloc<uint64_t>(nnew);
-        k_new_sizes<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, cv, L, nsz, nh);
-        CDBG_CHECK_LAUNCH();
-        uint64_t* loff = A.alloc<uint64_t>(nnew + 1);
-        prim::exclusive_scan<uint64_t, uint64_t>(nsz, loff, nnew, A, st, loff + nnew);
-        const uint64_t ladd = read_dev(loff + nnew, st);
-        dict.cls_hash.reserve(base + nnew, st);
-        dict.cls_off.reserve(base + nnew + 1, st);
-        dict.pool.reserve(dict.pool_n + ladd + 1, st);
-        dict.bit_off.reserve(base + nnew, st);
-        CDBG_CUDA(cudaMemcpyAsync(dict.cls_hash.p + base, nh, 8 * nnew, cudaMemcpyDeviceToDevice, st));
-        // cls_off[base + 1 + j] = pool_n + loff[j + 1]; absolute list offsets for the encoder
-        add_offsets(loff + 1, nnew, dict.pool_n, dict.cls_off.p + base + 1, st);
-        uint64_t* loff_abs = A.alloc<uint64_t>(nnew + 1);
-        add_offsets(loff, nnew + 1, dict.pool_n, loff_abs, st);
-        k_new_copy<<<grid(nnew, 8), 256, 0, st>>>(nnew, rcand, cv, L, loff, dict.pool.p + dict.pool_n);
-        CDBG_CHECK_LAUNCH();
-        // encode
+    uint32_t* cid = A.alloc<uint32_t>(nc + 1);
+    if (nc) {
+        // candidate encodings (also the equality key)
         const uint32_t nw = (C + 31) / 32;
         int wpb = (int)std::max<uint64_t>(1, std::min<uint64_t>(8, (96 * 1024) / (4ull * nw)));
         const size_t shm = (size_t)wpb * nw * 4;
@@ -1493,40 +1491,137 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             CDBG_CUDA(cudaFuncSetAttribute(k_encode<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
             CDBG_CUDA(cudaFuncSetAttribute(k_encode<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         }
-        uint64_t* nbits = A.alloc<uint64_t>(nnew);
-        uint64_t* boff = A.alloc<uint64_t>(nnew + 1);
-        k_encode<false><<<grid(nnew, wpb), wpb * 32, shm, st>>>(nnew, loff_abs, dict.pool.p, C, nbits, nullptr,
-                                                                  nullptr);
+        uint64_t* cbits = A.alloc<uint64_t>(nc);
+        uint64_t* cb = A.alloc<uint64_t>(nc + 1);
+        {
+            CDBG_PROF("k_encode", st);
+            k_encode<false><<<grid(nc, wpb), wpb * 32, shm, st>>>(nc, cv, L, C, cbits, nullptr, nullptr);
+        }
         CDBG_CHECK_LAUNCH();
-        prim::exclusive_scan<uint64_t, uint64_t>(nbits, boff, nnew, A, st, boff + nnew);
-        const uint64_t badd = read_dev(boff + nnew, st);
-        add_offsets(boff, nnew + 1, dict.nbits, boff, st);  // absolute bit offsets
-        CDBG_CUDA(cudaMemcpyAsync(dict.bit_off.p + base, boff, 8 * nnew, cudaMemcpyDeviceToDevice, st));
-        const uint64_t need_words = (dict.nbits + badd + 63) / 64 + 2;
-        dict.words.reserve(need_words, st, true);
-        k_encode<true><<<grid(nnew, wpb), wpb * 32, shm, st>>>(nnew, loff_abs, dict.pool.p, C, nullptr, boff,
-                                                                 dict.words.p);
+        prim::exclusive_scan<uint64_t, uint64_t>(cbits, cb, nc, A, st, cb + nc);
+        const uint64_t ctot = read_dev(cb + nc, st);
+        const uint64_t cwn = ctot / 64 + 4;
+        uint64_t* cw = A.alloc<uint64_t>(cwn);
+        CDBG_CUDA(cudaMemsetAsync(cw, 0, 8 * cwn, st));
+        {
+            CDBG_PROF("k_encode", st);
+            k_encode<true><<<grid(nc, wpb), wpb * 32, shm, st>>>(nc, cv, L, C, nullptr, cb, cw);
+        }
         CDBG_CHECK_LAUNCH();
-        dict.n = base + nnew;
-        dict.cls_hash.n = dict.cls_off.n = dict.bit_off.n = dict.n;
-        dict.cls_off.n = dict.n + 1;
-        dict.pool_n += ladd;
-        dict.pool.n = dict.pool_n;
-        dict.nbits += badd;
-        dict.words.n = (dict.nbits + 63) / 64;
-        dict.total_integers += ladd;
-        dict.ensure_table(base, st, d_err);
+        {
+            CDBG_PROF("k_dict_lookup", st);
+            k_dict_lookup<<<grid(nc, 256), 256, 0, st>>>(nc, cv, cw, cb, dict.view(), cid);
+        }
+        CDBG_CHECK_LAUNCH();
+        // ---- new classes
+        uint32_t* nflag = A.alloc<uint32_t>(nc);
+        uint64_t* npos = A.alloc<uint64_t>(nc + 1);
+        k_new_flags<<<grid(nc, 256), 256, 0, st>>>(nc, cid, nflag);
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(nflag, npos, nc, A, st, npos + nc);
+        const uint64_t nn = read_dev(npos + nc, st);
+        if (nn) {
+            uint64_t* nkey = A.alloc<uint64_t>(nn);
+            uint32_t* nidx = A.alloc<uint32_t>(nn);
+            k_new_gather<<<grid(nc, 256), 256, 0, st>>>(nc, nflag, npos, cv, nkey, nidx);
+            CDBG_CHECK_LAUNCH();
+            prim::radix_sort_pairs<uint32_t>(nkey, nidx, nn, 0, 64, A, st);
+            uint32_t* head = A.alloc<uint32_t>(nn);
+            uint64_t* hpos = A.alloc<uint64_t>(nn + 1);
+            k_run_heads<<<grid(nn, 256), 256, 0, st>>>(nn, nkey, head);
+            CDBG_CHECK_LAUNCH();
+            prim::exclusive_scan<uint32_t, uint64_t>(head, hpos, nn, A, st, hpos + nn);
+            const uint64_t nruns = read_dev(hpos + nn, st);
+            uint64_t* run_start = A.alloc<uint64_t>(nruns + 1);
+            k_run_starts<<<grid(nn, 256), 256, 0, st>>>(nn, head, hpos, run_start);
+            CDBG_CHECK_LAUNCH();
+            uint32_t* rep = A.alloc<uint32_t>(nc);
+            uint32_t* rep_first = A.alloc<uint32_t>(nc);
+            uint32_t* collided = A.alloc<uint32_t>(nruns + 1);
+            CDBG_CUDA(cudaMemsetAsync(rep_first, 0xff, 4 * nc, st));
+            CDBG_CUDA(cudaMemsetAsync(collided, 0, 4 * (nruns + 1), st));
+            {
+                CDBG_PROF("k_member_match", st);
+                k_member_match<<<grid(nn, 256), 256, 0, st>>>(nn, head, hpos, run_start, nidx, cv, cw, cb, rep,
+                                                               rep_first, collided);
+            }
+            CDBG_CHECK_LAUNCH();
+            {
+                unsigned long long* ncol = A.alloc<unsigned long long>(1);
+                CDBG_CUDA(cudaMemsetAsync(ncol, 0, 8, st));
+                k_count_flags<<<grid(nruns, 256), 256, 0, st>>>(nruns, collided, ncol);
+                CDBG_CHECK_LAUNCH();
+                if (read_dev(ncol, st)) {
+                    k_group_collided<<<grid(nruns, 128), 128, 0, st>>>(nruns, collided, run_start, nn, nidx, cv, cw,
+                                                                       cb, rep, rep_first);
+                    CDBG_CHECK_LAUNCH();
+                }
+            }
+            uint32_t* is_rep = A.alloc<uint32_t>(nn);
+            uint64_t* rpos2 = A.alloc<uint64_t>(nn + 1);
+            k_rep_keys<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, is_rep);
+            CDBG_CHECK_LAUNCH();
+            prim::exclusive_scan<uint32_t, uint64_t>(is_rep, rpos2, nn, A, st, rpos2 + nn);
+            const uint64_t nnew = read_dev(rpos2 + nn, st);
+            uint64_t* rkey = A.alloc<uint64_t>(nnew);
+            uint32_t* rcand = A.alloc<uint32_t>(nnew);
+            k_rep_gather<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, is_rep, rpos2, rep_first, rkey, rcand);
+            CDBG_CHECK_LAUNCH();
+            prim::radix_sort_pairs<uint32_t>(rkey, rcand, nnew, 0, 32, A, st);
+            const uint64_t base = dict.n;
+            k_assign_new<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, base, cid);
+            CDBG_CHECK_LAUNCH();
+            k_assign_members<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, cid);
+            CDBG_CHECK_LAUNCH();
+            // append to the dictionary: hashes, bit offsets, encodings
+            uint64_t* nbits = A.alloc<uint64_t>(nnew);
+            uint64_t* nh = A.alloc<uint64_t>(nnew);
+            uint64_t* boff = A.alloc<uint64_t>(nnew + 1);
+            unsigned long long* ints = A.alloc<unsigned long long>(1);
+            CDBG_CUDA(cudaMemsetAsync(ints, 0, 8, st));
+            k_new_sizes<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, cv, L, cb, nbits, nh, ints);
+            CDBG_CHECK_LAUNCH();
+            prim::exclusive_scan<uint64_t, uint64_t>(nbits, boff, nnew, A, st, boff + nnew);
+            const uint64_t badd = read_dev(boff + nnew, st);
+            add_offsets(boff, nnew + 1, dict.nbits, boff, st);  // absolute bit offsets
+            dict.cls_hash.reserve(base + nnew, st);
+            dict.bit_off.reserve(base + nnew + 1, st);
+            CDBG_CUDA(cudaMemcpyAsync(dict.cls_hash.p + base, nh, 8 * nnew, cudaMemcpyDeviceToDevice, st));
+            CDBG_CUDA(cudaMemcpyAsync(dict.bit_off.p + base, boff, 8 * (nnew + 1), cudaMemcpyDeviceToDevice, st));
+            dict.words.reserve((dict.nbits + badd + 63) / 64 + 4, st, true);
+            {
+                CDBG_PROF("k_append_bits", st);
+                k_append_bits<<<grid(nnew, 8), 256, 0, st>>>(nnew, rcand, cw, cb, boff, dict.words.p);
+            }
+            CDBG_CHECK_LAUNCH();
+            dict.total_integers += read_dev(ints, st);
+            dict.n = base + nnew;
+            dict.cls_hash.n = dict.n;
+            dict.bit_off.n = dict.n + 1;
+            dict.nbits += badd;
+            dict.words.n = (dict.nbits + 63) / 64;
+            dict.ensure_table(base, st, d_err);
+        }
     }
     // ---- node class ids
     uint32_t* n_cid = A.alloc<uint32_t>(D);
-    k_node_cid<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_cand, nrc, cid, n_cid);
+    {
+        CDBG_PROF("k_node_cid", st);
+        k_node_cid<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_cand, nrc, cid, n_cid);
+    }
     CDBG_CHECK_LAUNCH();
     // ---- extension masks, links, chains
     uint8_t* n_mask = A.alloc<uint8_t>(D);
-    k_ext_mask<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, k, n_mask);
+    {
+        CDBG_PROF("k_ext_mask", st);
+        k_ext_mask<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, k, n_mask);
+    }
     CDBG_CHECK_LAUNCH();
     uint32_t* link = A.alloc<uint32_t>(2 * D);
-    k_links<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, n_mask, k, link);
+    {
+        CDBG_PROF("k_links", st);
+        k_links<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, n_mask, k, link);
+    }
     CDBG_CHECK_LAUNCH();
     chain_ws W;
     W.link = link;
@@ -1546,9 +1641,15 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(W.seed_len, 0, 4 * D, st));
     CDBG_CUDA(cudaMemsetAsync(W.covered, 0, D, st));
     CDBG_CUDA(cudaMemsetAsync(W.cursor, 0, 8, st));
-    k_chain_paths<<<grid(D, 128), 128, 0, st>>>(W, d_err);
+    {
+        CDBG_PROF("k_chain_paths", st);
+        k_chain_paths<<<grid(D, 128), 128, 0, st>>>(W, d_err);
+    }
     CDBG_CHECK_LAUNCH();
-    k_chain_cycles<<<grid(D, 128), 128, 0, st>>>(W, d_err);
+    {
+        CDBG_PROF("k_chain_cycles", st);
+        k_chain_cycles<<<grid(D, 128), 128, 0, st>>>(W, d_err);
+    }
     CDBG_CHECK_LAUNCH();
     // ---- fragments
     uint64_t* fsz = A.alloc<uint64_t>(D);
@@ -1556,14 +1657,20 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint64_t* foff = A.alloc<uint64_t>(D + 1);
     unsigned long long* seqt = A.alloc<unsigned long long>(1);
     CDBG_CUDA(cudaMemsetAsync(seqt, 0, 8, st));
-    k_frag_sizes<<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.fe, n_cid, k, fsz, is_seed, seqt);
+    {
+        CDBG_PROF("k_frag_sizes", st);
+        k_frag_sizes<<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.fe, n_cid, k, fsz, is_seed, seqt);
+    }
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint64_t, uint64_t>(fsz, foff, D, A, st, foff + D);
     const uint64_t fbytes = read_dev(foff + D, st);
     check_device_error_word(d_err, st, "unitig walk");
     uint8_t* fb = A.alloc<uint8_t>(fbytes + 8);
-    k_frag_write<K><<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.seed_open, W.fe, n_cid, n_key, k,
-                                                   foff, fb);
+    {
+        CDBG_PROF("k_frag_write", st);
+        k_frag_write<K><<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.seed_open, W.fe, n_cid, n_key, k,
+                                                       foff, fb);
+    }
     CDBG_CHECK_LAUNCH();
     uint64_t nfr = 0;
     {
@@ -1612,8 +1719,11 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     uint64_t* rhash = A.alloc<uint64_t>(n + 1);
     uint64_t* occ = A.alloc<uint64_t>(n + 1);
     if (n) {
-        k_rec_prep<<<grid(n, 256), 256, 0, st>>>(n, rs.len, p.k, rs.bucket_start, B, nk, rbucket, rs.col_off,
-                                                 rs.colors, rhash);
+        {
+            CDBG_PROF("k_rec_prep", st);
+            k_rec_prep<<<grid(n, 256), 256, 0, st>>>(n, rs.len, p.k, rs.bucket_start, B, nk, rbucket, rs.col_off,
+                                                     rs.colors, rhash);
+        }
         CDBG_CHECK_LAUNCH();
     }
     prim::exclusive_scan<uint64_t, uint64_t>(nk, occ, n, A, st, occ + n);
@@ -1628,13 +1738,17 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     if (budget == 0) {
         size_t fr = 0, tot = 0;
         CDBG_CUDA(cudaMemGetInfo(&fr, &tot));
-        // ~160 B of device memory per k-mer occurrence in the batch, worst case
-        budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(fr / 2) / 160));
+        const uint64_t avail = (uint64_t)fr + A.cached_free();
+        // ~160 B of device memory per k-mer occurrence in the batch, worst
+        // case; keep 45% of the available memory for outputs and the dictionary
+        budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(avail * 0.55) / 160));
     }
     rec_view R{rs.start, rs.len, rs.flags, rs.col_off, rs.colors, rbucket, occ, rs.words};
     class_dict dict;
     dict.init(st);
-    dvec<uint8_t> dfrag;
+    dvec<uint8_t> local_frag;
+    dvec<uint8_t>& dfrag = out.d_frag_out ? *out.d_frag_out : local_frag;
+    dfrag.n = 0;
     uint32_t b = 0;
     while (b < B) {
         const uint32_t s = b;
@@ -1660,34 +1774,40 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
         if (dict.n)
             CDBG_CUDA(cudaMemcpyAsync(out.offsets.data(), dict.bit_off.p, 8 * dict.n, cudaMemcpyDeviceToHost, st));
     }
-    if (p.keep_lists) {
-        out.list_off.resize(dict.n + 1);
-        out.lists.resize(dict.pool_n);
-        CDBG_CUDA(cudaMemcpyAsync(out.list_off.data(), dict.cls_off.p, 8 * (dict.n + 1), cudaMemcpyDeviceToHost, st));
-        if (dict.pool_n)
-            CDBG_CUDA(cudaMemcpyAsync(out.lists.data(), dict.pool.p, 4 * dict.pool_n, cudaMemcpyDeviceToHost, st));
-    }
     CDBG_CUDA(cudaStreamSynchronize(st));
     A.release(mark);
     if (!p.to_host) {
-        // device-resident outputs in the arena (valid until the arena is reset)
-        out.d_frag = A.alloc<uint8_t>(dfrag.n + 8);
-        out.d_words = A.alloc<uint64_t>(nwords + 1);
-        out.d_offsets = A.alloc<uint64_t>(dict.n + 1);
-        if (dfrag.n) CDBG_CUDA(cudaMemcpyAsync(out.d_frag, dfrag.p, dfrag.n, cudaMemcpyDeviceToDevice, st));
-        if (nwords) CDBG_CUDA(cudaMemcpyAsync(out.d_words, dict.words.p, 8 * nwords, cudaMemcpyDeviceToDevice, st));
-        if (dict.n)
-            CDBG_CUDA(cudaMemcpyAsync(out.d_offsets, dict.bit_off.p, 8 * dict.n, cudaMemcpyDeviceToDevice, st));
-        CDBG_CUDA(cudaStreamSynchronize(st));
+        // hand the dictionary's storage to the caller (no copies)
+        std::swap(out.d_words_out->p, dict.words.p);
+        std::swap(out.d_words_out->cap, dict.words.cap);
+        out.d_words_out->n = nwords;
+        std::swap(out.d_offsets_out->p, dict.bit_off.p);
+        std::swap(out.d_offsets_out->cap, dict.bit_off.cap);
+        out.d_offsets_out->n = dict.n;
+        out.d_frag = out.d_frag_out->p;
+        out.d_words = out.d_words_out->p;
+        out.d_offsets = out.d_offsets_out->p;
     }
 }
 }  // namespace
 
 void run_phase2(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStream_t st, uint32_t* d_err,
                 phase2_result& out) {
-    out = phase2_result();
+    {
+        // keep the caller's device output buffers across the reset
+        auto f = out.d_frag_out;
+        auto w = out.d_words_out;
+        auto o = out.d_offsets_out;
+        out = phase2_result();
+        out.d_frag_out = f;
+        out.d_words_out = w;
+        out.d_offsets_out = o;
+    }
+    if (!p.to_host && !(out.d_frag_out && out.d_words_out && out.d_offsets_out))
+        throw std::runtime_error("device-resident phase-2 outputs need caller buffers");
     if (p.k < 2 || p.k > 63) throw std::runtime_error("k must be in [2, 63]");
     if (p.num_colors == 0) throw std::runtime_error("num_colors must be > 0");
+    if (rs.n >= (1ull << 31)) throw std::runtime_error("more than 2^31 bucket records in one build");
     if (p.k <= 31)
         run_all<uint64_t>(rs, p, A, st, d_err, out);
     else

@@ -26,9 +26,11 @@ struct phase2_result {
     uint64_t nbits = 0;
     uint64_t n_classes = 0;
     uint64_t total_integers = 0;
-    // class lists (only when keep_lists): concatenated ascending colors
-    std::vector<uint32_t> lists;
-    std::vector<uint64_t> list_off;
+    // device-resident outputs (when !to_host) are written into these
+    // caller-owned buffers, which outlive the arena
+    dvec<uint8_t>* d_frag_out = nullptr;
+    dvec<uint64_t>* d_words_out = nullptr;
+    dvec<uint64_t>* d_offsets_out = nullptr;
     // counters
     uint64_t n_occ = 0, n_distinct = 0, n_fragments = 0, total_seq_bytes = 0;
     uint64_t n_multi = 0;
@@ -40,7 +42,6 @@ struct phase2_params {
     uint32_t num_colors = 0;
     uint64_t batch_occ = 0;   // k-mer occurrences per batch (0 = auto)
     bool to_host = true;      // copy outputs to host vectors
-    bool keep_lists = false;  // also return the class color lists
 };
 
 // Run phase 2 over all buckets of `rs` (records grouped by bucket).

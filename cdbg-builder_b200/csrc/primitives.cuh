@@ -112,12 +112,18 @@ void exclusive_scan(T const* in, U* out, uint64_t n, dev_arena& A, cudaStream_t 
     U* offs = nullptr;
     if (tiles > 1) {
         U* sums = A.alloc<U>(tiles);
-        k_tile_sums<T, U><<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, sums);
+        {
+            CDBG_PROF("k_tile_sums", st);
+            k_tile_sums<T, U><<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, sums);
+        }
         CDBG_CHECK_LAUNCH();
         exclusive_scan<U, U>(sums, sums, tiles, A, st, (U*)nullptr);
         offs = sums;
     }
-    k_tile_scan<T, U><<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, offs, out, total_dev);
+    {
+        CDBG_PROF("k_tile_scan", st);
+        k_tile_scan<T, U><<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, offs, out, total_dev);
+    }
     CDBG_CHECK_LAUNCH();
     A.release(m);
 }
@@ -262,7 +268,10 @@ int radix_sort_pairs(uint64_t* keys, V* vals, uint64_t n, int begin_bit, int end
     {
         uint64_t blocks = ceil_div(n, (uint64_t)RS_THREADS * 16);
         if (blocks > 148 * 8) blocks = 148 * 8;
-        k_rs_histograms<<<(unsigned)blocks, RS_THREADS, 0, st>>>(keys, n, begin_bit, npasses, hist);
+        {
+            CDBG_PROF("k_rs_histograms", st);
+            k_rs_histograms<<<(unsigned)blocks, RS_THREADS, 0, st>>>(keys, n, begin_bit, npasses, hist);
+        }
         CDBG_CHECK_LAUNCH();
     }
     std::vector<unsigned long long> h((size_t)npasses * RS_BINS);
@@ -283,11 +292,17 @@ int radix_sort_pairs(uint64_t* keys, V* vals, uint64_t n, int begin_bit, int end
             if (h[(size_t)p * RS_BINS + d] == n) trivial = true;
         if (trivial) continue;
         const int shift = begin_bit + p * RS_BITS;
-        k_rs_upsweep<<<(unsigned)ntiles, RS_THREADS, 0, st>>>(kin, n, shift, (uint32_t)ntiles, counts);
+        {
+            CDBG_PROF("k_rs_upsweep", st);
+            k_rs_upsweep<<<(unsigned)ntiles, RS_THREADS, 0, st>>>(kin, n, shift, (uint32_t)ntiles, counts);
+        }
         CDBG_CHECK_LAUNCH();
         exclusive_scan<uint32_t, uint64_t>(counts, offs, ntiles * RS_BINS, A, st);
-        k_rs_downsweep<V><<<(unsigned)ntiles, RS_THREADS, 0, st>>>(kin, vin, kout, vout, n, shift,
-                                                                   (uint32_t)ntiles, offs);
+        {
+            CDBG_PROF("k_rs_downsweep", st);
+            k_rs_downsweep<V><<<(unsigned)ntiles, RS_THREADS, 0, st>>>(kin, vin, kout, vout, n, shift,
+                                                                       (uint32_t)ntiles, offs);
+        }
         CDBG_CHECK_LAUNCH();
         std::swap(kin, kout);
         std::swap(vin, vout);

@@ -42,6 +42,23 @@ void cdbg_engine_destroy(cdbg_engine* e);
 const char* cdbg_last_error(void);
 int cdbg_gpu_version(void);
 
+/* Run all work of the engine on a caller-owned CUDA stream (a cudaStream_t
+ * passed as void*; NULL restores the engine's own stream), so the caller can
+ * bracket calls with its own CUDA events.  No counterpart in the reference
+ * (CPU only); measurement plumbing. */
+int cdbg_engine_set_stream(cdbg_engine* e, void* stream);
+
+/* Kernel launches issued by this library in this process so far. */
+uint64_t cdbg_launch_count(void);
+
+/* Per-kernel device time (CUDA events around each launch on the launching
+ * stream): enable = 1 starts collecting (and clears), 0 stops.  Stats copy
+ * up to `cap` kernels: NUL-separated names into `names`, total ms and
+ * launches; the return value is the number of kernels (or < 0). */
+int cdbg_engine_profile(cdbg_engine* e, int32_t enable);
+int cdbg_engine_kernel_stats(cdbg_engine* e, char* names, uint64_t names_cap, double* ms,
+                             uint64_t* launches, uint32_t cap);
+
 /* Sequences of many inputs back to back: seq[seq_off[i] .. seq_off[i+1]) is
  * sequence i (ASCII; A/C/G/T in either case are bases, anything else splits
  * runs), of color seq_color[i].  With on_device = 1 all three pointers are
@@ -158,6 +175,10 @@ typedef struct cdbg_build_result {
 
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
                    cdbg_build_result* r);
+
+/* Copy `bytes` from a device pointer returned by cdbg_gpu_build
+ * (outputs_to_host = 0) into host memory, on the engine's stream. */
+int cdbg_engine_copy_out(cdbg_engine* e, const void* device_src, void* host_dst, uint64_t bytes);
 
 #ifdef __cplusplus
 }

@@ -93,3 +93,19 @@ def test_in_memory_build_matches_file_path(engine, tmp_path):
     assert list(native.result_class_offsets(r)) == offsets
     assert np.array_equal(native.result_class_words(r), words)
     assert decoded == classes
+
+
+def test_device_resident_outputs_match_host_outputs(engine, tmp_path):
+    """cdbg_gpu_build with outputs left in HBM returns the same bytes."""
+    lst = _fresh(tmp_path, 21, 5)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    hs = native.HostSequences(files)
+    r = engine.build(hs.batch, 31, 128, 5)
+    frag, words = native.result_frag_bytes(r), native.result_class_words(r).tobytes()
+    offs = native.result_class_offsets(r).tobytes()
+    for _ in range(2):  # twice: outputs are reused buffers
+        rd = engine.build(hs.batch, 31, 128, 5, outputs_to_host=False)
+        assert rd.frag_nbytes == len(frag) and rd.n_color_sets == r.n_color_sets
+        assert engine.copy_out(rd.frag_bytes, rd.frag_nbytes) == frag
+        assert engine.copy_out(rd.class_words, len(words)) == words
+        assert engine.copy_out(rd.class_offsets, len(offs)) == offs
