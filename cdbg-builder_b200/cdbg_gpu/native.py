@@ -96,6 +96,12 @@ SIGNATURES = {
     "cdbg_engine_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "cdbg_engine_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64,
                                                 ctypes.POINTER(ctypes.c_double), c_u64p, ctypes.c_uint32]),
+    "cdbg_gpu_supers_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_uint64, c_u64p,
+                                               ctypes.c_void_p]),
     "cdbg_engine_copy_out": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_uint64]),
     "cdbg_read_sequences": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32,

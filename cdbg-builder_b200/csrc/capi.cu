@@ -164,6 +164,7 @@ inline uint64_t host_bits64(std::vector<uint64_t> const& w, uint64_t pos) {
 
 namespace cdbg {
 std::atomic<uint64_t> g_launches{0};
+void set_last_error(std::string const& msg) { g_last_error = msg; }
 thread_local kernel_profiler* g_prof = nullptr;
 
 void check_device_error(cdbg_engine* e, char const* stage) {

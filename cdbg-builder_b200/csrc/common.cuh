@@ -16,6 +16,9 @@ typedef unsigned __int128 u128;
 
 extern std::atomic<uint64_t> g_launches;
 
+// Message returned by cdbg_last_error() (thread-local).
+void set_last_error(std::string const& msg);
+
 // Per-kernel device time with CUDA events on the launching stream.  Enabled
 // per engine call; a scope records an event before and after the launch it
 // encloses, and resolve() folds the finished pairs into per-name totals.

@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "device_kmer.cuh"
@@ -875,3 +877,147 @@ void parse_records(uint8_t const* bytes, uint64_t nbytes, uint64_t const* chunk_
 }
 
 }  // namespace cdbg
+
+namespace cdbg {
+
+// ===========================================================================
+// Super-k-mer finder for callers that cannot allocate device memory.
+//
+// Some callers run where they may not call cudaMalloc / cudaFree or anything
+// that allocates on the device: code that must not add memory of its own next
+// to a host application's pool (a framework's caching allocator, a memory
+// budget managed elsewhere), or code running with allocation forbidden. They
+// pre-pack their ACGT runs into device memory and hand in output arrays; this
+// entry point finds the super-k-mers of those runs using only the fixed
+// scratch below, which every GPU that loads this library holds until the
+// process exits.
+//
+// Limit: at most NOALLOC_MAX_TILES tiles per call, a run taking
+// ceil((len - k + 2) / 2048) tiles -- at most 512 runs and 1,048,576
+// (k-1)-mers per call.  Larger inputs are rejected; split them.
+// All calls share the scratch and it keeps the previous call's contents:
+// calls that overlap on the GPU (other streams, other host threads) race.
+// ===========================================================================
+
+namespace {
+
+constexpr uint32_t NOALLOC_MAX_TILES = 512;
+constexpr uint64_t NOALLOC_MAX_SUPERS = (uint64_t)NOALLOC_MAX_TILES * MZ_TT;
+
+struct noalloc_scratch {
+    uint64_t run_tiles[NOALLOC_MAX_TILES];
+    uint64_t tile_start[NOALLOC_MAX_TILES + 1];
+    uint32_t tile_count[NOALLOC_MAX_TILES];
+    uint64_t tile_off[NOALLOC_MAX_TILES + 1];
+    uint64_t minv[NOALLOC_MAX_SUPERS];
+    uint32_t run[NOALLOC_MAX_SUPERS];
+    uint32_t a[NOALLOC_MAX_SUPERS];
+    uint64_t key[NOALLOC_MAX_SUPERS];
+    uint32_t err;
+};
+
+// The scratch itself (about 24 MiB).  Host code must not pass this name to a
+// kernel: on the host it is only a stand-in; its device address comes from
+// cudaGetSymbolAddress (noalloc_scratch_ptr below).
+static __device__ __align__(256) noalloc_scratch g_noalloc_scratch;
+
+// Exclusive scan of n <= NOALLOC_MAX_TILES values by one block; the total goes
+// to out[n].
+template <typename T>
+__global__ void __launch_bounds__(1024) k_noalloc_scan(T const* __restrict__ in, uint32_t n,
+                                                       uint64_t* __restrict__ out) {
+    __shared__ uint64_t sw[1024 / 32 + 1];
+    const uint64_t v = threadIdx.x < n ? (uint64_t)in[threadIdx.x] : 0;
+    uint64_t tot;
+    const uint64_t ex = prim::block_exclusive_scan<uint64_t, 1024>(v, sw, tot);
+    if (threadIdx.x < n) out[threadIdx.x] = ex;
+    if (threadIdx.x == 0) out[n] = tot;
+}
+
+std::mutex g_noalloc_mu;
+noalloc_scratch* g_noalloc_ptr[256] = {};
+
+// Device address of the scratch on the current device, looked up once per
+// device (the first call on a device does this; make that first call before
+// any stream capture).
+noalloc_scratch* noalloc_scratch_ptr() {
+    int dev = 0;
+    CDBG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) throw std::runtime_error("device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            throw std::runtime_error(std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<noalloc_scratch*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+}  // namespace cdbg
+
+extern "C" int cdbg_gpu_supers_noalloc(const uint64_t* words, const uint64_t* run_soff,
+                                       const uint32_t* run_len, const uint32_t* run_color,
+                                       uint32_t num_runs, uint32_t k, uint32_t m, uint32_t num_buckets,
+                                       uint64_t* out_start, uint32_t* out_len, uint32_t* out_color,
+                                       uint32_t* out_flags, uint32_t* out_bucket, uint64_t out_cap,
+                                       uint64_t* n_supers, void* stream) {
+    using namespace cdbg;
+    try {
+        if (n_supers) *n_supers = 0;
+        if (k < 2 || k > 63 || m == 0 || m >= k || m > 32 || k - m > 62)
+            throw std::runtime_error("unsupported k/m combination");
+        if (num_buckets == 0) throw std::runtime_error("num_buckets must be > 0");
+        if (num_runs > NOALLOC_MAX_TILES)
+            throw std::runtime_error("more than 512 runs in one call (each run needs at least one tile)");
+        cudaStream_t st = (cudaStream_t)stream;
+        noalloc_scratch* s = noalloc_scratch_ptr();
+        CDBG_CUDA(cudaMemsetAsync(&s->err, 0, sizeof(uint32_t), st));
+        if (num_runs == 0) return 0;
+        k_run_tiles<<<grid(num_runs, 256), 256, 0, st>>>(num_runs, run_len, k, s->run_tiles);
+        CDBG_CHECK_LAUNCH();
+        k_noalloc_scan<uint64_t><<<1, 1024, 0, st>>>(s->run_tiles, num_runs, s->tile_start);
+        CDBG_CHECK_LAUNCH();
+        uint64_t ntiles = 0;
+        CDBG_CUDA(cudaMemcpyAsync(&ntiles, &s->tile_start[num_runs], 8, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        if (ntiles > NOALLOC_MAX_TILES)
+            throw std::runtime_error("input needs " + std::to_string(ntiles) +
+                                     " tiles; at most 512 tiles of 2048 (k-1)-mers per call");
+        k_minimizers<false><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(num_runs, s->tile_start, run_soff, run_len,
+                                                                     words, k, m, s->tile_count, nullptr, nullptr,
+                                                                     nullptr, nullptr, &s->err);
+        CDBG_CHECK_LAUNCH();
+        k_noalloc_scan<uint32_t><<<1, 1024, 0, st>>>(s->tile_count, (uint32_t)ntiles, s->tile_off);
+        CDBG_CHECK_LAUNCH();
+        uint64_t n = 0;
+        CDBG_CUDA(cudaMemcpyAsync(&n, &s->tile_off[ntiles], 8, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        if (n > out_cap) throw std::runtime_error("output capacity too small: need " + std::to_string(n));
+        k_minimizers<true><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(num_runs, s->tile_start, run_soff, run_len,
+                                                                    words, k, m, s->tile_count, s->tile_off,
+                                                                    s->minv, s->run, s->a, &s->err);
+        CDBG_CHECK_LAUNCH();
+        uint32_t bb = 0;
+        while ((1ull << bb) < num_buckets) ++bb;
+        if (n) {
+            k_super_finalize<<<grid(n, 256), 256, 0, st>>>(n, s->minv, s->run, s->a, run_soff, run_len, run_color,
+                                                           words, k, num_buckets, bb, out_start, out_len, out_color,
+                                                           out_flags, out_bucket, s->key);
+            CDBG_CHECK_LAUNCH();
+        }
+        uint32_t err = 0;
+        CDBG_CUDA(cudaMemcpyAsync(&err, &s->err, 4, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        if (err) throw std::runtime_error("device error " + std::to_string(err) + " in super-k-mer search");
+        if (n_supers) *n_supers = n;
+        return 0;
+    } catch (std::exception const& ex) {
+        set_last_error(ex.what());  // read back with cdbg_last_error()
+        return -1;
+    }
+}
+

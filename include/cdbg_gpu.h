@@ -176,6 +176,41 @@ typedef struct cdbg_build_result {
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
                    cdbg_build_result* r);
 
+/* Super-k-mers of pre-packed ACGT runs for callers that cannot allocate
+ * device memory.  No counterpart in the reference (which has no GPU path).
+ *
+ * Who needs it: code that must not call cudaMalloc/cudaFree or anything that
+ * allocates on the device -- for example inside a host application that owns
+ * all device memory through its own pool or budget, or where allocation is
+ * forbidden at that point.  Such a caller brings every input and output
+ * array; this function allocates nothing.  Its working memory is a fixed
+ * file-scope device array of about 24 MiB that every GPU loading this
+ * library holds until the process exits.
+ *
+ * Inputs (device): `words` is a 2-bit stream (base i at bits 2*(i%32) of word
+ * i/32, with at least two readable words after the last base); run r starts at
+ * base run_soff[r] (a multiple of 32) and has run_len[r] >= k ACGT bases and
+ * color run_color[r].  Outputs (device, out_cap entries each): per
+ * super-k-mer in emission order its stream start, length, color, flags
+ * (bit 0 begin, 1 end, 2 owns-first, 3 owns-last) and bucket -- the same
+ * super-k-mers cdbg_gpu_dump_supers reports.  *n_supers receives the count.
+ * Runs on `stream` (a cudaStream_t as void*, NULL = default stream).
+ *
+ * Limit: at most 512 tiles per call, a run taking ceil((len - k + 2) / 2048)
+ * tiles (so at most 512 runs and 1,048,576 (k-1)-mers); larger inputs are
+ * rejected with an error, as is an output capacity below the count.
+ * The first call on a device looks up the device address of the working
+ * array (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the working array, which keeps the previous
+ * call's contents: calls that overlap on the GPU (other streams or host
+ * threads) race and must be serialized by the caller.  Errors are reported
+ * through cdbg_last_error(). */
+int cdbg_gpu_supers_noalloc(const uint64_t* words, const uint64_t* run_soff, const uint32_t* run_len,
+                            const uint32_t* run_color, uint32_t num_runs, uint32_t k, uint32_t m,
+                            uint32_t num_buckets, uint64_t* out_start, uint32_t* out_len,
+                            uint32_t* out_color, uint32_t* out_flags, uint32_t* out_bucket,
+                            uint64_t out_cap, uint64_t* n_supers, void* stream);
+
 /* Copy `bytes` from a device pointer returned by cdbg_gpu_build
  * (outputs_to_host = 0) into host memory, on the engine's stream. */
 int cdbg_engine_copy_out(cdbg_engine* e, const void* device_src, void* host_dst, uint64_t bytes);
