@@ -562,12 +562,31 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         pp.k = k;
         pp.num_colors = p->num_colors;
         pp.batch_occ = p->batch_occ;
-        pp.to_host = p->outputs_to_host != 0;
+        pp.to_host = false;  // outputs accumulate in HBM; one D2H at the end when asked
         cdbg::phase2_result out;
         out.d_frag_out = &e->out_frag;
         out.d_words_out = &e->out_words;
         out.d_offsets_out = &e->out_offsets;
         cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, out);
+        const uint64_t nwords = (out.nbits + 63) / 64;
+        if (p->outputs_to_host) {
+            void* hf = e->h_frag.ensure(out.frag_nbytes + 8);
+            void* hw = e->h_words.ensure(8 * nwords + 8);
+            void* ho = e->h_offsets.ensure(8 * out.n_classes + 8);
+            if (out.frag_nbytes)
+                CDBG_CUDA(cudaMemcpyAsync(hf, out.d_frag, out.frag_nbytes, cudaMemcpyDeviceToHost, e->st));
+            if (nwords) CDBG_CUDA(cudaMemcpyAsync(hw, out.d_words, 8 * nwords, cudaMemcpyDeviceToHost, e->st));
+            if (out.n_classes)
+                CDBG_CUDA(cudaMemcpyAsync(ho, out.d_offsets, 8 * out.n_classes, cudaMemcpyDeviceToHost, e->st));
+            res.frag_bytes = (const uint8_t*)hf;
+            res.class_words = (const uint64_t*)hw;
+            res.class_offsets = (const uint64_t*)ho;
+            res.d2h_bytes = out.frag_nbytes + 8 * nwords + 8 * out.n_classes;
+        } else {
+            res.frag_bytes = out.d_frag;
+            res.class_words = out.d_words;
+            res.class_offsets = out.d_offsets;
+        }
         CDBG_CUDA(cudaEventRecord(ev[2], e->st));
         CDBG_CUDA(cudaEventSynchronize(ev[2]));
         float ms1 = 0, ms2 = 0;
@@ -588,19 +607,6 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         res.total_integers = out.total_integers;
         res.class_bits = out.nbits;
         res.frag_nbytes = out.frag_nbytes;
-        if (pp.to_host) {
-            e->h_frag.swap(out.frag);
-            e->h_words.swap(out.words);
-            e->h_offsets.swap(out.offsets);
-            res.frag_bytes = e->h_frag.data();
-            res.class_words = e->h_words.data();
-            res.class_offsets = e->h_offsets.data();
-            res.d2h_bytes = e->h_frag.size() + 8 * e->h_words.size() + 8 * e->h_offsets.size();
-        } else {
-            res.frag_bytes = out.d_frag;
-            res.class_words = out.d_words;
-            res.class_offsets = out.d_offsets;
-        }
         *r = res;
         return 0;
     } catch (std::exception const& ex) {

@@ -9,6 +9,28 @@
 #include "arena.cuh"
 #include "common.cuh"
 
+// Page-locked host buffer grown on demand and kept by the engine, so host
+// copies of build outputs run at full PCIe speed without re-pinning per call.
+struct pinned_buffer {
+    void* p = nullptr;
+    size_t cap = 0;
+    pinned_buffer() = default;
+    pinned_buffer(pinned_buffer const&) = delete;
+    ~pinned_buffer() {
+        if (p) cudaFreeHost(p);
+    }
+    void* ensure(size_t n) {
+        if (n <= cap && p) return p;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        size_t c = n > 2 * cap ? n : 2 * cap;
+        if (c == 0) c = 4096;
+        CDBG_CUDA(cudaMallocHost(&p, c));
+        cap = c;
+        return p;
+    }
+};
+
 struct cdbg_engine {
     int device = 0;
     cudaStream_t st = nullptr;      // stream all work runs on
@@ -20,9 +42,8 @@ struct cdbg_engine {
     cdbg::dvec<uint8_t> out_frag;
     cdbg::dvec<uint64_t> out_words, out_offsets;
     uint32_t* d_err = nullptr;  // device error word (outside the arena)
-    // outputs of the last cdbg_gpu_build (host copies)
-    std::vector<uint8_t> h_frag;
-    std::vector<uint64_t> h_words, h_offsets;
+    // host copies of the last cdbg_gpu_build's outputs (outputs_to_host = 1)
+    pinned_buffer h_frag, h_words, h_offsets;
 };
 
 namespace cdbg {

@@ -802,6 +802,115 @@ __global__ void k_assign_members(uint64_t n, uint32_t const* __restrict__ nidx, 
     if (rep[c] != c) cid[c] = cid[rep[c]];
 }
 
+__global__ void k_iota32(uint64_t n, uint32_t* __restrict__ p) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = (uint32_t)i;
+}
+
+__device__ __forceinline__ bool lists_equal(uint32_t const* a, uint64_t na, uint32_t const* b, uint64_t nb) {
+    if (na != nb) return false;
+    for (uint64_t i = 0; i < na; ++i)
+        if (a[i] != b[i]) return false;
+    return true;
+}
+
+// Members of an equal-hash run of candidates against the run head, on the
+// raw ascending color lists; rep[c] = head when equal, a differing member
+// marks its run for the exact fallback.
+__global__ void k_member_match_raw(uint64_t n, uint32_t const* __restrict__ head, uint64_t const* __restrict__ hpos,
+                                   uint64_t const* __restrict__ run_start, uint32_t const* __restrict__ nidx,
+                                   cand_view cv, list_src L, uint32_t* __restrict__ rep,
+                                   uint32_t* __restrict__ rep_first, uint32_t* __restrict__ collided) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t run = hpos[i] + head[i] - 1;
+    const uint32_t c = nidx[i];
+    const uint32_t h = nidx[run_start[run]];
+    if (c == h) {
+        rep[c] = c;
+        atomicMin(&rep_first[c], cv.first[c]);
+        return;
+    }
+    uint32_t const *pc, *ph;
+    uint64_t nc, nh;
+    cand_list(L, cv.kind_id[c], pc, nc);
+    cand_list(L, cv.kind_id[h], ph, nh);
+    if (lists_equal(pc, nc, ph, nh)) {
+        rep[c] = h;
+        atomicMin(&rep_first[h], cv.first[c]);
+    } else {
+        rep[c] = c;
+        collided[run] = 1;
+    }
+}
+
+__global__ void k_group_collided_raw(uint64_t nruns, uint32_t const* __restrict__ collided,
+                                     uint64_t const* __restrict__ run_start, uint64_t n,
+                                     uint32_t const* __restrict__ nidx, cand_view cv, list_src L,
+                                     uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns || !collided[r]) return;
+    const uint64_t i = run_start[r];
+    const uint64_t e = (r + 1 < nruns) ? run_start[r + 1] : n;
+    for (uint64_t j = i; j < e; ++j) {
+        const uint32_t cj = nidx[j];
+        uint32_t const* pj;
+        uint64_t lj;
+        cand_list(L, cv.kind_id[cj], pj, lj);
+        uint32_t rr = cj;
+        for (uint64_t q = i; q < j; ++q) {
+            const uint32_t cq = nidx[q];
+            if (rep[cq] != cq) continue;
+            uint32_t const* pq;
+            uint64_t lq;
+            cand_list(L, cv.kind_id[cq], pq, lq);
+            if (lists_equal(pj, lj, pq, lq)) {
+                rr = cq;
+                break;
+            }
+        }
+        rep[cj] = rr;
+        const uint32_t f = cv.first[cj];
+        if (rr == cj)
+            rep_first[cj] = f;
+        else if (f < rep_first[rr])
+            rep_first[rr] = f;
+    }
+}
+
+__global__ void k_rep_flags(uint64_t nc, uint32_t const* __restrict__ rep, uint32_t* __restrict__ is_rep) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) is_rep[c] = rep[c] == (uint32_t)c ? 1u : 0u;
+}
+
+// Compact the representatives into their own candidate view.
+__global__ void k_rep_compact(uint64_t nc, uint32_t const* __restrict__ is_rep, uint64_t const* __restrict__ pos,
+                              cand_view cv, uint32_t const* __restrict__ rep_first, cand_view rv,
+                              uint32_t* __restrict__ rep_index) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc || !is_rep[c]) return;
+    const uint64_t p = pos[c];
+    rv.kind_id[p] = cv.kind_id[c];
+    rv.first[p] = rep_first[c];
+    rv.hash[p] = cv.hash[c];
+    rep_index[c] = (uint32_t)p;
+}
+
+// New representatives (not in the dictionary): keys = first appearance.
+__global__ void k_new_reps(uint64_t nr, uint32_t const* __restrict__ rcid, uint64_t const* __restrict__ npos,
+                           cand_view rv, uint64_t* __restrict__ key, uint32_t* __restrict__ idx) {
+    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nr || rcid[j] != NONE32) return;
+    key[npos[j]] = rv.first[j];
+    idx[npos[j]] = (uint32_t)j;
+}
+
+__global__ void k_cand_cid(uint64_t nc, uint32_t const* __restrict__ rep, uint32_t const* __restrict__ rep_index,
+                           uint32_t const* __restrict__ rcid, uint32_t* __restrict__ cid) {
+    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) cid[c] = rcid[rep_index[rep[c]]];
+}
+
 // Per new class: encoded length, hash and color count.
 __global__ void k_new_sizes(uint64_t nnew, uint32_t const* __restrict__ rcand, cand_view cv, list_src L,
                             uint64_t const* __restrict__ cb, uint64_t* __restrict__ nbits,
@@ -1483,7 +1592,59 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     list_src L{R.col_off, R.colors, poff, pool, msize};
     uint32_t* cid = A.alloc<uint32_t>(nc + 1);
     if (nc) {
-        // candidate encodings (also the equality key)
+        // 1. group candidates with equal color sets (sort by set hash, then
+        //    compare raw lists inside equal-hash runs)
+        uint64_t* skey = A.alloc<uint64_t>(nc);
+        uint32_t* sidx = A.alloc<uint32_t>(nc);
+        CDBG_CUDA(cudaMemcpyAsync(skey, cv.hash, 8 * nc, cudaMemcpyDeviceToDevice, st));
+        k_iota32<<<grid(nc, 256), 256, 0, st>>>(nc, sidx);
+        CDBG_CHECK_LAUNCH();
+        prim::radix_sort_pairs<uint32_t>(skey, sidx, nc, 0, 64, A, st);
+        uint32_t* head = A.alloc<uint32_t>(nc);
+        uint64_t* hpos = A.alloc<uint64_t>(nc + 1);
+        k_run_heads<<<grid(nc, 256), 256, 0, st>>>(nc, skey, head);
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(head, hpos, nc, A, st, hpos + nc);
+        const uint64_t nruns = read_dev(hpos + nc, st);
+        uint64_t* run_start = A.alloc<uint64_t>(nruns + 1);
+        k_run_starts<<<grid(nc, 256), 256, 0, st>>>(nc, head, hpos, run_start);
+        CDBG_CHECK_LAUNCH();
+        uint32_t* rep = A.alloc<uint32_t>(nc);
+        uint32_t* rep_first = A.alloc<uint32_t>(nc);
+        uint32_t* collided = A.alloc<uint32_t>(nruns + 1);
+        CDBG_CUDA(cudaMemsetAsync(rep_first, 0xff, 4 * nc, st));
+        CDBG_CUDA(cudaMemsetAsync(collided, 0, 4 * (nruns + 1), st));
+        {
+            CDBG_PROF("k_member_match", st);
+            k_member_match_raw<<<grid(nc, 256), 256, 0, st>>>(nc, head, hpos, run_start, sidx, cv, L, rep, rep_first,
+                                                               collided);
+        }
+        CDBG_CHECK_LAUNCH();
+        {
+            unsigned long long* ncol = A.alloc<unsigned long long>(1);
+            CDBG_CUDA(cudaMemsetAsync(ncol, 0, 8, st));
+            k_count_flags<<<grid(nruns, 256), 256, 0, st>>>(nruns, collided, ncol);
+            CDBG_CHECK_LAUNCH();
+            if (read_dev(ncol, st)) {
+                k_group_collided_raw<<<grid(nruns, 128), 128, 0, st>>>(nruns, collided, run_start, nc, sidx, cv, L,
+                                                                       rep, rep_first);
+                CDBG_CHECK_LAUNCH();
+            }
+        }
+        // 2. representatives: compact, encode, look up in the dictionary
+        uint32_t* is_rep = A.alloc<uint32_t>(nc);
+        uint64_t* rpos = A.alloc<uint64_t>(nc + 1);
+        k_rep_flags<<<grid(nc, 256), 256, 0, st>>>(nc, rep, is_rep);
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(is_rep, rpos, nc, A, st, rpos + nc);
+        const uint64_t nr = read_dev(rpos + nc, st);
+        cand_view rv;
+        rv.kind_id = A.alloc<uint32_t>(nr + 1);
+        rv.first = A.alloc<uint32_t>(nr + 1);
+        rv.hash = A.alloc<uint64_t>(nr + 1);
+        uint32_t* rep_index = A.alloc<uint32_t>(nc);
+        k_rep_compact<<<grid(nc, 256), 256, 0, st>>>(nc, is_rep, rpos, cv, rep_first, rv, rep_index);
+        CDBG_CHECK_LAUNCH();
         const uint32_t nw = (C + 31) / 32;
         int wpb = (int)std::max<uint64_t>(1, std::min<uint64_t>(8, (96 * 1024) / (4ull * nw)));
         const size_t shm = (size_t)wpb * nw * 4;
@@ -1491,95 +1652,51 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             CDBG_CUDA(cudaFuncSetAttribute(k_encode<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
             CDBG_CUDA(cudaFuncSetAttribute(k_encode<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         }
-        uint64_t* cbits = A.alloc<uint64_t>(nc);
-        uint64_t* cb = A.alloc<uint64_t>(nc + 1);
+        uint64_t* cbits = A.alloc<uint64_t>(nr);
+        uint64_t* cb = A.alloc<uint64_t>(nr + 1);
         {
             CDBG_PROF("k_encode", st);
-            k_encode<false><<<grid(nc, wpb), wpb * 32, shm, st>>>(nc, cv, L, C, cbits, nullptr, nullptr);
+            k_encode<false><<<grid(nr, wpb), wpb * 32, shm, st>>>(nr, rv, L, C, cbits, nullptr, nullptr);
         }
         CDBG_CHECK_LAUNCH();
-        prim::exclusive_scan<uint64_t, uint64_t>(cbits, cb, nc, A, st, cb + nc);
-        const uint64_t ctot = read_dev(cb + nc, st);
+        prim::exclusive_scan<uint64_t, uint64_t>(cbits, cb, nr, A, st, cb + nr);
+        const uint64_t ctot = read_dev(cb + nr, st);
         const uint64_t cwn = ctot / 64 + 4;
         uint64_t* cw = A.alloc<uint64_t>(cwn);
         CDBG_CUDA(cudaMemsetAsync(cw, 0, 8 * cwn, st));
         {
             CDBG_PROF("k_encode", st);
-            k_encode<true><<<grid(nc, wpb), wpb * 32, shm, st>>>(nc, cv, L, C, nullptr, cb, cw);
+            k_encode<true><<<grid(nr, wpb), wpb * 32, shm, st>>>(nr, rv, L, C, nullptr, cb, cw);
         }
         CDBG_CHECK_LAUNCH();
+        uint32_t* rcid = A.alloc<uint32_t>(nr + 1);
         {
             CDBG_PROF("k_dict_lookup", st);
-            k_dict_lookup<<<grid(nc, 256), 256, 0, st>>>(nc, cv, cw, cb, dict.view(), cid);
+            k_dict_lookup<<<grid(nr, 256), 256, 0, st>>>(nr, rv, cw, cb, dict.view(), rcid);
         }
         CDBG_CHECK_LAUNCH();
-        // ---- new classes
-        uint32_t* nflag = A.alloc<uint32_t>(nc);
-        uint64_t* npos = A.alloc<uint64_t>(nc + 1);
-        k_new_flags<<<grid(nc, 256), 256, 0, st>>>(nc, cid, nflag);
+        // 3. new classes in order of first appearance
+        uint32_t* nflag = A.alloc<uint32_t>(nr);
+        uint64_t* npos = A.alloc<uint64_t>(nr + 1);
+        k_new_flags<<<grid(nr, 256), 256, 0, st>>>(nr, rcid, nflag);
         CDBG_CHECK_LAUNCH();
-        prim::exclusive_scan<uint32_t, uint64_t>(nflag, npos, nc, A, st, npos + nc);
-        const uint64_t nn = read_dev(npos + nc, st);
-        if (nn) {
-            uint64_t* nkey = A.alloc<uint64_t>(nn);
-            uint32_t* nidx = A.alloc<uint32_t>(nn);
-            k_new_gather<<<grid(nc, 256), 256, 0, st>>>(nc, nflag, npos, cv, nkey, nidx);
-            CDBG_CHECK_LAUNCH();
-            prim::radix_sort_pairs<uint32_t>(nkey, nidx, nn, 0, 64, A, st);
-            uint32_t* head = A.alloc<uint32_t>(nn);
-            uint64_t* hpos = A.alloc<uint64_t>(nn + 1);
-            k_run_heads<<<grid(nn, 256), 256, 0, st>>>(nn, nkey, head);
-            CDBG_CHECK_LAUNCH();
-            prim::exclusive_scan<uint32_t, uint64_t>(head, hpos, nn, A, st, hpos + nn);
-            const uint64_t nruns = read_dev(hpos + nn, st);
-            uint64_t* run_start = A.alloc<uint64_t>(nruns + 1);
-            k_run_starts<<<grid(nn, 256), 256, 0, st>>>(nn, head, hpos, run_start);
-            CDBG_CHECK_LAUNCH();
-            uint32_t* rep = A.alloc<uint32_t>(nc);
-            uint32_t* rep_first = A.alloc<uint32_t>(nc);
-            uint32_t* collided = A.alloc<uint32_t>(nruns + 1);
-            CDBG_CUDA(cudaMemsetAsync(rep_first, 0xff, 4 * nc, st));
-            CDBG_CUDA(cudaMemsetAsync(collided, 0, 4 * (nruns + 1), st));
-            {
-                CDBG_PROF("k_member_match", st);
-                k_member_match<<<grid(nn, 256), 256, 0, st>>>(nn, head, hpos, run_start, nidx, cv, cw, cb, rep,
-                                                               rep_first, collided);
-            }
-            CDBG_CHECK_LAUNCH();
-            {
-                unsigned long long* ncol = A.alloc<unsigned long long>(1);
-                CDBG_CUDA(cudaMemsetAsync(ncol, 0, 8, st));
-                k_count_flags<<<grid(nruns, 256), 256, 0, st>>>(nruns, collided, ncol);
-                CDBG_CHECK_LAUNCH();
-                if (read_dev(ncol, st)) {
-                    k_group_collided<<<grid(nruns, 128), 128, 0, st>>>(nruns, collided, run_start, nn, nidx, cv, cw,
-                                                                       cb, rep, rep_first);
-                    CDBG_CHECK_LAUNCH();
-                }
-            }
-            uint32_t* is_rep = A.alloc<uint32_t>(nn);
-            uint64_t* rpos2 = A.alloc<uint64_t>(nn + 1);
-            k_rep_keys<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, is_rep);
-            CDBG_CHECK_LAUNCH();
-            prim::exclusive_scan<uint32_t, uint64_t>(is_rep, rpos2, nn, A, st, rpos2 + nn);
-            const uint64_t nnew = read_dev(rpos2 + nn, st);
+        prim::exclusive_scan<uint32_t, uint64_t>(nflag, npos, nr, A, st, npos + nr);
+        const uint64_t nnew = read_dev(npos + nr, st);
+        if (nnew) {
             uint64_t* rkey = A.alloc<uint64_t>(nnew);
             uint32_t* rcand = A.alloc<uint32_t>(nnew);
-            k_rep_gather<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, is_rep, rpos2, rep_first, rkey, rcand);
+            k_new_reps<<<grid(nr, 256), 256, 0, st>>>(nr, rcid, npos, rv, rkey, rcand);
             CDBG_CHECK_LAUNCH();
             prim::radix_sort_pairs<uint32_t>(rkey, rcand, nnew, 0, 32, A, st);
             const uint64_t base = dict.n;
-            k_assign_new<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, base, cid);
+            k_assign_new<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, base, rcid);
             CDBG_CHECK_LAUNCH();
-            k_assign_members<<<grid(nn, 256), 256, 0, st>>>(nn, nidx, rep, cid);
-            CDBG_CHECK_LAUNCH();
-            // append to the dictionary: hashes, bit offsets, encodings
             uint64_t* nbits = A.alloc<uint64_t>(nnew);
             uint64_t* nh = A.alloc<uint64_t>(nnew);
             uint64_t* boff = A.alloc<uint64_t>(nnew + 1);
             unsigned long long* ints = A.alloc<unsigned long long>(1);
             CDBG_CUDA(cudaMemsetAsync(ints, 0, 8, st));
-            k_new_sizes<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, cv, L, cb, nbits, nh, ints);
+            k_new_sizes<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, rv, L, cb, nbits, nh, ints);
             CDBG_CHECK_LAUNCH();
             prim::exclusive_scan<uint64_t, uint64_t>(nbits, boff, nnew, A, st, boff + nnew);
             const uint64_t badd = read_dev(boff + nnew, st);
@@ -1602,6 +1719,9 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             dict.words.n = (dict.nbits + 63) / 64;
             dict.ensure_table(base, st, d_err);
         }
+        // 4. every candidate takes its representative's class id
+        k_cand_cid<<<grid(nc, 256), 256, 0, st>>>(nc, rep, rep_index, rcid, cid);
+        CDBG_CHECK_LAUNCH();
     }
     // ---- node class ids
     uint32_t* n_cid = A.alloc<uint32_t>(D);
