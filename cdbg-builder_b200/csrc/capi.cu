@@ -486,6 +486,7 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         pp.batch_occ = a->batch_occ;
         pp.to_host = true;
         cdbg::phase2_result res;
+        res.state = &e->p2;
         cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, res);
         const double dev_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - td).count();
         // frag spill
@@ -564,9 +565,7 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         pp.batch_occ = p->batch_occ;
         pp.to_host = false;  // outputs accumulate in HBM; one D2H at the end when asked
         cdbg::phase2_result out;
-        out.d_frag_out = &e->out_frag;
-        out.d_words_out = &e->out_words;
-        out.d_offsets_out = &e->out_offsets;
+        out.state = &e->p2;
         cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, out);
         const uint64_t nwords = (out.nbits + 63) / 64;
         if (p->outputs_to_host) {

@@ -8,6 +8,7 @@
 
 #include "arena.cuh"
 #include "common.cuh"
+#include "phase2.cuh"
 
 // Page-locked host buffer grown on demand and kept by the engine, so host
 // copies of build outputs run at full PCIe speed without re-pinning per call.
@@ -38,9 +39,8 @@ struct cdbg_engine {
     cdbg::kernel_profiler prof;
     cdbg::dev_arena A;   // per-stage scratch
     cdbg::dev_arena P;   // phase-1 outputs kept through phase 2 (in-memory build)
-    // device-resident outputs of the last cdbg_gpu_build (outputs_to_host = 0)
-    cdbg::dvec<uint8_t> out_frag;
-    cdbg::dvec<uint64_t> out_words, out_offsets;
+    // class dictionary + device-resident outputs, reused across builds
+    cdbg::phase2_state p2;
     uint32_t* d_err = nullptr;  // device error word (outside the arena)
     // host copies of the last cdbg_gpu_build's outputs (outputs_to_host = 1)
     pinned_buffer h_frag, h_words, h_offsets;

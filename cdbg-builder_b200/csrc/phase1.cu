@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -205,21 +206,34 @@ __device__ __forceinline__ bool tma_load_1d(void* smem_dst, void const* gsrc, ui
     return ok != 0;
 }
 
-template <bool EMIT>
+// MODE 0: count the cuts of each tile (tile_count).  MODE 1: write them at
+// tile_off.  MODE 2: one pass -- tiles take indices in launch order from
+// tile_counter, publish their count in `status` and read their predecessors'
+// prefix (decoupled look-back, bounded waits), then write at most `cap`
+// entries; the grand total ends in the last tile's status.
+template <int MODE>
 __global__ void __launch_bounds__(MZ_THREADS)
     k_minimizers(uint32_t nruns, uint64_t const* __restrict__ tile_start,
                  uint64_t const* __restrict__ soff, uint32_t const* __restrict__ len,
                  uint64_t const* __restrict__ words, uint32_t k, uint32_t m,
                  uint32_t* __restrict__ tile_count, uint64_t const* __restrict__ tile_off,
                  uint64_t* __restrict__ out_min, uint32_t* __restrict__ out_run,
-                 uint32_t* __restrict__ out_a, uint32_t* err) {
+                 uint32_t* __restrict__ out_a, uint32_t* err, uint32_t* tile_counter = nullptr,
+                 unsigned long long* status = nullptr, uint64_t ntiles = 0, uint64_t cap = 0) {
     __shared__ __align__(16) uint64_t sw[MZ_WMAX];
     __shared__ uint64_t sh[MZ_HMAX];
     __shared__ uint64_t smin[MZ_TT + 1];
     __shared__ uint32_t sred[MZ_THREADS / 32 + 1];
     __shared__ __align__(8) uint64_t bar;
+    __shared__ uint64_t s_tile, s_excl;
 
-    const uint64_t tile = blockIdx.x;
+    uint64_t tile = blockIdx.x;
+    if (MODE == 2) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        tile = s_tile;
+        if (tile >= ntiles) return;
+    }
     const uint32_t r = upper_bound_u64(tile_start, nruns + 1, tile) - 1;
     const uint64_t t_local = tile - tile_start[r];
     const uint32_t L = len[r];
@@ -236,7 +250,10 @@ __global__ void __launch_bounds__(MZ_THREADS)
     const uint64_t wa = (pa >> 5) & ~uint64_t(1);
     const uint64_t wb = ((pb + 31) >> 5) + 1;
     const uint32_t nw = (uint32_t)(((wb - wa) + 1) & ~uint64_t(1));
-    if (!tma_load_1d(sw, words + wa, nw * 8u, &bar, err)) return;  // uniform across the block
+    if (!tma_load_1d(sw, words + wa, nw * 8u, &bar, err)) {  // uniform across the block
+        if (MODE == 2 && threadIdx.x == 0) atomicExch(&status[tile], (2ull << 62));  // unblock successors
+        return;
+    }
     const uint32_t rel0 = (uint32_t)(pa - wa * 32);  // stream offset of base e0 in sw
     auto base_at = [&](uint32_t q) -> uint32_t {     // q relative to e0
         const uint32_t x = rel0 + q;
@@ -312,18 +329,58 @@ __global__ void __launch_bounds__(MZ_THREADS)
     }
     uint32_t tot;
     const uint32_t ex = prim::block_exclusive_scan<uint32_t, MZ_THREADS>(cnt, sred, tot);
-    if (!EMIT) {
+    if (MODE == 0) {
         if (threadIdx.x == 0) tile_count[tile] = tot;
         return;
     }
-    uint64_t o = tile_off[tile] + ex;
+    uint64_t base;
+    if (MODE == 1) {
+        base = tile_off[tile];
+    } else {
+        constexpr unsigned long long AGG = 1ull << 62, INC = 2ull << 62, VAL = (1ull << 62) - 1;
+        if (threadIdx.x == 0) {
+            uint64_t excl = 0;
+            bool ok = true;
+            if (tile == 0) {
+                atomicExch(&status[0], INC | tot);
+            } else {
+                atomicExch(&status[tile], AGG | tot);
+                for (uint64_t j = tile - 1;; --j) {
+                    unsigned long long v = 0;
+                    // the predecessor took its index earlier, so it is running or done
+                    for (uint32_t spin = 0; spin < (1u << 26); ++spin) {
+                        v = *(volatile unsigned long long*)&status[j];
+                        if (v >> 62) break;
+                    }
+                    if (!(v >> 62)) {
+                        ok = false;
+                        break;
+                    }
+                    excl += v & VAL;
+                    if ((v >> 62) == 2 || j == 0) break;
+                }
+                atomicExch(&status[tile], INC | ((excl + tot) & VAL));
+            }
+            if (!ok) {
+                set_error(err, ERR_CHAIN_LIMIT);
+                excl = ~0ull;
+            }
+            s_excl = excl;
+        }
+        __syncthreads();
+        base = s_excl;
+        if (base == ~0ull) return;
+    }
+    uint64_t o = base + ex;
     for (uint32_t c = c0; c < c0 + MZ_PER && c < ncut; ++c) {
         const uint64_t j = j0 + c;
         const uint32_t q = c + off;
         if (j == 0 || smin[q] != smin[q - 1]) {
-            out_min[o] = smin[q];
-            out_run[o] = r;
-            out_a[o] = (uint32_t)j;
+            if (MODE == 1 || o < cap) {
+                out_min[o] = smin[q];
+                out_run[o] = r;
+                out_a[o] = (uint32_t)j;
+            }
             ++o;
         }
     }
@@ -693,26 +750,47 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint64_t, uint64_t>(ntl, tstart, rt.n, A, st, tstart + rt.n);
     const uint64_t ntiles = read_dev(tstart + rt.n, st);
-    uint32_t* tcount = A.alloc<uint32_t>(ntiles);
-    uint64_t* toff = A.alloc<uint64_t>(ntiles + 1);
+    // one pass with a capacity of 1/4 of the (k-1)-mers (about 2.5x the
+    // density of random sequence); the exact two-pass path if it overflows
+    const uint64_t npos = rt.n_kmers + rt.n;
+    uint64_t cap = std::max<uint64_t>(1ull << 20, npos / 4);
+    uint64_t* minv = A.alloc<uint64_t>(cap);
+    uint32_t* run = A.alloc<uint32_t>(cap);
+    uint32_t* aa = A.alloc<uint32_t>(cap);
+    unsigned long long* status = A.alloc<unsigned long long>(ntiles);
+    uint32_t* counter = A.alloc<uint32_t>(1);
+    CDBG_CUDA(cudaMemsetAsync(status, 0, 8 * ntiles, st));
+    CDBG_CUDA(cudaMemsetAsync(counter, 0, 4, st));
     {
         CDBG_PROF("k_minimizers", st);
-        k_minimizers<false><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
-            rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, nullptr, nullptr, nullptr, nullptr, d_err);
+        k_minimizers<2><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(rt.n, tstart, rt.soff, rt.len, rt.words, k, m,
+                                                                 nullptr, nullptr, minv, run, aa, d_err, counter,
+                                                                 status, ntiles, cap);
     }
     CDBG_CHECK_LAUNCH();
-    prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, ntiles, A, st, toff + ntiles);
-    const uint64_t n = read_dev(toff + ntiles, st);
+    uint64_t n = read_dev(status + ntiles - 1, st) & ((1ull << 62) - 1);
+    if (n > cap) {
+        uint32_t* tcount = A.alloc<uint32_t>(ntiles);
+        uint64_t* toff = A.alloc<uint64_t>(ntiles + 1);
+        {
+            CDBG_PROF("k_minimizers", st);
+            k_minimizers<0><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+                rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, nullptr, nullptr, nullptr, nullptr, d_err);
+        }
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, ntiles, A, st, toff + ntiles);
+        n = read_dev(toff + ntiles, st);
+        minv = A.alloc<uint64_t>(n);
+        run = A.alloc<uint32_t>(n);
+        aa = A.alloc<uint32_t>(n);
+        {
+            CDBG_PROF("k_minimizers", st);
+            k_minimizers<1><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+                rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, toff, minv, run, aa, d_err);
+        }
+        CDBG_CHECK_LAUNCH();
+    }
     if (n >= 0xffffffffull) throw std::runtime_error("more than 2^32 super-k-mers in one call");
-    uint64_t* minv = A.alloc<uint64_t>(n);
-    uint32_t* run = A.alloc<uint32_t>(n);
-    uint32_t* aa = A.alloc<uint32_t>(n);
-    {
-        CDBG_PROF("k_minimizers", st);
-        k_minimizers<true><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
-            rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, toff, minv, run, aa, d_err);
-    }
-    CDBG_CHECK_LAUNCH();
     out.n = n;
     out.start = A.alloc<uint64_t>(n);
     out.len = A.alloc<uint32_t>(n);

@@ -239,7 +239,8 @@ __global__ void k_init_tables(uint64_t T, K* key, uint32_t* meta, unsigned long 
 
 template <typename K>
 __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_t R0, uint64_t nrec,
-                                                uint64_t O0, uint64_t nocc, uint32_t k, uint32_t* err) {
+                                                uint64_t O0, uint64_t nocc, uint32_t k,
+                                                uint32_t* __restrict__ occ_slot, uint32_t* err) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nocc) return;
     const occ_info<K> oi = decode_occ<K>(R, R0, nrec, O0 + t, k);
@@ -247,8 +248,11 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     const uint64_t s = table_upsert<K>(T.key, T.tab_off[tb], T.tab_cap[tb], oi.can);
     if (s == ~0ull) {
         set_error(err, ERR_TABLE_FULL);
+        occ_slot[t] = NONE32;
         return;
     }
+    // slot of this occurrence, bit 31 = owned (read by k_multi_pairs)
+    occ_slot[t] = (uint32_t)s | (oi.owned ? 0x80000000u : 0u);
     const uint32_t mo = oi.contrib | (oi.owned ? M_PRIMARY : 0u);
     if (mo && (T.meta[s] & mo) != mo) atomicOr(&T.meta[s], mo);
     const unsigned long long rk = ((unsigned long long)oi.r << 32) | oi.idx;
@@ -299,26 +303,25 @@ __global__ void k_make_nodes(uint64_t T, K const* __restrict__ key, uint32_t con
     n_bucket[n] = rbucket[rk >> 32];
 }
 
-// (node << 32 | record) for owned occurrences of multi-record k-mers.
-template <typename K, bool WRITE>
+// (node << 32 | record) for owned occurrences of multi-record k-mers, from the
+// slot each occurrence recorded at insert time.
+template <bool WRITE>
 __global__ void __launch_bounds__(256)
-    k_multi_pairs(rec_view R, tables<K> T, uint64_t R0, uint64_t nrec, uint64_t O0, uint64_t nocc,
-                  uint32_t k, uint32_t const* __restrict__ n_rec, unsigned long long* __restrict__ cnt,
+    k_multi_pairs(uint64_t const* __restrict__ occ, uint64_t R0, uint64_t nrec, uint64_t O0, uint64_t nocc,
+                  uint32_t const* __restrict__ occ_slot, uint32_t const* __restrict__ node,
+                  uint32_t const* __restrict__ n_rec, unsigned long long* __restrict__ cnt,
                   uint64_t* __restrict__ pairs) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool emit = false;
     uint64_t val = 0;
     if (t < nocc) {
-        const occ_info<K> oi = decode_occ<K>(R, R0, nrec, O0 + t, k);
-        if (oi.owned) {
-            const uint32_t tb = R.bucket[oi.r] - T.b0;
-            const uint64_t s = table_find<K>(T.key, T.tab_off[tb], T.tab_cap[tb], oi.can);
-            if (s != ~0ull) {
-                const uint32_t n = T.node[s];
-                if (n_rec[n] == MULTI_TAG) {
-                    emit = true;
-                    val = ((uint64_t)n << 32) | oi.r;
-                }
+        const uint32_t v = occ_slot[t];
+        if (v != NONE32 && (v & 0x80000000u)) {
+            const uint32_t n = node[v & 0x7fffffffu];
+            if (n_rec[n] == MULTI_TAG) {
+                const uint32_t rr = upper_bound_u64(occ + R0, nrec + 1, O0 + t) - 1;
+                emit = true;
+                val = ((uint64_t)n << 32) | (uint32_t)(R0 + rr);
             }
         }
     }
@@ -1240,29 +1243,38 @@ __global__ void k_chain_cycles(chain_ws W, uint32_t* err) {
 // ---- fragments --------------------------------------------------------------
 __device__ __forceinline__ uint32_t frag_cid(uint32_t const* n_cid, uint32_t node) { return n_cid[node]; }
 
-__global__ void k_frag_sizes(uint64_t D, uint32_t const* __restrict__ seed_start, uint32_t const* __restrict__ seed_len,
-                             uint32_t const* __restrict__ fe, uint32_t const* __restrict__ n_cid, uint32_t k,
-                             uint64_t* __restrict__ sz, uint32_t* __restrict__ is_seed,
-                             unsigned long long* __restrict__ seq_total) {
+// Seed nodes in node order (= fragment order): seed_of[f] = node of fragment f.
+__global__ void k_seed_flags(uint64_t D, uint32_t const* __restrict__ seed_len, uint32_t* __restrict__ is_seed) {
     uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= D) return;
-    const uint32_t len = seed_len[n];
-    if (!len) {
-        sz[n] = 0;
-        is_seed[n] = 0;
-        return;
+    if (n < D) is_seed[n] = seed_len[n] ? 1u : 0u;
+}
+__global__ void k_seed_list(uint64_t D, uint32_t const* __restrict__ is_seed, uint64_t const* __restrict__ fpos,
+                            uint32_t* __restrict__ seed_of) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < D && is_seed[n]) seed_of[fpos[n]] = (uint32_t)n;
+}
+
+// Thread per fragment: serialized size (frag_unitig_writer::write_batch layout).
+__global__ void k_frag_sizes(uint64_t F, uint32_t const* __restrict__ seed_of, uint32_t const* __restrict__ seed_start,
+                             uint32_t const* __restrict__ seed_len, uint32_t const* __restrict__ fe,
+                             uint32_t const* __restrict__ n_cid, uint32_t k, uint64_t* __restrict__ sz,
+                             unsigned long long* __restrict__ seq_total) {
+    uint64_t f = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t seq = 0;
+    if (f < F) {
+        const uint32_t n = seed_of[f];
+        const uint32_t len = seed_len[n], a = seed_start[n];
+        uint32_t runs = 1, prev = frag_cid(n_cid, fe[a] >> 1);
+        for (uint32_t j = 1; j < len; ++j) {
+            const uint32_t c = frag_cid(n_cid, fe[a + j] >> 1);
+            runs += c != prev;
+            prev = c;
+        }
+        seq = (uint64_t)k + len - 1;
+        sz[f] = 1 + 4 + 12ull * runs + 4 + seq;
     }
-    is_seed[n] = 1;
-    const uint32_t a = seed_start[n];
-    uint32_t runs = 1, prev = frag_cid(n_cid, fe[a] >> 1);
-    for (uint32_t j = 1; j < len; ++j) {
-        const uint32_t c = frag_cid(n_cid, fe[a + j] >> 1);
-        if (c != prev) ++runs;
-        prev = c;
-    }
-    const uint64_t seq = (uint64_t)k + len - 1;
-    sz[n] = 1 + 4 + 12ull * runs + 4 + seq;
-    atomicAdd(seq_total, (unsigned long long)seq);
+    seq = prim::warp_inclusive_scan(seq);
+    if ((threadIdx.x & 31) == 31 && seq) atomicAdd(seq_total, (unsigned long long)seq);
 }
 
 __device__ __forceinline__ void put_bytes(uint8_t* o, uint64_t v, int n) {
@@ -1270,19 +1282,19 @@ __device__ __forceinline__ void put_bytes(uint8_t* o, uint64_t v, int n) {
 }
 
 template <typename K>
-__global__ void k_frag_write(uint64_t D, uint32_t const* __restrict__ seed_start, uint32_t const* __restrict__ seed_len,
-                             uint8_t const* __restrict__ seed_open, uint32_t const* __restrict__ fe,
-                             uint32_t const* __restrict__ n_cid, K const* __restrict__ n_key, uint32_t k,
-                             uint64_t const* __restrict__ off, uint8_t* __restrict__ out) {
-    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= D) return;
-    const uint32_t len = seed_len[n];
-    if (!len) return;
+__global__ void k_frag_write(uint64_t F, uint32_t const* __restrict__ seed_of, uint32_t const* __restrict__ seed_start,
+                             uint32_t const* __restrict__ seed_len, uint8_t const* __restrict__ seed_open,
+                             uint32_t const* __restrict__ fe, uint32_t const* __restrict__ n_cid,
+                             K const* __restrict__ n_key, uint32_t k, uint64_t const* __restrict__ off,
+                             uint8_t* __restrict__ out) {
+    uint64_t f = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) return;
     typedef kmer_ops<K> ops;
+    const uint32_t n = seed_of[f];
+    const uint32_t len = seed_len[n];
     const uint32_t a = seed_start[n];
-    uint8_t* o = out + off[n];
+    uint8_t* o = out + off[f];
     o[0] = seed_open[n];
-    // runs
     uint32_t runs = 0;
     uint8_t* rp = o + 5;
     uint32_t prev = frag_cid(n_cid, fe[a] >> 1), cnt = 1;
@@ -1319,7 +1331,7 @@ __global__ void k_frag_write(uint64_t D, uint32_t const* __restrict__ seed_start
     }
 }
 
-
+// ---------------------------------------------------------------------------
 // ---- small helpers ----------------------------------------------------------
 __global__ void k_count_flags(uint64_t n, uint32_t const* __restrict__ f, unsigned long long* __restrict__ c) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1378,18 +1390,26 @@ __global__ void k_dict_insert(uint64_t c0, uint64_t c1, uint64_t const* __restri
 // its 64-bit set hash and its bit range in the encoded .color_sets vector; an
 // open-addressing table hash -> class id.  Equality is tested on encodings.
 struct class_dict {
-    dvec<uint64_t> cls_hash;  // n
-    dvec<uint64_t> bit_off;   // n + 1 (last = nbits)
-    dvec<uint64_t> words;     // encoded classes, zero beyond nbits
-    dvec<uint64_t> slot_hash;
-    dvec<uint32_t> slot_cid;
+    dvec<uint64_t>& cls_hash;  // n
+    dvec<uint64_t>& bit_off;   // n + 1 (last = nbits)
+    dvec<uint64_t>& words;     // encoded classes, zero beyond nbits
+    dvec<uint64_t>& slot_hash;
+    dvec<uint32_t>& slot_cid;
     uint64_t n = 0, nbits = 0, total_integers = 0, mask = 0;
 
+    explicit class_dict(phase2_state& S)
+        : cls_hash(S.cls_hash), bit_off(S.bit_off), words(S.words), slot_hash(S.slot_hash), slot_cid(S.slot_cid) {}
+
+    // Start empty, keeping the storage of a previous build (words are zeroed
+    // where the previous build wrote).
     void init(cudaStream_t st) {
         bit_off.reserve(1024, st);
         CDBG_CUDA(cudaMemsetAsync(bit_off.p, 0, 8, st));
         bit_off.n = 1;
         words.reserve(1024, st, true);
+        if (words.n) CDBG_CUDA(cudaMemsetAsync(words.p, 0, 8 * std::min(words.n + 4, words.cap), st));
+        words.n = 0;
+        cls_hash.n = 0;
     }
     dict_view view() const { return dict_view{slot_hash.p, slot_cid.p, mask, bit_off.p, words.p}; }
     // Make room for n classes (load <= 1/2); classes [first_new, n) still need
@@ -1431,11 +1451,14 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint64_t T = 0;
     for (uint32_t b = 0; b < nb; ++b) {
         const uint64_t o = bocc[b0 + b + 1] - bocc[b0 + b];
-        const uint64_t cap = o ? std::max<uint64_t>(64, o + o / 2 + 16) : 0;
+        // load factor <= 1/2: short unsuccessful probes for the neighbour lookups
+        const uint64_t cap = o ? std::max<uint64_t>(64, 2 * o + 16) : 0;
         toff[b] = T;
         tcap[b] = cap;
         T += cap;
     }
+    if (T >= (1ull << 31)) throw std::runtime_error("k-mer table of one bucket batch exceeds 2^31 slots");
+    uint32_t* occ_slot = A.alloc<uint32_t>(nocc);
     uint64_t* d_toff = A.alloc<uint64_t>(nb);
     uint64_t* d_tcap = A.alloc<uint64_t>(nb);
     CDBG_CUDA(cudaMemcpyAsync(d_toff, toff.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
@@ -1458,7 +1481,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     // ---- load
     {
         CDBG_PROF("k_insert", st);
-        k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, d_err);
+        k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, occ_slot, d_err);
     }
     CDBG_CHECK_LAUNCH();
     // ---- nodes in first-insertion order
@@ -1493,7 +1516,8 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
     {
         CDBG_PROF("k_multi_pairs", st);
-        k_multi_pairs<K, false><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, nullptr);
+        k_multi_pairs<false><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, TB.node, n_rec, cnt,
+                                                              nullptr);
     }
     CDBG_CHECK_LAUNCH();
     const uint64_t npairs = read_dev(cnt, st);
@@ -1510,7 +1534,8 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
         {
             CDBG_PROF("k_multi_pairs", st);
-            k_multi_pairs<K, true><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, n_rec, cnt, pairs);
+            k_multi_pairs<true><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, TB.node, n_rec,
+                                                                 cnt, pairs);
         }
         CDBG_CHECK_LAUNCH();
         uint32_t* dummy = A.alloc<uint32_t>(npairs);
@@ -1771,37 +1796,35 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         k_chain_cycles<<<grid(D, 128), 128, 0, st>>>(W, d_err);
     }
     CDBG_CHECK_LAUNCH();
-    // ---- fragments
-    uint64_t* fsz = A.alloc<uint64_t>(D);
+    // ---- fragments, in seed order
     uint32_t* is_seed = A.alloc<uint32_t>(D);
-    uint64_t* foff = A.alloc<uint64_t>(D + 1);
+    uint64_t* fpos = A.alloc<uint64_t>(D + 1);
+    k_seed_flags<<<grid(D, 256), 256, 0, st>>>(D, W.seed_len, is_seed);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(is_seed, fpos, D, A, st, fpos + D);
+    const uint64_t nfr = read_dev(fpos + D, st);
+    check_device_error_word(d_err, st, "unitig walk");
+    uint32_t* seed_of = A.alloc<uint32_t>(nfr + 1);
+    k_seed_list<<<grid(D, 256), 256, 0, st>>>(D, is_seed, fpos, seed_of);
+    CDBG_CHECK_LAUNCH();
+    uint64_t* fsz = A.alloc<uint64_t>(nfr + 1);
+    uint64_t* foff = A.alloc<uint64_t>(nfr + 1);
     unsigned long long* seqt = A.alloc<unsigned long long>(1);
     CDBG_CUDA(cudaMemsetAsync(seqt, 0, 8, st));
-    {
+    if (nfr) {
         CDBG_PROF("k_frag_sizes", st);
-        k_frag_sizes<<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.fe, n_cid, k, fsz, is_seed, seqt);
+        k_frag_sizes<<<grid(nfr, 256), 256, 0, st>>>(nfr, seed_of, W.seed_start, W.seed_len, W.fe, n_cid, k, fsz, seqt);
     }
     CDBG_CHECK_LAUNCH();
-    prim::exclusive_scan<uint64_t, uint64_t>(fsz, foff, D, A, st, foff + D);
-    const uint64_t fbytes = read_dev(foff + D, st);
-    check_device_error_word(d_err, st, "unitig walk");
+    prim::exclusive_scan<uint64_t, uint64_t>(fsz, foff, nfr, A, st, foff + nfr);
+    const uint64_t fbytes = read_dev(foff + nfr, st);
     uint8_t* fb = A.alloc<uint8_t>(fbytes + 8);
-    {
+    if (nfr) {
         CDBG_PROF("k_frag_write", st);
-        k_frag_write<K><<<grid(D, 256), 256, 0, st>>>(D, W.seed_start, W.seed_len, W.seed_open, W.fe, n_cid, n_key, k,
-                                                       foff, fb);
+        k_frag_write<K><<<grid(nfr, 256), 256, 0, st>>>(nfr, seed_of, W.seed_start, W.seed_len, W.seed_open, W.fe,
+                                                         n_cid, n_key, k, foff, fb);
     }
     CDBG_CHECK_LAUNCH();
-    uint64_t nfr = 0;
-    {
-        std::vector<uint32_t> dummy;
-        (void)dummy;
-        unsigned long long* fc = A.alloc<unsigned long long>(1);
-        CDBG_CUDA(cudaMemsetAsync(fc, 0, 8, st));
-        k_count_flags<<<grid(D, 256), 256, 0, st>>>(D, is_seed, fc);
-        CDBG_CHECK_LAUNCH();
-        nfr = read_dev(fc, st);
-    }
     const uint64_t seq_total = read_dev(seqt, st);
     out.n_fragments += nfr;
     out.total_seq_bytes += seq_total;
@@ -1859,15 +1882,16 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
         size_t fr = 0, tot = 0;
         CDBG_CUDA(cudaMemGetInfo(&fr, &tot));
         const uint64_t avail = (uint64_t)fr + A.cached_free();
-        // ~160 B of device memory per k-mer occurrence in the batch, worst
+        // ~200 B of device memory per k-mer occurrence in the batch, worst
         // case; keep 45% of the available memory for outputs and the dictionary
-        budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(avail * 0.55) / 160));
+        budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(avail * 0.55) / 200));
     }
     rec_view R{rs.start, rs.len, rs.flags, rs.col_off, rs.colors, rbucket, occ, rs.words};
-    class_dict dict;
+    phase2_state local_state;
+    phase2_state& S = out.state ? *out.state : local_state;
+    class_dict dict(S);
     dict.init(st);
-    dvec<uint8_t> local_frag;
-    dvec<uint8_t>& dfrag = out.d_frag_out ? *out.d_frag_out : local_frag;
+    dvec<uint8_t>& dfrag = S.frag;
     dfrag.n = 0;
     uint32_t b = 0;
     while (b < B) {
@@ -1897,16 +1921,10 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     CDBG_CUDA(cudaStreamSynchronize(st));
     A.release(mark);
     if (!p.to_host) {
-        // hand the dictionary's storage to the caller (no copies)
-        std::swap(out.d_words_out->p, dict.words.p);
-        std::swap(out.d_words_out->cap, dict.words.cap);
-        out.d_words_out->n = nwords;
-        std::swap(out.d_offsets_out->p, dict.bit_off.p);
-        std::swap(out.d_offsets_out->cap, dict.bit_off.cap);
-        out.d_offsets_out->n = dict.n;
-        out.d_frag = out.d_frag_out->p;
-        out.d_words = out.d_words_out->p;
-        out.d_offsets = out.d_offsets_out->p;
+        // outputs stay in the persistent state
+        out.d_frag = S.frag.p;
+        out.d_words = S.words.p;
+        out.d_offsets = S.bit_off.p;
     }
 }
 }  // namespace
@@ -1914,17 +1932,12 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
 void run_phase2(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStream_t st, uint32_t* d_err,
                 phase2_result& out) {
     {
-        // keep the caller's device output buffers across the reset
-        auto f = out.d_frag_out;
-        auto w = out.d_words_out;
-        auto o = out.d_offsets_out;
+        // keep the caller's persistent storage across the reset
+        phase2_state* S = out.state;
         out = phase2_result();
-        out.d_frag_out = f;
-        out.d_words_out = w;
-        out.d_offsets_out = o;
+        out.state = S;
     }
-    if (!p.to_host && !(out.d_frag_out && out.d_words_out && out.d_offsets_out))
-        throw std::runtime_error("device-resident phase-2 outputs need caller buffers");
+    if (!p.to_host && !out.state) throw std::runtime_error("device-resident phase-2 outputs need persistent storage");
     if (p.k < 2 || p.k > 63) throw std::runtime_error("k must be in [2, 63]");
     if (p.num_colors == 0) throw std::runtime_error("num_colors must be > 0");
     if (rs.n >= (1ull << 31)) throw std::runtime_error("more than 2^31 bucket records in one build");

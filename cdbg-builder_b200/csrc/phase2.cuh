@@ -11,6 +11,19 @@
 
 namespace cdbg {
 
+// Device storage that outlives one build (kept by the engine so repeated
+// builds reuse it): the color-class dictionary and the device-resident frag
+// bytes.  After a build with outputs left on the device, words/bit_off/frag
+// hold that build's .color_sets words, class offsets and frag spill.
+struct phase2_state {
+    dvec<uint64_t> cls_hash;   // per class: 64-bit set hash
+    dvec<uint64_t> bit_off;    // per class: bit offset (n + 1 entries)
+    dvec<uint64_t> words;      // encoded classes
+    dvec<uint64_t> slot_hash;  // open-addressing table hash -> class
+    dvec<uint32_t> slot_cid;
+    dvec<uint8_t> frag;        // frag spill bytes (device-resident builds)
+};
+
 // Outputs of phase 2, accumulated over bucket batches.
 struct phase2_result {
     // frag_unitigs.bin bytes (unitig_spill.hpp:642-665 record layout), in
@@ -26,11 +39,9 @@ struct phase2_result {
     uint64_t nbits = 0;
     uint64_t n_classes = 0;
     uint64_t total_integers = 0;
-    // device-resident outputs (when !to_host) are written into these
-    // caller-owned buffers, which outlive the arena
-    dvec<uint8_t>* d_frag_out = nullptr;
-    dvec<uint64_t>* d_words_out = nullptr;
-    dvec<uint64_t>* d_offsets_out = nullptr;
+    // persistent storage to use (required when !to_host: the device
+    // outputs live in it); null = temporary storage for this call
+    phase2_state* state = nullptr;
     // counters
     uint64_t n_occ = 0, n_distinct = 0, n_fragments = 0, total_seq_bytes = 0;
     uint64_t n_multi = 0;
