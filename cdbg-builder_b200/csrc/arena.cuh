@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -34,7 +36,8 @@ public:
     void* alloc_bytes(size_t bytes) {
         bytes = (bytes + 255) & ~size_t(255);
         if (bytes == 0) bytes = 256;
-        while (m_cur < m_chunks.size()) {
+        // 1. the current chunk
+        if (m_cur < m_chunks.size()) {
             chunk& c = m_chunks[m_cur];
             if (c.used + bytes <= c.size) {
                 void* p = static_cast<char*>(c.ptr) + c.used;
@@ -42,14 +45,43 @@ public:
                 track_();
                 return p;
             }
-            ++m_cur;
-            if (m_cur < m_chunks.size()) m_chunks[m_cur].used = 0;
         }
+        // 2. a later chunk that fits (every chunk after the current one is free);
+        //    move it right after the current one so no free chunk is skipped
+        const size_t next = m_chunks.empty() ? 0 : m_cur + 1;
+        for (size_t i = next; i < m_chunks.size(); ++i) {
+            if (m_chunks[i].size >= bytes) {
+                std::swap(m_chunks[i], m_chunks[next]);
+                m_cur = next;
+                m_chunks[m_cur].used = bytes;
+                track_();
+                return m_chunks[m_cur].ptr;
+            }
+        }
+        // 3. a new chunk; on failure give back the free chunks and retry exact
         size_t sz = bytes > m_chunk_bytes ? bytes : m_chunk_bytes;
         void* p = nullptr;
-        CDBG_CUDA(cudaMalloc(&p, sz));
-        m_chunks.push_back({p, sz, bytes});
-        m_cur = m_chunks.size() - 1;
+        cudaError_t e = cudaMalloc(&p, sz);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            while (m_chunks.size() > next) {
+                cudaFree(m_chunks.back().ptr);
+                m_chunks.pop_back();
+            }
+            sz = bytes;
+            e = cudaMalloc(&p, sz);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                size_t fr = 0, tot = 0;
+                cudaMemGetInfo(&fr, &tot);
+                throw std::runtime_error("device out of memory: request " + std::to_string(bytes >> 20) +
+                                         " MiB, free " + std::to_string(fr >> 20) + " MiB of " +
+                                         std::to_string(tot >> 20) + " MiB, arena holds " +
+                                         std::to_string(reserved_bytes() >> 20) + " MiB");
+            }
+        }
+        m_chunks.insert(m_chunks.begin() + next, chunk{p, sz, bytes});
+        m_cur = next;
         track_();
         return p;
     }
@@ -104,7 +136,7 @@ private:
     }
     std::vector<chunk> m_chunks;
     size_t m_cur = 0;
-    size_t m_chunk_bytes = size_t(1) << 30;
+    size_t m_chunk_bytes = size_t(4) << 30;
     size_t m_peak = 0;
 };
 

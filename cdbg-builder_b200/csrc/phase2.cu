@@ -38,6 +38,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "device_kmer.cuh"
@@ -110,13 +111,37 @@ __device__ __forceinline__ u128 key_load(u128 const* a) {
     return ((u128)v.y << 64) | (u128)v.x;
 }
 
+// One table slot: everything the load stage aggregates for a k-mer sits in
+// the same 32-byte sector (48 bytes for 128-bit k-mers), so an occurrence
+// touches one sector instead of one per field.
+template <typename K>
+struct slot_t;
+template <>
+struct alignas(32) slot_t<uint64_t> {
+    uint64_t key;
+    unsigned long long rank;  // first insertion (record << 32 | index)
+    uint32_t rmin, rmax;      // owned records: min / max id
+    uint32_t meta;            // boundary side bits, primary bit
+    uint32_t node;            // node index once numbered
+};
+template <>
+struct alignas(16) slot_t<u128> {
+    u128 key;
+    unsigned long long rank;
+    uint32_t rmin, rmax;
+    uint32_t meta;
+    uint32_t node;
+};
+static_assert(sizeof(slot_t<uint64_t>) == 32, "slot layout");
+static_assert(sizeof(slot_t<u128>) == 48, "slot layout");
+
 // Insert-or-find; returns the slot (absolute) or NONE64 when the region is full.
 template <typename K>
-__device__ __forceinline__ uint64_t table_upsert(K* keys, uint64_t off, uint64_t cap, K x) {
+__device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off, uint64_t cap, K x) {
     const K EMPTY = kmer_ops<K>::empty();
     uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
     for (uint64_t i = 0; i < cap; ++i) {
-        K* a = keys + off + s;
+        K* a = &slots[off + s].key;
         if (sizeof(K) == 8) {
             const K cur = key_load(a);
             if (cur == x) return off + s;
@@ -134,11 +159,11 @@ __device__ __forceinline__ uint64_t table_upsert(K* keys, uint64_t off, uint64_t
 }
 
 template <typename K>
-__device__ __forceinline__ uint64_t table_find(K const* keys, uint64_t off, uint64_t cap, K x) {
+__device__ __forceinline__ uint64_t table_find(slot_t<K> const* slots, uint64_t off, uint64_t cap, K x) {
     const K EMPTY = kmer_ops<K>::empty();
     uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
     for (uint64_t i = 0; i < cap; ++i) {
-        const K cur = key_load(keys + off + s);
+        const K cur = key_load(&slots[off + s].key);
         if (cur == x) return off + s;
         if (cur == EMPTY) return ~0ull;
         if (++s == cap) s = 0;
@@ -159,12 +184,7 @@ struct rec_view {
 
 template <typename K>
 struct tables {
-    K* key;
-    uint32_t* meta;
-    unsigned long long* rank;
-    uint32_t* rmin;
-    uint32_t* rmax;
-    uint32_t* node;
+    slot_t<K>* slots;
     uint64_t const* tab_off;  // per batch bucket
     uint64_t const* tab_cap;
     uint32_t b0;
@@ -180,12 +200,46 @@ struct occ_info {
     bool owned;
 };
 
+// Record holding occurrence o of the current block.  Every record has at least
+// one k-mer in practice, so the block's OCC_BLOCK occurrences fall within
+// OCC_BLOCK + 1 records starting at the record of its first occurrence: one
+// global binary search per block, then a search in shared memory.  Empty
+// records (len < k) can push an occurrence past the window; it then falls
+// back to the global search.
+constexpr int OCC_BLOCK = 256;
+struct occ_window {
+    uint64_t occ[OCC_BLOCK + 2];
+    uint64_t r0;
+};
+__device__ __forceinline__ void load_occ_window(occ_window& w, uint64_t const* occ, uint64_t R0, uint64_t nrec,
+                                                uint64_t o_first) {
+    if (threadIdx.x == 0) w.r0 = R0 + upper_bound_u64(occ + R0, nrec + 1, o_first) - 1;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < OCC_BLOCK + 2; i += blockDim.x) {
+        const uint64_t r = w.r0 + i;
+        w.occ[i] = (r <= R0 + nrec) ? occ[r] : ~0ull;
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ uint64_t window_record(occ_window const& w, uint64_t const* occ, uint64_t R0,
+                                                  uint64_t nrec, uint64_t o) {
+    if (o < w.occ[OCC_BLOCK + 1]) {
+        uint32_t lo = 0, hi = OCC_BLOCK + 2;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (w.occ[mid] <= o)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        return w.r0 + lo - 1;
+    }
+    return R0 + upper_bound_u64(occ + R0, nrec + 1, o) - 1;
+}
+
 template <typename K>
-__device__ __forceinline__ occ_info<K> decode_occ(rec_view const& R, uint64_t R0, uint64_t nrec,
-                                                  uint64_t o, uint32_t k) {
+__device__ __forceinline__ occ_info<K> decode_occ_r(rec_view const& R, uint64_t r, uint64_t o, uint32_t k) {
     occ_info<K> oi;
-    const uint32_t rr = upper_bound_u64(R.occ + R0, nrec + 1, o) - 1;
-    const uint64_t r = R0 + rr;
     oi.r = (uint32_t)r;
     oi.idx = (uint32_t)(o - R.occ[r]);
     const uint32_t nk = R.len[r] - k + 1;
@@ -226,26 +280,31 @@ __global__ void k_gather_u64(uint64_t n, uint64_t const* __restrict__ src,
 }
 
 template <typename K>
-__global__ void k_init_tables(uint64_t T, K* key, uint32_t* meta, unsigned long long* rank,
-                              uint32_t* rmin, uint32_t* rmax) {
+__global__ void k_init_tables(uint64_t T, slot_t<K>* slots) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= T) return;
-    key[i] = kmer_ops<K>::empty();
-    meta[i] = 0;
-    rank[i] = ~0ull;
-    rmin[i] = NONE32;
-    rmax[i] = 0;
+    slot_t<K> e;
+    e.key = kmer_ops<K>::empty();
+    e.rank = ~0ull;
+    e.rmin = NONE32;
+    e.rmax = 0;
+    e.meta = 0;
+    e.node = NONE32;
+    slots[i] = e;
 }
 
 template <typename K>
 __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_t R0, uint64_t nrec,
                                                 uint64_t O0, uint64_t nocc, uint32_t k,
                                                 uint32_t* __restrict__ occ_slot, uint32_t* err) {
+    __shared__ occ_window win;
+    load_occ_window(win, R.occ, R0, nrec, O0 + (uint64_t)blockIdx.x * OCC_BLOCK);
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nocc) return;
-    const occ_info<K> oi = decode_occ<K>(R, R0, nrec, O0 + t, k);
+    const uint64_t rec = window_record(win, R.occ, R0, nrec, O0 + t);
+    const occ_info<K> oi = decode_occ_r<K>(R, rec, O0 + t, k);
     const uint32_t tb = R.bucket[oi.r] - T.b0;
-    const uint64_t s = table_upsert<K>(T.key, T.tab_off[tb], T.tab_cap[tb], oi.can);
+    const uint64_t s = table_upsert<K>(T.slots, T.tab_off[tb], T.tab_cap[tb], oi.can);
     if (s == ~0ull) {
         set_error(err, ERR_TABLE_FULL);
         occ_slot[t] = NONE32;
@@ -254,22 +313,23 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     // slot of this occurrence, bit 31 = owned (read by k_multi_pairs)
     occ_slot[t] = (uint32_t)s | (oi.owned ? 0x80000000u : 0u);
     const uint32_t mo = oi.contrib | (oi.owned ? M_PRIMARY : 0u);
-    if (mo && (T.meta[s] & mo) != mo) atomicOr(&T.meta[s], mo);
+    slot_t<K>& e = T.slots[s];
+    if (mo && (e.meta & mo) != mo) atomicOr(&e.meta, mo);
     const unsigned long long rk = ((unsigned long long)oi.r << 32) | oi.idx;
-    if (rk < T.rank[s]) atomicMin(&T.rank[s], rk);
+    if (rk < e.rank) atomicMin(&e.rank, rk);
     if (oi.owned) {
-        if (oi.r < T.rmin[s]) atomicMin(&T.rmin[s], oi.r);
-        if (oi.r > T.rmax[s]) atomicMax(&T.rmax[s], oi.r);
+        if (oi.r < e.rmin) atomicMin(&e.rmin, oi.r);
+        if (oi.r > e.rmax) atomicMax(&e.rmax, oi.r);
     }
 }
 
 // Bit q of `bits` <- first occurrence of each distinct k-mer.
 template <typename K>
-__global__ void k_firstbits(uint64_t T, K const* __restrict__ key, unsigned long long const* __restrict__ rank,
-                            uint64_t const* __restrict__ occ, uint64_t O0, uint32_t* __restrict__ bits) {
+__global__ void k_firstbits(uint64_t T, slot_t<K> const* __restrict__ slots, uint64_t const* __restrict__ occ,
+                            uint64_t O0, uint32_t* __restrict__ bits) {
     uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= T || key[s] == kmer_ops<K>::empty()) return;
-    const unsigned long long rk = rank[s];
+    if (s >= T || slots[s].key == kmer_ops<K>::empty()) return;
+    const unsigned long long rk = slots[s].rank;
     const uint64_t q = occ[rk >> 32] + (rk & 0xffffffffull) - O0;
     atomicOr(&bits[q >> 5], 1u << (q & 31));
 }
@@ -280,25 +340,25 @@ __global__ void k_popc(uint64_t n, uint32_t const* __restrict__ bits, uint32_t* 
 }
 
 template <typename K>
-__global__ void k_make_nodes(uint64_t T, K const* __restrict__ key, uint32_t const* __restrict__ meta,
-                             unsigned long long const* __restrict__ rank, uint32_t const* __restrict__ rmin,
-                             uint32_t const* __restrict__ rmax, uint64_t const* __restrict__ occ, uint64_t O0,
+__global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, uint64_t const* __restrict__ occ, uint64_t O0,
                              uint32_t const* __restrict__ bits, uint64_t const* __restrict__ wpre,
-                             uint32_t const* __restrict__ rbucket, uint32_t* __restrict__ node_of_slot,
-                             K* __restrict__ n_key, uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
-                             uint32_t* __restrict__ n_bucket) {
+                             uint32_t const* __restrict__ rbucket, K* __restrict__ n_key, uint8_t* __restrict__ n_meta,
+                             uint32_t* __restrict__ n_rec, uint32_t* __restrict__ n_bucket,
+                             uint32_t* __restrict__ node_of_slot) {
     uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= T || key[s] == kmer_ops<K>::empty()) return;
-    const unsigned long long rk = rank[s];
+    if (s >= T) return;
+    slot_t<K> e = slots[s];
+    if (e.key == kmer_ops<K>::empty()) return;
+    const unsigned long long rk = e.rank;
     const uint64_t q = occ[rk >> 32] + (rk & 0xffffffffull) - O0;
     const uint32_t w = bits[q >> 5];
     const uint64_t n = wpre[q >> 5] + __popc(w & ((1u << (q & 31)) - 1u));
+    slots[s].node = (uint32_t)n;
     node_of_slot[s] = (uint32_t)n;
-    n_key[n] = key[s];
-    const uint32_t m = meta[s];
-    n_meta[n] = (uint8_t)m;
+    n_key[n] = e.key;
+    n_meta[n] = (uint8_t)e.meta;
     uint32_t rec = NONE32;
-    if (m & M_PRIMARY) rec = (rmin[s] == rmax[s]) ? rmin[s] : MULTI_TAG;
+    if (e.meta & M_PRIMARY) rec = (e.rmin == e.rmax) ? e.rmin : MULTI_TAG;
     n_rec[n] = rec;
     n_bucket[n] = rbucket[rk >> 32];
 }
@@ -308,20 +368,21 @@ __global__ void k_make_nodes(uint64_t T, K const* __restrict__ key, uint32_t con
 template <bool WRITE>
 __global__ void __launch_bounds__(256)
     k_multi_pairs(uint64_t const* __restrict__ occ, uint64_t R0, uint64_t nrec, uint64_t O0, uint64_t nocc,
-                  uint32_t const* __restrict__ occ_slot, uint32_t const* __restrict__ node,
+                  uint32_t const* __restrict__ occ_slot, uint32_t const* __restrict__ node_of_slot,
                   uint32_t const* __restrict__ n_rec, unsigned long long* __restrict__ cnt,
                   uint64_t* __restrict__ pairs) {
+    __shared__ occ_window win;
+    load_occ_window(win, occ, R0, nrec, O0 + (uint64_t)blockIdx.x * OCC_BLOCK);
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool emit = false;
     uint64_t val = 0;
     if (t < nocc) {
         const uint32_t v = occ_slot[t];
         if (v != NONE32 && (v & 0x80000000u)) {
-            const uint32_t n = node[v & 0x7fffffffu];
+            const uint32_t n = node_of_slot[v & 0x7fffffffu];
             if (n_rec[n] == MULTI_TAG) {
-                const uint32_t rr = upper_bound_u64(occ + R0, nrec + 1, O0 + t) - 1;
                 emit = true;
-                val = ((uint64_t)n << 32) | (uint32_t)(R0 + rr);
+                val = ((uint64_t)n << 32) | (uint32_t)window_record(win, occ, R0, nrec, O0 + t);
             }
         }
     }
@@ -450,6 +511,89 @@ __global__ void k_union(uint64_t M, uint64_t const* __restrict__ moff, uint64_t 
     }
 }
 
+// ---- multi-record unions as bitmaps -----------------------------------------
+constexpr uint32_t HEAVY_COLORS = 64;  // records with at least this many colors get a bitmap
+
+__global__ void k_heavy_flags(uint64_t nu, uint64_t const* __restrict__ upairs, uint64_t const* __restrict__ col_off,
+                              uint32_t R0, uint32_t* __restrict__ flag) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nu) return;
+    const uint32_t r = (uint32_t)(upairs[i] & 0xffffffffu);
+    if (col_off[r + 1] - col_off[r] >= HEAVY_COLORS) flag[r - R0] = 1u;
+}
+
+// Warp per heavy record: its colors as a bitmap in rbits[hpos[r - R0] * nw].
+__global__ void k_heavy_bitmaps(uint64_t nrec, uint32_t const* __restrict__ flag, uint64_t const* __restrict__ hpos,
+                                uint32_t R0, uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors,
+                                uint32_t nw, uint32_t* __restrict__ rbits) {
+    extern __shared__ uint32_t smem_bm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* bm = smem_bm + (size_t)wib * nw;
+    const uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (i >= nrec || !flag[i]) return;
+    for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
+    __syncwarp();
+    const uint64_t c0 = col_off[R0 + i], c1 = col_off[R0 + i + 1];
+    for (uint64_t c = c0 + lane; c < c1; c += 32) {
+        const uint32_t v = colors[c];
+        atomicOr(&bm[v >> 5], 1u << (v & 31));
+    }
+    __syncwarp();
+    uint32_t* out = rbits + hpos[i] * (uint64_t)nw;
+    for (uint32_t w = lane; w < nw; w += 32) out[w] = bm[w];
+}
+
+// Warp per multi-record node: OR of its records' color sets (bitmap words for
+// heavy records, per-color bits for the rest) -> mbits, size, set hash.
+__global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ moff, uint64_t const* __restrict__ upairs,
+                           uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors, uint32_t R0,
+                           uint32_t const* __restrict__ hflag, uint64_t const* __restrict__ hpos,
+                           uint32_t const* __restrict__ rbits, uint32_t nw, uint32_t* __restrict__ mbits,
+                           uint32_t* __restrict__ msize, uint64_t* __restrict__ mhash) {
+    extern __shared__ uint32_t smem_bm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* bm = smem_bm + (size_t)wib * nw;
+    const uint64_t m = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (m >= M) return;
+    for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
+    __syncwarp();
+    for (uint64_t p = moff[m]; p < moff[m + 1]; ++p) {
+        const uint32_t r = (uint32_t)(upairs[p] & 0xffffffffu);
+        if (hflag[r - R0]) {
+            uint32_t const* rb = rbits + hpos[r - R0] * (uint64_t)nw;
+            for (uint32_t w = lane; w < nw; w += 32) bm[w] |= rb[w];  // lanes own distinct words
+        } else {
+            __syncwarp();
+            const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
+            for (uint64_t c = c0 + lane; c < c1; c += 32) {
+                const uint32_t v = colors[c];
+                atomicOr(&bm[v >> 5], 1u << (v & 31));
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    uint32_t cnt = 0;
+    uint64_t acc = 0;
+    uint32_t* out = mbits + m * (uint64_t)nw;
+    for (uint32_t w = lane; w < nw; w += 32) {
+        uint32_t x = bm[w];
+        out[w] = x;
+        cnt += __popc(x);
+        while (x) {
+            const uint32_t b = __ffs(x) - 1;
+            x &= x - 1;
+            acc += elem_mix(w * 32 + b);
+        }
+    }
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    acc = warp_sum64(acc);
+    if (lane == 0) {
+        msize[m] = cnt;
+        mhash[m] = set_hash_final(acc, cnt);
+    }
+}
+
 // rec_first[r] = smallest node index whose color set is record r's list.
 __global__ void k_rec_first(uint64_t D, uint32_t const* __restrict__ n_rec, uint32_t R0,
                             uint32_t* __restrict__ rec_first) {
@@ -491,19 +635,63 @@ __global__ void k_cand_multi(uint64_t M, uint64_t base, uint32_t const* __restri
 struct list_src {
     uint64_t const* col_off;
     uint32_t const* colors;
-    uint64_t const* poff;
+    uint64_t const* poff;   // list mode: multi-node unions as ascending lists
     uint32_t const* pool;
     uint32_t const* msize;
+    uint32_t const* mbits;  // bitmap mode: multi-node unions as C-bit bitmaps
+    uint32_t nw;            // 32-bit words per bitmap
 };
 __device__ __forceinline__ void cand_list(list_src const& L, uint32_t kind_id, uint32_t const*& p, uint64_t& n) {
     if (kind_id & MULTI_TAG) {
         const uint32_t m = kind_id & ~MULTI_TAG;
-        p = L.pool + L.poff[m];
+        p = L.pool ? L.pool + L.poff[m] : nullptr;
         n = L.msize[m];
     } else {
         p = L.colors + L.col_off[kind_id];
         n = L.col_off[kind_id + 1] - L.col_off[kind_id];
     }
+}
+
+// A candidate color set: an ascending list, or a bitmap (multi-node unions
+// in bitmap mode), with its size.
+struct cand_set {
+    uint32_t const* list;
+    uint32_t const* bm;
+    uint64_t n;
+};
+__device__ __forceinline__ cand_set cand_get(list_src const& L, uint32_t kind_id) {
+    cand_set c;
+    c.bm = nullptr;
+    if ((kind_id & MULTI_TAG) && L.mbits) {
+        const uint32_t m = kind_id & ~MULTI_TAG;
+        c.list = nullptr;
+        c.bm = L.mbits + (uint64_t)m * L.nw;
+        c.n = L.msize[m];
+        return c;
+    }
+    cand_list(L, kind_id, c.list, c.n);
+    return c;
+}
+__device__ __forceinline__ bool sets_equal(cand_set const& a, cand_set const& b, uint32_t nw) {
+    if (a.n != b.n) return false;
+    if (a.bm && b.bm) {
+        for (uint32_t w = 0; w < nw; ++w)
+            if (a.bm[w] != b.bm[w]) return false;
+        return true;
+    }
+    if (!a.bm && !b.bm) {
+        for (uint64_t i = 0; i < a.n; ++i)
+            if (a.list[i] != b.list[i]) return false;
+        return true;
+    }
+    // list against bitmap of the same size: equal iff every element is set
+    const cand_set& l = a.bm ? b : a;
+    const cand_set& m = a.bm ? a : b;
+    for (uint64_t i = 0; i < l.n; ++i) {
+        const uint32_t v = l.list[i];
+        if (!((m.bm[v >> 5] >> (v & 31)) & 1u)) return false;
+    }
+    return true;
 }
 
 // ---- bit ranges -------------------------------------------------------------
@@ -569,14 +757,17 @@ __global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint
     uint32_t* bm = smem_bm + (size_t)wib * nw;
     const uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
     if (j >= nc) return;
-    uint32_t const* lp;
-    uint64_t N;
-    cand_list(L, cv.kind_id[j], lp, N);
-    for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
-    __syncwarp();
-    for (uint64_t i = lane; i < N; i += 32) {
-        const uint32_t v = lp[i];
-        atomicOr(&bm[v >> 5], 1u << (v & 31));
+    const cand_set cs = cand_get(L, cv.kind_id[j]);
+    const uint64_t N = cs.n;
+    if (cs.bm) {
+        for (uint32_t w = lane; w < nw; w += 32) bm[w] = cs.bm[w];
+    } else {
+        for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
+        __syncwarp();
+        for (uint64_t i = lane; i < N; i += 32) {
+            const uint32_t v = cs.list[i];
+            atomicOr(&bm[v >> 5], 1u << (v & 31));
+        }
     }
     __syncwarp();
     const uint64_t sparse_t = (uint64_t)(0.25 * (double)C);
@@ -834,11 +1025,7 @@ __global__ void k_member_match_raw(uint64_t n, uint32_t const* __restrict__ head
         atomicMin(&rep_first[c], cv.first[c]);
         return;
     }
-    uint32_t const *pc, *ph;
-    uint64_t nc, nh;
-    cand_list(L, cv.kind_id[c], pc, nc);
-    cand_list(L, cv.kind_id[h], ph, nh);
-    if (lists_equal(pc, nc, ph, nh)) {
+    if (sets_equal(cand_get(L, cv.kind_id[c]), cand_get(L, cv.kind_id[h]), L.nw)) {
         rep[c] = h;
         atomicMin(&rep_first[h], cv.first[c]);
     } else {
@@ -857,17 +1044,12 @@ __global__ void k_group_collided_raw(uint64_t nruns, uint32_t const* __restrict_
     const uint64_t e = (r + 1 < nruns) ? run_start[r + 1] : n;
     for (uint64_t j = i; j < e; ++j) {
         const uint32_t cj = nidx[j];
-        uint32_t const* pj;
-        uint64_t lj;
-        cand_list(L, cv.kind_id[cj], pj, lj);
+        const cand_set sj = cand_get(L, cv.kind_id[cj]);
         uint32_t rr = cj;
         for (uint64_t q = i; q < j; ++q) {
             const uint32_t cq = nidx[q];
             if (rep[cq] != cq) continue;
-            uint32_t const* pq;
-            uint64_t lq;
-            cand_list(L, cv.kind_id[cq], pq, lq);
-            if (lists_equal(pj, lj, pq, lq)) {
+            if (sets_equal(sj, cand_get(L, cv.kind_id[cq]), L.nw)) {
                 rr = cq;
                 break;
             }
@@ -958,8 +1140,8 @@ __global__ void k_node_cid(uint64_t D, uint32_t const* __restrict__ n_rec, uint3
 // ---- extension masks and clean links -------------------------------------
 template <typename K>
 __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb, K x) {
-    const uint64_t s = table_find<K>(T.key, T.tab_off[tb], T.tab_cap[tb], x);
-    return s == ~0ull ? NONE32 : T.node[s];
+    const uint64_t s = table_find<K>(T.slots, T.tab_off[tb], T.tab_cap[tb], x);
+    return s == ~0ull ? NONE32 : T.slots[s].node;
 }
 
 template <typename K>
@@ -1464,18 +1646,13 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemcpyAsync(d_toff, toff.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
     CDBG_CUDA(cudaMemcpyAsync(d_tcap, tcap.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
     tables<K> TB;
-    TB.key = A.alloc<K>(T);
-    TB.meta = A.alloc<uint32_t>(T);
-    TB.rank = A.alloc<unsigned long long>(T);
-    TB.rmin = A.alloc<uint32_t>(T);
-    TB.rmax = A.alloc<uint32_t>(T);
-    TB.node = A.alloc<uint32_t>(T);
+    TB.slots = A.alloc<slot_t<K>>(T);
     TB.tab_off = d_toff;
     TB.tab_cap = d_tcap;
     TB.b0 = b0;
     {
         CDBG_PROF("k_init_tables", st);
-        k_init_tables<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax);
+        k_init_tables<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots);
     }
     CDBG_CHECK_LAUNCH();
     // ---- load
@@ -1490,7 +1667,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(bits, 0, 4 * nwb, st));
     {
         CDBG_PROF("k_firstbits", st);
-        k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.rank, R.occ, O0, bits);
+        k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, R.occ, O0, bits);
     }
     CDBG_CHECK_LAUNCH();
     uint32_t* wcnt = A.alloc<uint32_t>(nwb);
@@ -1501,14 +1678,15 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     const uint64_t D = read_dev(wpre + nwb, st);
     if (D >= (1ull << 31)) throw std::runtime_error("too many distinct k-mers in one bucket batch");
     check_device_error_word(d_err, st, "k-mer table insert");
+    uint32_t* node_of_slot = A.alloc<uint32_t>(T);
     K* n_key = A.alloc<K>(D);
     uint8_t* n_meta = A.alloc<uint8_t>(D);
     uint32_t* n_rec = A.alloc<uint32_t>(D);
     uint32_t* n_bucket = A.alloc<uint32_t>(D);
     {
         CDBG_PROF("k_make_nodes", st);
-        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.key, TB.meta, TB.rank, TB.rmin, TB.rmax, R.occ, O0, bits,
-                                                       wpre, R.bucket, TB.node, n_key, n_meta, n_rec, n_bucket);
+        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, R.occ, O0, bits, wpre, R.bucket, n_key, n_meta,
+                                                       n_rec, n_bucket, node_of_slot);
     }
     CDBG_CHECK_LAUNCH();
     // ---- multi-record k-mers
@@ -1516,7 +1694,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
     {
         CDBG_PROF("k_multi_pairs", st);
-        k_multi_pairs<false><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, TB.node, n_rec, cnt,
+        k_multi_pairs<false><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, node_of_slot, n_rec, cnt,
                                                               nullptr);
     }
     CDBG_CHECK_LAUNCH();
@@ -1529,12 +1707,13 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint64_t* mhash = nullptr;
     uint64_t* poff = nullptr;
     uint32_t* pool = nullptr;
+    uint32_t* mbits = nullptr;
     if (npairs) {
         uint64_t* pairs = A.alloc<uint64_t>(npairs);
         CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
         {
             CDBG_PROF("k_multi_pairs", st);
-            k_multi_pairs<true><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, TB.node, n_rec,
+            k_multi_pairs<true><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, node_of_slot, n_rec,
                                                                  cnt, pairs);
         }
         CDBG_CHECK_LAUNCH();
@@ -1566,26 +1745,55 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         const uint32_t nw = (C + 31) / 32;
         int wpb = (int)std::max<uint64_t>(1, std::min<uint64_t>(8, (96 * 1024) / (4ull * nw)));
         const size_t shm = (size_t)wpb * nw * 4;
-        if (shm > 48 * 1024) {
-            CDBG_CUDA(cudaFuncSetAttribute(k_union<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-            CDBG_CUDA(cudaFuncSetAttribute(k_union<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        if (p.union_bitmaps) {
+            // heavy records (>= 64 colors) used by multi-record nodes get a bitmap once
+            uint32_t* hflag = A.alloc<uint32_t>(nrec);
+            uint64_t* hpos = A.alloc<uint64_t>(nrec + 1);
+            CDBG_CUDA(cudaMemsetAsync(hflag, 0, 4 * nrec, st));
+            k_heavy_flags<<<grid(nu, 256), 256, 0, st>>>(nu, upairs, R.col_off, (uint32_t)R0, hflag);
+            CDBG_CHECK_LAUNCH();
+            prim::exclusive_scan<uint32_t, uint64_t>(hflag, hpos, nrec, A, st, hpos + nrec);
+            const uint64_t nheavy = read_dev(hpos + nrec, st);
+            uint32_t* rbits = A.alloc<uint32_t>(nheavy * nw + 1);
+            if (shm > 48 * 1024) {
+                CDBG_CUDA(cudaFuncSetAttribute(k_heavy_bitmaps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+                CDBG_CUDA(cudaFuncSetAttribute(k_union_bm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+            }
+            if (nheavy) {
+                CDBG_PROF("k_heavy_bitmaps", st);
+                k_heavy_bitmaps<<<grid(nrec, wpb), wpb * 32, shm, st>>>(nrec, hflag, hpos, (uint32_t)R0, R.col_off,
+                                                                        R.colors, nw, rbits);
+            }
+            CDBG_CHECK_LAUNCH();
+            mbits = A.alloc<uint32_t>(M * nw + 1);
+            {
+                CDBG_PROF("k_union", st);
+                k_union_bm<<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, (uint32_t)R0,
+                                                                 hflag, hpos, rbits, nw, mbits, msize, mhash);
+            }
+            CDBG_CHECK_LAUNCH();
+        } else {
+            if (shm > 48 * 1024) {
+                CDBG_CUDA(cudaFuncSetAttribute(k_union<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+                CDBG_CUDA(cudaFuncSetAttribute(k_union<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+            }
+            {
+                CDBG_PROF("k_union", st);
+                k_union<false><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize,
+                                                                     mhash, nullptr, nullptr);
+            }
+            CDBG_CHECK_LAUNCH();
+            poff = A.alloc<uint64_t>(M + 1);
+            prim::exclusive_scan<uint32_t, uint64_t>(msize, poff, M, A, st, poff + M);
+            const uint64_t ptot = read_dev(poff + M, st);
+            pool = A.alloc<uint32_t>(ptot + 1);
+            {
+                CDBG_PROF("k_union", st);
+                k_union<true><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize,
+                                                                    mhash, poff, pool);
+            }
+            CDBG_CHECK_LAUNCH();
         }
-        {
-            CDBG_PROF("k_union", st);
-            k_union<false><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
-                                                                 nullptr, nullptr);
-        }
-        CDBG_CHECK_LAUNCH();
-        poff = A.alloc<uint64_t>(M + 1);
-        prim::exclusive_scan<uint32_t, uint64_t>(msize, poff, M, A, st, poff + M);
-        const uint64_t ptot = read_dev(poff + M, st);
-        pool = A.alloc<uint32_t>(ptot + 1);
-        {
-            CDBG_PROF("k_union", st);
-            k_union<true><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize, mhash,
-                                                                poff, pool);
-        }
-        CDBG_CHECK_LAUNCH();
     }
     out.n_multi += M;
     // ---- candidates: used records, then multi nodes
@@ -1614,7 +1822,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         k_cand_multi<<<grid(M, 256), 256, 0, st>>>(M, nrc, mnode, mhash, cv);
         CDBG_CHECK_LAUNCH();
     }
-    list_src L{R.col_off, R.colors, poff, pool, msize};
+    list_src L{R.col_off, R.colors, poff, pool, msize, mbits, (C + 31) / 32};
     uint32_t* cid = A.alloc<uint32_t>(nc + 1);
     if (nc) {
         // 1. group candidates with equal color sets (sort by set hash, then
@@ -1884,7 +2092,7 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
         const uint64_t avail = (uint64_t)fr + A.cached_free();
         // ~200 B of device memory per k-mer occurrence in the batch, worst
         // case; keep 45% of the available memory for outputs and the dictionary
-        budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(avail * 0.55) / 200));
+        budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(avail * 0.5) / 220));
     }
     rec_view R{rs.start, rs.len, rs.flags, rs.col_off, rs.colors, rbucket, occ, rs.words};
     phase2_state local_state;
@@ -1941,10 +2149,15 @@ void run_phase2(record_set const& rs, phase2_params const& p, dev_arena& A, cuda
     if (p.k < 2 || p.k > 63) throw std::runtime_error("k must be in [2, 63]");
     if (p.num_colors == 0) throw std::runtime_error("num_colors must be > 0");
     if (rs.n >= (1ull << 31)) throw std::runtime_error("more than 2^31 bucket records in one build");
-    if (p.k <= 31)
-        run_all<uint64_t>(rs, p, A, st, d_err, out);
+    phase2_params q = p;
+    // bitmaps cost C/8 bytes per multi-record k-mer: lists above 8192 colors;
+    // CDBG_UNION_LISTS=1 forces the list path (tests cover both)
+    char const* env = std::getenv("CDBG_UNION_LISTS");
+    if (q.num_colors > 8192 || (env && env[0] == '1')) q.union_bitmaps = false;
+    if (q.k <= 31)
+        run_all<uint64_t>(rs, q, A, st, d_err, out);
     else
-        run_all<u128>(rs, p, A, st, d_err, out);
+        run_all<u128>(rs, q, A, st, d_err, out);
 }
 
 }  // namespace cdbg

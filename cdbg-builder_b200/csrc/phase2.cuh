@@ -53,6 +53,9 @@ struct phase2_params {
     uint32_t num_colors = 0;
     uint64_t batch_occ = 0;   // k-mer occurrences per batch (0 = auto)
     bool to_host = true;      // copy outputs to host vectors
+    // multi-record color unions as C-bit bitmaps (else as lists; bitmaps cost
+    // C/8 bytes per such k-mer, so very large color counts use lists)
+    bool union_bitmaps = true;
 };
 
 // Run phase 2 over all buckets of `rs` (records grouped by bucket).

@@ -109,3 +109,16 @@ def test_device_resident_outputs_match_host_outputs(engine, tmp_path):
         assert engine.copy_out(rd.frag_bytes, rd.frag_nbytes) == frag
         assert engine.copy_out(rd.class_words, len(words)) == words
         assert engine.copy_out(rd.class_offsets, len(offs)) == offs
+
+
+def test_union_list_path_matches_bitmap_path(engine, tmp_path, monkeypatch):
+    """Multi-record color unions as lists (used above 8192 colors) give the
+    same bytes as the bitmap path."""
+    lst = _fresh(tmp_path, 31, 8)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    hs = native.HostSequences(files)
+    r = engine.build(hs.batch, 31, 128, 8)
+    a = (native.result_frag_bytes(r), native.result_class_words(r).tobytes())
+    monkeypatch.setenv("CDBG_UNION_LISTS", "1")
+    r2 = engine.build(hs.batch, 31, 128, 8)
+    assert (native.result_frag_bytes(r2), native.result_class_words(r2).tobytes()) == a
