@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="pangenome")
     ap.add_argument("--genomes", type=int, default=0, help="override genome count (0 = workload's)")
-    ap.add_argument("--cpu-sample-genomes", type=int, default=24)
+    ap.add_argument("--cpu-sample-genomes", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch-occ", type=int, default=0)
@@ -138,6 +138,11 @@ def run_reference_sample(genomes, k, blog2, threads, seed, workdir):
     return kmers, t1 + t2, {"bucket_write_s": t1, "bucket_process_s": t2}
 
 
+def workload_name(n_genomes, k, B):
+    return ("pangenome: %d genomes x 4.8 Mbp (0.1-2%% SNPs, 1-200 contigs), k=%d, m=12, %d buckets"
+            % (n_genomes, k, B))
+
+
 def reference_arm(a):
     rank, _, world = dist_env()
     if rank != 0:
@@ -166,8 +171,8 @@ def reference_arm(a):
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1000 * statistics.median(secs), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "pangenome: 1000 genomes x 4.8 Mbp, k=31, m=12, -b 12 (sampled)",
-                       "sample": sample},
+            "config": {"workload": workload_name(1000, k, 1 << blog2), "sample": sample,
+                       "parallelism": "reference cdbg-build -t %d" % threads},
             "cpu_baseline": {"value": v, "unit": "k-mers/s", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": v, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -274,21 +279,29 @@ def main_gpu(a):
         e2e = {"value": world * kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
                "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes)}
 
-    # ---- roofline for the dominant kernel
+    # ---- roofline: the dominant kernel with an algorithmic-bytes figure, and
+    # the whole phase-1 + phase-2 path
     peak, peak_kind = peaks()
-    dom = max(kstats.items(), key=lambda kv: kv[1][0]) if kstats else None
+    w = 8 if k <= 31 else 16
     roof = None
-    if dom:
-        name, (tot_ms, nl) = dom
-        w = 8 if k <= 31 else 16
-        per_launch_ms = tot_ms / nl
-        # algorithmic bytes per launch (DESIGN.md "roofline accounting")
+    for name, (tot_ms, nl) in sorted(kstats.items(), key=lambda kv: -kv[1][0]):
         alg = algorithmic_bytes(name, r, w, a.steps, nl)
-        ach = alg / (per_launch_ms / 1000.0) / 1e9 if alg else None
+        if alg is None:
+            continue
+        per_launch_ms = tot_ms / nl
+        ach = alg / (per_launch_ms / 1000.0) / 1e9
+        tr = TRAFFIC_PER_UNIT.get(name)
         roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": (ach / peak) if ach else None, "traffic": None, "peak_kind": peak_kind,
-                "ms_per_launch": per_launch_ms, "launches_per_step": nl / a.steps,
-                "share_of_step": tot_ms / (ms * a.steps)}
+                "frac": ach / peak, "traffic": (tr[0] * units(name, r) * a.steps / nl) if tr else None,
+                "traffic_source": tr[1] if tr else None, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
+                "launches_per_step": nl / a.steps, "share_of_step": tot_ms / (ms * a.steps)}
+        break
+    path_bytes = path_algorithmic_bytes(r, w)
+    path_ach = path_bytes / (ms / 1000.0) / 1e9
+    if roof is not None:
+        roof["path"] = {"bytes_per_step": path_bytes, "achieved": path_ach, "frac": path_ach / peak,
+                        "formula": "Nb/4 + 2*record_bytes + 2*Nocc*(w+4) + D*(w+8) + frag_bytes"}
 
     # ---- CPU baseline (reference, bounded sample), rank 0 at N = 1
     cpu = None
@@ -303,12 +316,11 @@ def main_gpu(a):
             shutil.rmtree(work, ignore_errors=True)
 
     if rank == 0:
-        top = sorted(kstats.items(), key=lambda kv: -kv[1][0])[:12]
+        top = sorted(kstats.items(), key=lambda kv: -kv[1][0])[:20]
         line = {"metric": "phase1+2 k-mers/s", "value": value, "unit": "k-mers/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-                "config": {"workload": "pangenome: %d genomes x 4.8 Mbp (0.1-2%% SNPs, 1-200 contigs), "
-                                       "k=%d, m=12, %d buckets, phase1+2 in HBM" % (n_genomes, k, B),
+                "config": {"workload": workload_name(n_genomes, k, B),
                            "kmers_per_step": kmers, "bases": int(seq.nbytes),
                            "l2": "inputs (%.1f GB) larger than L2" % (seq.nbytes / 1e9),
                            "parallelism": "replicas%d" % world, "generate_s": gen_s},
@@ -330,22 +342,59 @@ def main_gpu(a):
     return 0
 
 
-def algorithmic_bytes(name, r, w, steps, launches):
-    """Algorithmic bytes of one launch of `name` (per-unit figures x units)."""
-    per_step = {
-        # phase 2 load: each k-mer occurrence read once (w + 4 B as a (k-mer, record) pair)
-        # and each distinct k-mer written once (w + 8 B: key + flags/rank/cid)
-        "k_insert": r.n_occ * (w + 4) + r.n_distinct * (w + 8),
-        "k_multi_pairs": r.n_occ * (w + 4),
-        "k_ext_mask": r.n_distinct * (w + 1),
-        "k_links": r.n_distinct * (w + 9),
-        "k_minimizers": r.n_kmers / 4.0 + r.n_supers * 16,
-        "k_rs_downsweep": 0,
+# Algorithmic bytes per unit of each kernel (the unit is the count named in
+# units()); probes, extra radix passes and re-reads are overhead, not counted.
+def _per_unit(w):
+    return {
+        # 2-bit stream read once (1/4 B per base) + one super-k-mer entry written
+        # (start 8, len 4, color 4, flags 4, bucket 4) per super-k-mer
+        "k_minimizers": None,  # two units, see algorithmic_bytes
+        # one (k-mer, record) read per occurrence + one table entry per distinct k-mer
+        "k_insert": None,
+        "k_multi_pairs": ("occ", 4 + 4),          # occurrence slot read + pair written
+        "k_ext_mask": ("distinct", w + 4 + 1),    # key + bucket read, mask written
+        "k_links": ("distinct", w + 4 + 1 + 8),   # key + bucket + mask read, two links written
+        "k_chain_paths": ("distinct", 8 + 1 + 1 + 4),  # links + flags + mask read, fragment element written
+        "k_frag_write": ("frag_bytes", 1),        # fragment records written
     }
-    v = per_step.get(name)
-    if v is None or v == 0:
-        return None
+
+
+def units(name, r):
+    u = {"occ": r.n_occ, "distinct": r.n_distinct, "frag_bytes": r.frag_nbytes,
+         "supers": r.n_supers, "bases": r.n_bases}
+    kind = {"k_minimizers": "bases", "k_insert": "occ"}.get(name)
+    if kind is None:
+        kind = _per_unit(8)[name][0]
+    return u[kind]
+
+
+def algorithmic_bytes(name, r, w, steps, launches):
+    """Algorithmic bytes of one launch of `name` (per-unit figure x units)."""
+    if name == "k_minimizers":
+        v = r.n_bases / 4.0 + r.n_supers * 24
+    elif name == "k_insert":
+        v = r.n_occ * (w + 4) + r.n_distinct * (w + 8)
+    else:
+        pu = _per_unit(w).get(name)
+        if pu is None:
+            return None
+        v = units(name, r) * pu[1]
     return v * steps / launches
+
+
+def path_algorithmic_bytes(r, w):
+    """Algorithmic bytes of one phase-1 + phase-2 pass: 2-bit input read, bucket
+    records written and read back, one write + one read of every (k-mer,
+    record) occurrence pair, one distinct k-mer table entry (key + cid + flags)
+    and the fragment bytes written."""
+    return (r.n_bases / 4.0 + 2 * r.record_bytes + 2 * r.n_occ * (w + 4) + r.n_distinct * (w + 8)
+            + r.frag_nbytes)
+
+
+# DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
+# of one capture, divided by the units that launch processed) and the summary
+# under profiles/ it comes from.
+TRAFFIC_PER_UNIT = {}
 
 
 if __name__ == "__main__":

@@ -81,6 +81,7 @@ class BuildResult(ctypes.Structure):
                 ("n_occ", ctypes.c_uint64), ("n_distinct", ctypes.c_uint64),
                 ("n_fragments", ctypes.c_uint64), ("total_seq_bytes", ctypes.c_uint64),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+                ("n_bases", ctypes.c_uint64), ("record_bytes", ctypes.c_uint64),
                 ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
                 ("ms_total", ctypes.c_double)]
 

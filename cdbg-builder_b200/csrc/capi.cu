@@ -555,8 +555,10 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err);
         cdbg::record_set rs;
         cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
+        unsigned long long* d_rec_bytes = e->P.alloc<unsigned long long>(1);
+        cdbg::record_bytes_async(rs, d_rec_bytes, e->st);
         cdbg::check_device_error(e, "phase 1");
-        const uint64_t n_kmers = rt.n_kmers, n_supers = sl.n;
+        const uint64_t n_kmers = rt.n_kmers, n_supers = sl.n, n_bases = rt.n_bases;
         e->A.reset();  // phase-1 scratch (staged input, super-k-mers, sort buffers)
         CDBG_CUDA(cudaEventRecord(ev[1], e->st));
         cdbg::phase2_params pp;
@@ -587,7 +589,10 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
             res.class_offsets = out.d_offsets;
         }
         CDBG_CUDA(cudaEventRecord(ev[2], e->st));
+        unsigned long long rec_bytes = 0;
+        CDBG_CUDA(cudaMemcpyAsync(&rec_bytes, d_rec_bytes, sizeof rec_bytes, cudaMemcpyDeviceToHost, e->st));
         CDBG_CUDA(cudaEventSynchronize(ev[2]));
+        CDBG_CUDA(cudaStreamSynchronize(e->st));
         float ms1 = 0, ms2 = 0;
         CDBG_CUDA(cudaEventElapsedTime(&ms1, ev[0], ev[1]));
         CDBG_CUDA(cudaEventElapsedTime(&ms2, ev[1], ev[2]));
@@ -597,6 +602,8 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         res.ms_total = ms1 + ms2;
         res.n_kmers = n_kmers;
         res.n_supers = n_supers;
+        res.n_bases = n_bases;
+        res.record_bytes = rec_bytes;
         res.n_records = rs.n;
         res.n_occ = out.n_occ;
         res.n_distinct = out.n_distinct;

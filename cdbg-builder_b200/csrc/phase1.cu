@@ -876,6 +876,39 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     prim::exclusive_scan<unsigned long long, uint64_t>(bc, rs.bucket_start, B, A, st, rs.bucket_start + B);
 }
 
+// Serialized size of every record summed into *sum (the uncompressed bytes
+// the bucket files would hold); same per-record arithmetic as k_rec_sizes.
+__global__ void k_rec_bytes_sum(uint64_t n, uint64_t const* __restrict__ coloff,
+                                uint32_t const* __restrict__ colors, uint32_t const* __restrict__ len,
+                                uint32_t const* __restrict__ flags, unsigned long long* __restrict__ sum) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long s = 0;
+    if (r < n) {
+        const uint64_t c0 = coloff[r], c1 = coloff[r + 1];
+        s = varint_len(c1 - c0);
+        uint32_t prev = 0;
+        for (uint64_t c = c0; c < c1; ++c) {
+            s += varint_len(colors[c] - prev);
+            prev = colors[c];
+        }
+        s += varint_len(((uint64_t)len[r] << 4) | (flags[r] & 0xfu));
+        s += (len[r] + 3) / 4;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(sum, s);
+}
+
+void record_bytes_async(record_set const& rs, unsigned long long* d_sum, cudaStream_t st) {
+    CDBG_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), st));
+    if (rs.n == 0) return;
+    {
+        CDBG_PROF("k_rec_bytes_sum", st);
+        k_rec_bytes_sum<<<grid(rs.n, 256), 256, 0, st>>>(rs.n, rs.col_off, rs.colors, rs.len, rs.flags, d_sum);
+    }
+    CDBG_CHECK_LAUNCH();
+}
+
 void serialize_records(record_set const& rs, dev_arena& A, cudaStream_t st, serialized_buckets& out) {
     out = serialized_buckets();
     out.rec_off = A.alloc<uint64_t>(rs.n + 1);

@@ -85,6 +85,10 @@ struct serialized_buckets {
 };
 void serialize_records(record_set const& rs, dev_arena& A, cudaStream_t st, serialized_buckets& out);
 
+// Sum of the serialized sizes of all records (reference record layout) into
+// the device word *d_sum, without synchronizing.
+void record_bytes_async(record_set const& rs, unsigned long long* d_sum, cudaStream_t st);
+
 // Parse serialized bucket bytes (device, 8-byte aligned, padded) into a
 // record_set.  chunk_off[nchunks + 1] are byte offsets where a record starts
 // (bucket and LZ4-frame starts); chunk_bucket[nchunks] the bucket of each.

@@ -1276,7 +1276,6 @@ __device__ void simulate_chain(chain_ws const& W, uint64_t c0, uint32_t L, bool 
     for (uint32_t i = 0; i < L; ++i) {
         ord[i] = ((unsigned long long)cn[i] << 32) | i;
         vis[i] = 0;
-        W.covered[cn[i]] = 1;
     }
     heap_sort(ord, L);
     uint64_t fcur = c0;
@@ -1347,43 +1346,186 @@ __device__ void simulate_chain(chain_ws const& W, uint64_t c0, uint32_t L, bool 
     }
 }
 
-// Paths: a node with at most one linked port starts a walk to the other end;
-// the end with the smaller node index owns the chain.
-__global__ void k_chain_paths(chain_ws W, uint32_t* err) {
-    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= W.D) return;
-    const uint32_t ll = W.link[2 * n], lr = W.link[2 * n + 1];
-    const int deg = (ll != NONE32) + (lr != NONE32);
-    if (deg == 2) return;
-    uint32_t c = (uint32_t)n;
-    bool rc = (lr == NONE32);  // walk out through the linked port
-    uint32_t L = 1;
-    if (deg == 1) {
-        uint32_t cc = c;
-        bool r = rc;
-        while (chain_step(W.link, cc, r)) {
-            if (++L > W.D) {
-                set_error(err, ERR_CHAIN_LIMIT);
-                return;
+// Seed loop of a chain of at most 64 nodes: the visited set is a register
+// mask and each seed is the unvisited position with the smallest node index
+// (a scan instead of a sort; chains hold one or two fragments in practice).
+// Same walk rules as simulate_chain.
+__device__ void simulate_chain_small(chain_ws const& W, uint64_t c0, uint32_t L, bool cyclic) {
+    uint32_t const* cn = W.ch_node + c0;
+    uint8_t const* crc = W.ch_rc + c0;
+    const uint64_t all = (L >= 64) ? ~0ull : ((1ull << L) - 1);
+    uint64_t vis = 0;
+    uint64_t fcur = c0;
+    while (vis != all) {
+        uint32_t p = 0, best = NONE32;
+        for (uint32_t q = 0; q < L; ++q) {
+            if ((vis >> q) & 1ull) continue;
+            const uint32_t nd = cn[q];
+            if (nd < best) {
+                best = nd;
+                p = q;
             }
         }
-        if (cc < n) return;  // the other end leads
+        vis |= 1ull << p;
+        const uint32_t s = best;
+        const int df = crc[p] ? -1 : 1;
+        const uint32_t sflags = W.meta[s] & 3u;
+        const uint32_t smask = W.mask[s];
+        uint32_t nb = 0, nf = 0;
+        bool open_l = false, open_r = false;
+        for (int dir = 0; dir < 2; ++dir) {
+            const bool forward = dir == 1;
+            if (!forward && sflags == M_LEFT) {
+                open_l = __popc(back_nib(smask, false)) <= 1;
+                continue;
+            }
+            if (forward && sflags == M_RIGHT) {
+                open_r = __popc(fwd_nib(smask, false)) <= 1;
+                continue;
+            }
+            const int step = forward ? df : -df;
+            int q = (int)p;
+            uint32_t cnt = 0;
+            for (;;) {
+                int q2 = q + step;
+                if (cyclic) {
+                    if (q2 < 0) q2 += (int)L;
+                    if (q2 >= (int)L) q2 -= (int)L;
+                } else if (q2 < 0 || q2 >= (int)L) {
+                    break;
+                }
+                if ((vis >> q2) & 1ull) break;
+                vis |= 1ull << q2;
+                ++cnt;
+                q = q2;
+                const uint32_t nd = cn[q];
+                const uint32_t f = W.meta[nd] & 3u;
+                if (f == M_LEFT || f == M_RIGHT) {
+                    const bool wrc = (df == 1) ? (crc[q] != 0) : (crc[q] == 0);
+                    if (forward)
+                        open_r = __popc(fwd_nib(W.mask[nd], wrc)) <= 1;
+                    else
+                        open_l = __popc(back_nib(W.mask[nd], wrc)) <= 1;
+                    break;
+                }
+            }
+            if (forward)
+                nf = cnt;
+            else
+                nb = cnt;
+        }
+        const uint32_t flen = nb + 1 + nf;
+        for (uint32_t j = 0; j < flen; ++j) {
+            int q = (int)p + df * ((int)j - (int)nb);
+            if (cyclic) {
+                q %= (int)L;
+                if (q < 0) q += (int)L;
+            }
+            const bool wrc = (df == 1) ? (crc[q] != 0) : (crc[q] == 0);
+            W.fe[fcur + j] = (cn[q] << 1) | (wrc ? 1u : 0u);
+        }
+        W.seed_start[s] = (uint32_t)fcur;
+        W.seed_len[s] = flen;
+        W.seed_open[s] = (uint8_t)((open_l ? 1 : 0) | (open_r ? 2 : 0));
+        fcur += flen;
     }
-    const uint64_t c0 = atomicAdd(W.cursor, (unsigned long long)L);
+}
+
+// Per-lane reservation of `want` consecutive entries of *cnt; every lane of
+// the warp must call it.
+__device__ __forceinline__ unsigned long long warp_reserve(uint32_t want, unsigned long long* cnt) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long incl = want;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long base = 0;
+    if (lane == 31 && total) base = atomicAdd(cnt, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    return base + incl - want;
+}
+
+// Path ends: nodes with at most one linked port, compacted.
+__global__ void __launch_bounds__(256) k_chain_ends(chain_ws W, uint32_t* __restrict__ ends,
+                                                    unsigned long long* __restrict__ nends) {
+    const uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool end = false;
+    if (n < W.D) {
+        const uint2 l = reinterpret_cast<uint2 const*>(W.link)[n];
+        end = (l.x == NONE32) || (l.y == NONE32);
+    }
+    const uint32_t b = __ballot_sync(0xffffffffu, end);
+    if (!b) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(b) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(nends, (unsigned long long)__popc(b));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (end) ends[base + __popc(b & lanemask_lt())] = (uint32_t)n;
+}
+
+// Each end walks to the other end; the end with the smaller node index leads
+// and reserves the chain's slots [c0, c0 + L).  heads[h] = (node | rc << 31,
+// L, c0 low, c0 high).
+__global__ void __launch_bounds__(256) k_chain_lead(chain_ws W, uint32_t const* __restrict__ ends, uint64_t nends,
+                                                    uint4* __restrict__ heads, unsigned long long* __restrict__ nheads,
+                                                    uint32_t* err) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c = 0, L = 0;
+    bool rc = false, lead = false;
+    if (i < nends) {
+        c = ends[i];
+        const uint32_t ll = W.link[2 * (uint64_t)c], lr = W.link[2 * (uint64_t)c + 1];
+        rc = (lr == NONE32);  // walk out through the linked port
+        L = 1;
+        lead = true;
+        if (ll != NONE32 || lr != NONE32) {
+            uint32_t cc = c;
+            bool r = rc;
+            while (chain_step(W.link, cc, r)) {
+                if (++L > W.D) {
+                    set_error(err, ERR_CHAIN_LIMIT);
+                    lead = false;
+                    break;
+                }
+            }
+            if (cc < c) lead = false;  // the other end leads
+        }
+    }
+    const unsigned long long c0 = warp_reserve(lead ? L : 0, W.cursor);
+    const unsigned long long h = warp_reserve(lead ? 1 : 0, nheads);
+    if (!lead) return;
     if (c0 + L > W.D) {  // chains partition the nodes; anything else is a bug
         set_error(err, ERR_CAPACITY);
         return;
     }
-    uint32_t i = 0;
-    uint32_t cc = c;
-    bool r = rc;
+    heads[h] = make_uint4(c | (rc ? 0x80000000u : 0u), L, (uint32_t)c0, (uint32_t)(c0 >> 32));
+}
+
+// One thread per path chain: lay the chain out at c0 and replay the seed loop.
+__global__ void __launch_bounds__(128) k_chain_paths(chain_ws W, uint4 const* __restrict__ heads, uint64_t nheads) {
+    const uint64_t h = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nheads) return;
+    const uint4 hd = heads[h];
+    uint32_t cc = hd.x & 0x7fffffffu;
+    bool r = (hd.x >> 31) != 0;
+    const uint32_t L = hd.y;
+    const uint64_t c0 = ((uint64_t)hd.w << 32) | hd.z;
     W.ch_node[c0] = cc;
     W.ch_rc[c0] = r ? 1 : 0;
-    while (++i < L && chain_step(W.link, cc, r)) {
+    W.covered[cc] = 1;
+    for (uint32_t i = 1; i < L && chain_step(W.link, cc, r); ++i) {
         W.ch_node[c0 + i] = cc;
         W.ch_rc[c0 + i] = r ? 1 : 0;
+        W.covered[cc] = 1;
     }
-    simulate_chain(W, c0, L, false);
+    if (L <= 64)
+        simulate_chain_small(W, c0, L, false);
+    else
+        simulate_chain(W, c0, L, false);
 }
 
 // Cycles: nodes left uncovered; the smallest node index of a cycle leads.
@@ -1419,7 +1561,10 @@ __global__ void k_chain_cycles(chain_ws W, uint32_t* err) {
         W.ch_node[c0 + i] = cc;
         W.ch_rc[c0 + i] = r ? 1 : 0;
     }
-    simulate_chain(W, c0, L, true);
+    if (L <= 64)
+        simulate_chain_small(W, c0, L, true);
+    else
+        simulate_chain(W, c0, L, true);
 }
 
 // ---- fragments --------------------------------------------------------------
@@ -1995,10 +2140,28 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(W.covered, 0, D, st));
     CDBG_CUDA(cudaMemsetAsync(W.cursor, 0, 8, st));
     {
-        CDBG_PROF("k_chain_paths", st);
-        k_chain_paths<<<grid(D, 128), 128, 0, st>>>(W, d_err);
+        uint32_t* ends = A.alloc<uint32_t>(D);
+        unsigned long long* cnt2 = A.alloc<unsigned long long>(2);
+        CDBG_CUDA(cudaMemsetAsync(cnt2, 0, 16, st));
+        {
+            CDBG_PROF("k_chain_ends", st);
+            k_chain_ends<<<grid(D, 256), 256, 0, st>>>(W, ends, cnt2);
+        }
+        CDBG_CHECK_LAUNCH();
+        const uint64_t nends = read_dev(cnt2, st);
+        uint4* heads = A.alloc<uint4>(nends + 1);
+        if (nends) {
+            CDBG_PROF("k_chain_lead", st);
+            k_chain_lead<<<grid(nends, 256), 256, 0, st>>>(W, ends, nends, heads, cnt2 + 1, d_err);
+        }
+        CDBG_CHECK_LAUNCH();
+        const uint64_t nheads = read_dev(cnt2 + 1, st);
+        if (nheads) {
+            CDBG_PROF("k_chain_paths", st);
+            k_chain_paths<<<grid(nheads, 128), 128, 0, st>>>(W, heads, nheads);
+        }
+        CDBG_CHECK_LAUNCH();
     }
-    CDBG_CHECK_LAUNCH();
     {
         CDBG_PROF("k_chain_cycles", st);
         k_chain_cycles<<<grid(D, 128), 128, 0, st>>>(W, d_err);

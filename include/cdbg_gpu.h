@@ -170,6 +170,8 @@ typedef struct cdbg_build_result {
     uint64_t total_integers;
     uint64_t n_kmers, n_supers, n_records, n_occ, n_distinct, n_fragments, total_seq_bytes;
     uint64_t h2d_bytes, d2h_bytes;
+    uint64_t n_bases;            /* bases in ACGT runs >= k */
+    uint64_t record_bytes;       /* serialized record bytes (uncompressed bucket-file contents) */
     double ms_phase1, ms_phase2, ms_total; /* device time (CUDA events) */
 } cdbg_build_result;
 
