@@ -237,3 +237,71 @@ def canonical_frag(fl, runs, seq, classes):
     if rs < seq:
         return (rs, tuple(reversed(per)), ((fl & 1) << 1) | ((fl >> 1) & 1))
     return (seq, tuple(per), fl)
+
+
+# ---- final outputs (.fa, .metadata.txt) written by phases 3 and 4 ----------
+
+def write_classes(path, classes):
+    """Class list file read by the phase-3/4 runner: u64 count, then per class
+    u32 n and n ascending u32 colors."""
+    with open(path, "wb") as f:
+        f.write(struct.pack("<Q", len(classes)))
+        for c in classes:
+            f.write(struct.pack("<I", len(c)))
+            if len(c):
+                f.write(np.asarray(c, dtype=np.uint32).tobytes())
+
+
+def read_fasta_unitigs(path):
+    """[(cid, seq)] of a phase-4 .fa (`>cid` headers, emit.hpp:93-175)."""
+    out = []
+    cid = None
+    with open(path) as f:
+        for line in f:
+            line = line.rstrip("\n")
+            if line.startswith(">"):
+                cid = int(line[1:].split()[0])
+            elif line:
+                out.append((cid, line))
+    return out
+
+
+def read_metadata(path):
+    """key -> int of a .metadata.txt (builder.hpp:754-764)."""
+    d = {}
+    with open(path) as f:
+        for line in f:
+            if "=" in line:
+                key, v = line.strip().split("=", 1)
+                d[key] = int(v)
+    return d
+
+
+def canonical_unitig(seq, k):
+    """Orientation- and rotation-free form of a unitig.  A unitig whose last
+    k-1 bases repeat its first k-1 may be a cycle, whose starting k-mer is
+    arbitrary: it is replaced by the smallest rotation of its k-mer cycle over
+    both strands (rotations of one k-mer cycle never belong to two different
+    unitigs of one build, so this cannot merge distinct unitigs)."""
+    rs = revcomp(seq)
+    if len(seq) > k - 1 and k > 1 and seq[-(k - 1):] == seq[:k - 1]:
+        best = None
+        for s in (seq, rs):
+            core = s[:len(s) - (k - 1)]
+            n = len(core)
+            for r in range(n):
+                rot = core[r:] + core[:r]
+                cand = rot + rot[:k - 1]
+                if best is None or cand < best:
+                    best = cand
+        return best
+    return min(seq, rs)
+
+
+def final_pairs(basename, k):
+    """Multiset of (canonical unitig, decoded color set) of a finished build,
+    its metadata and its color-set family."""
+    from collections import Counter
+    _, _, _, classes = read_color_sets(basename + ".color_sets")
+    pairs = Counter((canonical_unitig(s, k), tuple(classes[c])) for c, s in read_fasta_unitigs(basename + ".fa"))
+    return pairs, read_metadata(basename + ".metadata.txt"), Counter(tuple(c) for c in classes)
