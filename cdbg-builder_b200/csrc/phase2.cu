@@ -885,14 +885,6 @@ __global__ void k_new_flags(uint64_t nc, uint32_t const* __restrict__ cid, uint3
     if (c < nc) flag[c] = cid[c] == NONE32 ? 1u : 0u;
 }
 
-__global__ void k_new_gather(uint64_t nc, uint32_t const* __restrict__ flag, uint64_t const* __restrict__ pos,
-                             cand_view cv, uint64_t* __restrict__ nkey, uint32_t* __restrict__ nidx) {
-    uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc || !flag[c]) return;
-    nkey[pos[c]] = cv.hash[c];
-    nidx[pos[c]] = (uint32_t)c;
-}
-
 __global__ void k_run_heads(uint64_t n, uint64_t const* __restrict__ key, uint32_t* __restrict__ head) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) head[i] = (i == 0 || key[i] != key[i - 1]) ? 1u : 0u;
@@ -905,95 +897,11 @@ __global__ void k_run_starts(uint64_t n, uint32_t const* __restrict__ head, uint
     if (i < n && head[i]) run_start[hpos[i]] = i;
 }
 
-// Every member of an equal-hash run against the run's head (normally the
-// whole run is one color set).  rep[c] = the head when equal; a member that
-// differs marks its run for the exact fallback below.
-__global__ void k_member_match(uint64_t n, uint32_t const* __restrict__ head, uint64_t const* __restrict__ hpos,
-                               uint64_t const* __restrict__ run_start, uint32_t const* __restrict__ nidx,
-                               cand_view cv, uint64_t const* __restrict__ cw, uint64_t const* __restrict__ cb,
-                               uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first,
-                               uint32_t* __restrict__ collided) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint64_t run = hpos[i] + head[i] - 1;  // inclusive count - 1
-    const uint32_t c = nidx[i];
-    const uint32_t h = nidx[run_start[run]];
-    if (c == h) {
-        rep[c] = c;
-        atomicMin(&rep_first[c], cv.first[c]);
-        return;
-    }
-    if (bits_equal(cw, cb[c], cb[c + 1] - cb[c], cw, cb[h], cb[h + 1] - cb[h])) {
-        rep[c] = h;
-        atomicMin(&rep_first[h], cv.first[c]);
-    } else {
-        rep[c] = c;
-        collided[run] = 1;
-    }
-}
-
-// Exact grouping of a run with a 64-bit hash collision (thread per run).
-__global__ void k_group_collided(uint64_t nruns, uint32_t const* __restrict__ collided,
-                                 uint64_t const* __restrict__ run_start, uint64_t n,
-                                 uint32_t const* __restrict__ nidx, cand_view cv,
-                                 uint64_t const* __restrict__ cw, uint64_t const* __restrict__ cb,
-                                 uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first) {
-    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nruns || !collided[r]) return;
-    const uint64_t i = run_start[r];
-    const uint64_t e = (r + 1 < nruns) ? run_start[r + 1] : n;
-    for (uint64_t j = i; j < e; ++j) {
-        const uint32_t cj = nidx[j];
-        uint32_t rr = cj;
-        for (uint64_t q = i; q < j; ++q) {
-            const uint32_t cq = nidx[q];
-            if (rep[cq] != cq) continue;
-            if (bits_equal(cw, cb[cj], cb[cj + 1] - cb[cj], cw, cb[cq], cb[cq + 1] - cb[cq])) {
-                rr = cq;
-                break;
-            }
-        }
-        rep[cj] = rr;
-        rep_first[cj] = NONE32;
-        const uint32_t f = cv.first[cj];
-        if (rr == cj)
-            rep_first[cj] = f;
-        else if (f < rep_first[rr])
-            rep_first[rr] = f;
-    }
-}
-
-__global__ void k_rep_keys(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
-                           uint32_t* __restrict__ is_rep) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t c = nidx[i];
-    is_rep[i] = rep[c] == c ? 1u : 0u;
-}
-
-__global__ void k_rep_gather(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ is_rep,
-                             uint64_t const* __restrict__ pos, uint32_t const* __restrict__ rep_first,
-                             uint64_t* __restrict__ rkey, uint32_t* __restrict__ rcand) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !is_rep[i]) return;
-    const uint32_t c = nidx[i];
-    rkey[pos[i]] = rep_first[c];
-    rcand[pos[i]] = c;
-}
-
 // New class j (in first-appearance order) = candidate rcand[j]; cid base+j.
 __global__ void k_assign_new(uint64_t nnew, uint32_t const* __restrict__ rcand, uint64_t base,
                              uint32_t* __restrict__ cid) {
     uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j < nnew) cid[rcand[j]] = (uint32_t)(base + j);
-}
-
-__global__ void k_assign_members(uint64_t n, uint32_t const* __restrict__ nidx, uint32_t const* __restrict__ rep,
-                                 uint32_t* __restrict__ cid) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t c = nidx[i];
-    if (rep[c] != c) cid[c] = cid[rep[c]];
 }
 
 __global__ void k_iota32(uint64_t n, uint32_t* __restrict__ p) {
