@@ -49,6 +49,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch-occ", type=int, default=0)
     ap.add_argument("--out", default="")
+    # serving workload
+    ap.add_argument("--requests", type=int, default=48, help="serving: requests in the stream")
+    ap.add_argument("--rate", type=float, default=30.0, help="serving: Poisson arrivals per second")
+    ap.add_argument("--slots", default="1,2,3,4",
+                    help="serving: concurrent builds; a list is swept and the best is reported")
+    ap.add_argument("--no-plain", action="store_true", help="serving: skip the plain one-at-a-time run")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
+    ap.add_argument("--serving-buckets", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -397,8 +405,107 @@ def path_algorithmic_bytes(r, w):
 TRAFFIC_PER_UNIT = {}
 
 
+# ---------------------------------------------------------------- serving
+def serving_requests(n_req, seed=7):
+    """The serving stream's requests: per request its own seeded ancestor, 2-300
+    genomes (log-uniform) of 0.5-8 Mbp (log-uniform), 0.1-2% divergence, k in
+    {31, 63}; returns [(seq, off, colors, n_genomes, k)] in pinned host memory."""
+    import numpy as np
+    import torch
+    from cdbg_gpu import synth
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_req):
+        n = int(round(np.exp(rng.uniform(np.log(2), np.log(300)))))
+        k = int(rng.choice([31, 63]))
+        p, _, _, _ = synth.preset("serving", seed=10000 + i)
+        seq, lens, per = synth.collection(p, n)
+        off = np.zeros(len(lens) + 1, dtype=np.uint64)
+        off[1:] = np.cumsum(lens)
+        colors = np.repeat(np.arange(n, dtype=np.uint32), per)
+        out.append((torch.from_numpy(seq).pin_memory(), torch.from_numpy(off.view(np.int64)).pin_memory(),
+                    torch.from_numpy(colors.view(np.int32)).pin_memory(), n, k, count_kmers(lens, k)))
+    return out
+
+
+def serve_stream(reqs, arrivals, slots, budget, B, batch_occ):
+    """Submit each request at its arrival time to a server; returns per-request
+    (latency s, queue wait s, device ms) and the makespan."""
+    from cdbg_gpu import native
+    srv = native.Server(0, slots=slots, hbm_budget=budget)
+    try:
+        t0 = srv.stats()["clock_s"]
+        ids = []
+        for (seq, off, col, n, k, _), at in zip(reqs, arrivals):
+            while srv.stats()["clock_s"] - t0 < at:
+                time.sleep(0.0005)
+            b = native.SeqBatch(seq.data_ptr(), seq.numel(), off.data_ptr(), col.data_ptr(), col.numel(), 0)
+            ids.append((srv.submit(b, k, B, n, batch_occ=batch_occ), t0 + at))
+        res = []
+        for rid, arr in ids:
+            r = srv.wait(rid, outputs=False)
+            if r["status"] != 0:
+                raise RuntimeError("request failed: " + r["error"])
+            res.append((r["t_done"] - arr, r["t_start"] - arr, r["ms_device"], r["t_done"]))
+        st = srv.stats()
+    finally:
+        srv.close()
+    makespan = max(x[3] for x in res) - (t0 + arrivals[0])
+    return res, makespan, st
+
+
+def main_serving(a):
+    import numpy as np
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    t = time.time()
+    reqs = serving_requests(a.requests)
+    gen_s = time.time() - t
+    rng = np.random.default_rng(11)
+    arrivals = np.cumsum(rng.exponential(1.0 / a.rate, size=len(reqs)))
+    arrivals -= arrivals[0]
+    budget = int(a.budget_gb * (1 << 30))
+    B = a.serving_buckets
+    kmers = sum(r[5] for r in reqs)
+    slot_list = [int(x) for x in str(a.slots).split(",") if x]
+    # warm-up: the whole stream once through a server (device memory pool and
+    # pinned output buffers reach their steady-state sizes), not timed
+    serve_stream(reqs, [0.0] * len(reqs), max(slot_list), budget, B, 0)
+
+    def summary(res, makespan, st):
+        lat = np.array([x[0] for x in res])
+        return {"builds_per_s": len(res) / makespan, "kmers_per_s": kmers / makespan,
+                "makespan_s": makespan, "latency_p50_s": float(np.percentile(lat, 50)),
+                "latency_p99_s": float(np.percentile(lat, 99)),
+                "queue_wait_p50_s": float(np.percentile([x[1] for x in res], 50)),
+                "peak_running": st["peak_running"], "peak_reserved_gb": st["peak_reserved_bytes"] / 2 ** 30}
+
+    by_slots = {}
+    for sl in slot_list:
+        by_slots[sl] = summary(*serve_stream(reqs, arrivals, sl, budget, B, 0))
+    best = max(by_slots, key=lambda sl: by_slots[sl]["builds_per_s"])
+    serving = dict(by_slots[best], slots=best)
+    plain = None if a.no_plain else summary(*serve_stream(reqs, arrivals, 1, budget, B, 1))
+    line = {"metric": "serving builds/s", "value": serving["builds_per_s"], "unit": "builds/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "serving: %d requests (Poisson %.1f/s), 2-300 genomes x 0.5-8 Mbp log-uniform, "
+                                   "k in {31, 63}, %d buckets, slots %s, %.0f GB HBM budget"
+                                   % (len(reqs), a.rate, B, a.slots, a.budget_gb),
+                       "total_kmers": kmers, "generate_s": gen_s},
+            "serving": serving, "by_slots": by_slots, "plain_sequential": plain,
+            "speedup_vs_plain": (serving["builds_per_s"] / plain["builds_per_s"]) if plain else None}
+    print(json.dumps(line))
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(json.dumps(line) + "\n")
+    return 0
+
+
 if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
         sys.exit(reference_arm(args))
+    if args.workload == "serving":
+        sys.exit(main_serving(args))
     sys.exit(main_gpu(args))

@@ -23,8 +23,9 @@ HOST = os.path.join(PKG, "host")
 OBJ = os.path.join(PKG, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+CUDA_INC = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(NVCC))), "include")
 CU_SOURCES = ["phase1.cu", "phase2.cu", "capi.cu"]
-HOST_SOURCES = ["io.cpp"]
+HOST_SOURCES = ["io.cpp", "server.cpp"]
 REFERENCE = os.environ.get("CDBG_REFERENCE_DIR", "/root/reference")
 
 
@@ -64,7 +65,7 @@ def build_gpu(force=False):
                      "-I" + INC, "-c", os.path.join(CSRC, s), "-o", o])
     for s in HOST_SOURCES:
         o = os.path.join(OBJ, s + ".o")
-        jobs.append(["g++", "-std=c++17", "-O3", "-fPIC", "-I" + INC, "-c",
+        jobs.append(["g++", "-std=c++17", "-O3", "-fPIC", "-I" + INC, "-I" + CUDA_INC, "-c",
                      os.path.join(HOST, s), "-o", o])
     with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
         list(ex.map(_run, jobs))

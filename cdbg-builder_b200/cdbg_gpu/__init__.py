@@ -6,4 +6,4 @@ C-ABI of include/cdbg_gpu.h); this package binds it, reads the on-disk
 artifacts and generates the synthetic benchmark workloads.
 """
 from . import formats, native, synth  # noqa: F401
-from .native import Engine, best_m, host_batch  # noqa: F401
+from .native import Engine, Server, best_m, host_batch  # noqa: F401

@@ -86,6 +86,30 @@ class BuildResult(ctypes.Structure):
                 ("ms_total", ctypes.c_double)]
 
 
+class ServerParams(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
+                ("bytes_per_base", ctypes.c_double), ("floor_bytes", ctypes.c_uint64)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("error", ctypes.c_char_p),
+                ("frag_bytes", ctypes.c_void_p), ("frag_nbytes", ctypes.c_uint64),
+                ("class_words", ctypes.c_void_p), ("class_bits", ctypes.c_uint64),
+                ("class_offsets", ctypes.c_void_p), ("n_color_sets", ctypes.c_uint64),
+                ("total_integers", ctypes.c_uint64), ("n_kmers", ctypes.c_uint64),
+                ("n_distinct", ctypes.c_uint64), ("n_fragments", ctypes.c_uint64),
+                ("need_bytes", ctypes.c_uint64), ("grant_bytes", ctypes.c_uint64),
+                ("t_submit", ctypes.c_double), ("t_start", ctypes.c_double), ("t_done", ctypes.c_double),
+                ("ms_device", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("waiting", ctypes.c_uint64),
+                ("running", ctypes.c_uint32), ("peak_running", ctypes.c_uint32),
+                ("reserved_bytes", ctypes.c_uint64), ("peak_reserved_bytes", ctypes.c_uint64),
+                ("clock_s", ctypes.c_double)]
+
+
 # symbol -> (restype, argtypes); the header's complete list
 SIGNATURES = {
     "cdbg_engine_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
@@ -117,6 +141,17 @@ SIGNATURES = {
                                        ctypes.POINTER(Phase2Stats)]),
     "cdbg_gpu_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
                                       ctypes.POINTER(BuildParams), ctypes.POINTER(BuildResult)]),
+    "cdbg_engine_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "cdbg_engine_memory": (ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p]),
+    "cdbg_engine_trim": (ctypes.c_int, [ctypes.c_void_p]),
+    "cdbg_server_create": (ctypes.c_int, [ctypes.POINTER(ServerParams), ctypes.POINTER(ctypes.c_void_p)]),
+    "cdbg_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
+                                          ctypes.POINTER(BuildParams), c_u64p]),
+    "cdbg_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(RequestResult)]),
+    "cdbg_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "cdbg_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "cdbg_server_destroy": (None, [ctypes.c_void_p]),
+    "cdbg_server_last_error": (ctypes.c_char_p, []),
 }
 
 _lib = None
@@ -234,6 +269,20 @@ class Engine:
     def __exit__(self, *a):
         self.close()
 
+    def set_memory_limit(self, nbytes):
+        """Cap the device memory of this engine's calls (0 = none)."""
+        _check(lib().cdbg_engine_set_memory_limit(self._h, nbytes))
+
+    def memory(self):
+        """(bytes held now, peak since the previous call)."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().cdbg_engine_memory(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def trim(self):
+        """Return cached device memory to the device pool."""
+        _check(lib().cdbg_engine_trim(self._h))
+
     def set_stream(self, stream_handle):
         """Run on a caller-owned cudaStream_t (int handle, e.g. torch's
         Stream.cuda_stream); None restores the engine's own stream."""
@@ -318,3 +367,73 @@ def result_class_offsets(r):
     if r.n_color_sets == 0:
         return np.zeros(0, dtype=np.uint64)
     return np.ctypeslib.as_array(ctypes.cast(r.class_offsets, c_u64p), shape=(r.n_color_sets,)).copy()
+
+
+class Server:
+    """Build server (include/cdbg_gpu.h cdbg_server_*): concurrent builds on
+    one GPU under an HBM budget.  submit() returns a request id; wait()
+    returns the finished request as a dict with its outputs (bytes, numpy
+    words and offsets) and timings on the server's clock."""
+
+    def __init__(self, device=0, slots=4, hbm_budget=150 << 30, bytes_per_base=0.0, floor_bytes=0):
+        L = lib()
+        p = ServerParams(device, slots, hbm_budget, bytes_per_base, floor_bytes)
+        h = ctypes.c_void_p()
+        if L.cdbg_server_create(ctypes.byref(p), ctypes.byref(h)) != 0:
+            raise RuntimeError(L.cdbg_server_last_error().decode(errors="replace"))
+        self.h = h
+        self._keep = {}
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(lib().cdbg_server_last_error().decode(errors="replace"))
+
+    def submit(self, batch, k, num_buckets, num_colors, m=0, batch_occ=0):
+        p = BuildParams(k, m, num_buckets, num_colors, batch_occ, 1)
+        rid = ctypes.c_uint64()
+        self._check(lib().cdbg_server_submit(self.h, ctypes.byref(batch), ctypes.byref(p), ctypes.byref(rid)))
+        self._keep[rid.value] = batch  # host buffers live until the request is done
+        return rid.value
+
+    def wait(self, rid, release=True, outputs=True):
+        """Finished request `rid` as a dict; with outputs=False only counts and
+        timings (no host copies of the outputs)."""
+        r = RequestResult()
+        self._check(lib().cdbg_server_wait(self.h, rid, ctypes.byref(r)))
+        out = {k: getattr(r, k) for k, _ in RequestResult._fields_
+               if k not in ("frag_bytes", "class_words", "class_offsets", "error")}
+        out["error"] = r.error.decode(errors="replace") if r.error else ""
+        if r.status == 0 and outputs:
+            out["frag"] = ctypes.string_at(r.frag_bytes, r.frag_nbytes) if r.frag_nbytes else b""
+            nw = (r.class_bits + 63) // 64
+            out["words"] = np.ctypeslib.as_array(ctypes.cast(r.class_words, c_u64p), (nw,)).copy() \
+                if nw else np.zeros(0, np.uint64)
+            out["offsets"] = np.ctypeslib.as_array(ctypes.cast(r.class_offsets, c_u64p), (r.n_color_sets,)).copy() \
+                if r.n_color_sets else np.zeros(0, np.uint64)
+        if release:
+            self._check(lib().cdbg_server_release(self.h, rid))
+            self._keep.pop(rid, None)
+        return out
+
+    def stats(self):
+        s = ServerStats()
+        self._check(lib().cdbg_server_stats(self.h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().cdbg_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -81,6 +81,28 @@ cdbg::seq_input stage_batch(cdbg_engine* e, cdbg_seq_batch const* b, uint64_t* h
     return in;
 }
 
+// Apply the engine's memory limit to both arenas for the coming call (after
+// their reset): cached memory above the limit is returned first.
+void apply_limit(cdbg_engine* e) {
+    if (!e->mem_limit) {
+        e->A.set_limit(0);
+        e->P.set_limit(0);
+        return;
+    }
+    const size_t lim = e->mem_limit;
+    if (e->p2.bytes() > lim / 4) e->p2.release();
+    const size_t ext = e->p2.bytes();
+    if (e->A.reserved_bytes() + e->P.reserved_bytes() + ext > lim) {
+        e->A.trim();
+        e->P.trim();
+    }
+    const size_t chunk = std::max<size_t>(size_t(256) << 20, std::min<size_t>(size_t(4) << 30, lim / 8));
+    e->A.set_chunk_bytes(chunk);
+    e->P.set_chunk_bytes(chunk);
+    e->A.set_limit(lim, &e->P, ext);
+    e->P.set_limit(lim, &e->A, ext);
+}
+
 // Per-call scope: route kernel timing to this engine's profiler and fold the
 // recorded launches into its totals when the call returns.
 struct call_scope {
@@ -230,8 +252,11 @@ int cdbg_engine_create(int device, cdbg_engine** out) {
         CDBG_CUDA(cudaSetDevice(device));
         auto* e = new cdbg_engine();
         e->device = device;
+        cdbg::device_pool(device);  // configure the pool the arenas draw from
         CDBG_CUDA(cudaStreamCreateWithFlags(&e->own_st, cudaStreamNonBlocking));
         e->st = e->own_st;
+        e->A.set_stream(e->st);
+        e->P.set_stream(e->st);
         CDBG_CUDA(cudaMalloc(&e->d_err, 16));
         CDBG_CUDA(cudaMemset(e->d_err, 0, 16));
         *out = e;
@@ -244,7 +269,11 @@ int cdbg_engine_create(int device, cdbg_engine** out) {
 void cdbg_engine_destroy(cdbg_engine* e) {
     if (!e) return;
     cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->st);
     e->A.free_all();
+    e->P.free_all();
+    e->p2.release();
+    cudaStreamSynchronize(e->st);
     if (e->d_err) cudaFree(e->d_err);
     e->prof.resolve();
     if (e->own_st) cudaStreamDestroy(e->own_st);
@@ -253,11 +282,55 @@ void cdbg_engine_destroy(cdbg_engine* e) {
 
 int cdbg_engine_set_stream(cdbg_engine* e, void* stream) {
     if (!e) return -1;
+    cudaSetDevice(e->device);
+    // memory the engine holds was ordered on the old stream
+    if (cudaStreamSynchronize(e->st) != cudaSuccess) {
+        g_last_error = "stream synchronize failed";
+        return -1;
+    }
     e->st = stream ? (cudaStream_t)stream : e->own_st;
+    e->A.set_stream(e->st);
+    e->P.set_stream(e->st);
+    e->p2.set_stream(e->st);
+    return 0;
+}
+
+int cdbg_engine_trim(cdbg_engine* e) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    cudaSetDevice(e->device);
+    e->A.reset();
+    e->P.reset();
+    e->A.trim();
+    e->P.trim();
+    e->p2.release();
     return 0;
 }
 
 uint64_t cdbg_launch_count(void) { return cdbg::g_launches.load(); }
+
+int cdbg_engine_set_memory_limit(cdbg_engine* e, uint64_t bytes) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    e->mem_limit = bytes;
+    return 0;
+}
+
+int cdbg_engine_memory(cdbg_engine* e, uint64_t* reserved, uint64_t* peak) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    if (reserved) *reserved = e->A.reserved_bytes() + e->P.reserved_bytes() + e->p2.bytes();
+    if (peak) *peak = e->A.peak_bytes() + e->P.peak_bytes() + e->p2.bytes();
+    e->A.reset_peak();
+    e->P.reset_peak();
+    return 0;
+}
 
 int cdbg_engine_copy_out(cdbg_engine* e, const void* device_src, void* host_dst, uint64_t bytes) {
     try {
@@ -310,6 +383,7 @@ int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, ui
         validate(k, m, num_buckets);
         CDBG_CUDA(cudaSetDevice(e->device));
         e->A.reset();
+        apply_limit(e);
         cdbg::seq_input in = stage_batch(e, b, nullptr);
         cdbg::run_table rt;
         cdbg::build_runs(in, k, e->A, e->st, rt, e->A);
@@ -373,6 +447,8 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
         const uint32_t m = a->m ? a->m : best_m(k);
         validate(k, m, a->num_buckets);
         CDBG_CUDA(cudaSetDevice(e->device));
+        e->A.reset();
+        apply_limit(e);
         const uint32_t T = host_threads(a->host_threads);
         std::vector<std::string> files(a->files, a->files + a->num_files);
         cdbg::io::bucket_file_set out(a->tmp_dir, a->num_buckets);
@@ -455,6 +531,7 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         const uint32_t B = a->num_buckets;
         if (a->k < 2 || a->k > 63) throw std::runtime_error("k must be in [2, 63]");
         e->A.reset();
+        apply_limit(e);
         // bucket bytes: decompress straight into pinned host memory
         uint8_t* pinned = nullptr;
         cdbg::io::bucket_bytes bb;
@@ -544,6 +621,7 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         CDBG_CUDA(cudaSetDevice(e->device));
         e->A.reset();
         e->P.reset();
+        apply_limit(e);
         cdbg_build_result res{};
         cudaEvent_t ev[4];
         for (auto& x : ev) CDBG_CUDA(cudaEventCreate(&x));

@@ -42,6 +42,7 @@ struct cdbg_engine {
     // class dictionary + device-resident outputs, reused across builds
     cdbg::phase2_state p2;
     uint32_t* d_err = nullptr;  // device error word (outside the arena)
+    uint64_t mem_limit = 0;     // device memory cap of this engine (0 = none)
     // host copies of the last cdbg_gpu_build's outputs (outputs_to_host = 1)
     pinned_buffer h_frag, h_words, h_offsets;
 };

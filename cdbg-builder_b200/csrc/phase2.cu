@@ -2158,9 +2158,9 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     CDBG_CUDA(cudaStreamSynchronize(st));
     uint64_t budget = p.batch_occ;
     if (budget == 0) {
-        size_t fr = 0, tot = 0;
-        CDBG_CUDA(cudaMemGetInfo(&fr, &tot));
-        const uint64_t avail = (uint64_t)fr + A.cached_free();
+        int dev = 0;
+        CDBG_CUDA(cudaGetDevice(&dev));
+        const uint64_t avail = std::min<uint64_t>(device_available(dev) + A.cached_free(), A.headroom());
         // ~200 B of device memory per k-mer occurrence in the batch, worst
         // case; keep 45% of the available memory for outputs and the dictionary
         budget = std::max<uint64_t>(1ull << 22, std::min<uint64_t>(1ull << 28, (uint64_t)(avail * 0.5) / 220));

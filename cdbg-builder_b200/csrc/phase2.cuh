@@ -22,6 +22,24 @@ struct phase2_state {
     dvec<uint64_t> slot_hash;  // open-addressing table hash -> class
     dvec<uint32_t> slot_cid;
     dvec<uint8_t> frag;        // frag spill bytes (device-resident builds)
+    // Order later frees on `st` (after a stream switch).
+    void set_stream(cudaStream_t st) {
+        cls_hash.st_last = bit_off.st_last = words.st_last = slot_hash.st_last = st;
+        slot_cid.st_last = st;
+        frag.st_last = st;
+    }
+    void release() {
+        cls_hash.release();
+        bit_off.release();
+        words.release();
+        slot_hash.release();
+        slot_cid.release();
+        frag.release();
+    }
+    size_t bytes() const {
+        return cls_hash.bytes() + bit_off.bytes() + words.bytes() + slot_hash.bytes() + slot_cid.bytes() +
+               frag.bytes();
+    }
 };
 
 // Outputs of phase 2, accumulated over bucket batches.

@@ -51,6 +51,21 @@ int cdbg_engine_set_stream(cdbg_engine* e, void* stream);
 /* Kernel launches issued by this library in this process so far. */
 uint64_t cdbg_launch_count(void);
 
+/* Cap the device memory the engine holds during its calls (arenas + class
+ * dictionary; 0 = no cap).  Phase 2 sizes its bucket batches to fit; work
+ * that cannot fit fails with an error instead of exceeding the cap.  The
+ * engine's share of the reference's -g budget (builder.hpp:258-267). */
+int cdbg_engine_set_memory_limit(cdbg_engine* e, uint64_t bytes);
+
+/* Device bytes the engine holds now and at peak since the previous call of
+ * this function (which restarts the peak). */
+int cdbg_engine_memory(cdbg_engine* e, uint64_t* reserved, uint64_t* peak);
+
+/* Give the engine's cached device memory back to the device's memory pool
+ * (stream-ordered, no device-wide synchronization), where other engines can
+ * take it.  Invalidates device pointers from its previous builds. */
+int cdbg_engine_trim(cdbg_engine* e);
+
 /* Per-kernel device time (CUDA events around each launch on the launching
  * stream): enable = 1 starts collecting (and clears), 0 stops.  Stats copy
  * up to `cap` kernels: NUL-separated names into `names`, total ms and
@@ -212,6 +227,60 @@ int cdbg_gpu_supers_noalloc(const uint64_t* words, const uint64_t* run_soff, con
                             uint32_t num_buckets, uint64_t* out_start, uint32_t* out_len,
                             uint32_t* out_color, uint32_t* out_flags, uint32_t* out_bucket,
                             uint64_t out_cap, uint64_t* n_supers, void* stream);
+
+/* ---- build server (continuous batching) -------------------------------- */
+
+/* Many independent builds on one GPU, accepted at any time.  No counterpart in
+ * the reference (one build per process).  `slots` engines run admitted
+ * requests concurrently, each on its own stream; a request is admitted when a
+ * slot is free and its device-memory estimate (bytes_per_base * input bases +
+ * floor_bytes) fits in what is left of hbm_budget -- or, when nothing runs, at
+ * once with the whole budget.  Requests start in arrival order.  Every
+ * request's outputs are those of the same build run alone. */
+typedef struct cdbg_server cdbg_server;
+
+typedef struct cdbg_server_params {
+    int device;
+    uint32_t slots;              /* concurrent builds (0 = 1) */
+    uint64_t hbm_budget;         /* device bytes for all admitted builds */
+    double bytes_per_base;       /* memory model (0 = 24) */
+    uint64_t floor_bytes;        /* memory model floor (0 = 2 GiB) */
+} cdbg_server_params;
+
+typedef struct cdbg_request_result {
+    int32_t status;              /* 0, or < 0 with `error` set */
+    const char* error;
+    /* owned by the server until cdbg_server_release */
+    const uint8_t* frag_bytes;   /* frag_unitigs.bin contents */
+    uint64_t frag_nbytes;
+    const uint64_t* class_words; /* .color_sets bit-vector words */
+    uint64_t class_bits;
+    const uint64_t* class_offsets;
+    uint64_t n_color_sets;
+    uint64_t total_integers, n_kmers, n_distinct, n_fragments;
+    uint64_t need_bytes, grant_bytes;   /* estimate and memory granted */
+    double t_submit, t_start, t_done;   /* seconds on the server's clock */
+    double ms_device;                   /* device time of the build */
+} cdbg_request_result;
+
+typedef struct cdbg_server_stats_t {
+    uint64_t completed, failed, waiting;
+    uint32_t running, peak_running;
+    uint64_t reserved_bytes, peak_reserved_bytes;
+    double clock_s;
+} cdbg_server_stats_t;
+
+int cdbg_server_create(const cdbg_server_params* p, cdbg_server** out);
+/* The batch's host buffers must stay valid until the request is done. */
+int cdbg_server_submit(cdbg_server* s, const cdbg_seq_batch* host_batch, const cdbg_build_params* p,
+                       uint64_t* request_id);
+/* Blocks until the request is done. */
+int cdbg_server_wait(cdbg_server* s, uint64_t request_id, cdbg_request_result* out);
+int cdbg_server_release(cdbg_server* s, uint64_t request_id);
+int cdbg_server_stats(cdbg_server* s, cdbg_server_stats_t* out);
+/* Finishes every submitted request, then frees the engines. */
+void cdbg_server_destroy(cdbg_server* s);
+const char* cdbg_server_last_error(void);
 
 /* Copy `bytes` from a device pointer returned by cdbg_gpu_build
  * (outputs_to_host = 0) into host memory, on the engine's stream. */
