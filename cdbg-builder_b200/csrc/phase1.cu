@@ -223,10 +223,17 @@ __global__ void __launch_bounds__(MZ_THREADS)
     __shared__ __align__(16) uint64_t sw[MZ_WMAX];
     __shared__ uint64_t sh[MZ_HMAX];
     __shared__ uint64_t smin[MZ_TT + 1];
-    __shared__ uint32_t sred[MZ_THREADS / 32 + 1];
+    __shared__ uint64_t stab[4][4];  // rotated ntHash seeds, by base
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint64_t s_tile, s_excl;
 
+    if (threadIdx.x < 16) {
+        // [0] seed(b), [1] rol(seed(b), m), [2] ror(seed(b^3), 1), [3] rol(seed(b^3), m-1):
+        // the terms of one rolling step, so the loop below has no variable rotations
+        const uint32_t b = threadIdx.x & 3, j = threadIdx.x >> 2;
+        const uint64_t sb = nt_seed(b), sc = nt_seed(b ^ 3u);
+        stab[j][b] = j == 0 ? sb : j == 1 ? rol64(sb, m) : j == 2 ? ror64(sc, 1) : rol64(sc, m - 1);
+    }
     uint64_t tile = blockIdx.x;
     if (MODE == 2) {
         if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -265,17 +272,16 @@ __global__ void __launch_bounds__(MZ_THREADS)
         const uint32_t q0 = threadIdx.x * per_h;
         const uint32_t q1 = min(q0 + per_h, nh);
         if (q0 < q1) {
+            // first m-mer in Horner form: fwd = xor_i rol(seed(b_i), m-1-i),
+            // rc = xor_i rol(seed(b_i ^ 3), i)
             uint64_t f = 0, rc = 0;
-            for (uint32_t i = 0; i < m; ++i) {
-                const uint32_t b = base_at(q0 + i);
-                f ^= rol64(nt_seed(b), m - 1 - i);
-                rc ^= rol64(nt_seed(b ^ 3u), i);
-            }
+            for (uint32_t i = 0; i < m; ++i) f = rol64(f, 1) ^ stab[0][base_at(q0 + i)];
+            for (uint32_t i = m; i-- > 0;) rc = rol64(rc, 1) ^ stab[0][base_at(q0 + i) ^ 3u];
             sh[q0] = f <= rc ? f : rc;
             for (uint32_t q = q0 + 1; q < q1; ++q) {
                 const uint32_t out = base_at(q - 1), in = base_at(q + m - 1);
-                f = rol64(f, 1) ^ rol64(nt_seed(out), m) ^ nt_seed(in);
-                rc = ror64(rc, 1) ^ ror64(nt_seed(out ^ 3u), 1) ^ rol64(nt_seed(in ^ 3u), m - 1);
+                f = rol64(f, 1) ^ stab[1][out] ^ stab[0][in];
+                rc = ror64(rc, 1) ^ stab[2][out] ^ stab[3][in];
                 sh[q] = f <= rc ? f : rc;
             }
         }
@@ -317,18 +323,42 @@ __global__ void __launch_bounds__(MZ_THREADS)
         }
     }
     __syncthreads();
-    // cut points j in [j0, j1): j == 0 or min(j) != min(j - 1)
+    // cut points j in [j0, j1): j == 0 or min(j) != min(j - 1).  Position c
+    // of the tile is handled in round c / MZ_THREADS by thread c % MZ_THREADS
+    // (consecutive threads read consecutive smin words: no bank conflicts);
+    // outputs keep position order through per-(round, warp) counts.
     const uint32_t off = (uint32_t)(j0 - e0);  // 0 or 1
     const uint32_t ncut = (uint32_t)(j1 - j0);
-    const uint32_t c0 = threadIdx.x * MZ_PER;
-    uint32_t cnt = 0;
-    for (uint32_t c = c0; c < c0 + MZ_PER && c < ncut; ++c) {
-        const uint64_t j = j0 + c;
-        const uint32_t q = c + off;
-        if (j == 0 || smin[q] != smin[q - 1]) ++cnt;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = MZ_THREADS / 32;
+    __shared__ uint32_t wcnt[MZ_PER * NW + 1];
+    uint32_t myflags = 0, myrank[MZ_PER];
+#pragma unroll
+    for (int rr = 0; rr < MZ_PER; ++rr) {
+        const uint32_t c = (uint32_t)rr * MZ_THREADS + threadIdx.x;
+        bool f = false;
+        if (c < ncut) {
+            const uint32_t q = c + off;
+            f = (j0 + c == 0) || smin[q] != smin[q - 1];
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, f);
+        myrank[rr] = __popc(bal & lanemask_lt());
+        if (f) myflags |= 1u << rr;
+        if (lane == 0) wcnt[rr * NW + warp] = __popc(bal);
     }
-    uint32_t tot;
-    const uint32_t ex = prim::block_exclusive_scan<uint32_t, MZ_THREADS>(cnt, sred, tot);
+    __syncthreads();
+    // exclusive prefix over (round, warp) in position order
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int i = 0; i < MZ_PER * NW; ++i) {
+            const uint32_t v = wcnt[i];
+            wcnt[i] = run;
+            run += v;
+        }
+        wcnt[MZ_PER * NW] = run;
+    }
+    __syncthreads();
+    const uint32_t tot = wcnt[MZ_PER * NW];
     if (MODE == 0) {
         if (threadIdx.x == 0) tile_count[tile] = tot;
         return;
@@ -371,17 +401,15 @@ __global__ void __launch_bounds__(MZ_THREADS)
         base = s_excl;
         if (base == ~0ull) return;
     }
-    uint64_t o = base + ex;
-    for (uint32_t c = c0; c < c0 + MZ_PER && c < ncut; ++c) {
-        const uint64_t j = j0 + c;
-        const uint32_t q = c + off;
-        if (j == 0 || smin[q] != smin[q - 1]) {
-            if (MODE == 1 || o < cap) {
-                out_min[o] = smin[q];
-                out_run[o] = r;
-                out_a[o] = (uint32_t)j;
-            }
-            ++o;
+#pragma unroll
+    for (int rr = 0; rr < MZ_PER; ++rr) {
+        if (!((myflags >> rr) & 1u)) continue;
+        const uint32_t c = (uint32_t)rr * MZ_THREADS + threadIdx.x;
+        const uint64_t o = base + wcnt[rr * NW + warp] + myrank[rr];
+        if (MODE == 1 || o < cap) {
+            out_min[o] = smin[c + off];
+            out_run[o] = r;
+            out_a[o] = (uint32_t)(j0 + c);
         }
     }
 }
