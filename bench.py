@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch-occ", type=int, default=0)
+    ap.add_argument("--autotune", action="store_true",
+                    help="run the autotuner on the workload before timing (default for skewed)")
+    ap.add_argument("--compare-plain", action="store_true",
+                    help="also time one step of the plain one-bucket-per-batch path (default for skewed)")
     ap.add_argument("--out", default="")
     # serving workload
     ap.add_argument("--requests", type=int, default=48, help="serving: requests in the stream")
@@ -146,9 +150,15 @@ def run_reference_sample(genomes, k, blog2, threads, seed, workdir):
     return kmers, t1 + t2, {"bucket_write_s": t1, "bucket_process_s": t2}
 
 
-def workload_name(n_genomes, k, B):
-    return ("pangenome: %d genomes x 4.8 Mbp (0.1-2%% SNPs, 1-200 contigs), k=%d, m=12, %d buckets"
-            % (n_genomes, k, B))
+def workload_name(n_genomes, k, B, workload="pangenome"):
+    from cdbg_gpu.native import best_m
+    shape = {
+        "pangenome": "%d genomes x 4.8 Mbp (0.1-2%% SNPs, 1-200 contigs)",
+        "small": "%d genomes x 5.0 Mbp (0.5%% SNPs, 20 indels, 1-3 contigs)",
+        "largek": "%d genomes x 4.8 Mbp + 2%% tandem repeats + 200 shared 1-5 kbp repeats each",
+        "skewed": "%d genomes x 1-6 Mbp log-uniform, 10%% homopolymer/dinucleotide runs",
+    }.get(workload, "%d genomes")
+    return "%s: %s, k=%d, m=%d, %d buckets" % (workload, shape % n_genomes, k, best_m(k), B)
 
 
 def reference_arm(a):
@@ -233,8 +243,16 @@ def main_gpu(a):
     eng = native.Engine(local)
     eng.set_stream(stream.cuda_stream)
 
-    def step(batch, to_host):
-        return eng.build(batch, k, B, n_genomes, batch_occ=a.batch_occ, outputs_to_host=to_host)
+    def step(batch, to_host, batch_occ=None):
+        return eng.build(batch, k, B, n_genomes, batch_occ=a.batch_occ if batch_occ is None else batch_occ,
+                         outputs_to_host=to_host)
+
+    skewed = a.workload == "skewed"
+    tuned = None
+    if a.autotune or skewed:
+        t0 = time.time()
+        tcfg, tms = eng.autotune(dev_batch, k, B, n_genomes)
+        tuned = {"tuning": tcfg, "best_ms": tms, "seconds": time.time() - t0}
 
     for _ in range(a.warmup):
         r = step(dev_batch, False)
@@ -287,6 +305,20 @@ def main_gpu(a):
         e2e = {"value": world * kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
                "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes)}
 
+    # ---- plain path: one bucket per batch (one launch sequence per bucket)
+    plain = None
+    if a.compare_plain or skewed:
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        rp = step(dev_batch, False, batch_occ=1)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        plain = {"ms_per_step": pms, "value": kmers / (pms / 1000.0), "phase_ms": {"phase1": rp.ms_phase1,
+                                                                                   "phase2": rp.ms_phase2},
+                 "batched_over_plain": pms / ms}
+
     # ---- roofline: the dominant kernel with an algorithmic-bytes figure, and
     # the whole phase-1 + phase-2 path
     peak, peak_kind = peaks()
@@ -327,8 +359,8 @@ def main_gpu(a):
         top = sorted(kstats.items(), key=lambda kv: -kv[1][0])[:20]
         line = {"metric": "phase1+2 k-mers/s", "value": value, "unit": "k-mers/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-                "config": {"workload": workload_name(n_genomes, k, B),
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64" if k <= 31 else "u128", "data": "synthetic",
+                "config": {"workload": workload_name(n_genomes, k, B, a.workload),
                            "kmers_per_step": kmers, "bases": int(seq.nbytes),
                            "l2": "inputs (%.1f GB) larger than L2" % (seq.nbytes / 1e9),
                            "parallelism": "replicas%d" % world, "generate_s": gen_s},
@@ -337,6 +369,7 @@ def main_gpu(a):
                            "color_sets": int(r.n_color_sets), "frag_bytes": int(r.frag_nbytes)},
                 "phase_ms": {"phase1": r.ms_phase1, "phase2": r.ms_phase2},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "autotune": tuned, "plain": plain,
                 "clocks": clocks,
                 "kernels_ms_per_step": {kname: round(v[0] / a.steps, 3) for kname, v in top}}
         s = json.dumps(line)

@@ -86,6 +86,11 @@ class BuildResult(ctypes.Structure):
                 ("ms_total", ctypes.c_double)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("batch_occ", ctypes.c_uint64), ("minimizer_tile", ctypes.c_uint32),
+                ("heavy_colors", ctypes.c_uint32)]
+
+
 class ServerParams(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
                 ("bytes_per_base", ctypes.c_double), ("floor_bytes", ctypes.c_uint64)]
@@ -144,6 +149,11 @@ SIGNATURES = {
     "cdbg_engine_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "cdbg_engine_memory": (ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p]),
     "cdbg_engine_trim": (ctypes.c_int, [ctypes.c_void_p]),
+    "cdbg_engine_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    "cdbg_engine_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    "cdbg_engine_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch), ctypes.POINTER(BuildParams),
+                                            ctypes.c_uint32, ctypes.POINTER(Tuning),
+                                            ctypes.POINTER(ctypes.c_double)]),
     "cdbg_server_create": (ctypes.c_int, [ctypes.POINTER(ServerParams), ctypes.POINTER(ctypes.c_void_p)]),
     "cdbg_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
                                           ctypes.POINTER(BuildParams), c_u64p]),
@@ -278,6 +288,23 @@ class Engine:
         a, b = ctypes.c_uint64(), ctypes.c_uint64()
         _check(lib().cdbg_engine_memory(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0):
+        _check(lib().cdbg_engine_set_tuning(self._h, ctypes.byref(Tuning(batch_occ, minimizer_tile, heavy_colors))))
+
+    def tuning(self):
+        t = Tuning()
+        _check(lib().cdbg_engine_get_tuning(self._h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+
+    def autotune(self, batch, k, num_buckets, num_colors, m=0, rounds=1):
+        """Search the performance knobs on `batch`; the engine keeps the best.
+        Returns (tuning dict, best device ms)."""
+        p = BuildParams(k, m, num_buckets, num_colors, 0, 0)
+        t, ms = Tuning(), ctypes.c_double()
+        _check(lib().cdbg_engine_autotune(self._h, ctypes.byref(batch), ctypes.byref(p), rounds, ctypes.byref(t),
+                                          ctypes.byref(ms)))
+        return {k2: getattr(t, k2) for k2, _ in Tuning._fields_}, ms.value
 
     def trim(self):
         """Return cached device memory to the device pool."""

@@ -388,7 +388,7 @@ int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, ui
         cdbg::run_table rt;
         cdbg::build_runs(in, k, e->A, e->st, rt, e->A);
         cdbg::super_list sl;
-        cdbg::find_supers(rt, k, m, num_buckets, e->A, e->st, sl, e->d_err);
+        cdbg::find_supers(rt, k, m, num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile);
         cdbg::check_device_error(e, "super-k-mers");
         const uint64_t n = sl.n;
         std::vector<uint64_t> start(n), words(rt.nwords);
@@ -482,7 +482,7 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
             cdbg::run_table rt;
             cdbg::build_runs(in, k, e->A, e->st, rt, e->A);
             cdbg::super_list sl;
-            cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err);
+            cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile);
             cdbg::record_set rs;
             cdbg::build_records(rt, sl, k, a->num_buckets, e->A, e->st, rs, e->d_err, e->A);
             cdbg::serialized_buckets sb;
@@ -560,7 +560,8 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         cdbg::phase2_params pp;
         pp.k = a->k;
         pp.num_colors = a->num_colors;
-        pp.batch_occ = a->batch_occ;
+        pp.batch_occ = a->batch_occ ? a->batch_occ : e->tune.batch_occ;
+        pp.heavy_colors = e->tune.heavy_colors;
         pp.to_host = true;
         cdbg::phase2_result res;
         res.state = &e->p2;
@@ -630,7 +631,7 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         cdbg::run_table rt;
         cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
         cdbg::super_list sl;
-        cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err);
+        cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile);
         cdbg::record_set rs;
         cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
         unsigned long long* d_rec_bytes = e->P.alloc<unsigned long long>(1);
@@ -642,7 +643,8 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         cdbg::phase2_params pp;
         pp.k = k;
         pp.num_colors = p->num_colors;
-        pp.batch_occ = p->batch_occ;
+        pp.batch_occ = p->batch_occ ? p->batch_occ : e->tune.batch_occ;
+        pp.heavy_colors = e->tune.heavy_colors;
         pp.to_host = false;  // outputs accumulate in HBM; one D2H at the end when asked
         cdbg::phase2_result out;
         out.state = &e->p2;
@@ -695,6 +697,89 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         return 0;
     } catch (std::exception const& ex) {
         if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
+int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
+    if (!e || !t) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    cdbg_tuning v = *t;
+    if (v.minimizer_tile == 0) v.minimizer_tile = 2048;
+    if (v.heavy_colors == 0) v.heavy_colors = 64;
+    if (v.minimizer_tile != 1024 && v.minimizer_tile != 2048) {
+        g_last_error = "minimizer_tile must be 1024 or 2048";
+        return -1;
+    }
+    e->tune = v;
+    return 0;
+}
+
+int cdbg_engine_get_tuning(cdbg_engine* e, cdbg_tuning* t) {
+    if (!e || !t) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    *t = e->tune;
+    return 0;
+}
+
+int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p, uint32_t rounds,
+                         cdbg_tuning* best, double* best_ms) {
+    if (!e || !b || !p) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    try {
+        if (rounds == 0) rounds = 1;
+        cdbg_build_params q = *p;
+        q.batch_occ = 0;  // the tuned split threshold applies
+        q.outputs_to_host = 0;
+        // best of `rounds` device times of one configuration
+        auto measure = [&](cdbg_tuning const& t) {
+            e->tune = t;
+            double v = 1e300;
+            for (uint32_t r = 0; r < rounds; ++r) {
+                cdbg_build_result res{};
+                if (cdbg_gpu_build(e, b, &q, &res) != 0) throw std::runtime_error(g_last_error);
+                v = std::min(v, res.ms_total);
+            }
+            return v;
+        };
+        cdbg_tuning cur = e->tune;
+        if (cur.minimizer_tile == 0) cur.minimizer_tile = 2048;
+        if (cur.heavy_colors == 0) cur.heavy_colors = 64;
+        measure(cur);  // warm-up: allocations reach their working sizes
+        double cur_ms = measure(cur);
+        auto consider = [&](cdbg_tuning const& t) {
+            const double ms = measure(t);
+            if (ms < cur_ms * 0.99) {  // keep only a clear gain
+                cur = t;
+                cur_ms = ms;
+            }
+        };
+        for (uint64_t v : {uint64_t(1) << 27, uint64_t(1) << 26, uint64_t(1) << 25, uint64_t(1) << 24}) {
+            cdbg_tuning t = cur;
+            t.batch_occ = v;
+            if (t.batch_occ != cur.batch_occ) consider(t);
+        }
+        for (uint32_t v : {1024u, 2048u}) {
+            cdbg_tuning t = cur;
+            t.minimizer_tile = v;
+            if (t.minimizer_tile != cur.minimizer_tile) consider(t);
+        }
+        for (uint32_t v : {16u, 32u, 64u, 128u, 256u}) {
+            cdbg_tuning t = cur;
+            t.heavy_colors = v;
+            if (t.heavy_colors != cur.heavy_colors) consider(t);
+        }
+        e->tune = cur;
+        if (best) *best = cur;
+        if (best_ms) *best_ms = cur_ms;
+        return 0;
+    } catch (std::exception const& ex) {
         return fail(ex);
     }
 }

@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "cdbg_gpu.h"
 #include "arena.cuh"
 #include "common.cuh"
 #include "phase2.cuh"
@@ -43,6 +44,7 @@ struct cdbg_engine {
     cdbg::phase2_state p2;
     uint32_t* d_err = nullptr;  // device error word (outside the arena)
     uint64_t mem_limit = 0;     // device memory cap of this engine (0 = none)
+    cdbg_tuning tune{0, 2048, 64};
     // host copies of the last cdbg_gpu_build's outputs (outputs_to_host = 1)
     pinned_buffer h_frag, h_words, h_offsets;
 };

@@ -163,10 +163,7 @@ __global__ void k_pack(uint8_t const* __restrict__ ascii, uint32_t nruns,
 
 // ------------------------------------------------------------ minimizer tile
 constexpr int MZ_THREADS = 256;
-constexpr int MZ_TT = 2048;                 // (k-1)-mers per tile
-constexpr int MZ_PER = MZ_TT / MZ_THREADS;  // 8
-constexpr int MZ_HMAX = MZ_TT + 1 + 64;     // m-mer hashes (W <= 62)
-constexpr int MZ_WMAX = (MZ_TT + 256) / 32 + 4;
+constexpr int MZ_TT = 2048;  // default (k-1)-mers per tile
 
 __device__ __forceinline__ uint32_t smem_u32(void const* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -211,7 +208,7 @@ __device__ __forceinline__ bool tma_load_1d(void* smem_dst, void const* gsrc, ui
 // tile_counter, publish their count in `status` and read their predecessors'
 // prefix (decoupled look-back, bounded waits), then write at most `cap`
 // entries; the grand total ends in the last tile's status.
-template <int MODE>
+template <int MODE, int TT = MZ_TT>
 __global__ void __launch_bounds__(MZ_THREADS)
     k_minimizers(uint32_t nruns, uint64_t const* __restrict__ tile_start,
                  uint64_t const* __restrict__ soff, uint32_t const* __restrict__ len,
@@ -220,9 +217,12 @@ __global__ void __launch_bounds__(MZ_THREADS)
                  uint64_t* __restrict__ out_min, uint32_t* __restrict__ out_run,
                  uint32_t* __restrict__ out_a, uint32_t* err, uint32_t* tile_counter = nullptr,
                  unsigned long long* status = nullptr, uint64_t ntiles = 0, uint64_t cap = 0) {
+    constexpr int MZ_PER = TT / MZ_THREADS;       // (k-1)-mers per thread
+    constexpr int MZ_HMAX = TT + 1 + 64;          // m-mer hashes (W <= 62)
+    constexpr int MZ_WMAX = (TT + 256) / 32 + 4;  // 2-bit words staged
     __shared__ __align__(16) uint64_t sw[MZ_WMAX];
     __shared__ uint64_t sh[MZ_HMAX];
-    __shared__ uint64_t smin[MZ_TT + 1];
+    __shared__ uint64_t smin[TT + 1];
     __shared__ uint64_t stab[4][4];  // rotated ntHash seeds, by base
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint64_t s_tile, s_excl;
@@ -246,8 +246,8 @@ __global__ void __launch_bounds__(MZ_THREADS)
     const uint32_t L = len[r];
     const uint32_t W = k - m;
     const uint64_t nk1 = (uint64_t)L - k + 2;  // (k-1)-mers 0..K
-    const uint64_t j0 = t_local * MZ_TT;
-    const uint64_t j1 = (j0 + MZ_TT < nk1) ? j0 + MZ_TT : nk1;
+    const uint64_t j0 = t_local * TT;
+    const uint64_t j1 = (j0 + TT < nk1) ? j0 + TT : nk1;
     const uint64_t e0 = j0 ? j0 - 1 : 0;
     const uint32_t nmin = (uint32_t)(j1 - e0);
     const uint32_t nh = nmin + W - 1;
@@ -414,12 +414,12 @@ __global__ void __launch_bounds__(MZ_THREADS)
     }
 }
 
-__global__ void k_run_tiles(uint32_t nruns, uint32_t const* __restrict__ len, uint32_t k,
+__global__ void k_run_tiles(uint32_t nruns, uint32_t const* __restrict__ len, uint32_t k, uint32_t tt,
                             uint64_t* __restrict__ ntiles) {
     uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nruns) return;
     const uint64_t nk1 = (uint64_t)len[r] - k + 2;
-    ntiles[r] = (nk1 + MZ_TT - 1) / MZ_TT;
+    ntiles[r] = (nk1 + tt - 1) / tt;
 }
 
 __global__ void k_run_kmers(uint32_t nruns, uint32_t const* __restrict__ len, uint32_t k,
@@ -766,15 +766,30 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
     rt.n_bases = h[1];
 }
 
+template <int TT>
+void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
+                    cudaStream_t st, super_list& out, uint32_t* d_err);
+
 void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
-                 cudaStream_t st, super_list& out, uint32_t* d_err) {
+                 cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile) {
+    if (tile == 1024)
+        find_supers_tt<1024>(rt, k, m, B, A, st, out, d_err);
+    else if (tile == 2048 || tile == 0)
+        find_supers_tt<2048>(rt, k, m, B, A, st, out, d_err);
+    else
+        throw std::runtime_error("minimizer tile must be 1024 or 2048");
+}
+
+template <int TT>
+void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
+                    cudaStream_t st, super_list& out, uint32_t* d_err) {
     out = super_list();
     if (rt.n == 0) return;
     if (k < 2 || m >= k || k - m > 62 || m > 32)
         throw std::runtime_error("unsupported k/m combination");
     uint64_t* ntl = A.alloc<uint64_t>(rt.n);
     uint64_t* tstart = A.alloc<uint64_t>(rt.n + 1);
-    k_run_tiles<<<grid(rt.n, 256), 256, 0, st>>>(rt.n, rt.len, k, ntl);
+    k_run_tiles<<<grid(rt.n, 256), 256, 0, st>>>(rt.n, rt.len, k, TT, ntl);
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint64_t, uint64_t>(ntl, tstart, rt.n, A, st, tstart + rt.n);
     const uint64_t ntiles = read_dev(tstart + rt.n, st);
@@ -791,7 +806,7 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
     CDBG_CUDA(cudaMemsetAsync(counter, 0, 4, st));
     {
         CDBG_PROF("k_minimizers", st);
-        k_minimizers<2><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(rt.n, tstart, rt.soff, rt.len, rt.words, k, m,
+        k_minimizers<2, TT><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(rt.n, tstart, rt.soff, rt.len, rt.words, k, m,
                                                                  nullptr, nullptr, minv, run, aa, d_err, counter,
                                                                  status, ntiles, cap);
     }
@@ -802,7 +817,7 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
         uint64_t* toff = A.alloc<uint64_t>(ntiles + 1);
         {
             CDBG_PROF("k_minimizers", st);
-            k_minimizers<0><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+            k_minimizers<0, TT><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
                 rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, nullptr, nullptr, nullptr, nullptr, d_err);
         }
         CDBG_CHECK_LAUNCH();
@@ -813,7 +828,7 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
         aa = A.alloc<uint32_t>(n);
         {
             CDBG_PROF("k_minimizers", st);
-            k_minimizers<1><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+            k_minimizers<1, TT><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
                 rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, toff, minv, run, aa, d_err);
         }
         CDBG_CHECK_LAUNCH();
@@ -1116,7 +1131,7 @@ extern "C" int cdbg_gpu_supers_noalloc(const uint64_t* words, const uint64_t* ru
         noalloc_scratch* s = noalloc_scratch_ptr();
         CDBG_CUDA(cudaMemsetAsync(&s->err, 0, sizeof(uint32_t), st));
         if (num_runs == 0) return 0;
-        k_run_tiles<<<grid(num_runs, 256), 256, 0, st>>>(num_runs, run_len, k, s->run_tiles);
+        k_run_tiles<<<grid(num_runs, 256), 256, 0, st>>>(num_runs, run_len, k, MZ_TT, s->run_tiles);
         CDBG_CHECK_LAUNCH();
         k_noalloc_scan<uint64_t><<<1, 1024, 0, st>>>(s->run_tiles, num_runs, s->tile_start);
         CDBG_CHECK_LAUNCH();

@@ -67,8 +67,9 @@ struct super_list {
     uint32_t* bucket = nullptr;
     uint64_t* key = nullptr;
 };
+// `tile` = (k-1)-mers per minimizer tile: 1024 or 2048 (0 = 2048).
 void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
-                 cudaStream_t st, super_list& out, uint32_t* d_err);
+                 cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile = 0);
 
 // Dedup super-k-mers into canonical bucket records.
 // Record arrays come from `out`, temporaries from A.

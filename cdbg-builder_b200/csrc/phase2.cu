@@ -78,8 +78,28 @@ __device__ __forceinline__ uint32_t upper_bound_u64(uint64_t const* a, uint64_t 
 }
 
 // ------------------------------------------------------------------ set hash
-__host__ __device__ __forceinline__ uint64_t elem_mix(uint32_t c) {
-    return mix64((uint64_t)c * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL);
+// Order-independent hash of a color set: the sum, over the 32-color words
+// that hold at least one color, of a mix of (word index, word bits), then
+// mixed with the set size.  A list and a bitmap of the same set hash alike;
+// one mix per nonzero word instead of one per color.
+__host__ __device__ __forceinline__ uint64_t word_mix(uint32_t w, uint32_t bits) {
+    return mix64((((uint64_t)w << 32) | bits) * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL);
+}
+// Sum of word_mix over an ascending color list.
+__host__ __device__ __forceinline__ uint64_t list_word_sum(uint32_t const* c, uint64_t n) {
+    uint64_t acc = 0;
+    uint32_t cw = 0xffffffffu, bits = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint32_t v = c[i], w = v >> 5;
+        if (w != cw) {
+            if (bits) acc += word_mix(cw, bits);
+            cw = w;
+            bits = 0;
+        }
+        bits |= 1u << (v & 31);
+    }
+    if (bits) acc += word_mix(cw, bits);
+    return acc;
 }
 __host__ __device__ __forceinline__ uint64_t set_hash_final(uint64_t acc, uint64_t n) {
     uint64_t h = mix64(acc ^ (n * 0xD6E8FEB86659FD93ULL));
@@ -267,10 +287,8 @@ __global__ void k_rec_prep(uint64_t n, uint32_t const* __restrict__ len, uint32_
     const uint32_t l = len[r];
     nk[r] = l >= k ? (uint64_t)(l - k + 1) : 0;
     rbucket[r] = upper_bound_u64(bstart, (uint64_t)B + 1, r) - 1;
-    uint64_t acc = 0;
     const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
-    for (uint64_t c = c0; c < c1; ++c) acc += elem_mix(colors[c]);
-    rhash[r] = set_hash_final(acc, c1 - c0);
+    rhash[r] = set_hash_final(list_word_sum(colors + c0, c1 - c0), c1 - c0);
 }
 
 __global__ void k_gather_u64(uint64_t n, uint64_t const* __restrict__ src,
@@ -483,12 +501,7 @@ __global__ void k_union(uint64_t M, uint64_t const* __restrict__ moff, uint64_t 
     for (uint32_t w = w0; w < w1; ++w) {
         uint32_t x = bm[w];
         cnt += __popc(x);
-        if (!WRITE)
-            while (x) {
-                const uint32_t b = __ffs(x) - 1;
-                x &= x - 1;
-                acc += elem_mix(w * 32 + b);
-            }
+        if (!WRITE && x) acc += word_mix(w, x);
     }
     uint32_t total;
     const uint32_t ex = warp_excl_scan32(cnt, total);
@@ -512,14 +525,13 @@ __global__ void k_union(uint64_t M, uint64_t const* __restrict__ moff, uint64_t 
 }
 
 // ---- multi-record unions as bitmaps -----------------------------------------
-constexpr uint32_t HEAVY_COLORS = 64;  // records with at least this many colors get a bitmap
-
+// Records with at least `heavy` colors get a bitmap.
 __global__ void k_heavy_flags(uint64_t nu, uint64_t const* __restrict__ upairs, uint64_t const* __restrict__ col_off,
-                              uint32_t R0, uint32_t* __restrict__ flag) {
+                              uint32_t R0, uint32_t heavy, uint32_t* __restrict__ flag) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nu) return;
     const uint32_t r = (uint32_t)(upairs[i] & 0xffffffffu);
-    if (col_off[r + 1] - col_off[r] >= HEAVY_COLORS) flag[r - R0] = 1u;
+    if (col_off[r + 1] - col_off[r] >= heavy) flag[r - R0] = 1u;
 }
 
 // Warp per heavy record: its colors as a bitmap in rbits[hpos[r - R0] * nw].
@@ -577,14 +589,10 @@ __global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ moff, uint64
     uint64_t acc = 0;
     uint32_t* out = mbits + m * (uint64_t)nw;
     for (uint32_t w = lane; w < nw; w += 32) {
-        uint32_t x = bm[w];
+        const uint32_t x = bm[w];
         out[w] = x;
         cnt += __popc(x);
-        while (x) {
-            const uint32_t b = __ffs(x) - 1;
-            x &= x - 1;
-            acc += elem_mix(w * 32 + b);
-        }
+        if (x) acc += word_mix(w, x);
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     acc = warp_sum64(acc);
@@ -1803,7 +1811,8 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             uint32_t* hflag = A.alloc<uint32_t>(nrec);
             uint64_t* hpos = A.alloc<uint64_t>(nrec + 1);
             CDBG_CUDA(cudaMemsetAsync(hflag, 0, 4 * nrec, st));
-            k_heavy_flags<<<grid(nu, 256), 256, 0, st>>>(nu, upairs, R.col_off, (uint32_t)R0, hflag);
+            k_heavy_flags<<<grid(nu, 256), 256, 0, st>>>(nu, upairs, R.col_off, (uint32_t)R0,
+                                                          std::max<uint32_t>(1, p.heavy_colors), hflag);
             CDBG_CHECK_LAUNCH();
             prim::exclusive_scan<uint32_t, uint64_t>(hflag, hpos, nrec, A, st, hpos + nrec);
             const uint64_t nheavy = read_dev(hpos + nrec, st);

@@ -74,6 +74,9 @@ struct phase2_params {
     // multi-record color unions as C-bit bitmaps (else as lists; bitmaps cost
     // C/8 bytes per such k-mer, so very large color counts use lists)
     bool union_bitmaps = true;
+    // records with at least this many colors get a precomputed bitmap in
+    // multi-record unions (performance only)
+    uint32_t heavy_colors = 64;
 };
 
 // Run phase 2 over all buckets of `rs` (records grouped by bucket).

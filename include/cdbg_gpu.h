@@ -48,6 +48,20 @@ int cdbg_gpu_version(void);
  * (CPU only); measurement plumbing. */
 int cdbg_engine_set_stream(cdbg_engine* e, void* stream);
 
+/* Performance knobs of an engine; none changes any output.  Zero fields
+ * take the defaults. */
+typedef struct cdbg_tuning {
+    uint64_t batch_occ;        /* phase-2 k-mer occurrences per bucket batch: the
+                                  threshold at which consecutive buckets split
+                                  into another batch (0 = from free HBM) */
+    uint32_t minimizer_tile;   /* (k-1)-mers per minimizer tile: 1024 or 2048 */
+    uint32_t heavy_colors;     /* records with >= this many colors get a bitmap
+                                  in multi-record unions (default 64) */
+} cdbg_tuning;
+
+int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t);
+int cdbg_engine_get_tuning(cdbg_engine* e, cdbg_tuning* t);
+
 /* Kernel launches issued by this library in this process so far. */
 uint64_t cdbg_launch_count(void);
 
@@ -192,6 +206,14 @@ typedef struct cdbg_build_result {
 
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
                    cdbg_build_result* r);
+
+/* Autotuner: builds `b` repeatedly, searching the knobs of cdbg_tuning one at
+ * a time (batch split threshold, minimizer tile, heavy-record threshold) and
+ * keeping each value that lowers the best of `rounds` device times; the
+ * engine keeps the winner.  Every trial's outputs are identical (the knobs
+ * are performance-only).  No counterpart in the reference. */
+int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
+                         uint32_t rounds, cdbg_tuning* best, double* best_ms);
 
 /* Super-k-mers of pre-packed ACGT runs for callers that cannot allocate
  * device memory.  No counterpart in the reference (which has no GPU path).
