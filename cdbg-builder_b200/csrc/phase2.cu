@@ -444,6 +444,44 @@ __global__ void k_multi_index(uint64_t n, uint64_t const* __restrict__ a, uint32
     n_rec[node] = MULTI_TAG | (uint32_t)m;
 }
 
+// Multi-record nodes in node order whose owning-record list equals the
+// previous one's (the k-mers of a stretch shared by the same records) share
+// one union: ghead[m] = 1 starts a new group.
+__global__ void k_multi_same(uint64_t M, uint64_t const* __restrict__ moff, uint64_t const* __restrict__ upairs,
+                             uint32_t* __restrict__ ghead) {
+    uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    bool same = false;
+    if (m > 0) {
+        const uint64_t a0 = moff[m - 1], a1 = moff[m], b1 = moff[m + 1];
+        if (a1 - a0 == b1 - a1) {
+            same = true;
+            for (uint64_t i = 0; i < a1 - a0; ++i)
+                if ((uint32_t)upairs[a0 + i] != (uint32_t)upairs[a1 + i]) {
+                    same = false;
+                    break;
+                }
+        }
+    }
+    ghead[m] = same ? 0u : 1u;
+}
+
+// Group g (of its head node m): node, record range; every multi node's group.
+__global__ void k_multi_groups(uint64_t M, uint32_t const* __restrict__ ghead, uint64_t const* __restrict__ gpos,
+                               uint32_t const* __restrict__ mnode, uint64_t const* __restrict__ moff,
+                               uint32_t* __restrict__ gnode, uint64_t* __restrict__ gbeg, uint64_t* __restrict__ gend,
+                               uint32_t* __restrict__ mgrp) {
+    uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const uint64_t g = gpos[m] + ghead[m] - 1;
+    mgrp[m] = (uint32_t)g;
+    if (ghead[m]) {
+        gnode[g] = mnode[m];
+        gbeg[g] = moff[m];
+        gend[g] = moff[m + 1];
+    }
+}
+
 // Warp-level helpers over a per-warp shared-memory bitmap of C bits.
 __device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
     for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -473,7 +511,8 @@ __device__ __forceinline__ uint64_t warp_excl_scan64(uint64_t v, uint64_t& total
 // Union of the color lists of a multi-record node.  Pass 0: size and hash;
 // pass 1: write the ascending list at pool[poff[m]].
 template <bool WRITE>
-__global__ void k_union(uint64_t M, uint64_t const* __restrict__ moff, uint64_t const* __restrict__ upairs,
+__global__ void k_union(uint64_t M, uint64_t const* __restrict__ mbeg, uint64_t const* __restrict__ mend,
+                        uint64_t const* __restrict__ upairs,
                         uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors,
                         uint32_t C, uint32_t* __restrict__ msize, uint64_t* __restrict__ mhash,
                         uint64_t const* __restrict__ poff, uint32_t* __restrict__ pool) {
@@ -485,7 +524,7 @@ __global__ void k_union(uint64_t M, uint64_t const* __restrict__ moff, uint64_t 
     if (m >= M) return;
     for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
     __syncwarp();
-    for (uint64_t p = moff[m]; p < moff[m + 1]; ++p) {
+    for (uint64_t p = mbeg[m]; p < mend[m]; ++p) {
         const uint32_t r = (uint32_t)(upairs[p] & 0xffffffffu);
         const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
         for (uint64_t c = c0 + lane; c < c1; c += 32) {
@@ -557,7 +596,8 @@ __global__ void k_heavy_bitmaps(uint64_t nrec, uint32_t const* __restrict__ flag
 
 // Warp per multi-record node: OR of its records' color sets (bitmap words for
 // heavy records, per-color bits for the rest) -> mbits, size, set hash.
-__global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ moff, uint64_t const* __restrict__ upairs,
+__global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ mbeg, uint64_t const* __restrict__ mend,
+                           uint64_t const* __restrict__ upairs,
                            uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors, uint32_t R0,
                            uint32_t const* __restrict__ hflag, uint64_t const* __restrict__ hpos,
                            uint32_t const* __restrict__ rbits, uint32_t nw, uint32_t* __restrict__ mbits,
@@ -569,7 +609,7 @@ __global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ moff, uint64
     if (m >= M) return;
     for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
     __syncwarp();
-    for (uint64_t p = moff[m]; p < moff[m + 1]; ++p) {
+    for (uint64_t p = mbeg[m]; p < mend[m]; ++p) {
         const uint32_t r = (uint32_t)(upairs[p] & 0xffffffffu);
         if (hflag[r - R0]) {
             uint32_t const* rb = rbits + hpos[r - R0] * (uint64_t)nw;
@@ -1043,13 +1083,13 @@ __global__ void k_append_bits(uint64_t nnew, uint32_t const* __restrict__ rcand,
 }
 
 __global__ void k_node_cid(uint64_t D, uint32_t const* __restrict__ n_rec, uint32_t R0,
-                           uint32_t const* __restrict__ rec_cand, uint64_t mbase,
+                           uint32_t const* __restrict__ rec_cand, uint64_t mbase, uint32_t const* __restrict__ mgrp,
                            uint32_t const* __restrict__ cid, uint32_t* __restrict__ n_cid) {
     uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= D) return;
     const uint32_t r = n_rec[n];
     uint32_t c = NONE32;
-    if (r != NONE32) c = (r & MULTI_TAG) ? cid[mbase + (r & ~MULTI_TAG)] : cid[rec_cand[r - R0]];
+    if (r != NONE32) c = (r & MULTI_TAG) ? cid[mbase + mgrp[r & ~MULTI_TAG]] : cid[rec_cand[r - R0]];
     n_cid[n] = c;
 }
 
@@ -1769,6 +1809,11 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint64_t* poff = nullptr;
     uint32_t* pool = nullptr;
     uint32_t* mbits = nullptr;
+    uint64_t G = 0;              // union groups
+    uint32_t* gnode = nullptr;   // first node of each group
+    uint64_t* gbeg = nullptr;    // record range of each group
+    uint64_t* gend = nullptr;
+    uint32_t* mgrp = nullptr;    // group of each multi node
     if (npairs) {
         uint64_t* pairs = A.alloc<uint64_t>(npairs);
         CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
@@ -1801,8 +1846,23 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         CDBG_CHECK_LAUNCH();
         k_set_u64<<<1, 1, 0, st>>>(moff + M, nu);
         CDBG_CHECK_LAUNCH();
-        msize = A.alloc<uint32_t>(M);
-        mhash = A.alloc<uint64_t>(M);
+        // one union per run of multi nodes with the same owning records
+        {
+            uint32_t* ghead = A.alloc<uint32_t>(M);
+            uint64_t* gpos = A.alloc<uint64_t>(M + 1);
+            k_multi_same<<<grid(M, 256), 256, 0, st>>>(M, moff, upairs, ghead);
+            CDBG_CHECK_LAUNCH();
+            prim::exclusive_scan<uint32_t, uint64_t>(ghead, gpos, M, A, st, gpos + M);
+            G = read_dev(gpos + M, st);
+            gnode = A.alloc<uint32_t>(G);
+            gbeg = A.alloc<uint64_t>(G);
+            gend = A.alloc<uint64_t>(G);
+            mgrp = A.alloc<uint32_t>(M);
+            k_multi_groups<<<grid(M, 256), 256, 0, st>>>(M, ghead, gpos, mnode, moff, gnode, gbeg, gend, mgrp);
+            CDBG_CHECK_LAUNCH();
+        }
+        msize = A.alloc<uint32_t>(G);
+        mhash = A.alloc<uint64_t>(G);
         const uint32_t nw = (C + 31) / 32;
         int wpb = (int)std::max<uint64_t>(1, std::min<uint64_t>(8, (96 * 1024) / (4ull * nw)));
         const size_t shm = (size_t)wpb * nw * 4;
@@ -1827,11 +1887,12 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
                                                                         R.colors, nw, rbits);
             }
             CDBG_CHECK_LAUNCH();
-            mbits = A.alloc<uint32_t>(M * nw + 1);
+            mbits = A.alloc<uint32_t>(G * nw + 1);
             {
                 CDBG_PROF("k_union", st);
-                k_union_bm<<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, (uint32_t)R0,
-                                                                 hflag, hpos, rbits, nw, mbits, msize, mhash);
+                k_union_bm<<<grid(G, wpb), wpb * 32, shm, st>>>(G, gbeg, gend, upairs, R.col_off, R.colors,
+                                                                 (uint32_t)R0, hflag, hpos, rbits, nw, mbits, msize,
+                                                                 mhash);
             }
             CDBG_CHECK_LAUNCH();
         } else {
@@ -1841,18 +1902,18 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             }
             {
                 CDBG_PROF("k_union", st);
-                k_union<false><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize,
-                                                                     mhash, nullptr, nullptr);
+                k_union<false><<<grid(G, wpb), wpb * 32, shm, st>>>(G, gbeg, gend, upairs, R.col_off, R.colors, C,
+                                                                     msize, mhash, nullptr, nullptr);
             }
             CDBG_CHECK_LAUNCH();
-            poff = A.alloc<uint64_t>(M + 1);
-            prim::exclusive_scan<uint32_t, uint64_t>(msize, poff, M, A, st, poff + M);
-            const uint64_t ptot = read_dev(poff + M, st);
+            poff = A.alloc<uint64_t>(G + 1);
+            prim::exclusive_scan<uint32_t, uint64_t>(msize, poff, G, A, st, poff + G);
+            const uint64_t ptot = read_dev(poff + G, st);
             pool = A.alloc<uint32_t>(ptot + 1);
             {
                 CDBG_PROF("k_union", st);
-                k_union<true><<<grid(M, wpb), wpb * 32, shm, st>>>(M, moff, upairs, R.col_off, R.colors, C, msize,
-                                                                    mhash, poff, pool);
+                k_union<true><<<grid(G, wpb), wpb * 32, shm, st>>>(G, gbeg, gend, upairs, R.col_off, R.colors, C,
+                                                                    msize, mhash, poff, pool);
             }
             CDBG_CHECK_LAUNCH();
         }
@@ -1872,7 +1933,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint32_t, uint64_t>(rkeep, rpos, nrec, A, st, rpos + nrec);
     const uint64_t nrc = read_dev(rpos + nrec, st);
-    const uint64_t nc = nrc + M;
+    const uint64_t nc = nrc + G;
     cand_view cv;
     cv.kind_id = A.alloc<uint32_t>(nc + 1);
     cv.first = A.alloc<uint32_t>(nc + 1);
@@ -1880,8 +1941,8 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint32_t* rec_cand = A.alloc<uint32_t>(nrec);
     k_cand_records<<<grid(nrec, 256), 256, 0, st>>>(nrec, (uint32_t)R0, rec_first, rkeep, rpos, d_rhash, cv, rec_cand);
     CDBG_CHECK_LAUNCH();
-    if (M) {
-        k_cand_multi<<<grid(M, 256), 256, 0, st>>>(M, nrc, mnode, mhash, cv);
+    if (G) {
+        k_cand_multi<<<grid(G, 256), 256, 0, st>>>(G, nrc, gnode, mhash, cv);
         CDBG_CHECK_LAUNCH();
     }
     list_src L{R.col_off, R.colors, poff, pool, msize, mbits, (C + 31) / 32};
@@ -2022,7 +2083,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint32_t* n_cid = A.alloc<uint32_t>(D);
     {
         CDBG_PROF("k_node_cid", st);
-        k_node_cid<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_cand, nrc, cid, n_cid);
+        k_node_cid<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_cand, nrc, mgrp, cid, n_cid);
     }
     CDBG_CHECK_LAUNCH();
     // ---- extension masks, links, chains
