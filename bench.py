@@ -69,6 +69,26 @@ def dist_env():
         int(os.environ.get("WORLD_SIZE", "1"))
 
 
+def max_over_ranks(v, world, device):
+    """The largest per-rank value over all ranks (the slowest rank's time)."""
+    return _reduce(v, world, device, "max")
+
+
+def sum_over_ranks(v, world, device):
+    """Per-rank counts summed over all ranks (units the whole job processed)."""
+    return _reduce(v, world, device, "sum")
+
+
+def _reduce(v, world, device, how):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if how == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def count_kmers(lens, k):
     import numpy as np
     l = lens.astype(np.int64)
@@ -278,12 +298,10 @@ def main_gpu(a):
     ms = ev0.elapsed_time(ev1) / a.steps
     kstats = eng.kernel_stats()
     eng.profile(False)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, "cuda")
+    job_kmers = sum_over_ranks(kmers, world, "cuda")  # every rank builds its own seeded collection
     r = res[-1]
-    value = world * kmers / (ms / 1000.0)
+    value = job_kmers / (ms / 1000.0)
 
     # ---- e2e: pinned host buffers in, host outputs out
     e2e = None
@@ -298,11 +316,8 @@ def main_gpu(a):
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / a.steps
-        if world > 1:
-            t = torch.tensor([ems], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": world * kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
+        ems = max_over_ranks(ems, world, "cuda")
+        e2e = {"value": job_kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
                "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes)}
 
     # ---- plain path: one bucket per batch (one launch sequence per bucket)
@@ -361,7 +376,7 @@ def main_gpu(a):
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64" if k <= 31 else "u128", "data": "synthetic",
                 "config": {"workload": workload_name(n_genomes, k, B, a.workload),
-                           "kmers_per_step": kmers, "bases": int(seq.nbytes),
+                           "kmers_per_step": int(job_kmers), "bases": int(seq.nbytes),
                            "l2": "inputs (%.1f GB) larger than L2" % (seq.nbytes / 1e9),
                            "parallelism": "replicas%d" % world, "generate_s": gen_s},
                 "counts": {"supers": int(r.n_supers), "records": int(r.n_records), "occ": int(r.n_occ),
