@@ -402,8 +402,8 @@ def main_gpu(a):
 # units()); probes, extra radix passes and re-reads are overhead, not counted.
 def _per_unit(w):
     return {
-        # 2-bit stream read once (1/4 B per base) + one super-k-mer entry written
-        # (start 8, len 4, color 4, flags 4, bucket 4) per super-k-mer
+        # 2-bit stream read once (1/4 B per base) + one cut entry written per
+        # super-k-mer (minimizer value 8, run 4, position 4)
         "k_minimizers": None,  # two units, see algorithmic_bytes
         # one (k-mer, record) read per occurrence + one table entry per distinct k-mer
         "k_insert": None,
@@ -427,7 +427,7 @@ def units(name, r):
 def algorithmic_bytes(name, r, w, steps, launches):
     """Algorithmic bytes of one launch of `name` (per-unit figure x units)."""
     if name == "k_minimizers":
-        v = r.n_bases / 4.0 + r.n_supers * 24
+        v = r.n_bases / 4.0 + r.n_supers * 16
     elif name == "k_insert":
         v = r.n_occ * (w + 4) + r.n_distinct * (w + 8)
     else:
@@ -450,7 +450,12 @@ def path_algorithmic_bytes(r, w):
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one capture, divided by the units that launch processed) and the summary
 # under profiles/ it comes from.
-TRAFFIC_PER_UNIT = {}
+TRAFFIC_PER_UNIT = {
+    "k_minimizers": (1.695, "profiles/phase12_top_kernels_pangenome40.md"),   # per base
+    "k_insert": (89.389, "profiles/phase12_top_kernels_pangenome40.md"),      # per occurrence
+    "k_ext_mask": (97.356, "profiles/phase12_top_kernels_pangenome40.md"),    # per distinct k-mer
+    "k_frag_write": (3.681, "profiles/phase12_top_kernels_pangenome40.md"),   # per fragment byte
+}
 
 
 # ---------------------------------------------------------------- serving

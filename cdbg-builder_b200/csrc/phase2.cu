@@ -231,9 +231,21 @@ struct occ_window {
     uint64_t occ[OCC_BLOCK + 2];
     uint64_t r0;
 };
+// blk_rec[b] = the record holding occurrence O0 + b * OCC_BLOCK, the first
+// occurrence of block b of the occurrence kernels (thread per record; a
+// record spans at most a few block starts).
+__global__ void k_block_records(uint64_t const* __restrict__ occ, uint64_t R0, uint64_t nrec, uint64_t O0,
+                                uint64_t nblocks, uint32_t* __restrict__ blk_rec) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrec) return;
+    const uint64_t a = occ[R0 + i] - O0, e = occ[R0 + i + 1] - O0;
+    for (uint64_t b = (a + OCC_BLOCK - 1) / OCC_BLOCK; b * OCC_BLOCK < e && b < nblocks; ++b)
+        blk_rec[b] = (uint32_t)(R0 + i);
+}
+
 __device__ __forceinline__ void load_occ_window(occ_window& w, uint64_t const* occ, uint64_t R0, uint64_t nrec,
-                                                uint64_t o_first) {
-    if (threadIdx.x == 0) w.r0 = R0 + upper_bound_u64(occ + R0, nrec + 1, o_first) - 1;
+                                                uint32_t const* __restrict__ blk_rec) {
+    if (threadIdx.x == 0) w.r0 = blk_rec[blockIdx.x];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < OCC_BLOCK + 2; i += blockDim.x) {
         const uint64_t r = w.r0 + i;
@@ -314,9 +326,10 @@ __global__ void k_init_tables(uint64_t T, slot_t<K>* slots) {
 template <typename K>
 __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_t R0, uint64_t nrec,
                                                 uint64_t O0, uint64_t nocc, uint32_t k,
+                                                uint32_t const* __restrict__ blk_rec,
                                                 uint32_t* __restrict__ occ_slot, uint32_t* err) {
     __shared__ occ_window win;
-    load_occ_window(win, R.occ, R0, nrec, O0 + (uint64_t)blockIdx.x * OCC_BLOCK);
+    load_occ_window(win, R.occ, R0, nrec, blk_rec);
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nocc) return;
     const uint64_t rec = window_record(win, R.occ, R0, nrec, O0 + t);
@@ -383,14 +396,12 @@ __global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, uint64_t
 
 // (node << 32 | record) for owned occurrences of multi-record k-mers, from the
 // slot each occurrence recorded at insert time.
-template <bool WRITE>
 __global__ void __launch_bounds__(256)
     k_multi_pairs(uint64_t const* __restrict__ occ, uint64_t R0, uint64_t nrec, uint64_t O0, uint64_t nocc,
+                  uint32_t const* __restrict__ blk_rec,
                   uint32_t const* __restrict__ occ_slot, uint32_t const* __restrict__ node_of_slot,
                   uint32_t const* __restrict__ n_rec, unsigned long long* __restrict__ cnt,
                   uint64_t* __restrict__ pairs) {
-    __shared__ occ_window win;
-    load_occ_window(win, occ, R0, nrec, O0 + (uint64_t)blockIdx.x * OCC_BLOCK);
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool emit = false;
     uint64_t val = 0;
@@ -400,7 +411,16 @@ __global__ void __launch_bounds__(256)
             const uint32_t n = node_of_slot[v & 0x7fffffffu];
             if (n_rec[n] == MULTI_TAG) {
                 emit = true;
-                val = ((uint64_t)n << 32) | (uint32_t)window_record(win, occ, R0, nrec, O0 + t);
+                {
+                    // the record lies between this block's first record and the
+                    // next block's (a few dozen records): search only there
+                    const uint64_t nblk = (nocc + OCC_BLOCK - 1) / OCC_BLOCK;
+                    const uint64_t b = t / OCC_BLOCK;
+                    const uint64_t rlo = blk_rec[b];
+                    const uint64_t rhi = (b + 1 < nblk) ? blk_rec[b + 1] : R0 + nrec - 1;
+                    const uint64_t r = rlo + upper_bound_u64(occ + rlo, rhi - rlo + 1, O0 + t) - 1;
+                    val = ((uint64_t)n << 32) | (uint32_t)r;
+                }
             }
         }
     }
@@ -412,7 +432,7 @@ __global__ void __launch_bounds__(256)
     unsigned long long base = 0;
     if (lane == leader) base = atomicAdd(cnt, (unsigned long long)__popc(b));
     base = __shfl_sync(0xffffffffu, base, leader);
-    if (WRITE && emit) pairs[base + __popc(b & lanemask_lt())] = val;
+    if (emit) pairs[base + __popc(b & lanemask_lt())] = val;
 }
 
 __global__ void k_unique_heads(uint64_t n, uint64_t const* __restrict__ a, uint32_t* __restrict__ keep) {
@@ -1101,7 +1121,7 @@ __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb,
 }
 
 template <typename K>
-__global__ void k_ext_mask(uint64_t D, tables<K> T, K const* __restrict__ n_key,
+__global__ void __launch_bounds__(256, 8) k_ext_mask(uint64_t D, tables<K> T, K const* __restrict__ n_key,
                            uint32_t const* __restrict__ n_bucket, uint32_t k, uint8_t* __restrict__ n_mask) {
     uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= D) return;
@@ -1110,14 +1130,17 @@ __global__ void k_ext_mask(uint64_t D, tables<K> T, K const* __restrict__ n_key,
     const K msk = ops::mask(k);
     const K rev = ops::revcomp(can, k);
     const uint32_t tb = n_bucket[n] - T.b0;
+    const uint32_t top = 2 * (k - 1);
     uint32_t out = 0;
+    // appending nt to x prepends 3 - nt to revcomp(x): (rc(x) >> 2) | (3 - nt) << 2(k-1)
 #pragma unroll
     for (uint32_t nt = 0; nt < 4; ++nt) {
-        K f = ((can << 2) | (K)nt) & msk;
-        K fr = ops::revcomp(f, k);
+        const K hi = (K)(3u - nt) << top;
+        const K f = ((can << 2) | (K)nt) & msk;
+        const K fr = (rev >> 2) | hi;
         if (node_lookup<K>(T, tb, f <= fr ? f : fr) != NONE32) out |= 1u << nt;
-        K r = ((rev << 2) | (K)nt) & msk;
-        K rr = ops::revcomp(r, k);
+        const K r = ((rev << 2) | (K)nt) & msk;
+        const K rr = (can >> 2) | hi;
         if (node_lookup<K>(T, tb, r <= rr ? r : rr) != NONE32) out |= 1u << (4 + nt);
     }
     n_mask[n] = (uint8_t)out;
@@ -1129,7 +1152,7 @@ __device__ __forceinline__ uint32_t back_nib(uint32_t m, bool rc) { return (rc ?
 // link[2n] = L port, link[2n+1] = R port: (node << 1) | rc of the state
 // reached, NONE32 when the step is not clean.
 template <typename K>
-__global__ void k_links(uint64_t D, tables<K> T, K const* __restrict__ n_key, uint32_t const* __restrict__ n_bucket,
+__global__ void __launch_bounds__(256, 8) k_links(uint64_t D, tables<K> T, K const* __restrict__ n_key, uint32_t const* __restrict__ n_bucket,
                         uint8_t const* __restrict__ n_mask, uint32_t k, uint32_t* __restrict__ link) {
     uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= D) return;
@@ -1138,14 +1161,17 @@ __global__ void k_links(uint64_t D, tables<K> T, K const* __restrict__ n_key, ui
     const uint32_t m = n_mask[n];
     const uint32_t tb = n_bucket[n] - T.b0;
     const K msk = ops::mask(k);
+    const uint32_t top = 2 * (k - 1);
+    const uint32_t nibr = fwd_nib(m, false), nibl = back_nib(m, false);
+    const K rev = (__popc(nibr) == 1 || __popc(nibl) == 1) ? ops::revcomp(can, k) : can;
     // R: forward from (can, rc = false)
     uint32_t lr = NONE32, ll = NONE32;
     {
-        const uint32_t nib = fwd_nib(m, false);
+        const uint32_t nib = nibr;
         if (__popc(nib) == 1) {
             const uint32_t nt = __ffs(nib) - 1;
             const K nf = ((can << 2) | (K)nt) & msk;
-            const K nr = ops::revcomp(nf, k);
+            const K nr = (rev >> 2) | ((K)(3u - nt) << top);
             const bool nrc = !(nf <= nr);
             const uint32_t nn = node_lookup<K>(T, tb, nrc ? nr : nf);
             if (nn != NONE32 && __popc(back_nib(n_mask[nn], nrc)) == 1) lr = (nn << 1) | (nrc ? 1u : 0u);
@@ -1153,12 +1179,11 @@ __global__ void k_links(uint64_t D, tables<K> T, K const* __restrict__ n_key, ui
     }
     // L: backward from (can, rc = false) = bstep(can, rc = true) then flip
     {
-        const uint32_t nib = back_nib(m, false);
+        const uint32_t nib = nibl;
         if (__popc(nib) == 1) {
             const uint32_t nt = __ffs(nib) - 1;
-            const K cur = ops::revcomp(can, k);
-            const K nf = ((cur << 2) | (K)nt) & msk;
-            const K nr = ops::revcomp(nf, k);
+            const K nf = ((rev << 2) | (K)nt) & msk;
+            const K nr = (can >> 2) | ((K)(3u - nt) << top);
             const bool srcc = !(nf <= nr);
             const bool nrc = !srcc;
             const uint32_t nn = node_lookup<K>(T, tb, srcc ? nr : nf);
@@ -1564,19 +1589,19 @@ __device__ __forceinline__ void put_bytes(uint8_t* o, uint64_t v, int n) {
     for (int i = 0; i < n; ++i) o[i] = (uint8_t)(v >> (8 * i));
 }
 
+// One fragment record (unitig_spill.hpp:491-522 layout) at `o` (shared or
+// global memory).  Each base after the first k-mer is the last base of the
+// oriented k-mer: the low 2 bits of the key, or the complement of its first
+// base when the walk is reverse -- no reverse complement per element.
 template <typename K>
-__global__ void k_frag_write(uint64_t F, uint32_t const* __restrict__ seed_of, uint32_t const* __restrict__ seed_start,
-                             uint32_t const* __restrict__ seed_len, uint8_t const* __restrict__ seed_open,
-                             uint32_t const* __restrict__ fe, uint32_t const* __restrict__ n_cid,
-                             K const* __restrict__ n_key, uint32_t k, uint64_t const* __restrict__ off,
-                             uint8_t* __restrict__ out) {
-    uint64_t f = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= F) return;
+__device__ __forceinline__ void emit_fragment(uint8_t* o, uint32_t n, uint32_t const* __restrict__ seed_start,
+                                              uint32_t const* __restrict__ seed_len,
+                                              uint8_t const* __restrict__ seed_open, uint32_t const* __restrict__ fe,
+                                              uint32_t const* __restrict__ n_cid, K const* __restrict__ n_key,
+                                              uint32_t k) {
     typedef kmer_ops<K> ops;
-    const uint32_t n = seed_of[f];
     const uint32_t len = seed_len[n];
     const uint32_t a = seed_start[n];
-    uint8_t* o = out + off[f];
     o[0] = seed_open[n];
     uint32_t runs = 0;
     uint8_t* rp = o + 5;
@@ -1606,12 +1631,55 @@ __global__ void k_frag_write(uint64_t F, uint32_t const* __restrict__ seed_of, u
         if (e & 1u) w = ops::revcomp(w, k);
         for (uint32_t i = 0; i < k; ++i) sp[k - 1 - i] = acgt[ops::low2(w >> (2 * i))];
     }
+    const uint32_t top = 2 * (k - 1);
     for (uint32_t j = 1; j < len; ++j) {
         const uint32_t e = fe[a + j];
-        K w = n_key[e >> 1];
-        if (e & 1u) w = ops::revcomp(w, k);
-        sp[k - 1 + j] = acgt[ops::low2(w)];
+        const K w = n_key[e >> 1];
+        const uint32_t b = (e & 1u) ? 3u - ops::low2(w >> top) : ops::low2(w);
+        sp[k - 1 + j] = acgt[b];
     }
+}
+
+// Fragments [f0, f0 + FW_THREADS) of a block occupy one contiguous byte range
+// of the output.  They are laid out in shared memory with the range's
+// 16-byte phase and stored with aligned 16-byte writes (bytes at the two
+// ragged ends one by one), instead of a few dozen scattered byte stores per
+// fragment.  A block whose range does not fit writes directly.
+constexpr int FW_THREADS = 128;
+constexpr int FW_BYTES = 32 * 1024;
+
+template <typename K>
+__global__ void __launch_bounds__(FW_THREADS)
+    k_frag_write(uint64_t F, uint32_t const* __restrict__ seed_of, uint32_t const* __restrict__ seed_start,
+                 uint32_t const* __restrict__ seed_len, uint8_t const* __restrict__ seed_open,
+                 uint32_t const* __restrict__ fe, uint32_t const* __restrict__ n_cid, K const* __restrict__ n_key,
+                 uint32_t k, uint64_t const* __restrict__ off, uint8_t* __restrict__ out) {
+    __shared__ __align__(16) uint8_t buf[FW_BYTES];
+    const uint64_t f0 = (uint64_t)blockIdx.x * FW_THREADS;
+    const uint64_t f1 = (f0 + FW_THREADS < F) ? f0 + FW_THREADS : F;
+    const uint64_t g0 = off[f0], g1 = off[f1];
+    const uint32_t phase = (uint32_t)(g0 & 15);
+    const uint64_t f = f0 + threadIdx.x;
+    if (g1 - g0 + phase > (uint64_t)FW_BYTES) {  // block-uniform
+        if (f < F) emit_fragment<K>(out + off[f], seed_of[f], seed_start, seed_len, seed_open, fe, n_cid, n_key, k);
+        return;
+    }
+    if (f < F)
+        emit_fragment<K>(buf + phase + (off[f] - g0), seed_of[f], seed_start, seed_len, seed_open, fe, n_cid, n_key,
+                         k);
+    __syncthreads();
+    const uint64_t a0 = (g0 + 15) & ~uint64_t(15);  // first aligned byte inside the range
+    const uint64_t a1 = g1 & ~uint64_t(15);         // end of the aligned part
+    if (a0 >= a1) {
+        for (uint64_t b = g0 + threadIdx.x; b < g1; b += FW_THREADS) out[b] = buf[phase + (b - g0)];
+        return;
+    }
+    for (uint64_t b = g0 + threadIdx.x; b < a0; b += FW_THREADS) out[b] = buf[phase + (b - g0)];
+    for (uint64_t b = a1 + threadIdx.x; b < g1; b += FW_THREADS) out[b] = buf[phase + (b - g0)];
+    const uint64_t nchunks = (a1 - a0) >> 4;
+    uint4 const* src = reinterpret_cast<uint4 const*>(buf + phase + (a0 - g0));  // 16-byte aligned
+    uint4* dst = reinterpret_cast<uint4*>(out + a0);
+    for (uint64_t c = threadIdx.x; c < nchunks; c += FW_THREADS) dst[c] = src[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -1757,9 +1825,14 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     }
     CDBG_CHECK_LAUNCH();
     // ---- load
+    // record of each occurrence block's first occurrence (k_insert, k_multi_pairs)
+    const uint64_t nblk = ceil_div(nocc, (uint64_t)OCC_BLOCK);
+    uint32_t* blk_rec = A.alloc<uint32_t>(nblk + 1);
+    k_block_records<<<grid(nrec, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nblk, blk_rec);
+    CDBG_CHECK_LAUNCH();
     {
         CDBG_PROF("k_insert", st);
-        k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, occ_slot, d_err);
+        k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, blk_rec, occ_slot, d_err);
     }
     CDBG_CHECK_LAUNCH();
     // ---- nodes in first-insertion order
@@ -1790,13 +1863,15 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
                                                        n_rec, n_bucket, node_of_slot);
     }
     CDBG_CHECK_LAUNCH();
-    // ---- multi-record k-mers
+    // ---- multi-record k-mers: (node, record) pairs in one pass, at most one
+    // per occurrence
     unsigned long long* cnt = A.alloc<unsigned long long>(1);
+    uint64_t* pairs = A.alloc<uint64_t>(nocc);
     CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
     {
         CDBG_PROF("k_multi_pairs", st);
-        k_multi_pairs<false><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, node_of_slot, n_rec, cnt,
-                                                              nullptr);
+        k_multi_pairs<<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, blk_rec, occ_slot, node_of_slot,
+                                                             n_rec, cnt, pairs);
     }
     CDBG_CHECK_LAUNCH();
     const uint64_t npairs = read_dev(cnt, st);
@@ -1815,14 +1890,6 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint64_t* gend = nullptr;
     uint32_t* mgrp = nullptr;    // group of each multi node
     if (npairs) {
-        uint64_t* pairs = A.alloc<uint64_t>(npairs);
-        CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
-        {
-            CDBG_PROF("k_multi_pairs", st);
-            k_multi_pairs<true><<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, occ_slot, node_of_slot, n_rec,
-                                                                 cnt, pairs);
-        }
-        CDBG_CHECK_LAUNCH();
         uint32_t* dummy = A.alloc<uint32_t>(npairs);
         prim::radix_sort_pairs<uint32_t>(pairs, dummy, npairs, 0, 64, A, st);
         uint32_t* keep = A.alloc<uint32_t>(npairs);
@@ -2170,8 +2237,8 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint8_t* fb = A.alloc<uint8_t>(fbytes + 8);
     if (nfr) {
         CDBG_PROF("k_frag_write", st);
-        k_frag_write<K><<<grid(nfr, 256), 256, 0, st>>>(nfr, seed_of, W.seed_start, W.seed_len, W.seed_open, W.fe,
-                                                         n_cid, n_key, k, foff, fb);
+        k_frag_write<K><<<grid(nfr, FW_THREADS), FW_THREADS, 0, st>>>(nfr, seed_of, W.seed_start, W.seed_len,
+                                                                       W.seed_open, W.fe, n_cid, n_key, k, foff, fb);
     }
     CDBG_CHECK_LAUNCH();
     const uint64_t seq_total = read_dev(seqt, st);
