@@ -254,6 +254,8 @@ int cdbg_engine_create(int device, cdbg_engine** out) {
         e->device = device;
         cdbg::device_pool(device);  // configure the pool the arenas draw from
         CDBG_CUDA(cudaStreamCreateWithFlags(&e->own_st, cudaStreamNonBlocking));
+        CDBG_CUDA(cudaStreamCreateWithFlags(&e->copy_st, cudaStreamNonBlocking));
+        CDBG_CUDA(cudaEventCreateWithFlags(&e->copy_ev, cudaEventDisableTiming));
         e->st = e->own_st;
         e->A.set_stream(e->st);
         e->P.set_stream(e->st);
@@ -276,6 +278,11 @@ void cdbg_engine_destroy(cdbg_engine* e) {
     cudaStreamSynchronize(e->st);
     if (e->d_err) cudaFree(e->d_err);
     e->prof.resolve();
+    if (e->copy_st) {
+        cudaStreamSynchronize(e->copy_st);
+        cudaStreamDestroy(e->copy_st);
+    }
+    if (e->copy_ev) cudaEventDestroy(e->copy_ev);
     if (e->own_st) cudaStreamDestroy(e->own_st);
     delete e;
 }
@@ -645,16 +652,31 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         pp.num_colors = p->num_colors;
         pp.batch_occ = p->batch_occ ? p->batch_occ : e->tune.batch_occ;
         pp.heavy_colors = e->tune.heavy_colors;
-        pp.to_host = false;  // outputs accumulate in HBM; one D2H at the end when asked
+        pp.to_host = false;  // outputs accumulate in HBM
+        if (p->outputs_to_host && e->h_frag.p && e->h_frag.cap) {
+            // stream each batch's fragments into the (already large enough,
+            // from earlier builds) pinned buffer while phase 2 goes on
+            pp.frag_host = (uint8_t*)e->h_frag.p;
+            pp.frag_host_cap = e->h_frag.cap;
+            pp.copy_st = e->copy_st;
+            pp.copy_ev = e->copy_ev;
+        }
         cdbg::phase2_result out;
         out.state = &e->p2;
         cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, out);
         const uint64_t nwords = (out.nbits + 63) / 64;
         if (p->outputs_to_host) {
-            void* hf = e->h_frag.ensure(out.frag_nbytes + 8);
+            const bool streamed = pp.frag_host && out.frag_host_copied == out.frag_nbytes;
+            if (pp.copy_st) {
+                // the compute stream (and the caller's events on it) wait for the copies
+                CDBG_CUDA(cudaEventRecord(e->copy_ev, e->copy_st));
+                CDBG_CUDA(cudaStreamWaitEvent(e->st, e->copy_ev, 0));
+            }
+            if (!streamed) CDBG_CUDA(cudaStreamSynchronize(e->copy_st));  // before the buffer may move
+            void* hf = streamed ? e->h_frag.p : e->h_frag.ensure(out.frag_nbytes + 8);
             void* hw = e->h_words.ensure(8 * nwords + 8);
             void* ho = e->h_offsets.ensure(8 * out.n_classes + 8);
-            if (out.frag_nbytes)
+            if (out.frag_nbytes && !streamed)
                 CDBG_CUDA(cudaMemcpyAsync(hf, out.d_frag, out.frag_nbytes, cudaMemcpyDeviceToHost, e->st));
             if (nwords) CDBG_CUDA(cudaMemcpyAsync(hw, out.d_words, 8 * nwords, cudaMemcpyDeviceToHost, e->st));
             if (out.n_classes)

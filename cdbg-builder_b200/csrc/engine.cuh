@@ -37,6 +37,8 @@ struct cdbg_engine {
     int device = 0;
     cudaStream_t st = nullptr;      // stream all work runs on
     cudaStream_t own_st = nullptr;  // the engine's own stream
+    cudaStream_t copy_st = nullptr; // device-to-host copies that overlap phase 2
+    cudaEvent_t copy_ev = nullptr;
     cdbg::kernel_profiler prof;
     cdbg::dev_arena A;   // per-stage scratch
     cdbg::dev_arena P;   // phase-1 outputs kept through phase 2 (in-memory build)

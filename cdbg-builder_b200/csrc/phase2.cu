@@ -2251,9 +2251,23 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         out.frag.resize(o + fbytes);
         CDBG_CUDA(cudaMemcpyAsync(out.frag.data() + o, fb, fbytes, cudaMemcpyDeviceToHost, st));
     } else {
+        const uint64_t old_n = dfrag.n;
+        if (p.copy_st && dfrag.n + fbytes + 8 > dfrag.cap) {
+            // growing frees the old buffer: after the host copies that read it
+            CDBG_CUDA(cudaEventRecord(p.copy_ev, p.copy_st));
+            CDBG_CUDA(cudaStreamWaitEvent(st, p.copy_ev, 0));
+        }
         dfrag.reserve(dfrag.n + fbytes + 8, st);
         CDBG_CUDA(cudaMemcpyAsync(dfrag.p + dfrag.n, fb, fbytes, cudaMemcpyDeviceToDevice, st));
         dfrag.n += fbytes;
+        if (p.copy_st && p.frag_host && out.frag_host_copied == old_n && dfrag.n <= p.frag_host_cap && fbytes) {
+            // this batch's fragments go to the host while the next batch runs
+            CDBG_CUDA(cudaEventRecord(p.copy_ev, st));
+            CDBG_CUDA(cudaStreamWaitEvent(p.copy_st, p.copy_ev, 0));
+            CDBG_CUDA(cudaMemcpyAsync(p.frag_host + old_n, dfrag.p + old_n, fbytes, cudaMemcpyDeviceToHost,
+                                      p.copy_st));
+            out.frag_host_copied = dfrag.n;
+        }
     }
     CDBG_CUDA(cudaStreamSynchronize(st));
     out.frag_nbytes += fbytes;

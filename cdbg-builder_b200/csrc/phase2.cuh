@@ -44,6 +44,7 @@ struct phase2_state {
 
 // Outputs of phase 2, accumulated over bucket batches.
 struct phase2_result {
+    uint64_t frag_host_copied = 0;  // leading frag bytes queued to params.frag_host
     // frag_unitigs.bin bytes (unitig_spill.hpp:642-665 record layout), in
     // bucket order and, per bucket, in seed order.
     std::vector<uint8_t> frag;          // host copy (when to_host)
@@ -77,6 +78,13 @@ struct phase2_params {
     // records with at least this many colors get a precomputed bitmap in
     // multi-record unions (performance only)
     uint32_t heavy_colors = 64;
+    // Device-resident mode: fragment bytes of each batch are also copied to
+    // this pinned host buffer on `copy_st` while later batches run, as long
+    // as they fit in `frag_host_cap` (nothing is streamed when null).
+    uint8_t* frag_host = nullptr;
+    uint64_t frag_host_cap = 0;
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t copy_ev = nullptr;
 };
 
 // Run phase 2 over all buckets of `rs` (records grouped by bucket).

@@ -122,3 +122,29 @@ def test_union_list_path_matches_bitmap_path(engine, tmp_path, monkeypatch):
     monkeypatch.setenv("CDBG_UNION_LISTS", "1")
     r2 = engine.build(hs.batch, 31, 128, 8)
     assert (native.result_frag_bytes(r2), native.result_class_words(r2).tobytes()) == a
+
+
+def test_streamed_host_outputs_match_across_build_sizes(tmp_path):
+    """Host outputs of in-memory builds, whose fragment bytes go to pinned
+    memory batch by batch while later batches run once the engine's buffer is
+    large enough (else in one copy at the end): identical whatever the order
+    of build sizes and bucket-batch sizes."""
+    small = native.HostSequences([l.strip() for l in open(_fresh(tmp_path / "s", 61, 3)) if l.strip()])
+    large = native.HostSequences([l.strip() for l in open(_fresh(tmp_path / "l", 62, 12)) if l.strip()])
+    B, k = 256, 31
+
+    def outs(e, hs, n, batch_occ=0):
+        r = e.build(hs.batch, k, B, n, batch_occ=batch_occ)
+        return native.result_frag_bytes(r), native.result_class_words(r).tobytes()
+
+    ref = native.Engine(0)
+    want_s, want_l = outs(ref, small, 3), outs(ref, large, 12)
+    ref.close()
+    e = native.Engine(0)
+    try:
+        assert outs(e, small, 3) == want_s          # nothing pinned yet: one copy at the end
+        assert outs(e, large, 12, 1 << 12) == want_l  # larger than the buffer: falls back
+        assert outs(e, large, 12, 1 << 12) == want_l  # streamed, many batches
+        assert outs(e, small, 3, 1 << 10) == want_s   # streamed into the larger buffer
+    finally:
+        e.close()
