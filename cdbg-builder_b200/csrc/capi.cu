@@ -489,7 +489,8 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
             cdbg::run_table rt;
             cdbg::build_runs(in, k, e->A, e->st, rt, e->A);
             cdbg::super_list sl;
-            cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile);
+            cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile,
+                              a->num_files < (1u << 28));
             cdbg::record_set rs;
             cdbg::build_records(rt, sl, k, a->num_buckets, e->A, e->st, rs, e->d_err, e->A);
             cdbg::serialized_buckets sb;
@@ -638,7 +639,8 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         cdbg::run_table rt;
         cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
         cdbg::super_list sl;
-        cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile);
+        cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile,
+                          p->num_colors < (1u << 28));
         cdbg::record_set rs;
         cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
         unsigned long long* d_rec_bytes = e->P.alloc<unsigned long long>(1);

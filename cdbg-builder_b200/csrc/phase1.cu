@@ -441,6 +441,42 @@ __global__ void k_run_kmers(uint32_t nruns, uint32_t const* __restrict__ len, ui
 }
 
 // Super-k-mer fields from the cut list (bucket_ingester.hpp:80-126).
+struct super_fields {
+    uint64_t start, key;
+    uint32_t len, color, flags, bucket;
+};
+__device__ __forceinline__ super_fields make_super(uint64_t i, uint64_t n, uint64_t const* __restrict__ minv,
+                                                   uint32_t const* __restrict__ run,
+                                                   uint32_t const* __restrict__ a_arr,
+                                                   uint64_t const* __restrict__ soff,
+                                                   uint32_t const* __restrict__ rlen,
+                                                   uint32_t const* __restrict__ rcolor,
+                                                   uint64_t const* __restrict__ words, uint32_t k, uint32_t B,
+                                                   uint32_t bb) {
+    super_fields o;
+    const uint32_t r = run[i];
+    const uint32_t a = a_arr[i];
+    const uint64_t K = (uint64_t)rlen[r] - k + 1;
+    const bool next_same = (i + 1 < n) && run[i + 1] == r;
+    const uint64_t b = next_same ? (uint64_t)a_arr[i + 1] - 1 : K;
+    const uint64_t fk = a ? a - 1 : 0;
+    const uint64_t lk = b < K - 1 ? b : K - 1;
+    o.len = (uint32_t)(lk - fk + k);
+    const uint64_t mv = minv[i];
+    uint32_t f = 0;
+    if (a == 0) f |= 1u;                             // IS_ACGT_BEGIN
+    if (!next_same) f |= 2u;                         // IS_ACGT_END
+    if (a == 0 || mv < minv[i - 1]) f |= 4u;         // OWNS_FIRST
+    if (!next_same || mv < minv[i + 1]) f |= 8u;     // OWNS_LAST
+    o.flags = f;
+    o.bucket = (uint32_t)((mv >> 1) % B);
+    o.start = soff[r] + fk;
+    o.color = rcolor[r];
+    const uint64_t h = super_hash_dev(words, o.start, o.len);
+    o.key = bb ? (((uint64_t)o.bucket << (64 - bb)) | (h >> bb)) : h;
+    return o;
+}
+
 __global__ void k_super_finalize(uint64_t n, uint64_t const* __restrict__ minv,
                                  uint32_t const* __restrict__ run, uint32_t const* __restrict__ a_arr,
                                  uint64_t const* __restrict__ soff, uint32_t const* __restrict__ rlen,
@@ -451,29 +487,30 @@ __global__ void k_super_finalize(uint64_t n, uint64_t const* __restrict__ minv,
                                  uint64_t* __restrict__ key) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t r = run[i];
-    const uint32_t a = a_arr[i];
-    const uint64_t K = (uint64_t)rlen[r] - k + 1;
-    const bool next_same = (i + 1 < n) && run[i + 1] == r;
-    const uint64_t b = next_same ? (uint64_t)a_arr[i + 1] - 1 : K;
-    const uint64_t fk = a ? a - 1 : 0;
-    const uint64_t lk = b < K - 1 ? b : K - 1;
-    const uint32_t l = (uint32_t)(lk - fk + k);
-    const uint64_t mv = minv[i];
-    uint32_t f = 0;
-    if (a == 0) f |= 1u;                             // IS_ACGT_BEGIN
-    if (!next_same) f |= 2u;                         // IS_ACGT_END
-    if (a == 0 || mv < minv[i - 1]) f |= 4u;         // OWNS_FIRST
-    if (!next_same || mv < minv[i + 1]) f |= 8u;     // OWNS_LAST
-    const uint32_t bk = (uint32_t)((mv >> 1) % B);
-    const uint64_t st = soff[r] + fk;
-    start[i] = st;
-    len[i] = l;
-    color[i] = rcolor[r];
-    flags[i] = f;
-    bucket[i] = bk;
-    const uint64_t h = super_hash_dev(words, st, l);
-    key[i] = bb ? (((uint64_t)bk << (64 - bb)) | (h >> bb)) : h;
+    const super_fields o = make_super(i, n, minv, run, a_arr, soff, rlen, rcolor, words, k, B, bb);
+    start[i] = o.start;
+    len[i] = o.len;
+    color[i] = o.color;
+    flags[i] = o.flags;
+    bucket[i] = o.bucket;
+    key[i] = o.key;
+}
+
+// Same fields packed 16 bytes per super-k-mer (start, len, color << 4 |
+// flags; colors < 2^28), so the key-order gather of the dedup touches one
+// sector per super-k-mer; the bucket is the key's top bits.
+__global__ void k_super_finalize_packed(uint64_t n, uint64_t const* __restrict__ minv,
+                                        uint32_t const* __restrict__ run, uint32_t const* __restrict__ a_arr,
+                                        uint64_t const* __restrict__ soff, uint32_t const* __restrict__ rlen,
+                                        uint32_t const* __restrict__ rcolor, uint64_t const* __restrict__ words,
+                                        uint32_t k, uint32_t B, uint32_t bb, uint4* __restrict__ packed,
+                                        uint64_t* __restrict__ key, uint32_t* err) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const super_fields o = make_super(i, n, minv, run, a_arr, soff, rlen, rcolor, words, k, B, bb);
+    if (o.color >> 28) set_error(err, ERR_FIELD_OVERFLOW);
+    packed[i] = make_uint4((uint32_t)o.start, (uint32_t)(o.start >> 32), o.len, (o.color << 4) | o.flags);
+    key[i] = o.key;
 }
 
 __device__ __forceinline__ bool same_bases(uint64_t const* __restrict__ words, uint64_t pa,
@@ -487,52 +524,87 @@ __device__ __forceinline__ bool same_bases(uint64_t const* __restrict__ words, u
     return true;
 }
 
-__global__ void k_group_heads(uint64_t n, uint64_t const* __restrict__ key,
-                              uint32_t const* __restrict__ idx, uint64_t const* __restrict__ start,
-                              uint32_t const* __restrict__ len, uint32_t const* __restrict__ color,
-                              uint64_t const* __restrict__ words, uint32_t* __restrict__ head,
-                              uint32_t* __restrict__ ckeep) {
+// Super-k-mer fields in key order (one gather per field), so the grouping and
+// record passes below read them sequentially.
+__global__ void k_permute_supers(uint64_t n, uint32_t const* __restrict__ idx, uint64_t const* __restrict__ start,
+                                 uint32_t const* __restrict__ len, uint32_t const* __restrict__ color,
+                                 uint32_t const* __restrict__ flags, uint64_t* __restrict__ p_start,
+                                 uint32_t* __restrict__ p_len, uint32_t* __restrict__ p_color,
+                                 uint32_t* __restrict__ p_flags) {
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const uint32_t i = idx[p];
+    p_start[p] = start[i];
+    p_len[p] = len[i];
+    p_color[p] = color[i];
+    p_flags[p] = flags[i];
+}
+
+__global__ void k_permute_packed(uint64_t n, uint32_t const* __restrict__ idx, uint4 const* __restrict__ packed,
+                                 uint64_t* __restrict__ p_start, uint32_t* __restrict__ p_len,
+                                 uint32_t* __restrict__ p_color, uint32_t* __restrict__ p_flags) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint4 v = packed[idx[p]];
+    p_start[p] = ((uint64_t)v.y << 32) | v.x;
+    p_len[p] = v.z;
+    p_color[p] = v.w >> 4;
+    p_flags[p] = v.w & 0xfu;
+}
+
+// head[p]: position p starts a new record (key, length or bases differ from
+// p - 1); ckeep[p]: p adds a color to its record (the first of each color).
+__global__ void k_group_heads_sorted(uint64_t n, uint64_t const* __restrict__ key,
+                                     uint64_t const* __restrict__ start, uint32_t const* __restrict__ len,
+                                     uint32_t const* __restrict__ color, uint64_t const* __restrict__ words,
+                                     uint32_t* __restrict__ head, uint32_t* __restrict__ ckeep) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
     bool h = true;
     if (p > 0) {
-        const uint32_t j = idx[p - 1];
-        h = !(key[p] == key[p - 1] && len[i] == len[j] && same_bases(words, start[i], start[j], len[i]));
-        ckeep[p] = (h || color[i] != color[j]) ? 1u : 0u;
+        h = !(key[p] == key[p - 1] && len[p] == len[p - 1] && same_bases(words, start[p], start[p - 1], len[p]));
+        ckeep[p] = (h || color[p] != color[p - 1]) ? 1u : 0u;
     } else {
         ckeep[p] = 1u;
     }
     head[p] = h ? 1u : 0u;
 }
 
-__global__ void k_records_fill(uint64_t n, uint32_t const* __restrict__ idx,
-                               uint32_t const* __restrict__ head, uint64_t const* __restrict__ rid_ex,
-                               uint32_t const* __restrict__ ckeep, uint64_t const* __restrict__ cpos,
-                               uint64_t const* __restrict__ start, uint32_t const* __restrict__ len,
-                               uint32_t const* __restrict__ color, uint32_t const* __restrict__ flags,
-                               uint32_t const* __restrict__ bucket, uint64_t* __restrict__ r_start,
-                               uint32_t* __restrict__ r_len, uint32_t* __restrict__ r_flags,
-                               uint64_t* __restrict__ r_coloff, uint32_t* __restrict__ colors,
-                               uint32_t* __restrict__ r_bucket) {
+__global__ void k_records_fill_sorted(uint64_t n, uint32_t const* __restrict__ head,
+                                      uint64_t const* __restrict__ rid_ex, uint32_t const* __restrict__ ckeep,
+                                      uint64_t const* __restrict__ cpos, uint64_t const* __restrict__ key,
+                                      uint32_t bb, uint64_t const* __restrict__ start,
+                                      uint32_t const* __restrict__ len, uint32_t const* __restrict__ color,
+                                      uint32_t const* __restrict__ flags, uint64_t* __restrict__ r_start,
+                                      uint32_t* __restrict__ r_len, uint32_t* __restrict__ r_flags,
+                                      uint64_t* __restrict__ r_coloff, uint32_t* __restrict__ colors,
+                                      uint32_t* __restrict__ r_bucket) {
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    const uint32_t i = idx[p];
     const uint64_t rid = rid_ex[p] + head[p] - 1;  // inclusive count - 1
     if (head[p]) {
-        r_start[rid] = start[i];
-        r_len[rid] = len[i];
+        r_start[rid] = start[p];
+        r_len[rid] = len[p];
         r_coloff[rid] = cpos[p];
-        r_bucket[rid] = bucket[i];
+        r_bucket[rid] = bb ? (uint32_t)(key[p] >> (64 - bb)) : 0u;
     }
-    atomicAnd(&r_flags[rid], flags[i]);
-    if (ckeep[p]) colors[cpos[p]] = color[i];
+    const uint32_t f = flags[p];
+    if (f != 0xfu) atomicAnd(&r_flags[rid], f);  // AND over the record's copies (starts at 0xf)
+    if (ckeep[p]) colors[cpos[p]] = color[p];
 }
 
-__global__ void k_bucket_hist(uint64_t n, uint32_t const* __restrict__ rb,
-                              unsigned long long* __restrict__ cnt) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) atomicAdd(&cnt[rb[i]], 1ull);
+// bucket_start[b] = first record of bucket b (records are in bucket order):
+// each record that starts a bucket fills the starts of the empty buckets
+// before it; the last record fills the rest with n.
+__global__ void k_bucket_bounds(uint64_t n, uint32_t const* __restrict__ rb, uint32_t B,
+                                uint64_t* __restrict__ bucket_start) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t b = rb[r];
+    const uint32_t prev = r ? rb[r - 1] + 1 : 0;
+    for (uint32_t x = prev; x <= b; ++x) bucket_start[x] = r;
+    if (r == n - 1)
+        for (uint32_t x = b + 1; x <= B; ++x) bucket_start[x] = n;
 }
 
 __global__ void k_fill_u32(uint32_t* p, uint64_t n, uint32_t v) {
@@ -768,21 +840,21 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
 
 template <int TT>
 void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
-                    cudaStream_t st, super_list& out, uint32_t* d_err);
+                    cudaStream_t st, super_list& out, uint32_t* d_err, bool packed);
 
 void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
-                 cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile) {
+                 cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile, bool packed) {
     if (tile == 1024)
-        find_supers_tt<1024>(rt, k, m, B, A, st, out, d_err);
+        find_supers_tt<1024>(rt, k, m, B, A, st, out, d_err, packed);
     else if (tile == 2048 || tile == 0)
-        find_supers_tt<2048>(rt, k, m, B, A, st, out, d_err);
+        find_supers_tt<2048>(rt, k, m, B, A, st, out, d_err, packed);
     else
         throw std::runtime_error("minimizer tile must be 1024 or 2048");
 }
 
 template <int TT>
 void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
-                    cudaStream_t st, super_list& out, uint32_t* d_err) {
+                    cudaStream_t st, super_list& out, uint32_t* d_err, bool packed) {
     out = super_list();
     if (rt.n == 0) return;
     if (k < 2 || m >= k || k - m > 62 || m > 32)
@@ -835,15 +907,20 @@ void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev
     }
     if (n >= 0xffffffffull) throw std::runtime_error("more than 2^32 super-k-mers in one call");
     out.n = n;
-    out.start = A.alloc<uint64_t>(n);
-    out.len = A.alloc<uint32_t>(n);
-    out.color = A.alloc<uint32_t>(n);
-    out.flags = A.alloc<uint32_t>(n);
-    out.bucket = A.alloc<uint32_t>(n);
     out.key = A.alloc<uint64_t>(n);
     uint32_t bb = 0;
     while ((1ull << bb) < B) ++bb;
-    {
+    if (packed) {
+        out.packed = A.alloc<uint4>(n);
+        CDBG_PROF("k_super_finalize", st);
+        k_super_finalize_packed<<<grid(n, 256), 256, 0, st>>>(n, minv, run, aa, rt.soff, rt.len, rt.color, rt.words,
+                                                               k, B, bb, out.packed, out.key, d_err);
+    } else {
+        out.start = A.alloc<uint64_t>(n);
+        out.len = A.alloc<uint32_t>(n);
+        out.color = A.alloc<uint32_t>(n);
+        out.flags = A.alloc<uint32_t>(n);
+        out.bucket = A.alloc<uint32_t>(n);
         CDBG_PROF("k_super_finalize", st);
         k_super_finalize<<<grid(n, 256), 256, 0, st>>>(n, minv, run, aa, rt.soff, rt.len, rt.color, rt.words,
                                                         k, B, bb, out.start, out.len, out.color, out.flags,
@@ -876,12 +953,24 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     uint64_t* skey = A.alloc<uint64_t>(n);
     CDBG_CUDA(cudaMemcpyAsync(skey, sl.key, n * 8, cudaMemcpyDeviceToDevice, st));
     prim::radix_sort_pairs<uint32_t>(skey, idx, n, 0, 64, A, st);
+    uint64_t* p_start = A.alloc<uint64_t>(n);
+    uint32_t* p_len = A.alloc<uint32_t>(n);
+    uint32_t* p_color = A.alloc<uint32_t>(n);
+    uint32_t* p_flags = A.alloc<uint32_t>(n);
+    {
+        CDBG_PROF("k_permute_supers", st);
+        if (sl.packed)
+            k_permute_packed<<<grid(n, 256), 256, 0, st>>>(n, idx, sl.packed, p_start, p_len, p_color, p_flags);
+        else
+            k_permute_supers<<<grid(n, 256), 256, 0, st>>>(n, idx, sl.start, sl.len, sl.color, sl.flags, p_start,
+                                                            p_len, p_color, p_flags);
+    }
+    CDBG_CHECK_LAUNCH();
     uint32_t* head = A.alloc<uint32_t>(n);
     uint32_t* ckeep = A.alloc<uint32_t>(n);
     {
         CDBG_PROF("k_group_heads", st);
-        k_group_heads<<<grid(n, 256), 256, 0, st>>>(n, skey, idx, sl.start, sl.len, sl.color, rt.words,
-                                                     head, ckeep);
+        k_group_heads_sorted<<<grid(n, 256), 256, 0, st>>>(n, skey, p_start, p_len, p_color, rt.words, head, ckeep);
     }
     CDBG_CHECK_LAUNCH();
     uint64_t* rid = A.alloc<uint64_t>(n + 1);
@@ -903,20 +992,19 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     uint32_t* rb = A.alloc<uint32_t>(nr);
     k_fill_u32<<<grid(nr, 256), 256, 0, st>>>(rs.flags, nr, 0xfu);
     CDBG_CHECK_LAUNCH();
+    uint32_t bb = 0;
+    while ((1ull << bb) < B) ++bb;
     {
         CDBG_PROF("k_records_fill", st);
-        k_records_fill<<<grid(n, 256), 256, 0, st>>>(n, idx, head, rid, ckeep, cpos, sl.start, sl.len,
-                                                      sl.color, sl.flags, sl.bucket, rs.start, rs.len,
-                                                      rs.flags, rs.col_off, rs.colors, rb);
+        k_records_fill_sorted<<<grid(n, 256), 256, 0, st>>>(n, head, rid, ckeep, cpos, skey, bb, p_start, p_len,
+                                                             p_color, p_flags, rs.start, rs.len, rs.flags,
+                                                             rs.col_off, rs.colors, rb);
     }
     CDBG_CHECK_LAUNCH();
     k_set_last_u64<<<1, 1, 0, st>>>(rs.col_off, nr, cpos + n);
     CDBG_CHECK_LAUNCH();
-    unsigned long long* bc = A.alloc<unsigned long long>(B);
-    CDBG_CUDA(cudaMemsetAsync(bc, 0, 8ull * B, st));
-    k_bucket_hist<<<grid(nr, 256), 256, 0, st>>>(nr, rb, bc);
+    k_bucket_bounds<<<grid(nr, 256), 256, 0, st>>>(nr, rb, B, rs.bucket_start);
     CDBG_CHECK_LAUNCH();
-    prim::exclusive_scan<unsigned long long, uint64_t>(bc, rs.bucket_start, B, A, st, rs.bucket_start + B);
 }
 
 // Serialized size of every record summed into *sum (the uncompressed bytes

@@ -66,10 +66,14 @@ struct super_list {
     uint32_t* flags = nullptr;
     uint32_t* bucket = nullptr;
     uint64_t* key = nullptr;
+    // packed form (start, len, color << 4 | flags) instead of the arrays above
+    uint4* packed = nullptr;
 };
-// `tile` = (k-1)-mers per minimizer tile: 1024 or 2048 (0 = 2048).
+// `tile` = (k-1)-mers per minimizer tile: 1024 or 2048 (0 = 2048).  With
+// `packed` (for build_records; colors must be < 2^28) only `key` and
+// `packed` are filled.
 void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
-                 cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile = 0);
+                 cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile = 0, bool packed = false);
 
 // Dedup super-k-mers into canonical bucket records.
 // Record arrays come from `out`, temporaries from A.
