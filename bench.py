@@ -345,7 +345,7 @@ def main_gpu(a):
             continue
         per_launch_ms = tot_ms / nl
         ach = alg / (per_launch_ms / 1000.0) / 1e9
-        tr = TRAFFIC_PER_UNIT.get(name)
+        tr = TRAFFIC_PER_UNIT.get(name) if k <= 31 else None  # captured with 64-bit k-mers
         roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "traffic": (tr[0] * units(name, r) * a.steps / nl) if tr else None,
                 "traffic_source": tr[1] if tr else None, "peak_kind": peak_kind,
@@ -448,8 +448,8 @@ def path_algorithmic_bytes(r, w):
 
 
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
-# of one capture, divided by the units that launch processed) and the summary
-# under profiles/ it comes from.
+# of one capture of the pangenome workload at 40 genomes, k=31, divided by the
+# units that launch processed) and the summary under profiles/ it comes from.
 TRAFFIC_PER_UNIT = {
     "k_minimizers": (1.695, "profiles/phase12_top_kernels_pangenome40.md"),   # per base
     "k_insert": (89.389, "profiles/phase12_top_kernels_pangenome40.md"),      # per occurrence

@@ -120,3 +120,26 @@ def test_gpu_phases_drive_reference_stitch_and_emit(engine, tmp_path, k):
     classes2 = formats.decode_classes(native.result_class_words(r), native.result_class_offsets(r), n)
     os.makedirs(tmp_path / "mem")
     _same(_phase34(frag2, classes2, n, k, str(tmp_path / "mem" / "out")), ref)
+
+
+@pytest.mark.gpu
+def test_gpu_pipeline_small_config_equals_reference(engine, tmp_path):
+    """The small benchmark configuration at full size (10 genomes of ~5.0 Mbp,
+    0.5% SNPs, 20 indels, mobile inserts, 1-3 contigs; k=31, -b 10): GPU phases
+    1 + 2 through the reference's phases 3 + 4 equal the reference's own
+    complete build (-t 1)."""
+    k = 31
+    _needs_ref(k)
+    p, n, k2, blog2 = synth.preset("small", seed=5)
+    assert (n, k2, blog2) == (10, 31, 10)
+    lst = synth.write_fasta(p, n, str(tmp_path / "in"))
+    ref = _reference_build(lst, k, blog2, str(tmp_path / "ref" / "out"), threads=1)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    bdir = str(tmp_path / "gb")
+    os.makedirs(bdir)
+    engine.phase1(files, k, 1 << blog2, bdir)
+    frag = str(tmp_path / "frag_unitigs.bin")
+    classes = []
+    engine.phase2(bdir, 1 << blog2, k, n, frag, None, on_class=lambda c: classes.append(list(c)))
+    os.makedirs(tmp_path / "mine")
+    _same(_phase34(frag, classes, n, k, str(tmp_path / "mine" / "out")), ref)
