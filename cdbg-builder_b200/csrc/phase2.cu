@@ -52,6 +52,7 @@ namespace {
 constexpr uint32_t NONE32 = 0xffffffffu;
 constexpr uint32_t MULTI_TAG = 0x80000000u;
 constexpr uint32_t M_LEFT = 1, M_RIGHT = 2, M_PRIMARY = 4;
+constexpr uint32_t M_MULTI = 8;  // table only: owned by two or more records
 constexpr uint32_t SK_BEGIN = 1, SK_END = 2, SK_OWNS_FIRST = 4, SK_OWNS_LAST = 8;
 constexpr uint64_t HASH_EMPTY = ~0ull;
 
@@ -131,29 +132,31 @@ __device__ __forceinline__ u128 key_load(u128 const* a) {
     return ((u128)v.y << 64) | (u128)v.x;
 }
 
-// One table slot: everything the load stage aggregates for a k-mer sits in
-// the same 32-byte sector (48 bytes for 128-bit k-mers), so an occurrence
-// touches one sector instead of one per field.
+// One table slot: everything the load stage aggregates for a k-mer in 16
+// bytes (32 for 128-bit k-mers), two slots per 32-byte sector.
+//   rank  first insertion: the batch's lowest occurrence index of the k-mer
+//         (occurrences are in (record, index) order); after numbering, the
+//         k-mer's node index
+//   om    bits 0-3: side bits, primary, M_MULTI; bits 4-31: the first owning
+//         record (relative to the batch) + 1, 0 when none
 template <typename K>
 struct slot_t;
 template <>
-struct alignas(32) slot_t<uint64_t> {
+struct alignas(16) slot_t<uint64_t> {
     uint64_t key;
-    unsigned long long rank;  // first insertion (record << 32 | index)
-    uint32_t rmin, rmax;      // owned records: min / max id
-    uint32_t meta;            // boundary side bits, primary bit
-    uint32_t node;            // node index once numbered
+    uint32_t rank;
+    uint32_t om;
 };
 template <>
 struct alignas(16) slot_t<u128> {
     u128 key;
-    unsigned long long rank;
-    uint32_t rmin, rmax;
-    uint32_t meta;
-    uint32_t node;
+    uint32_t rank;
+    uint32_t om;
+    uint64_t pad;
 };
-static_assert(sizeof(slot_t<uint64_t>) == 32, "slot layout");
-static_assert(sizeof(slot_t<u128>) == 48, "slot layout");
+static_assert(sizeof(slot_t<uint64_t>) == 16, "slot layout");
+static_assert(sizeof(slot_t<u128>) == 32, "slot layout");
+constexpr uint64_t MAX_BATCH_RECORDS = (1ull << 28) - 2;  // owner field of `om`
 
 // Insert-or-find; returns the slot (absolute) or NONE64 when the region is full.
 template <typename K>
@@ -315,11 +318,9 @@ __global__ void k_init_tables(uint64_t T, slot_t<K>* slots) {
     if (i >= T) return;
     slot_t<K> e;
     e.key = kmer_ops<K>::empty();
-    e.rank = ~0ull;
-    e.rmin = NONE32;
-    e.rmax = 0;
-    e.meta = 0;
-    e.node = NONE32;
+    e.rank = NONE32;
+    e.om = 0;
+    if constexpr (sizeof(K) == 16) e.pad = 0;
     slots[i] = e;
 }
 
@@ -345,23 +346,37 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     occ_slot[t] = (uint32_t)s | (oi.owned ? 0x80000000u : 0u);
     const uint32_t mo = oi.contrib | (oi.owned ? M_PRIMARY : 0u);
     slot_t<K>& e = T.slots[s];
-    if (mo && (e.meta & mo) != mo) atomicOr(&e.meta, mo);
-    const unsigned long long rk = ((unsigned long long)oi.r << 32) | oi.idx;
-    if (rk < e.rank) atomicMin(&e.rank, rk);
-    if (oi.owned) {
-        if (oi.r < e.rmin) atomicMin(&e.rmin, oi.r);
-        if (oi.r > e.rmax) atomicMax(&e.rmax, oi.r);
+    if ((uint32_t)t < e.rank) atomicMin(&e.rank, (uint32_t)t);
+    if (!oi.owned) {
+        if (mo && (e.om & mo) != mo) atomicOr(&e.om, mo);
+        return;
+    }
+    // owner: the first owning record, M_MULTI once a second one appears.
+    // `om` only gains bits, so the loop ends after a few changes by others.
+    const uint32_t own = (uint32_t)(oi.r - R0 + 1) << 4;
+    uint32_t old = *(volatile uint32_t*)&e.om;
+    for (int it = 0;; ++it) {
+        const uint32_t cur = old & ~0xfu;
+        const uint32_t want = (cur == own || (old & M_MULTI)) ? (old | mo)
+                              : (cur == 0)                   ? (old | own | mo)
+                                                             : (old | M_MULTI | mo);
+        if (want == old) break;
+        const uint32_t prev = atomicCAS(&e.om, old, want);
+        if (prev == old) break;
+        old = prev;
+        if (it == 64) {
+            set_error(err, ERR_CAPACITY);
+            break;
+        }
     }
 }
 
 // Bit q of `bits` <- first occurrence of each distinct k-mer.
 template <typename K>
-__global__ void k_firstbits(uint64_t T, slot_t<K> const* __restrict__ slots, uint64_t const* __restrict__ occ,
-                            uint64_t O0, uint32_t* __restrict__ bits) {
+__global__ void k_firstbits(uint64_t T, slot_t<K> const* __restrict__ slots, uint32_t* __restrict__ bits) {
     uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= T || slots[s].key == kmer_ops<K>::empty()) return;
-    const unsigned long long rk = slots[s].rank;
-    const uint64_t q = occ[rk >> 32] + (rk & 0xffffffffull) - O0;
+    const uint32_t q = slots[s].rank;
     atomicOr(&bits[q >> 5], 1u << (q & 31));
 }
 
@@ -370,28 +385,29 @@ __global__ void k_popc(uint64_t n, uint32_t const* __restrict__ bits, uint32_t* 
     if (i < n) cnt[i] = __popc(bits[i]);
 }
 
+// Number the distinct k-mers in first-insertion order; the slot's rank field
+// becomes the node index.  The bucket is the slot's table (tab_off is
+// ascending over the batch's buckets).
 template <typename K>
-__global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, uint64_t const* __restrict__ occ, uint64_t O0,
+__global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, tables<K> TB, uint32_t nb, uint64_t R0,
                              uint32_t const* __restrict__ bits, uint64_t const* __restrict__ wpre,
-                             uint32_t const* __restrict__ rbucket, K* __restrict__ n_key, uint8_t* __restrict__ n_meta,
-                             uint32_t* __restrict__ n_rec, uint32_t* __restrict__ n_bucket,
-                             uint32_t* __restrict__ node_of_slot) {
+                             K* __restrict__ n_key, uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
+                             uint32_t* __restrict__ n_bucket, uint32_t* __restrict__ node_of_slot) {
     uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= T) return;
-    slot_t<K> e = slots[s];
+    const slot_t<K> e = slots[s];
     if (e.key == kmer_ops<K>::empty()) return;
-    const unsigned long long rk = e.rank;
-    const uint64_t q = occ[rk >> 32] + (rk & 0xffffffffull) - O0;
+    const uint32_t q = e.rank;
     const uint32_t w = bits[q >> 5];
     const uint64_t n = wpre[q >> 5] + __popc(w & ((1u << (q & 31)) - 1u));
-    slots[s].node = (uint32_t)n;
-    node_of_slot[s] = (uint32_t)n;
+    slots[s].rank = (uint32_t)n;
+    node_of_slot[s] = (uint32_t)n;  // compact copy for the per-occurrence pass
     n_key[n] = e.key;
-    n_meta[n] = (uint8_t)e.meta;
+    n_meta[n] = (uint8_t)(e.om & 7u);
     uint32_t rec = NONE32;
-    if (e.meta & M_PRIMARY) rec = (e.rmin == e.rmax) ? e.rmin : MULTI_TAG;
+    if (e.om & M_PRIMARY) rec = (e.om & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (e.om >> 4) - 1);
     n_rec[n] = rec;
-    n_bucket[n] = rbucket[rk >> 32];
+    n_bucket[n] = TB.b0 + upper_bound_u64(TB.tab_off, nb + 1, s) - 1;
 }
 
 // (node << 32 | record) for owned occurrences of multi-record k-mers, from the
@@ -1117,7 +1133,7 @@ __global__ void k_node_cid(uint64_t D, uint32_t const* __restrict__ n_rec, uint3
 template <typename K>
 __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb, K x) {
     const uint64_t s = table_find<K>(T.slots, T.tab_off[tb], T.tab_cap[tb], x);
-    return s == ~0ull ? NONE32 : T.slots[s].node;
+    return s == ~0ull ? NONE32 : T.slots[s].rank;  // node index
 }
 
 template <typename K>
@@ -1798,7 +1814,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     auto mark = A.mark();
     // ---- tables
     const uint32_t nb = b1 - b0;
-    std::vector<uint64_t> toff(nb), tcap(nb);
+    std::vector<uint64_t> toff(nb + 1), tcap(nb);
     uint64_t T = 0;
     for (uint32_t b = 0; b < nb; ++b) {
         const uint64_t o = bocc[b0 + b + 1] - bocc[b0 + b];
@@ -1808,11 +1824,13 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         tcap[b] = cap;
         T += cap;
     }
+    toff[nb] = T;
     if (T >= (1ull << 31)) throw std::runtime_error("k-mer table of one bucket batch exceeds 2^31 slots");
+    if (nrec > MAX_BATCH_RECORDS) throw std::runtime_error("more than 2^28 - 2 records in one bucket");
     uint32_t* occ_slot = A.alloc<uint32_t>(nocc);
-    uint64_t* d_toff = A.alloc<uint64_t>(nb);
+    uint64_t* d_toff = A.alloc<uint64_t>(nb + 1);
     uint64_t* d_tcap = A.alloc<uint64_t>(nb);
-    CDBG_CUDA(cudaMemcpyAsync(d_toff, toff.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
+    CDBG_CUDA(cudaMemcpyAsync(d_toff, toff.data(), 8ull * (nb + 1), cudaMemcpyHostToDevice, st));
     CDBG_CUDA(cudaMemcpyAsync(d_tcap, tcap.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
     tables<K> TB;
     TB.slots = A.alloc<slot_t<K>>(T);
@@ -1841,7 +1859,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(bits, 0, 4 * nwb, st));
     {
         CDBG_PROF("k_firstbits", st);
-        k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, R.occ, O0, bits);
+        k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, bits);
     }
     CDBG_CHECK_LAUNCH();
     uint32_t* wcnt = A.alloc<uint32_t>(nwb);
@@ -1852,15 +1870,15 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     const uint64_t D = read_dev(wpre + nwb, st);
     if (D >= (1ull << 31)) throw std::runtime_error("too many distinct k-mers in one bucket batch");
     check_device_error_word(d_err, st, "k-mer table insert");
-    uint32_t* node_of_slot = A.alloc<uint32_t>(T);
     K* n_key = A.alloc<K>(D);
     uint8_t* n_meta = A.alloc<uint8_t>(D);
     uint32_t* n_rec = A.alloc<uint32_t>(D);
     uint32_t* n_bucket = A.alloc<uint32_t>(D);
+    uint32_t* node_of_slot = A.alloc<uint32_t>(T);
     {
         CDBG_PROF("k_make_nodes", st);
-        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, R.occ, O0, bits, wpre, R.bucket, n_key, n_meta,
-                                                       n_rec, n_bucket, node_of_slot);
+        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, TB, nb, R0, bits, wpre, n_key, n_meta, n_rec,
+                                                       n_bucket, node_of_slot);
     }
     CDBG_CHECK_LAUNCH();
     // ---- multi-record k-mers: (node, record) pairs in one pass, at most one
@@ -2326,11 +2344,13 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     uint32_t b = 0;
     while (b < B) {
         const uint32_t s = b;
-        uint64_t acc = 0;
+        uint64_t acc = 0, recs = 0;
         while (b < B) {
             const uint64_t ob = bocc[b + 1] - bocc[b];
-            if (b > s && acc + ob > budget) break;
+            const uint64_t rb = hbstart[b + 1] - hbstart[b];
+            if (b > s && (acc + ob > budget || recs + rb > MAX_BATCH_RECORDS)) break;
             acc += ob;
+            recs += rb;
             ++b;
         }
         run_batch<K>(rs, R, p, s, b, bocc, A, st, d_err, dict, out, hbstart, rhash, dfrag);
