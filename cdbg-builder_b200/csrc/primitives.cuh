@@ -60,31 +60,51 @@ __device__ __forceinline__ U block_exclusive_scan(U v, U* smem_warp, U& total) {
     return r;
 }
 
+// Tile sums: thread t adds elements t, t + 256, ... of the tile (coalesced).
 template <typename T, typename U>
 __global__ void __launch_bounds__(SCAN_THREADS) k_tile_sums(T const* __restrict__ in, uint64_t n,
                                                             U* __restrict__ sums) {
     __shared__ U sw[SCAN_THREADS / 32 + 1];
-    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
     U s = 0;
 #pragma unroll
-    for (int i = 0; i < SCAN_ITEMS; ++i)
-        if (base + i < n) s += (U)in[base + i];
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        const uint64_t j = base + (uint64_t)i * SCAN_THREADS + threadIdx.x;
+        if (j < n) s += (U)in[j];
+    }
     U tot;
     block_exclusive_scan<U, SCAN_THREADS>(s, sw, tot);
     if (threadIdx.x == 0) sums[blockIdx.x] = tot;
 }
 
+// Shared-memory index of tile element j, padded so that a thread reading its
+// SCAN_ITEMS consecutive elements meets no bank conflict (4- and 8-byte types).
+template <typename V>
+__device__ __forceinline__ uint32_t scan_pad(uint32_t j) {
+    return j + (j >> (sizeof(V) == 8 ? 4 : 5));
+}
+
+// Tile scan: coalesced loads and stores through shared memory; each thread
+// scans SCAN_ITEMS consecutive elements.
 template <typename T, typename U>
 __global__ void __launch_bounds__(SCAN_THREADS) k_tile_scan(T const* __restrict__ in, uint64_t n,
                                                             U const* __restrict__ offs,
                                                             U* __restrict__ out, U* total_out) {
     __shared__ U sw[SCAN_THREADS / 32 + 1];
-    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+    __shared__ T sin[SCAN_TILE + SCAN_TILE / 16];
+    __shared__ U sout[SCAN_TILE + SCAN_TILE / 16];
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        const uint32_t j = (uint32_t)i * SCAN_THREADS + threadIdx.x;
+        sin[scan_pad<T>(j)] = (base + j < n) ? in[base + j] : T(0);
+    }
+    __syncthreads();
     T v[SCAN_ITEMS];
     U s = 0;
 #pragma unroll
     for (int i = 0; i < SCAN_ITEMS; ++i) {
-        v[i] = (base + i < n) ? in[base + i] : T(0);
+        v[i] = sin[scan_pad<T>(threadIdx.x * SCAN_ITEMS + i)];
         s += (U)v[i];
     }
     U tot;
@@ -92,10 +112,16 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_tile_scan(T const* __restrict_
     p += offs ? offs[blockIdx.x] : U(0);
 #pragma unroll
     for (int i = 0; i < SCAN_ITEMS; ++i) {
-        if (base + i < n) out[base + i] = p;
+        sout[scan_pad<U>(threadIdx.x * SCAN_ITEMS + i)] = p;
         p += (U)v[i];
     }
     if (total_out && blockIdx.x == gridDim.x - 1 && threadIdx.x == SCAN_THREADS - 1) *total_out = p;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        const uint32_t j = (uint32_t)i * SCAN_THREADS + threadIdx.x;
+        if (base + j < n) out[base + j] = sout[scan_pad<U>(j)];
+    }
 }
 
 // out[i] = sum(in[0..i)), in place allowed (out == in when T == U).  When
