@@ -81,7 +81,7 @@ class BuildResult(ctypes.Structure):
                 ("n_occ", ctypes.c_uint64), ("n_distinct", ctypes.c_uint64),
                 ("n_fragments", ctypes.c_uint64), ("total_seq_bytes", ctypes.c_uint64),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
-                ("n_bases", ctypes.c_uint64), ("record_bytes", ctypes.c_uint64),
+                ("n_bases", ctypes.c_uint64),
                 ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
                 ("ms_total", ctypes.c_double)]
 
@@ -149,6 +149,7 @@ SIGNATURES = {
     "cdbg_engine_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "cdbg_engine_memory": (ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p]),
     "cdbg_engine_trim": (ctypes.c_int, [ctypes.c_void_p]),
+    "cdbg_engine_record_bytes": (ctypes.c_int, [ctypes.c_void_p, c_u64p]),
     "cdbg_engine_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     "cdbg_engine_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     "cdbg_engine_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch), ctypes.POINTER(BuildParams),
@@ -305,6 +306,12 @@ class Engine:
         _check(lib().cdbg_engine_autotune(self._h, ctypes.byref(batch), ctypes.byref(p), rounds, ctypes.byref(t),
                                           ctypes.byref(ms)))
         return {k2: getattr(t, k2) for k2, _ in Tuning._fields_}, ms.value
+
+    def record_bytes(self):
+        """Serialized bucket-record bytes of the last build()."""
+        v = ctypes.c_uint64()
+        _check(lib().cdbg_engine_record_bytes(self._h, ctypes.byref(v)))
+        return v.value
 
     def trim(self):
         """Return cached device memory to the device pool."""

@@ -310,6 +310,7 @@ int cdbg_engine_trim(cdbg_engine* e) {
     cudaSetDevice(e->device);
     e->A.reset();
     e->P.reset();
+    e->have_rs = false;
     e->A.trim();
     e->P.trim();
     e->p2.release();
@@ -630,6 +631,7 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         CDBG_CUDA(cudaSetDevice(e->device));
         e->A.reset();
         e->P.reset();
+        e->have_rs = false;
         apply_limit(e);
         cdbg_build_result res{};
         cudaEvent_t ev[4];
@@ -643,8 +645,8 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
                           p->num_colors < (1u << 28));
         cdbg::record_set rs;
         cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
-        unsigned long long* d_rec_bytes = e->P.alloc<unsigned long long>(1);
-        cdbg::record_bytes_async(rs, d_rec_bytes, e->st);
+        e->last_rs = rs;  // for cdbg_engine_record_bytes (lives in P until the next call)
+        e->have_rs = true;
         cdbg::check_device_error(e, "phase 1");
         const uint64_t n_kmers = rt.n_kmers, n_supers = sl.n, n_bases = rt.n_bases;
         e->A.reset();  // phase-1 scratch (staged input, super-k-mers, sort buffers)
@@ -693,8 +695,6 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
             res.class_offsets = out.d_offsets;
         }
         CDBG_CUDA(cudaEventRecord(ev[2], e->st));
-        unsigned long long rec_bytes = 0;
-        CDBG_CUDA(cudaMemcpyAsync(&rec_bytes, d_rec_bytes, sizeof rec_bytes, cudaMemcpyDeviceToHost, e->st));
         CDBG_CUDA(cudaEventSynchronize(ev[2]));
         CDBG_CUDA(cudaStreamSynchronize(e->st));
         float ms1 = 0, ms2 = 0;
@@ -707,7 +707,6 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         res.n_kmers = n_kmers;
         res.n_supers = n_supers;
         res.n_bases = n_bases;
-        res.record_bytes = rec_bytes;
         res.n_records = rs.n;
         res.n_occ = out.n_occ;
         res.n_distinct = out.n_distinct;
@@ -721,6 +720,27 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         return 0;
     } catch (std::exception const& ex) {
         if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
+int cdbg_engine_record_bytes(cdbg_engine* e, uint64_t* bytes) {
+    if (!e || !bytes) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    call_scope scope_(e);
+    try {
+        if (!e->have_rs) throw std::runtime_error("no in-memory build to measure");
+        CDBG_CUDA(cudaSetDevice(e->device));
+        unsigned long long* d = e->P.alloc<unsigned long long>(1);
+        cdbg::record_bytes_async(e->last_rs, d, e->st);
+        unsigned long long v = 0;
+        CDBG_CUDA(cudaMemcpyAsync(&v, d, sizeof v, cudaMemcpyDeviceToHost, e->st));
+        CDBG_CUDA(cudaStreamSynchronize(e->st));
+        *bytes = v;
+        return 0;
+    } catch (std::exception const& ex) {
         return fail(ex);
     }
 }

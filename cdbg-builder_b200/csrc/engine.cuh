@@ -9,6 +9,7 @@
 #include "cdbg_gpu.h"
 #include "arena.cuh"
 #include "common.cuh"
+#include "phase1.cuh"
 #include "phase2.cuh"
 
 // Page-locked host buffer grown on demand and kept by the engine, so host
@@ -47,6 +48,8 @@ struct cdbg_engine {
     uint32_t* d_err = nullptr;  // device error word (outside the arena)
     uint64_t mem_limit = 0;     // device memory cap of this engine (0 = none)
     cdbg_tuning tune{0, 2048, 64};
+    cdbg::record_set last_rs;  // records of the last in-memory build (in P)
+    bool have_rs = false;
     // host copies of the last cdbg_gpu_build's outputs (outputs_to_host = 1)
     pinned_buffer h_frag, h_words, h_offsets;
 };

@@ -410,6 +410,37 @@ __global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, tables<K
     n_bucket[n] = TB.b0 + upper_bound_u64(TB.tab_off, nb + 1, s) - 1;
 }
 
+// Block-wide reservation of `want` consecutive entries of *cnt per thread,
+// one atomic per block (a counter shared by millions of warps serializes
+// their atomics).  Every thread of the block must call it.
+template <int THREADS>
+__device__ __forceinline__ unsigned long long block_reserve(uint32_t want, unsigned long long* cnt) {
+    __shared__ unsigned long long s_warp[THREADS / 32];
+    __shared__ unsigned long long s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long incl = want;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long run = 0;
+        for (int w = 0; w < THREADS / 32; ++w) {
+            const unsigned long long v = s_warp[w];
+            s_warp[w] = run;
+            run += v;
+        }
+        s_base = run ? atomicAdd(cnt, run) : 0ull;
+    }
+    __syncthreads();
+    const unsigned long long r = s_base + s_warp[warp] + incl - want;
+    __syncthreads();  // the shared words may be reused by the next call
+    return r;
+}
+
 // (node << 32 | record) for owned occurrences of multi-record k-mers, from the
 // slot each occurrence recorded at insert time.
 __global__ void __launch_bounds__(256)
@@ -440,15 +471,8 @@ __global__ void __launch_bounds__(256)
             }
         }
     }
-    // warp-aggregated counter reservation
-    const uint32_t b = __ballot_sync(0xffffffffu, emit);
-    if (!b) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(b) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(cnt, (unsigned long long)__popc(b));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (emit) pairs[base + __popc(b & lanemask_lt())] = val;
+    const unsigned long long at = block_reserve<256>(emit ? 1u : 0u, cnt);
+    if (emit) pairs[at] = val;
 }
 
 __global__ void k_unique_heads(uint64_t n, uint64_t const* __restrict__ a, uint32_t* __restrict__ keep) {
@@ -1428,23 +1452,6 @@ __device__ void simulate_chain_small(chain_ws const& W, uint64_t c0, uint32_t L,
     }
 }
 
-// Per-lane reservation of `want` consecutive entries of *cnt; every lane of
-// the warp must call it.
-__device__ __forceinline__ unsigned long long warp_reserve(uint32_t want, unsigned long long* cnt) {
-    const int lane = threadIdx.x & 31;
-    unsigned long long incl = want;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned long long base = 0;
-    if (lane == 31 && total) base = atomicAdd(cnt, total);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    return base + incl - want;
-}
-
 // Path ends: nodes with at most one linked port, compacted.
 __global__ void __launch_bounds__(256) k_chain_ends(chain_ws W, uint32_t* __restrict__ ends,
                                                     unsigned long long* __restrict__ nends) {
@@ -1454,14 +1461,8 @@ __global__ void __launch_bounds__(256) k_chain_ends(chain_ws W, uint32_t* __rest
         const uint2 l = reinterpret_cast<uint2 const*>(W.link)[n];
         end = (l.x == NONE32) || (l.y == NONE32);
     }
-    const uint32_t b = __ballot_sync(0xffffffffu, end);
-    if (!b) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(b) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(nends, (unsigned long long)__popc(b));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (end) ends[base + __popc(b & lanemask_lt())] = (uint32_t)n;
+    const unsigned long long at = block_reserve<256>(end ? 1u : 0u, nends);
+    if (end) ends[at] = (uint32_t)n;
 }
 
 // Each end walks to the other end; the end with the smaller node index leads
@@ -1492,8 +1493,8 @@ __global__ void __launch_bounds__(256) k_chain_lead(chain_ws W, uint32_t const* 
             if (cc < c) lead = false;  // the other end leads
         }
     }
-    const unsigned long long c0 = warp_reserve(lead ? L : 0, W.cursor);
-    const unsigned long long h = warp_reserve(lead ? 1 : 0, nheads);
+    const unsigned long long c0 = block_reserve<256>(lead ? L : 0, W.cursor);
+    const unsigned long long h = block_reserve<256>(lead ? 1 : 0, nheads);
     if (!lead) return;
     if (c0 + L > W.D) {  // chains partition the nodes; anything else is a bug
         set_error(err, ERR_CAPACITY);

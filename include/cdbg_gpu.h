@@ -200,12 +200,16 @@ typedef struct cdbg_build_result {
     uint64_t n_kmers, n_supers, n_records, n_occ, n_distinct, n_fragments, total_seq_bytes;
     uint64_t h2d_bytes, d2h_bytes;
     uint64_t n_bases;            /* bases in ACGT runs >= k */
-    uint64_t record_bytes;       /* serialized record bytes (uncompressed bucket-file contents) */
     double ms_phase1, ms_phase2, ms_total; /* device time (CUDA events) */
 } cdbg_build_result;
 
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
                    cdbg_build_result* r);
+
+/* Serialized size of the bucket records of the engine's last cdbg_gpu_build
+ * (the uncompressed bytes its bucket files would hold), counted on the device
+ * outside the build.  Valid until the engine's next call. */
+int cdbg_engine_record_bytes(cdbg_engine* e, uint64_t* bytes);
 
 /* Autotuner: builds `b` repeatedly, searching the knobs of cdbg_tuning one at
  * a time (batch split threshold, minimizer tile, heavy-record threshold) and
