@@ -61,50 +61,73 @@ __device__ __forceinline__ uint32_t upper_bound_u64(uint64_t const* a, uint32_t 
     return lo;
 }
 
+__device__ __forceinline__ uint32_t byte_valid(uint32_t c) {
+    const uint32_t l = c | 0x20u;
+    return (l == 'a' || l == 'c' || l == 'g' || l == 't') ? 1u : 0u;
+}
+
 // Run boundary events over positions [0, nbytes]: (pos << 1) | 1 for a run
 // start, (pos << 1) for a run end.  Sequence starts (and nbytes) split runs.
+// Each thread owns 32 positions as bit masks: V = valid bases, S = sequence
+// starts, P = validity of the byte before each position; then
+//   ends   = P & (~V | S)
+//   starts = V & (S | ~P)
+// (a full 32-byte chunk is read with two 16-byte loads when aligned).
 template <bool WRITE>
 __global__ void __launch_bounds__(EV_THREADS)
     k_run_events(uint8_t const* __restrict__ ascii, uint64_t nbytes,
                  uint64_t const* __restrict__ seq_off, uint32_t num_seqs,
                  uint32_t* __restrict__ tile_count, uint64_t const* __restrict__ tile_off,
                  uint64_t* __restrict__ events) {
+    static_assert(EV_PER_THREAD == 32, "one 32-bit mask per thread");
     __shared__ uint32_t sw[EV_THREADS / 32 + 1];
     const uint64_t p0 = (uint64_t)blockIdx.x * EV_TILE + (uint64_t)threadIdx.x * EV_PER_THREAD;
-    uint32_t cnt = 0;
-    uint64_t ev[2 * EV_PER_THREAD];
+    uint32_t E = 0, St = 0;
     if (p0 <= nbytes) {
-        const uint64_t pend = (p0 + EV_PER_THREAD < nbytes + 1) ? p0 + EV_PER_THREAD : nbytes + 1;
-        // first sequence boundary strictly after p0; is p0 itself a sequence start?
-        uint32_t s = upper_bound_u64(seq_off, num_seqs + 1, p0);
-        uint64_t next_start = (s <= num_seqs) ? seq_off[s] : ~0ull;
-        bool start_here = (s > 0 && seq_off[s - 1] == p0);
+        uint32_t V = 0;
+        if (p0 + 32 <= nbytes && ((reinterpret_cast<uintptr_t>(ascii) & 15) == 0)) {
+            const uint4 a = reinterpret_cast<uint4 const*>(ascii + p0)[0];
+            const uint4 b = reinterpret_cast<uint4 const*>(ascii + p0)[1];
+            const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 32; ++i) V |= byte_valid((w[i >> 2] >> (8 * (i & 3))) & 0xffu) << i;
+        } else {
+            const uint32_t n = (uint32_t)((nbytes - p0) < 32 ? (nbytes - p0) : 32);
+            for (uint32_t i = 0; i < n; ++i) V |= byte_valid(ascii[p0 + i]) << i;
+        }
+        // sequence starts in [p0, p0 + 32), and nbytes itself
+        uint32_t S = 0;
+        uint32_t s = upper_bound_u64(seq_off, num_seqs + 1, p0);  // first boundary > p0
+        if (s > 0 && seq_off[s - 1] == p0) S |= 1u;
+        for (; s <= num_seqs && seq_off[s] < p0 + 32; ++s) S |= 1u << (uint32_t)(seq_off[s] - p0);
+        if (nbytes - p0 < 32) S |= 1u << (uint32_t)(nbytes - p0);
         // validity of the byte before p0, whatever sequence it belongs to: a
         // run of the previous sequence that ends exactly at p0 is closed here
-        bool pvalid = (p0 > 0) ? (nuc_code(ascii[p0 - 1]) != 0xffu) : false;
-        for (uint64_t p = p0; p < pend; ++p) {
-            bool is_seq_start = (p == p0) ? start_here : false;
-            while (p == next_start) {
-                is_seq_start = true;
-                ++s;
-                next_start = (s <= num_seqs) ? seq_off[s] : ~0ull;
-            }
-            if (p == nbytes) is_seq_start = true;
-            const bool valid = (p < nbytes) && nuc_code(ascii[p]) != 0xffu;
-            if (pvalid && (!valid || is_seq_start)) ev[cnt++] = p << 1;          // run end
-            if (valid && (is_seq_start || !pvalid)) ev[cnt++] = (p << 1) | 1u;  // run start
-            pvalid = valid;
+        const uint32_t pin = (p0 > 0) ? byte_valid(ascii[p0 - 1]) : 0u;
+        const uint32_t P = (V << 1) | pin;
+        E = P & (~V | S);
+        St = V & (S | ~P);
+        if (nbytes - p0 < 31) {  // positions past nbytes are not positions
+            const uint32_t keep = (2u << (uint32_t)(nbytes - p0)) - 1u;
+            E &= keep;
+            St &= keep;
         }
     }
+    const uint32_t cnt = __popc(E) + __popc(St);
+    uint32_t tot;
+    const uint32_t ex = prim::block_exclusive_scan<uint32_t, EV_THREADS>(cnt, sw, tot);
     if (!WRITE) {
-        uint32_t tot;
-        prim::block_exclusive_scan<uint32_t, EV_THREADS>(cnt, sw, tot);
         if (threadIdx.x == 0) tile_count[blockIdx.x] = tot;
-    } else {
-        uint32_t tot;
-        uint32_t ex = prim::block_exclusive_scan<uint32_t, EV_THREADS>(cnt, sw, tot);
-        uint64_t o = tile_off[blockIdx.x] + ex;
-        for (uint32_t i = 0; i < cnt; ++i) events[o + i] = ev[i];
+        return;
+    }
+    uint64_t o = tile_off[blockIdx.x] + ex;
+    uint32_t m = E | St;
+    while (m) {
+        const uint32_t i = __ffs(m) - 1;
+        m &= m - 1;
+        const uint64_t p = p0 + i;
+        if ((E >> i) & 1u) events[o++] = p << 1;           // run end
+        if ((St >> i) & 1u) events[o++] = (p << 1) | 1u;   // run start
     }
 }
 
