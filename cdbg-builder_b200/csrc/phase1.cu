@@ -264,7 +264,11 @@ __global__ void __launch_bounds__(MZ_THREADS)
         tile = s_tile;
         if (tile >= ntiles) return;
     }
-    const uint32_t r = upper_bound_u64(tile_start, nruns + 1, tile) - 1;
+    // the tile's run: one search by thread 0, shared
+    __shared__ uint32_t s_run;
+    if (threadIdx.x == 0) s_run = upper_bound_u64(tile_start, nruns + 1, tile) - 1;
+    __syncthreads();
+    const uint32_t r = s_run;
     const uint64_t t_local = tile - tile_start[r];
     const uint32_t L = len[r];
     const uint32_t W = k - m;
@@ -310,40 +314,34 @@ __global__ void __launch_bounds__(MZ_THREADS)
         }
     }
     __syncthreads();
-    // sliding minimum: smin[q] = min h[q .. q + W - 1]
-    const uint32_t per_m = (nmin + MZ_THREADS - 1) / MZ_THREADS;
+    // sliding minimum smin[q] = min h[q .. q + W - 1] by segments of W hashes
+    // (van Herk / Gil-Werman): with suf[q] the minimum from q to the end of its
+    // segment and pre[q] the minimum from its segment's start to q,
+    // smin[q] = min(suf[q], pre[q + W - 1]).  One thread per segment writes
+    // suf into smin and turns sh into pre in place; then every position takes
+    // its minimum.  No data-dependent rescans.
     {
-        const uint32_t q0 = threadIdx.x * per_m;
-        const uint32_t q1 = min(q0 + per_m, nmin);
-        if (q0 < q1) {
-            uint64_t cur = ~0ull;
-            uint32_t cp = 0;
-            for (uint32_t i = 0; i < W; ++i) {
-                const uint64_t v = sh[q0 + i];
-                if (v <= cur) {
-                    cur = v;
-                    cp = q0 + i;
-                }
+        const uint32_t nseg = (nh + W - 1) / W;
+        for (uint32_t g = threadIdx.x; g < nseg; g += MZ_THREADS) {
+            const uint32_t a = g * W, e = min(a + W, nh);
+            uint64_t run = ~0ull;
+            for (uint32_t q = e; q-- > a;) {
+                const uint64_t v = sh[q];
+                run = v < run ? v : run;
+                if (q < nmin) smin[q] = run;
             }
-            smin[q0] = cur;
-            for (uint32_t q = q0 + 1; q < q1; ++q) {
-                const uint64_t v = sh[q + W - 1];
-                if (cp < q) {
-                    cur = ~0ull;
-                    for (uint32_t i = q; i < q + W; ++i) {
-                        const uint64_t x = sh[i];
-                        if (x <= cur) {
-                            cur = x;
-                            cp = i;
-                        }
-                    }
-                } else if (v <= cur) {
-                    cur = v;
-                    cp = q + W - 1;
-                }
-                smin[q] = cur;
+            run = ~0ull;
+            for (uint32_t q = a; q < e; ++q) {
+                const uint64_t v = sh[q];
+                run = v < run ? v : run;
+                sh[q] = run;
             }
         }
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < nmin; q += MZ_THREADS) {
+        const uint64_t a = smin[q], b = sh[q + W - 1];
+        smin[q] = a < b ? a : b;
     }
     __syncthreads();
     // cut points j in [j0, j1): j == 0 or min(j) != min(j - 1).  Position c
