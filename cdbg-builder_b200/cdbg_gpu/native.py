@@ -124,6 +124,8 @@ SIGNATURES = {
     "cdbg_engine_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "cdbg_launch_count": (ctypes.c_uint64, []),
     "cdbg_engine_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "cdbg_engine_kernel_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64,
+                                                ctypes.POINTER(ctypes.c_double), ctypes.c_uint32]),
     "cdbg_engine_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64,
                                                 ctypes.POINTER(ctypes.c_double), c_u64p, ctypes.c_uint32]),
     "cdbg_gpu_supers_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -336,6 +338,17 @@ class Engine:
             raise RuntimeError("kernel stats failed")
         keys = names.raw.split(b"\0")[:min(n, cap)]
         return {keys[i].decode(): (ms[i], ln[i]) for i in range(min(n, cap))}
+
+    def kernel_bytes(self):
+        """{kernel name: algorithmic bytes} declared by the launch sites while profiling."""
+        cap = 256
+        names = ctypes.create_string_buffer(64 * cap)
+        b = (ctypes.c_double * cap)()
+        n = lib().cdbg_engine_kernel_bytes(self._h, names, len(names), b, cap)
+        if n < 0:
+            raise RuntimeError("kernel bytes failed")
+        keys = names.raw.split(b"\0")[:min(n, cap)]
+        return {keys[i].decode(): b[i] for i in range(min(n, cap))}
 
     def dump_supers(self, batch, k, m, num_buckets, path):
         n = ctypes.c_uint64()

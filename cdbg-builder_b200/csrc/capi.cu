@@ -356,9 +356,27 @@ int cdbg_engine_copy_out(cdbg_engine* e, const void* device_src, void* host_dst,
 int cdbg_engine_profile(cdbg_engine* e, int32_t enable) {
     if (!e) return -1;
     e->prof.resolve();
-    if (enable) e->prof.totals.clear();
+    if (enable) {
+        e->prof.totals.clear();
+        e->prof.bytes.clear();
+    }
     e->prof.on = enable != 0;
     return 0;
+}
+
+int cdbg_engine_kernel_bytes(cdbg_engine* e, char* names, uint64_t names_cap, double* bytes, uint32_t cap) {
+    if (!e) return -1;
+    uint32_t i = 0;
+    uint64_t used = 0;
+    for (auto const& kv : e->prof.bytes) {
+        if (i >= cap) break;
+        const uint64_t len = kv.first.size() + 1;
+        if (names && used + len <= names_cap) std::memcpy(names + used, kv.first.c_str(), len);
+        used += len;
+        if (bytes) bytes[i] = kv.second;
+        ++i;
+    }
+    return (int)e->prof.bytes.size();
 }
 
 int cdbg_engine_kernel_stats(cdbg_engine* e, char* names, uint64_t names_cap, double* ms,

@@ -31,6 +31,7 @@ struct kernel_profiler {
     std::vector<pending> open;
     std::vector<cudaEvent_t> pool;
     std::map<std::string, std::pair<double, uint64_t>> totals;  // ms, launches
+    std::map<std::string, double> bytes;  // algorithmic bytes declared at the launch sites
     cudaEvent_t get() {
         if (!pool.empty()) {
             cudaEvent_t e = pool.back();
@@ -66,10 +67,12 @@ struct prof_scope {
     cudaStream_t st;
     char const* name;
     cudaEvent_t a{};
-    prof_scope(char const* n, cudaStream_t s) : p(g_prof && g_prof->on ? g_prof : nullptr), st(s), name(n) {
+    prof_scope(char const* n, cudaStream_t s, double alg_bytes = 0)
+        : p(g_prof && g_prof->on ? g_prof : nullptr), st(s), name(n) {
         if (p) {
             a = p->get();
             cudaEventRecord(a, st);
+            if (alg_bytes > 0) p->bytes[name] += alg_bytes;
         }
     }
     ~prof_scope() {
@@ -81,6 +84,9 @@ struct prof_scope {
     }
 };
 #define CDBG_PROF(name, st) ::cdbg::prof_scope cdbg_prof_scope_(name, st)
+// Same, declaring the algorithmic bytes the launch reads and writes (the
+// roofline numerator: data it must move, not probes or re-reads).
+#define CDBG_PROF_BYTES(name, st, bytes) ::cdbg::prof_scope cdbg_prof_scope_(name, st, (double)(bytes))
 
 #define CDBG_CUDA(call)                                                                        \
     do {                                                                                       \

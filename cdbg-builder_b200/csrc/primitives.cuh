@@ -325,7 +325,8 @@ int radix_sort_pairs(uint64_t* keys, V* vals, uint64_t n, int begin_bit, int end
         CDBG_CHECK_LAUNCH();
         exclusive_scan<uint32_t, uint64_t>(counts, offs, ntiles * RS_BINS, A, st);
         {
-            CDBG_PROF("k_rs_downsweep", st);
+            // one read and one write of every (key, value) pair
+            CDBG_PROF_BYTES("k_rs_downsweep", st, 2.0 * n * (sizeof(uint64_t) + sizeof(V)));
             k_rs_downsweep<V><<<(unsigned)ntiles, RS_THREADS, 0, st>>>(kin, vin, kout, vout, n, shift,
                                                                        (uint32_t)ntiles, offs);
         }

@@ -87,6 +87,10 @@ int cdbg_engine_trim(cdbg_engine* e);
 int cdbg_engine_profile(cdbg_engine* e, int32_t enable);
 int cdbg_engine_kernel_stats(cdbg_engine* e, char* names, uint64_t names_cap, double* ms,
                              uint64_t* launches, uint32_t cap);
+/* Algorithmic bytes (data a launch must read and write, without probes,
+ * re-reads or extra passes) summed per kernel over the profiled launches,
+ * for the kernels whose launch sites declare them; same name layout. */
+int cdbg_engine_kernel_bytes(cdbg_engine* e, char* names, uint64_t names_cap, double* bytes, uint32_t cap);
 
 /* Sequences of many inputs back to back: seq[seq_off[i] .. seq_off[i+1]) is
  * sequence i (ASCII; A/C/G/T in either case are bases, anything else splits
