@@ -386,22 +386,33 @@ __global__ void k_popc(uint64_t n, uint32_t const* __restrict__ bits, uint32_t* 
 }
 
 // Number the distinct k-mers in first-insertion order; the slot's rank field
-// becomes the node index.  The bucket is the slot's table (tab_off is
-// ascending over the batch's buckets).
+// becomes the node index, and slot_of_node maps back.
 template <typename K>
-__global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, tables<K> TB, uint32_t nb, uint64_t R0,
-                             uint32_t const* __restrict__ bits, uint64_t const* __restrict__ wpre,
-                             K* __restrict__ n_key, uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
-                             uint32_t* __restrict__ n_bucket, uint32_t* __restrict__ node_of_slot) {
+__global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, uint32_t const* __restrict__ bits,
+                             uint64_t const* __restrict__ wpre, uint32_t* __restrict__ node_of_slot,
+                             uint32_t* __restrict__ slot_of_node) {
     uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= T) return;
-    const slot_t<K> e = slots[s];
-    if (e.key == kmer_ops<K>::empty()) return;
-    const uint32_t q = e.rank;
+    if (slots[s].key == kmer_ops<K>::empty()) return;
+    const uint32_t q = slots[s].rank;
     const uint32_t w = bits[q >> 5];
     const uint64_t n = wpre[q >> 5] + __popc(w & ((1u << (q & 31)) - 1u));
     slots[s].rank = (uint32_t)n;
     node_of_slot[s] = (uint32_t)n;  // compact copy for the per-occurrence pass
+    slot_of_node[n] = (uint32_t)s;
+}
+
+// Node arrays in node order (sequential writes; one slot read per node).  The
+// bucket is the slot's table (tab_off is ascending over the batch's buckets).
+template <typename K>
+__global__ void k_node_fields(uint64_t D, uint32_t const* __restrict__ slot_of_node,
+                              slot_t<K> const* __restrict__ slots, tables<K> TB, uint32_t nb, uint64_t R0,
+                              K* __restrict__ n_key, uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
+                              uint32_t* __restrict__ n_bucket) {
+    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D) return;
+    const uint32_t s = slot_of_node[n];
+    const slot_t<K> e = slots[s];
     n_key[n] = e.key;
     n_meta[n] = (uint8_t)(e.om & 7u);
     uint32_t rec = NONE32;
@@ -1876,10 +1887,16 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint32_t* n_rec = A.alloc<uint32_t>(D);
     uint32_t* n_bucket = A.alloc<uint32_t>(D);
     uint32_t* node_of_slot = A.alloc<uint32_t>(T);
+    uint32_t* slot_of_node = A.alloc<uint32_t>(D);
     {
         CDBG_PROF("k_make_nodes", st);
-        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, TB, nb, R0, bits, wpre, n_key, n_meta, n_rec,
-                                                       n_bucket, node_of_slot);
+        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, bits, wpre, node_of_slot, slot_of_node);
+    }
+    CDBG_CHECK_LAUNCH();
+    {
+        CDBG_PROF("k_node_fields", st);
+        k_node_fields<K><<<grid(D, 256), 256, 0, st>>>(D, slot_of_node, TB.slots, TB, nb, R0, n_key, n_meta, n_rec,
+                                                        n_bucket);
     }
     CDBG_CHECK_LAUNCH();
     // ---- multi-record k-mers: (node, record) pairs in one pass, at most one
