@@ -636,6 +636,103 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
     }
 }
 
+namespace {
+
+// Phase 1 of an in-memory build from host sequences, overlapped with the
+// upload: the sequence bytes go to the device in pieces on the copy stream,
+// and the runs and super-k-mers of each piece are found while the later
+// pieces are still in flight.  Pieces end at sequence boundaries, so no run
+// spans two of them; all pieces pack into one 2-bit stream, and their
+// super-k-mer lists are concatenated in input order (the order the single
+// pass produces).
+void phase1_pipelined(cdbg_engine* e, cdbg_seq_batch const* b, uint32_t k, uint32_t m, uint32_t B,
+                      uint32_t pieces, cdbg::run_table& rt_all, cdbg::super_list& sl_all, uint64_t* h2d) {
+    const uint64_t N = b->seq_bytes;
+    const uint32_t S = b->num_seqs;
+    cudaStream_t st = e->st;
+    uint8_t* d_ascii = e->A.alloc<uint8_t>(N + 16);
+    uint32_t* d_color = e->A.alloc<uint32_t>((uint64_t)S + 1);
+    CDBG_CUDA(cudaMemcpyAsync(d_color, b->seq_color, 4ull * S, cudaMemcpyHostToDevice, st));
+    // piece boundaries (sequence indices) near equal byte shares
+    std::vector<uint32_t> cut{0};
+    for (uint32_t s = 1; s < S && cut.size() < pieces; ++s)
+        if (b->seq_off[s] >= (N / pieces) * cut.size()) cut.push_back(s);
+    cut.push_back(S);
+    const size_t np = cut.size() - 1;
+    // every piece's offsets rebased to its first byte, uploaded before the
+    // sequence bytes (a small upload queued behind them would stall the host)
+    std::vector<uint64_t> off((uint64_t)S + np);
+    std::vector<uint64_t> off_at(np);
+    {
+        uint64_t o = 0;
+        for (size_t i = 0; i < np; ++i) {
+            off_at[i] = o;
+            const uint64_t b0 = b->seq_off[cut[i]];
+            for (uint32_t s = cut[i]; s <= cut[i + 1]; ++s) off[o++] = b->seq_off[s] - b0;
+        }
+    }
+    uint64_t* d_off = e->A.alloc<uint64_t>(off.size());
+    CDBG_CUDA(cudaMemcpyAsync(d_off, off.data(), 8 * off.size(), cudaMemcpyHostToDevice, st));
+    // the copies start after this call's allocations and small uploads (ordered on st)
+    CDBG_CUDA(cudaEventRecord(e->copy_ev, st));
+    CDBG_CUDA(cudaStreamWaitEvent(e->copy_st, e->copy_ev, 0));
+    std::vector<cudaEvent_t> ev(np);
+    for (auto& x : ev) CDBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    for (size_t i = 0; i < np; ++i) {
+        const uint64_t b0 = b->seq_off[cut[i]], b1 = b->seq_off[cut[i + 1]];
+        if (b1 > b0)
+            CDBG_CUDA(cudaMemcpyAsync(d_ascii + b0, b->seq + b0, b1 - b0, cudaMemcpyHostToDevice, e->copy_st));
+        CDBG_CUDA(cudaEventRecord(ev[i], e->copy_st));
+    }
+    // every kept run has >= k bases and is padded to whole words
+    const uint64_t cap = N / 32 + N / std::max<uint32_t>(k, 1) + 64 * np + 64;
+    uint64_t* words = e->P.alloc<uint64_t>(cap);
+    uint64_t base = 0, n_kmers = 0, n_bases = 0;
+    std::vector<cdbg::super_list> lists;
+    for (size_t i = 0; i < np; ++i) {
+        const uint64_t b0 = b->seq_off[cut[i]], b1 = b->seq_off[cut[i + 1]];
+        const uint32_t ns = cut[i + 1] - cut[i];
+        CDBG_CUDA(cudaStreamWaitEvent(st, ev[i], 0));
+        cdbg::seq_input in;
+        in.ascii = d_ascii + b0;
+        in.nbytes = b1 - b0;
+        in.seq_off = d_off + off_at[i];
+        in.seq_color = d_color + cut[i];
+        in.num_seqs = ns;
+        cdbg::run_table rt;
+        cdbg::build_runs(in, k, e->A, st, rt, e->P, words, base, cap);
+        if (rt.n == 0) continue;
+        base = rt.nwords - 8;
+        n_kmers += rt.n_kmers;
+        n_bases += rt.n_bases;
+        cdbg::super_list sl;
+        cdbg::find_supers(rt, k, m, B, e->A, st, sl, e->d_err, e->tune.minimizer_tile, true);
+        if (sl.n) lists.push_back(sl);
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    uint64_t n = 0;
+    for (auto const& l : lists) n += l.n;
+    if (n >= 0xffffffffull) throw std::runtime_error("more than 2^32 super-k-mers in one call");
+    sl_all = cdbg::super_list();
+    sl_all.n = n;
+    sl_all.key = e->A.alloc<uint64_t>(n + 1);
+    sl_all.packed = e->A.alloc<uint4>(n + 1);
+    uint64_t o = 0;
+    for (auto const& l : lists) {
+        CDBG_CUDA(cudaMemcpyAsync(sl_all.key + o, l.key, 8 * l.n, cudaMemcpyDeviceToDevice, st));
+        CDBG_CUDA(cudaMemcpyAsync(sl_all.packed + o, l.packed, 16 * l.n, cudaMemcpyDeviceToDevice, st));
+        o += l.n;
+    }
+    rt_all = cdbg::run_table();
+    rt_all.words = words;
+    rt_all.nwords = base + 8;
+    rt_all.n_kmers = n_kmers;
+    rt_all.n_bases = n_bases;
+    if (h2d) *h2d += N + 8ull * (S + 1) + 4ull * S;
+}
+
+}  // namespace
+
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p, cdbg_build_result* r) {
     if (!e) {
         g_last_error = "null engine";
@@ -655,12 +752,16 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         cudaEvent_t ev[4];
         for (auto& x : ev) CDBG_CUDA(cudaEventCreate(&x));
         CDBG_CUDA(cudaEventRecord(ev[0], e->st));
-        cdbg::seq_input in = stage_batch(e, b, &res.h2d_bytes);
         cdbg::run_table rt;
-        cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
         cdbg::super_list sl;
-        cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile,
-                          p->num_colors < (1u << 28));
+        const bool packed = p->num_colors < (1u << 28);
+        if (!b->on_device && packed && b->num_seqs >= 8 && b->seq_bytes >= (64ull << 20)) {
+            phase1_pipelined(e, b, k, m, p->num_buckets, 4, rt, sl, &res.h2d_bytes);
+        } else {
+            cdbg::seq_input in = stage_batch(e, b, &res.h2d_bytes);
+            cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
+            cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile, packed);
+        }
         cdbg::record_set rs;
         cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
         e->last_rs = rs;  // for cdbg_engine_record_bytes (lives in P until the next call)

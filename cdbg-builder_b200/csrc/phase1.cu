@@ -628,6 +628,11 @@ __global__ void k_bucket_bounds(uint64_t n, uint32_t const* __restrict__ rb, uin
         for (uint32_t x = b + 1; x <= B; ++x) bucket_start[x] = n;
 }
 
+__global__ void k_add_u64(uint64_t* p, uint64_t n, uint64_t v) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] += v;
+}
+
 __global__ void k_fill_u32(uint32_t* p, uint64_t n, uint32_t v) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
@@ -788,7 +793,7 @@ T read_dev(T const* p, cudaStream_t st) {
 
 // ----------------------------------------------------------------- host side
 void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt,
-                dev_arena& out) {
+                dev_arena& out, uint64_t* words_out, uint64_t word_base, uint64_t words_cap) {
     rt = run_table();
     const uint64_t npos = in.nbytes + 1;
     const uint64_t tiles = ceil_div(npos, EV_TILE);
@@ -838,14 +843,28 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
     prim::exclusive_scan<uint64_t, uint64_t>(padded, rt.soff, nruns, A, st, rt.soff + nruns);
     const uint64_t total = read_dev(rt.soff + nruns, st);
     const uint64_t nwd = total / 32;
-    rt.nwords = nwd + 8;
-    rt.words = out.alloc<uint64_t>(rt.nwords);
-    CDBG_CUDA(cudaMemsetAsync(rt.words + nwd, 0, 8 * 8, st));
+    uint64_t* dst;
+    if (words_out) {
+        // this batch's runs go at word `word_base` of a shared stream
+        if (word_base + nwd + 8 > words_cap) throw std::runtime_error("2-bit stream capacity exceeded");
+        rt.words = words_out;
+        rt.nwords = word_base + nwd + 8;
+        dst = words_out + word_base;
+    } else {
+        rt.nwords = nwd + 8;
+        rt.words = out.alloc<uint64_t>(rt.nwords);
+        dst = rt.words;
+    }
+    CDBG_CUDA(cudaMemsetAsync(dst + nwd, 0, 8 * 8, st));
     if (nwd) {
         {
             CDBG_PROF("k_pack", st);
-            k_pack<<<grid(nwd, 256), 256, 0, st>>>(in.ascii, rt.n, rt.soff, rt.src, rt.len, nwd, rt.words);
+            k_pack<<<grid(nwd, 256), 256, 0, st>>>(in.ascii, rt.n, rt.soff, rt.src, rt.len, nwd, dst);
         }
+        CDBG_CHECK_LAUNCH();
+    }
+    if (words_out && word_base) {
+        k_add_u64<<<grid(nruns + 1, 256), 256, 0, st>>>(rt.soff, nruns + 1, word_base * 32);
         CDBG_CHECK_LAUNCH();
     }
     unsigned long long* acc = A.alloc<unsigned long long>(2);

@@ -53,8 +53,11 @@ struct phase1_stats {
 };
 
 // Runs + packing: ASCII -> 2-bit stream of ACGT runs >= k.
-// The 2-bit stream (rt.words) comes from `out`, everything else from A.
-void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt, dev_arena& out);
+// The 2-bit stream (rt.words) comes from `out`, everything else from A.  With
+// `words_out`, the runs are packed at word `word_base` of that stream instead
+// (capacity `words_cap` words) and rt.soff / rt.words / rt.nwords refer to it.
+void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, run_table& rt, dev_arena& out,
+                uint64_t* words_out = nullptr, uint64_t word_base = 0, uint64_t words_cap = 0);
 
 // Super-k-mer occurrences of every run (for parity tests): arrays in input
 // order, allocated from the arena.  Returns the count.

@@ -148,3 +148,35 @@ def test_streamed_host_outputs_match_across_build_sizes(tmp_path):
         assert outs(e, small, 3, 1 << 10) == want_s   # streamed into the larger buffer
     finally:
         e.close()
+
+
+def test_pipelined_host_upload_matches_device_input():
+    """Host inputs of 64 MB and more are uploaded in pieces while phase 1
+    works on the pieces already on the device; the outputs equal those of
+    the same sequences given already in device memory (one pass)."""
+    import torch
+    p, _, k, blog2 = synth.preset("small", seed=9)
+    n = 16
+    seq, lens, per = synth.collection(p, n)
+    assert seq.nbytes >= (64 << 20)
+    off = np.zeros(len(lens) + 1, dtype=np.uint64)
+    off[1:] = np.cumsum(lens)
+    colors = np.repeat(np.arange(n, dtype=np.uint32), per)
+    e = native.Engine(0)
+    try:
+        r = e.build(native.array_batch(seq, off, colors), k, 1 << blog2, n)
+        host = (native.result_frag_bytes(r), native.result_class_words(r), native.result_class_offsets(r),
+                r.n_kmers, r.n_supers, r.n_records)
+        d_seq = torch.from_numpy(seq).cuda()
+        d_off = torch.from_numpy(off.view(np.int64)).cuda()
+        d_col = torch.from_numpy(colors.view(np.int32)).cuda()
+        torch.cuda.synchronize()
+        b = native.SeqBatch(d_seq.data_ptr(), seq.nbytes, d_off.data_ptr(), d_col.data_ptr(), len(colors), 1)
+        r2 = e.build(b, k, 1 << blog2, n)
+        dev = (native.result_frag_bytes(r2), native.result_class_words(r2), native.result_class_offsets(r2),
+               r2.n_kmers, r2.n_supers, r2.n_records)
+    finally:
+        e.close()
+    assert host[0] == dev[0]
+    assert np.array_equal(host[1], dev[1]) and np.array_equal(host[2], dev[2])
+    assert host[3:] == dev[3:]
