@@ -783,6 +783,12 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
             pp.frag_host_cap = e->h_frag.cap;
             pp.copy_st = e->copy_st;
             pp.copy_ev = e->copy_ev;
+            if (e->h_words.p && e->h_offsets.p) {
+                pp.words_host = (uint64_t*)e->h_words.p;
+                pp.words_host_cap = e->h_words.cap / 8;
+                pp.offs_host = (uint64_t*)e->h_offsets.p;
+                pp.offs_host_cap = e->h_offsets.cap / 8;
+            }
         }
         cdbg::phase2_result out;
         out.state = &e->p2;
@@ -795,15 +801,24 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
                 CDBG_CUDA(cudaEventRecord(e->copy_ev, e->copy_st));
                 CDBG_CUDA(cudaStreamWaitEvent(e->st, e->copy_ev, 0));
             }
-            if (!streamed) CDBG_CUDA(cudaStreamSynchronize(e->copy_st));  // before the buffer may move
+            // a streamed prefix is kept only if its buffer holds the whole output
+            const bool w_ok = pp.words_host && 8 * nwords + 8 <= e->h_words.cap;
+            const bool o_ok = pp.offs_host && 8 * out.n_classes + 8 <= e->h_offsets.cap;
+            if (!streamed || !w_ok || !o_ok)
+                CDBG_CUDA(cudaStreamSynchronize(e->copy_st));  // before a buffer may move
             void* hf = streamed ? e->h_frag.p : e->h_frag.ensure(out.frag_nbytes + 8);
-            void* hw = e->h_words.ensure(8 * nwords + 8);
-            void* ho = e->h_offsets.ensure(8 * out.n_classes + 8);
+            void* hw = w_ok ? e->h_words.p : e->h_words.ensure(8 * nwords + 8);
+            void* ho = o_ok ? e->h_offsets.p : e->h_offsets.ensure(8 * out.n_classes + 8);
             if (out.frag_nbytes && !streamed)
                 CDBG_CUDA(cudaMemcpyAsync(hf, out.d_frag, out.frag_nbytes, cudaMemcpyDeviceToHost, e->st));
-            if (nwords) CDBG_CUDA(cudaMemcpyAsync(hw, out.d_words, 8 * nwords, cudaMemcpyDeviceToHost, e->st));
-            if (out.n_classes)
-                CDBG_CUDA(cudaMemcpyAsync(ho, out.d_offsets, 8 * out.n_classes, cudaMemcpyDeviceToHost, e->st));
+            const uint64_t wfrom = w_ok ? out.words_host_copied : 0;
+            if (nwords > wfrom)
+                CDBG_CUDA(cudaMemcpyAsync((uint64_t*)hw + wfrom, out.d_words + wfrom, 8 * (nwords - wfrom),
+                                          cudaMemcpyDeviceToHost, e->st));
+            const uint64_t ofrom = o_ok ? out.offs_host_copied : 0;
+            if (out.n_classes > ofrom)
+                CDBG_CUDA(cudaMemcpyAsync((uint64_t*)ho + ofrom, out.d_offsets + ofrom, 8 * (out.n_classes - ofrom),
+                                          cudaMemcpyDeviceToHost, e->st));
             res.frag_bytes = (const uint8_t*)hf;
             res.class_words = (const uint64_t*)hw;
             res.class_offsets = (const uint64_t*)ho;

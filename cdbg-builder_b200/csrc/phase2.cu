@@ -2160,6 +2160,11 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             prim::exclusive_scan<uint64_t, uint64_t>(nbits, boff, nnew, A, st, boff + nnew);
             const uint64_t badd = read_dev(boff + nnew, st);
             add_offsets(boff, nnew + 1, dict.nbits, boff, st);  // absolute bit offsets
+            if (p.copy_st) {
+                // growing frees the old arrays: after the host copies that read them
+                CDBG_CUDA(cudaEventRecord(p.copy_ev, p.copy_st));
+                CDBG_CUDA(cudaStreamWaitEvent(st, p.copy_ev, 0));
+            }
             dict.cls_hash.reserve(base + nnew, st);
             dict.bit_off.reserve(base + nnew + 1, st);
             CDBG_CUDA(cudaMemcpyAsync(dict.cls_hash.p + base, nh, 8 * nnew, cudaMemcpyDeviceToDevice, st));
@@ -2303,6 +2308,27 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             CDBG_CUDA(cudaMemcpyAsync(p.frag_host + old_n, dfrag.p + old_n, fbytes, cudaMemcpyDeviceToHost,
                                       p.copy_st));
             out.frag_host_copied = dfrag.n;
+        }
+    }
+    if (!p.to_host && p.copy_st) {
+        // completed class words (all but the one later classes still fill) and
+        // class offsets go to the host while the next batch runs
+        const uint64_t wdone = dict.nbits / 64;
+        const bool words_go = p.words_host && out.words_host_copied < wdone && wdone <= p.words_host_cap;
+        const bool offs_go = p.offs_host && out.offs_host_copied < dict.n && dict.n <= p.offs_host_cap;
+        if (words_go || offs_go) {
+            CDBG_CUDA(cudaEventRecord(p.copy_ev, st));
+            CDBG_CUDA(cudaStreamWaitEvent(p.copy_st, p.copy_ev, 0));
+        }
+        if (words_go) {
+            CDBG_CUDA(cudaMemcpyAsync(p.words_host + out.words_host_copied, dict.words.p + out.words_host_copied,
+                                      8 * (wdone - out.words_host_copied), cudaMemcpyDeviceToHost, p.copy_st));
+            out.words_host_copied = wdone;
+        }
+        if (offs_go) {
+            CDBG_CUDA(cudaMemcpyAsync(p.offs_host + out.offs_host_copied, dict.bit_off.p + out.offs_host_copied,
+                                      8 * (dict.n - out.offs_host_copied), cudaMemcpyDeviceToHost, p.copy_st));
+            out.offs_host_copied = dict.n;
         }
     }
     CDBG_CUDA(cudaStreamSynchronize(st));

@@ -45,6 +45,8 @@ struct phase2_state {
 // Outputs of phase 2, accumulated over bucket batches.
 struct phase2_result {
     uint64_t frag_host_copied = 0;  // leading frag bytes queued to params.frag_host
+    uint64_t words_host_copied = 0; // leading class words queued to params.words_host
+    uint64_t offs_host_copied = 0;  // leading class offsets queued to params.offs_host
     // frag_unitigs.bin bytes (unitig_spill.hpp:642-665 record layout), in
     // bucket order and, per bucket, in seed order.
     std::vector<uint8_t> frag;          // host copy (when to_host)
@@ -83,6 +85,12 @@ struct phase2_params {
     // as they fit in `frag_host_cap` (nothing is streamed when null).
     uint8_t* frag_host = nullptr;
     uint64_t frag_host_cap = 0;
+    // likewise the class dictionary's completed bit-vector words and class
+    // offsets (capacities in entries)
+    uint64_t* words_host = nullptr;
+    uint64_t words_host_cap = 0;
+    uint64_t* offs_host = nullptr;
+    uint64_t offs_host_cap = 0;
     cudaStream_t copy_st = nullptr;
     cudaEvent_t copy_ev = nullptr;
 };

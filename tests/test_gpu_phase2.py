@@ -125,17 +125,18 @@ def test_union_list_path_matches_bitmap_path(engine, tmp_path, monkeypatch):
 
 
 def test_streamed_host_outputs_match_across_build_sizes(tmp_path):
-    """Host outputs of in-memory builds, whose fragment bytes go to pinned
-    memory batch by batch while later batches run once the engine's buffer is
-    large enough (else in one copy at the end): identical whatever the order
-    of build sizes and bucket-batch sizes."""
+    """Host outputs of in-memory builds, whose fragment bytes, class words
+    and class offsets go to pinned memory batch by batch while later batches
+    run once the engine's buffers are large enough (else in one copy at the
+    end): identical whatever the order of build sizes and bucket-batch sizes."""
     small = native.HostSequences([l.strip() for l in open(_fresh(tmp_path / "s", 61, 3)) if l.strip()])
     large = native.HostSequences([l.strip() for l in open(_fresh(tmp_path / "l", 62, 12)) if l.strip()])
     B, k = 256, 31
 
     def outs(e, hs, n, batch_occ=0):
         r = e.build(hs.batch, k, B, n, batch_occ=batch_occ)
-        return native.result_frag_bytes(r), native.result_class_words(r).tobytes()
+        return (native.result_frag_bytes(r), native.result_class_words(r).tobytes(),
+                native.result_class_offsets(r).tobytes())
 
     ref = native.Engine(0)
     want_s, want_l = outs(ref, small, 3), outs(ref, large, 12)
