@@ -7,16 +7,18 @@
 //  load     one thread per k-mer occurrence rolls its canonical k-mer straight
 //           from the 2-bit record stream and aggregates it into its bucket's
 //           open-addressing table (load_bucket, bucket_walker.hpp:166-255):
-//           boundary side bits OR-ed, `primary` OR-ed, owned records' min/max
-//           record id, and the first-insertion rank (record, index) by atomicMin.
+//           boundary side bits and `primary` OR-ed, the first owning record
+//           plus a second-owner bit, and the first-insertion rank (the
+//           occurrence index, in (record, index) order) by atomicMin.
 //  nodes    distinct k-mers are numbered in first-insertion order -- the
 //           iteration order of the reference's insertion-ordered map, which is
 //           its seed and class order -- by marking each k-mer's first
 //           occurrence in a bitmap over the batch's occurrences and scanning it.
 //  resolve  a primary k-mer owned by one record has that record's color set;
 //           one owned by several records gets the union of their sets
-//           (bucket_walker.hpp:360-428), built in a per-warp shared-memory
-//           bitmap.  Sets are hashed (order-independent 64-bit set hash) and
+//           (bucket_walker.hpp:360-428), built once per run of k-mers with the
+//           same owning records in a per-warp shared-memory bitmap.  Sets are
+//           hashed (order-independent 64-bit set hash) and
 //           interned in a global device dictionary with full list equality;
 //           new classes get global ids in order of first appearance (bucket,
 //           then insertion rank), which is the id order of the reference's
