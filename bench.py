@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch-occ", type=int, default=0)
+    ap.add_argument("--table-slots-q", type=int, default=0,
+                    help="k-mer table slots per 4 occurrences, 5..16 (0 = library default)")
     ap.add_argument("--autotune", action="store_true",
                     help="run the autotuner on the workload before timing (default for skewed)")
     ap.add_argument("--compare-plain", action="store_true",
@@ -269,6 +271,8 @@ def main_gpu(a):
 
     skewed = a.workload == "skewed"
     tuned = None
+    if a.table_slots_q:
+        eng.set_tuning(table_slots_q=a.table_slots_q)
     if a.autotune or skewed:
         t0 = time.time()
         tcfg, tms = eng.autotune(dev_batch, k, B, n_genomes)
@@ -383,7 +387,8 @@ def main_gpu(a):
                 "config": {"workload": workload_name(n_genomes, k, B, a.workload),
                            "kmers_per_step": int(job_kmers), "bases": int(seq.nbytes),
                            "l2": "inputs (%.1f GB) larger than L2" % (seq.nbytes / 1e9),
-                           "parallelism": "replicas%d" % world, "generate_s": gen_s},
+                           "parallelism": "replicas%d" % world, "generate_s": gen_s,
+                           "tuning": eng.tuning()},
                 "counts": {"supers": int(r.n_supers), "records": int(r.n_records), "occ": int(r.n_occ),
                            "distinct": int(r.n_distinct), "fragments": int(r.n_fragments),
                            "color_sets": int(r.n_color_sets), "frag_bytes": int(r.frag_nbytes)},

@@ -88,7 +88,7 @@ class BuildResult(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("batch_occ", ctypes.c_uint64), ("minimizer_tile", ctypes.c_uint32),
-                ("heavy_colors", ctypes.c_uint32)]
+                ("heavy_colors", ctypes.c_uint32), ("table_slots_q", ctypes.c_uint32)]
 
 
 class ServerParams(ctypes.Structure):
@@ -292,8 +292,9 @@ class Engine:
         _check(lib().cdbg_engine_memory(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
-    def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0):
-        _check(lib().cdbg_engine_set_tuning(self._h, ctypes.byref(Tuning(batch_occ, minimizer_tile, heavy_colors))))
+    def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0, table_slots_q=0):
+        _check(lib().cdbg_engine_set_tuning(self._h, ctypes.byref(Tuning(batch_occ, minimizer_tile, heavy_colors,
+                                                                         table_slots_q))))
 
     def tuning(self):
         t = Tuning()

@@ -589,6 +589,7 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         pp.num_colors = a->num_colors;
         pp.batch_occ = a->batch_occ ? a->batch_occ : e->tune.batch_occ;
         pp.heavy_colors = e->tune.heavy_colors;
+        pp.table_slots_q = e->tune.table_slots_q;
         pp.to_host = true;
         cdbg::phase2_result res;
         res.state = &e->p2;
@@ -775,6 +776,7 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         pp.num_colors = p->num_colors;
         pp.batch_occ = p->batch_occ ? p->batch_occ : e->tune.batch_occ;
         pp.heavy_colors = e->tune.heavy_colors;
+        pp.table_slots_q = e->tune.table_slots_q;
         pp.to_host = false;  // outputs accumulate in HBM
         if (p->outputs_to_host && e->h_frag.p && e->h_frag.cap) {
             // stream each batch's fragments into the (already large enough,
@@ -887,8 +889,13 @@ int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
     cdbg_tuning v = *t;
     if (v.minimizer_tile == 0) v.minimizer_tile = 2048;
     if (v.heavy_colors == 0) v.heavy_colors = 64;
+    if (v.table_slots_q == 0) v.table_slots_q = 8;
     if (v.minimizer_tile != 1024 && v.minimizer_tile != 2048) {
         g_last_error = "minimizer_tile must be 1024 or 2048";
+        return -1;
+    }
+    if (v.table_slots_q < 5 || v.table_slots_q > 16) {
+        g_last_error = "table_slots_q must be in [5, 16]";
         return -1;
     }
     e->tune = v;
@@ -929,6 +936,7 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
         cdbg_tuning cur = e->tune;
         if (cur.minimizer_tile == 0) cur.minimizer_tile = 2048;
         if (cur.heavy_colors == 0) cur.heavy_colors = 64;
+        if (cur.table_slots_q == 0) cur.table_slots_q = 8;
         measure(cur);  // warm-up: allocations reach their working sizes
         double cur_ms = measure(cur);
         auto consider = [&](cdbg_tuning const& t) {
@@ -952,6 +960,11 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
             cdbg_tuning t = cur;
             t.heavy_colors = v;
             if (t.heavy_colors != cur.heavy_colors) consider(t);
+        }
+        for (uint32_t v : {8u, 6u, 5u}) {
+            cdbg_tuning t = cur;
+            t.table_slots_q = v;
+            if (t.table_slots_q != cur.table_slots_q) consider(t);
         }
         e->tune = cur;
         if (best) *best = cur;

@@ -581,6 +581,37 @@ __device__ __forceinline__ uint64_t warp_excl_scan64(uint64_t v, uint64_t& total
     return x - v;
 }
 
+// OR the ascending list [c0, c1) of `list` into the shared bitmap `bm` of
+// `nw` words (all 32 lanes call it).  A dense list (at least one element per
+// 4 bit positions: 8 or more lanes per word) has the lanes holding the same
+// word (consecutive lanes) combine their bits first, the first of them alone
+// touching shared memory; a sparser one ORs lane by lane.  An unsorted list
+// is ORed correctly either way.
+__device__ __forceinline__ void warp_or_list(uint32_t* bm, uint32_t const* __restrict__ list, uint64_t c0,
+                                             uint64_t c1, uint32_t nw, int lane) {
+    if ((c1 - c0) * 4 < (uint64_t)nw * 32) {
+        for (uint64_t c = c0 + lane; c < c1; c += 32) {
+            const uint32_t v = list[c];
+            atomicOr(&bm[v >> 5], 1u << (v & 31));
+        }
+        return;
+    }
+    for (uint64_t base = c0; base < c1; base += 32) {
+        const bool in = base + lane < c1;
+        const uint32_t v = in ? list[base + lane] : NONE32;
+        const uint32_t w = v >> 5;
+        uint32_t b = in ? 1u << (v & 31) : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t ob = __shfl_down_sync(0xffffffffu, b, o);
+            const uint32_t ow = __shfl_down_sync(0xffffffffu, w, o);
+            if (lane + o < 32 && ow == w) b |= ob;
+        }
+        const uint32_t pw = __shfl_up_sync(0xffffffffu, w, 1);
+        if (in && (lane == 0 || pw != w)) atomicOr(&bm[w], b);
+    }
+}
+
 // Union of the color lists of a multi-record node.  Pass 0: size and hash;
 // pass 1: write the ascending list at pool[poff[m]].
 template <bool WRITE>
@@ -599,11 +630,7 @@ __global__ void k_union(uint64_t M, uint64_t const* __restrict__ mbeg, uint64_t 
     __syncwarp();
     for (uint64_t p = mbeg[m]; p < mend[m]; ++p) {
         const uint32_t r = (uint32_t)(upairs[p] & 0xffffffffu);
-        const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
-        for (uint64_t c = c0 + lane; c < c1; c += 32) {
-            const uint32_t v = colors[c];
-            atomicOr(&bm[v >> 5], 1u << (v & 31));
-        }
+        warp_or_list(bm, colors, col_off[r], col_off[r + 1], nw, lane);
     }
     __syncwarp();
     const uint32_t per = (nw + 31) / 32;
@@ -657,11 +684,7 @@ __global__ void k_heavy_bitmaps(uint64_t nrec, uint32_t const* __restrict__ flag
     if (i >= nrec || !flag[i]) return;
     for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
     __syncwarp();
-    const uint64_t c0 = col_off[R0 + i], c1 = col_off[R0 + i + 1];
-    for (uint64_t c = c0 + lane; c < c1; c += 32) {
-        const uint32_t v = colors[c];
-        atomicOr(&bm[v >> 5], 1u << (v & 31));
-    }
+    warp_or_list(bm, colors, col_off[R0 + i], col_off[R0 + i + 1], nw, lane);
     __syncwarp();
     uint32_t* out = rbits + hpos[i] * (uint64_t)nw;
     for (uint32_t w = lane; w < nw; w += 32) out[w] = bm[w];
@@ -689,11 +712,7 @@ __global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ mbeg, uint64
             for (uint32_t w = lane; w < nw; w += 32) bm[w] |= rb[w];  // lanes own distinct words
         } else {
             __syncwarp();
-            const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
-            for (uint64_t c = c0 + lane; c < c1; c += 32) {
-                const uint32_t v = colors[c];
-                atomicOr(&bm[v >> 5], 1u << (v & 31));
-            }
+            warp_or_list(bm, colors, col_off[r], col_off[r + 1], nw, lane);
             __syncwarp();
         }
     }
@@ -885,10 +904,7 @@ __global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint
     } else {
         for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
         __syncwarp();
-        for (uint64_t i = lane; i < N; i += 32) {
-            const uint32_t v = cs.list[i];
-            atomicOr(&bm[v >> 5], 1u << (v & 31));
-        }
+        warp_or_list(bm, cs.list, 0, N, nw, lane);
     }
     __syncwarp();
     const uint64_t sparse_t = (uint64_t)(0.25 * (double)C);
@@ -1030,37 +1046,161 @@ __global__ void k_iota32(uint64_t n, uint32_t* __restrict__ p) {
     if (i < n) p[i] = (uint32_t)i;
 }
 
-__device__ __forceinline__ bool lists_equal(uint32_t const* a, uint64_t na, uint32_t const* b, uint64_t nb) {
-    if (na != nb) return false;
-    for (uint64_t i = 0; i < na; ++i)
-        if (a[i] != b[i]) return false;
+// Set comparison split by length.  A set of at most SHORT_SET words is
+// compared by its own lane, eight loads in flight at a time; a longer one by
+// the whole warp, lanes reading consecutive words (one coalesced line per
+// list per 32 words, four lines in flight per round).
+constexpr uint64_t SHORT_SET = 32;
+
+__device__ __forceinline__ uint64_t set_words(cand_set const& a, cand_set const& b, uint32_t nw) {
+    return (a.bm && b.bm) ? nw : a.n;
+}
+
+// Lane-local equality of two sets of equal size.
+__device__ __forceinline__ bool lane_sets_equal(cand_set const& a, cand_set const& b, uint32_t nw) {
+    const bool ba = a.bm != nullptr, bb = b.bm != nullptr;
+    if (ba == bb) {
+        uint32_t const* x = ba ? a.bm : a.list;
+        uint32_t const* y = ba ? b.bm : b.list;
+        const uint64_t len = ba ? nw : a.n;
+        for (uint64_t base = 0; base < len; base += 8) {
+            uint32_t u[8], v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const bool in = base + q < len;
+                u[q] = in ? x[base + q] : 0u;
+                v[q] = in ? y[base + q] : 0u;
+            }
+            bool bad = false;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) bad |= u[q] != v[q];
+            if (bad) return false;
+        }
+        return true;
+    }
+    // list against bitmap of the same size: equal iff every element is set
+    const cand_set& l = ba ? b : a;
+    const cand_set& m = ba ? a : b;
+    for (uint64_t base = 0; base < l.n; base += 8) {
+        uint32_t u[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) u[q] = base + q < l.n ? l.list[base + q] : NONE32;
+        bool bad = false;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (u[q] != NONE32) bad |= !((m.bm[u[q] >> 5] >> (u[q] & 31)) & 1u);
+        if (bad) return false;
+    }
     return true;
 }
 
+// Warp-wide equality of two sets of equal size (all 32 lanes call it with the
+// same arguments).
+__device__ __forceinline__ bool warp_sets_equal(cand_set const& a, cand_set const& b, uint32_t nw, int lane) {
+    const bool ba = a.bm != nullptr, bb = b.bm != nullptr;
+    if (ba == bb) {
+        uint32_t const* x = ba ? a.bm : a.list;
+        uint32_t const* y = ba ? b.bm : b.list;
+        const uint64_t len = ba ? nw : a.n;
+        for (uint64_t base = 0; base < len; base += 128) {
+            uint32_t u[4], v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint64_t j = base + 32 * q + lane;
+                u[q] = j < len ? x[j] : 0u;
+                v[q] = j < len ? y[j] : 0u;
+            }
+            bool bad = false;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) bad |= u[q] != v[q];
+            if (__any_sync(0xffffffffu, bad)) return false;
+        }
+        return true;
+    }
+    const cand_set& l = ba ? b : a;
+    const cand_set& m = ba ? a : b;
+    for (uint64_t base = 0; base < l.n; base += 128) {
+        uint32_t u[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint64_t j = base + 32 * q + lane;
+            u[q] = j < l.n ? l.list[j] : NONE32;
+        }
+        bool bad = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (u[q] != NONE32) bad |= !((m.bm[u[q] >> 5] >> (u[q] & 31)) & 1u);
+        if (__any_sync(0xffffffffu, bad)) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ cand_set shfl_set(cand_set const& s, int src) {
+    cand_set r;
+    r.list = (uint32_t const*)__shfl_sync(0xffffffffu, (unsigned long long)s.list, src);
+    r.bm = (uint32_t const*)__shfl_sync(0xffffffffu, (unsigned long long)s.bm, src);
+    r.n = __shfl_sync(0xffffffffu, (unsigned long long)s.n, src);
+    return r;
+}
+
 // Members of an equal-hash run of candidates against the run head, on the
-// raw ascending color lists; rep[c] = head when equal, a differing member
-// marks its run for the exact fallback.
-__global__ void k_member_match_raw(uint64_t n, uint32_t const* __restrict__ head, uint64_t const* __restrict__ hpos,
-                                   uint64_t const* __restrict__ run_start, uint32_t const* __restrict__ nidx,
-                                   cand_view cv, list_src L, uint32_t* __restrict__ rep,
-                                   uint32_t* __restrict__ rep_first, uint32_t* __restrict__ collided) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint64_t run = hpos[i] + head[i] - 1;
-    const uint32_t c = nidx[i];
-    const uint32_t h = nidx[run_start[run]];
-    if (c == h) {
-        rep[c] = c;
-        atomicMin(&rep_first[c], cv.first[c]);
-        return;
+// raw ascending color lists (or bitmaps); rep[c] = head when equal, a
+// differing member marks its run for the exact fallback.  Each lane fetches
+// its own pair of sets; short pairs are compared by the lane, long ones by
+// the warp in turn.  The grid covers n in whole blocks of 256 threads.
+__global__ void __launch_bounds__(256) k_member_match_raw(
+    uint64_t n, uint32_t const* __restrict__ head, uint64_t const* __restrict__ hpos,
+    uint64_t const* __restrict__ run_start, uint32_t const* __restrict__ nidx, cand_view cv, list_src L,
+    uint32_t* __restrict__ rep, uint32_t* __restrict__ rep_first, uint32_t* __restrict__ collided) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int need = 0;  // 0: decided, 1: lane compares, 2: warp compares
+    bool eq = false;
+    uint64_t run = 0;
+    uint32_t c = 0, h = 0;
+    cand_set sc{nullptr, nullptr, 0}, sh{nullptr, nullptr, 0};
+    if (i < n) {
+        run = hpos[i] + head[i] - 1;
+        c = nidx[i];
+        h = nidx[run_start[run]];
+        if (c == h) {
+            rep[c] = c;
+        } else {
+            sc = cand_get(L, cv.kind_id[c]);
+            sh = cand_get(L, cv.kind_id[h]);
+            need = sc.n != sh.n ? 3 : (set_words(sc, sh, L.nw) <= SHORT_SET ? 1 : 2);
+        }
     }
-    if (sets_equal(cand_get(L, cv.kind_id[c]), cand_get(L, cv.kind_id[h]), L.nw)) {
-        rep[c] = h;
-        atomicMin(&rep_first[h], cv.first[c]);
-    } else {
-        rep[c] = c;
-        collided[run] = 1;
+    if (need == 1) eq = lane_sets_equal(sc, sh, L.nw);
+    uint32_t todo = __ballot_sync(0xffffffffu, need == 2);
+    while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const bool e = warp_sets_equal(shfl_set(sc, src), shfl_set(sh, src), L.nw, lane);
+        if (lane == src) eq = e;
     }
+    if (need) {
+        if (eq) {
+            rep[c] = h;
+        } else {
+            rep[c] = c;
+            collided[run] = 1;
+        }
+    }
+    // rep_first[h] = min first appearance over the head and its equal
+    // members.  A run's positions are consecutive, so the warp takes the
+    // minimum per run first and one lane per run issues the atomic: a run of
+    // millions of equal sets would otherwise serialize on one address.
+    uint32_t f = (i < n && (c == h || eq)) ? cv.first[c] : NONE32;
+    const uint64_t key = i < n ? run : ~0ull;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t of = __shfl_down_sync(0xffffffffu, f, o);
+        const uint64_t ok = __shfl_down_sync(0xffffffffu, key, o);
+        if (lane + o < 32 && ok == key) f = min(f, of);
+    }
+    const uint64_t pk = __shfl_up_sync(0xffffffffu, key, 1);
+    if (i < n && (lane == 0 || pk != key) && f != NONE32) atomicMin(&rep_first[h], f);
 }
 
 __global__ void k_group_collided_raw(uint64_t nruns, uint32_t const* __restrict__ collided,
@@ -1125,19 +1265,22 @@ __global__ void k_cand_cid(uint64_t nc, uint32_t const* __restrict__ rep, uint32
     if (c < nc) cid[c] = rcid[rep_index[rep[c]]];
 }
 
-// Per new class: encoded length, hash and color count.
+// Per new class: encoded length, hash and color count (summed per warp,
+// one atomic per warp on the shared counter).
 __global__ void k_new_sizes(uint64_t nnew, uint32_t const* __restrict__ rcand, cand_view cv, list_src L,
                             uint64_t const* __restrict__ cb, uint64_t* __restrict__ nbits,
                             uint64_t* __restrict__ hashes, unsigned long long* __restrict__ ints) {
-    uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nnew) return;
-    const uint32_t c = rcand[j];
-    uint32_t const* p;
-    uint64_t n;
-    cand_list(L, cv.kind_id[c], p, n);
-    nbits[j] = cb[c + 1] - cb[c];
-    hashes[j] = cv.hash[c];
-    atomicAdd(ints, (unsigned long long)n);
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t n = 0;
+    if (j < nnew) {
+        const uint32_t c = rcand[j];
+        uint32_t const* p;
+        cand_list(L, cv.kind_id[c], p, n);
+        nbits[j] = cb[c + 1] - cb[c];
+        hashes[j] = cv.hash[c];
+    }
+    const uint64_t sum = warp_sum64(n);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(ints, (unsigned long long)sum);
 }
 
 // Append new classes' encodings to the dictionary's bit vector (warp per class;
@@ -1828,12 +1971,15 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     auto mark = A.mark();
     // ---- tables
     const uint32_t nb = b1 - b0;
+    const uint64_t q = std::min<uint32_t>(16, std::max<uint32_t>(5, p.table_slots_q));
     std::vector<uint64_t> toff(nb + 1), tcap(nb);
     uint64_t T = 0;
     for (uint32_t b = 0; b < nb; ++b) {
         const uint64_t o = bocc[b0 + b + 1] - bocc[b0 + b];
-        // load factor <= 1/2: short unsuccessful probes for the neighbour lookups
-        const uint64_t cap = o ? std::max<uint64_t>(64, 2 * o + 16) : 0;
+        // slots per occurrence q/4 > 1 (distinct <= occurrences): the default
+        // 2 keeps the load factor <= 1/2 for short unsuccessful probes in the
+        // neighbour lookups
+        const uint64_t cap = o ? std::max<uint64_t>(64, (o * q + 3) / 4 + 16) : 0;
         toff[b] = T;
         tcap[b] = cap;
         T += cap;

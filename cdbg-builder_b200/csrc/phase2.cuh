@@ -80,6 +80,8 @@ struct phase2_params {
     // records with at least this many colors get a precomputed bitmap in
     // multi-record unions (performance only)
     uint32_t heavy_colors = 64;
+    // k-mer table slots per 4 occurrences of a bucket, 5..16 (performance only)
+    uint32_t table_slots_q = 8;
     // Device-resident mode: fragment bytes of each batch are also copied to
     // this pinned host buffer on `copy_st` while later batches run, as long
     // as they fit in `frag_host_cap` (nothing is streamed when null).

@@ -57,6 +57,10 @@ typedef struct cdbg_tuning {
     uint32_t minimizer_tile;   /* (k-1)-mers per minimizer tile: 1024 or 2048 */
     uint32_t heavy_colors;     /* records with >= this many colors get a bitmap
                                   in multi-record unions (default 64) */
+    uint32_t table_slots_q;    /* k-mer table slots per 4 occurrences of a
+                                  bucket, 5..16 (default 8: a load factor of at
+                                  most 1/2 over occurrences; fewer slots move
+                                  fewer table bytes, longer probes) */
 } cdbg_tuning;
 
 int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t);

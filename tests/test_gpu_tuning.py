@@ -1,5 +1,6 @@
 """GPU: the performance knobs (bucket-batch split threshold, minimizer tile,
-heavy-record bitmap threshold) and the autotuner never change outputs."""
+heavy-record bitmap threshold, k-mer table slots per occurrence) and the
+autotuner never change outputs."""
 import numpy as np
 import pytest
 
@@ -32,7 +33,8 @@ def test_knobs_do_not_change_outputs(k):
     try:
         want = _out(e, b, k, B, n)
         for t in (dict(minimizer_tile=1024), dict(heavy_colors=1), dict(heavy_colors=100000),
-                  dict(batch_occ=1 << 12), dict(batch_occ=1, minimizer_tile=1024, heavy_colors=16)):
+                  dict(batch_occ=1 << 12), dict(batch_occ=1, minimizer_tile=1024, heavy_colors=16),
+                  dict(table_slots_q=5), dict(table_slots_q=16), dict(table_slots_q=5, batch_occ=1 << 14)):
             e.set_tuning(**t)
             got = _out(e, b, k, B, n)
             assert got[0] == want[0], t
@@ -50,6 +52,7 @@ def test_autotune_keeps_outputs(engine):
         t, ms = e.autotune(b, 31, B, n)
         assert ms > 0
         assert t["minimizer_tile"] in (1024, 2048)
+        assert 5 <= t["table_slots_q"] <= 16
         assert e.tuning() == t
         got = _out(e, b, 31, B, n)
         assert got[0] == want[0]
