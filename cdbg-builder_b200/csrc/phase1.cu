@@ -388,35 +388,13 @@ __global__ void __launch_bounds__(MZ_THREADS)
     if (MODE == 1) {
         base = tile_off[tile];
     } else {
-        constexpr unsigned long long AGG = 1ull << 62, INC = 2ull << 62, VAL = (1ull << 62) - 1;
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 32) {
             uint64_t excl = 0;
-            bool ok = true;
-            if (tile == 0) {
-                atomicExch(&status[0], INC | tot);
-            } else {
-                atomicExch(&status[tile], AGG | tot);
-                for (uint64_t j = tile - 1;; --j) {
-                    unsigned long long v = 0;
-                    // the predecessor took its index earlier, so it is running or done
-                    for (uint32_t spin = 0; spin < (1u << 26); ++spin) {
-                        v = *(volatile unsigned long long*)&status[j];
-                        if (v >> 62) break;
-                    }
-                    if (!(v >> 62)) {
-                        ok = false;
-                        break;
-                    }
-                    excl += v & VAL;
-                    if ((v >> 62) == 2 || j == 0) break;
-                }
-                atomicExch(&status[tile], INC | ((excl + tot) & VAL));
+            const bool ok = prim::lookback_exclusive(status, tile, tot, excl);
+            if (threadIdx.x == 0) {
+                if (!ok) set_error(err, ERR_CHAIN_LIMIT);
+                s_excl = ok ? excl : ~0ull;
             }
-            if (!ok) {
-                set_error(err, ERR_CHAIN_LIMIT);
-                excl = ~0ull;
-            }
-            s_excl = excl;
         }
         __syncthreads();
         base = s_excl;

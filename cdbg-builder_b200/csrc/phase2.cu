@@ -454,49 +454,108 @@ __device__ __forceinline__ unsigned long long block_reserve(uint32_t want, unsig
     return r;
 }
 
-// (node << 32 | record) for owned occurrences of multi-record k-mers, from the
-// slot each occurrence recorded at insert time.
-__global__ void __launch_bounds__(256)
+// (node, record) of the owned occurrences of multi-record k-mers, from the
+// slot each occurrence recorded at insert time, written in occurrence order
+// (records ascend within a node, so a stable sort by node alone orders the
+// pairs by (node, record)).  A block handles MP_ROUNDS consecutive
+// occurrence blocks of OCC_BLOCK (one per round); blocks take tile indices in
+// launch order and find their output offset by decoupled look-back; the grid
+// is exactly one block per tile.
+constexpr int MP_ROUNDS = 8;
+__global__ void __launch_bounds__(OCC_BLOCK)
     k_multi_pairs(uint64_t const* __restrict__ occ, uint64_t R0, uint64_t nrec, uint64_t O0, uint64_t nocc,
                   uint32_t const* __restrict__ blk_rec,
                   uint32_t const* __restrict__ occ_slot, uint32_t const* __restrict__ node_of_slot,
-                  uint32_t const* __restrict__ n_rec, unsigned long long* __restrict__ cnt,
-                  uint64_t* __restrict__ pairs) {
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    bool emit = false;
-    uint64_t val = 0;
-    if (t < nocc) {
-        const uint32_t v = occ_slot[t];
-        if (v != NONE32 && (v & 0x80000000u)) {
-            const uint32_t n = node_of_slot[v & 0x7fffffffu];
-            if (n_rec[n] == MULTI_TAG) {
-                emit = true;
-                {
-                    // the record lies between this block's first record and the
-                    // next block's (a few dozen records): search only there
-                    const uint64_t nblk = (nocc + OCC_BLOCK - 1) / OCC_BLOCK;
-                    const uint64_t b = t / OCC_BLOCK;
+                  uint32_t const* __restrict__ n_rec, uint32_t* __restrict__ tile_counter,
+                  unsigned long long* __restrict__ status, unsigned long long* __restrict__ cnt,
+                  uint32_t* __restrict__ pnode, uint32_t* __restrict__ prec, uint64_t cap, uint32_t* err) {
+    constexpr int NW = OCC_BLOCK / 32;
+    static_assert(MP_ROUNDS * NW == 64, "warp 0 scans two counts per lane");
+    __shared__ uint64_t s_tile;
+    __shared__ uint32_t wcnt[MP_ROUNDS * NW];
+    __shared__ unsigned long long s_base;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t nblk = (nocc + OCC_BLOCK - 1) / OCC_BLOCK;
+    uint32_t node[MP_ROUNDS], rec[MP_ROUNDS], rank[MP_ROUNDS], emit = 0;
+#pragma unroll
+    for (int rr = 0; rr < MP_ROUNDS; ++rr) {
+        const uint64_t b = tile * MP_ROUNDS + rr;  // occurrence block
+        const uint64_t t = b * OCC_BLOCK + threadIdx.x;
+        bool e = false;
+        node[rr] = 0;
+        rec[rr] = 0;
+        if (t < nocc) {
+            const uint32_t v = occ_slot[t];
+            if (v != NONE32 && (v & 0x80000000u)) {
+                const uint32_t n = node_of_slot[v & 0x7fffffffu];
+                if (n_rec[n] == MULTI_TAG) {
+                    // the record lies between this occurrence block's first record
+                    // and the next one's (a few dozen records): search only there
                     const uint64_t rlo = blk_rec[b];
                     const uint64_t rhi = (b + 1 < nblk) ? blk_rec[b + 1] : R0 + nrec - 1;
-                    const uint64_t r = rlo + upper_bound_u64(occ + rlo, rhi - rlo + 1, O0 + t) - 1;
-                    val = ((uint64_t)n << 32) | (uint32_t)r;
+                    node[rr] = n;
+                    rec[rr] = (uint32_t)(rlo + upper_bound_u64(occ + rlo, rhi - rlo + 1, O0 + t) - 1);
+                    e = true;
                 }
             }
         }
+        const uint32_t bal = __ballot_sync(0xffffffffu, e);
+        rank[rr] = __popc(bal & lanemask_lt());
+        if (e) emit |= 1u << rr;
+        if (lane == 0) wcnt[rr * NW + warp] = __popc(bal);
     }
-    const unsigned long long at = block_reserve<256>(emit ? 1u : 0u, cnt);
-    if (emit) pairs[at] = val;
+    __syncthreads();
+    if (warp == 0) {
+        // exclusive prefix of the (round, warp) counts in position order
+        const uint32_t c0 = wcnt[2 * lane], c1 = wcnt[2 * lane + 1];
+        uint32_t x = c0 + c1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+        const uint32_t ex = x - c0 - c1;
+        wcnt[2 * lane] = ex;
+        wcnt[2 * lane + 1] = ex + c0;
+        uint64_t excl = 0;
+        const bool ok = prim::lookback_exclusive(status, tile, tot, excl);
+        if (lane == 0) {
+            if (!ok) set_error(err, ERR_CHAIN_LIMIT);
+            if (tot) atomicAdd(cnt, (unsigned long long)tot);
+            s_base = excl;
+        }
+    }
+    __syncthreads();
+    const unsigned long long base = s_base;
+#pragma unroll
+    for (int rr = 0; rr < MP_ROUNDS; ++rr) {
+        if (!((emit >> rr) & 1u)) continue;
+        const unsigned long long at = base + wcnt[rr * NW + warp] + rank[rr];
+        if (at < cap) {
+            pnode[at] = node[rr];
+            prec[at] = rec[rr];
+        }
+    }
 }
 
-__global__ void k_unique_heads(uint64_t n, uint64_t const* __restrict__ a, uint32_t* __restrict__ keep) {
+// First of each run of equal (node, record) pairs (a record may own a k-mer
+// at two positions).
+__global__ void k_unique_pairs(uint64_t n, uint32_t const* __restrict__ pn, uint32_t const* __restrict__ pr,
+                               uint32_t* __restrict__ keep) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) keep[i] = (i == 0 || a[i] != a[i - 1]) ? 1u : 0u;
+    if (i < n) keep[i] = (i == 0 || pn[i] != pn[i - 1] || pr[i] != pr[i - 1]) ? 1u : 0u;
 }
 
-__global__ void k_compact_u64(uint64_t n, uint64_t const* __restrict__ a, uint32_t const* __restrict__ keep,
-                              uint64_t const* __restrict__ pos, uint64_t* __restrict__ out) {
+// Kept pairs as (node << 32 | record).
+__global__ void k_compact_pairs(uint64_t n, uint32_t const* __restrict__ pn, uint32_t const* __restrict__ pr,
+                                uint32_t const* __restrict__ keep, uint64_t const* __restrict__ pos,
+                                uint64_t* __restrict__ out) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && keep[i]) out[pos[i]] = a[i];
+    if (i < n && keep[i]) out[pos[i]] = ((uint64_t)pn[i] << 32) | pr[i];
 }
 
 __global__ void k_node_heads(uint64_t n, uint64_t const* __restrict__ a, uint32_t* __restrict__ head) {
@@ -692,12 +751,17 @@ __global__ void k_heavy_bitmaps(uint64_t nrec, uint32_t const* __restrict__ flag
 
 // Warp per multi-record node: OR of its records' color sets (bitmap words for
 // heavy records, per-color bits for the rest) -> mbits, size, set hash.
-__global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ mbeg, uint64_t const* __restrict__ mend,
-                           uint64_t const* __restrict__ upairs,
-                           uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors, uint32_t R0,
-                           uint32_t const* __restrict__ hflag, uint64_t const* __restrict__ hpos,
-                           uint32_t const* __restrict__ rbits, uint32_t nw, uint32_t* __restrict__ mbits,
-                           uint32_t* __restrict__ msize, uint64_t* __restrict__ mhash) {
+// The records' metadata is fetched 32 at a time, one record per lane; heavy
+// records' bitmap words are ORed into registers (lane owns words lane + 32u,
+// u < WPL), two records' lines in flight at a time; the rest set bits in the
+// warp's shared bitmap.
+template <int WPL>
+__global__ void __launch_bounds__(256) k_union_bm(
+    uint64_t M, uint64_t const* __restrict__ mbeg, uint64_t const* __restrict__ mend,
+    uint64_t const* __restrict__ upairs, uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors,
+    uint32_t R0, uint32_t const* __restrict__ hflag, uint64_t const* __restrict__ hpos,
+    uint32_t const* __restrict__ rbits, uint32_t nw, uint32_t* __restrict__ mbits, uint32_t* __restrict__ msize,
+    uint64_t* __restrict__ mhash) {
     extern __shared__ uint32_t smem_bm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     uint32_t* bm = smem_bm + (size_t)wib * nw;
@@ -705,32 +769,66 @@ __global__ void k_union_bm(uint64_t M, uint64_t const* __restrict__ mbeg, uint64
     if (m >= M) return;
     for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
     __syncwarp();
-    for (uint64_t p = mbeg[m]; p < mend[m]; ++p) {
-        const uint32_t r = (uint32_t)(upairs[p] & 0xffffffffu);
-        if (hflag[r - R0]) {
-            uint32_t const* rb = rbits + hpos[r - R0] * (uint64_t)nw;
-            for (uint32_t w = lane; w < nw; w += 32) bm[w] |= rb[w];  // lanes own distinct words
-        } else {
-            __syncwarp();
-            warp_or_list(bm, colors, col_off[r], col_off[r + 1], nw, lane);
-            __syncwarp();
+    uint32_t acc[WPL];
+#pragma unroll
+    for (int u = 0; u < WPL; ++u) acc[u] = 0;
+    const uint64_t pend = mend[m];
+    for (uint64_t p0 = mbeg[m]; p0 < pend; p0 += 32) {
+        const uint64_t p = p0 + lane;
+        bool heavy = false, light = false;
+        uint64_t src = 0, c0 = 0, c1 = 0;
+        if (p < pend) {
+            const uint32_t r = (uint32_t)(upairs[p] & 0xffffffffu);
+            heavy = hflag[r - R0] != 0;
+            light = !heavy;
+            if (heavy) {
+                src = hpos[r - R0] * (uint64_t)nw;
+            } else {
+                c0 = col_off[r];
+                c1 = col_off[r + 1];
+            }
+        }
+        uint32_t hm = __ballot_sync(0xffffffffu, heavy);
+        while (hm) {
+            const int q0 = __ffs(hm) - 1;
+            hm &= hm - 1;
+            const bool two = hm != 0;
+            const int q1 = two ? __ffs(hm) - 1 : q0;
+            if (two) hm &= hm - 1;
+            const uint64_t s0 = __shfl_sync(0xffffffffu, src, q0);
+            const uint64_t s1 = __shfl_sync(0xffffffffu, src, q1);
+#pragma unroll
+            for (int u = 0; u < WPL; ++u) {
+                const uint32_t w = lane + 32 * u;
+                if (w < nw) acc[u] |= rbits[s0 + w] | rbits[s1 + w];
+            }
+        }
+        uint32_t lm = __ballot_sync(0xffffffffu, light);
+        while (lm) {
+            const int q = __ffs(lm) - 1;
+            lm &= lm - 1;
+            warp_or_list(bm, colors, __shfl_sync(0xffffffffu, c0, q), __shfl_sync(0xffffffffu, c1, q), nw, lane);
         }
     }
     __syncwarp();
     uint32_t cnt = 0;
-    uint64_t acc = 0;
+    uint64_t hs = 0;
     uint32_t* out = mbits + m * (uint64_t)nw;
-    for (uint32_t w = lane; w < nw; w += 32) {
-        const uint32_t x = bm[w];
-        out[w] = x;
-        cnt += __popc(x);
-        if (x) acc += word_mix(w, x);
+#pragma unroll
+    for (int u = 0; u < WPL; ++u) {
+        const uint32_t w = lane + 32 * u;
+        if (w < nw) {
+            const uint32_t x = bm[w] | acc[u];
+            out[w] = x;
+            cnt += __popc(x);
+            if (x) hs += word_mix(w, x);
+        }
     }
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    acc = warp_sum64(acc);
+    hs = warp_sum64(hs);
     if (lane == 0) {
         msize[m] = cnt;
-        mhash[m] = set_hash_final(acc, cnt);
+        mhash[m] = set_hash_final(hs, cnt);
     }
 }
 
@@ -2050,12 +2148,19 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     // ---- multi-record k-mers: (node, record) pairs in one pass, at most one
     // per occurrence
     unsigned long long* cnt = A.alloc<unsigned long long>(1);
-    uint64_t* pairs = A.alloc<uint64_t>(nocc);
+    uint32_t* tile_counter = A.alloc<uint32_t>(1);
+    const uint64_t mp_tiles = ceil_div(nblk, (uint64_t)MP_ROUNDS);
+    unsigned long long* status = A.alloc<unsigned long long>(mp_tiles);
+    uint32_t* pnode = A.alloc<uint32_t>(nocc);
+    uint32_t* prec = A.alloc<uint32_t>(nocc);
     CDBG_CUDA(cudaMemsetAsync(cnt, 0, 8, st));
+    CDBG_CUDA(cudaMemsetAsync(tile_counter, 0, 4, st));
+    CDBG_CUDA(cudaMemsetAsync(status, 0, 8 * mp_tiles, st));
     {
         CDBG_PROF("k_multi_pairs", st);
-        k_multi_pairs<<<grid(nocc, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nocc, blk_rec, occ_slot, node_of_slot,
-                                                             n_rec, cnt, pairs);
+        k_multi_pairs<<<(unsigned)mp_tiles, OCC_BLOCK, 0, st>>>(R.occ, R0, nrec, O0, nocc, blk_rec, occ_slot,
+                                                            node_of_slot, n_rec, tile_counter, status, cnt, pnode,
+                                                            prec, nocc, d_err);
     }
     CDBG_CHECK_LAUNCH();
     const uint64_t npairs = read_dev(cnt, st);
@@ -2074,16 +2179,17 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint64_t* gend = nullptr;
     uint32_t* mgrp = nullptr;    // group of each multi node
     if (npairs) {
-        uint32_t* dummy = A.alloc<uint32_t>(npairs);
-        prim::radix_sort_pairs<uint32_t>(pairs, dummy, npairs, 0, 64, A, st);
+        // stable by node (records already ascend within a node): the node bits only
+        const int node_bits = D > 1 ? 64 - __builtin_clzll(D - 1) : 1;
+        prim::radix_sort_pairs<uint32_t, uint32_t>(pnode, prec, npairs, 0, node_bits, A, st);
         uint32_t* keep = A.alloc<uint32_t>(npairs);
         uint64_t* kpos = A.alloc<uint64_t>(npairs + 1);
-        k_unique_heads<<<grid(npairs, 256), 256, 0, st>>>(npairs, pairs, keep);
+        k_unique_pairs<<<grid(npairs, 256), 256, 0, st>>>(npairs, pnode, prec, keep);
         CDBG_CHECK_LAUNCH();
         prim::exclusive_scan<uint32_t, uint64_t>(keep, kpos, npairs, A, st, kpos + npairs);
         const uint64_t nu = read_dev(kpos + npairs, st);
         upairs = A.alloc<uint64_t>(nu);
-        k_compact_u64<<<grid(npairs, 256), 256, 0, st>>>(npairs, pairs, keep, kpos, upairs);
+        k_compact_pairs<<<grid(npairs, 256), 256, 0, st>>>(npairs, pnode, prec, keep, kpos, upairs);
         CDBG_CHECK_LAUNCH();
         uint32_t* head = A.alloc<uint32_t>(nu);
         uint64_t* hpos = A.alloc<uint64_t>(nu + 1);
@@ -2128,10 +2234,8 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             prim::exclusive_scan<uint32_t, uint64_t>(hflag, hpos, nrec, A, st, hpos + nrec);
             const uint64_t nheavy = read_dev(hpos + nrec, st);
             uint32_t* rbits = A.alloc<uint32_t>(nheavy * nw + 1);
-            if (shm > 48 * 1024) {
+            if (shm > 48 * 1024)
                 CDBG_CUDA(cudaFuncSetAttribute(k_heavy_bitmaps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-                CDBG_CUDA(cudaFuncSetAttribute(k_union_bm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-            }
             if (nheavy) {
                 CDBG_PROF("k_heavy_bitmaps", st);
                 k_heavy_bitmaps<<<grid(nrec, wpb), wpb * 32, shm, st>>>(nrec, hflag, hpos, (uint32_t)R0, R.col_off,
@@ -2141,9 +2245,22 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             mbits = A.alloc<uint32_t>(G * nw + 1);
             {
                 CDBG_PROF("k_union", st);
-                k_union_bm<<<grid(G, wpb), wpb * 32, shm, st>>>(G, gbeg, gend, upairs, R.col_off, R.colors,
-                                                                 (uint32_t)R0, hflag, hpos, rbits, nw, mbits, msize,
-                                                                 mhash);
+                auto launch = [&](auto kern) {
+                    if (shm > 48 * 1024)
+                        CDBG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+                    kern<<<grid(G, wpb), wpb * 32, shm, st>>>(G, gbeg, gend, upairs, R.col_off, R.colors, (uint32_t)R0,
+                                                              hflag, hpos, rbits, nw, mbits, msize, mhash);
+                };
+                if (nw <= 32)
+                    launch(k_union_bm<1>);
+                else if (nw <= 64)
+                    launch(k_union_bm<2>);
+                else if (nw <= 128)
+                    launch(k_union_bm<4>);
+                else if (nw <= 256)
+                    launch(k_union_bm<8>);
+                else
+                    throw std::runtime_error("bitmap unions need at most 8192 colors");
             }
             CDBG_CHECK_LAUNCH();
         } else {

@@ -1,5 +1,5 @@
 // Device-wide primitives written for this project: exclusive scan and a
-// stable LSD radix sort of (u64 key, value) pairs.
+// stable LSD radix sort of (key, value) pairs, u32 or u64 keys.
 //
 // Radix sort: one fused histogram pass computes the digit histograms of every
 // requested pass in a single read of the keys; passes whose digit is constant
@@ -154,6 +154,56 @@ void exclusive_scan(T const* in, U* out, uint64_t n, dev_arena& A, cudaStream_t 
     A.release(m);
 }
 
+// ------------------------------------------------------------ ordered output
+// Decoupled look-back for tiles that take their indices in launch order from
+// an atomic counter.  One warp of the tile calls it (all 32 lanes, the same
+// arguments): lane 0 publishes the tile's count `tot` in status[tile]; the
+// warp reads its predecessors' status 32 at a time (lane l the l-th nearest),
+// adds their counts back to the nearest published inclusive prefix, lane 0
+// publishes the tile's own inclusive prefix, and every lane gets the
+// exclusive one in `excl`.  status[] is zeroed before the launch.  A
+// predecessor took its index earlier, so it is running or done; every wait is
+// still bounded, and on a timeout the tile publishes what it has (so its
+// successors never wait on it) and returns false.
+constexpr unsigned long long LB_AGG = 1ull << 62, LB_INC = 2ull << 62, LB_VAL = (1ull << 62) - 1;
+__device__ __forceinline__ bool lookback_exclusive(unsigned long long* status, uint64_t tile, uint64_t tot,
+                                                   uint64_t& excl) {
+    const int lane = threadIdx.x & 31;
+    excl = 0;
+    if (tile == 0) {
+        if (lane == 0) atomicExch(&status[0], LB_INC | tot);
+        return true;
+    }
+    if (lane == 0) atomicExch(&status[tile], LB_AGG | tot);
+    bool ok = true;
+    uint64_t sum = 0;
+    for (uint64_t end = tile;;) {  // window: tiles end - 1 - lane
+        unsigned long long v = LB_INC;  // before tile 0: an inclusive prefix of 0
+        if (end >= (uint64_t)lane + 1) {
+            const uint64_t j = end - 1 - lane;
+            for (uint32_t spin = 0; spin < (1u << 24); ++spin) {
+                v = *(volatile unsigned long long*)&status[j];
+                if (v >> 62) break;
+            }
+        }
+        if (!__all_sync(0xffffffffu, (v >> 62) != 0)) {
+            ok = false;
+            break;
+        }
+        const uint32_t inc = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+        const int stop = inc ? __ffs(inc) - 1 : 31;  // nearest inclusive lane
+        uint64_t x = lane <= stop ? (v & LB_VAL) : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        sum += x;
+        if (inc) break;
+        end -= 32;
+    }
+    if (lane == 0) atomicExch(&status[tile], LB_INC | ((sum + tot) & LB_VAL));
+    excl = sum;
+    return ok;
+}
+
 // ------------------------------------------------------------------ radix sort
 constexpr int RS_THREADS = 256;
 constexpr int RS_ITEMS = 8;
@@ -164,7 +214,8 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 
 // Histograms of all passes [begin_bit, end_bit) in one read.  hist is
 // npasses x 256 u64, zeroed by the caller.
-__global__ void __launch_bounds__(RS_THREADS) k_rs_histograms(uint64_t const* __restrict__ keys,
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_histograms(K const* __restrict__ keys,
                                                               uint64_t n, int begin_bit,
                                                               int npasses,
                                                               unsigned long long* hist) {
@@ -173,7 +224,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_histograms(uint64_t const* __
     __syncthreads();
     const uint64_t stride = (uint64_t)gridDim.x * RS_THREADS;
     for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += stride) {
-        const uint64_t k = keys[i];
+        const K k = keys[i];
         for (int p = 0; p < npasses; ++p)
             atomicAdd(&h[p][(k >> (begin_bit + p * RS_BITS)) & (RS_BINS - 1)], 1u);
     }
@@ -185,7 +236,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_histograms(uint64_t const* __
 }
 
 // counts[d * ntiles + tile] = number of keys of tile with digit d.
-__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(uint64_t const* __restrict__ keys,
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(K const* __restrict__ keys,
                                                            uint64_t n, int shift, uint32_t ntiles,
                                                            uint32_t* __restrict__ counts) {
     __shared__ uint32_t h[RS_BINS];
@@ -201,14 +253,14 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(uint64_t const* __res
     counts[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
-template <typename V>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(uint64_t const* __restrict__ keys_in,
+template <typename K, typename V>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(K const* __restrict__ keys_in,
                                                              V const* __restrict__ vals_in,
-                                                             uint64_t* __restrict__ keys_out,
+                                                             K* __restrict__ keys_out,
                                                              V* __restrict__ vals_out, uint64_t n,
                                                              int shift, uint32_t ntiles,
                                                              uint64_t const* __restrict__ offs) {
-    __shared__ uint64_t sk[RS_TILE];
+    __shared__ K sk[RS_TILE];
     __shared__ V sv[RS_TILE];
     __shared__ uint32_t wcnt[RS_WARPS][RS_BINS];  // per-warp digit counts, then prefixes
     __shared__ uint32_t dstart[RS_BINS];          // tile-local start of each digit
@@ -222,14 +274,14 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(uint64_t const* __r
     const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
     const uint32_t tile_n = (uint32_t)((n - base) < (uint64_t)RS_TILE ? (n - base) : RS_TILE);
     // Warp w owns tile positions [w*256, (w+1)*256): rounds of 32 in order.
-    uint64_t k[RS_ITEMS];
+    K k[RS_ITEMS];
     V v[RS_ITEMS];
     uint32_t rk[RS_ITEMS];
 #pragma unroll
     for (int r = 0; r < RS_ITEMS; ++r) {
         const uint32_t pos = (uint32_t)warp * (RS_ITEMS * 32) + (uint32_t)r * 32 + lane;
         const bool ok = pos < tile_n;
-        k[r] = ok ? keys_in[base + pos] : ~0ull;
+        k[r] = ok ? keys_in[base + pos] : ~K(0);
         v[r] = ok ? vals_in[base + pos] : V(0);
         const uint32_t d = ok ? (uint32_t)((k[r] >> shift) & (RS_BINS - 1)) : RS_BINS;  // sentinel
         const uint32_t active = __ballot_sync(0xffffffffu, ok);
@@ -272,7 +324,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(uint64_t const* __r
     }
     __syncthreads();
     for (uint32_t p = threadIdx.x; p < tile_n; p += RS_THREADS) {
-        const uint64_t key = sk[p];
+        const K key = sk[p];
         const uint32_t d = (uint32_t)((key >> shift) & (RS_BINS - 1));
         const uint64_t dst = gbase[d] + (p - dstart[d]);
         keys_out[dst] = key;
@@ -283,9 +335,11 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(uint64_t const* __r
 // Stable sort of (keys, vals) by key bits [begin_bit, end_bit).  Results end
 // in (keys, vals); the arena provides the ping-pong buffers.  Needs a host
 // synchronize (to read the digit histograms); returns the number of passes run.
-template <typename V>
-int radix_sort_pairs(uint64_t* keys, V* vals, uint64_t n, int begin_bit, int end_bit,
+template <typename V, typename K = uint64_t>
+int radix_sort_pairs(K* keys, V* vals, uint64_t n, int begin_bit, int end_bit,
                      dev_arena& A, cudaStream_t st) {
+    static_assert(sizeof(K) == 4 || sizeof(K) == 8, "u32 or u64 keys");
+    if (end_bit > 8 * (int)sizeof(K)) end_bit = 8 * (int)sizeof(K);
     if (n <= 1 || end_bit <= begin_bit) return 0;
     const int npasses = (end_bit - begin_bit + RS_BITS - 1) / RS_BITS;
     auto m = A.mark();
@@ -305,11 +359,11 @@ int radix_sort_pairs(uint64_t* keys, V* vals, uint64_t n, int begin_bit, int end
     CDBG_CUDA(cudaStreamSynchronize(st));
 
     const uint64_t ntiles = ceil_div(n, RS_TILE);
-    uint64_t* k2 = A.alloc<uint64_t>(n);
+    K* k2 = A.alloc<K>(n);
     V* v2 = A.alloc<V>(n);
     uint32_t* counts = A.alloc<uint32_t>(ntiles * RS_BINS);
     uint64_t* offs = A.alloc<uint64_t>(ntiles * RS_BINS);
-    uint64_t *kin = keys, *kout = k2;
+    K *kin = keys, *kout = k2;
     V *vin = vals, *vout = v2;
     int ran = 0;
     for (int p = 0; p < npasses; ++p) {
@@ -326,8 +380,8 @@ int radix_sort_pairs(uint64_t* keys, V* vals, uint64_t n, int begin_bit, int end
         exclusive_scan<uint32_t, uint64_t>(counts, offs, ntiles * RS_BINS, A, st);
         {
             // one read and one write of every (key, value) pair
-            CDBG_PROF_BYTES("k_rs_downsweep", st, 2.0 * n * (sizeof(uint64_t) + sizeof(V)));
-            k_rs_downsweep<V><<<(unsigned)ntiles, RS_THREADS, 0, st>>>(kin, vin, kout, vout, n, shift,
+            CDBG_PROF_BYTES("k_rs_downsweep", st, 2.0 * n * (sizeof(K) + sizeof(V)));
+            k_rs_downsweep<K, V><<<(unsigned)ntiles, RS_THREADS, 0, st>>>(kin, vin, kout, vout, n, shift,
                                                                        (uint32_t)ntiles, offs);
         }
         CDBG_CHECK_LAUNCH();
@@ -336,7 +390,7 @@ int radix_sort_pairs(uint64_t* keys, V* vals, uint64_t n, int begin_bit, int end
         ++ran;
     }
     if (kin != keys) {
-        CDBG_CUDA(cudaMemcpyAsync(keys, kin, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+        CDBG_CUDA(cudaMemcpyAsync(keys, kin, n * sizeof(K), cudaMemcpyDeviceToDevice, st));
         CDBG_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(V), cudaMemcpyDeviceToDevice, st));
     }
     A.release(m);
