@@ -128,11 +128,6 @@ __device__ __forceinline__ u128 key_cas(u128* a, u128 cmp, u128 val) {
         : "memory");
     return ((u128)ohi << 64) | (u128)olo;
 }
-__device__ __forceinline__ uint64_t key_load(uint64_t const* a) { return *(volatile uint64_t const*)a; }
-__device__ __forceinline__ u128 key_load(u128 const* a) {
-    const ulonglong2 v = *reinterpret_cast<ulonglong2 const*>(a);
-    return ((u128)v.y << 64) | (u128)v.x;
-}
 
 // One table slot: everything the load stage aggregates for a k-mer in 16
 // bytes (32 for 128-bit k-mers), two slots per 32-byte sector.
@@ -160,37 +155,43 @@ static_assert(sizeof(slot_t<uint64_t>) == 16, "slot layout");
 static_assert(sizeof(slot_t<u128>) == 32, "slot layout");
 constexpr uint64_t MAX_BATCH_RECORDS = (1ull << 28) - 2;  // owner field of `om`
 
-// Insert-or-find; returns the slot (absolute) or NONE64 when the region is full.
-template <typename K>
-__device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off, uint64_t cap, K x) {
-    const K EMPTY = kmer_ops<K>::empty();
-    uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
-    for (uint64_t i = 0; i < cap; ++i) {
-        K* a = &slots[off + s].key;
-        if (sizeof(K) == 8) {
-            const K cur = key_load(a);
-            if (cur == x) return off + s;
-            if (cur == EMPTY) {
-                const K old = key_cas(a, EMPTY, x);
-                if (old == EMPTY || old == x) return off + s;
-            }
-        } else {
-            const K old = key_cas(a, EMPTY, x);  // atomic 128-bit read-or-claim
-            if (old == EMPTY || old == x) return off + s;
-        }
-        if (++s == cap) s = 0;
-    }
-    return ~0ull;
+// A 64-bit-key slot's key and (rank | om << 32) in one 16-byte load that
+// bypasses L1.
+__device__ __forceinline__ void slot_load(slot_t<uint64_t> const* e, uint64_t& key, uint64_t& ro) {
+    asm volatile("ld.volatile.global.v2.u64 {%0, %1}, [%2];" : "=l"(key), "=l"(ro) : "l"(e) : "memory");
 }
 
+// Insert-or-find; returns the slot (absolute) or NONE64 when the region is
+// full.  `ro` receives the slot's (rank | om << 32) as read while probing: a
+// value the slot held, so possibly older than the current one (rank only
+// falls and om only gains bits, which the caller's updates rely on).
 template <typename K>
-__device__ __forceinline__ uint64_t table_find(slot_t<K> const* slots, uint64_t off, uint64_t cap, K x) {
+__device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off, uint64_t cap, K x, uint64_t& ro) {
     const K EMPTY = kmer_ops<K>::empty();
     uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
     for (uint64_t i = 0; i < cap; ++i) {
-        const K cur = key_load(&slots[off + s].key);
-        if (cur == x) return off + s;
-        if (cur == EMPTY) return ~0ull;
+        slot_t<K>* e = &slots[off + s];
+        if constexpr (sizeof(K) == 8) {
+            uint64_t cur, v;
+            slot_load(e, cur, v);
+            if (cur == x) {
+                ro = v;
+                return off + s;
+            }
+            if (cur == EMPTY) {
+                const K old = key_cas(&e->key, EMPTY, x);
+                if (old == EMPTY || old == x) {
+                    ro = v;
+                    return off + s;
+                }
+            }
+        } else {
+            const K old = key_cas(&e->key, EMPTY, x);  // atomic 128-bit read-or-claim
+            if (old == EMPTY || old == x) {
+                ro = *(volatile uint64_t const*)&e->rank;
+                return off + s;
+            }
+        }
         if (++s == cap) s = 0;
     }
     return ~0ull;
@@ -338,7 +339,8 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     const uint64_t rec = window_record(win, R.occ, R0, nrec, O0 + t);
     const occ_info<K> oi = decode_occ_r<K>(R, rec, O0 + t, k);
     const uint32_t tb = R.bucket[oi.r] - T.b0;
-    const uint64_t s = table_upsert<K>(T.slots, T.tab_off[tb], T.tab_cap[tb], oi.can);
+    uint64_t ro = 0;
+    const uint64_t s = table_upsert<K>(T.slots, T.tab_off[tb], T.tab_cap[tb], oi.can, ro);
     if (s == ~0ull) {
         set_error(err, ERR_TABLE_FULL);
         occ_slot[t] = NONE32;
@@ -347,16 +349,19 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     // slot of this occurrence, bit 31 = owned (read by k_multi_pairs)
     occ_slot[t] = (uint32_t)s | (oi.owned ? 0x80000000u : 0u);
     const uint32_t mo = oi.contrib | (oi.owned ? M_PRIMARY : 0u);
+    // rank and om as read while probing (never newer than the slot): the
+    // reduction and the updates below stay correct, and a k-mer whose slot
+    // already holds everything this occurrence adds costs no further access
     slot_t<K>& e = T.slots[s];
-    if ((uint32_t)t < e.rank) atomicMin(&e.rank, (uint32_t)t);
+    if ((uint32_t)t < (uint32_t)ro) atomicMin(&e.rank, (uint32_t)t);
+    uint32_t old = (uint32_t)(ro >> 32);
     if (!oi.owned) {
-        if (mo && (e.om & mo) != mo) atomicOr(&e.om, mo);
+        if (mo && (old & mo) != mo) atomicOr(&e.om, mo);
         return;
     }
     // owner: the first owning record, M_MULTI once a second one appears.
     // `om` only gains bits, so the loop ends after a few changes by others.
     const uint32_t own = (uint32_t)(oi.r - R0 + 1) << 4;
-    uint32_t old = *(volatile uint32_t*)&e.om;
     for (int it = 0;; ++it) {
         const uint32_t cur = old & ~0xfu;
         const uint32_t want = (cur == own || (old & M_MULTI)) ? (old | mo)
@@ -1408,10 +1413,30 @@ __global__ void k_node_cid(uint64_t D, uint32_t const* __restrict__ n_rec, uint3
 }
 
 // ---- extension masks and clean links -------------------------------------
+// Node index of k-mer x, NONE32 when absent.  The tables are read-only once
+// the nodes are numbered, so the probes go through the read-only path, and a
+// 64-bit-key slot's probe load brings its rank (the node index) along.
 template <typename K>
 __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb, K x) {
-    const uint64_t s = table_find<K>(T.slots, T.tab_off[tb], T.tab_cap[tb], x);
-    return s == ~0ull ? NONE32 : T.slots[s].rank;  // node index
+    const K EMPTY = kmer_ops<K>::empty();
+    const uint64_t off = T.tab_off[tb], cap = T.tab_cap[tb];
+    uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
+    for (uint64_t i = 0; i < cap; ++i) {
+        slot_t<K> const* e = &T.slots[off + s];
+        if constexpr (sizeof(K) == 8) {
+            const ulonglong2 v = __ldg(reinterpret_cast<ulonglong2 const*>(e));
+            if (v.x == x) return (uint32_t)v.y;
+            if (v.x == EMPTY) return NONE32;
+        } else {
+            const ulonglong2 kv = __ldg(reinterpret_cast<ulonglong2 const*>(e));
+            const uint32_t rank = __ldg(&e->rank);
+            const K cur = ((u128)kv.y << 64) | (u128)kv.x;
+            if (cur == x) return rank;
+            if (cur == EMPTY) return NONE32;
+        }
+        if (++s == cap) s = 0;
+    }
+    return NONE32;
 }
 
 template <typename K>
