@@ -40,6 +40,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdlib>
 #include <vector>
 
@@ -392,38 +393,34 @@ __global__ void k_popc(uint64_t n, uint32_t const* __restrict__ bits, uint32_t* 
     if (i < n) cnt[i] = __popc(bits[i]);
 }
 
-// Number the distinct k-mers in first-insertion order; the slot's rank field
-// becomes the node index, and slot_of_node maps back.
+// Number the distinct k-mers in first-insertion order, scanning the
+// occurrences: occurrence t is the first of its k-mer iff bit t of `bits` is
+// set, and its node index is the number of first occurrences before it.  The
+// slot's rank field becomes the node index, and the node arrays are written
+// in node order.  The bucket is the slot's table (tab_off ascends over the batch's
+// buckets).  Reads are sequential except one slot per node.
 template <typename K>
-__global__ void k_make_nodes(uint64_t T, slot_t<K>* __restrict__ slots, uint32_t const* __restrict__ bits,
-                             uint64_t const* __restrict__ wpre, uint32_t* __restrict__ node_of_slot,
-                             uint32_t* __restrict__ slot_of_node) {
-    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= T) return;
-    if (slots[s].key == kmer_ops<K>::empty()) return;
-    const uint32_t q = slots[s].rank;
-    const uint32_t w = bits[q >> 5];
-    const uint64_t n = wpre[q >> 5] + __popc(w & ((1u << (q & 31)) - 1u));
-    slots[s].rank = (uint32_t)n;
-    node_of_slot[s] = (uint32_t)n;  // compact copy for the per-occurrence pass
-    slot_of_node[n] = (uint32_t)s;
-}
-
-// Node arrays in node order (sequential writes; one slot read per node).  The
-// bucket is the slot's table (tab_off is ascending over the batch's buckets).
-template <typename K>
-__global__ void k_node_fields(uint64_t D, uint32_t const* __restrict__ slot_of_node,
-                              slot_t<K> const* __restrict__ slots, tables<K> TB, uint32_t nb, uint64_t R0,
-                              K* __restrict__ n_key, uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
-                              uint32_t* __restrict__ n_bucket) {
-    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= D) return;
-    const uint32_t s = slot_of_node[n];
-    const slot_t<K> e = slots[s];
-    n_key[n] = e.key;
-    n_meta[n] = (uint8_t)(e.om & 7u);
+__global__ void __launch_bounds__(256) k_make_nodes(uint64_t nocc, uint32_t const* __restrict__ occ_slot,
+                                                    uint32_t const* __restrict__ bits,
+                                                    uint64_t const* __restrict__ wpre, slot_t<K>* __restrict__ slots,
+                                                    tables<K> TB, uint32_t nb, uint64_t R0,
+                                                    K* __restrict__ n_key,
+                                                    uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
+                                                    uint32_t* __restrict__ n_bucket) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nocc) return;
+    const uint32_t w = bits[t >> 5];
+    if (!((w >> (t & 31)) & 1u)) return;
+    const uint64_t n = wpre[t >> 5] + __popc(w & ((1u << (t & 31)) - 1u));
+    const uint32_t s = occ_slot[t] & 0x7fffffffu;
+    slot_t<K>& e = slots[s];
+    const K key = e.key;
+    const uint32_t om = e.om;
+    e.rank = (uint32_t)n;
+    n_key[n] = key;
+    n_meta[n] = (uint8_t)(om & 7u);
     uint32_t rec = NONE32;
-    if (e.om & M_PRIMARY) rec = (e.om & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (e.om >> 4) - 1);
+    if (om & M_PRIMARY) rec = (om & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (om >> 4) - 1);
     n_rec[n] = rec;
     n_bucket[n] = TB.b0 + upper_bound_u64(TB.tab_off, nb + 1, s) - 1;
 }
@@ -470,7 +467,7 @@ constexpr int MP_ROUNDS = 8;
 __global__ void __launch_bounds__(OCC_BLOCK)
     k_multi_pairs(uint64_t const* __restrict__ occ, uint64_t R0, uint64_t nrec, uint64_t O0, uint64_t nocc,
                   uint32_t const* __restrict__ blk_rec,
-                  uint32_t const* __restrict__ occ_slot, uint32_t const* __restrict__ node_of_slot,
+                  uint32_t const* __restrict__ occ_slot, uint32_t const* __restrict__ slot_rank, uint32_t rank_stride,
                   uint32_t const* __restrict__ n_rec, uint32_t* __restrict__ tile_counter,
                   unsigned long long* __restrict__ status, unsigned long long* __restrict__ cnt,
                   uint32_t* __restrict__ pnode, uint32_t* __restrict__ prec, uint64_t cap, uint32_t* err) {
@@ -495,7 +492,7 @@ __global__ void __launch_bounds__(OCC_BLOCK)
         if (t < nocc) {
             const uint32_t v = occ_slot[t];
             if (v != NONE32 && (v & 0x80000000u)) {
-                const uint32_t n = node_of_slot[v & 0x7fffffffu];
+                const uint32_t n = __ldg(slot_rank + (uint64_t)(v & 0x7fffffffu) * rank_stride);
                 if (n_rec[n] == MULTI_TAG) {
                     // the record lies between this occurrence block's first record
                     // and the next one's (a few dozen records): search only there
@@ -2157,17 +2154,10 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     uint8_t* n_meta = A.alloc<uint8_t>(D);
     uint32_t* n_rec = A.alloc<uint32_t>(D);
     uint32_t* n_bucket = A.alloc<uint32_t>(D);
-    uint32_t* node_of_slot = A.alloc<uint32_t>(T);
-    uint32_t* slot_of_node = A.alloc<uint32_t>(D);
     {
         CDBG_PROF("k_make_nodes", st);
-        k_make_nodes<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, bits, wpre, node_of_slot, slot_of_node);
-    }
-    CDBG_CHECK_LAUNCH();
-    {
-        CDBG_PROF("k_node_fields", st);
-        k_node_fields<K><<<grid(D, 256), 256, 0, st>>>(D, slot_of_node, TB.slots, TB, nb, R0, n_key, n_meta, n_rec,
-                                                        n_bucket);
+        k_make_nodes<K><<<grid(nocc, 256), 256, 0, st>>>(nocc, occ_slot, bits, wpre, TB.slots, TB, nb, R0,
+                                                         n_key, n_meta, n_rec, n_bucket);
     }
     CDBG_CHECK_LAUNCH();
     // ---- multi-record k-mers: (node, record) pairs in one pass, at most one
@@ -2184,7 +2174,11 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     {
         CDBG_PROF("k_multi_pairs", st);
         k_multi_pairs<<<(unsigned)mp_tiles, OCC_BLOCK, 0, st>>>(R.occ, R0, nrec, O0, nocc, blk_rec, occ_slot,
-                                                            node_of_slot, n_rec, tile_counter, status, cnt, pnode,
+                                                            reinterpret_cast<uint32_t const*>(
+                                                                reinterpret_cast<char const*>(TB.slots) +
+                                                                offsetof(slot_t<K>, rank)),
+                                                            (uint32_t)(sizeof(slot_t<K>) / 4), n_rec,
+                                                            tile_counter, status, cnt, pnode,
                                                             prec, nocc, d_err);
     }
     CDBG_CHECK_LAUNCH();
