@@ -368,15 +368,30 @@ __global__ void __launch_bounds__(MZ_THREADS)
         if (lane == 0) wcnt[rr * NW + warp] = __popc(bal);
     }
     __syncthreads();
-    // exclusive prefix over (round, warp) in position order
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int i = 0; i < MZ_PER * NW; ++i) {
-            const uint32_t v = wcnt[i];
-            wcnt[i] = run;
-            run += v;
+    // exclusive prefix over (round, warp) in position order, by warp 0
+    if (warp == 0) {
+        constexpr int E = MZ_PER * NW, PL = (E + 31) / 32;
+        uint32_t c[PL], s = 0;
+#pragma unroll
+        for (int j = 0; j < PL; ++j) {
+            const int i = lane * PL + j;
+            c[j] = i < E ? wcnt[i] : 0u;
+            s += c[j];
         }
-        wcnt[MZ_PER * NW] = run;
+        uint32_t x = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        uint32_t ex = x - s;
+#pragma unroll
+        for (int j = 0; j < PL; ++j) {
+            const int i = lane * PL + j;
+            if (i < E) wcnt[i] = ex;
+            ex += c[j];
+        }
+        if (lane == 31) wcnt[E] = x;
     }
     __syncthreads();
     const uint32_t tot = wcnt[MZ_PER * NW];

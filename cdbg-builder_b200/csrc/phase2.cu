@@ -755,7 +755,7 @@ __global__ void k_heavy_bitmaps(uint64_t nrec, uint32_t const* __restrict__ flag
 // heavy records, per-color bits for the rest) -> mbits, size, set hash.
 // The records' metadata is fetched 32 at a time, one record per lane; heavy
 // records' bitmap words are ORed into registers (lane owns words lane + 32u,
-// u < WPL), two records' lines in flight at a time; the rest set bits in the
+// u < WPL), four records' lines in flight at a time; the rest set bits in the
 // warp's shared bitmap.
 template <int WPL>
 __global__ void __launch_bounds__(256) k_union_bm(
@@ -792,17 +792,20 @@ __global__ void __launch_bounds__(256) k_union_bm(
         }
         uint32_t hm = __ballot_sync(0xffffffffu, heavy);
         while (hm) {
-            const int q0 = __ffs(hm) - 1;
-            hm &= hm - 1;
-            const bool two = hm != 0;
-            const int q1 = two ? __ffs(hm) - 1 : q0;
-            if (two) hm &= hm - 1;
-            const uint64_t s0 = __shfl_sync(0xffffffffu, src, q0);
-            const uint64_t s1 = __shfl_sync(0xffffffffu, src, q1);
+            // four records' lines in flight (a record repeats when fewer remain)
+            int q[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                q[j] = hm ? __ffs(hm) - 1 : q[0];
+                if (hm) hm &= hm - 1;
+            }
+            uint64_t s[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) s[j] = __shfl_sync(0xffffffffu, src, q[j]);
 #pragma unroll
             for (int u = 0; u < WPL; ++u) {
                 const uint32_t w = lane + 32 * u;
-                if (w < nw) acc[u] |= rbits[s0 + w] | rbits[s1 + w];
+                if (w < nw) acc[u] |= rbits[s[0] + w] | rbits[s[1] + w] | rbits[s[2] + w] | rbits[s[3] + w];
             }
         }
         uint32_t lm = __ballot_sync(0xffffffffu, light);
