@@ -476,14 +476,14 @@ def path_algorithmic_bytes(r, w, record_bytes):
 # DRAM bytes per algorithmic byte of kernels whose launch sites declare their
 # algorithmic bytes (one capture; the ratio carries to other sizes).
 TRAFFIC_RATIO = {
-    # first phase-1 pass at 40 genomes: 20,646,311 pairs, 495.5 MB algorithmic, 472.9 MB DRAM
-    "k_rs_downsweep": (472923136 / 495511464, "profiles/phase12_top_kernels_pangenome40.md"),
+    # first phase-1 pass at 40 genomes: 20,646,311 pairs, 495.5 MB algorithmic, 472.2 MB DRAM
+    "k_rs_downsweep": (472166144 / 495511464, "profiles/phase12_top_kernels_pangenome40.md"),
 }
 
 TRAFFIC_PER_UNIT = {
-    "k_minimizers": (1.687, "profiles/phase12_top_kernels_pangenome40.md"),   # per base
-    "k_insert": (61.409, "profiles/phase12_top_kernels_pangenome40.md"),      # per occurrence
-    "k_ext_mask": (55.173, "profiles/phase12_top_kernels_pangenome40.md"),    # per distinct k-mer
+    "k_minimizers": (1.691, "profiles/phase12_top_kernels_pangenome40.md"),   # per base
+    "k_insert": (61.321, "profiles/phase12_top_kernels_pangenome40.md"),      # per occurrence
+    "k_ext_mask": (55.196, "profiles/phase12_top_kernels_pangenome40.md"),    # per distinct k-mer
     "k_frag_write": (3.688, "profiles/phase12_top_kernels_pangenome40.md"),   # per fragment byte
 }
 
