@@ -103,14 +103,21 @@ void apply_limit(cdbg_engine* e) {
     e->P.set_limit(lim, &e->A, ext);
 }
 
-// Per-call scope: route kernel timing to this engine's profiler and fold the
-// recorded launches into its totals when the call returns.
+// Per-call scope: route kernel timing to this engine's profiler and small
+// device reads to its mailbox, and fold the recorded launches into its totals
+// when the call returns.
 struct call_scope {
     cdbg_engine* e;
-    explicit call_scope(cdbg_engine* en) : e(en) { cdbg::g_prof = &e->prof; }
+    cdbg::kernel_profiler* prev_prof;
+    cdbg::host_mailbox* prev_mailbox;
+    explicit call_scope(cdbg_engine* en) : e(en), prev_prof(cdbg::g_prof), prev_mailbox(cdbg::g_mailbox) {
+        cdbg::g_prof = &e->prof;
+        cdbg::g_mailbox = &e->mailbox;
+    }
     ~call_scope() {
         if (e->prof.on) e->prof.resolve();
-        cdbg::g_prof = nullptr;
+        cdbg::g_prof = prev_prof;  // calls nest (the autotuner builds through the public entry)
+        cdbg::g_mailbox = prev_mailbox;
     }
 };
 
@@ -188,11 +195,11 @@ namespace cdbg {
 std::atomic<uint64_t> g_launches{0};
 void set_last_error(std::string const& msg) { g_last_error = msg; }
 thread_local kernel_profiler* g_prof = nullptr;
+thread_local host_mailbox* g_mailbox = nullptr;
 
 void check_device_error(cdbg_engine* e, char const* stage) {
     uint32_t v = 0;
-    CDBG_CUDA(cudaMemcpyAsync(&v, e->d_err, 4, cudaMemcpyDeviceToHost, e->st));
-    CDBG_CUDA(cudaStreamSynchronize(e->st));
+    read_small(&v, e->d_err, 4, e->st);
     if (v) {
         CDBG_CUDA(cudaMemsetAsync(e->d_err, 0, 4, e->st));
         throw std::runtime_error(std::string("device error ") + std::to_string(v) + " in " + stage);
@@ -261,6 +268,9 @@ int cdbg_engine_create(int device, cdbg_engine** out) {
         e->P.set_stream(e->st);
         CDBG_CUDA(cudaMalloc(&e->d_err, 16));
         CDBG_CUDA(cudaMemset(e->d_err, 0, 16));
+        e->mailbox.bytes = size_t(256) << 10;
+        CDBG_CUDA(cudaHostAlloc(&e->mailbox.h, e->mailbox.bytes, cudaHostAllocMapped));
+        CDBG_CUDA(cudaHostGetDevicePointer(&e->mailbox.d, e->mailbox.h, 0));
         *out = e;
         return 0;
     } catch (std::exception const& ex) {
@@ -284,6 +294,7 @@ void cdbg_engine_destroy(cdbg_engine* e) {
     }
     if (e->copy_ev) cudaEventDestroy(e->copy_ev);
     if (e->own_st) cudaStreamDestroy(e->own_st);
+    if (e->mailbox.h) cudaFreeHost(e->mailbox.h);
     delete e;
 }
 

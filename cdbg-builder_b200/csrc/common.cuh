@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <cstring>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -144,5 +145,44 @@ __device__ __forceinline__ uint64_t stream_bits64(uint64_t const* __restrict__ w
     if (s) lo |= __ldg(words + w + 1) << (64 - s);
     return lo;
 }
+
+// ---- small device -> host reads
+// The host waits for a few bytes of device memory (a count, a flag, digit
+// histograms).  With a mailbox installed for the calling thread (mapped pinned
+// host memory, installed by the engine for the duration of each call), a
+// one-block kernel stores the bytes into it over PCIe, and no copy engine is
+// involved: a cudaMemcpyAsync would wait behind the large output copies that
+// stream to the host on the engine's copy stream (tens of milliseconds each)
+// and stall every batch.  Without a mailbox it is a cudaMemcpyAsync.
+struct host_mailbox {
+    void* h = nullptr;  // host address
+    void* d = nullptr;  // device address of the same pages
+    size_t bytes = 0;
+};
+extern thread_local host_mailbox* g_mailbox;
+
+namespace {
+__global__ void k_mail_bytes(uint8_t const* __restrict__ src, uint8_t* __restrict__ dst, uint64_t n) {
+    if (((uintptr_t)src & 7) == 0 && (n & 7) == 0) {
+        for (uint64_t i = threadIdx.x; i < n / 8; i += blockDim.x)
+            reinterpret_cast<uint64_t*>(dst)[i] = reinterpret_cast<uint64_t const*>(src)[i];
+    } else {
+        for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+    }
+}
+
+inline void read_small(void* host_dst, void const* dev_src, size_t n, cudaStream_t st) {
+    host_mailbox* mb = g_mailbox;
+    if (mb && mb->h && n <= mb->bytes) {
+        k_mail_bytes<<<1, 256, 0, st>>>(static_cast<uint8_t const*>(dev_src), static_cast<uint8_t*>(mb->d), n);
+        CDBG_CHECK_LAUNCH();
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        std::memcpy(host_dst, mb->h, n);
+    } else {
+        CDBG_CUDA(cudaMemcpyAsync(host_dst, dev_src, n, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+    }
+}
+}  // namespace
 
 }  // namespace cdbg

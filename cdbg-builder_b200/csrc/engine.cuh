@@ -52,6 +52,10 @@ struct cdbg_engine {
     bool have_rs = false;
     // host copies of the last cdbg_gpu_build's outputs (outputs_to_host = 1)
     pinned_buffer h_frag, h_words, h_offsets;
+    // mapped pinned page for the small reads the host waits on (counts, flags,
+    // histograms): written by a kernel, so they never queue behind the output
+    // copies on the copy engine
+    cdbg::host_mailbox mailbox;
 };
 
 namespace cdbg {

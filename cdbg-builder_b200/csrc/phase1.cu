@@ -777,8 +777,7 @@ inline unsigned grid(uint64_t n, unsigned t) { return (unsigned)ceil_div(n, t); 
 template <typename T>
 T read_dev(T const* p, cudaStream_t st) {
     T v;
-    CDBG_CUDA(cudaMemcpyAsync(&v, p, sizeof(T), cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaStreamSynchronize(st));
+    read_small(&v, p, sizeof(T), st);
     return v;
 }
 
@@ -865,8 +864,7 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
     k_run_kmers<<<grid(nruns, 256), 256, 0, st>>>(rt.n, rt.len, k, acc);
     CDBG_CHECK_LAUNCH();
     unsigned long long h[2];
-    CDBG_CUDA(cudaMemcpyAsync(h, acc, 16, cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaStreamSynchronize(st));
+    read_small(h, acc, 16, st);
     rt.n_kmers = h[0];
     rt.n_bases = h[1];
 }
@@ -1011,9 +1009,8 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     prim::exclusive_scan<uint32_t, uint64_t>(head, rid, n, A, st, rid + n);
     prim::exclusive_scan<uint32_t, uint64_t>(ckeep, cpos, n, A, st, cpos + n);
     uint64_t tot[2];
-    CDBG_CUDA(cudaMemcpyAsync(&tot[0], rid + n, 8, cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaMemcpyAsync(&tot[1], cpos + n, 8, cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaStreamSynchronize(st));
+    read_small(&tot[0], rid + n, 8, st);
+    read_small(&tot[1], cpos + n, 8, st);
     const uint64_t nr = tot[0], nc = tot[1];
     rs.n = nr;
     rs.ncolors = nc;

@@ -64,8 +64,7 @@ inline unsigned grid(uint64_t n, unsigned t) { return (unsigned)ceil_div(n, t); 
 template <typename T>
 T read_dev(T const* p, cudaStream_t st) {
     T v;
-    CDBG_CUDA(cudaMemcpyAsync(&v, p, sizeof(T), cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaStreamSynchronize(st));
+    read_small(&v, p, sizeof(T), st);
     return v;
 }
 
@@ -2447,7 +2446,8 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             prim::exclusive_scan<uint64_t, uint64_t>(nbits, boff, nnew, A, st, boff + nnew);
             const uint64_t badd = read_dev(boff + nnew, st);
             add_offsets(boff, nnew + 1, dict.nbits, boff, st);  // absolute bit offsets
-            if (p.copy_st) {
+            if (p.copy_st && (dict.bit_off.cap < base + nnew + 1 ||
+                              dict.words.cap < (dict.nbits + badd + 63) / 64 + 4)) {
                 // growing frees the old arrays: after the host copies that read them
                 CDBG_CUDA(cudaEventRecord(p.copy_ev, p.copy_st));
                 CDBG_CUDA(cudaStreamWaitEvent(st, p.copy_ev, 0));
@@ -2653,9 +2653,8 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     k_gather_u64<<<grid(B + 1, 256), 256, 0, st>>>(B + 1, occ, rs.bucket_start, d_bocc);
     CDBG_CHECK_LAUNCH();
     std::vector<uint64_t> bocc(B + 1), hbstart(B + 1);
-    CDBG_CUDA(cudaMemcpyAsync(bocc.data(), d_bocc, 8ull * (B + 1), cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaMemcpyAsync(hbstart.data(), rs.bucket_start, 8ull * (B + 1), cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaStreamSynchronize(st));
+    read_small(bocc.data(), d_bocc, 8ull * (B + 1), st);
+    read_small(hbstart.data(), rs.bucket_start, 8ull * (B + 1), st);
     uint64_t budget = p.batch_occ;
     if (budget == 0) {
         int dev = 0;

@@ -355,8 +355,7 @@ int radix_sort_pairs(K* keys, V* vals, uint64_t n, int begin_bit, int end_bit,
         CDBG_CHECK_LAUNCH();
     }
     std::vector<unsigned long long> h((size_t)npasses * RS_BINS);
-    CDBG_CUDA(cudaMemcpyAsync(h.data(), hist, h.size() * 8, cudaMemcpyDeviceToHost, st));
-    CDBG_CUDA(cudaStreamSynchronize(st));
+    read_small(h.data(), hist, h.size() * 8, st);
 
     const uint64_t ntiles = ceil_div(n, RS_TILE);
     K* k2 = A.alloc<K>(n);
