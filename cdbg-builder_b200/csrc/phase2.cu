@@ -1001,6 +1001,30 @@ __global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint
     if (j >= nc) return;
     const cand_set cs = cand_get(L, cv.kind_id[j]);
     const uint64_t N = cs.n;
+    const uint64_t sparse_t = (uint64_t)(0.25 * (double)C);
+    const uint64_t dense_t = (uint64_t)(0.75 * (double)C);
+    const uint32_t hdr = delta_bits(N);
+    if (!ENC) {
+        // sizes that need no bitmap: the plain-bitmap range has a fixed size,
+        // and a sparse set held as an ascending list has its gaps in the list
+        if (N >= sparse_t && N < dense_t) {
+            if (lane == 0) nbits[j] = hdr + C;
+            return;
+        }
+        if (cs.list && N < sparse_t) {
+            uint64_t acc = 0;
+            for (uint64_t base = 0; base < N; base += 32) {
+                const uint64_t i = base + lane;
+                const uint32_t v = i < N ? cs.list[i] : 0u;
+                uint32_t pv = __shfl_up_sync(0xffffffffu, v, 1);
+                if (lane == 0 && base) pv = cs.list[base - 1];
+                if (i < N) acc += delta_bits(i == 0 ? (uint64_t)v : (uint64_t)(v - pv - 1));
+            }
+            acc = warp_sum64(acc);
+            if (lane == 0) nbits[j] = hdr + acc;
+            return;
+        }
+    }
     if (cs.bm) {
         for (uint32_t w = lane; w < nw; w += 32) bm[w] = cs.bm[w];
     } else {
@@ -1009,10 +1033,7 @@ __global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint
         warp_or_list(bm, cs.list, 0, N, nw, lane);
     }
     __syncwarp();
-    const uint64_t sparse_t = (uint64_t)(0.25 * (double)C);
-    const uint64_t dense_t = (uint64_t)(0.75 * (double)C);
     uint64_t pos = ENC ? boff[j] : 0;
-    const uint32_t hdr = delta_bits(N);
     if (ENC && lane == 0) put_delta(words, pos, N);
     pos += hdr;
     if (N >= sparse_t && N < dense_t) {
