@@ -754,8 +754,8 @@ __global__ void k_heavy_bitmaps(uint64_t nrec, uint32_t const* __restrict__ flag
 // heavy records, per-color bits for the rest) -> mbits, size, set hash.
 // The records' metadata is fetched 32 at a time, one record per lane; heavy
 // records' bitmap words are ORed into registers (lane owns words lane + 32u,
-// u < WPL), four records' lines in flight at a time; the rest set bits in the
-// warp's shared bitmap.
+// u < WPL), four records' lines in flight at a time; the rest have their
+// colors spread over the lanes and set bits in the warp's shared bitmap.
 template <int WPL>
 __global__ void __launch_bounds__(256) k_union_bm(
     uint64_t M, uint64_t const* __restrict__ mbeg, uint64_t const* __restrict__ mend,
@@ -807,11 +807,31 @@ __global__ void __launch_bounds__(256) k_union_bm(
                 if (w < nw) acc[u] |= rbits[s[0] + w] | rbits[s[1] + w] | rbits[s[2] + w] | rbits[s[3] + w];
             }
         }
-        uint32_t lm = __ballot_sync(0xffffffffu, light);
-        while (lm) {
-            const int q = __ffs(lm) - 1;
-            lm &= lm - 1;
-            warp_or_list(bm, colors, __shfl_sync(0xffffffffu, c0, q), __shfl_sync(0xffffffffu, c1, q), nw, lane);
+        // light records: their colors laid end to end over the warp, 32 at a
+        // time (lane e finds its record by a search over the length prefix)
+        const uint32_t len = light ? (uint32_t)(c1 - c0) : 0u;  // < 8192 colors in bitmap mode
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t excl = incl - len;
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        for (uint32_t e0 = 0; e0 < total; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            int q = 0;  // the last lane whose range starts at or before e
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const uint32_t ex = __shfl_sync(0xffffffffu, excl, (q + step) & 31);
+                if (q + step <= 31 && ex <= e) q += step;
+            }
+            const uint64_t cq = __shfl_sync(0xffffffffu, c0, q);
+            const uint32_t xq = __shfl_sync(0xffffffffu, excl, q);
+            if (e < total) {
+                const uint32_t v = colors[cq + (e - xq)];
+                atomicOr(&bm[v >> 5], 1u << (v & 31));
+            }
         }
     }
     __syncwarp();
