@@ -733,21 +733,29 @@ __global__ void k_heavy_flags(uint64_t nu, uint64_t const* __restrict__ upairs, 
     if (col_off[r + 1] - col_off[r] >= heavy) flag[r - R0] = 1u;
 }
 
-// Warp per heavy record: its colors as a bitmap in rbits[hpos[r - R0] * nw].
+// Heavy records' colors as bitmaps in rbits[hpos[r - R0] * nw].
 __global__ void k_heavy_bitmaps(uint64_t nrec, uint32_t const* __restrict__ flag, uint64_t const* __restrict__ hpos,
                                 uint32_t R0, uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors,
                                 uint32_t nw, uint32_t* __restrict__ rbits) {
     extern __shared__ uint32_t smem_bm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     uint32_t* bm = smem_bm + (size_t)wib * nw;
-    const uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
-    if (i >= nrec || !flag[i]) return;
-    for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
-    __syncwarp();
-    warp_or_list(bm, colors, col_off[R0 + i], col_off[R0 + i + 1], nw, lane);
-    __syncwarp();
-    uint32_t* out = rbits + hpos[i] * (uint64_t)nw;
-    for (uint32_t w = lane; w < nw; w += 32) out[w] = bm[w];
+    // 32 records per warp: the lanes read the flags at once (few records are
+    // heavy), then the warp builds each heavy record's bitmap
+    const uint64_t i0 = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + wib) * 32;
+    if (i0 >= nrec) return;
+    uint32_t fm = __ballot_sync(0xffffffffu, i0 + lane < nrec && flag[i0 + lane]);
+    while (fm) {
+        const uint64_t i = i0 + (uint32_t)(__ffs(fm) - 1);
+        fm &= fm - 1;
+        for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0;
+        __syncwarp();
+        warp_or_list(bm, colors, col_off[R0 + i], col_off[R0 + i + 1], nw, lane);
+        __syncwarp();
+        uint32_t* out = rbits + hpos[i] * (uint64_t)nw;
+        for (uint32_t w = lane; w < nw; w += 32) out[w] = bm[w];
+        __syncwarp();
+    }
 }
 
 // Warp per multi-record node: OR of its records' color sets (bitmap words for
@@ -934,6 +942,14 @@ __device__ __forceinline__ cand_set cand_get(list_src const& L, uint32_t kind_id
     cand_list(L, kind_id, c.list, c.n);
     return c;
 }
+__device__ __forceinline__ cand_set shfl_set(cand_set const& s, int src) {
+    cand_set r;
+    r.list = (uint32_t const*)__shfl_sync(0xffffffffu, (unsigned long long)s.list, src);
+    r.bm = (uint32_t const*)__shfl_sync(0xffffffffu, (unsigned long long)s.bm, src);
+    r.n = __shfl_sync(0xffffffffu, (unsigned long long)s.n, src);
+    return r;
+}
+
 __device__ __forceinline__ bool sets_equal(cand_set const& a, cand_set const& b, uint32_t nw) {
     if (a.n != b.n) return false;
     if (a.bm && b.bm) {
@@ -1008,18 +1024,13 @@ __device__ __forceinline__ uint64_t put_delta(uint64_t* w, uint64_t pos, uint64_
     return pos + l;
 }
 
-// Warp per candidate class.  Pass 0 (ENC = false): encoded size -> nbits[j].
-// Pass 1: write at bit offset boff[j] of `words` (zeroed).
+// One candidate class by the whole warp (bm: the warp's C-bit shared bitmap).
+// Pass 0 (ENC = false): encoded size -> nbits[j].  Pass 1: write at bit
+// offset pos0 of `words` (zeroed).
 template <bool ENC>
-__global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint64_t* __restrict__ nbits,
-                         uint64_t const* __restrict__ boff, uint64_t* __restrict__ words) {
-    extern __shared__ uint32_t smem_bm[];
-    const uint32_t nw = (C + 31) / 32;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    uint32_t* bm = smem_bm + (size_t)wib * nw;
-    const uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
-    if (j >= nc) return;
-    const cand_set cs = cand_get(L, cv.kind_id[j]);
+__device__ __forceinline__ void encode_one(cand_set const& cs, uint64_t j, uint64_t pos0, uint32_t C, uint32_t nw,
+                                           uint32_t* bm, int lane, uint64_t* __restrict__ nbits,
+                                           uint64_t* __restrict__ words) {
     const uint64_t N = cs.n;
     const uint64_t sparse_t = (uint64_t)(0.25 * (double)C);
     const uint64_t dense_t = (uint64_t)(0.75 * (double)C);
@@ -1053,7 +1064,7 @@ __global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint
         warp_or_list(bm, cs.list, 0, N, nw, lane);
     }
     __syncwarp();
-    uint64_t pos = ENC ? boff[j] : 0;
+    uint64_t pos = pos0;
     if (ENC && lane == 0) put_delta(words, pos, N);
     pos += hdr;
     if (N >= sparse_t && N < dense_t) {
@@ -1122,6 +1133,34 @@ __global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint
             p = put_delta(words, p, pv < 0 ? (uint64_t)v : (uint64_t)(v - pv - 1));
             pv = v;
         }
+    }
+}
+
+// Warp per 32 candidate classes: the lanes fetch the 32 candidates' sets
+// (and pass-1 offsets) at once, then the warp encodes them one by one, so the
+// dependent metadata loads are paid once per 32 candidates.
+template <bool ENC>
+__global__ void k_encode(uint64_t nc, cand_view cv, list_src L, uint32_t C, uint64_t* __restrict__ nbits,
+                         uint64_t const* __restrict__ boff, uint64_t* __restrict__ words) {
+    extern __shared__ uint32_t smem_bm[];
+    const uint32_t nw = (C + 31) / 32;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* bm = smem_bm + (size_t)wib * nw;
+    const uint64_t j0 = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + wib) * 32;
+    if (j0 >= nc) return;
+    const uint64_t jl = j0 + lane;
+    cand_set mine{nullptr, nullptr, 0};
+    uint64_t pos = 0;
+    if (jl < nc) {
+        mine = cand_get(L, cv.kind_id[jl]);
+        if (ENC) pos = boff[jl];
+    }
+    const uint32_t cnt = nc - j0 < 32 ? (uint32_t)(nc - j0) : 32u;
+    for (uint32_t q = 0; q < cnt; ++q) {
+        const cand_set cs = shfl_set(mine, (int)q);
+        const uint64_t p = __shfl_sync(0xffffffffu, pos, (int)q);
+        encode_one<ENC>(cs, j0 + q, p, C, nw, bm, lane, nbits, words);
+        __syncwarp();  // the next candidate reuses the bitmap
     }
 }
 
@@ -1276,14 +1315,6 @@ __device__ __forceinline__ bool warp_sets_equal(cand_set const& a, cand_set cons
         if (__any_sync(0xffffffffu, bad)) return false;
     }
     return true;
-}
-
-__device__ __forceinline__ cand_set shfl_set(cand_set const& s, int src) {
-    cand_set r;
-    r.list = (uint32_t const*)__shfl_sync(0xffffffffu, (unsigned long long)s.list, src);
-    r.bm = (uint32_t const*)__shfl_sync(0xffffffffu, (unsigned long long)s.bm, src);
-    r.n = __shfl_sync(0xffffffffu, (unsigned long long)s.n, src);
-    return r;
 }
 
 // Members of an equal-hash run of candidates against the run head, on the
@@ -2300,7 +2331,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
                 CDBG_CUDA(cudaFuncSetAttribute(k_heavy_bitmaps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
             if (nheavy) {
                 CDBG_PROF("k_heavy_bitmaps", st);
-                k_heavy_bitmaps<<<grid(nrec, wpb), wpb * 32, shm, st>>>(nrec, hflag, hpos, (uint32_t)R0, R.col_off,
+                k_heavy_bitmaps<<<grid(ceil_div(nrec, 32), wpb), wpb * 32, shm, st>>>(nrec, hflag, hpos, (uint32_t)R0, R.col_off,
                                                                         R.colors, nw, rbits);
             }
             CDBG_CHECK_LAUNCH();
@@ -2442,7 +2473,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         uint64_t* cb = A.alloc<uint64_t>(nr + 1);
         {
             CDBG_PROF("k_encode", st);
-            k_encode<false><<<grid(nr, wpb), wpb * 32, shm, st>>>(nr, rv, L, C, cbits, nullptr, nullptr);
+            k_encode<false><<<grid(ceil_div(nr, 32), wpb), wpb * 32, shm, st>>>(nr, rv, L, C, cbits, nullptr, nullptr);
         }
         CDBG_CHECK_LAUNCH();
         prim::exclusive_scan<uint64_t, uint64_t>(cbits, cb, nr, A, st, cb + nr);
@@ -2452,7 +2483,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         CDBG_CUDA(cudaMemsetAsync(cw, 0, 8 * cwn, st));
         {
             CDBG_PROF("k_encode", st);
-            k_encode<true><<<grid(nr, wpb), wpb * 32, shm, st>>>(nr, rv, L, C, nullptr, cb, cw);
+            k_encode<true><<<grid(ceil_div(nr, 32), wpb), wpb * 32, shm, st>>>(nr, rv, L, C, nullptr, cb, cw);
         }
         CDBG_CHECK_LAUNCH();
         uint32_t* rcid = A.alloc<uint32_t>(nr + 1);
