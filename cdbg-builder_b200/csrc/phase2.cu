@@ -80,6 +80,23 @@ __device__ __forceinline__ uint32_t upper_bound_u64(uint64_t const* a, uint64_t 
     return (uint32_t)lo;
 }
 
+// upper_bound(off, n1, x) - 1 (the bucket of x, `off` ascending) for the
+// active lanes of a warp whose x ascend with the lane (consecutive records or
+// occurrences, so nearly always one bucket): the first active lane searches,
+// the others take its bucket when x lies in its range and search otherwise.
+// Every lane of the warp calls it.
+__device__ __forceinline__ uint32_t warp_bucket_of(uint64_t const* off, uint64_t n1, uint64_t x, bool active) {
+    const uint32_t am = __ballot_sync(0xffffffffu, active);
+    if (!am) return 0;
+    const int leader = __ffs(am) - 1;
+    const uint64_t xl = __shfl_sync(0xffffffffu, x, leader);
+    uint32_t b = 0;
+    if ((int)(threadIdx.x & 31) == leader) b = upper_bound_u64(off, n1, xl) - 1;
+    b = __shfl_sync(0xffffffffu, b, leader);
+    if (active && !(off[b] <= x && x < off[b + 1])) b = upper_bound_u64(off, n1, x) - 1;
+    return b;
+}
+
 // ------------------------------------------------------------------ set hash
 // Order-independent hash of a color set: the sum, over the 32-color words
 // that hold at least one color, of a mix of (word index, word bits), then
@@ -300,11 +317,12 @@ __global__ void k_rec_prep(uint64_t n, uint32_t const* __restrict__ len, uint32_
                            uint64_t* __restrict__ nk, uint32_t* __restrict__ rbucket,
                            uint64_t const* __restrict__ col_off, uint32_t const* __restrict__ colors,
                            uint64_t* __restrict__ rhash) {
-    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t b = warp_bucket_of(bstart, (uint64_t)B + 1, r, r < n);
     if (r >= n) return;
     const uint32_t l = len[r];
     nk[r] = l >= k ? (uint64_t)(l - k + 1) : 0;
-    rbucket[r] = upper_bound_u64(bstart, (uint64_t)B + 1, r) - 1;
+    rbucket[r] = b;
     const uint64_t c0 = col_off[r], c1 = col_off[r + 1];
     rhash[r] = set_hash_final(list_word_sum(colors + c0, c1 - c0), c1 - c0);
 }
@@ -407,11 +425,13 @@ __global__ void __launch_bounds__(256) k_make_nodes(uint64_t nocc, uint32_t cons
                                                     uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
                                                     uint32_t* __restrict__ n_bucket) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nocc) return;
-    const uint32_t w = bits[t >> 5];
-    if (!((w >> (t & 31)) & 1u)) return;
+    const uint32_t w = t < nocc ? bits[t >> 5] : 0u;
+    const bool first = (w >> (t & 31)) & 1u;
+    const uint32_t s = first ? occ_slot[t] & 0x7fffffffu : 0u;
+    // the slot's table: consecutive occurrences lie in one bucket's slot range
+    const uint32_t tb = warp_bucket_of(TB.tab_off, nb + 1, s, first);
+    if (!first) return;
     const uint64_t n = wpre[t >> 5] + __popc(w & ((1u << (t & 31)) - 1u));
-    const uint32_t s = occ_slot[t] & 0x7fffffffu;
     slot_t<K>& e = slots[s];
     const K key = e.key;
     const uint32_t om = e.om;
@@ -421,7 +441,7 @@ __global__ void __launch_bounds__(256) k_make_nodes(uint64_t nocc, uint32_t cons
     uint32_t rec = NONE32;
     if (om & M_PRIMARY) rec = (om & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (om >> 4) - 1);
     n_rec[n] = rec;
-    n_bucket[n] = TB.b0 + upper_bound_u64(TB.tab_off, nb + 1, s) - 1;
+    n_bucket[n] = TB.b0 + tb;
 }
 
 // Block-wide reservation of `want` consecutive entries of *cnt per thread,
