@@ -1,0 +1,31 @@
+"""CPU: `bench.py --impl reference` (the reference's own CPU build of the path,
+timed on a bounded sample of the pangenome workload) prints one JSON line with
+the bench contract's keys, on the same metric and workload as the GPU arm."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT, ref_bin
+
+
+def test_reference_arm_prints_one_contract_line():
+    if not ref_bin("cdbg-build", 31):
+        pytest.skip("oracle/_ref not built")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--cpu-sample-genomes", "1"], capture_output=True, text=True, cwd=ROOT,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == "phase1+2 k-mers/s" and d["unit"] == "k-mers/s"
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 1
+    assert d["value"] > 0 and d["ms_per_step"] > 0
+    assert d["config"]["workload"].startswith("pangenome: 1000 genomes")
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
