@@ -6,17 +6,22 @@ insert, 1-200 contigs), k = 31, m = 12, 4096 buckets.  A step is one full pass
 of phase 1 + phase 2 over the whole collection (all k-mers), producing the
 frag spill and the color classes.
 
-  value   k-mers/s with the sequences already resident in HBM and the outputs
-          left on the device (cdbg_gpu_build, on_device = 1).
-  e2e     the same call with pinned host input buffers and host outputs: the
-          H2D copy of the sequences and the D2H copy of the frag bytes and the
-          color-set words are inside every timed step.
+  value     k-mers/s with the sequences already resident in HBM and the
+            outputs left on the device (cdbg_gpu_build, on_device = 1); CUDA
+            events on the stream the library launches on.
+  e2e       the reference's inputs and outputs: the collection as gzip FASTA
+            files on disk in, frag_unitigs.bin and .color_sets files out
+            (cdbg_gpu_build_files: host inflate and parse overlapped with the
+            upload and phase 1, phase 2 in HBM, outputs written); wall time
+            of each call.
+  e2e_host  pinned host sequences in, host outputs out (cdbg_gpu_build).
 
-Time is measured with CUDA events on the stream the library launches on
-(the engine runs on a torch stream), max over ranks.  `--impl reference`
-times the reference's own CPU build (oracle/_ref/cdbg-build, built from its
-sources) on a bounded sample with all host cores.  With --gpus N each rank
-builds its own collection (independent replicas, weak scaling).
+Max over ranks.  `--impl reference` times the reference's own phase 1 +
+phase 2 (oracle/_ref/ref_phase12: the builder's ingest_bucketed, close and
+process_buckets, built from the reference's sources) with all host cores on
+bounded samples of the same collection: step i runs slice i mod 8 of every
+genome.  With --gpus N each rank builds its own collection (independent
+replicas, weak scaling).
 """
 import argparse
 import json
@@ -33,7 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "cdbg-builder_b200"))
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-REF_BIN = os.path.join(ROOT, "oracle", "_ref", "cdbg-build")
+REF_P12 = os.path.join(ROOT, "oracle", "_ref", "ref_phase12")
 
 
 def parse():
@@ -44,9 +49,11 @@ def parse():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="pangenome")
     ap.add_argument("--genomes", type=int, default=0, help="override genome count (0 = workload's)")
-    ap.add_argument("--cpu-sample-genomes", type=int, default=128)
+    ap.add_argument("--ref-slices", type=int, default=8,
+                    help="reference CPU runs: 1/N of every genome per step (rotating over the N slices)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-dir", default="", help="directory for the e2e input/output files (default: temp)")
     ap.add_argument("--batch-occ", type=int, default=0)
     ap.add_argument("--table-slots-q", type=int, default=0,
                     help="k-mer table slots per 4 occurrences, 5..16 (0 = library default)")
@@ -150,26 +157,105 @@ def peaks():
 
 
 # ---------------------------------------------------------------- reference arm
-def run_reference_sample(genomes, k, blog2, threads, seed, workdir):
-    """One reference build of `genomes` genomes; returns (kmers, seconds p1+p2, detail)."""
-    from cdbg_gpu import synth
-    p, _, _, _ = synth.preset("pangenome", seed=seed)
-    ind = os.path.join(workdir, "in")
-    if not os.path.exists(os.path.join(ind, "filenames.txt")):
-        synth.write_fasta(p, genomes, ind, gzip_level=1)
-    _, lens, _ = synth.collection(p, genomes)
-    kmers = count_kmers(lens, k)
-    out = os.path.join(workdir, "o")
+def write_slice(seq, lens, per, s, nslices, k, out_dir, threads):
+    """Slice s of nslices of every genome of a collection (bases [s*T/S,
+    (s+1)*T/S) of each genome's concatenated contigs, contig boundaries kept),
+    one gzip FASTA file per genome (= one color), like the workload's inputs.
+    Returns (filenames list path, k-mers in the slice)."""
+    import zlib
+    from concurrent.futures import ThreadPoolExecutor
+    import numpy as np
+    os.makedirs(out_dir, exist_ok=True)
+    lens = lens.astype(np.int64)
+    ends = np.cumsum(lens)
+    g_first = np.concatenate(([0], np.cumsum(per)))  # first contig of each genome
+    contig_start = ends - lens
+    names = []
+    kmers = [0] * len(per)
+
+    def one(g):
+        c0, c1 = int(g_first[g]), int(g_first[g + 1])
+        gs, ge = int(contig_start[c0]), int(ends[c1 - 1])
+        T = ge - gs
+        a, b = gs + T * s // nslices, gs + T * (s + 1) // nslices
+        parts, km = [], 0
+        for c in range(c0, c1):
+            x, y = max(a, int(contig_start[c])), min(b, int(ends[c]))
+            if y > x:
+                parts.append(b">g%d_%d\n" % (g, c) + seq[x:y].tobytes() + b"\n")
+                km += max(y - x - k + 1, 0)
+        path = os.path.join(out_dir, "g%d.fa.gz" % g)
+        co = zlib.compressobj(1, zlib.DEFLATED, 31)
+        with open(path, "wb") as f:
+            f.write(co.compress(b"".join(parts)))
+            f.write(co.flush())
+        kmers[g] = km
+        return path
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        names = list(ex.map(one, range(len(per))))
+    lst = os.path.join(out_dir, "filenames.txt")
+    with open(lst, "w") as f:
+        f.write("".join(n + "\n" for n in names))
+    return lst, sum(kmers)
+
+
+def run_ref_phase12(filelist, k, B, threads, workdir):
+    """The reference's own phase 1 + phase 2 (oracle/_ref/ref_phase12: the
+    builder's ingest_bucketed, close and process_buckets, nothing after) over
+    the files; returns (seconds of the whole span, detail)."""
+    tmp = os.path.join(workdir, "tmp")
+    out = os.path.join(workdir, "out")
+    shutil.rmtree(tmp, ignore_errors=True)
     shutil.rmtree(out, ignore_errors=True)
-    os.makedirs(out)
-    r = subprocess.run([REF_BIN, "-i", os.path.join(ind, "filenames.txt"), "-k", str(k), "-o",
-                        os.path.join(out, "out"), "-t", str(threads), "-b", str(blog2), "-d",
-                        os.path.join(out, "tmp")], capture_output=True, text=True)
+    binp = REF_P12 + ("-largek" if k > 31 else "")
+    r = subprocess.run([binp, filelist, str(k), "0", str(B), str(threads), tmp, out], capture_output=True,
+                       text=True)
     if r.returncode != 0:
-        raise RuntimeError("reference build failed: " + r.stderr[-500:])
+        raise RuntimeError("reference phase 1 + 2 failed: " + r.stderr[-500:])
+    t = float(re.search(r"phase12_seconds=([0-9.eE+-]+)", r.stdout).group(1))
     t1 = float(re.search(r"\[bucket-write\] ([0-9.eE+-]+) s", r.stdout).group(1))
     t2 = float(re.search(r"\[bucket-process\] ([0-9.eE+-]+) s", r.stdout).group(1))
-    return kmers, t1 + t2, {"bucket_write_s": t1, "bucket_process_s": t2}
+    shutil.rmtree(tmp, ignore_errors=True)
+    shutil.rmtree(out, ignore_errors=True)
+    return t, {"phase12_s": t, "bucket_write_s": t1, "bucket_process_s": t2}
+
+
+class ReferenceSample:
+    """Bounded samples of the benchmark's own collection for the reference's
+    CPU build: the same seeded genomes as the GPU arm's (rank 0), cut into
+    `nslices` slices of every genome, so a sample keeps every color and the
+    collection's divergence structure; step i runs slice i mod nslices, so
+    consecutive steps cover the whole collection."""
+
+    def __init__(self, workload, n_genomes, nslices, threads, seed=1):
+        from cdbg_gpu import synth
+        p, _, self.k, blog2 = synth.preset(workload, seed=seed)
+        self.B = 1 << blog2
+        self.n, self.S, self.threads = n_genomes, nslices, threads
+        self.seq, self.lens, self.per = synth.collection(p, n_genomes)
+        self.work = tempfile.mkdtemp(prefix="cdbg_ref_")
+        self.slices = {}
+
+    def slice(self, s):
+        s %= self.S
+        if s not in self.slices:
+            self.slices[s] = write_slice(self.seq, self.lens, self.per, s, self.S, self.k,
+                                         os.path.join(self.work, "s%d" % s), self.threads)
+        return self.slices[s]
+
+    def run(self, s):
+        lst, kmers = self.slice(s)
+        t, det = run_ref_phase12(lst, self.k, self.B, self.threads, os.path.join(self.work, "run"))
+        return kmers, t, det
+
+    def describe(self, kmers):
+        return ("slice i mod %d (1/%d of every one of the %d genomes, gzip FASTA) per step, ~%d k-mers; "
+                "reference ingest_bucketed + close + process_buckets with -t %d, -b %d" % (
+                    self.S, self.S, self.n, kmers, self.threads, self.B.bit_length() - 1))
+
+    def close(self):
+        shutil.rmtree(self.work, ignore_errors=True)
 
 
 def workload_name(n_genomes, k, B, workload="pangenome"):
@@ -183,38 +269,52 @@ def workload_name(n_genomes, k, B, workload="pangenome"):
     return "%s: %s, k=%d, m=%d, %d buckets" % (workload, shape % n_genomes, k, best_m(k), B)
 
 
+def workload_config(workload, n_genomes, k, B, seq_bytes):
+    """The `config` both arms print (identical, so the lines compare)."""
+    from cdbg_gpu.native import best_m
+    return {"workload": workload_name(n_genomes, k, B, workload), "genomes": n_genomes, "k": k, "m": best_m(k),
+            "buckets": B,
+            "l2": ("inputs (%.1f GB) larger than L2" % (seq_bytes / 1e9)) if seq_bytes > 126e6 else
+                  ("inputs (%.0f MB) smaller than L2, not flushed between steps" % (seq_bytes / 1e6))}
+
+
 def reference_arm(a):
     rank, _, world = dist_env()
     if rank != 0:
         return 0
-    if not os.path.exists(REF_BIN):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cdbg-build not built"}))
+    if not os.path.exists(REF_P12):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_phase12 not built"}))
         return 0
+    from cdbg_gpu import synth
     threads = os.cpu_count() or 1
-    k, blog2 = 31, 12
-    g = a.cpu_sample_genomes
-    work = tempfile.mkdtemp(prefix="cdbg_ref_")
+    _, n_genomes, k, blog2 = synth.preset(a.workload)
+    if a.genomes:
+        n_genomes = a.genomes
+    R = ReferenceSample(a.workload, n_genomes, a.ref_slices, threads)
     try:
+        i = 0
         for _ in range(a.warmup):
-            run_reference_sample(g, k, blog2, threads, 1, work)
-        vals, secs = [], []
-        kmers = 0
+            R.run(i)
+            i += 1
+        km_tot, s_tot, secs, det = 0, 0.0, [], None
         for _ in range(a.steps):
-            kmers, s, det = run_reference_sample(g, k, blog2, threads, 1, work)
-            vals.append(kmers / s)
+            km, s, det = R.run(i)
+            i += 1
+            km_tot += km
+            s_tot += s
             secs.append(s)
+        sample = R.describe(km_tot // max(a.steps, 1))
+        cfg = workload_config(a.workload, n_genomes, k, R.B, R.seq.nbytes)
     finally:
-        shutil.rmtree(work, ignore_errors=True)
-    v = statistics.median(vals)
-    sample = "%d of 1000 pangenome genomes (~4.8 Mbp, gzip FASTA), %d k-mers per step" % (g, kmers)
+        R.close()
+    v = km_tot / s_tot
     line = {"impl": "reference", "metric": "phase1+2 k-mers/s", "value": v, "unit": "k-mers/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": 1000 * statistics.median(secs), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": workload_name(1000, k, 1 << blog2), "sample": sample,
-                       "parallelism": "reference cdbg-build -t %d" % threads},
+            "ms_per_step": 1000 * s_tot / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64" if k <= 31 else "u128", "data": "synthetic",
+            "config": cfg, "sample": sample,
             "cpu_baseline": {"value": v, "unit": "k-mers/s", "cores": threads, "kind": "reference",
-                             "sample": sample},
+                             "sample": sample, "last_step": det},
             "e2e": {"value": v, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -320,22 +420,52 @@ def main_gpu(a):
     r = res[-1]
     value = job_kmers / (ms / 1000.0)
 
-    # ---- e2e: pinned host buffers in, host outputs out
+    # ---- e2e: the reference's inputs and outputs -- the collection as gzip
+    # FASTA files on disk in, frag_unitigs.bin and .color_sets files out --
+    # through cdbg_gpu_build_files (host inflate/parse overlapped with the
+    # upload and phase 1, phase 2 in HBM, device Elias-Fano finalize, file
+    # writes); wall time of each call, max over ranks
     e2e = None
+    e2e_host = None
     if not a.no_e2e:
+        fdir = tempfile.mkdtemp(prefix="cdbg_e2e_", dir=a.e2e_dir or None)
+        try:
+            lst = synth.write_fasta(p, n_genomes, os.path.join(fdir, "in"), gzip_level=1)
+            files = [l.strip() for l in open(lst) if l.strip()]
+            gz_bytes = sum(os.path.getsize(f) for f in files)
+            frag_p, cs_p = os.path.join(fdir, "frag_unitigs.bin"), os.path.join(fdir, "out.color_sets")
+            for _ in range(max(1, min(a.warmup, 2))):
+                eng.build_files(files, k, B, frag_p, cs_p)
+            barrier()
+            torch.cuda.synchronize()
+            walls = []
+            for _ in range(a.steps):
+                t0 = time.perf_counter()
+                re2 = eng.build_files(files, k, B, frag_p, cs_p)
+                walls.append(time.perf_counter() - t0)
+            ems = 1000.0 * sum(walls) / len(walls)
+            ems = max_over_ranks(ems, world, "cuda")
+            e2e = {"value": job_kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
+                   "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes),
+                   "path": "cdbg_gpu_build_files: %d gzip FASTA files (%.2f GB) -> frag_unitigs.bin (%.2f GB) + "
+                           ".color_sets, wall time per call" % (len(files), gz_bytes / 1e9,
+                                                                 re2.frag_nbytes / 1e9)}
+        finally:
+            shutil.rmtree(fdir, ignore_errors=True)
+        # the same build from pinned host sequences to host outputs
         step(host_batch, True)
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(a.steps):
-            re2 = step(host_batch, True)
+            re3 = step(host_batch, True)
         e1.record(stream)
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1) / a.steps
-        ems = max_over_ranks(ems, world, "cuda")
-        e2e = {"value": job_kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
-               "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes)}
+        hms = max_over_ranks(e0.elapsed_time(e1) / a.steps, world, "cuda")
+        e2e_host = {"value": job_kmers / (hms / 1000.0), "unit": "k-mers/s", "ms_per_step": hms,
+                    "h2d_bytes_per_step": int(re3.h2d_bytes), "d2h_bytes_per_step": int(re3.d2h_bytes),
+                    "path": "cdbg_gpu_build: pinned host ASCII sequences -> host outputs"}
 
     # ---- plain path: one bucket per batch (one launch sequence per bucket)
     plain = None
@@ -382,31 +512,30 @@ def main_gpu(a):
 
     # ---- CPU baseline (reference, bounded sample), rank 0 at N = 1
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(REF_BIN):
-        work = tempfile.mkdtemp(prefix="cdbg_cpu_")
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(REF_P12):
+        R = ReferenceSample(a.workload, n_genomes, a.ref_slices, os.cpu_count() or 1)
         try:
-            km, s, det = run_reference_sample(a.cpu_sample_genomes, k, blog2, os.cpu_count() or 1, 1, work)
+            km, s, det = R.run(0)
             cpu = {"value": km / s, "unit": "k-mers/s", "cores": os.cpu_count(), "kind": "reference",
-                   "sample": "%d of %d genomes, %d k-mers, reference cdbg-build -t %d -b %d (%s)" % (
-                       a.cpu_sample_genomes, n_genomes, km, os.cpu_count(), blog2, json.dumps(det))}
+                   "sample": R.describe(km), "step": det}
         finally:
-            shutil.rmtree(work, ignore_errors=True)
+            R.close()
 
     if rank == 0:
         top = sorted(kstats.items(), key=lambda kv: -kv[1][0])[:20]
         line = {"metric": "phase1+2 k-mers/s", "value": value, "unit": "k-mers/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64" if k <= 31 else "u128", "data": "synthetic",
-                "config": {"workload": workload_name(n_genomes, k, B, a.workload),
-                           "kmers_per_step": int(job_kmers), "bases": int(seq.nbytes),
-                           "l2": "inputs (%.1f GB) larger than L2" % (seq.nbytes / 1e9),
-                           "parallelism": "replicas%d" % world, "generate_s": gen_s,
-                           "tuning": eng.tuning()},
+                "config": workload_config(a.workload, n_genomes, k, B, seq.nbytes),
+                "parallelism": "replicas%d" % world,
+                "workload_detail": {"kmers_per_step": int(job_kmers), "bases": int(seq.nbytes),
+                                    "generate_s": gen_s, "tuning": eng.tuning()},
                 "counts": {"supers": int(r.n_supers), "records": int(r.n_records), "occ": int(r.n_occ),
                            "distinct": int(r.n_distinct), "fragments": int(r.n_fragments),
                            "color_sets": int(r.n_color_sets), "frag_bytes": int(r.frag_nbytes)},
                 "phase_ms": {"phase1": r.ms_phase1, "phase2": r.ms_phase2},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_host": e2e_host,
+                "gpu_launches": int(launches),
                 "autotune": tuned, "plain": plain,
                 "clocks": clocks,
                 "kernels_ms_per_step": {kname: round(v[0] / a.steps, 3) for kname, v in top}}

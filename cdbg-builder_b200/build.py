@@ -26,7 +26,8 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CUDA_INC = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(NVCC))), "include")
 CU_SOURCES = ["phase1.cu", "phase2.cu", "capi.cu"]
 HOST_SOURCES = ["io.cpp", "server.cpp"]
-REFERENCE = os.environ.get("CDBG_REFERENCE_DIR", "/root/reference")
+# the reference checkout sits beside this repository unless the variable says otherwise
+REFERENCE = os.environ.get("CDBG_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def _run(cmd, cwd=None):

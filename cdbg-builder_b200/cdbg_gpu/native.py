@@ -72,6 +72,13 @@ class BuildParams(ctypes.Structure):
                 ("outputs_to_host", ctypes.c_int32)]
 
 
+class BuildFilesArgs(ctypes.Structure):
+    _fields_ = [("files", ctypes.POINTER(ctypes.c_char_p)), ("num_files", ctypes.c_uint32),
+                ("k", ctypes.c_uint32), ("m", ctypes.c_uint32), ("num_buckets", ctypes.c_uint32),
+                ("host_threads", ctypes.c_uint32), ("batch_occ", ctypes.c_uint64),
+                ("frag_path", ctypes.c_char_p), ("color_sets_path", ctypes.c_char_p)]
+
+
 class BuildResult(ctypes.Structure):
     _fields_ = [("frag_bytes", ctypes.c_void_p), ("frag_nbytes", ctypes.c_uint64),
                 ("class_words", ctypes.c_void_p), ("class_bits", ctypes.c_uint64),
@@ -88,7 +95,8 @@ class BuildResult(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("batch_occ", ctypes.c_uint64), ("minimizer_tile", ctypes.c_uint32),
-                ("heavy_colors", ctypes.c_uint32), ("table_slots_q", ctypes.c_uint32)]
+                ("heavy_colors", ctypes.c_uint32), ("table_slots_q", ctypes.c_uint32),
+                ("union_lists", ctypes.c_uint32)]
 
 
 class ServerParams(ctypes.Structure):
@@ -144,10 +152,14 @@ SIGNATURES = {
     "cdbg_gpu_dump_supers": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                             ctypes.c_char_p, c_u64p]),
+    "cdbg_gpu_sort_pairs_u64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_uint64]),
     "cdbg_gpu_phase2": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Phase2Args),
                                        ctypes.POINTER(Phase2Stats)]),
     "cdbg_gpu_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
                                       ctypes.POINTER(BuildParams), ctypes.POINTER(BuildResult)]),
+    "cdbg_gpu_build_files": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BuildFilesArgs),
+                                            ctypes.POINTER(BuildResult)]),
     "cdbg_engine_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "cdbg_engine_memory": (ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p]),
     "cdbg_engine_trim": (ctypes.c_int, [ctypes.c_void_p]),
@@ -292,9 +304,9 @@ class Engine:
         _check(lib().cdbg_engine_memory(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
-    def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0, table_slots_q=0):
+    def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0, table_slots_q=0, union_lists=0):
         _check(lib().cdbg_engine_set_tuning(self._h, ctypes.byref(Tuning(batch_occ, minimizer_tile, heavy_colors,
-                                                                         table_slots_q))))
+                                                                         table_slots_q, union_lists))))
 
     def tuning(self):
         t = Tuning()
@@ -351,6 +363,10 @@ class Engine:
         keys = names.raw.split(b"\0")[:min(n, cap)]
         return {keys[i].decode(): b[i] for i in range(min(n, cap))}
 
+    def sort_pairs_u64(self, keys_ptr, vals_ptr, n):
+        """Stable in-place sort of n device (u64 key, u32 value) pairs by key."""
+        _check(lib().cdbg_gpu_sort_pairs_u64(self._h, keys_ptr, vals_ptr, n))
+
     def dump_supers(self, batch, k, m, num_buckets, path):
         n = ctypes.c_uint64()
         _check(lib().cdbg_gpu_dump_supers(self._h, ctypes.byref(batch), k, m, num_buckets,
@@ -386,6 +402,18 @@ class Engine:
         buf = ctypes.create_string_buffer(max(1, nbytes))
         _check(lib().cdbg_engine_copy_out(self._h, ctypes.c_void_p(device_ptr), buf, nbytes))
         return buf.raw[:nbytes]
+
+    def build_files(self, files, k, num_buckets, frag_path=None, color_sets_path=None, m=0, host_threads=0,
+                    batch_occ=0):
+        """cdbg_gpu_build_files: files in, frag_unitigs.bin / .color_sets out
+        (or, with no paths, outputs in host memory)."""
+        arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
+        a = BuildFilesArgs(arr, len(files), k, m, num_buckets, host_threads, batch_occ,
+                           frag_path.encode() if frag_path else None,
+                           color_sets_path.encode() if color_sets_path else None)
+        r = BuildResult()
+        _check(lib().cdbg_gpu_build_files(self._h, ctypes.byref(a), ctypes.byref(r)))
+        return r
 
     def build(self, batch, k, num_buckets, num_colors, m=0, batch_occ=0, outputs_to_host=True):
         p = BuildParams(k, m, num_buckets, num_colors, batch_occ, 1 if outputs_to_host else 0)

@@ -3,7 +3,11 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <map>
 #include <cstdio>
 #include <cstring>
@@ -18,6 +22,7 @@
 #include "engine.cuh"
 #include "phase1.cuh"
 #include "phase2.cuh"
+#include "primitives.cuh"
 
 namespace {
 
@@ -408,6 +413,24 @@ int cdbg_engine_kernel_stats(cdbg_engine* e, char* names, uint64_t names_cap, do
     return (int)e->prof.totals.size();
 }
 
+int cdbg_gpu_sort_pairs_u64(cdbg_engine* e, uint64_t* keys, uint32_t* vals, uint64_t n) {
+    if (!e) {
+        g_last_error = "null engine";
+        return -1;
+    }
+    call_scope scope_(e);
+    try {
+        CDBG_CUDA(cudaSetDevice(e->device));
+        e->A.reset();
+        cdbg::prim::sort_pairs_u64_exact<uint32_t>(keys, vals, n, e->A, e->st, e->d_err);
+        CDBG_CUDA(cudaStreamSynchronize(e->st));
+        cdbg::check_device_error(e, "sort");
+        return 0;
+    } catch (std::exception const& ex) {
+        return fail(ex);
+    }
+}
+
 int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, uint32_t m,
                          uint32_t num_buckets, const char* dump_path, uint64_t* n_supers) {
     if (!e) {
@@ -601,6 +624,7 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         pp.batch_occ = a->batch_occ ? a->batch_occ : e->tune.batch_occ;
         pp.heavy_colors = e->tune.heavy_colors;
         pp.table_slots_q = e->tune.table_slots_q;
+        pp.union_bitmaps = e->tune.union_lists == 0;
         pp.to_host = true;
         cdbg::phase2_result res;
         res.state = &e->p2;
@@ -743,9 +767,159 @@ void phase1_pipelined(cdbg_engine* e, cdbg_seq_batch const* b, uint32_t k, uint3
     if (h2d) *h2d += N + 8ull * (S + 1) + 4ull * S;
 }
 
-}  // namespace
+// Phase 1 of an in-memory build from files: the files are read (inflate +
+// parse, host threads) in groups into the engine's pinned input buffer on a
+// reader thread, while each group already read is uploaded (copy stream) and
+// runs through build_runs / find_supers; the groups' runs pack into one 2-bit
+// stream and their super-k-mer lists concatenate in file order, the order a
+// single pass produces.  The buffers are sized from the files' inflated-size
+// hints; returns false (nothing launched that matters) when a file inflates
+// to more than its hint says, and the caller reads the files whole instead.
+bool phase1_from_files(cdbg_engine* e, std::vector<std::string> const& files, uint32_t threads, uint32_t k,
+                       uint32_t m, uint32_t B, cdbg::run_table& rt_all, cdbg::super_list& sl_all, uint64_t* h2d,
+                       uint64_t* input_bytes) {
+    cudaStream_t st = e->st;
+    const size_t nf = files.size();
+    uint64_t N = 0;
+    for (auto const& f : files) N += cdbg::io::inflated_size_hint(f);
+    char* h_in = (char*)e->h_in.ensure(N + 64);
+    // groups of consecutive files: enough of them to overlap reading with
+    // the device work, few enough that each keeps the reader threads busy
+    const size_t ng = std::max<size_t>(1, std::min<size_t>(nf, std::min<uint64_t>(16, N / (32ull << 20) + 1)));
+    std::vector<size_t> gfirst(ng + 1);
+    for (size_t g = 0; g <= ng; ++g) gfirst[g] = nf * g / ng;
+    struct group {
+        cdbg::io::seq_batch meta;
+        uint64_t at = 0, nbytes = 0;
+        int state = 0;  // 0 pending, 1 ready, 2 too large, 3 failed
+        std::string err;
+    };
+    std::vector<group> G(ng);
+    std::mutex mu;
+    std::condition_variable cv;
+    std::atomic<bool> stop{false};
+    std::thread reader([&] {
+        uint64_t used = 0;
+        for (size_t g = 0; g < ng && !stop; ++g) {
+            int stt = 1;
+            std::string err;
+            uint64_t nb = 0;
+            try {
+                cdbg::io::seq_batch mb;
+                if (cdbg::io::read_files_into(files, gfirst[g], gfirst[g + 1] - gfirst[g], (uint32_t)gfirst[g],
+                                              threads, h_in + used, N - used, mb)) {
+                    nb = mb.off.back();
+                    G[g].meta = std::move(mb);
+                } else {
+                    stt = 2;
+                }
+            } catch (std::exception const& ex) {
+                stt = 3;
+                err = ex.what();
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                G[g].at = used;
+                G[g].nbytes = nb;
+                G[g].state = stt;
+                G[g].err = err;
+            }
+            cv.notify_all();
+            if (stt != 1) break;
+            used += nb;
+        }
+    });
+    struct join_on_exit {
+        std::thread& t;
+        std::atomic<bool>& s;
+        ~join_on_exit() {
+            s = true;
+            if (t.joinable()) t.join();
+        }
+    } joiner{reader, stop};
+    uint8_t* d_ascii = e->A.alloc<uint8_t>(N + 16);
+    const uint64_t cap = N / 32 + N / std::max<uint32_t>(k, 1) + 64 * ng + 64;
+    uint64_t* words = e->P.alloc<uint64_t>(cap);
+    uint64_t base = 0, n_kmers = 0, n_bases = 0, up = 0, inb = 0;
+    std::vector<cdbg::super_list> lists;
+    cudaEvent_t ev;
+    CDBG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (size_t g = 0; g < ng; ++g) {
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return G[g].state != 0; });
+        }
+        if (G[g].state == 3) {
+            cudaEventDestroy(ev);
+            throw std::runtime_error(G[g].err);
+        }
+        if (G[g].state == 2) {
+            cudaEventDestroy(ev);
+            return false;
+        }
+        auto const& mb = G[g].meta;
+        const uint32_t ns = (uint32_t)mb.color.size();
+        inb += mb.input_bytes;
+        if (ns == 0 || G[g].nbytes == 0) continue;
+        uint64_t* d_off = e->A.alloc<uint64_t>((uint64_t)ns + 1);
+        uint32_t* d_col = e->A.alloc<uint32_t>(ns);
+        CDBG_CUDA(cudaMemcpyAsync(d_off, mb.off.data(), 8ull * (ns + 1), cudaMemcpyHostToDevice, st));
+        CDBG_CUDA(cudaMemcpyAsync(d_col, mb.color.data(), 4ull * ns, cudaMemcpyHostToDevice, st));
+        CDBG_CUDA(cudaEventRecord(e->copy_ev, st));
+        CDBG_CUDA(cudaStreamWaitEvent(e->copy_st, e->copy_ev, 0));
+        CDBG_CUDA(cudaMemcpyAsync(d_ascii + G[g].at, h_in + G[g].at, G[g].nbytes, cudaMemcpyHostToDevice,
+                                  e->copy_st));
+        CDBG_CUDA(cudaEventRecord(ev, e->copy_st));
+        CDBG_CUDA(cudaStreamWaitEvent(st, ev, 0));
+        up += G[g].nbytes + 12ull * ns + 8;
+        cdbg::seq_input in;
+        in.ascii = d_ascii + G[g].at;
+        in.nbytes = G[g].nbytes;
+        in.seq_off = d_off;
+        in.seq_color = d_col;
+        in.num_seqs = ns;
+        cdbg::run_table rt;
+        cdbg::build_runs(in, k, e->A, st, rt, e->P, words, base, cap);
+        if (rt.n == 0) continue;
+        base = rt.nwords - 8;
+        n_kmers += rt.n_kmers;
+        n_bases += rt.n_bases;
+        cdbg::super_list sl;
+        cdbg::find_supers(rt, k, m, B, e->A, st, sl, e->d_err, e->tune.minimizer_tile, true);
+        if (sl.n) lists.push_back(sl);
+    }
+    cudaEventDestroy(ev);
+    uint64_t n = 0;
+    for (auto const& l : lists) n += l.n;
+    if (n >= 0xffffffffull) throw std::runtime_error("more than 2^32 super-k-mers in one call");
+    sl_all = cdbg::super_list();
+    sl_all.n = n;
+    sl_all.key = e->A.alloc<uint64_t>(n + 1);
+    sl_all.packed = e->A.alloc<uint4>(n + 1);
+    uint64_t o = 0;
+    for (auto const& l : lists) {
+        CDBG_CUDA(cudaMemcpyAsync(sl_all.key + o, l.key, 8 * l.n, cudaMemcpyDeviceToDevice, st));
+        CDBG_CUDA(cudaMemcpyAsync(sl_all.packed + o, l.packed, 16 * l.n, cudaMemcpyDeviceToDevice, st));
+        o += l.n;
+    }
+    rt_all = cdbg::run_table();
+    rt_all.words = words;
+    rt_all.nwords = base + 8;
+    rt_all.n_kmers = n_kmers;
+    rt_all.n_bases = n_bases;
+    if (h2d) *h2d += up;
+    if (input_bytes) *input_bytes = inb;
+    return true;
+}
 
-int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p, cdbg_build_result* r) {
+// Phase 1 of an in-memory build: fills rt / sl (records come after), adding
+// the bytes it uploads to *h2d; returns false to make the build start over
+// from a host batch (see phase1_from_files).
+using phase1_fn = std::function<bool(cdbg::run_table&, cdbg::super_list&, uint64_t*)>;
+
+// An in-memory build (phases 1 + 2 in HBM) with the given phase 1.
+int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phase1, cdbg_build_result* r,
+               bool* redo) {
     if (!e) {
         g_last_error = "null engine";
         return -1;
@@ -766,13 +940,14 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         CDBG_CUDA(cudaEventRecord(ev[0], e->st));
         cdbg::run_table rt;
         cdbg::super_list sl;
-        const bool packed = p->num_colors < (1u << 28);
-        if (!b->on_device && packed && b->num_seqs >= 8 && b->seq_bytes >= (64ull << 20)) {
-            phase1_pipelined(e, b, k, m, p->num_buckets, 4, rt, sl, &res.h2d_bytes);
-        } else {
-            cdbg::seq_input in = stage_batch(e, b, &res.h2d_bytes);
-            cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
-            cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile, packed);
+        if (!phase1(rt, sl, &res.h2d_bytes)) {
+            for (auto& x : ev) cudaEventDestroy(x);
+            CDBG_CUDA(cudaStreamSynchronize(e->st));
+            CDBG_CUDA(cudaStreamSynchronize(e->copy_st));
+            e->A.reset();
+            e->P.reset();
+            if (redo) *redo = true;
+            return 0;
         }
         cdbg::record_set rs;
         cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
@@ -788,6 +963,7 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
         pp.batch_occ = p->batch_occ ? p->batch_occ : e->tune.batch_occ;
         pp.heavy_colors = e->tune.heavy_colors;
         pp.table_slots_q = e->tune.table_slots_q;
+        pp.union_bitmaps = e->tune.union_lists == 0;
         pp.to_host = false;  // outputs accumulate in HBM
         if (p->outputs_to_host && e->h_frag.p && e->h_frag.cap) {
             // stream each batch's fragments into the (already large enough,
@@ -871,6 +1047,119 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
     }
 }
 
+}  // namespace
+
+int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p, cdbg_build_result* r) {
+    if (!e || !b || !p || !r) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    const uint32_t k = p->k;
+    const uint32_t m = p->m ? p->m : best_m(k);
+    auto ph1 = [&](cdbg::run_table& rt, cdbg::super_list& sl, uint64_t* h2d) {
+        const bool packed = p->num_colors < (1u << 28);
+        if (!b->on_device && packed && b->num_seqs >= 8 && b->seq_bytes >= (64ull << 20)) {
+            phase1_pipelined(e, b, k, m, p->num_buckets, 4, rt, sl, h2d);
+        } else {
+            cdbg::seq_input in = stage_batch(e, b, h2d);
+            cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
+            cdbg::find_supers(rt, k, m, p->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile, packed);
+        }
+        return true;
+    };
+    return build_core(e, p, ph1, r, nullptr);
+}
+
+int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_build_result* r) {
+    if (!e || !a || !r || (!a->files && a->num_files)) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    try {
+        if (a->num_files == 0) throw std::runtime_error("no input files");
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<std::string> files(a->files, a->files + a->num_files);
+        const uint32_t th = host_threads(a->host_threads);
+        cdbg_build_params p{};
+        p.k = a->k;
+        p.m = a->m;
+        p.num_buckets = a->num_buckets;
+        p.num_colors = a->num_files;
+        p.batch_occ = a->batch_occ;
+        p.outputs_to_host = a->frag_path || a->color_sets_path ? 0 : 1;
+        const uint32_t m = p.m ? p.m : best_m(p.k);
+        uint64_t inb = 0;
+        auto ph1 = [&](cdbg::run_table& rt, cdbg::super_list& sl, uint64_t* h2d) {
+            if (p.num_colors >= (1u << 28)) return false;
+            return phase1_from_files(e, files, th, p.k, m, p.num_buckets, rt, sl, h2d, &inb);
+        };
+        bool redo = false;
+        int rc = build_core(e, &p, ph1, r, &redo);
+        if (rc != 0) return rc;
+        if (redo) {
+            // a file inflated past its size hint: read everything, then build
+            cdbg::io::seq_batch hb;
+            cdbg::io::read_files(files, 0, files.size(), 0, th, hb);
+            inb = hb.input_bytes;
+            cdbg_seq_batch b{hb.seq.data(), hb.seq.size(), hb.off.data(), hb.color.data(),
+                             (uint32_t)hb.color.size(), 0};
+            rc = cdbg_gpu_build(e, &b, &p, r);
+            if (rc != 0) return rc;
+        }
+        if (!p.outputs_to_host) {
+            // outputs are in HBM: the frag bytes, color-set words and the
+            // Elias-Fano encoding of the class offsets (made on the device)
+            // come to pinned memory and go to the files
+            call_scope scope_(e);
+            CDBG_CUDA(cudaSetDevice(e->device));
+            cdbg::ef_encoded ef;
+            const uint64_t nwords = (r->class_bits + 63) / 64;
+            if (a->color_sets_path)
+                cdbg::ef_encode(r->class_offsets, r->n_color_sets, r->class_bits, e->A, e->st, ef);
+            uint8_t* hf = (uint8_t*)e->h_frag.ensure(r->frag_nbytes + 8);
+            uint64_t* hw = (uint64_t*)e->h_words.ensure(8 * nwords + 8);
+            uint64_t* hl = (uint64_t*)e->h_offsets.ensure(8 * (ef.low_words + ef.high_words) + 16);
+            if (r->frag_nbytes)
+                CDBG_CUDA(cudaMemcpyAsync(hf, r->frag_bytes, r->frag_nbytes, cudaMemcpyDeviceToHost, e->st));
+            if (a->color_sets_path) {
+                if (nwords)
+                    CDBG_CUDA(cudaMemcpyAsync(hw, r->class_words, 8 * nwords, cudaMemcpyDeviceToHost, e->st));
+                if (ef.low_words)
+                    CDBG_CUDA(cudaMemcpyAsync(hl, ef.low, 8 * ef.low_words, cudaMemcpyDeviceToHost, e->st));
+                if (ef.high_words)
+                    CDBG_CUDA(cudaMemcpyAsync(hl + ef.low_words, ef.high, 8 * ef.high_words,
+                                              cudaMemcpyDeviceToHost, e->st));
+            }
+            CDBG_CUDA(cudaStreamSynchronize(e->st));
+            r->d2h_bytes = r->frag_nbytes + (a->color_sets_path ? 8 * (nwords + ef.low_words + ef.high_words) : 0);
+            std::thread cs_writer;
+            std::exception_ptr cs_err;
+            if (a->color_sets_path)
+                cs_writer = std::thread([&] {
+                    try {
+                        cdbg::io::write_color_sets_ef(a->color_sets_path, a->num_files, hw, r->class_bits,
+                                                      ef.n, ef.l, hl, hl + ef.low_words, ef.high_bits);
+                    } catch (...) {
+                        cs_err = std::current_exception();
+                    }
+                });
+            if (a->frag_path) cdbg::io::write_file_parallel(a->frag_path, hf, r->frag_nbytes, th);
+            if (cs_writer.joinable()) cs_writer.join();
+            if (cs_err) std::rethrow_exception(cs_err);
+            r->frag_bytes = hf;
+            r->class_words = hw;
+            r->class_offsets = nullptr;  // in the file, Elias-Fano coded
+            e->A.reset();
+        }
+        (void)inb;
+        r->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return 0;
+    } catch (std::exception const& ex) {
+        if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
 int cdbg_engine_record_bytes(cdbg_engine* e, uint64_t* bytes) {
     if (!e || !bytes) {
         g_last_error = "null argument";
@@ -898,15 +1187,19 @@ int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
         return -1;
     }
     cdbg_tuning v = *t;
-    if (v.minimizer_tile == 0) v.minimizer_tile = 2048;
+    if (v.minimizer_tile == 0) v.minimizer_tile = 4096;
     if (v.heavy_colors == 0) v.heavy_colors = 64;
     if (v.table_slots_q == 0) v.table_slots_q = 8;
-    if (v.minimizer_tile != 1024 && v.minimizer_tile != 2048) {
-        g_last_error = "minimizer_tile must be 1024 or 2048";
+    if (v.minimizer_tile != 1024 && v.minimizer_tile != 2048 && v.minimizer_tile != 4096) {
+        g_last_error = "minimizer_tile must be 1024, 2048 or 4096";
         return -1;
     }
     if (v.table_slots_q < 5 || v.table_slots_q > 16) {
         g_last_error = "table_slots_q must be in [5, 16]";
+        return -1;
+    }
+    if (v.union_lists > 1) {
+        g_last_error = "union_lists must be 0 or 1";
         return -1;
     }
     e->tune = v;
@@ -945,7 +1238,7 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
             return v;
         };
         cdbg_tuning cur = e->tune;
-        if (cur.minimizer_tile == 0) cur.minimizer_tile = 2048;
+        if (cur.minimizer_tile == 0) cur.minimizer_tile = 4096;
         if (cur.heavy_colors == 0) cur.heavy_colors = 64;
         if (cur.table_slots_q == 0) cur.table_slots_q = 8;
         measure(cur);  // warm-up: allocations reach their working sizes
@@ -962,7 +1255,7 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
             t.batch_occ = v;
             if (t.batch_occ != cur.batch_occ) consider(t);
         }
-        for (uint32_t v : {1024u, 2048u}) {
+        for (uint32_t v : {2048u, 4096u}) {
             cdbg_tuning t = cur;
             t.minimizer_tile = v;
             if (t.minimizer_tile != cur.minimizer_tile) consider(t);

@@ -226,11 +226,32 @@ __device__ __forceinline__ bool tma_load_1d(void* smem_dst, void const* gsrc, ui
     return ok != 0;
 }
 
+// Shared memory of one minimizer tile of TT (k-1)-mers: the staged 2-bit
+// words, the m-mer hashes (padded one slot per 32 so that threads hashing
+// consecutive chunks store to different banks) and the per-position minima.
+template <int TT>
+struct mz_layout {
+    static constexpr int WMAX = (TT + 256) / 32 + 4;       // 2-bit words staged
+    static constexpr int HMAX = TT + 1 + 64;               // m-mer hashes (W <= 62)
+    static constexpr int HPAD = HMAX + HMAX / 32 + 1;
+    static constexpr size_t bytes = sizeof(uint64_t) * (WMAX + HPAD + TT + 1);
+};
+__device__ __forceinline__ uint32_t mz_pad(uint32_t q) { return q + (q >> 5); }
+
+// 32 bases starting at stream offset x of the staged words (base x in the
+// low two bits).
+__device__ __forceinline__ uint64_t mz_window(uint64_t const* sw, uint32_t x) {
+    const uint64_t lo = sw[x >> 5], hi = sw[(x >> 5) + 1];
+    const uint32_t s = 2 * (x & 31);
+    return s ? (lo >> s) | (hi << (64 - s)) : lo;
+}
+
 // MODE 0: count the cuts of each tile (tile_count).  MODE 1: write them at
 // tile_off.  MODE 2: one pass -- tiles take indices in launch order from
 // tile_counter, publish their count in `status` and read their predecessors'
 // prefix (decoupled look-back, bounded waits), then write at most `cap`
 // entries; the grand total ends in the last tile's status.
+// Dynamic shared memory: mz_layout<TT>::bytes.
 template <int MODE, int TT = MZ_TT>
 __global__ void __launch_bounds__(MZ_THREADS)
     k_minimizers(uint32_t nruns, uint64_t const* __restrict__ tile_start,
@@ -240,13 +261,17 @@ __global__ void __launch_bounds__(MZ_THREADS)
                  uint64_t* __restrict__ out_min, uint32_t* __restrict__ out_run,
                  uint32_t* __restrict__ out_a, uint32_t* err, uint32_t* tile_counter = nullptr,
                  unsigned long long* status = nullptr, uint64_t ntiles = 0, uint64_t cap = 0) {
-    constexpr int MZ_PER = TT / MZ_THREADS;       // (k-1)-mers per thread
-    constexpr int MZ_HMAX = TT + 1 + 64;          // m-mer hashes (W <= 62)
-    constexpr int MZ_WMAX = (TT + 256) / 32 + 4;  // 2-bit words staged
-    __shared__ __align__(16) uint64_t sw[MZ_WMAX];
-    __shared__ uint64_t sh[MZ_HMAX];
-    __shared__ uint64_t smin[TT + 1];
+    using LY = mz_layout<TT>;
+    constexpr int MZ_PER = TT / MZ_THREADS;  // (k-1)-mers per thread
+    // m-mers hashed per thread: one chunk each covers the tile and its halo
+    constexpr int HC = (LY::HMAX + MZ_THREADS - 1) / MZ_THREADS;
+    static_assert(HC <= 32, "a hashing chunk must fit one 32-base window");
+    extern __shared__ __align__(16) uint64_t mz_dyn[];
+    uint64_t* sw = mz_dyn;                   // staged words (16-byte aligned for the bulk copy)
+    uint64_t* sh = mz_dyn + LY::WMAX;        // hashes, then prefix minima (padded index)
+    uint64_t* smin = sh + LY::HPAD;          // suffix minima, then window minima
     __shared__ uint64_t stab[4][4];  // rotated ntHash seeds, by base
+    __shared__ uint64_t tf[16], tr[16];  // rolling terms by (out base, in base)
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint64_t s_tile, s_excl;
 
@@ -256,6 +281,11 @@ __global__ void __launch_bounds__(MZ_THREADS)
         const uint32_t b = threadIdx.x & 3, j = threadIdx.x >> 2;
         const uint64_t sb = nt_seed(b), sc = nt_seed(b ^ 3u);
         stab[j][b] = j == 0 ? sb : j == 1 ? rol64(sb, m) : j == 2 ? ror64(sc, 1) : rol64(sc, m - 1);
+    } else if (threadIdx.x < 32) {
+        // one rolling step of base `o` leaving and base `i` entering, both strands
+        const uint32_t o = (threadIdx.x - 16) >> 2, i = threadIdx.x & 3;
+        tf[(o << 2) | i] = rol64(nt_seed(o), m) ^ nt_seed(i);
+        tr[(o << 2) | i] = ror64(nt_seed(o ^ 3u), 1) ^ rol64(nt_seed(i ^ 3u), m - 1);
     }
     uint64_t tile = blockIdx.x;
     if (MODE == 2) {
@@ -289,27 +319,32 @@ __global__ void __launch_bounds__(MZ_THREADS)
         return;
     }
     const uint32_t rel0 = (uint32_t)(pa - wa * 32);  // stream offset of base e0 in sw
-    auto base_at = [&](uint32_t q) -> uint32_t {     // q relative to e0
-        const uint32_t x = rel0 + q;
-        return (uint32_t)(sw[x >> 5] >> (2 * (x & 31))) & 3u;
-    };
-    // canonical m-mer hashes h[0..nh) (h[q] = m-mer at base e0 + q)
-    const uint32_t per_h = (nh + MZ_THREADS - 1) / MZ_THREADS;
+    // canonical m-mer hashes h[0..nh) (h[q] = m-mer at base e0 + q): thread c
+    // hashes the HC m-mers from c * HC on, the first in Horner form
+    // (fwd = xor_i rol(seed(b_i), m-1-i), rc = xor_i rol(seed(b_i ^ 3), i)),
+    // the others rolled with one (out, in) table entry per strand.  Its bases
+    // sit in two 32-base register windows, so every extraction in the unrolled
+    // loop is a constant shift.
     {
-        const uint32_t q0 = threadIdx.x * per_h;
-        const uint32_t q1 = min(q0 + per_h, nh);
-        if (q0 < q1) {
-            // first m-mer in Horner form: fwd = xor_i rol(seed(b_i), m-1-i),
-            // rc = xor_i rol(seed(b_i ^ 3), i)
+        const uint32_t q0 = threadIdx.x * HC;
+        if (q0 < nh) {
+            const uint32_t cnt = min((uint32_t)HC, nh - q0);
+            const uint32_t x0 = rel0 + q0;
+            const uint64_t wout = mz_window(sw, x0);          // bases q0 .. q0 + 31
+            const uint64_t win = mz_window(sw, x0 + m - 1);   // bases q0 + m - 1 .. + 31
             uint64_t f = 0, rc = 0;
-            for (uint32_t i = 0; i < m; ++i) f = rol64(f, 1) ^ stab[0][base_at(q0 + i)];
-            for (uint32_t i = m; i-- > 0;) rc = rol64(rc, 1) ^ stab[0][base_at(q0 + i) ^ 3u];
-            sh[q0] = f <= rc ? f : rc;
-            for (uint32_t q = q0 + 1; q < q1; ++q) {
-                const uint32_t out = base_at(q - 1), in = base_at(q + m - 1);
-                f = rol64(f, 1) ^ stab[1][out] ^ stab[0][in];
-                rc = ror64(rc, 1) ^ stab[2][out] ^ stab[3][in];
-                sh[q] = f <= rc ? f : rc;
+            for (uint32_t i = 0; i < m; ++i) f = rol64(f, 1) ^ stab[0][(uint32_t)(wout >> (2 * i)) & 3u];
+            for (uint32_t i = m; i-- > 0;) rc = rol64(rc, 1) ^ stab[0][((uint32_t)(wout >> (2 * i)) & 3u) ^ 3u];
+            sh[mz_pad(q0)] = f <= rc ? f : rc;
+#pragma unroll
+            for (int j = 1; j < HC; ++j) {
+                if ((uint32_t)j < cnt) {
+                    const uint32_t pr = (((uint32_t)(wout >> (2 * (j - 1))) & 3u) << 2) |
+                                        ((uint32_t)(win >> (2 * j)) & 3u);
+                    f = rol64(f, 1) ^ tf[pr];
+                    rc = ror64(rc, 1) ^ tr[pr];
+                    sh[mz_pad(q0 + j)] = f <= rc ? f : rc;
+                }
             }
         }
     }
@@ -326,21 +361,21 @@ __global__ void __launch_bounds__(MZ_THREADS)
             const uint32_t a = g * W, e = min(a + W, nh);
             uint64_t run = ~0ull;
             for (uint32_t q = e; q-- > a;) {
-                const uint64_t v = sh[q];
+                const uint64_t v = sh[mz_pad(q)];
                 run = v < run ? v : run;
                 if (q < nmin) smin[q] = run;
             }
             run = ~0ull;
             for (uint32_t q = a; q < e; ++q) {
-                const uint64_t v = sh[q];
+                const uint64_t v = sh[mz_pad(q)];
                 run = v < run ? v : run;
-                sh[q] = run;
+                sh[mz_pad(q)] = run;
             }
         }
     }
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < nmin; q += MZ_THREADS) {
-        const uint64_t a = smin[q], b = sh[q + W - 1];
+        const uint64_t a = smin[q], b = sh[mz_pad(q + W - 1)];
         smin[q] = a < b ? a : b;
     }
     __syncthreads();
@@ -426,6 +461,16 @@ __global__ void __launch_bounds__(MZ_THREADS)
             out_a[o] = (uint32_t)(j0 + c);
         }
     }
+}
+
+// Dynamic shared memory of a k_minimizers<MODE, TT> launch (opting in above
+// the 48 KB default where the tile needs it).
+template <int MODE, int TT>
+size_t mz_smem() {
+    constexpr size_t b = mz_layout<TT>::bytes;
+    if (b > 48 * 1024)
+        CDBG_CUDA(cudaFuncSetAttribute(k_minimizers<MODE, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b));
+    return b;
 }
 
 __global__ void k_run_tiles(uint32_t nruns, uint32_t const* __restrict__ len, uint32_t k, uint32_t tt,
@@ -877,10 +922,12 @@ void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_ar
                  cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile, bool packed) {
     if (tile == 1024)
         find_supers_tt<1024>(rt, k, m, B, A, st, out, d_err, packed);
-    else if (tile == 2048 || tile == 0)
+    else if (tile == 2048)
         find_supers_tt<2048>(rt, k, m, B, A, st, out, d_err, packed);
+    else if (tile == 4096 || tile == 0)
+        find_supers_tt<4096>(rt, k, m, B, A, st, out, d_err, packed);
     else
-        throw std::runtime_error("minimizer tile must be 1024 or 2048");
+        throw std::runtime_error("minimizer tile must be 1024, 2048 or 4096");
 }
 
 template <int TT>
@@ -909,7 +956,7 @@ void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev
     CDBG_CUDA(cudaMemsetAsync(counter, 0, 4, st));
     {
         CDBG_PROF("k_minimizers", st);
-        k_minimizers<2, TT><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(rt.n, tstart, rt.soff, rt.len, rt.words, k, m,
+        k_minimizers<2, TT><<<(unsigned)ntiles, MZ_THREADS, mz_smem<2, TT>(), st>>>(rt.n, tstart, rt.soff, rt.len, rt.words, k, m,
                                                                  nullptr, nullptr, minv, run, aa, d_err, counter,
                                                                  status, ntiles, cap);
     }
@@ -920,7 +967,7 @@ void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev
         uint64_t* toff = A.alloc<uint64_t>(ntiles + 1);
         {
             CDBG_PROF("k_minimizers", st);
-            k_minimizers<0, TT><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+            k_minimizers<0, TT><<<(unsigned)ntiles, MZ_THREADS, mz_smem<0, TT>(), st>>>(
                 rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, nullptr, nullptr, nullptr, nullptr, d_err);
         }
         CDBG_CHECK_LAUNCH();
@@ -931,7 +978,7 @@ void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev
         aa = A.alloc<uint32_t>(n);
         {
             CDBG_PROF("k_minimizers", st);
-            k_minimizers<1, TT><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(
+            k_minimizers<1, TT><<<(unsigned)ntiles, MZ_THREADS, mz_smem<1, TT>(), st>>>(
                 rt.n, tstart, rt.soff, rt.len, rt.words, k, m, tcount, toff, minv, run, aa, d_err);
         }
         CDBG_CHECK_LAUNCH();
@@ -983,7 +1030,7 @@ void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, 
     // sort a copy of the keys (the super list keeps its input order)
     uint64_t* skey = A.alloc<uint64_t>(n);
     CDBG_CUDA(cudaMemcpyAsync(skey, sl.key, n * 8, cudaMemcpyDeviceToDevice, st));
-    prim::radix_sort_pairs<uint32_t>(skey, idx, n, 0, 64, A, st);
+    prim::sort_pairs_u64_exact<uint32_t>(skey, idx, n, A, st, d_err);
     uint64_t* p_start = A.alloc<uint64_t>(n);
     uint32_t* p_len = A.alloc<uint32_t>(n);
     uint32_t* p_color = A.alloc<uint32_t>(n);
@@ -1193,6 +1240,22 @@ struct noalloc_scratch {
 // cudaGetSymbolAddress (noalloc_scratch_ptr below).
 static __device__ __align__(256) noalloc_scratch g_noalloc_scratch;
 
+// Tiles per run like k_run_tiles, for caller-supplied runs: a run shorter
+// than k has no k-mer and would make the tile arithmetic wrap, so it counts
+// zero tiles and sets `err` (the host reads it before any tile kernel runs).
+__global__ void k_noalloc_run_tiles(uint32_t nruns, uint32_t const* __restrict__ len, uint32_t k, uint32_t tt,
+                                    uint64_t* __restrict__ ntiles, uint32_t* err) {
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nruns) return;
+    const uint32_t L = len[r];
+    if (L < k) {
+        set_error(err, ERR_BAD_RECORD);
+        ntiles[r] = 0;
+        return;
+    }
+    ntiles[r] = ((uint64_t)L - k + 2 + tt - 1) / tt;
+}
+
 // Exclusive scan of n <= NOALLOC_MAX_TILES values by one block; the total goes
 // to out[n].
 template <typename T>
@@ -1211,7 +1274,8 @@ noalloc_scratch* g_noalloc_ptr[256] = {};
 
 // Device address of the scratch on the current device, looked up once per
 // device (the first call on a device does this; make that first call before
-// any stream capture).
+// any stream capture).  The address stays cached for the life of the process,
+// so it is stale after the caller resets the device (cudaDeviceReset).
 noalloc_scratch* noalloc_scratch_ptr() {
     int dev = 0;
     CDBG_CUDA(cudaGetDevice(&dev));
@@ -1245,34 +1309,55 @@ extern "C" int cdbg_gpu_supers_noalloc(const uint64_t* words, const uint64_t* ru
         if (num_buckets == 0) throw std::runtime_error("num_buckets must be > 0");
         if (num_runs > NOALLOC_MAX_TILES)
             throw std::runtime_error("more than 512 runs in one call (each run needs at least one tile)");
+        // the tile kernel stages words from `words` with bulk copies, which
+        // need 16-byte aligned global addresses
+        if (reinterpret_cast<uintptr_t>(words) & 15u)
+            throw std::runtime_error("words must be 16-byte aligned");
         cudaStream_t st = (cudaStream_t)stream;
         noalloc_scratch* s = noalloc_scratch_ptr();
         CDBG_CUDA(cudaMemsetAsync(&s->err, 0, sizeof(uint32_t), st));
         if (num_runs == 0) return 0;
-        k_run_tiles<<<grid(num_runs, 256), 256, 0, st>>>(num_runs, run_len, k, MZ_TT, s->run_tiles);
+        k_noalloc_run_tiles<<<grid(num_runs, 256), 256, 0, st>>>(num_runs, run_len, k, MZ_TT, s->run_tiles,
+                                                                 &s->err);
         CDBG_CHECK_LAUNCH();
         k_noalloc_scan<uint64_t><<<1, 1024, 0, st>>>(s->run_tiles, num_runs, s->tile_start);
         CDBG_CHECK_LAUNCH();
-        uint64_t ntiles = 0;
-        CDBG_CUDA(cudaMemcpyAsync(&ntiles, &s->tile_start[num_runs], 8, cudaMemcpyDeviceToHost, st));
+        struct {
+            uint64_t v;
+            uint32_t err;
+        } rb{0, 0};
+        CDBG_CUDA(cudaMemcpyAsync(&rb.v, &s->tile_start[num_runs], 8, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaMemcpyAsync(&rb.err, &s->err, 4, cudaMemcpyDeviceToHost, st));
         CDBG_CUDA(cudaStreamSynchronize(st));
+        if (rb.err) throw std::runtime_error("a run is shorter than k bases");
+        const uint64_t ntiles = rb.v;
         if (ntiles > NOALLOC_MAX_TILES)
             throw std::runtime_error("input needs " + std::to_string(ntiles) +
                                      " tiles; at most 512 tiles of 2048 (k-1)-mers per call");
-        k_minimizers<false><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(num_runs, s->tile_start, run_soff, run_len,
-                                                                     words, k, m, s->tile_count, nullptr, nullptr,
-                                                                     nullptr, nullptr, &s->err);
+        // a tile that gives up (bounded staging wait) writes no count: start
+        // from zero rather than the previous call's counts
+        CDBG_CUDA(cudaMemsetAsync(s->tile_count, 0, sizeof(uint32_t) * ntiles, st));
+        k_minimizers<0><<<(unsigned)ntiles, MZ_THREADS, mz_smem<0, MZ_TT>(), st>>>(num_runs, s->tile_start, run_soff, run_len,
+                                                                 words, k, m, s->tile_count, nullptr, nullptr,
+                                                                 nullptr, nullptr, &s->err);
         CDBG_CHECK_LAUNCH();
         k_noalloc_scan<uint32_t><<<1, 1024, 0, st>>>(s->tile_count, (uint32_t)ntiles, s->tile_off);
         CDBG_CHECK_LAUNCH();
-        uint64_t n = 0;
-        CDBG_CUDA(cudaMemcpyAsync(&n, &s->tile_off[ntiles], 8, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaMemcpyAsync(&rb.v, &s->tile_off[ntiles], 8, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaMemcpyAsync(&rb.err, &s->err, 4, cudaMemcpyDeviceToHost, st));
         CDBG_CUDA(cudaStreamSynchronize(st));
+        if (rb.err) throw std::runtime_error("device error " + std::to_string(rb.err) + " in super-k-mer count");
+        const uint64_t n = rb.v;
         if (n > out_cap) throw std::runtime_error("output capacity too small: need " + std::to_string(n));
-        k_minimizers<true><<<(unsigned)ntiles, MZ_THREADS, 0, st>>>(num_runs, s->tile_start, run_soff, run_len,
-                                                                    words, k, m, s->tile_count, s->tile_off,
-                                                                    s->minv, s->run, s->a, &s->err);
+        k_minimizers<1><<<(unsigned)ntiles, MZ_THREADS, mz_smem<1, MZ_TT>(), st>>>(num_runs, s->tile_start, run_soff, run_len,
+                                                                 words, k, m, s->tile_count, s->tile_off,
+                                                                 s->minv, s->run, s->a, &s->err);
         CDBG_CHECK_LAUNCH();
+        // a tile that gave up wrote none of its cuts, and the scratch still
+        // holds the previous call's entries there: stop before they are used
+        CDBG_CUDA(cudaMemcpyAsync(&rb.err, &s->err, 4, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        if (rb.err) throw std::runtime_error("device error " + std::to_string(rb.err) + " in super-k-mer cuts");
         uint32_t bb = 0;
         while ((1ull << bb) < num_buckets) ++bb;
         if (n) {

@@ -2294,7 +2294,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     if (npairs) {
         // stable by node (records already ascend within a node): the node bits only
         const int node_bits = D > 1 ? 64 - __builtin_clzll(D - 1) : 1;
-        prim::radix_sort_pairs<uint32_t, uint32_t>(pnode, prec, npairs, 0, node_bits, A, st);
+        prim::radix_sort_pairs<uint32_t, uint32_t>(pnode, prec, npairs, 0, node_bits, A, st, d_err);
         uint32_t* keep = A.alloc<uint32_t>(npairs);
         uint64_t* kpos = A.alloc<uint64_t>(npairs + 1);
         k_unique_pairs<<<grid(npairs, 256), 256, 0, st>>>(npairs, pnode, prec, keep);
@@ -2436,7 +2436,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         CDBG_CUDA(cudaMemcpyAsync(skey, cv.hash, 8 * nc, cudaMemcpyDeviceToDevice, st));
         k_iota32<<<grid(nc, 256), 256, 0, st>>>(nc, sidx);
         CDBG_CHECK_LAUNCH();
-        prim::radix_sort_pairs<uint32_t>(skey, sidx, nc, 0, 64, A, st);
+        prim::sort_pairs_u64_exact<uint32_t>(skey, sidx, nc, A, st, d_err);
         uint32_t* head = A.alloc<uint32_t>(nc);
         uint64_t* hpos = A.alloc<uint64_t>(nc + 1);
         k_run_heads<<<grid(nc, 256), 256, 0, st>>>(nc, skey, head);
@@ -2524,7 +2524,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             uint32_t* rcand = A.alloc<uint32_t>(nnew);
             k_new_reps<<<grid(nr, 256), 256, 0, st>>>(nr, rcid, npos, rv, rkey, rcand);
             CDBG_CHECK_LAUNCH();
-            prim::radix_sort_pairs<uint32_t>(rkey, rcand, nnew, 0, 32, A, st);
+            prim::radix_sort_pairs<uint32_t>(rkey, rcand, nnew, 0, 32, A, st, d_err);
             const uint64_t base = dict.n;
             k_assign_new<<<grid(nnew, 256), 256, 0, st>>>(nnew, rcand, base, rcid);
             CDBG_CHECK_LAUNCH();
@@ -2814,14 +2814,57 @@ void run_phase2(record_set const& rs, phase2_params const& p, dev_arena& A, cuda
     if (p.num_colors == 0) throw std::runtime_error("num_colors must be > 0");
     if (rs.n >= (1ull << 31)) throw std::runtime_error("more than 2^31 bucket records in one build");
     phase2_params q = p;
-    // bitmaps cost C/8 bytes per multi-record k-mer: lists above 8192 colors;
-    // CDBG_UNION_LISTS=1 forces the list path (tests cover both)
-    char const* env = std::getenv("CDBG_UNION_LISTS");
-    if (q.num_colors > 8192 || (env && env[0] == '1')) q.union_bitmaps = false;
+    // bitmaps cost C/8 bytes per multi-record k-mer: lists above 8192 colors
+    if (q.num_colors > 8192) q.union_bitmaps = false;
     if (q.k <= 31)
         run_all<uint64_t>(rs, q, A, st, d_err, out);
     else
         run_all<u128>(rs, q, A, st, d_err, out);
+}
+
+namespace {
+// One value per thread: its l low bits OR-ed into the low vector (a value
+// spans at most two words) and its bit in the high vector.
+__global__ void k_ef_encode(uint64_t const* __restrict__ offsets, uint64_t nclasses, uint64_t total, uint64_t l,
+                            unsigned long long* __restrict__ low, unsigned long long* __restrict__ high) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > nclasses) return;
+    const uint64_t v = i < nclasses ? offsets[i] : total;
+    if (l) {
+        const uint64_t pos = i * l, lo = v & ((uint64_t(1) << l) - 1);
+        atomicOr(&low[pos >> 6], (unsigned long long)(lo << (pos & 63)));
+        if ((pos & 63) + l > 64) atomicOr(&low[(pos >> 6) + 1], (unsigned long long)(lo >> (64 - (pos & 63))));
+    }
+    const uint64_t hp = (v >> l) + i;
+    atomicOr(&high[hp >> 6], 1ull << (hp & 63));
+}
+}  // namespace
+
+void ef_encode(uint64_t const* d_offsets, uint64_t nclasses, uint64_t total_bits, dev_arena& A, cudaStream_t st,
+               ef_encoded& out) {
+    out = ef_encoded();
+    const uint64_t n = nclasses + 1, U = total_bits;
+    uint64_t l = 0;
+    if (U > n) {
+        const uint64_t q = U / n;
+        while ((uint64_t(1) << (l + 1)) <= q) ++l;
+    }
+    out.n = n;
+    out.l = l;
+    out.high_bits = n + (U >> l) + 1;
+    out.low_words = (n * l + 63) / 64;
+    out.high_words = (out.high_bits + 63) / 64;
+    out.low = A.alloc<uint64_t>(out.low_words + 1);
+    out.high = A.alloc<uint64_t>(out.high_words + 1);
+    CDBG_CUDA(cudaMemsetAsync(out.low, 0, 8 * (out.low_words + 1), st));
+    CDBG_CUDA(cudaMemsetAsync(out.high, 0, 8 * (out.high_words + 1), st));
+    {
+        CDBG_PROF("k_ef_encode", st);
+        k_ef_encode<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_offsets, nclasses, U, l,
+                                                                  (unsigned long long*)out.low,
+                                                                  (unsigned long long*)out.high);
+    }
+    CDBG_CHECK_LAUNCH();
 }
 
 }  // namespace cdbg

@@ -97,6 +97,19 @@ struct phase2_params {
     cudaEvent_t copy_ev = nullptr;
 };
 
+// Elias-Fano encoding of the class bit offsets plus the total bit count, the
+// finalize step of the .color_sets file (streaming_color_set_dict.hpp:221-294):
+// n = nclasses + 1 values, l low bits each (l = floor(log2(U / n)) when
+// U > n, else 0), value i sets bit (v >> l) + i of the high vector.  Device
+// arrays from the arena.
+struct ef_encoded {
+    uint64_t n = 0, l = 0, high_bits = 0, low_words = 0, high_words = 0;
+    uint64_t* low = nullptr;
+    uint64_t* high = nullptr;
+};
+void ef_encode(uint64_t const* d_offsets, uint64_t nclasses, uint64_t total_bits, dev_arena& A, cudaStream_t st,
+               ef_encoded& out);
+
 // Run phase 2 over all buckets of `rs` (records grouped by bucket).
 void run_phase2(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStream_t st,
                 uint32_t* d_err, phase2_result& out);

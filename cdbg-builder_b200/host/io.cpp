@@ -4,6 +4,7 @@
 
 #include <zlib.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cerrno>
 #include <cstdio>
@@ -155,6 +156,82 @@ void read_files(std::vector<std::string> const& files, size_t first, size_t coun
         }
         out.input_bytes += pf[i].disk;
     }
+}
+
+uint64_t inflated_size_hint(std::string const& path) {
+    std::error_code ec;
+    const uint64_t sz = std::filesystem::file_size(path, ec);
+    if (ec) throw std::runtime_error("could not open input file: " + path);
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("could not open input file: " + path);
+    unsigned char head[2] = {0, 0}, tail[4] = {0, 0, 0, 0};
+    const bool gz = std::fread(head, 1, 2, f) == 2 && head[0] == 0x1f && head[1] == 0x8b;
+    uint64_t v = sz;
+    if (gz && sz >= 18 && std::fseek(f, -4, SEEK_END) == 0 && std::fread(tail, 1, 4, f) == 4) {
+        const uint64_t isize = (uint64_t)tail[0] | ((uint64_t)tail[1] << 8) | ((uint64_t)tail[2] << 16) |
+                               ((uint64_t)tail[3] << 24);
+        // the size field is mod 2^32: take the largest size congruent to it
+        // that deflate's maximum ratio (1032:1) allows
+        const uint64_t lim = sz * 1032;
+        v = isize;
+        while (v + (uint64_t(1) << 32) <= lim) v += uint64_t(1) << 32;
+    }
+    std::fclose(f);
+    return v;
+}
+
+bool read_files_into(std::vector<std::string> const& files, size_t first, size_t count, uint32_t color_base,
+                     uint32_t threads, char* dst, uint64_t cap, seq_batch& out) {
+    struct per_file {
+        std::string seq;
+        std::vector<uint64_t> lens;
+        uint64_t disk = 0;
+    };
+    std::vector<per_file> pf(count);
+    parallel_for(count, threads, [&](size_t i) {
+        std::string const& path = files[first + i];
+        std::error_code ec;
+        auto sz = std::filesystem::file_size(path, ec);
+        pf[i].disk = ec ? 0 : (uint64_t)sz;
+        std::string raw = slurp(path);
+        pf[i].seq.reserve(raw.size());
+        parse_fastx(raw.data(), raw.size(), [&](char const* s, size_t l) {
+            pf[i].seq.append(s, l);
+            pf[i].lens.push_back(l);
+        });
+    });
+    std::vector<uint64_t> at(count + 1, 0);
+    for (size_t i = 0; i < count; ++i) at[i + 1] = at[i] + pf[i].seq.size();
+    if (at[count] > cap) return false;
+    parallel_for(count, threads, [&](size_t i) {
+        if (!pf[i].seq.empty()) std::memcpy(dst + at[i], pf[i].seq.data(), pf[i].seq.size());
+    });
+    for (size_t i = 0; i < count; ++i) {
+        for (uint64_t l : pf[i].lens) {
+            out.off.push_back(out.off.back() + l);
+            out.color.push_back(color_base + (uint32_t)i);
+        }
+        out.input_bytes += pf[i].disk;
+    }
+    return true;
+}
+
+void write_file_parallel(std::string const& path, uint8_t const* data, uint64_t n, uint32_t threads) {
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot open output file: " + path + ": " + std::strerror(errno));
+    std::fclose(f);
+    if (n == 0) return;
+    std::filesystem::resize_file(path, n);
+    const uint64_t piece = std::max<uint64_t>(64ull << 20, (n + threads - 1) / std::max<uint32_t>(threads, 1));
+    const size_t np = (size_t)((n + piece - 1) / piece);
+    parallel_for(np, threads, [&](size_t i) {
+        std::FILE* g = std::fopen(path.c_str(), "r+b");
+        if (!g) throw std::runtime_error("cannot open output file: " + path);
+        const uint64_t a = i * piece, b = std::min<uint64_t>(n, a + piece);
+        bool ok = std::fseek(g, (long)a, SEEK_SET) == 0 && std::fwrite(data + a, 1, b - a, g) == b - a;
+        ok = (std::fclose(g) == 0) && ok;
+        if (!ok) throw std::runtime_error("short write to " + path);
+    });
 }
 
 // ---------------------------------------------------------------- buckets
@@ -334,6 +411,27 @@ void write_color_sets(std::string const& path, uint32_t C, uint64_t const* words
     ok = ok && std::fwrite(&U, 8, 1, f) == 1 && std::fwrite(&n, 8, 1, f) == 1 && std::fwrite(&l, 8, 1, f) == 1;
     wbv(low, n * l);
     wbv(high, hbits);
+    std::fclose(f);
+    if (!ok) throw std::runtime_error("short write to " + path);
+}
+
+void write_color_sets_ef(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
+                         uint64_t nvalues, uint64_t l, uint64_t const* low, uint64_t const* high,
+                         uint64_t high_bits) {
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot open color-set output: " + path);
+    const uint32_t st = (uint32_t)(0.25 * C), dt = (uint32_t)(0.75 * C);
+    const uint64_t nwords = (nbits + 63) / 64;
+    bool ok = std::fwrite(&C, 4, 1, f) == 1 && std::fwrite(&st, 4, 1, f) == 1 &&
+              std::fwrite(&dt, 4, 1, f) == 1 && std::fwrite(&nbits, 8, 1, f) == 1 &&
+              std::fwrite(&nwords, 8, 1, f) == 1;
+    if (ok && nwords) ok = std::fwrite(words, 8, nwords, f) == nwords;
+    const uint64_t U = nbits, lbits = nvalues * l, lw = (lbits + 63) / 64, hw = (high_bits + 63) / 64;
+    ok = ok && std::fwrite(&U, 8, 1, f) == 1 && std::fwrite(&nvalues, 8, 1, f) == 1 && std::fwrite(&l, 8, 1, f) == 1;
+    ok = ok && std::fwrite(&lbits, 8, 1, f) == 1 && std::fwrite(&lw, 8, 1, f) == 1;
+    if (ok && lw) ok = std::fwrite(low, 8, lw, f) == lw;
+    ok = ok && std::fwrite(&high_bits, 8, 1, f) == 1 && std::fwrite(&hw, 8, 1, f) == 1;
+    if (ok && hw) ok = std::fwrite(high, 8, hw, f) == hw;
     std::fclose(f);
     if (!ok) throw std::runtime_error("short write to " + path);
 }

@@ -34,6 +34,22 @@ std::string slurp(std::string const& path);
 void read_files(std::vector<std::string> const& files, size_t first, size_t count,
                 uint32_t color_base, uint32_t threads, seq_batch& out);
 
+// Upper bound of the bytes inflating `path` yields: the gzip trailer's size
+// field for a gzip file (exact for a single-member file under 4 GiB), the
+// file size for a plain one.  A multi-member gzip file can exceed it; callers
+// that size buffers from it check what they read.
+uint64_t inflated_size_hint(std::string const& path);
+
+// read_files with the sequence bytes written to dst[0 .. cap) (out.seq stays
+// empty; out.off / out.color / out.input_bytes as read_files).  Returns false,
+// with nothing written past cap, when the sequences need more than cap bytes.
+bool read_files_into(std::vector<std::string> const& files, size_t first, size_t count, uint32_t color_base,
+                     uint32_t threads, char* dst, uint64_t cap, seq_batch& out);
+
+// Write n bytes to `path` with `threads` threads (positional writes of
+// disjoint ranges).
+void write_file_parallel(std::string const& path, uint8_t const* data, uint64_t n, uint32_t threads);
+
 // ---- bucket files (bucket_io.hpp:19-40) ------------------------------------
 // Append one LZ4 frame per non-empty bucket slice to open bucket files.
 class bucket_file_set {
@@ -77,6 +93,12 @@ void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
 // the low and high bit vectors each as [u64 num_bits][u64 num_words][words]).
 void write_color_sets(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
                       uint64_t const* offsets, uint64_t nclasses);
+
+// The same file from an Elias-Fano encoding made elsewhere (on the device):
+// l low bits per value, the low and high bit vectors as words.
+void write_color_sets_ef(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
+                         uint64_t nvalues, uint64_t l, uint64_t const* low, uint64_t const* high,
+                         uint64_t high_bits);
 
 }  // namespace io
 }  // namespace cdbg

@@ -4,8 +4,9 @@
  * Plain pointers and sizes only.  Every function returns 0 on success and a
  * negative code on failure; cdbg_last_error() then describes the failure
  * (thread-local).  The reference throws std::runtime_error in the same
- * situations (bucket_io.hpp:255-272, 681-699; seq_reader.hpp:48); the C++
- * adapter in INTEGRATION.md turns a non-zero return back into that exception.
+ * situations (bucket_io.hpp:255-272, 681-699; seq_reader.hpp:48); a C++
+ * adapter on the caller's side turns a non-zero return back into that
+ * exception.
  *
  * Reference interfaces replaced (paths relative to the reference repository):
  *   cdbg_gpu_phase1  <- ingest_bucketed(files, k, m, B, bucket_writer&, T, ...)
@@ -54,13 +55,17 @@ typedef struct cdbg_tuning {
     uint64_t batch_occ;        /* phase-2 k-mer occurrences per bucket batch: the
                                   threshold at which consecutive buckets split
                                   into another batch (0 = from free HBM) */
-    uint32_t minimizer_tile;   /* (k-1)-mers per minimizer tile: 1024 or 2048 */
+    uint32_t minimizer_tile;   /* (k-1)-mers per minimizer tile: 1024, 2048 or
+                                  4096 (default 4096) */
     uint32_t heavy_colors;     /* records with >= this many colors get a bitmap
                                   in multi-record unions (default 64) */
     uint32_t table_slots_q;    /* k-mer table slots per 4 occurrences of a
                                   bucket, 5..16 (default 8: a load factor of at
                                   most 1/2 over occurrences; fewer slots move
                                   fewer table bytes, longer probes) */
+    uint32_t union_lists;      /* 1: multi-record color unions as sorted color
+                                  lists, the path taken above 8192 colors
+                                  (0 = C-bit bitmaps while C <= 8192) */
 } cdbg_tuning;
 
 int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t);
@@ -152,6 +157,13 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
 int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, uint32_t m,
                          uint32_t num_buckets, const char* dump_path, uint64_t* n_supers);
 
+/* Stable sort of n device (key, value) pairs by the full 64-bit key, in place
+ * on the engine's stream: the sort phase 1 uses to order super-k-mers by
+ * (bucket, hash) and phase 2 to group candidate color sets by hash (4 radix
+ * passes over the top 32 key bits, then only the runs that tie there are
+ * sorted on the rest).  Test aid, no counterpart in the reference. */
+int cdbg_gpu_sort_pairs_u64(cdbg_engine* e, uint64_t* keys, uint32_t* vals, uint64_t n);
+
 /* ---- phase 2 ------------------------------------------------------------ */
 
 /* Called once per new color class in global cid order (the order the
@@ -214,6 +226,28 @@ typedef struct cdbg_build_result {
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
                    cdbg_build_result* r);
 
+/* The in-memory build from files, end to end: gzip/plain FASTA/FASTQ files
+ * (file i = color i) in, frag_unitigs.bin and a finalized .color_sets out --
+ * the inputs and outputs of the reference's phase 1 + phase 2 (builder.hpp:
+ * 180-271) without its bucket files.  Host threads inflate and parse the
+ * files in groups while the device already runs phase 1 on the groups read
+ * before; phase 2 follows in HBM; the Elias-Fano finalize of the class
+ * offsets (streaming_color_set_dict.hpp:221-294) runs on the device; the
+ * outputs are written with parallel writes.  With both paths NULL the
+ * outputs stay in host memory (the result's pointers, as cdbg_gpu_build with
+ * outputs_to_host = 1).  r->ms_total is the call's wall time here. */
+typedef struct cdbg_build_files_args {
+    const char* const* files;
+    uint32_t num_files;
+    uint32_t k, m, num_buckets;    /* m = 0: compute_best_m(k) */
+    uint32_t host_threads;         /* 0 = all cores */
+    uint64_t batch_occ;            /* 0 = auto */
+    const char* frag_path;         /* may be NULL */
+    const char* color_sets_path;   /* may be NULL */
+} cdbg_build_files_args;
+
+int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_build_result* r);
+
 /* Serialized size of the bucket records of the engine's last cdbg_gpu_build
  * (the uncompressed bytes its bucket files would hold), counted on the device
  * outside the build.  Valid until the engine's next call. */
@@ -239,9 +273,11 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
  * library holds until the process exits.
  *
  * Inputs (device): `words` is a 2-bit stream (base i at bits 2*(i%32) of word
- * i/32, with at least two readable words after the last base); run r starts at
- * base run_soff[r] (a multiple of 32) and has run_len[r] >= k ACGT bases and
- * color run_color[r].  Outputs (device, out_cap entries each): per
+ * i/32, with at least two readable words after the last base), 16-byte
+ * aligned; run r starts at base run_soff[r] (a multiple of 32) and has
+ * run_len[r] >= k ACGT bases and color run_color[r].  A misaligned `words`
+ * or a run shorter than k is rejected with an error before any tile runs.
+ * Outputs (device, out_cap entries each): per
  * super-k-mer in emission order its stream start, length, color, flags
  * (bit 0 begin, 1 end, 2 owns-first, 3 owns-last) and bucket -- the same
  * super-k-mers cdbg_gpu_dump_supers reports.  *n_supers receives the count.
@@ -252,10 +288,13 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
  * rejected with an error, as is an output capacity below the count.
  * The first call on a device looks up the device address of the working
  * array (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the working array, which keeps the previous
- * call's contents: calls that overlap on the GPU (other streams or host
- * threads) race and must be serialized by the caller.  Errors are reported
- * through cdbg_last_error(). */
+ * capture.  That address stays cached for the life of the process: after a
+ * cudaDeviceReset it is stale, so do not call this function again in that
+ * process.  Each call synchronizes `stream` to read counts back to the host.
+ * All calls share the working array, which keeps the previous call's
+ * contents: calls that overlap on the GPU (other streams or host threads)
+ * race and must be serialized by the caller.  Errors are reported through
+ * cdbg_last_error(). */
 int cdbg_gpu_supers_noalloc(const uint64_t* words, const uint64_t* run_soff, const uint32_t* run_len,
                             const uint32_t* run_color, uint32_t num_runs, uint32_t k, uint32_t m,
                             uint32_t num_buckets, uint64_t* out_start, uint32_t* out_len,

@@ -111,7 +111,7 @@ def test_device_resident_outputs_match_host_outputs(engine, tmp_path):
         assert engine.copy_out(rd.class_offsets, len(offs)) == offs
 
 
-def test_union_list_path_matches_bitmap_path(engine, tmp_path, monkeypatch):
+def test_union_list_path_matches_bitmap_path(engine, tmp_path):
     """Multi-record color unions as lists (used above 8192 colors) give the
     same bytes as the bitmap path."""
     lst = _fresh(tmp_path, 31, 8)
@@ -119,8 +119,11 @@ def test_union_list_path_matches_bitmap_path(engine, tmp_path, monkeypatch):
     hs = native.HostSequences(files)
     r = engine.build(hs.batch, 31, 128, 8)
     a = (native.result_frag_bytes(r), native.result_class_words(r).tobytes())
-    monkeypatch.setenv("CDBG_UNION_LISTS", "1")
-    r2 = engine.build(hs.batch, 31, 128, 8)
+    engine.set_tuning(union_lists=1)
+    try:
+        r2 = engine.build(hs.batch, 31, 128, 8)
+    finally:
+        engine.set_tuning()
     assert (native.result_frag_bytes(r2), native.result_class_words(r2).tobytes()) == a
 
 

@@ -32,9 +32,11 @@ def test_knobs_do_not_change_outputs(k):
     e = native.Engine(0)
     try:
         want = _out(e, b, k, B, n)
-        for t in (dict(minimizer_tile=1024), dict(heavy_colors=1), dict(heavy_colors=100000),
+        for t in (dict(minimizer_tile=1024), dict(minimizer_tile=2048), dict(heavy_colors=1),
+                  dict(heavy_colors=100000),
                   dict(batch_occ=1 << 12), dict(batch_occ=1, minimizer_tile=1024, heavy_colors=16),
-                  dict(table_slots_q=5), dict(table_slots_q=16), dict(table_slots_q=5, batch_occ=1 << 14)):
+                  dict(table_slots_q=5), dict(table_slots_q=16), dict(table_slots_q=5, batch_occ=1 << 14),
+                  dict(union_lists=1, heavy_colors=1)):
             e.set_tuning(**t)
             got = _out(e, b, k, B, n)
             assert got[0] == want[0], t
@@ -51,7 +53,7 @@ def test_autotune_keeps_outputs(engine):
     try:
         t, ms = e.autotune(b, 31, B, n)
         assert ms > 0
-        assert t["minimizer_tile"] in (1024, 2048)
+        assert t["minimizer_tile"] in (1024, 2048, 4096)
         assert 5 <= t["table_slots_q"] <= 16
         assert e.tuning() == t
         got = _out(e, b, 31, B, n)

@@ -10,7 +10,7 @@ import pytest
 
 from conftest import ROOT
 
-REF = os.environ.get("CDBG_REFERENCE", "/root/reference")
+REF = os.environ.get("CDBG_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 LIB = os.path.join(ROOT, "cdbg-builder_b200", "libcdbg_gpu.so")
 
 USE = r'''

@@ -109,6 +109,40 @@ def test_noalloc_matches_dump_supers_twice(engine, tmp_path):
         assert got == open(ref, "rb").read(), "call %d differs" % call
 
 
+def _call(L, words_ptr, soff, lens, k, m=12, B=64, cap=16):
+    import torch
+    ds = torch.from_numpy(np.asarray(soff, dtype=np.uint64).view(np.int64)).cuda()
+    dl = torch.from_numpy(np.asarray(lens, dtype=np.uint32).view(np.int32)).cuda()
+    dc = torch.zeros(len(lens), dtype=torch.int32, device="cuda")
+    out = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    n = ctypes.c_uint64()
+    rc = L.cdbg_gpu_supers_noalloc(words_ptr, ds.data_ptr(), dl.data_ptr(), dc.data_ptr(), len(lens), k, m, B,
+                                   out.data_ptr(), out.data_ptr(), out.data_ptr(), out.data_ptr(),
+                                   out.data_ptr(), cap, ctypes.byref(n), None)
+    torch.cuda.synchronize()
+    return rc
+
+
+def test_noalloc_rejects_bad_inputs_then_recovers(engine, tmp_path):
+    """Inputs past the fixed working array, runs shorter than k and a
+    misaligned stream are refused with an error before any tile kernel reads
+    them; a valid call afterwards still matches the allocating entry point."""
+    import torch
+    L = native.lib()
+    k = 31
+    # one run of 1.1M bases: few runs, but more than 512 tiles of 2048 (k-1)-mers
+    words = torch.zeros(1_100_000 // 32 + 16, dtype=torch.int64, device="cuda")
+    assert _call(L, words.data_ptr(), [0], [1_100_000], k) != 0
+    assert b"tiles" in L.cdbg_last_error()
+    # a run of k - 1 bases has no k-mer
+    assert _call(L, words.data_ptr(), [0, 64], [40, k - 1], k) != 0
+    assert b"shorter than k" in L.cdbg_last_error()
+    # the stream must be 16-byte aligned (8 bytes into a buffer is not)
+    assert _call(L, words.data_ptr() + 8, [0], [40], k) != 0
+    assert b"aligned" in L.cdbg_last_error()
+    test_noalloc_matches_dump_supers_twice(engine, tmp_path)
+
+
 def test_noalloc_rejects_oversized_input(engine):
     import torch
     L = native.lib()
