@@ -55,7 +55,7 @@ class Phase2Args(ctypes.Structure):
                 ("frag_path", ctypes.c_char_p), ("color_sets_path", ctypes.c_char_p),
                 ("on_class", CLASS_CB), ("ctx", ctypes.c_void_p),
                 ("delete_consumed", ctypes.c_int32), ("host_threads", ctypes.c_uint32),
-                ("batch_occ", ctypes.c_uint64)]
+                ("batch_occ", ctypes.c_uint64), ("pass_bytes", ctypes.c_uint64)]
 
 
 class Phase2Stats(ctypes.Structure):
@@ -63,7 +63,8 @@ class Phase2Stats(ctypes.Structure):
                 ("n_distinct", ctypes.c_uint64), ("n_fragments", ctypes.c_uint64),
                 ("total_seq_bytes", ctypes.c_uint64), ("n_color_sets", ctypes.c_uint64),
                 ("total_integers", ctypes.c_uint64), ("color_bits", ctypes.c_uint64),
-                ("seconds_total", ctypes.c_double), ("seconds_device", ctypes.c_double)]
+                ("seconds_total", ctypes.c_double), ("seconds_device", ctypes.c_double),
+                ("n_passes", ctypes.c_uint64)]
 
 
 class BuildParams(ctypes.Structure):
@@ -96,7 +97,7 @@ class BuildResult(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("batch_occ", ctypes.c_uint64), ("minimizer_tile", ctypes.c_uint32),
                 ("heavy_colors", ctypes.c_uint32), ("table_slots_q", ctypes.c_uint32),
-                ("union_lists", ctypes.c_uint32)]
+                ("union_lists", ctypes.c_uint32), ("table_group_mb", ctypes.c_uint32)]
 
 
 class ServerParams(ctypes.Structure):
@@ -304,9 +305,11 @@ class Engine:
         _check(lib().cdbg_engine_memory(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
-    def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0, table_slots_q=0, union_lists=0):
+    def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0, table_slots_q=0, union_lists=0,
+                   table_group_mb=0):
         _check(lib().cdbg_engine_set_tuning(self._h, ctypes.byref(Tuning(batch_occ, minimizer_tile, heavy_colors,
-                                                                         table_slots_q, union_lists))))
+                                                                         table_slots_q, union_lists,
+                                                                         table_group_mb))))
 
     def tuning(self):
         t = Tuning()
@@ -383,7 +386,7 @@ class Engine:
         return s, unc
 
     def phase2(self, tmp_dir, num_buckets, k, num_colors, frag_path, color_sets_path=None,
-               on_class=None, delete_consumed=False, host_threads=0, batch_occ=0):
+               on_class=None, delete_consumed=False, host_threads=0, batch_occ=0, pass_bytes=0):
         cb = CLASS_CB(0)
         if on_class is not None:
             def _cb(ctx, p, n):
@@ -392,7 +395,7 @@ class Engine:
             cb = CLASS_CB(_cb)
         a = Phase2Args(tmp_dir.encode(), num_buckets, k, num_colors, frag_path.encode(),
                        color_sets_path.encode() if color_sets_path else None, cb, None,
-                       1 if delete_consumed else 0, host_threads, batch_occ)
+                       1 if delete_consumed else 0, host_threads, batch_occ, pass_bytes)
         s = Phase2Stats()
         _check(lib().cdbg_gpu_phase2(self._h, ctypes.byref(a), ctypes.byref(s)))
         return s

@@ -495,6 +495,13 @@ int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, ui
     }
 }
 
+namespace {
+bool phase1_from_files(cdbg_engine* e, std::vector<std::string> const& files, uint32_t threads, uint32_t k,
+                       uint32_t m, uint32_t B, cdbg::run_table& rt_all, cdbg::super_list& sl_all, uint64_t* h2d,
+                       uint64_t* input_bytes, uint32_t color_base = 0, bool packed = true,
+                       uint64_t* seq_bytes = nullptr);
+}  // namespace
+
 int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats* s) {
     if (!e) {
         g_last_error = "null engine";
@@ -508,12 +515,28 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
         validate(k, m, a->num_buckets);
         CDBG_CUDA(cudaSetDevice(e->device));
         e->A.reset();
+        e->P.reset();
+        e->have_rs = false;
         apply_limit(e);
         const uint32_t T = host_threads(a->host_threads);
         std::vector<std::string> files(a->files, a->files + a->num_files);
         cdbg::io::bucket_file_set out(a->tmp_dir, a->num_buckets);
         cdbg_phase1_stats st{};
-        const uint64_t chunk = a->chunk_bytes ? a->chunk_bytes : (8ull << 30);
+        // chunks of whole files by inflated size: one chunk is one device
+        // pass (records are deduplicated within a chunk, the reference's own
+        // compaction is per 64 KiB window); the default chunk is a share of
+        // the device memory this engine may use
+        uint64_t chunk = a->chunk_bytes;
+        if (chunk == 0) {
+            size_t fr = 0, tot = 0;
+            CDBG_CUDA(cudaMemGetInfo(&fr, &tot));
+            uint64_t avail = fr + e->A.cached_free() + e->P.cached_free();
+            if (e->mem_limit) avail = std::min<uint64_t>(avail, e->mem_limit);
+            chunk = std::max<uint64_t>(64ull << 20, avail / 24);
+        }
+        std::vector<uint64_t> hint(files.size());
+        for (size_t i = 0; i < files.size(); ++i) hint[i] = cdbg::io::inflated_size_hint(files[i]);
+        const bool packed = a->num_files < (1u << 28);
         double dev_s = 0;
         size_t f0 = 0;
         while (f0 < files.size()) {
@@ -521,47 +544,79 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
             size_t f1 = f0;
             uint64_t acc = 0;
             while (f1 < files.size()) {
-                std::error_code ec;
-                uint64_t sz = std::filesystem::file_size(files[f1], ec);
-                if (ec) sz = 0;
-                const bool gz = files[f1].size() > 3 && files[f1].compare(files[f1].size() - 3, 3, ".gz") == 0;
-                if (gz) sz *= 4;  // inflated size estimate
-                if (f1 > f0 && acc + sz > chunk) break;
-                acc += sz;
+                if (f1 > f0 && acc + hint[f1] > chunk) break;
+                acc += hint[f1];
                 ++f1;
             }
-            cdbg::io::seq_batch hb;
-            cdbg::io::read_files(files, f0, f1 - f0, (uint32_t)f0, T, hb);
-            st.input_bytes += hb.input_bytes;
-            st.seq_bytes += hb.seq.size();
             auto td = std::chrono::steady_clock::now();
             e->A.reset();
-            cdbg_seq_batch b{hb.seq.data(), hb.seq.size(), hb.off.data(), hb.color.data(),
-                             (uint32_t)hb.color.size(), 0};
-            cdbg::seq_input in = stage_batch(e, &b, nullptr);
+            e->P.reset();
+            std::vector<std::string> cf(files.begin() + f0, files.begin() + f1);
             cdbg::run_table rt;
-            cdbg::build_runs(in, k, e->A, e->st, rt, e->A);
             cdbg::super_list sl;
-            cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile,
-                              a->num_files < (1u << 28));
+            uint64_t inb = 0, nseq = 0;
+            // the files are read on host threads while the device already
+            // runs phase 1 on the ones read before
+            if (!phase1_from_files(e, cf, T, k, m, a->num_buckets, rt, sl, nullptr, &inb, (uint32_t)f0, packed,
+                                   &nseq)) {
+                // a file inflated past its size hint: read the chunk whole
+                e->A.reset();
+                e->P.reset();
+                cdbg::io::seq_batch hb;
+                cdbg::io::read_files(files, f0, f1 - f0, (uint32_t)f0, T, hb);
+                inb = hb.input_bytes;
+                nseq = hb.seq.size();
+                cdbg_seq_batch b{hb.seq.data(), hb.seq.size(), hb.off.data(), hb.color.data(),
+                                 (uint32_t)hb.color.size(), 0};
+                cdbg::seq_input in = stage_batch(e, &b, nullptr);
+                cdbg::build_runs(in, k, e->A, e->st, rt, e->P);
+                cdbg::find_supers(rt, k, m, a->num_buckets, e->A, e->st, sl, e->d_err, e->tune.minimizer_tile,
+                                  packed);
+                CDBG_CUDA(cudaStreamSynchronize(e->st));
+            }
+            st.input_bytes += inb;
+            st.seq_bytes += nseq;
             cdbg::record_set rs;
             cdbg::build_records(rt, sl, k, a->num_buckets, e->A, e->st, rs, e->d_err, e->A);
             cdbg::serialized_buckets sb;
             cdbg::serialize_records(rs, e->A, e->st, sb);
             cdbg::check_device_error(e, "phase 1");
-            std::vector<uint8_t> raw(sb.nbytes);
+            // the serialized records come back in bucket ranges: host threads
+            // compress and append one range while the next is still copying
             std::vector<uint64_t> boff(a->num_buckets + 1);
-            if (sb.nbytes)
-                CDBG_CUDA(cudaMemcpyAsync(raw.data(), sb.bytes, sb.nbytes, cudaMemcpyDeviceToHost, e->st));
             CDBG_CUDA(cudaMemcpyAsync(boff.data(), sb.bucket_off, 8ull * (a->num_buckets + 1),
                                       cudaMemcpyDeviceToHost, e->st));
             CDBG_CUDA(cudaStreamSynchronize(e->st));
+            uint8_t* raw = (uint8_t*)e->h_frag.ensure(sb.nbytes + 64);
+            std::vector<uint32_t> rcut{0};
+            const uint64_t per = std::max<uint64_t>(16ull << 20, sb.nbytes / 16);
+            for (uint32_t b = 1; b < a->num_buckets; ++b)
+                if (boff[b] - boff[rcut.back()] >= per) rcut.push_back(b);
+            rcut.push_back(a->num_buckets);
+            std::vector<cudaEvent_t> rev(rcut.size() - 1);
+            for (auto& x : rev) CDBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+            for (size_t r = 0; r + 1 < rcut.size(); ++r) {
+                const uint64_t lo = boff[rcut[r]], hi = boff[rcut[r + 1]];
+                if (hi > lo)
+                    CDBG_CUDA(cudaMemcpyAsync(raw + lo, sb.bytes + lo, hi - lo, cudaMemcpyDeviceToHost, e->st));
+                CDBG_CUDA(cudaEventRecord(rev[r], e->st));
+            }
             dev_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - td).count();
+            try {
+                for (size_t r = 0; r + 1 < rcut.size(); ++r) {
+                    CDBG_CUDA(cudaEventSynchronize(rev[r]));
+                    out.append_frames_range(raw, boff.data(), rcut[r], rcut[r + 1], T);
+                }
+            } catch (...) {
+                for (auto& x : rev) cudaEventDestroy(x);
+                throw;
+            }
+            for (auto& x : rev) cudaEventDestroy(x);
             st.n_kmers += rt.n_kmers;
             st.n_supers += sl.n;
             st.n_records += rs.n;
-            out.append_frames(raw.data(), boff.data(), T);
             e->A.reset();
+            e->P.reset();
             f0 = f1;
         }
         out.close();
@@ -585,61 +640,123 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
         return -1;
     }
     call_scope scope_(e);
+    std::thread reader;
     try {
         auto t0 = std::chrono::steady_clock::now();
         CDBG_CUDA(cudaSetDevice(e->device));
         const uint32_t T = host_threads(a->host_threads);
         const uint32_t B = a->num_buckets;
         if (a->k < 2 || a->k > 63) throw std::runtime_error("k must be in [2, 63]");
+        if (B == 0) throw std::runtime_error("num_buckets must be > 0");
         e->A.reset();
         apply_limit(e);
-        // bucket bytes: decompress straight into pinned host memory
-        uint8_t* pinned = nullptr;
-        cdbg::io::bucket_bytes bb;
-        cdbg::io::read_bucket_files(
-            a->tmp_dir, B, T,
-            [&](uint64_t n) -> uint8_t* {
-                CDBG_CUDA(cudaMallocHost(&pinned, n));
-                return pinned;
-            },
-            bb, a->delete_consumed != 0);
-        auto td = std::chrono::steady_clock::now();
-        uint8_t* dbytes = e->A.alloc<uint8_t>(bb.nbytes + 64);
-        CDBG_CUDA(cudaMemcpyAsync(dbytes, bb.data, bb.nbytes + 64, cudaMemcpyHostToDevice, e->st));
-        const uint32_t nch = (uint32_t)bb.chunk_bucket.size();
-        uint64_t* dco = e->A.alloc<uint64_t>(nch + 1);
-        uint32_t* dcb = e->A.alloc<uint32_t>(nch + 1);
-        CDBG_CUDA(cudaMemcpyAsync(dco, bb.chunk_off.data(), 8ull * (nch + 1), cudaMemcpyHostToDevice, e->st));
-        if (nch)
-            CDBG_CUDA(cudaMemcpyAsync(dcb, bb.chunk_bucket.data(), 4ull * nch, cudaMemcpyHostToDevice, e->st));
-        CDBG_CUDA(cudaStreamSynchronize(e->st));
-        cudaFreeHost(pinned);
-        pinned = nullptr;
-        cdbg::record_set rs;
-        cdbg::parse_records(dbytes, bb.nbytes, dco, dcb, nch, B, e->A, e->st, rs, e->d_err);
-        cdbg::check_device_error(e, "bucket record parse");
-        cdbg::phase2_params pp;
-        pp.k = a->k;
-        pp.num_colors = a->num_colors;
-        pp.batch_occ = a->batch_occ ? a->batch_occ : e->tune.batch_occ;
-        pp.heavy_colors = e->tune.heavy_colors;
-        pp.table_slots_q = e->tune.table_slots_q;
-        pp.union_bitmaps = e->tune.union_lists == 0;
-        pp.to_host = true;
-        cdbg::phase2_result res;
-        res.state = &e->p2;
-        cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, res);
-        const double dev_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - td).count();
-        // frag spill
-        {
-            std::FILE* f = std::fopen(a->frag_path, "wb");
-            if (!f) throw std::runtime_error(std::string("cannot open frag spill: ") + a->frag_path);
-            if (!res.frag.empty() && std::fwrite(res.frag.data(), 1, res.frag.size(), f) != res.frag.size()) {
-                std::fclose(f);
-                throw std::runtime_error(std::string("short write to ") + a->frag_path);
-            }
-            std::fclose(f);
+        const std::string dir = a->tmp_dir;
+        // buckets in consecutive ranges of at most pass_bytes uncompressed
+        // bytes (a bucket larger than that is a range of its own), the
+        // reference's bucket-at-a-time admission (bucket_walker.hpp:643-672)
+        // at range granularity: a range is read and decompressed on host
+        // threads while the device processes the range before it
+        const std::vector<uint64_t> unc = cdbg::io::bucket_sizes(dir, B, T);
+        uint64_t pass = a->pass_bytes;
+        if (pass == 0) {
+            size_t fr = 0, tot = 0;
+            CDBG_CUDA(cudaMemGetInfo(&fr, &tot));
+            uint64_t avail = fr + e->A.cached_free();
+            if (e->mem_limit) avail = std::min<uint64_t>(avail, e->mem_limit);
+            pass = std::max<uint64_t>(64ull << 20, std::min<uint64_t>(16ull << 30, avail / 16));
         }
+        std::vector<uint32_t> rb{0};
+        {
+            uint64_t acc = 0;
+            for (uint32_t b = 0; b < B; ++b) {
+                if (b > rb.back() && acc + unc[b] > pass) {
+                    rb.push_back(b);
+                    acc = 0;
+                }
+                acc += unc[b];
+            }
+            rb.push_back(B);
+        }
+        const size_t nr = rb.size() - 1;
+        uint64_t maxr = 0;
+        for (size_t i = 0; i < nr; ++i) {
+            uint64_t r = 0;
+            for (uint32_t b = rb[i]; b < rb[i + 1]; ++b) r += unc[b];
+            maxr = std::max(maxr, r);
+        }
+        uint8_t* hbuf[2] = {(uint8_t*)e->h_bk[0].ensure(maxr + 128), (uint8_t*)e->h_bk[1].ensure(maxr + 128)};
+        cdbg::io::bucket_bytes bb[2];
+        std::exception_ptr rerr;
+        auto read_range = [&](size_t i) {
+            try {
+                cdbg::io::read_bucket_range(dir, B, rb[i], rb[i + 1], T, [&](uint64_t) { return hbuf[i & 1]; },
+                                            bb[i & 1]);
+            } catch (...) {
+                rerr = std::current_exception();
+            }
+        };
+        std::FILE* ff = std::fopen(a->frag_path, "wb");
+        if (!ff) throw std::runtime_error(std::string("cannot open frag spill: ") + a->frag_path);
+        struct file_closer {
+            std::FILE*& f;
+            ~file_closer() {
+                if (f) std::fclose(f);
+            }
+        } fc{ff};
+        cdbg_phase2_stats st{};
+        cdbg::phase2_result res;
+        double dev_s = 0;
+        read_range(0);
+        for (size_t i = 0; i < nr; ++i) {
+            if (reader.joinable()) reader.join();
+            if (rerr) std::rethrow_exception(rerr);
+            if (i + 1 < nr) reader = std::thread(read_range, i + 1);
+            auto td = std::chrono::steady_clock::now();
+            cdbg::io::bucket_bytes& cb = bb[i & 1];
+            e->A.reset();
+            uint8_t* dbytes = e->A.alloc<uint8_t>(cb.nbytes + 64);
+            CDBG_CUDA(cudaMemcpyAsync(dbytes, cb.data, cb.nbytes + 64, cudaMemcpyHostToDevice, e->st));
+            const uint32_t nch = (uint32_t)cb.chunk_bucket.size();
+            uint64_t* dco = e->A.alloc<uint64_t>(nch + 1);
+            uint32_t* dcb = e->A.alloc<uint32_t>(nch + 1);
+            CDBG_CUDA(cudaMemcpyAsync(dco, cb.chunk_off.data(), 8ull * (nch + 1), cudaMemcpyHostToDevice, e->st));
+            if (nch)
+                CDBG_CUDA(cudaMemcpyAsync(dcb, cb.chunk_bucket.data(), 4ull * nch, cudaMemcpyHostToDevice, e->st));
+            cdbg::record_set rs;
+            cdbg::parse_records(dbytes, cb.nbytes, dco, dcb, nch, B, e->A, e->st, rs, e->d_err);
+            cdbg::check_device_error(e, "bucket record parse");
+            cdbg::phase2_params pp;
+            pp.k = a->k;
+            pp.num_colors = a->num_colors;
+            pp.batch_occ = a->batch_occ ? a->batch_occ : e->tune.batch_occ;
+            pp.heavy_colors = e->tune.heavy_colors;
+            pp.table_slots_q = e->tune.table_slots_q;
+            pp.union_bitmaps = e->tune.union_lists == 0;
+            pp.group_bytes = (uint64_t)(e->tune.table_group_mb ? e->tune.table_group_mb : 64) << 20;
+            pp.to_host = true;
+            pp.keep_dict = i > 0;
+            pp.copy_dict = i + 1 == nr;
+            res.state = &e->p2;
+            cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, res);
+            dev_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - td).count();
+            // this range's fragments, then (only then) its bucket files go
+            if (!res.frag.empty() && std::fwrite(res.frag.data(), 1, res.frag.size(), ff) != res.frag.size())
+                throw std::runtime_error(std::string("short write to ") + a->frag_path);
+            if (a->delete_consumed) {
+                if (std::fflush(ff) != 0) throw std::runtime_error(std::string("short write to ") + a->frag_path);
+                cdbg::io::delete_bucket_files(dir, rb[i], rb[i + 1]);
+            }
+            st.n_records += rs.n;
+            st.n_kmers += res.n_occ;
+            st.n_distinct += res.n_distinct;
+            st.n_fragments += res.n_fragments;
+            st.total_seq_bytes += res.total_seq_bytes;
+        }
+        if (std::fclose(ff) != 0) {
+            ff = nullptr;
+            throw std::runtime_error(std::string("short write to ") + a->frag_path);
+        }
+        ff = nullptr;
         if (a->color_sets_path)
             cdbg::io::write_color_sets(a->color_sets_path, a->num_colors, res.words.data(), res.nbits,
                                        res.offsets.data(), res.n_classes);
@@ -651,22 +768,18 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
             }
         }
         if (s) {
-            cdbg_phase2_stats st{};
-            st.n_records = rs.n;
-            st.n_kmers = res.n_occ;
-            st.n_distinct = res.n_distinct;
-            st.n_fragments = res.n_fragments;
-            st.total_seq_bytes = res.total_seq_bytes;
             st.n_color_sets = res.n_classes;
             st.total_integers = res.total_integers;
             st.color_bits = res.nbits;
             st.seconds_device = dev_s;
             st.seconds_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            st.n_passes = nr;
             *s = st;
         }
         e->A.reset();
         return 0;
     } catch (std::exception const& ex) {
+        if (reader.joinable()) reader.join();
         if (e) e->A.reset();
         return fail(ex);
     }
@@ -777,7 +890,7 @@ void phase1_pipelined(cdbg_engine* e, cdbg_seq_batch const* b, uint32_t k, uint3
 // to more than its hint says, and the caller reads the files whole instead.
 bool phase1_from_files(cdbg_engine* e, std::vector<std::string> const& files, uint32_t threads, uint32_t k,
                        uint32_t m, uint32_t B, cdbg::run_table& rt_all, cdbg::super_list& sl_all, uint64_t* h2d,
-                       uint64_t* input_bytes) {
+                       uint64_t* input_bytes, uint32_t color_base, bool packed, uint64_t* seq_bytes) {
     cudaStream_t st = e->st;
     const size_t nf = files.size();
     uint64_t N = 0;
@@ -806,8 +919,8 @@ bool phase1_from_files(cdbg_engine* e, std::vector<std::string> const& files, ui
             uint64_t nb = 0;
             try {
                 cdbg::io::seq_batch mb;
-                if (cdbg::io::read_files_into(files, gfirst[g], gfirst[g + 1] - gfirst[g], (uint32_t)gfirst[g],
-                                              threads, h_in + used, N - used, mb)) {
+                if (cdbg::io::read_files_into(files, gfirst[g], gfirst[g + 1] - gfirst[g],
+                                              color_base + (uint32_t)gfirst[g], threads, h_in + used, N - used, mb)) {
                     nb = mb.off.back();
                     G[g].meta = std::move(mb);
                 } else {
@@ -885,21 +998,42 @@ bool phase1_from_files(cdbg_engine* e, std::vector<std::string> const& files, ui
         n_kmers += rt.n_kmers;
         n_bases += rt.n_bases;
         cdbg::super_list sl;
-        cdbg::find_supers(rt, k, m, B, e->A, st, sl, e->d_err, e->tune.minimizer_tile, true);
+        cdbg::find_supers(rt, k, m, B, e->A, st, sl, e->d_err, e->tune.minimizer_tile, packed);
         if (sl.n) lists.push_back(sl);
     }
     cudaEventDestroy(ev);
+    if (seq_bytes) {
+        uint64_t tot = 0;
+        for (auto const& gr : G) tot += gr.nbytes;
+        *seq_bytes = tot;
+    }
     uint64_t n = 0;
     for (auto const& l : lists) n += l.n;
     if (n >= 0xffffffffull) throw std::runtime_error("more than 2^32 super-k-mers in one call");
     sl_all = cdbg::super_list();
     sl_all.n = n;
     sl_all.key = e->A.alloc<uint64_t>(n + 1);
-    sl_all.packed = e->A.alloc<uint4>(n + 1);
+    if (packed) {
+        sl_all.packed = e->A.alloc<uint4>(n + 1);
+    } else {
+        sl_all.start = e->A.alloc<uint64_t>(n + 1);
+        sl_all.len = e->A.alloc<uint32_t>(n + 1);
+        sl_all.color = e->A.alloc<uint32_t>(n + 1);
+        sl_all.flags = e->A.alloc<uint32_t>(n + 1);
+        sl_all.bucket = e->A.alloc<uint32_t>(n + 1);
+    }
     uint64_t o = 0;
     for (auto const& l : lists) {
         CDBG_CUDA(cudaMemcpyAsync(sl_all.key + o, l.key, 8 * l.n, cudaMemcpyDeviceToDevice, st));
-        CDBG_CUDA(cudaMemcpyAsync(sl_all.packed + o, l.packed, 16 * l.n, cudaMemcpyDeviceToDevice, st));
+        if (packed) {
+            CDBG_CUDA(cudaMemcpyAsync(sl_all.packed + o, l.packed, 16 * l.n, cudaMemcpyDeviceToDevice, st));
+        } else {
+            CDBG_CUDA(cudaMemcpyAsync(sl_all.start + o, l.start, 8 * l.n, cudaMemcpyDeviceToDevice, st));
+            CDBG_CUDA(cudaMemcpyAsync(sl_all.len + o, l.len, 4 * l.n, cudaMemcpyDeviceToDevice, st));
+            CDBG_CUDA(cudaMemcpyAsync(sl_all.color + o, l.color, 4 * l.n, cudaMemcpyDeviceToDevice, st));
+            CDBG_CUDA(cudaMemcpyAsync(sl_all.flags + o, l.flags, 4 * l.n, cudaMemcpyDeviceToDevice, st));
+            CDBG_CUDA(cudaMemcpyAsync(sl_all.bucket + o, l.bucket, 4 * l.n, cudaMemcpyDeviceToDevice, st));
+        }
         o += l.n;
     }
     rt_all = cdbg::run_table();
@@ -964,6 +1098,7 @@ int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phas
         pp.heavy_colors = e->tune.heavy_colors;
         pp.table_slots_q = e->tune.table_slots_q;
         pp.union_bitmaps = e->tune.union_lists == 0;
+        pp.group_bytes = (uint64_t)(e->tune.table_group_mb ? e->tune.table_group_mb : 64) << 20;
         pp.to_host = false;  // outputs accumulate in HBM
         if (p->outputs_to_host && e->h_frag.p && e->h_frag.cap) {
             // stream each batch's fragments into the (already large enough,
@@ -1202,6 +1337,7 @@ int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
         g_last_error = "union_lists must be 0 or 1";
         return -1;
     }
+    if (v.table_group_mb == 0) v.table_group_mb = 64;
     e->tune = v;
     return 0;
 }
@@ -1241,6 +1377,7 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
         if (cur.minimizer_tile == 0) cur.minimizer_tile = 4096;
         if (cur.heavy_colors == 0) cur.heavy_colors = 64;
         if (cur.table_slots_q == 0) cur.table_slots_q = 8;
+        if (cur.table_group_mb == 0) cur.table_group_mb = 64;
         measure(cur);  // warm-up: allocations reach their working sizes
         double cur_ms = measure(cur);
         auto consider = [&](cdbg_tuning const& t) {
@@ -1269,6 +1406,11 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
             cdbg_tuning t = cur;
             t.table_slots_q = v;
             if (t.table_slots_q != cur.table_slots_q) consider(t);
+        }
+        for (uint32_t v : {32u, 64u, 96u, 192u}) {
+            cdbg_tuning t = cur;
+            t.table_group_mb = v;
+            if (t.table_group_mb != cur.table_group_mb) consider(t);
         }
         e->tune = cur;
         if (best) *best = cur;

@@ -182,12 +182,15 @@ __device__ __forceinline__ void slot_load(slot_t<uint64_t> const* e, uint64_t& k
 // full.  `ro` receives the slot's (rank | om << 32) as read while probing: a
 // value the slot held, so possibly older than the current one (rank only
 // falls and om only gains bits, which the caller's updates rely on).
+// `slots` holds the slots from absolute index off0 on (the tables of the
+// bucket group being processed); returned indices are absolute.
 template <typename K>
-__device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off, uint64_t cap, K x, uint64_t& ro) {
+__device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off0, uint64_t off, uint64_t cap, K x,
+                                                 uint64_t& ro) {
     const K EMPTY = kmer_ops<K>::empty();
     uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
     for (uint64_t i = 0; i < cap; ++i) {
-        slot_t<K>* e = &slots[off + s];
+        slot_t<K>* e = &slots[off + s - off0];
         if constexpr (sizeof(K) == 8) {
             uint64_t cur, v;
             slot_load(e, cur, v);
@@ -225,12 +228,16 @@ struct rec_view {
     uint64_t const* words;
 };
 
+// The k-mer tables of buckets b0, b0 + 1, ...: bucket b0 + i's table is
+// the tab_cap[i] slots from absolute slot tab_off[i]; `slots` holds the slots
+// from absolute index off0 on (one bucket group's tables at a time).
 template <typename K>
 struct tables {
     slot_t<K>* slots;
-    uint64_t const* tab_off;  // per batch bucket
+    uint64_t const* tab_off;
     uint64_t const* tab_cap;
     uint32_t b0;
+    uint64_t off0;
 };
 
 // Occurrence o of the batch -> (record, index, canonical k-mer, contrib, owned).
@@ -267,8 +274,8 @@ __global__ void k_block_records(uint64_t const* __restrict__ occ, uint64_t R0, u
 }
 
 __device__ __forceinline__ void load_occ_window(occ_window& w, uint64_t const* occ, uint64_t R0, uint64_t nrec,
-                                                uint32_t const* __restrict__ blk_rec) {
-    if (threadIdx.x == 0) w.r0 = blk_rec[blockIdx.x];
+                                                uint32_t const* __restrict__ blk_rec, uint64_t blk) {
+    if (threadIdx.x == 0) w.r0 = blk_rec[blk];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < OCC_BLOCK + 2; i += blockDim.x) {
         const uint64_t r = w.r0 + i;
@@ -345,20 +352,22 @@ __global__ void k_init_tables(uint64_t T, slot_t<K>* slots) {
     slots[i] = e;
 }
 
+// Occurrences t0 .. t0 + nocc - 1 of the batch (one bucket group's).
 template <typename K>
 __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_t R0, uint64_t nrec,
-                                                uint64_t O0, uint64_t nocc, uint32_t k,
+                                                uint64_t O0, uint64_t t0, uint64_t nocc, uint32_t k,
                                                 uint32_t const* __restrict__ blk_rec,
                                                 uint32_t* __restrict__ occ_slot, uint32_t* err) {
     __shared__ occ_window win;
-    load_occ_window(win, R.occ, R0, nrec, blk_rec);
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nocc) return;
+    // the window of the occurrence block holding this block's first occurrence
+    load_occ_window(win, R.occ, R0, nrec, blk_rec, (t0 + (uint64_t)blockIdx.x * blockDim.x) / OCC_BLOCK);
+    const uint64_t t = t0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= t0 + nocc) return;
     const uint64_t rec = window_record(win, R.occ, R0, nrec, O0 + t);
     const occ_info<K> oi = decode_occ_r<K>(R, rec, O0 + t, k);
     const uint32_t tb = R.bucket[oi.r] - T.b0;
     uint64_t ro = 0;
-    const uint64_t s = table_upsert<K>(T.slots, T.tab_off[tb], T.tab_cap[tb], oi.can, ro);
+    const uint64_t s = table_upsert<K>(T.slots, T.off0, T.tab_off[tb], T.tab_cap[tb], oi.can, ro);
     if (s == ~0ull) {
         set_error(err, ERR_TABLE_FULL);
         occ_slot[t] = NONE32;
@@ -370,7 +379,7 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     // rank and om as read while probing (never newer than the slot): the
     // reduction and the updates below stay correct, and a k-mer whose slot
     // already holds everything this occurrence adds costs no further access
-    slot_t<K>& e = T.slots[s];
+    slot_t<K>& e = T.slots[s - T.off0];
     if ((uint32_t)t < (uint32_t)ro) atomicMin(&e.rank, (uint32_t)t);
     uint32_t old = (uint32_t)(ro >> 32);
     if (!oi.owned) {
@@ -405,43 +414,100 @@ __global__ void k_firstbits(uint64_t T, slot_t<K> const* __restrict__ slots, uin
     atomicOr(&bits[q >> 5], 1u << (q & 31));
 }
 
-__global__ void k_popc(uint64_t n, uint32_t const* __restrict__ bits, uint32_t* __restrict__ cnt) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) cnt[i] = __popc(bits[i]);
+
+// Number the distinct k-mers of one bucket group in first-insertion order,
+// scanning its occurrences t0 .. t0 + nocc - 1: occurrence t is the first of
+// its k-mer iff bit t of `bits` is set, and its node index is *nbase plus the
+// number of first occurrences before it in the group.  Tiles of MN_ROUNDS x
+// 256 occurrences take indices in launch order and find their offset by
+// decoupled look-back; the last tile stores *nbase + the group's count in
+// *nnext (the next group's base).  The slot's rank field becomes the node
+// index, and the node arrays are written in node order; the bucket is the
+// slot's table (tab_off ascends over the group's buckets).
+constexpr int MN_ROUNDS = 8;
+template <typename K>
+__global__ void __launch_bounds__(256) k_make_nodes(uint64_t t0, uint64_t nocc, uint32_t const* __restrict__ occ_slot,
+                                                    uint32_t const* __restrict__ bits, tables<K> TB, uint32_t nb,
+                                                    uint64_t R0, unsigned long long const* nbase,
+                                                    unsigned long long* nnext, uint32_t* tile_counter,
+                                                    unsigned long long* status, K* __restrict__ n_key,
+                                                    uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
+                                                    uint32_t* __restrict__ n_bucket, uint32_t* err) {
+    constexpr int NW = 256 / 32;
+    static_assert(MN_ROUNDS * NW == 64, "warp 0 scans two counts per lane");
+    __shared__ uint64_t s_tile;
+    __shared__ uint32_t wcnt[MN_ROUNDS * NW];
+    __shared__ unsigned long long s_base;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    const uint64_t ntiles = (nocc + MN_ROUNDS * 256 - 1) / (MN_ROUNDS * 256);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t rank[MN_ROUNDS], first = 0;
+#pragma unroll
+    for (int rr = 0; rr < MN_ROUNDS; ++rr) {
+        const uint64_t l = (tile * MN_ROUNDS + rr) * 256 + threadIdx.x;
+        const uint64_t t = t0 + l;
+        const bool f = l < nocc && ((bits[t >> 5] >> (t & 31)) & 1u);
+        const uint32_t bal = __ballot_sync(0xffffffffu, f);
+        rank[rr] = __popc(bal & lanemask_lt());
+        if (f) first |= 1u << rr;
+        if (lane == 0) wcnt[rr * NW + warp] = __popc(bal);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t c0 = wcnt[2 * lane], c1 = wcnt[2 * lane + 1];
+        uint32_t x = c0 + c1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+        const uint32_t ex = x - c0 - c1;
+        wcnt[2 * lane] = ex;
+        wcnt[2 * lane + 1] = ex + c0;
+        uint64_t excl = 0;
+        const bool ok = prim::lookback_exclusive(status, tile, tot, excl);
+        if (lane == 0) {
+            if (!ok) set_error(err, ERR_CHAIN_LIMIT);
+            s_base = *nbase + excl;
+            if (tile == ntiles - 1) *nnext = *nbase + excl + tot;
+        }
+    }
+    __syncthreads();
+    const unsigned long long base = s_base;
+#pragma unroll
+    for (int rr = 0; rr < MN_ROUNDS; ++rr) {
+        const bool f = (first >> rr) & 1u;
+        const uint64_t t = t0 + (tile * MN_ROUNDS + rr) * 256 + threadIdx.x;
+        const uint32_t s = f ? occ_slot[t] & 0x7fffffffu : 0u;
+        const uint32_t tb = warp_bucket_of(TB.tab_off, nb + 1, s, f);
+        if (!f) continue;
+        const uint64_t n = base + wcnt[rr * NW + warp] + rank[rr];
+        slot_t<K>& e = TB.slots[s - TB.off0];
+        const K key = e.key;
+        const uint32_t om = e.om;
+        e.rank = (uint32_t)n;
+        n_key[n] = key;
+        n_meta[n] = (uint8_t)(om & 7u);
+        uint32_t rec = NONE32;
+        if (om & M_PRIMARY) rec = (om & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (om >> 4) - 1);
+        n_rec[n] = rec;
+        n_bucket[n] = TB.b0 + tb;
+    }
 }
 
-// Number the distinct k-mers in first-insertion order, scanning the
-// occurrences: occurrence t is the first of its k-mer iff bit t of `bits` is
-// set, and its node index is the number of first occurrences before it.  The
-// slot's rank field becomes the node index, and the node arrays are written
-// in node order.  The bucket is the slot's table (tab_off ascends over the batch's
-// buckets).  Reads are sequential except one slot per node.
+// Occurrences t0 .. t0 + nocc - 1: the slot index becomes the k-mer's node
+// index (bit 31, owned, kept), so later stages need no table.
 template <typename K>
-__global__ void __launch_bounds__(256) k_make_nodes(uint64_t nocc, uint32_t const* __restrict__ occ_slot,
-                                                    uint32_t const* __restrict__ bits,
-                                                    uint64_t const* __restrict__ wpre, slot_t<K>* __restrict__ slots,
-                                                    tables<K> TB, uint32_t nb, uint64_t R0,
-                                                    K* __restrict__ n_key,
-                                                    uint8_t* __restrict__ n_meta, uint32_t* __restrict__ n_rec,
-                                                    uint32_t* __restrict__ n_bucket) {
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t w = t < nocc ? bits[t >> 5] : 0u;
-    const bool first = (w >> (t & 31)) & 1u;
-    const uint32_t s = first ? occ_slot[t] & 0x7fffffffu : 0u;
-    // the slot's table: consecutive occurrences lie in one bucket's slot range
-    const uint32_t tb = warp_bucket_of(TB.tab_off, nb + 1, s, first);
-    if (!first) return;
-    const uint64_t n = wpre[t >> 5] + __popc(w & ((1u << (t & 31)) - 1u));
-    slot_t<K>& e = slots[s];
-    const K key = e.key;
-    const uint32_t om = e.om;
-    e.rank = (uint32_t)n;
-    n_key[n] = key;
-    n_meta[n] = (uint8_t)(om & 7u);
-    uint32_t rec = NONE32;
-    if (om & M_PRIMARY) rec = (om & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (om >> 4) - 1);
-    n_rec[n] = rec;
-    n_bucket[n] = TB.b0 + tb;
+__global__ void k_occ_nodes(uint64_t t0, uint64_t nocc, uint32_t* __restrict__ occ_slot,
+                            slot_t<K> const* __restrict__ slots, uint64_t off0) {
+    const uint64_t t = t0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= t0 + nocc) return;
+    const uint32_t v = occ_slot[t];
+    if (v == NONE32) return;
+    occ_slot[t] = slots[(v & 0x7fffffffu) - off0].rank | (v & 0x80000000u);
 }
 
 // Block-wide reservation of `want` consecutive entries of *cnt per thread,
@@ -511,7 +577,8 @@ __global__ void __launch_bounds__(OCC_BLOCK)
         if (t < nocc) {
             const uint32_t v = occ_slot[t];
             if (v != NONE32 && (v & 0x80000000u)) {
-                const uint32_t n = __ldg(slot_rank + (uint64_t)(v & 0x7fffffffu) * rank_stride);
+                const uint32_t n = slot_rank ? __ldg(slot_rank + (uint64_t)(v & 0x7fffffffu) * rank_stride)
+                                             : (v & 0x7fffffffu);
                 if (n_rec[n] == MULTI_TAG) {
                     // the record lies between this occurrence block's first record
                     // and the next one's (a few dozen records): search only there
@@ -1510,7 +1577,7 @@ __global__ void k_node_cid(uint64_t D, uint32_t const* __restrict__ n_rec, uint3
 template <typename K>
 __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb, K x) {
     const K EMPTY = kmer_ops<K>::empty();
-    const uint64_t off = T.tab_off[tb], cap = T.tab_cap[tb];
+    const uint64_t off = T.tab_off[tb] - T.off0, cap = T.tab_cap[tb];
     uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
     for (uint64_t i = 0; i < cap; ++i) {
         slot_t<K> const* e = &T.slots[off + s];
@@ -1530,11 +1597,14 @@ __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb,
     return NONE32;
 }
 
+// Nodes [*nb, *ne) (one bucket group's, numbered on the device).
 template <typename K>
-__global__ void __launch_bounds__(256, 8) k_ext_mask(uint64_t D, tables<K> T, K const* __restrict__ n_key,
-                           uint32_t const* __restrict__ n_bucket, uint32_t k, uint8_t* __restrict__ n_mask) {
-    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= D) return;
+__global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* nb, unsigned long long const* ne,
+                                                     tables<K> T, K const* __restrict__ n_key,
+                                                     uint32_t const* __restrict__ n_bucket, uint32_t k,
+                                                     uint8_t* __restrict__ n_mask) {
+    const uint64_t n = *nb + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= *ne) return;
     typedef kmer_ops<K> ops;
     const K can = n_key[n];
     const K msk = ops::mask(k);
@@ -1562,10 +1632,13 @@ __device__ __forceinline__ uint32_t back_nib(uint32_t m, bool rc) { return (rc ?
 // link[2n] = L port, link[2n+1] = R port: (node << 1) | rc of the state
 // reached, NONE32 when the step is not clean.
 template <typename K>
-__global__ void __launch_bounds__(256, 8) k_links(uint64_t D, tables<K> T, K const* __restrict__ n_key, uint32_t const* __restrict__ n_bucket,
-                        uint8_t const* __restrict__ n_mask, uint32_t k, uint32_t* __restrict__ link) {
-    uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= D) return;
+__global__ void __launch_bounds__(256, 8) k_links(unsigned long long const* nb, unsigned long long const* ne,
+                                                  tables<K> T, K const* __restrict__ n_key,
+                                                  uint32_t const* __restrict__ n_bucket,
+                                                  uint8_t const* __restrict__ n_mask, uint32_t k,
+                                                  uint32_t* __restrict__ link) {
+    const uint64_t n = *nb + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= *ne) return;
     typedef kmer_ops<K> ops;
     const K can = n_key[n];
     const uint32_t m = n_mask[n];
@@ -2083,6 +2156,7 @@ __global__ void k_add_offsets(uint64_t n, uint64_t const* __restrict__ src, uint
     if (i < n) dst[i] = src[i] + add;
 }
 __global__ void k_set_u64(uint64_t* p, uint64_t v) { *p = v; }
+__global__ void k_copy_u64(unsigned long long const* src, unsigned long long* dst) { *dst = *src; }
 __global__ void k_used_flags(uint64_t n, uint32_t const* __restrict__ first, uint32_t* __restrict__ keep) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) keep[i] = first[i] != NONE32 ? 1u : 0u;
@@ -2183,7 +2257,11 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     const uint64_t nocc = O1 - O0;
     if (nocc == 0) return;
     auto mark = A.mark();
-    // ---- tables
+    // ---- tables: one open-addressing table per bucket, processed in bucket
+    // groups whose tables fit in L2 (p.group_bytes): a group's tables are
+    // built, numbered and probed (insert, first occurrences, nodes, extension
+    // masks, links) while they are cache-resident, and the next group reuses
+    // their memory
     const uint32_t nb = b1 - b0;
     const uint64_t q = std::min<uint32_t>(16, std::max<uint32_t>(5, p.table_slots_q));
     std::vector<uint64_t> toff(nb + 1), tcap(nb);
@@ -2201,59 +2279,106 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     toff[nb] = T;
     if (T >= (1ull << 31)) throw std::runtime_error("k-mer table of one bucket batch exceeds 2^31 slots");
     if (nrec > MAX_BATCH_RECORDS) throw std::runtime_error("more than 2^28 - 2 records in one bucket");
+    const uint64_t gslots = std::max<uint64_t>(1024, p.group_bytes / sizeof(slot_t<K>));
+    std::vector<uint32_t> gb{0};  // group boundaries (batch-relative buckets)
+    for (uint32_t b = 1; b <= nb; ++b)
+        if (b == nb || toff[b + 1] - toff[gb.back()] > gslots) gb.push_back(b);
+    if (gb.back() != nb) gb.push_back(nb);
+    const size_t ng = gb.size() - 1;
+    uint64_t Tmax = 0;
+    for (size_t g = 0; g < ng; ++g) Tmax = std::max<uint64_t>(Tmax, toff[gb[g + 1]] - toff[gb[g]]);
     uint32_t* occ_slot = A.alloc<uint32_t>(nocc);
     uint64_t* d_toff = A.alloc<uint64_t>(nb + 1);
     uint64_t* d_tcap = A.alloc<uint64_t>(nb);
     CDBG_CUDA(cudaMemcpyAsync(d_toff, toff.data(), 8ull * (nb + 1), cudaMemcpyHostToDevice, st));
     CDBG_CUDA(cudaMemcpyAsync(d_tcap, tcap.data(), 8ull * nb, cudaMemcpyHostToDevice, st));
-    tables<K> TB;
-    TB.slots = A.alloc<slot_t<K>>(T);
-    TB.tab_off = d_toff;
-    TB.tab_cap = d_tcap;
-    TB.b0 = b0;
-    {
-        CDBG_PROF("k_init_tables", st);
-        k_init_tables<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots);
-    }
-    CDBG_CHECK_LAUNCH();
-    // ---- load
+    slot_t<K>* slots = A.alloc<slot_t<K>>(Tmax + 1);
     // record of each occurrence block's first occurrence (k_insert, k_multi_pairs)
     const uint64_t nblk = ceil_div(nocc, (uint64_t)OCC_BLOCK);
     uint32_t* blk_rec = A.alloc<uint32_t>(nblk + 1);
     k_block_records<<<grid(nrec, 256), 256, 0, st>>>(R.occ, R0, nrec, O0, nblk, blk_rec);
     CDBG_CHECK_LAUNCH();
-    {
-        CDBG_PROF("k_insert", st);
-        k_insert<K><<<grid(nocc, 256), 256, 0, st>>>(R, TB, R0, nrec, O0, nocc, k, blk_rec, occ_slot, d_err);
-    }
-    CDBG_CHECK_LAUNCH();
-    // ---- nodes in first-insertion order
     const uint64_t nwb = ceil_div(nocc, 32);
     uint32_t* bits = A.alloc<uint32_t>(nwb);
     CDBG_CUDA(cudaMemsetAsync(bits, 0, 4 * nwb, st));
-    {
-        CDBG_PROF("k_firstbits", st);
-        k_firstbits<K><<<grid(T, 256), 256, 0, st>>>(T, TB.slots, bits);
+    // node arrays, sized for the worst case (every occurrence a distinct
+    // k-mer): the groups number their nodes on the device, without a host
+    // round trip per group
+    K* n_key = A.alloc<K>(nocc);
+    uint8_t* n_meta = A.alloc<uint8_t>(nocc);
+    uint32_t* n_rec = A.alloc<uint32_t>(nocc);
+    uint32_t* n_bucket = A.alloc<uint32_t>(nocc);
+    uint8_t* n_mask = A.alloc<uint8_t>(nocc);
+    uint32_t* link = A.alloc<uint32_t>(2 * nocc);
+    // look-back state of every group's numbering, zeroed once
+    std::vector<uint64_t> gtile(ng + 1, 0);
+    for (size_t g = 0; g < ng; ++g)
+        gtile[g + 1] = gtile[g] + ceil_div(bocc[b0 + gb[g + 1]] - bocc[b0 + gb[g]], (uint64_t)MN_ROUNDS * 256);
+    unsigned long long* mn_status = A.alloc<unsigned long long>(gtile[ng] + 1);
+    uint32_t* mn_counter = A.alloc<uint32_t>(ng + 1);
+    unsigned long long* ncnt = A.alloc<unsigned long long>(2);  // node bases, alternating by group
+    CDBG_CUDA(cudaMemsetAsync(mn_status, 0, 8 * (gtile[ng] + 1), st));
+    CDBG_CUDA(cudaMemsetAsync(mn_counter, 0, 4 * (ng + 1), st));
+    CDBG_CUDA(cudaMemsetAsync(ncnt, 0, 16, st));
+    for (size_t g = 0; g < ng; ++g) {
+        const uint32_t g0 = gb[g], g1 = gb[g + 1];
+        const uint64_t t0 = bocc[b0 + g0] - O0, tn = bocc[b0 + g1] - bocc[b0 + g0];
+        const uint64_t Tg = toff[g1] - toff[g0];
+        if (tn == 0) {
+            // no occurrence: the next group starts from the same node count
+            k_copy_u64<<<1, 1, 0, st>>>(ncnt + (g & 1), ncnt + ((g + 1) & 1));
+            CDBG_CHECK_LAUNCH();
+            continue;
+        }
+        tables<K> TG;
+        TG.slots = slots;
+        TG.tab_off = d_toff + g0;
+        TG.tab_cap = d_tcap + g0;
+        TG.b0 = b0 + g0;
+        TG.off0 = toff[g0];
+        {
+            CDBG_PROF("k_init_tables", st);
+            k_init_tables<K><<<grid(Tg, 256), 256, 0, st>>>(Tg, slots);
+        }
+        CDBG_CHECK_LAUNCH();
+        {
+            CDBG_PROF("k_insert", st);
+            k_insert<K><<<grid(tn, 256), 256, 0, st>>>(R, TG, R0, nrec, O0, t0, tn, k, blk_rec, occ_slot, d_err);
+        }
+        CDBG_CHECK_LAUNCH();
+        {
+            CDBG_PROF("k_firstbits", st);
+            k_firstbits<K><<<grid(Tg, 256), 256, 0, st>>>(Tg, slots, bits);
+        }
+        CDBG_CHECK_LAUNCH();
+        unsigned long long* nbase = ncnt + (g & 1);
+        unsigned long long* nnext = ncnt + ((g + 1) & 1);
+        {
+            CDBG_PROF("k_make_nodes", st);
+            k_make_nodes<K><<<(unsigned)(gtile[g + 1] - gtile[g]), 256, 0, st>>>(
+                t0, tn, occ_slot, bits, TG, g1 - g0, R0, nbase, nnext, mn_counter + g, mn_status + gtile[g],
+                n_key, n_meta, n_rec, n_bucket, d_err);
+        }
+        CDBG_CHECK_LAUNCH();
+        {
+            CDBG_PROF("k_ext_mask", st);
+            k_ext_mask<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, TG, n_key, n_bucket, k, n_mask);
+        }
+        CDBG_CHECK_LAUNCH();
+        {
+            CDBG_PROF("k_links", st);
+            k_links<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, TG, n_key, n_bucket, n_mask, k, link);
+        }
+        CDBG_CHECK_LAUNCH();
+        {
+            CDBG_PROF("k_occ_nodes", st);
+            k_occ_nodes<K><<<grid(tn, 256), 256, 0, st>>>(t0, tn, occ_slot, slots, toff[g0]);
+        }
+        CDBG_CHECK_LAUNCH();
     }
-    CDBG_CHECK_LAUNCH();
-    uint32_t* wcnt = A.alloc<uint32_t>(nwb);
-    uint64_t* wpre = A.alloc<uint64_t>(nwb + 1);
-    k_popc<<<grid(nwb, 256), 256, 0, st>>>(nwb, bits, wcnt);
-    CDBG_CHECK_LAUNCH();
-    prim::exclusive_scan<uint32_t, uint64_t>(wcnt, wpre, nwb, A, st, wpre + nwb);
-    const uint64_t D = read_dev(wpre + nwb, st);
+    const uint64_t D = read_dev(ncnt + (ng & 1), st);
     if (D >= (1ull << 31)) throw std::runtime_error("too many distinct k-mers in one bucket batch");
     check_device_error_word(d_err, st, "k-mer table insert");
-    K* n_key = A.alloc<K>(D);
-    uint8_t* n_meta = A.alloc<uint8_t>(D);
-    uint32_t* n_rec = A.alloc<uint32_t>(D);
-    uint32_t* n_bucket = A.alloc<uint32_t>(D);
-    {
-        CDBG_PROF("k_make_nodes", st);
-        k_make_nodes<K><<<grid(nocc, 256), 256, 0, st>>>(nocc, occ_slot, bits, wpre, TB.slots, TB, nb, R0,
-                                                         n_key, n_meta, n_rec, n_bucket);
-    }
-    CDBG_CHECK_LAUNCH();
     // ---- multi-record k-mers: (node, record) pairs in one pass, at most one
     // per occurrence
     unsigned long long* cnt = A.alloc<unsigned long long>(1);
@@ -2268,11 +2393,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     {
         CDBG_PROF("k_multi_pairs", st);
         k_multi_pairs<<<(unsigned)mp_tiles, OCC_BLOCK, 0, st>>>(R.occ, R0, nrec, O0, nocc, blk_rec, occ_slot,
-                                                            reinterpret_cast<uint32_t const*>(
-                                                                reinterpret_cast<char const*>(TB.slots) +
-                                                                offsetof(slot_t<K>, rank)),
-                                                            (uint32_t)(sizeof(slot_t<K>) / 4), n_rec,
-                                                            tile_counter, status, cnt, pnode,
+                                                            nullptr, 0, n_rec, tile_counter, status, cnt, pnode,
                                                             prec, nocc, d_err);
     }
     CDBG_CHECK_LAUNCH();
@@ -2573,19 +2694,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         k_node_cid<<<grid(D, 256), 256, 0, st>>>(D, n_rec, (uint32_t)R0, rec_cand, nrc, mgrp, cid, n_cid);
     }
     CDBG_CHECK_LAUNCH();
-    // ---- extension masks, links, chains
-    uint8_t* n_mask = A.alloc<uint8_t>(D);
-    {
-        CDBG_PROF("k_ext_mask", st);
-        k_ext_mask<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, k, n_mask);
-    }
-    CDBG_CHECK_LAUNCH();
-    uint32_t* link = A.alloc<uint32_t>(2 * D);
-    {
-        CDBG_PROF("k_links", st);
-        k_links<K><<<grid(D, 256), 256, 0, st>>>(D, TB, n_key, n_bucket, n_mask, k, link);
-    }
-    CDBG_CHECK_LAUNCH();
+    // ---- chains (extension masks and links were made with the tables)
     chain_ws W;
     W.link = link;
     W.meta = n_meta;
@@ -2760,7 +2869,14 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     phase2_state local_state;
     phase2_state& S = out.state ? *out.state : local_state;
     class_dict dict(S);
-    dict.init(st);
+    if (p.keep_dict) {
+        dict.n = S.n;
+        dict.nbits = S.nbits;
+        dict.total_integers = S.total_integers;
+        dict.mask = S.mask;
+    } else {
+        dict.init(st);
+    }
     dvec<uint8_t>& dfrag = S.frag;
     dfrag.n = 0;
     uint32_t b = 0;
@@ -2778,11 +2894,15 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
         run_batch<K>(rs, R, p, s, b, bocc, A, st, d_err, dict, out, hbstart, rhash, dfrag);
     }
     // outputs
+    S.n = dict.n;
+    S.nbits = dict.nbits;
+    S.total_integers = dict.total_integers;
+    S.mask = dict.mask;
     out.n_classes = dict.n;
     out.nbits = dict.nbits;
     out.total_integers = dict.total_integers;
     const uint64_t nwords = (dict.nbits + 63) / 64;
-    if (p.to_host) {
+    if (p.to_host && p.copy_dict) {
         out.words.resize(nwords);
         out.offsets.resize(dict.n);
         if (nwords)

@@ -22,6 +22,8 @@ struct phase2_state {
     dvec<uint64_t> slot_hash;  // open-addressing table hash -> class
     dvec<uint32_t> slot_cid;
     dvec<uint8_t> frag;        // frag spill bytes (device-resident builds)
+    // dictionary size, kept so that a later call can continue it
+    uint64_t n = 0, nbits = 0, total_integers = 0, mask = 0;
     // Order later frees on `st` (after a stream switch).
     void set_stream(cudaStream_t st) {
         cls_hash.st_last = bit_off.st_last = words.st_last = slot_hash.st_last = st;
@@ -82,6 +84,17 @@ struct phase2_params {
     uint32_t heavy_colors = 64;
     // k-mer table slots per 4 occurrences of a bucket, 5..16 (performance only)
     uint32_t table_slots_q = 8;
+    // continue the class dictionary of the previous call on the same state
+    // (bucket ranges of one build processed call by call) instead of
+    // starting it empty
+    bool keep_dict = false;
+    // with to_host: copy the dictionary's words and offsets to the host
+    // (the last call of a range-by-range build only)
+    bool copy_dict = true;
+    // table bytes of one bucket group: the buckets of a batch are processed in
+    // groups whose tables fit in L2 (performance only; a bucket whose table
+    // alone is larger forms a group of its own)
+    uint64_t group_bytes = 64ull << 20;
     // Device-resident mode: fragment bytes of each batch are also copied to
     // this pinned host buffer on `copy_st` while later batches run, as long
     // as they fit in `frag_host_cap` (nothing is streamed when null).

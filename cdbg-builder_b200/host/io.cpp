@@ -20,6 +20,8 @@ int LZ4_compressBound(int inputSize);
 int LZ4_compress_default(const char* src, char* dst, int srcSize, int dstCapacity);
 int LZ4_decompress_safe(const char* src, char* dst, int compressedSize, int dstCapacity);
 }
+// LZ4's largest block input (lz4.h LZ4_MAX_INPUT_SIZE)
+static constexpr uint64_t LZ4_MAX_INPUT = 0x7E000000;
 
 namespace cdbg {
 namespace io {
@@ -253,21 +255,21 @@ bucket_file_set::~bucket_file_set() {
 std::string bucket_file_set::path(uint32_t b) const { return m_dir + "/bucket_" + std::to_string(b) + ".bin"; }
 
 void bucket_file_set::append_frames(uint8_t const* raw, uint64_t const* boff, uint32_t threads) {
-    // One frame per bucket slice, capped at 64 MiB of input per frame so the
-    // int-sized LZ4 API is never exceeded (records never straddle a frame:
-    // frame splits happen only at slice starts, which are record starts).
-    std::vector<uint64_t> comp(m_B, 0);
-    parallel_for(m_B, threads, [&](size_t b) {
-        uint64_t a = boff[b], e = boff[b + 1];
+    append_frames_range(raw, boff, 0, m_B, threads);
+}
+
+void bucket_file_set::append_frames_range(uint8_t const* raw, uint64_t const* boff, uint32_t b_lo, uint32_t b_hi,
+                                          uint32_t threads) {
+    // One LZ4 frame per bucket slice (records never straddle a frame: the
+    // slice is whole records of one device serialization).
+    std::vector<uint64_t> comp(b_hi - b_lo, 0);
+    parallel_for(b_hi - b_lo, threads, [&](size_t i) {
+        const size_t b = b_lo + i;
+        const uint64_t a = boff[b], e = boff[b + 1];
         if (a == e) return;
+        if (e - a > (uint64_t)LZ4_MAX_INPUT) throw std::runtime_error("bucket slice too large for one LZ4 frame");
         std::FILE* f = (std::FILE*)m_files[b];
         std::vector<char> out;
-        const uint64_t cap = 64ull << 20;
-        // split only at record boundaries: a slice above the cap is written
-        // as one frame per <= cap piece only when the caller's slice is
-        // already record aligned -- slices come from one device serialization
-        // per chunk, so the slice itself is the frame.
-        (void)cap;
         const int src = (int)(e - a);
         out.resize((size_t)LZ4_compressBound(src));
         int c = LZ4_compress_default((char const*)raw + a, out.data(), src, (int)out.size());
@@ -277,7 +279,7 @@ void bucket_file_set::append_frames(uint8_t const* raw, uint64_t const* boff, ui
             std::fwrite(out.data(), 1, (size_t)c, f) != (size_t)c)
             throw std::runtime_error("short write to " + path((uint32_t)b));
         m_unc[b] += (uint64_t)src;
-        comp[b] = 8 + (uint64_t)c;
+        comp[i] = 8 + (uint64_t)c;
     });
     for (uint64_t c : comp) m_comp += c;
 }
@@ -297,6 +299,38 @@ void bucket_file_set::close() {
 void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
                        std::function<uint8_t*(uint64_t)> const& alloc, bucket_bytes& out,
                        bool delete_after) {
+    read_bucket_range(dir, B, 0, B, threads, alloc, out);
+    if (delete_after) delete_bucket_files(dir, 0, B);
+}
+
+void delete_bucket_files(std::string const& dir, uint32_t b_lo, uint32_t b_hi) {
+    for (uint32_t b = b_lo; b < b_hi; ++b) {
+        std::error_code ec;
+        std::filesystem::remove(dir + "/bucket_" + std::to_string(b) + ".bin", ec);
+    }
+}
+
+std::vector<uint64_t> bucket_sizes(std::string const& dir, uint32_t B, uint32_t threads) {
+    std::vector<uint64_t> unc(B, 0);
+    parallel_for(B, threads, [&](size_t b) {
+        std::string p = dir + "/bucket_" + std::to_string(b) + ".bin";
+        std::FILE* f = std::fopen(p.c_str(), "rb");
+        if (!f) return;
+        uint32_t hdr[2];
+        while (std::fread(hdr, 4, 1, f) == 1 && hdr[0] != 0) {
+            if (std::fread(hdr + 1, 4, 1, f) != 1 || std::fseek(f, (long)hdr[1], SEEK_CUR) != 0) {
+                std::fclose(f);
+                throw std::runtime_error("short read of frame header on " + p);
+            }
+            unc[b] += hdr[0];
+        }
+        std::fclose(f);
+    });
+    return unc;
+}
+
+void read_bucket_range(std::string const& dir, uint32_t B, uint32_t b_lo, uint32_t b_hi, uint32_t threads,
+                       std::function<uint8_t*(uint64_t)> const& alloc, bucket_bytes& out) {
     struct frame {
         uint32_t u, c;
         long pos;
@@ -304,8 +338,9 @@ void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
     std::vector<std::vector<frame>> frames(B);
     std::vector<std::vector<char>> comp(B);
     out.bucket_unc.assign(B, 0);
-    // pass 1: read each file whole (compressed), index its frames
-    parallel_for(B, threads, [&](size_t b) {
+    // pass 1: read each file of the range whole (compressed), index its frames
+    parallel_for(b_hi - b_lo, threads, [&](size_t i) {
+        const size_t b = b_lo + i;
         std::string p = dir + "/bucket_" + std::to_string(b) + ".bin";
         std::FILE* f = std::fopen(p.c_str(), "rb");
         if (!f) return;  // a missing bucket file is an empty bucket
@@ -337,10 +372,6 @@ void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
             q += c;
             out.bucket_unc[b] += u;
         }
-        if (delete_after) {
-            std::error_code ec;
-            std::filesystem::remove(p, ec);
-        }
     });
     uint64_t total = 0;
     for (uint64_t u : out.bucket_unc) total += u;
@@ -361,7 +392,8 @@ void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
     }
     out.chunk_off.push_back(total);
     // pass 2: decompress in parallel into place
-    parallel_for(B, threads, [&](size_t b) {
+    parallel_for(b_hi - b_lo, threads, [&](size_t i) {
+        const size_t b = b_lo + i;
         uint64_t o = bstart[b];
         for (auto const& fr : frames[b]) {
             int d = LZ4_decompress_safe(comp[b].data() + fr.pos, (char*)out.data + o, (int)fr.c, (int)fr.u);

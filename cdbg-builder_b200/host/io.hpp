@@ -59,6 +59,9 @@ public:
     std::string path(uint32_t b) const;
     // raw: serialized records of all buckets; boff: B + 1 byte offsets.
     void append_frames(uint8_t const* raw, uint64_t const* boff, uint32_t threads);
+    // The same for buckets [b_lo, b_hi) only (raw + boff[b] is bucket b's slice).
+    void append_frames_range(uint8_t const* raw, uint64_t const* boff, uint32_t b_lo, uint32_t b_hi,
+                             uint32_t threads);
     // EOF markers, close; returns per-bucket uncompressed bytes.
     void close();
     std::vector<uint64_t> const& unc_bytes() const { return m_unc; }
@@ -85,6 +88,14 @@ struct bucket_bytes {
 void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
                        std::function<uint8_t*(uint64_t)> const& alloc, bucket_bytes& out,
                        bool delete_after);
+// The same for buckets [b_lo, b_hi) only (bucket_unc still has B entries,
+// zero outside the range; chunk_bucket holds absolute bucket numbers).
+void read_bucket_range(std::string const& dir, uint32_t B, uint32_t b_lo, uint32_t b_hi, uint32_t threads,
+                       std::function<uint8_t*(uint64_t)> const& alloc, bucket_bytes& out);
+// Uncompressed bytes of every bucket file, from its frame headers only.
+std::vector<uint64_t> bucket_sizes(std::string const& dir, uint32_t B, uint32_t threads);
+// Remove bucket files [b_lo, b_hi).
+void delete_bucket_files(std::string const& dir, uint32_t b_lo, uint32_t b_hi);
 
 // ---- .color_sets finalize layout (streaming_color_set_dict.hpp:221-294) ----
 // header [u32 C][u32 floor(.25C)][u32 floor(.75C)][u64 bits][u64 words],

@@ -66,6 +66,9 @@ typedef struct cdbg_tuning {
     uint32_t union_lists;      /* 1: multi-record color unions as sorted color
                                   lists, the path taken above 8192 colors
                                   (0 = C-bit bitmaps while C <= 8192) */
+    uint32_t table_group_mb;   /* k-mer table MiB per bucket group: a batch's
+                                  buckets are processed in groups whose
+                                  tables stay in L2 (default 64) */
 } cdbg_tuning;
 
 int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t);
@@ -180,9 +183,16 @@ typedef struct cdbg_phase2_args {
     const char* color_sets_path; /* finalized .color_sets, or NULL */
     cdbg_class_cb on_class;      /* may be NULL */
     void* ctx;
-    int32_t delete_consumed;     /* remove bucket files after reading */
+    int32_t delete_consumed;     /* remove each bucket file once its fragments
+                                    are written */
     uint32_t host_threads;
     uint64_t batch_occ;          /* k-mer occurrences per device batch (0 = auto) */
+    uint64_t pass_bytes;         /* uncompressed bucket bytes read per pass:
+                                    buckets are processed in consecutive ranges
+                                    of at most this size (a larger bucket is a
+                                    range of its own), the next range read on
+                                    host threads while the device processes
+                                    this one (0 = from free device memory) */
 } cdbg_phase2_args;
 
 typedef struct cdbg_phase2_stats {
@@ -195,6 +205,7 @@ typedef struct cdbg_phase2_stats {
     uint64_t total_integers;     /* sum of class sizes */
     uint64_t color_bits;         /* encoded bits of all classes */
     double seconds_total, seconds_device;
+    uint64_t n_passes;           /* bucket ranges processed */
 } cdbg_phase2_stats;
 
 int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats* s);

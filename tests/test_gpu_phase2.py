@@ -2,6 +2,7 @@
 oracle/_ref runs): frag_unitigs.bin and .color_sets must be byte-identical."""
 import filecmp
 import os
+import shutil
 
 import numpy as np
 import pytest
@@ -184,3 +185,45 @@ def test_pipelined_host_upload_matches_device_input():
     assert host[0] == dev[0]
     assert np.array_equal(host[1], dev[1]) and np.array_equal(host[2], dev[2])
     assert host[3:] == dev[3:]
+
+
+def test_phase2_range_by_range_matches_one_pass(engine, tmp_path):
+    """The drop-in phase 2 reads buckets range by range (the class
+    dictionary continues across ranges); with ranges of a few buckets each,
+    or a memory cap below the total bucket bytes, the frag file and
+    .color_sets equal the one-pass result and the reference's own
+    process_buckets, and delete_consumed leaves no bucket file behind."""
+    r2 = ref_bin("ref_phase2", 31)
+    lst = _fresh(tmp_path, 311, 12)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    B, k = 128, 31
+    bdir = tmp_path / "gb"
+    os.makedirs(bdir)
+    _, unc = engine.phase1(files, k, B, str(bdir))
+    total = int(unc.sum())
+    one = (str(tmp_path / "f1"), str(tmp_path / "c1"))
+    s1 = engine.phase2(str(bdir), B, k, 12, *one, pass_bytes=total * 2)
+    assert s1.n_passes == 1
+    many = (str(tmp_path / "f2"), str(tmp_path / "c2"))
+    s2 = engine.phase2(str(bdir), B, k, 12, *many, pass_bytes=max(1, total // 9))
+    assert s2.n_passes >= 9
+    for a, b in zip(one, many):
+        assert filecmp.cmp(a, b, shallow=False)
+    if r2:
+        run_ref([r2, str(bdir), str(B), str(k), "12", "1", str(tmp_path / "ref")])
+        assert filecmp.cmp(one[0], str(tmp_path / "ref" / "frag_unitigs.bin"), shallow=False)
+        assert filecmp.cmp(one[1], str(tmp_path / "ref" / "out.color_sets"), shallow=False)
+    # a memory cap below the bucket bytes: automatic ranges, same bytes, and
+    # every bucket file removed once its fragments are written
+    e2 = native.Engine(0)
+    try:
+        e2.set_memory_limit(max(total // 3, 64 << 20))
+        capped = (str(tmp_path / "f3"), str(tmp_path / "c3"))
+        copy = tmp_path / "gb2"
+        shutil.copytree(bdir, copy)
+        e2.phase2(str(copy), B, k, 12, *capped, delete_consumed=True, pass_bytes=max(1, total // 5))
+        for a, b in zip(one, capped):
+            assert filecmp.cmp(a, b, shallow=False)
+        assert not [f for f in os.listdir(copy) if f.startswith("bucket_")]
+    finally:
+        e2.close()
