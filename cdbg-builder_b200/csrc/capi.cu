@@ -757,9 +757,22 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
             throw std::runtime_error(std::string("short write to ") + a->frag_path);
         }
         ff = nullptr;
-        if (a->color_sets_path)
-            cdbg::io::write_color_sets(a->color_sets_path, a->num_colors, res.words.data(), res.nbits,
-                                       res.offsets.data(), res.n_classes);
+        if (a->color_sets_path) {
+            // the Elias-Fano finalize of the class offsets runs on the device,
+            // over the offsets the dictionary holds there
+            e->A.reset();
+            cdbg::ef_encoded ef;
+            cdbg::ef_encode(e->p2.bit_off.p, res.n_classes, res.nbits, e->A, e->st, ef);
+            std::vector<uint64_t> lh(ef.low_words + ef.high_words + 1);
+            if (ef.low_words)
+                CDBG_CUDA(cudaMemcpyAsync(lh.data(), ef.low, 8 * ef.low_words, cudaMemcpyDeviceToHost, e->st));
+            if (ef.high_words)
+                CDBG_CUDA(cudaMemcpyAsync(lh.data() + ef.low_words, ef.high, 8 * ef.high_words,
+                                          cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaStreamSynchronize(e->st));
+            cdbg::io::write_color_sets_ef(a->color_sets_path, a->num_colors, res.words.data(), res.nbits, ef.n,
+                                          ef.l, lh.data(), lh.data() + ef.low_words, ef.high_bits);
+        }
         if (a->on_class) {
             std::vector<uint32_t> cls;
             for (uint64_t c = 0; c < res.n_classes; ++c) {

@@ -405,48 +405,6 @@ void read_bucket_range(std::string const& dir, uint32_t B, uint32_t b_lo, uint32
     });
 }
 
-void write_color_sets(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
-                      uint64_t const* offsets, uint64_t nclasses) {
-    std::FILE* f = std::fopen(path.c_str(), "wb");
-    if (!f) throw std::runtime_error("cannot open color-set output: " + path);
-    const uint32_t st = (uint32_t)(0.25 * C), dt = (uint32_t)(0.75 * C);
-    const uint64_t nwords = (nbits + 63) / 64;
-    bool ok = std::fwrite(&C, 4, 1, f) == 1 && std::fwrite(&st, 4, 1, f) == 1 &&
-              std::fwrite(&dt, 4, 1, f) == 1 && std::fwrite(&nbits, 8, 1, f) == 1 &&
-              std::fwrite(&nwords, 8, 1, f) == 1;
-    if (ok && nwords) ok = std::fwrite(words, 8, nwords, f) == nwords;
-    // Elias-Fano over offsets[0..n) + the total bit count
-    const uint64_t n = nclasses + 1, U = nbits;
-    uint64_t l = 0;
-    if (U > n) {
-        const uint64_t q = U / n;
-        while ((uint64_t(1) << (l + 1)) <= q) ++l;
-    }
-    std::vector<uint64_t> low(((n * l) + 63) / 64, 0);
-    const uint64_t hbits = n + (U >> l) + 1;
-    std::vector<uint64_t> high((hbits + 63) / 64, 0);
-    for (uint64_t i = 0; i < n; ++i) {
-        const uint64_t v = i < nclasses ? offsets[i] : nbits;
-        if (l) {
-            const uint64_t pos = i * l, lo = v & ((uint64_t(1) << l) - 1);
-            low[pos >> 6] |= lo << (pos & 63);
-            if ((pos & 63) + l > 64) low[(pos >> 6) + 1] |= lo >> (64 - (pos & 63));
-        }
-        const uint64_t hp = (v >> l) + i;
-        high[hp >> 6] |= uint64_t(1) << (hp & 63);
-    }
-    auto wbv = [&](std::vector<uint64_t> const& w, uint64_t bits) {
-        const uint64_t sz = w.size();
-        ok = ok && std::fwrite(&bits, 8, 1, f) == 1 && std::fwrite(&sz, 8, 1, f) == 1;
-        if (ok && sz) ok = std::fwrite(w.data(), 8, sz, f) == sz;
-    };
-    ok = ok && std::fwrite(&U, 8, 1, f) == 1 && std::fwrite(&n, 8, 1, f) == 1 && std::fwrite(&l, 8, 1, f) == 1;
-    wbv(low, n * l);
-    wbv(high, hbits);
-    std::fclose(f);
-    if (!ok) throw std::runtime_error("short write to " + path);
-}
-
 void write_color_sets_ef(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
                          uint64_t nvalues, uint64_t l, uint64_t const* low, uint64_t const* high,
                          uint64_t high_bits) {

@@ -101,12 +101,9 @@ void delete_bucket_files(std::string const& dir, uint32_t b_lo, uint32_t b_hi);
 // header [u32 C][u32 floor(.25C)][u32 floor(.75C)][u64 bits][u64 words],
 // the words, then Elias-Fano of the class bit offsets plus the total, in the
 // layout of this project's `bits` stand-in (u64 universe, u64 n, u64 l, then
-// the low and high bit vectors each as [u64 num_bits][u64 num_words][words]).
-void write_color_sets(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
-                      uint64_t const* offsets, uint64_t nclasses);
-
-// The same file from an Elias-Fano encoding made elsewhere (on the device):
-// l low bits per value, the low and high bit vectors as words.
+// the low and high bit vectors each as [u64 num_bits][u64 num_words][words]),
+// the encoding made on the device (ef_encode): l low bits per value, the low
+// and high bit vectors as words.
 void write_color_sets_ef(std::string const& path, uint32_t C, uint64_t const* words, uint64_t nbits,
                          uint64_t nvalues, uint64_t l, uint64_t const* low, uint64_t const* high,
                          uint64_t high_bits);
