@@ -63,11 +63,13 @@ def parse():
                     help="also time one step of the plain one-bucket-per-batch path (default for skewed)")
     ap.add_argument("--out", default="")
     # serving workload
-    ap.add_argument("--requests", type=int, default=48, help="serving: requests in the stream")
+    ap.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
     ap.add_argument("--rate", type=float, default=30.0, help="serving: Poisson arrivals per second")
     ap.add_argument("--slots", default="1,2,3,4",
                     help="serving: concurrent builds; a list is swept and the best is reported")
     ap.add_argument("--no-plain", action="store_true", help="serving: skip the plain one-at-a-time run")
+    ap.add_argument("--plain-requests", type=int, default=48,
+                    help="serving: requests of the stream the plain one-at-a-time path serves")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
     ap.add_argument("--serving-buckets", type=int, default=1024)
     return ap.parse_args()
@@ -618,26 +620,37 @@ TRAFFIC_PER_UNIT = {
 
 
 # ---------------------------------------------------------------- serving
-def serving_requests(n_req, seed=7):
+def serving_requests(n_req, seed=7, host_bytes=0):
     """The serving stream's requests: per request its own seeded ancestor, 2-300
     genomes (log-uniform) of 0.5-8 Mbp (log-uniform), 0.1-2% divergence, k in
-    {31, 63}; returns [(seq, off, colors, n_genomes, k)] in pinned host memory."""
+    {31, 63}; returns ([(seq, off, colors, n_genomes, k, kmers)] in pinned
+    host memory, number of distinct collections).  When the collections of
+    all requests would not fit in `host_bytes` of host memory, the first ones
+    that fit are generated and the later requests submit them again in turn
+    (each submission is still a whole build)."""
     import numpy as np
     import torch
     from cdbg_gpu import synth
     rng = np.random.default_rng(seed)
-    out = []
+    shapes = []
     for i in range(n_req):
         n = int(round(np.exp(rng.uniform(np.log(2), np.log(300)))))
         k = int(rng.choice([31, 63]))
+        shapes.append((n, k))
+    out, used = [], 0
+    for i, (n, k) in enumerate(shapes):
         p, _, _, _ = synth.preset("serving", seed=10000 + i)
         seq, lens, per = synth.collection(p, n)
+        if host_bytes and out and used + seq.nbytes > host_bytes:
+            break
+        used += seq.nbytes
         off = np.zeros(len(lens) + 1, dtype=np.uint64)
         off[1:] = np.cumsum(lens)
         colors = np.repeat(np.arange(n, dtype=np.uint32), per)
         out.append((torch.from_numpy(seq).pin_memory(), torch.from_numpy(off.view(np.int64)).pin_memory(),
                     torch.from_numpy(colors.view(np.int32)).pin_memory(), n, k, count_kmers(lens, k)))
-    return out
+    distinct = len(out)
+    return [out[i % distinct] for i in range(n_req)], distinct
 
 
 def serve_stream(reqs, arrivals, slots, budget, B, batch_occ):
@@ -672,7 +685,12 @@ def main_serving(a):
     if rank != 0:
         return 0
     t = time.time()
-    reqs = serving_requests(a.requests)
+    try:
+        import psutil
+        host = int(psutil.virtual_memory().available * 0.4)
+    except Exception:
+        host = 64 << 30
+    reqs, distinct = serving_requests(a.requests, host_bytes=host)
     gen_s = time.time() - t
     rng = np.random.default_rng(11)
     arrivals = np.cumsum(rng.exponential(1.0 / a.rate, size=len(reqs)))
@@ -687,7 +705,8 @@ def main_serving(a):
 
     def summary(res, makespan, st):
         lat = np.array([x[0] for x in res])
-        return {"builds_per_s": len(res) / makespan, "kmers_per_s": kmers / makespan,
+        km = sum(r[5] for r in reqs[:len(res)])
+        return {"builds_per_s": len(res) / makespan, "kmers_per_s": km / makespan,
                 "makespan_s": makespan, "latency_p50_s": float(np.percentile(lat, 50)),
                 "latency_p99_s": float(np.percentile(lat, 99)),
                 "queue_wait_p50_s": float(np.percentile([x[1] for x in res], 50)),
@@ -698,15 +717,22 @@ def main_serving(a):
         by_slots[sl] = summary(*serve_stream(reqs, arrivals, sl, budget, B, 0))
     best = max(by_slots, key=lambda sl: by_slots[sl]["builds_per_s"])
     serving = dict(by_slots[best], slots=best)
-    plain = None if a.no_plain else summary(*serve_stream(reqs, arrivals, 1, budget, B, 1))
+    # the plain path (one request at a time, one bucket per batch) is an order
+    # of magnitude slower: it serves the stream's first requests only
+    npl = min(len(reqs), a.plain_requests)
+    plain = None if a.no_plain else summary(*serve_stream(reqs[:npl], list(arrivals[:npl]), 1, budget, B, 1))
+    if plain:
+        plain["requests"] = npl
+    one_slot = by_slots.get(1)
     line = {"metric": "serving builds/s", "value": serving["builds_per_s"], "unit": "builds/s",
             "n_gpus": 1, "higher_is_better": True, "dtype": "u64", "data": "synthetic",
             "config": {"workload": "serving: %d requests (Poisson %.1f/s), 2-300 genomes x 0.5-8 Mbp log-uniform, "
                                    "k in {31, 63}, %d buckets, slots %s, %.0f GB HBM budget"
                                    % (len(reqs), a.rate, B, a.slots, a.budget_gb),
-                       "total_kmers": kmers, "generate_s": gen_s},
+                       "total_kmers": kmers, "generate_s": gen_s, "distinct_collections": distinct},
             "serving": serving, "by_slots": by_slots, "plain_sequential": plain,
-            "speedup_vs_plain": (serving["builds_per_s"] / plain["builds_per_s"]) if plain else None}
+            "speedup_vs_plain": (serving["builds_per_s"] / plain["builds_per_s"]) if plain else None,
+            "speedup_vs_one_slot_batched": (serving["builds_per_s"] / one_slot["builds_per_s"]) if one_slot else None}
     print(json.dumps(line))
     if a.out:
         with open(a.out, "w") as f:

@@ -70,7 +70,8 @@ class Phase2Stats(ctypes.Structure):
 class BuildParams(ctypes.Structure):
     _fields_ = [("k", ctypes.c_uint32), ("m", ctypes.c_uint32), ("num_buckets", ctypes.c_uint32),
                 ("num_colors", ctypes.c_uint32), ("batch_occ", ctypes.c_uint64),
-                ("outputs_to_host", ctypes.c_int32)]
+                ("outputs_to_host", ctypes.c_int32), ("bucket_lo", ctypes.c_uint32),
+                ("bucket_hi", ctypes.c_uint32)]
 
 
 class BuildFilesArgs(ctypes.Structure):
@@ -92,6 +93,13 @@ class BuildResult(ctypes.Structure):
                 ("n_bases", ctypes.c_uint64),
                 ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
                 ("ms_total", ctypes.c_double)]
+
+
+class Merged(ctypes.Structure):
+    _fields_ = [("frag_bytes", ctypes.c_void_p), ("frag_nbytes", ctypes.c_uint64),
+                ("class_words", ctypes.c_void_p), ("class_bits", ctypes.c_uint64),
+                ("class_offsets", ctypes.c_void_p), ("n_color_sets", ctypes.c_uint64),
+                ("handle", ctypes.c_void_p)]
 
 
 class Tuning(ctypes.Structure):
@@ -178,6 +186,11 @@ SIGNATURES = {
     "cdbg_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
     "cdbg_server_destroy": (None, [ctypes.c_void_p]),
     "cdbg_server_last_error": (ctypes.c_char_p, []),
+    "cdbg_merge_shards": (ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), c_u64p,
+                                         ctypes.POINTER(ctypes.c_void_p), c_u64p,
+                                         ctypes.POINTER(ctypes.c_void_p), c_u64p, ctypes.c_void_p]),
+    "cdbg_merged_free": (None, [ctypes.c_void_p]),
+    "cdbg_merge_last_error": (ctypes.c_char_p, []),
 }
 
 _lib = None
@@ -418,8 +431,9 @@ class Engine:
         _check(lib().cdbg_gpu_build_files(self._h, ctypes.byref(a), ctypes.byref(r)))
         return r
 
-    def build(self, batch, k, num_buckets, num_colors, m=0, batch_occ=0, outputs_to_host=True):
-        p = BuildParams(k, m, num_buckets, num_colors, batch_occ, 1 if outputs_to_host else 0)
+    def build(self, batch, k, num_buckets, num_colors, m=0, batch_occ=0, outputs_to_host=True, buckets=None):
+        lo, hi = buckets if buckets else (0, 0)
+        p = BuildParams(k, m, num_buckets, num_colors, batch_occ, 1 if outputs_to_host else 0, lo, hi)
         r = BuildResult()
         _check(lib().cdbg_gpu_build(self._h, ctypes.byref(batch), ctypes.byref(p), ctypes.byref(r)))
         return r

@@ -1096,6 +1096,12 @@ int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phas
             if (redo) *redo = true;
             return 0;
         }
+        if (p->bucket_hi > p->bucket_lo) {
+            if (p->bucket_hi > p->num_buckets) throw std::runtime_error("bucket range beyond num_buckets");
+            cdbg::keep_bucket_range(sl, p->num_buckets, p->bucket_lo, p->bucket_hi, e->A, e->st);
+        } else if (p->bucket_lo || p->bucket_hi) {
+            throw std::runtime_error("empty bucket range");
+        }
         cdbg::record_set rs;
         cdbg::build_records(rt, sl, k, p->num_buckets, e->A, e->st, rs, e->d_err, e->P);
         e->last_rs = rs;  // for cdbg_engine_record_bytes (lives in P until the next call)

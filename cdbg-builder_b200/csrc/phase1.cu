@@ -22,6 +22,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1005,6 +1006,57 @@ void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev
                                                         out.bucket, out.key);
     }
     CDBG_CHECK_LAUNCH();
+}
+
+namespace {
+__device__ __forceinline__ uint32_t key_bucket(uint64_t key, uint32_t bb) {
+    return bb ? (uint32_t)(key >> (64 - bb)) : 0u;
+}
+__global__ void k_range_flags(uint64_t n, uint64_t const* __restrict__ key, uint32_t bb, uint32_t lo, uint32_t hi,
+                              uint32_t* __restrict__ keep) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = key_bucket(key[i], bb);
+    keep[i] = (b >= lo && b < hi) ? 1u : 0u;
+}
+template <typename T>
+__global__ void k_compact(uint64_t n, uint32_t const* __restrict__ keep, uint64_t const* __restrict__ pos,
+                          T const* __restrict__ in, T* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && keep[i]) out[pos[i]] = in[i];
+}
+}  // namespace
+
+void keep_bucket_range(super_list& sl, uint32_t B, uint32_t lo, uint32_t hi, dev_arena& A, cudaStream_t st) {
+    if (lo == 0 && hi >= B) return;
+    const uint64_t n = sl.n;
+    if (n == 0) return;
+    uint32_t bb = 0;
+    while ((1ull << bb) < B) ++bb;
+    uint32_t* keep = A.alloc<uint32_t>(n);
+    uint64_t* pos = A.alloc<uint64_t>(n + 1);
+    k_range_flags<<<grid(n, 256), 256, 0, st>>>(n, sl.key, bb, lo, hi, keep);
+    CDBG_CHECK_LAUNCH();
+    prim::exclusive_scan<uint32_t, uint64_t>(keep, pos, n, A, st, pos + n);
+    const uint64_t m = read_dev(pos + n, st);
+    super_list o = sl;
+    o.n = m;
+    auto pack = [&](auto* in, auto*& out) {
+        using T = std::remove_pointer_t<std::remove_reference_t<decltype(in)>>;
+        if (!in) return;
+        T* dst = A.alloc<T>(m + 1);
+        k_compact<T><<<grid(n, 256), 256, 0, st>>>(n, keep, pos, in, dst);
+        CDBG_CHECK_LAUNCH();
+        out = dst;
+    };
+    pack(sl.key, o.key);
+    pack(sl.packed, o.packed);
+    pack(sl.start, o.start);
+    pack(sl.len, o.len);
+    pack(sl.color, o.color);
+    pack(sl.flags, o.flags);
+    pack(sl.bucket, o.bucket);
+    sl = o;
 }
 
 void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, dev_arena& A,

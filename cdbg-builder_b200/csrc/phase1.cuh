@@ -78,6 +78,10 @@ struct super_list {
 void find_supers(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev_arena& A,
                  cudaStream_t st, super_list& out, uint32_t* d_err, uint32_t tile = 0, bool packed = false);
 
+// Keep only the super-k-mers of buckets [lo, hi) (input order kept), in new
+// arrays from A: one rank's share of a build split by bucket range.
+void keep_bucket_range(super_list& sl, uint32_t B, uint32_t lo, uint32_t hi, dev_arena& A, cudaStream_t st);
+
 // Dedup super-k-mers into canonical bucket records.
 // Record arrays come from `out`, temporaries from A.
 void build_records(run_table const& rt, super_list& sl, uint32_t k, uint32_t B, dev_arena& A,

@@ -1,0 +1,177 @@
+// Merging the outputs of a build split by bucket range across ranks (one GPU
+// each).  No counterpart in the reference, which builds in one process.
+//
+// Rank r of G builds buckets [B*r/G, B*(r+1)/G) of the whole collection: its
+// bucket records are exactly the single build's records of those buckets, so
+// its fragments are the single build's fragments of those buckets, in the same
+// order, except that their color-set ids are the rank's own (first appearance
+// within its buckets).  The single build numbers color sets by first
+// appearance over buckets 0..B-1, which is rank 0's classes in its order, then
+// rank 1's classes that rank 0 did not have, and so on.  A class is its
+// encoded bit string (the hybrid encoding of hybrid_color_sets.hpp:48-95 is a
+// function of the set and the color count), so the merge deduplicates bit
+// strings, appends each new one to the global bit vector, and rewrites the
+// ids in the fragment records (unitig_spill.hpp:642-665 layout).
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "cdbg_gpu.h"
+
+namespace {
+
+thread_local std::string t_err;
+
+uint64_t get_bits(uint64_t const* w, uint64_t pos, uint32_t n) {  // n <= 64
+    if (n == 0) return 0;
+    const uint64_t i = pos >> 6;
+    const uint32_t s = (uint32_t)(pos & 63);
+    uint64_t v = w[i] >> s;
+    if (s && s + n > 64) v |= w[i + 1] << (64 - s);
+    return n == 64 ? v : (v & ((uint64_t(1) << n) - 1));
+}
+
+struct bit_appender {
+    std::vector<uint64_t> w;
+    uint64_t n = 0;
+    void put(uint64_t v, uint32_t len) {  // len <= 64
+        if (len == 0) return;
+        if ((n >> 6) + 2 > w.size()) w.resize((n >> 6) + 2 + w.size() / 2, 0);
+        const uint32_t s = (uint32_t)(n & 63);
+        w[n >> 6] |= v << s;
+        if (s && s + len > 64) w[(n >> 6) + 1] |= v >> (64 - s);
+        n += len;
+    }
+};
+
+// Bits [a, b) of a shard's words as whole words from bit 0 (the key of a class).
+void extract(uint64_t const* w, uint64_t a, uint64_t b, std::vector<uint64_t>& out) {
+    out.assign((b - a + 63) / 64, 0);
+    for (uint64_t p = a, i = 0; p < b; p += 64, ++i) out[i] = get_bits(w, p, (uint32_t)std::min<uint64_t>(64, b - p));
+}
+
+uint64_t hash_words(std::vector<uint64_t> const& v, uint64_t nbits) {
+    uint64_t h = 0x9E3779B97F4A7C15ULL ^ nbits;
+    for (uint64_t x : v) {
+        h ^= x + 0x9E3779B97F4A7C15ULL + (h << 6) + (h >> 2);
+        h *= 0xff51afd7ed558ccdULL;
+    }
+    return h;
+}
+
+struct merged_out {
+    std::vector<uint8_t> frag;
+    std::vector<uint64_t> words;
+    std::vector<uint64_t> offsets;
+};
+
+}  // namespace
+
+extern "C" {
+
+int cdbg_merge_shards(uint32_t num_shards, const uint8_t* const* frag, const uint64_t* frag_nbytes,
+                      const uint64_t* const* class_words, const uint64_t* class_bits,
+                      const uint64_t* const* class_offsets, const uint64_t* n_classes, cdbg_merged* out) {
+    if (!out || (num_shards && (!frag || !frag_nbytes || !class_words || !class_bits || !class_offsets ||
+                                !n_classes))) {
+        t_err = "null argument";
+        return -1;
+    }
+    try {
+        auto* m = new merged_out();
+        try {
+            bit_appender gw;
+            std::unordered_multimap<uint64_t, uint64_t> seen;  // key hash -> global id
+            std::vector<uint64_t> key, other;
+            uint64_t total_frag = 0;
+            for (uint32_t s = 0; s < num_shards; ++s) total_frag += frag_nbytes[s];
+            m->frag.reserve(total_frag);
+            for (uint32_t s = 0; s < num_shards; ++s) {
+                const uint64_t nc = n_classes[s];
+                std::vector<uint64_t> map(nc);
+                for (uint64_t c = 0; c < nc; ++c) {
+                    const uint64_t a = class_offsets[s][c];
+                    const uint64_t b = c + 1 < nc ? class_offsets[s][c + 1] : class_bits[s];
+                    if (b < a || b > class_bits[s]) throw std::runtime_error("bad class offsets");
+                    extract(class_words[s], a, b, key);
+                    const uint64_t h = hash_words(key, b - a);
+                    uint64_t gid = UINT64_MAX;
+                    auto range = seen.equal_range(h);
+                    for (auto it = range.first; it != range.second && gid == UINT64_MAX; ++it) {
+                        const uint64_t g = it->second;
+                        const uint64_t ga = m->offsets[g];
+                        const uint64_t gb = g + 1 < m->offsets.size() ? m->offsets[g + 1] : gw.n;
+                        if (gb - ga != b - a) continue;
+                        extract(gw.w.data(), ga, gb, other);
+                        if (other == key) gid = g;
+                    }
+                    if (gid == UINT64_MAX) {
+                        gid = m->offsets.size();
+                        m->offsets.push_back(gw.n);
+                        for (uint64_t p = a; p < b; p += 64) {
+                            const uint32_t len = (uint32_t)std::min<uint64_t>(64, b - p);
+                            gw.put(get_bits(class_words[s], p, len), len);
+                        }
+                        seen.emplace(h, gid);
+                    }
+                    map[c] = gid;
+                }
+                // the shard's fragments with global ids
+                const uint8_t* d = frag[s];
+                const uint64_t n = frag_nbytes[s];
+                uint64_t p = 0;
+                while (p < n) {
+                    if (p + 5 > n) throw std::runtime_error("truncated fragment record");
+                    uint32_t nr;
+                    std::memcpy(&nr, d + p + 1, 4);
+                    const uint64_t q0 = m->frag.size();
+                    const uint64_t rec_end_runs = p + 5 + 12ull * nr;
+                    if (rec_end_runs + 4 > n) throw std::runtime_error("truncated fragment record");
+                    uint32_t sl;
+                    std::memcpy(&sl, d + rec_end_runs, 4);
+                    const uint64_t end = rec_end_runs + 4 + sl;
+                    if (end > n) throw std::runtime_error("truncated fragment record");
+                    m->frag.insert(m->frag.end(), d + p, d + end);
+                    for (uint32_t r = 0; r < nr; ++r) {
+                        uint64_t cid;
+                        std::memcpy(&cid, d + p + 5 + 12ull * r, 8);
+                        if (cid != UINT64_MAX) {  // a foreign run keeps its marker
+                            if (cid >= nc) throw std::runtime_error("fragment color-set id out of range");
+                            const uint64_t g = map[cid];
+                            std::memcpy(m->frag.data() + q0 + 5 + 12ull * r, &g, 8);
+                        }
+                    }
+                    p = end;
+                }
+            }
+            m->words.assign(gw.w.begin(), gw.w.begin() + (gw.n + 63) / 64);
+            out->frag_bytes = m->frag.data();
+            out->frag_nbytes = m->frag.size();
+            out->class_words = m->words.data();
+            out->class_bits = gw.n;
+            out->class_offsets = m->offsets.data();
+            out->n_color_sets = m->offsets.size();
+            out->handle = m;
+            return 0;
+        } catch (...) {
+            delete m;
+            throw;
+        }
+    } catch (std::exception const& ex) {
+        t_err = ex.what();
+        return -1;
+    }
+}
+
+void cdbg_merged_free(cdbg_merged* m) {
+    if (!m || !m->handle) return;
+    delete static_cast<merged_out*>(m->handle);
+    m->handle = nullptr;
+}
+
+const char* cdbg_merge_last_error(void) { return t_err.c_str(); }
+
+}  // extern "C"

@@ -216,6 +216,10 @@ typedef struct cdbg_build_params {
     uint32_t k, m, num_buckets, num_colors;
     uint64_t batch_occ;          /* 0 = auto */
     int32_t outputs_to_host;     /* 1 = copy frag bytes and color-set words to host */
+    /* Build only buckets [bucket_lo, bucket_hi) (both 0 = all): one rank's
+     * share of a build split by bucket range, whose outputs
+     * cdbg_merge_shards combines.  The rank still reads the whole input. */
+    uint32_t bucket_lo, bucket_hi;
 } cdbg_build_params;
 
 typedef struct cdbg_build_result {
@@ -258,6 +262,32 @@ typedef struct cdbg_build_files_args {
 } cdbg_build_files_args;
 
 int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_build_result* r);
+
+/* ---- builds split across ranks ----------------------------------------- */
+
+/* Merge the outputs of a build split by bucket range (cdbg_build_params
+ * bucket_lo/bucket_hi), shards given in bucket order, into the outputs of the
+ * whole build: the fragments back to back with their color-set ids rewritten
+ * to the whole build's ids, and the color-set bit vector and offsets of the
+ * whole build (its classes numbered by first appearance over all buckets, as
+ * one build numbers them).  Host only (no GPU needed).  No counterpart in
+ * the reference, which builds in one process.  The result's buffers belong to
+ * the library until cdbg_merged_free; errors via cdbg_merge_last_error(). */
+typedef struct cdbg_merged {
+    const uint8_t* frag_bytes;
+    uint64_t frag_nbytes;
+    const uint64_t* class_words;
+    uint64_t class_bits;
+    const uint64_t* class_offsets;
+    uint64_t n_color_sets;
+    void* handle;
+} cdbg_merged;
+
+int cdbg_merge_shards(uint32_t num_shards, const uint8_t* const* frag, const uint64_t* frag_nbytes,
+                      const uint64_t* const* class_words, const uint64_t* class_bits,
+                      const uint64_t* const* class_offsets, const uint64_t* n_classes, cdbg_merged* out);
+void cdbg_merged_free(cdbg_merged* m);
+const char* cdbg_merge_last_error(void);
 
 /* Serialized size of the bucket records of the engine's last cdbg_gpu_build
  * (the uncompressed bytes its bucket files would hold), counted on the device
