@@ -115,14 +115,18 @@ struct call_scope {
     cdbg_engine* e;
     cdbg::kernel_profiler* prev_prof;
     cdbg::host_mailbox* prev_mailbox;
-    explicit call_scope(cdbg_engine* en) : e(en), prev_prof(cdbg::g_prof), prev_mailbox(cdbg::g_mailbox) {
+    int prev_bits;
+    explicit call_scope(cdbg_engine* en)
+        : e(en), prev_prof(cdbg::g_prof), prev_mailbox(cdbg::g_mailbox), prev_bits(cdbg::g_radix_bits) {
         cdbg::g_prof = &e->prof;
         cdbg::g_mailbox = &e->mailbox;
+        cdbg::g_radix_bits = e->tune.radix_bits == 11 ? 11 : 8;
     }
     ~call_scope() {
         if (e->prof.on) e->prof.resolve();
         cdbg::g_prof = prev_prof;  // calls nest (the autotuner builds through the public entry)
         cdbg::g_mailbox = prev_mailbox;
+        cdbg::g_radix_bits = prev_bits;
     }
 };
 
@@ -201,6 +205,7 @@ std::atomic<uint64_t> g_launches{0};
 void set_last_error(std::string const& msg) { g_last_error = msg; }
 thread_local kernel_profiler* g_prof = nullptr;
 thread_local host_mailbox* g_mailbox = nullptr;
+thread_local int g_radix_bits = 8;
 
 void check_device_error(cdbg_engine* e, char const* stage) {
     uint32_t v = 0;
@@ -1357,6 +1362,11 @@ int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
         return -1;
     }
     if (v.table_group_mb == 0) v.table_group_mb = 64;
+    if (v.radix_bits == 0) v.radix_bits = 8;
+    if (v.radix_bits != 8 && v.radix_bits != 11) {
+        g_last_error = "radix_bits must be 8 or 11";
+        return -1;
+    }
     e->tune = v;
     return 0;
 }
@@ -1397,6 +1407,7 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
         if (cur.heavy_colors == 0) cur.heavy_colors = 64;
         if (cur.table_slots_q == 0) cur.table_slots_q = 8;
         if (cur.table_group_mb == 0) cur.table_group_mb = 64;
+        if (cur.radix_bits == 0) cur.radix_bits = 8;
         measure(cur);  // warm-up: allocations reach their working sizes
         double cur_ms = measure(cur);
         auto consider = [&](cdbg_tuning const& t) {
@@ -1430,6 +1441,11 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
             cdbg_tuning t = cur;
             t.table_group_mb = v;
             if (t.table_group_mb != cur.table_group_mb) consider(t);
+        }
+        for (uint32_t v : {8u, 11u}) {
+            cdbg_tuning t = cur;
+            t.radix_bits = v;
+            if (t.radix_bits != cur.radix_bits) consider(t);
         }
         e->tune = cur;
         if (best) *best = cur;

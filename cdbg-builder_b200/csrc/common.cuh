@@ -160,6 +160,9 @@ struct host_mailbox {
     size_t bytes = 0;
 };
 extern thread_local host_mailbox* g_mailbox;
+// Radix digit width of the sorts run by this host thread's current engine
+// call (8 or 11 bits; a performance knob, cdbg_tuning.radix_bits).
+extern thread_local int g_radix_bits;
 
 namespace {
 __global__ void k_mail_bytes(uint8_t const* __restrict__ src, uint8_t* __restrict__ dst, uint64_t n) {

@@ -472,16 +472,19 @@ int radix_sort_pairs_w(K* keys, V* vals, uint64_t n, int begin_bit, int end_bit,
     return ran;
 }
 
-// Stable sort of (keys, vals) by key bits [begin_bit, end_bit) with 8-bit
-// digits.  Results end in (keys, vals); the arena provides the ping-pong
-// buffers.  Needs a host synchronize (to read the digit histograms); returns
-// the number of passes run.  A look-back that gives up sets *err.
+// Stable sort of (keys, vals) by key bits [begin_bit, end_bit) with 8-bit or
+// 11-bit digits (g_radix_bits: the engine's tuning; 11 bits take 3 passes
+// where 8 bits take 4, with 8x the counters and look-back state per tile).
+// Results end in (keys, vals); the arena provides the ping-pong buffers.
+// Needs a host synchronize (to read the digit histograms); returns the number
+// of passes run.  A look-back that gives up sets *err.
 template <typename V, typename K = uint64_t>
 int radix_sort_pairs(K* keys, V* vals, uint64_t n, int begin_bit, int end_bit, dev_arena& A, cudaStream_t st,
                      uint32_t* err) {
     static_assert(sizeof(K) == 4 || sizeof(K) == 8, "u32 or u64 keys");
     if (end_bit > 8 * (int)sizeof(K)) end_bit = 8 * (int)sizeof(K);
     if (n <= 1 || end_bit <= begin_bit) return 0;
+    if (g_radix_bits == 11) return radix_sort_pairs_w<11, V, K>(keys, vals, n, begin_bit, end_bit, A, st, err);
     return radix_sort_pairs_w<RS_BITS, V, K>(keys, vals, n, begin_bit, end_bit, A, st, err);
 }
 

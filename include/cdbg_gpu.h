@@ -69,6 +69,7 @@ typedef struct cdbg_tuning {
     uint32_t table_group_mb;   /* k-mer table MiB per bucket group: a batch's
                                   buckets are processed in groups whose
                                   tables stay in L2 (default 64) */
+    uint32_t radix_bits;       /* radix sort digit width: 8 or 11 (default 8) */
 } cdbg_tuning;
 
 int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t);

@@ -65,3 +65,19 @@ def test_sparse_ties_take_the_run_fixup(engine):
     k = hi | lo
     k[1::5] = k[0::5]  # exact duplicates
     _check(engine, k)
+
+
+@pytest.mark.parametrize("n", [5000, 1_000_000])
+def test_eleven_bit_digits_give_the_same_order(engine, n):
+    """The radix_bits knob (11-bit digits: 3 passes where 8-bit digits take
+    4) sorts exactly alike."""
+    rng = np.random.default_rng(n + 1)
+    k = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+    k[::3] = k[1::3][: len(k[::3])] if len(k[1::3]) >= len(k[::3]) else k[::3]
+    engine.set_tuning(radix_bits=11)
+    try:
+        _check(engine, k)
+        hi = rng.integers(0, 1 << 20, size=n, dtype=np.uint64) << np.uint64(32)
+        _check(engine, hi | rng.integers(0, 8, size=n, dtype=np.uint64))
+    finally:
+        engine.set_tuning()
