@@ -23,6 +23,7 @@ int main(int argc, char**) {
     cdbg::gpu::ingest_bucketed(g, files, 31, 0, 1024, "tmp", 1, &unc);
     cdbg::streaming_color_set_dict d(4, "x.color_sets");
     cdbg::gpu::process_buckets(g, "tmp", 1024, 31, 4, "tmp/frag_unitigs.bin", d, false, 1);
+    cdbg::gpu::build_in_memory(g, files, 31, 0, 1024, "tmp/frag_unitigs.bin", "x.color_sets", 1);
 }
 '''
 
