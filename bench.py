@@ -53,6 +53,9 @@ def parse():
                     help="reference CPU runs: 1/N of every genome per step (rotating over the N slices)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--check", action="store_true",
+                    help="also check the benchmarked path's outputs on the reference arm's first sample "
+                         "against the reference's own phase 2 (one thread), byte for byte")
     ap.add_argument("--e2e-dir", default="", help="directory for the e2e input/output files (default: temp)")
     ap.add_argument("--batch-occ", type=int, default=0)
     ap.add_argument("--table-slots-q", type=int, default=0,
@@ -523,6 +526,35 @@ def main_gpu(a):
         finally:
             R.close()
 
+    # ---- parity of the benchmarked path on the reference arm's sample: the
+    # in-memory build from files against the reference's own process_buckets
+    # (one thread: deterministic ids and order) on this build's bucket files
+    check = None
+    if rank == 0 and a.check:
+        R = ReferenceSample(a.workload, n_genomes, a.ref_slices, os.cpu_count() or 1)
+        try:
+            lst, skm = R.slice(0)
+            sfiles = [l.strip() for l in open(lst) if l.strip()]
+            wd = os.path.join(R.work, "check")
+            bd = os.path.join(wd, "buckets")
+            os.makedirs(bd)
+            eng.phase1(sfiles, k, B, bd)
+            r2 = os.path.join(ROOT, "oracle", "_ref", "ref_phase2" + ("-largek" if k > 31 else ""))
+            t0 = time.time()
+            rr = subprocess.run([r2, bd, str(B), str(k), str(n_genomes), "1", os.path.join(wd, "ref")],
+                                capture_output=True, text=True)
+            ref_s = time.time() - t0
+            gf, gc = os.path.join(wd, "frag_unitigs.bin"), os.path.join(wd, "out.color_sets")
+            eng.build_files(sfiles, k, B, gf, gc)
+            same = lambda x, y: open(x, "rb").read() == open(y, "rb").read()
+            check = {"sample": R.describe(skm).split(";")[0].replace("slice i mod", "slice 0 of"),
+                     "kmers": skm, "ref_rc": rr.returncode, "ref_phase2_t1_s": ref_s,
+                     "frag_unitigs_equal": rr.returncode == 0 and same(gf, os.path.join(wd, "ref", "frag_unitigs.bin")),
+                     "color_sets_equal": rr.returncode == 0 and same(gc, os.path.join(wd, "ref", "out.color_sets")),
+                     "frag_bytes": os.path.getsize(gf)}
+        finally:
+            R.close()
+
     if rank == 0:
         top = sorted(kstats.items(), key=lambda kv: -kv[1][0])[:20]
         line = {"metric": "phase1+2 k-mers/s", "value": value, "unit": "k-mers/s", "n_gpus": world,
@@ -538,7 +570,7 @@ def main_gpu(a):
                 "phase_ms": {"phase1": r.ms_phase1, "phase2": r.ms_phase2},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_host": e2e_host,
                 "gpu_launches": int(launches),
-                "autotune": tuned, "plain": plain,
+                "autotune": tuned, "plain": plain, "check": check,
                 "clocks": clocks,
                 "kernels_ms_per_step": {kname: round(v[0] / a.steps, 3) for kname, v in top}}
         s = json.dumps(line)

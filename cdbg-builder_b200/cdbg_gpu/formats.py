@@ -170,8 +170,28 @@ def decode_class(words, pos, C):
     return [v for v in range(C) if v not in absent]
 
 
-def read_color_sets(path):
-    """(C, words ndarray, class offsets list, decoded classes list)."""
+def ef_values(low, high, n, l):
+    """The n values of an Elias-Fano sequence (l low bits each), vectorized."""
+    bits = np.unpackbits(np.asarray(high, dtype=np.uint64).view(np.uint8), bitorder="little")
+    pos = np.flatnonzero(bits)[:n].astype(np.uint64)
+    hi = pos - np.arange(len(pos), dtype=np.uint64)
+    if l == 0:
+        return hi
+    q = np.arange(len(pos), dtype=np.uint64) * np.uint64(l)
+    w = (q >> np.uint64(6)).astype(np.int64)
+    sh = q & np.uint64(63)
+    lw = np.append(np.asarray(low, dtype=np.uint64), np.uint64(0))
+    v = lw[w] >> sh
+    spill = sh + np.uint64(l) > np.uint64(64)
+    nxt = np.where(spill, lw[np.minimum(w + 1, len(lw) - 1)] << ((np.uint64(64) - sh) & np.uint64(63)),
+                   np.uint64(0))
+    lo = (v | nxt) & np.uint64((1 << l) - 1)
+    return (hi << np.uint64(l)) | lo
+
+
+def read_color_sets(path, decode=True):
+    """(C, words ndarray, class offsets list, decoded classes list, or None
+    without decode)."""
     with open(path, "rb") as f:
         data = f.read()
     C, st, dt, nbits, nwords = struct.unpack_from("<IIIQQ", data, 0)
@@ -188,28 +208,11 @@ def read_color_sets(path):
     hb, hw = struct.unpack_from("<QQ", data, p)
     p += 16
     high = np.frombuffer(data, dtype=np.uint64, count=hw, offset=p) if hw else np.zeros(0, np.uint64)
-    offs = []
-    i = 0
-    for wi in range(hw):
-        w = int(high[wi])
-        while w:
-            bit = (w & -w).bit_length() - 1
-            pos = wi * 64 + bit
-            hi = pos - i
-            lo = 0
-            if l:
-                q = i * l
-                lo = 0
-                for j in range(l):
-                    qq = q + j
-                    lo |= ((int(low[qq >> 6]) >> (qq & 63)) & 1) << j
-            offs.append((hi << l) | lo)
-            i += 1
-            w &= w - 1
+    offs = [int(x) for x in ef_values(low, high, n, l)]
     offsets = offs[:-1]
     if nwords == 0:
         words = np.zeros(1, dtype=np.uint64)
-    classes = [decode_class(np.append(words, np.uint64(0)), o, C) for o in offsets]
+    classes = [decode_class(np.append(words, np.uint64(0)), o, C) for o in offsets] if decode else None
     return C, words[:nwords], offsets, classes
 
 

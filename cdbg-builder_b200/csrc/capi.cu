@@ -737,7 +737,7 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
             pp.heavy_colors = e->tune.heavy_colors;
             pp.table_slots_q = e->tune.table_slots_q;
             pp.union_bitmaps = e->tune.union_lists == 0;
-            pp.group_bytes = (uint64_t)(e->tune.table_group_mb ? e->tune.table_group_mb : 64) << 20;
+            pp.group_bytes = e->tune.table_group_mb ? (uint64_t)e->tune.table_group_mb << 20 : ~0ull;
             pp.to_host = true;
             pp.keep_dict = i > 0;
             pp.copy_dict = i + 1 == nr;
@@ -1122,7 +1122,7 @@ int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phas
         pp.heavy_colors = e->tune.heavy_colors;
         pp.table_slots_q = e->tune.table_slots_q;
         pp.union_bitmaps = e->tune.union_lists == 0;
-        pp.group_bytes = (uint64_t)(e->tune.table_group_mb ? e->tune.table_group_mb : 64) << 20;
+        pp.group_bytes = e->tune.table_group_mb ? (uint64_t)e->tune.table_group_mb << 20 : ~0ull;
         pp.to_host = false;  // outputs accumulate in HBM
         if (p->outputs_to_host && e->h_frag.p && e->h_frag.cap) {
             // stream each batch's fragments into the (already large enough,
@@ -1361,7 +1361,6 @@ int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
         g_last_error = "union_lists must be 0 or 1";
         return -1;
     }
-    if (v.table_group_mb == 0) v.table_group_mb = 64;
     if (v.radix_bits == 0) v.radix_bits = 8;
     if (v.radix_bits != 8 && v.radix_bits != 11) {
         g_last_error = "radix_bits must be 8 or 11";
@@ -1406,7 +1405,6 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
         if (cur.minimizer_tile == 0) cur.minimizer_tile = 4096;
         if (cur.heavy_colors == 0) cur.heavy_colors = 64;
         if (cur.table_slots_q == 0) cur.table_slots_q = 8;
-        if (cur.table_group_mb == 0) cur.table_group_mb = 64;
         if (cur.radix_bits == 0) cur.radix_bits = 8;
         measure(cur);  // warm-up: allocations reach their working sizes
         double cur_ms = measure(cur);
@@ -1437,7 +1435,7 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
             t.table_slots_q = v;
             if (t.table_slots_q != cur.table_slots_q) consider(t);
         }
-        for (uint32_t v : {32u, 64u, 96u, 192u}) {
+        for (uint32_t v : {0u, 64u, 256u}) {
             cdbg_tuning t = cur;
             t.table_group_mb = v;
             if (t.table_group_mb != cur.table_group_mb) consider(t);

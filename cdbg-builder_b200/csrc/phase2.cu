@@ -2258,10 +2258,10 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     if (nocc == 0) return;
     auto mark = A.mark();
     // ---- tables: one open-addressing table per bucket, processed in bucket
-    // groups whose tables fit in L2 (p.group_bytes): a group's tables are
-    // built, numbered and probed (insert, first occurrences, nodes, extension
-    // masks, links) while they are cache-resident, and the next group reuses
-    // their memory
+    // groups of at most p.group_bytes of tables (one group per batch by
+    // default): a group's tables are built, numbered and probed (insert, first
+    // occurrences, nodes, extension masks, links) before the next group
+    // reuses their memory, so a group that fits in L2 stays cache-resident
     const uint32_t nb = b1 - b0;
     const uint64_t q = std::min<uint32_t>(16, std::max<uint32_t>(5, p.table_slots_q));
     std::vector<uint64_t> toff(nb + 1), tcap(nb);

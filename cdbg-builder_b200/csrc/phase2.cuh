@@ -92,9 +92,10 @@ struct phase2_params {
     // (the last call of a range-by-range build only)
     bool copy_dict = true;
     // table bytes of one bucket group: the buckets of a batch are processed in
-    // groups whose tables fit in L2 (performance only; a bucket whose table
-    // alone is larger forms a group of its own)
-    uint64_t group_bytes = 64ull << 20;
+    // groups whose tables fit in this size (performance only; a bucket whose
+    // table alone is larger forms a group of its own; the default is one group
+    // per batch)
+    uint64_t group_bytes = ~0ull;
     // Device-resident mode: fragment bytes of each batch are also copied to
     // this pinned host buffer on `copy_st` while later batches run, as long
     // as they fit in `frag_host_cap` (nothing is streamed when null).

@@ -67,8 +67,10 @@ typedef struct cdbg_tuning {
                                   lists, the path taken above 8192 colors
                                   (0 = C-bit bitmaps while C <= 8192) */
     uint32_t table_group_mb;   /* k-mer table MiB per bucket group: a batch's
-                                  buckets are processed in groups whose
-                                  tables stay in L2 (default 64) */
+                                  buckets are processed in groups of at most
+                                  this many table bytes, each built, numbered
+                                  and probed while cache-resident (0, the
+                                  default: one group per batch) */
     uint32_t radix_bits;       /* radix sort digit width: 8 or 11 (default 8) */
 } cdbg_tuning;
 

@@ -938,6 +938,34 @@ int oracle_phase1(char const* filelist, uint32_t k, uint32_t m, uint32_t B, char
     }
 }
 
+// k-mer occurrences per bucket (the super-k-mers' k-mers, before any
+// deduplication) of a filenames list: counts[B].  Test aid: shows how skewed
+// a workload's buckets are.
+int oracle_bucket_kmers(char const* filelist, uint32_t k, uint32_t m, uint32_t B, uint64_t* counts) {
+    try {
+        if (m == 0) m = best_m(k);
+        auto files = read_list(filelist);
+        for (uint32_t b = 0; b < B; ++b) counts[b] = 0;
+        std::vector<std::vector<uint8_t>> runs;
+        std::vector<super_occ> occ;
+        for (uint32_t c = 0; c < files.size(); ++c) {
+            for (auto const& s : read_sequences(files[c])) {
+                runs.clear();
+                acgt_runs(s, k, runs);
+                for (auto const& r : runs) {
+                    occ.clear();
+                    emit_supers(r.data(), (uint32_t)r.size(), k, m, B, c, occ);
+                    for (auto const& o : occ) counts[o.bucket] += o.len - k + 1;
+                }
+            }
+        }
+        return 0;
+    } catch (std::exception const& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 // Phase 2 over a directory of bucket files, buckets 0..B-1 in order (the
 // reference's process_buckets at one thread): writes <out_dir>/frag_unitigs.bin
 // and <out_dir>/out.color_sets (finalized).

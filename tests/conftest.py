@@ -35,6 +35,7 @@ class Oracle:
         L.oracle_phase1.argtypes = [cp, u32, u32, u32, cp, cp, vp, vp]
         L.oracle_phase2.argtypes = [cp, u32, u32, u32, cp, vp, vp, vp]
         L.oracle_last_error.restype = cp
+        L.oracle_bucket_kmers.argtypes = [cp, u32, u32, u32, vp]
         L.oracle_best_m.argtypes = [u32]
         L.oracle_best_m.restype = u32
         L.oracle_mhashes.argtypes = [vp, u32, u32, vp]
@@ -51,6 +52,14 @@ class Oracle:
         if rc:
             raise RuntimeError(self.L.oracle_last_error().decode())
         return ns.value, nk.value
+
+    def bucket_kmers(self, filelist, k, B, m=0):
+        """k-mer occurrences per bucket, before deduplication."""
+        import numpy as np
+        c = np.zeros(B, dtype=np.uint64)
+        if self.L.oracle_bucket_kmers(filelist.encode(), k, m, B, c.ctypes.data) != 0:
+            raise RuntimeError(self.L.oracle_last_error().decode())
+        return c
 
     def phase2(self, bucket_dir, B, k, C, out_dir):
         os.makedirs(out_dir, exist_ok=True)
