@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--batch-occ", type=int, default=0)
     ap.add_argument("--table-slots-q", type=int, default=0,
                     help="k-mer table slots per 4 occurrences, 5..16 (0 = library default)")
+    ap.add_argument("--tuning", default="", help='knobs of cdbg_tuning as JSON, e.g. {"minimizer_tile": 2048}')
     ap.add_argument("--autotune", action="store_true",
                     help="run the autotuner on the workload before timing (default for skewed)")
     ap.add_argument("--compare-plain", action="store_true",
@@ -376,8 +377,11 @@ def main_gpu(a):
 
     skewed = a.workload == "skewed"
     tuned = None
-    if a.table_slots_q:
-        eng.set_tuning(table_slots_q=a.table_slots_q)
+    if a.table_slots_q or a.tuning:
+        knobs = json.loads(a.tuning) if a.tuning else {}
+        if a.table_slots_q:
+            knobs["table_slots_q"] = a.table_slots_q
+        eng.set_tuning(**knobs)
     if a.autotune or skewed:
         t0 = time.time()
         tcfg, tms = eng.autotune(dev_batch, k, B, n_genomes)

@@ -477,22 +477,35 @@ __global__ void __launch_bounds__(256) k_make_nodes(uint64_t t0, uint64_t nocc, 
     }
     __syncthreads();
     const unsigned long long base = s_base;
+    // every round's slot loads go out before any store, so a thread keeps
+    // its MN_ROUNDS random slot reads in flight at once
+    uint32_t sl[MN_ROUNDS];
+#pragma unroll
+    for (int rr = 0; rr < MN_ROUNDS; ++rr) {
+        const uint64_t t = t0 + (tile * MN_ROUNDS + rr) * 256 + threadIdx.x;
+        sl[rr] = ((first >> rr) & 1u) ? __ldg(occ_slot + t) & 0x7fffffffu : 0u;
+    }
+    K key[MN_ROUNDS];
+    uint32_t om[MN_ROUNDS];
+#pragma unroll
+    for (int rr = 0; rr < MN_ROUNDS; ++rr) {
+        if ((first >> rr) & 1u) {
+            slot_t<K> const* e = TB.slots + (sl[rr] - TB.off0);
+            key[rr] = e->key;
+            om[rr] = e->om;
+        }
+    }
 #pragma unroll
     for (int rr = 0; rr < MN_ROUNDS; ++rr) {
         const bool f = (first >> rr) & 1u;
-        const uint64_t t = t0 + (tile * MN_ROUNDS + rr) * 256 + threadIdx.x;
-        const uint32_t s = f ? occ_slot[t] & 0x7fffffffu : 0u;
-        const uint32_t tb = warp_bucket_of(TB.tab_off, nb + 1, s, f);
+        const uint32_t tb = warp_bucket_of(TB.tab_off, nb + 1, sl[rr], f);
         if (!f) continue;
         const uint64_t n = base + wcnt[rr * NW + warp] + rank[rr];
-        slot_t<K>& e = TB.slots[s - TB.off0];
-        const K key = e.key;
-        const uint32_t om = e.om;
-        e.rank = (uint32_t)n;
-        n_key[n] = key;
-        n_meta[n] = (uint8_t)(om & 7u);
+        TB.slots[sl[rr] - TB.off0].rank = (uint32_t)n;
+        n_key[n] = key[rr];
+        n_meta[n] = (uint8_t)(om[rr] & 7u);
         uint32_t rec = NONE32;
-        if (om & M_PRIMARY) rec = (om & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (om >> 4) - 1);
+        if (om[rr] & M_PRIMARY) rec = (om[rr] & M_MULTI) ? MULTI_TAG : (uint32_t)(R0 + (om[rr] >> 4) - 1);
         n_rec[n] = rec;
         n_bucket[n] = TB.b0 + tb;
     }
@@ -2370,11 +2383,15 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             k_links<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, TG, n_key, n_bucket, n_mask, k, link);
         }
         CDBG_CHECK_LAUNCH();
-        {
-            CDBG_PROF("k_occ_nodes", st);
-            k_occ_nodes<K><<<grid(tn, 256), 256, 0, st>>>(t0, tn, occ_slot, slots, toff[g0]);
+        if (ng > 1) {
+            // the next group reuses this group's table memory: occurrences
+            // keep their node index instead of their slot
+            {
+                CDBG_PROF("k_occ_nodes", st);
+                k_occ_nodes<K><<<grid(tn, 256), 256, 0, st>>>(t0, tn, occ_slot, slots, toff[g0]);
+            }
+            CDBG_CHECK_LAUNCH();
         }
-        CDBG_CHECK_LAUNCH();
     }
     const uint64_t D = read_dev(ncnt + (ng & 1), st);
     if (D >= (1ull << 31)) throw std::runtime_error("too many distinct k-mers in one bucket batch");
@@ -2392,9 +2409,14 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(status, 0, 8 * mp_tiles, st));
     {
         CDBG_PROF("k_multi_pairs", st);
+        // one group: the table is still whole, and an occurrence's slot holds
+        // its node index (rank field); several: occ_slot holds node indices
+        uint32_t const* rankp = ng == 1 ? reinterpret_cast<uint32_t const*>(
+                                              reinterpret_cast<char const*>(slots) + offsetof(slot_t<K>, rank))
+                                        : nullptr;
         k_multi_pairs<<<(unsigned)mp_tiles, OCC_BLOCK, 0, st>>>(R.occ, R0, nrec, O0, nocc, blk_rec, occ_slot,
-                                                            nullptr, 0, n_rec, tile_counter, status, cnt, pnode,
-                                                            prec, nocc, d_err);
+                                                            rankp, (uint32_t)(sizeof(slot_t<K>) / 4), n_rec,
+                                                            tile_counter, status, cnt, pnode, prec, nocc, d_err);
     }
     CDBG_CHECK_LAUNCH();
     const uint64_t npairs = read_dev(cnt, st);

@@ -109,23 +109,95 @@ bool parse_fastx(char const* d, size_t n, std::function<void(char const*, size_t
 }
 
 std::string slurp(std::string const& path) {
+    // inflate straight into a buffer sized from the file's size hint (grown
+    // if the file inflates to more), no intermediate copy
+    const uint64_t hint = inflated_size_hint(path);
     gzFile f = gzopen(path.c_str(), "rb");
     if (!f) throw std::runtime_error("could not open input file: " + path);
-    gzbuffer(f, 1 << 20);
+    gzbuffer(f, 1 << 18);
     std::string out;
-    std::vector<char> buf(1 << 22);
+    out.resize((size_t)std::max<uint64_t>(hint, 4096) + 1);
+    size_t n = 0;
     for (;;) {
-        int r = gzread(f, buf.data(), (unsigned)buf.size());
+        if (n == out.size()) out.resize(out.size() * 2);
+        const size_t want = std::min<size_t>(out.size() - n, 1u << 30);
+        const int r = gzread(f, &out[n], (unsigned)want);
         if (r < 0) {
             gzclose(f);
             throw std::runtime_error("gzip read error on " + path);
         }
         if (r == 0) break;
-        out.append(buf.data(), (size_t)r);
+        n += (size_t)r;
     }
     gzclose(f);
+    out.resize(n);
     return out;
 }
+
+namespace {
+// FASTA records of d[0, n) with the same rules as parse_fastx, the sequence
+// bytes appended to `seq` and one length per record to `lens`, scanning lines
+// with memchr.  Returns false, with seq and lens left as they were, on a
+// header or line start that parse_fastx reads as FASTQ ('@' header or a '+'
+// line): the caller then parses the file with parse_fastx.
+bool parse_fasta_fast(char const* d, size_t n, std::string& seq, std::vector<uint64_t>& lens) {
+    const size_t seq0 = seq.size(), lens0 = lens.size();
+    auto fail = [&] {
+        seq.resize(seq0);
+        lens.resize(lens0);
+        return false;
+    };
+    size_t p = 0;
+    int last = 0;
+    for (;;) {
+        if (last == 0) {
+            while (p < n && d[p] != '>' && d[p] != '@') ++p;
+            if (p >= n) return true;
+            last = d[p++];
+        }
+        if (last == '@') return fail();
+        if (p >= n) return true;  // header char at EOF: nothing to read
+        char c = 0;
+        while (p < n && !is_space(d[p])) ++p;
+        if (p < n) c = d[p++];
+        if (c != '\n') {
+            void const* q = std::memchr(d + p, '\n', n - p);
+            p = q ? (size_t)((char const*)q - d) + 1 : n;
+        }
+        const size_t start = seq.size();
+        int cc = -1;
+        while (p < n) {
+            cc = (unsigned char)d[p++];
+            if (cc == '>' || cc == '+' || cc == '@') break;
+            cc = -1;
+            if (d[p - 1] == '\n') continue;
+            const size_t e = p - 1;
+            void const* q = std::memchr(d + p, '\n', n - p);
+            const size_t le = q ? (size_t)((char const*)q - d) : n;
+            seq.append(d + e, le - e);
+            p = le < n ? le + 1 : n;
+        }
+        if (cc == '+') return fail();
+        if (cc == '>' || cc == '@') last = cc;
+        lens.push_back(seq.size() - start);
+        if (cc == -1) return true;
+    }
+}
+
+// One input file inflated and parsed: sequence bytes back to back and one
+// length per record.
+void read_one(std::string const& path, std::string& seq, std::vector<uint64_t>& lens) {
+    std::string raw = slurp(path);
+    seq.clear();
+    lens.clear();
+    seq.reserve(raw.size());
+    if (parse_fasta_fast(raw.data(), raw.size(), seq, lens)) return;
+    parse_fastx(raw.data(), raw.size(), [&](char const* s, size_t l) {
+        seq.append(s, l);
+        lens.push_back(l);
+    });
+}
+}  // namespace
 
 void read_files(std::vector<std::string> const& files, size_t first, size_t count,
                 uint32_t color_base, uint32_t threads, seq_batch& out) {
@@ -140,12 +212,7 @@ void read_files(std::vector<std::string> const& files, size_t first, size_t coun
         std::error_code ec;
         auto sz = std::filesystem::file_size(path, ec);
         pf[i].disk = ec ? 0 : (uint64_t)sz;
-        std::string raw = slurp(path);
-        pf[i].seq.reserve(raw.size());
-        parse_fastx(raw.data(), raw.size(), [&](char const* s, size_t l) {
-            pf[i].seq.append(s, l);
-            pf[i].lens.push_back(l);
-        });
+        read_one(path, pf[i].seq, pf[i].lens);
     });
     uint64_t total = out.seq.size();
     for (auto const& f : pf) total += f.seq.size();
@@ -195,12 +262,7 @@ bool read_files_into(std::vector<std::string> const& files, size_t first, size_t
         std::error_code ec;
         auto sz = std::filesystem::file_size(path, ec);
         pf[i].disk = ec ? 0 : (uint64_t)sz;
-        std::string raw = slurp(path);
-        pf[i].seq.reserve(raw.size());
-        parse_fastx(raw.data(), raw.size(), [&](char const* s, size_t l) {
-            pf[i].seq.append(s, l);
-            pf[i].lens.push_back(l);
-        });
+        read_one(path, pf[i].seq, pf[i].lens);
     });
     std::vector<uint64_t> at(count + 1, 0);
     for (size_t i = 0; i < count; ++i) at[i + 1] = at[i] + pf[i].seq.size();

@@ -98,17 +98,18 @@ def _run_case(engine, oracle, tmp_path, name):
     return dict(k=k, B=B, lst=lst, words=ref_words, offs=ref_offs, nbits=int(r.class_bits), gb=gb, n=n)
 
 
-def _widest_classes(c, count=300):
-    """Color counts of the classes with the longest encodings."""
-    offs = np.asarray(list(c["offs"]) + [c["nbits"]], dtype=np.int64)
-    size = np.diff(offs)
+def _class_sizes(c, count=4000):
+    """Color counts of a random sample of the classes (the size leads each
+    class's encoding)."""
     w = np.append(c["words"], np.uint64(0))
-    return [len(formats.decode_class(w, int(offs[i]), c["n"])) for i in np.argsort(-size)[:count]]
+    offs = c["offs"]
+    idx = np.random.default_rng(0).choice(len(offs), size=min(count, len(offs)), replace=False)
+    return [formats.read_delta(formats._Bits(w, int(offs[i]))) for i in idx]
 
 
 def test_pangenome_cut_matches_reference(engine, oracle, tmp_path):
     c = _run_case(engine, oracle, tmp_path, "pangenome128")
-    assert max(_widest_classes(c)) >= 100             # classes hundreds of colors wide
+    assert max(_class_sizes(c)) >= 100                # classes a hundred colors wide and more
     heavy = 0
     for b in range(0, c["B"], 256):                   # records of >= 64 colors exist
         for _, cols, _ in formats.parse_records(formats.read_bucket_raw(str(c["gb"] / ("bucket_%d.bin" % b)))):
