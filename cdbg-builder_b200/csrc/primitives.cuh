@@ -239,7 +239,7 @@ struct rs_smem {
 };
 
 template <int BITS, int ITEMS, typename K, typename V>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(K const* __restrict__ keys_in,
+__global__ void __launch_bounds__(RS_THREADS, 3) k_rs_onesweep(K const* __restrict__ keys_in,
                                                             V const* __restrict__ vals_in,
                                                             K* __restrict__ keys_out, V* __restrict__ vals_out,
                                                             uint64_t n, int shift, uint32_t* tile_counter,

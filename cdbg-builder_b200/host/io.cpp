@@ -13,6 +13,10 @@
 #include <stdexcept>
 #include <thread>
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <unistd.h>
+
 extern "C" {
 // System LZ4 block API (liblz4.so.1), the functions the reference calls at
 // bucket_io.hpp:259-263 and :695.
@@ -281,21 +285,50 @@ bool read_files_into(std::vector<std::string> const& files, size_t first, size_t
 }
 
 void write_file_parallel(std::string const& path, uint8_t const* data, uint64_t n, uint32_t threads) {
-    std::FILE* f = std::fopen(path.c_str(), "wb");
-    if (!f) throw std::runtime_error("cannot open output file: " + path + ": " + std::strerror(errno));
-    std::fclose(f);
-    if (n == 0) return;
-    std::filesystem::resize_file(path, n);
-    const uint64_t piece = std::max<uint64_t>(64ull << 20, (n + threads - 1) / std::max<uint32_t>(threads, 1));
+    const int fd = ::open(path.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0) throw std::runtime_error("cannot open output file: " + path + ": " + std::strerror(errno));
+    if (n == 0) {
+        ::close(fd);
+        return;
+    }
+    if (::ftruncate(fd, (off_t)n) != 0) {
+        ::close(fd);
+        throw std::runtime_error("cannot size output file: " + path + ": " + std::strerror(errno));
+    }
+    const uint64_t piece = std::max<uint64_t>(32ull << 20, (n + threads - 1) / std::max<uint32_t>(threads, 1));
     const size_t np = (size_t)((n + piece - 1) / piece);
+    // threads copy disjoint ranges into a shared mapping of the file (buffered
+    // writes to one file serialize on its inode lock; page faults do not)
+    void* map = ::mmap(nullptr, n, PROT_READ | PROT_WRITE, MAP_SHARED, fd, 0);
+    if (map != MAP_FAILED) {
+        try {
+            parallel_for(np, threads, [&](size_t i) {
+                const uint64_t a = i * piece, b = std::min<uint64_t>(n, a + piece);
+                std::memcpy((uint8_t*)map + a, data + a, b - a);
+            });
+        } catch (...) {
+            ::munmap(map, n);
+            ::close(fd);
+            throw;
+        }
+        const bool ok = ::munmap(map, n) == 0;
+        if (::close(fd) != 0 || !ok) throw std::runtime_error("short write to " + path);
+        return;
+    }
+    std::atomic<bool> bad{false};
     parallel_for(np, threads, [&](size_t i) {
-        std::FILE* g = std::fopen(path.c_str(), "r+b");
-        if (!g) throw std::runtime_error("cannot open output file: " + path);
-        const uint64_t a = i * piece, b = std::min<uint64_t>(n, a + piece);
-        bool ok = std::fseek(g, (long)a, SEEK_SET) == 0 && std::fwrite(data + a, 1, b - a, g) == b - a;
-        ok = (std::fclose(g) == 0) && ok;
-        if (!ok) throw std::runtime_error("short write to " + path);
+        uint64_t a = i * piece;
+        const uint64_t b = std::min<uint64_t>(n, a + piece);
+        while (a < b) {
+            const ssize_t w = ::pwrite(fd, data + a, (size_t)std::min<uint64_t>(b - a, 1ull << 30), (off_t)a);
+            if (w <= 0) {
+                bad = true;
+                return;
+            }
+            a += (uint64_t)w;
+        }
     });
+    if (::close(fd) != 0 || bad) throw std::runtime_error("short write to " + path);
 }
 
 // ---------------------------------------------------------------- buckets
