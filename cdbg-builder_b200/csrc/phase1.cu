@@ -247,6 +247,54 @@ __device__ __forceinline__ uint64_t mz_window(uint64_t const* sw, uint32_t x) {
     return s ? (lo >> s) | (hi << (64 - s)) : lo;
 }
 
+// Rolling-hash tables of one tile, filled by threads 0..31: stab[j][b] =
+// [0] seed(b), [1] rol(seed(b), m), [2] ror(seed(b^3), 1), [3] rol(seed(b^3),
+// m-1), and tf/tr[(out << 2) | in] = one rolling step of base `out` leaving and
+// base `in` entering, forward and reverse-complement strand.
+__device__ __forceinline__ void mz_tables(uint64_t (*stab)[4], uint64_t* tf, uint64_t* tr, uint32_t m) {
+    if (threadIdx.x < 16) {
+        const uint32_t b = threadIdx.x & 3, j = threadIdx.x >> 2;
+        const uint64_t sb = nt_seed(b), sc = nt_seed(b ^ 3u);
+        stab[j][b] = j == 0 ? sb : j == 1 ? rol64(sb, m) : j == 2 ? ror64(sc, 1) : rol64(sc, m - 1);
+    } else if (threadIdx.x < 32) {
+        const uint32_t o = (threadIdx.x - 16) >> 2, i = threadIdx.x & 3;
+        tf[(o << 2) | i] = rol64(nt_seed(o), m) ^ nt_seed(i);
+        tr[(o << 2) | i] = ror64(nt_seed(o ^ 3u), 1) ^ rol64(nt_seed(i ^ 3u), m - 1);
+    }
+}
+
+// Canonical m-mer hashes h[0..nh) of a staged tile (h[q] = the m-mer at
+// stream offset rel0 + q of sw) into sh[mz_pad(q)]: thread c hashes the HC
+// m-mers from c * HC on, the first in Horner form (fwd = xor_i rol(seed(b_i),
+// m-1-i), rc = xor_i rol(seed(b_i ^ 3), i)), the others rolled with one
+// (out, in) table entry per strand.  Its bases sit in two 32-base register
+// windows, so every extraction in the unrolled loop is a constant shift.
+template <int HC>
+__device__ __forceinline__ void mz_hash(uint64_t const* sw, uint64_t* sh, uint64_t const (*stab)[4],
+                                        uint64_t const* tf, uint64_t const* tr, uint32_t rel0, uint32_t nh,
+                                        uint32_t m) {
+    const uint32_t q0 = threadIdx.x * HC;
+    if (q0 >= nh) return;
+    const uint32_t cnt = min((uint32_t)HC, nh - q0);
+    const uint32_t x0 = rel0 + q0;
+    const uint64_t wout = mz_window(sw, x0);         // bases q0 .. q0 + 31
+    const uint64_t win = mz_window(sw, x0 + m - 1);  // bases q0 + m - 1 .. + 31
+    uint64_t f = 0, rc = 0;
+    for (uint32_t i = 0; i < m; ++i) f = rol64(f, 1) ^ stab[0][(uint32_t)(wout >> (2 * i)) & 3u];
+    for (uint32_t i = m; i-- > 0;) rc = rol64(rc, 1) ^ stab[0][((uint32_t)(wout >> (2 * i)) & 3u) ^ 3u];
+    sh[mz_pad(q0)] = f <= rc ? f : rc;
+#pragma unroll
+    for (int j = 1; j < HC; ++j) {
+        if ((uint32_t)j < cnt) {
+            const uint32_t pr =
+                (((uint32_t)(wout >> (2 * (j - 1))) & 3u) << 2) | ((uint32_t)(win >> (2 * j)) & 3u);
+            f = rol64(f, 1) ^ tf[pr];
+            rc = ror64(rc, 1) ^ tr[pr];
+            sh[mz_pad(q0 + j)] = f <= rc ? f : rc;
+        }
+    }
+}
+
 // MODE 0: count the cuts of each tile (tile_count).  MODE 1: write them at
 // tile_off.  MODE 2: one pass -- tiles take indices in launch order from
 // tile_counter, publish their count in `status` and read their predecessors'
@@ -276,18 +324,7 @@ __global__ void __launch_bounds__(MZ_THREADS)
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint64_t s_tile, s_excl;
 
-    if (threadIdx.x < 16) {
-        // [0] seed(b), [1] rol(seed(b), m), [2] ror(seed(b^3), 1), [3] rol(seed(b^3), m-1):
-        // the terms of one rolling step, so the loop below has no variable rotations
-        const uint32_t b = threadIdx.x & 3, j = threadIdx.x >> 2;
-        const uint64_t sb = nt_seed(b), sc = nt_seed(b ^ 3u);
-        stab[j][b] = j == 0 ? sb : j == 1 ? rol64(sb, m) : j == 2 ? ror64(sc, 1) : rol64(sc, m - 1);
-    } else if (threadIdx.x < 32) {
-        // one rolling step of base `o` leaving and base `i` entering, both strands
-        const uint32_t o = (threadIdx.x - 16) >> 2, i = threadIdx.x & 3;
-        tf[(o << 2) | i] = rol64(nt_seed(o), m) ^ nt_seed(i);
-        tr[(o << 2) | i] = ror64(nt_seed(o ^ 3u), 1) ^ rol64(nt_seed(i ^ 3u), m - 1);
-    }
+    mz_tables(stab, tf, tr, m);
     uint64_t tile = blockIdx.x;
     if (MODE == 2) {
         if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -320,35 +357,8 @@ __global__ void __launch_bounds__(MZ_THREADS)
         return;
     }
     const uint32_t rel0 = (uint32_t)(pa - wa * 32);  // stream offset of base e0 in sw
-    // canonical m-mer hashes h[0..nh) (h[q] = m-mer at base e0 + q): thread c
-    // hashes the HC m-mers from c * HC on, the first in Horner form
-    // (fwd = xor_i rol(seed(b_i), m-1-i), rc = xor_i rol(seed(b_i ^ 3), i)),
-    // the others rolled with one (out, in) table entry per strand.  Its bases
-    // sit in two 32-base register windows, so every extraction in the unrolled
-    // loop is a constant shift.
-    {
-        const uint32_t q0 = threadIdx.x * HC;
-        if (q0 < nh) {
-            const uint32_t cnt = min((uint32_t)HC, nh - q0);
-            const uint32_t x0 = rel0 + q0;
-            const uint64_t wout = mz_window(sw, x0);          // bases q0 .. q0 + 31
-            const uint64_t win = mz_window(sw, x0 + m - 1);   // bases q0 + m - 1 .. + 31
-            uint64_t f = 0, rc = 0;
-            for (uint32_t i = 0; i < m; ++i) f = rol64(f, 1) ^ stab[0][(uint32_t)(wout >> (2 * i)) & 3u];
-            for (uint32_t i = m; i-- > 0;) rc = rol64(rc, 1) ^ stab[0][((uint32_t)(wout >> (2 * i)) & 3u) ^ 3u];
-            sh[mz_pad(q0)] = f <= rc ? f : rc;
-#pragma unroll
-            for (int j = 1; j < HC; ++j) {
-                if ((uint32_t)j < cnt) {
-                    const uint32_t pr = (((uint32_t)(wout >> (2 * (j - 1))) & 3u) << 2) |
-                                        ((uint32_t)(win >> (2 * j)) & 3u);
-                    f = rol64(f, 1) ^ tf[pr];
-                    rc = ror64(rc, 1) ^ tr[pr];
-                    sh[mz_pad(q0 + j)] = f <= rc ? f : rc;
-                }
-            }
-        }
-    }
+    // canonical m-mer hashes h[0..nh) (h[q] = m-mer at base e0 + q)
+    mz_hash<HC>(sw, sh, stab, tf, tr, rel0, nh, m);
     __syncthreads();
     // sliding minimum smin[q] = min h[q .. q + W - 1] by segments of W hashes
     // (van Herk / Gil-Werman): with suf[q] the minimum from q to the end of its
@@ -460,6 +470,134 @@ __global__ void __launch_bounds__(MZ_THREADS)
             out_min[o] = smin[c + off];
             out_run[o] = r;
             out_a[o] = (uint32_t)(j0 + c);
+        }
+    }
+}
+
+// The one-pass form (MODE 2) for a window known at compile time (W = k - m:
+// 19 for k = 31 and 49 for k = 63 with the default m), 4096 (k-1)-mers per
+// tile.  After the hashes are staged in shared memory, each thread takes 16
+// consecutive (k-1)-mers and finds their window minima in registers: the
+// suffix minima of its own 16 hashes, then one running prefix minimum over
+// the W - 1 hashes after them, which closes one window per step once it
+// reaches past the own 16 (van Herk with the thread's block as the segment).
+// The thread also knows the window minimum of the position before its first,
+// so it finds its cuts alone; a block scan of the per-thread cut counts and
+// the tile look-back place them in order.  No per-position minimum array and
+// no stage barriers beyond the hash staging: shared memory is the staged words
+// and the hashes only.
+constexpr int MZR_C = 16;
+constexpr int MZR_TT = MZ_THREADS * MZR_C;
+template <int W>
+__global__ void __launch_bounds__(MZ_THREADS)
+    k_minimizers_reg(uint32_t nruns, uint64_t const* __restrict__ tile_start, uint64_t const* __restrict__ soff,
+                     uint32_t const* __restrict__ len, uint64_t const* __restrict__ words, uint32_t k, uint32_t m,
+                     uint64_t* __restrict__ out_min, uint32_t* __restrict__ out_run, uint32_t* __restrict__ out_a,
+                     uint32_t* err, uint32_t* tile_counter, unsigned long long* status, uint64_t ntiles,
+                     uint64_t cap) {
+    static_assert(W >= 18 && W <= 62, "window of 18..62 m-mers");
+    using LY = mz_layout<MZR_TT>;
+    constexpr int HC = (LY::HMAX + MZ_THREADS - 1) / MZ_THREADS;
+    extern __shared__ __align__(16) uint64_t mz_dyn[];
+    uint64_t* sw = mz_dyn;
+    uint64_t* sh = mz_dyn + LY::WMAX;
+    __shared__ uint64_t stab[4][4];
+    __shared__ uint64_t tf[16], tr[16];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint64_t s_tile, s_excl;
+    __shared__ uint32_t s_run;
+    __shared__ uint32_t sws[MZ_THREADS / 32 + 1];
+    mz_tables(stab, tf, tr, m);
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= ntiles) return;
+    if (threadIdx.x == 0) s_run = upper_bound_u64(tile_start, nruns + 1, tile) - 1;
+    __syncthreads();
+    const uint32_t r = s_run;
+    const uint64_t t_local = tile - tile_start[r];
+    const uint32_t L = len[r];
+    const uint64_t nk1 = (uint64_t)L - k + 2;  // (k-1)-mers 0..K
+    const uint64_t j0 = t_local * MZR_TT;
+    const uint64_t j1 = (j0 + MZR_TT < nk1) ? j0 + MZR_TT : nk1;
+    const uint64_t e0 = j0 ? j0 - 1 : 0;
+    const uint32_t nmin = (uint32_t)(j1 - e0);
+    const uint32_t nh = nmin + W - 1;
+    // bases [e0, j1 + k - 2) of the run
+    const uint64_t pa = soff[r] + e0;
+    const uint64_t pb = soff[r] + j1 + k - 2;
+    const uint64_t wa = (pa >> 5) & ~uint64_t(1);
+    const uint64_t wb = ((pb + 31) >> 5) + 1;
+    const uint32_t nw = (uint32_t)(((wb - wa) + 1) & ~uint64_t(1));
+    if (!tma_load_1d(sw, words + wa, nw * 8u, &bar, err)) {  // uniform across the block
+        if (threadIdx.x == 0) atomicExch(&status[tile], (2ull << 62));  // unblock successors
+        return;
+    }
+    mz_hash<HC>(sw, sh, stab, tf, tr, (uint32_t)(pa - wa * 32), nh, m);
+    __syncthreads();
+    const uint32_t ncut = (uint32_t)(j1 - j0);
+    const uint32_t c0 = threadIdx.x * MZR_C;       // first (k-1)-mer of this thread, from j0
+    const uint32_t p0 = (uint32_t)(j0 - e0) + c0;  // its hash index
+    uint64_t mn[MZR_C];
+    uint32_t mask = 0;
+    if (c0 < ncut) {
+        uint64_t run = ~0ull;
+#pragma unroll
+        for (int o = MZR_C - 1; o >= 0; --o) {
+            const uint64_t v = sh[mz_pad(p0 + o)];
+            run = v < run ? v : run;
+            mn[o] = run;
+        }
+        const uint64_t own = run;  // minimum of the own 16 hashes
+        uint64_t P = ~0ull, Pprev = ~0ull;
+#pragma unroll
+        for (int j = 0; j < W - 1; ++j) {
+            const uint64_t v = sh[mz_pad(p0 + MZR_C + j)];
+            P = v < P ? v : P;
+            if (j == W - 18) Pprev = P;
+            if (j >= W - 17) {
+                const int o = j - (W - 17);
+                mn[o] = mn[o] < P ? mn[o] : P;
+            }
+        }
+        // window [p0 - 1, p0 + W - 2]: the hash before, the own 16, then the
+        // first W - 18 hashes after them
+        uint64_t prev = ~0ull;
+        if (p0 > 0) {
+            const uint64_t hb = sh[mz_pad(p0 - 1)];
+            prev = hb < own ? hb : own;
+            prev = prev < Pprev ? prev : Pprev;
+        }
+#pragma unroll
+        for (int o = 0; o < MZR_C; ++o) {
+            const uint32_t c = c0 + o;
+            const uint64_t before = o ? mn[o - 1] : prev;
+            if (c < ncut && (j0 + c == 0 || mn[o] != before)) mask |= 1u << o;
+        }
+    }
+    uint32_t tot;
+    const uint32_t ex = prim::block_exclusive_scan<uint32_t, MZ_THREADS>(__popc(mask), sws, tot);
+    if (threadIdx.x < 32) {
+        uint64_t excl = 0;
+        const bool ok = prim::lookback_exclusive(status, tile, tot, excl);
+        if (threadIdx.x == 0) {
+            if (!ok) set_error(err, ERR_CHAIN_LIMIT);
+            s_excl = ok ? excl : ~0ull;
+        }
+    }
+    __syncthreads();
+    const uint64_t base = s_excl;
+    if (base == ~0ull) return;
+    uint64_t at = base + ex;
+#pragma unroll
+    for (int o = 0; o < MZR_C; ++o) {
+        if ((mask >> o) & 1u) {
+            if (at < cap) {
+                out_min[at] = mn[o];
+                out_run[at] = r;
+                out_a[at] = (uint32_t)(j0 + c0 + o);
+            }
+            ++at;
         }
     }
 }
@@ -957,9 +1095,19 @@ void find_supers_tt(run_table const& rt, uint32_t k, uint32_t m, uint32_t B, dev
     CDBG_CUDA(cudaMemsetAsync(counter, 0, 4, st));
     {
         CDBG_PROF("k_minimizers", st);
-        k_minimizers<2, TT><<<(unsigned)ntiles, MZ_THREADS, mz_smem<2, TT>(), st>>>(rt.n, tstart, rt.soff, rt.len, rt.words, k, m,
-                                                                 nullptr, nullptr, minv, run, aa, d_err, counter,
-                                                                 status, ntiles, cap);
+        // the register-window form for the two windows of the default m
+        // (k = 31 and k = 63); the shared-memory form otherwise
+        constexpr size_t reg_smem = sizeof(uint64_t) * (mz_layout<MZR_TT>::WMAX + mz_layout<MZR_TT>::HPAD);
+        if (TT == MZR_TT && k - m == 19)
+            k_minimizers_reg<19><<<(unsigned)ntiles, MZ_THREADS, reg_smem, st>>>(
+                rt.n, tstart, rt.soff, rt.len, rt.words, k, m, minv, run, aa, d_err, counter, status, ntiles, cap);
+        else if (TT == MZR_TT && k - m == 49)
+            k_minimizers_reg<49><<<(unsigned)ntiles, MZ_THREADS, reg_smem, st>>>(
+                rt.n, tstart, rt.soff, rt.len, rt.words, k, m, minv, run, aa, d_err, counter, status, ntiles, cap);
+        else
+            k_minimizers<2, TT><<<(unsigned)ntiles, MZ_THREADS, mz_smem<2, TT>(), st>>>(
+                rt.n, tstart, rt.soff, rt.len, rt.words, k, m, nullptr, nullptr, minv, run, aa, d_err, counter,
+                status, ntiles, cap);
     }
     CDBG_CHECK_LAUNCH();
     uint64_t n = read_dev(status + ntiles - 1, st) & ((1ull << 62) - 1);
