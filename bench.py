@@ -163,6 +163,22 @@ def peaks():
 
 
 # ---------------------------------------------------------------- reference arm
+def scratch_base(want_bytes=40 << 30):
+    """Where both arms keep their input and output files: a RAM-backed file
+    system when the host has one with room (the outputs of a step are several
+    GB; written to a disk, steps back to back end up waiting on its write-back,
+    which neither arm's own work decides), else the default temporary
+    directory."""
+    d = "/dev/shm"
+    try:
+        st = os.statvfs(d)
+        if os.access(d, os.W_OK) and st.f_bavail * st.f_frsize >= want_bytes:
+            return d
+    except OSError:
+        pass
+    return None
+
+
 def write_slice(seq, lens, per, s, nslices, k, out_dir, threads):
     """Slice s of nslices of every genome of a collection (bases [s*T/S,
     (s+1)*T/S) of each genome's concatenated contigs, contig boundaries kept),
@@ -240,7 +256,7 @@ class ReferenceSample:
         self.B = 1 << blog2
         self.n, self.S, self.threads = n_genomes, nslices, threads
         self.seq, self.lens, self.per = synth.collection(p, n_genomes)
-        self.work = tempfile.mkdtemp(prefix="cdbg_ref_")
+        self.work = tempfile.mkdtemp(prefix="cdbg_ref_", dir=scratch_base())
         self.slices = {}
 
     def slice(self, s):
@@ -257,8 +273,9 @@ class ReferenceSample:
 
     def describe(self, kmers):
         return ("slice i mod %d (1/%d of every one of the %d genomes, gzip FASTA) per step, ~%d k-mers; "
-                "reference ingest_bucketed + close + process_buckets with -t %d, -b %d" % (
-                    self.S, self.S, self.n, kmers, self.threads, self.B.bit_length() - 1))
+                "reference ingest_bucketed + close + process_buckets with -t %d, -b %d, files in %s" % (
+                    self.S, self.S, self.n, kmers, self.threads, self.B.bit_length() - 1,
+                    os.path.dirname(self.work)))
 
     def close(self):
         shutil.rmtree(self.work, ignore_errors=True)
@@ -437,7 +454,7 @@ def main_gpu(a):
     e2e = None
     e2e_host = None
     if not a.no_e2e:
-        fdir = tempfile.mkdtemp(prefix="cdbg_e2e_", dir=a.e2e_dir or None)
+        fdir = tempfile.mkdtemp(prefix="cdbg_e2e_", dir=a.e2e_dir or scratch_base())
         try:
             lst = synth.write_fasta(p, n_genomes, os.path.join(fdir, "in"), gzip_level=1)
             files = [l.strip() for l in open(lst) if l.strip()]
@@ -457,8 +474,8 @@ def main_gpu(a):
             e2e = {"value": job_kmers / (ems / 1000.0), "unit": "k-mers/s", "ms_per_step": ems,
                    "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes),
                    "path": "cdbg_gpu_build_files: %d gzip FASTA files (%.2f GB) -> frag_unitigs.bin (%.2f GB) + "
-                           ".color_sets, wall time per call" % (len(files), gz_bytes / 1e9,
-                                                                 re2.frag_nbytes / 1e9)}
+                           ".color_sets in %s, wall time per call" % (len(files), gz_bytes / 1e9,
+                                                                       re2.frag_nbytes / 1e9, os.path.dirname(fdir))}
         finally:
             shutil.rmtree(fdir, ignore_errors=True)
         # the same build from pinned host sequences to host outputs

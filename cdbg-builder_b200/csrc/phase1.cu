@@ -67,6 +67,15 @@ __device__ __forceinline__ uint32_t byte_valid(uint32_t c) {
     return (l == 'a' || l == 'c' || l == 'g' || l == 't') ? 1u : 0u;
 }
 
+// Boundary bitmap of the input: bit p set for every sequence start p and for
+// p = nbytes (seq_off[num_seqs]), one thread per offset.
+__global__ void k_seq_starts(uint64_t const* __restrict__ seq_off, uint32_t num_seqs, uint32_t* __restrict__ bits) {
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s > num_seqs) return;
+    const uint64_t p = seq_off[s];
+    atomicOr(&bits[p >> 5], 1u << (uint32_t)(p & 31));
+}
+
 // Run boundary events over positions [0, nbytes]: (pos << 1) | 1 for a run
 // start, (pos << 1) for a run end.  Sequence starts (and nbytes) split runs.
 // Each thread owns 32 positions as bit masks: V = valid bases, S = sequence
@@ -76,8 +85,7 @@ __device__ __forceinline__ uint32_t byte_valid(uint32_t c) {
 // (a full 32-byte chunk is read with two 16-byte loads when aligned).
 template <bool WRITE>
 __global__ void __launch_bounds__(EV_THREADS)
-    k_run_events(uint8_t const* __restrict__ ascii, uint64_t nbytes,
-                 uint64_t const* __restrict__ seq_off, uint32_t num_seqs,
+    k_run_events(uint8_t const* __restrict__ ascii, uint64_t nbytes, uint32_t const* __restrict__ starts,
                  uint32_t* __restrict__ tile_count, uint64_t const* __restrict__ tile_off,
                  uint64_t* __restrict__ events) {
     static_assert(EV_PER_THREAD == 32, "one 32-bit mask per thread");
@@ -96,12 +104,9 @@ __global__ void __launch_bounds__(EV_THREADS)
             const uint32_t n = (uint32_t)((nbytes - p0) < 32 ? (nbytes - p0) : 32);
             for (uint32_t i = 0; i < n; ++i) V |= byte_valid(ascii[p0 + i]) << i;
         }
-        // sequence starts in [p0, p0 + 32), and nbytes itself
-        uint32_t S = 0;
-        uint32_t s = upper_bound_u64(seq_off, num_seqs + 1, p0);  // first boundary > p0
-        if (s > 0 && seq_off[s - 1] == p0) S |= 1u;
-        for (; s <= num_seqs && seq_off[s] < p0 + 32; ++s) S |= 1u << (uint32_t)(seq_off[s] - p0);
-        if (nbytes - p0 < 32) S |= 1u << (uint32_t)(nbytes - p0);
+        // sequence starts in [p0, p0 + 32), and nbytes itself (bit i of word
+        // p0 / 32 of the boundary bitmap; p0 is a multiple of 32)
+        const uint32_t S = starts[p0 >> 5];
         // validity of the byte before p0, whatever sequence it belongs to: a
         // run of the previous sequence that ends exactly at p0 is closed here
         const uint32_t pin = (p0 > 0) ? byte_valid(ascii[p0 - 1]) : 0u;
@@ -975,10 +980,16 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
     const uint64_t tiles = ceil_div(npos, EV_TILE);
     uint32_t* tcount = A.alloc<uint32_t>(tiles);
     uint64_t* toff = A.alloc<uint64_t>(tiles + 1);
+    // bit p of `starts`: a sequence starts at p (or p = nbytes)
+    const uint64_t nsw = (in.nbytes >> 5) + 2;
+    uint32_t* starts = A.alloc<uint32_t>(nsw);
+    CDBG_CUDA(cudaMemsetAsync(starts, 0, 4 * nsw, st));
+    k_seq_starts<<<grid((uint64_t)in.num_seqs + 1, 256), 256, 0, st>>>(in.seq_off, in.num_seqs, starts);
+    CDBG_CHECK_LAUNCH();
     {
         CDBG_PROF("k_run_events", st);
-        k_run_events<false><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
-                                                                     in.num_seqs, tcount, nullptr, nullptr);
+        k_run_events<false><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, starts, tcount, nullptr,
+                                                                     nullptr);
     }
     CDBG_CHECK_LAUNCH();
     prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, tiles, A, st, toff + tiles);
@@ -988,8 +999,7 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
     uint64_t* ev = A.alloc<uint64_t>(nev);
     {
         CDBG_PROF("k_run_events", st);
-        k_run_events<true><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, in.seq_off,
-                                                                    in.num_seqs, tcount, toff, ev);
+        k_run_events<true><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, starts, tcount, toff, ev);
     }
     CDBG_CHECK_LAUNCH();
     uint64_t* src = A.alloc<uint64_t>(nraw);
