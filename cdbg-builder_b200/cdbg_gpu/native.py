@@ -106,7 +106,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("batch_occ", ctypes.c_uint64), ("minimizer_tile", ctypes.c_uint32),
                 ("heavy_colors", ctypes.c_uint32), ("table_slots_q", ctypes.c_uint32),
                 ("union_lists", ctypes.c_uint32), ("table_group_mb", ctypes.c_uint32),
-                ("radix_bits", ctypes.c_uint32), ("probe_filter", ctypes.c_uint32)]
+                ("radix_bits", ctypes.c_uint32)]
 
 
 class ServerParams(ctypes.Structure):
@@ -320,11 +320,10 @@ class Engine:
         return a.value, b.value
 
     def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0, table_slots_q=0, union_lists=0,
-                   table_group_mb=0, radix_bits=0, probe_filter=0):
+                   table_group_mb=0, radix_bits=0):
         _check(lib().cdbg_engine_set_tuning(self._h, ctypes.byref(Tuning(batch_occ, minimizer_tile, heavy_colors,
                                                                          table_slots_q, union_lists,
-                                                                         table_group_mb, radix_bits,
-                                                                         probe_filter))))
+                                                                         table_group_mb, radix_bits))))
 
     def tuning(self):
         t = Tuning()

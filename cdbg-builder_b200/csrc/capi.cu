@@ -738,7 +738,6 @@ int cdbg_gpu_phase2(cdbg_engine* e, const cdbg_phase2_args* a, cdbg_phase2_stats
             pp.table_slots_q = e->tune.table_slots_q;
             pp.union_bitmaps = e->tune.union_lists == 0;
             pp.group_bytes = e->tune.table_group_mb ? (uint64_t)e->tune.table_group_mb << 20 : ~0ull;
-        pp.neighbour_filter = e->tune.probe_filter;
             pp.to_host = true;
             pp.keep_dict = i > 0;
             pp.copy_dict = i + 1 == nr;
@@ -1124,7 +1123,6 @@ int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phas
         pp.table_slots_q = e->tune.table_slots_q;
         pp.union_bitmaps = e->tune.union_lists == 0;
         pp.group_bytes = e->tune.table_group_mb ? (uint64_t)e->tune.table_group_mb << 20 : ~0ull;
-        pp.neighbour_filter = e->tune.probe_filter;
         pp.to_host = false;  // outputs accumulate in HBM
         if (p->outputs_to_host && e->h_frag.p && e->h_frag.cap) {
             // stream each batch's fragments into the (already large enough,
@@ -1368,10 +1366,6 @@ int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
         g_last_error = "radix_bits must be 8 or 11";
         return -1;
     }
-    if (v.probe_filter > 2) {
-        g_last_error = "probe_filter must be 0, 1 or 2";
-        return -1;
-    }
     e->tune = v;
     return 0;
 }
@@ -1450,11 +1444,6 @@ int cdbg_engine_autotune(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_bui
             cdbg_tuning t = cur;
             t.radix_bits = v;
             if (t.radix_bits != cur.radix_bits) consider(t);
-        }
-        for (uint32_t v : {0u, 2u}) {
-            cdbg_tuning t = cur;
-            t.probe_filter = v;
-            if (t.probe_filter != cur.probe_filter) consider(t);
         }
         e->tune = cur;
         if (best) *best = cur;

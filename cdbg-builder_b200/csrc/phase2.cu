@@ -1611,40 +1611,11 @@ __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb,
 }
 
 // Nodes [*nb, *ne) (one bucket group's, numbered on the device).
-// Presence filter of one bucket group's k-mers: a blocked Bloom filter of
-// 2^fbits 64-bit words, two bits of one word per k-mer, sized to stay in L2.
-// It has no false negatives, so a candidate neighbour whose bits are not both
-// set is absent without probing its table (most of the 8 candidates of a
-// k-mer are absent, and each probe is a random access far outside L2).
-struct presence_filter {
-    unsigned long long* w;
-    uint32_t fbits;  // 0: no filter
-};
-template <typename K>
-__device__ __forceinline__ uint64_t filter_hash(K x) {
-    return mix64(kmer_ops<K>::hash(x) ^ 0x5bd1e9955bd1e995ULL);
-}
-template <typename K>
-__device__ __forceinline__ bool filter_maybe(presence_filter const& f, K x) {
-    if (!f.fbits) return true;
-    const uint64_t h = filter_hash<K>(x);
-    const uint64_t m = (1ull << (h & 63)) | (1ull << ((h >> 6) & 63));
-    return (__ldg(&f.w[h >> (64 - f.fbits)]) & m) == m;
-}
-template <typename K>
-__global__ void k_filter_fill(unsigned long long const* nb, unsigned long long const* ne,
-                              K const* __restrict__ n_key, presence_filter f) {
-    const uint64_t n = *nb + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= *ne) return;
-    const uint64_t h = filter_hash<K>(n_key[n]);
-    atomicOr(&f.w[h >> (64 - f.fbits)], (1ull << (h & 63)) | (1ull << ((h >> 6) & 63)));
-}
-
 template <typename K>
 __global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* nb, unsigned long long const* ne,
                                                      tables<K> T, K const* __restrict__ n_key,
                                                      uint32_t const* __restrict__ n_bucket, uint32_t k,
-                                                     uint8_t* __restrict__ n_mask, presence_filter flt) {
+                                                     uint8_t* __restrict__ n_mask) {
     const uint64_t n = *nb + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= *ne) return;
     typedef kmer_ops<K> ops;
@@ -1660,12 +1631,10 @@ __global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* n
         const K hi = (K)(3u - nt) << top;
         const K f = ((can << 2) | (K)nt) & msk;
         const K fr = (rev >> 2) | hi;
-        const K cf = f <= fr ? f : fr;
-        if (filter_maybe<K>(flt, cf) && node_lookup<K>(T, tb, cf) != NONE32) out |= 1u << nt;
+        if (node_lookup<K>(T, tb, f <= fr ? f : fr) != NONE32) out |= 1u << nt;
         const K r = ((rev << 2) | (K)nt) & msk;
         const K rr = (can >> 2) | hi;
-        const K cr = r <= rr ? r : rr;
-        if (filter_maybe<K>(flt, cr) && node_lookup<K>(T, tb, cr) != NONE32) out |= 1u << (4 + nt);
+        if (node_lookup<K>(T, tb, r <= rr ? r : rr) != NONE32) out |= 1u << (4 + nt);
     }
     n_mask[n] = (uint8_t)out;
 }
@@ -2364,20 +2333,6 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
     CDBG_CUDA(cudaMemsetAsync(mn_status, 0, 8 * (gtile[ng] + 1), st));
     CDBG_CUDA(cudaMemsetAsync(mn_counter, 0, 4 * (ng + 1), st));
     CDBG_CUDA(cudaMemsetAsync(ncnt, 0, 16, st));
-    // presence filter for the neighbour probes: about 4 bits per occurrence of
-    // the largest group (distinct k-mers are fewer), at most 64 MiB so that it
-    // stays in L2; none for small groups, whose tables are cache-resident anyway
-    presence_filter flt{nullptr, 0};
-    {
-        uint64_t gmax = 0;
-        for (size_t g = 0; g < ng; ++g) gmax = std::max<uint64_t>(gmax, bocc[b0 + gb[g + 1]] - bocc[b0 + gb[g]]);
-        if (p.neighbour_filter == 1 || (p.neighbour_filter == 0 && gmax >= (1ull << 22))) {
-            uint32_t fb = 10;
-            while (fb < 23 && (64ull << fb) < 4 * gmax) ++fb;  // 2^23 words = 64 MiB
-            flt.fbits = fb;
-            flt.w = A.alloc<unsigned long long>(1ull << fb);
-        }
-    }
     for (size_t g = 0; g < ng; ++g) {
         const uint32_t g0 = gb[g], g1 = gb[g + 1];
         const uint64_t t0 = bocc[b0 + g0] - O0, tn = bocc[b0 + g1] - bocc[b0 + g0];
@@ -2418,17 +2373,9 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
                 n_key, n_meta, n_rec, n_bucket, d_err);
         }
         CDBG_CHECK_LAUNCH();
-        if (flt.fbits) {
-            CDBG_CUDA(cudaMemsetAsync(flt.w, 0, 8ull << flt.fbits, st));
-            {
-                CDBG_PROF("k_filter_fill", st);
-                k_filter_fill<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, n_key, flt);
-            }
-            CDBG_CHECK_LAUNCH();
-        }
         {
             CDBG_PROF("k_ext_mask", st);
-            k_ext_mask<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, TG, n_key, n_bucket, k, n_mask, flt);
+            k_ext_mask<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, TG, n_key, n_bucket, k, n_mask);
         }
         CDBG_CHECK_LAUNCH();
         {

@@ -96,10 +96,6 @@ struct phase2_params {
     // table alone is larger forms a group of its own; the default is one group
     // per batch)
     uint64_t group_bytes = ~0ull;
-    // probe a neighbour's table only when an L2-resident presence filter of
-    // the group's k-mers says it may be there (performance only)
-    // 0: when a group has >= 2^22 occurrences, 1: always, 2: never
-    uint32_t neighbour_filter = 0;
     // Device-resident mode: fragment bytes of each batch are also copied to
     // this pinned host buffer on `copy_st` while later batches run, as long
     // as they fit in `frag_host_cap` (nothing is streamed when null).

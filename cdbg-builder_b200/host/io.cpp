@@ -14,6 +14,8 @@
 #include <thread>
 
 #include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/vfs.h>
 #include <unistd.h>
 
 extern "C" {
@@ -296,21 +298,40 @@ void write_file_parallel(std::string const& path, uint8_t const* data, uint64_t 
     }
     const uint64_t piece = std::max<uint64_t>(32ull << 20, (n + threads - 1) / std::max<uint32_t>(threads, 1));
     const size_t np = (size_t)((n + piece - 1) / piece);
-    // positional writes of disjoint ranges (a shared mapping was slower: one
-    // page fault per 4 KiB page)
     std::atomic<bool> bad{false};
-    parallel_for(np, threads, [&](size_t i) {
-        uint64_t a = i * piece;
-        const uint64_t b = std::min<uint64_t>(n, a + piece);
-        while (a < b) {
-            const ssize_t w = ::pwrite(fd, data + a, (size_t)std::min<uint64_t>(b - a, 1ull << 30), (off_t)a);
-            if (w <= 0) {
-                bad = true;
-                return;
+    // On a RAM-backed file system (tmpfs) writes to one file take the file's
+    // lock one call at a time, so parallel writes run as one; a shared
+    // mapping filled by several threads fills its pages in parallel.  On a
+    // disk file system the mapping is slower (its page faults and dirty-page
+    // accounting), and positional writes of disjoint ranges are used.  The
+    // space is reserved first (fallocate), so a full file system is an error
+    // here rather than a fault in the copy.
+    struct statfs fs;
+    constexpr long kTmpfsMagic = 0x01021994;
+    void* map = MAP_FAILED;
+    if (::fstatfs(fd, &fs) == 0 && (long)fs.f_type == kTmpfsMagic && ::fallocate(fd, 0, 0, (off_t)n) == 0)
+        map = ::mmap(nullptr, (size_t)n, PROT_WRITE, MAP_SHARED, fd, 0);
+    if (map != MAP_FAILED) {
+        uint8_t* dst = (uint8_t*)map;
+        parallel_for(np, threads, [&](size_t i) {
+            const uint64_t a = i * piece, b = std::min<uint64_t>(n, a + piece);
+            std::memcpy(dst + a, data + a, (size_t)(b - a));
+        });
+        if (::munmap(map, (size_t)n) != 0) bad = true;
+    } else {
+        parallel_for(np, threads, [&](size_t i) {
+            uint64_t a = i * piece;
+            const uint64_t b = std::min<uint64_t>(n, a + piece);
+            while (a < b) {
+                const ssize_t w = ::pwrite(fd, data + a, (size_t)std::min<uint64_t>(b - a, 1ull << 30), (off_t)a);
+                if (w <= 0) {
+                    bad = true;
+                    return;
+                }
+                a += (uint64_t)w;
             }
-            a += (uint64_t)w;
-        }
-    });
+        });
+    }
     if (::close(fd) != 0 || bad) throw std::runtime_error("short write to " + path);
 }
 

@@ -72,9 +72,6 @@ typedef struct cdbg_tuning {
                                   and probed while cache-resident (0, the
                                   default: one group per batch) */
     uint32_t radix_bits;       /* radix sort digit width: 8 or 11 (default 8) */
-    uint32_t probe_filter;     /* neighbour probes behind an L2-resident
-                                  presence filter: 0 for groups of >= 2^22
-                                  occurrences (default), 1 always, 2 never */
 } cdbg_tuning;
 
 int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t);

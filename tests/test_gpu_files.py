@@ -50,6 +50,17 @@ def test_build_files_equals_dropin(engine, tmp_path, k, gz, n):
     # outputs kept in host memory instead of files
     rh = engine.build_files(files, k, B)
     assert native.result_frag_bytes(rh) == open(want_frag, "rb").read()
+    # outputs on a RAM-backed file system (filled through a shared mapping)
+    if os.path.isdir("/dev/shm") and os.access("/dev/shm", os.W_OK):
+        import tempfile
+        d = tempfile.mkdtemp(prefix="cdbg_test_", dir="/dev/shm")
+        try:
+            frag2, cs2 = os.path.join(d, "frag_unitigs.bin"), os.path.join(d, "out.color_sets")
+            engine.build_files(files, k, B, frag2, cs2, host_threads=4)
+            assert filecmp.cmp(frag2, want_frag, shallow=False)
+            assert filecmp.cmp(cs2, want_cs, shallow=False)
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
 
 
 def test_multi_member_gzip_falls_back_to_whole_read(engine, tmp_path):

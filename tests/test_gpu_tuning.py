@@ -37,8 +37,7 @@ def test_knobs_do_not_change_outputs(k):
                   dict(batch_occ=1 << 12), dict(batch_occ=1, minimizer_tile=1024, heavy_colors=16),
                   dict(table_slots_q=5), dict(table_slots_q=16), dict(table_slots_q=5, batch_occ=1 << 14),
                   dict(union_lists=1, heavy_colors=1), dict(table_group_mb=1), dict(table_group_mb=1024),
-                  dict(radix_bits=11), dict(radix_bits=11, table_group_mb=2, minimizer_tile=1024),
-                  dict(probe_filter=1), dict(probe_filter=1, table_group_mb=1), dict(probe_filter=2)):
+                  dict(radix_bits=11), dict(radix_bits=11, table_group_mb=2, minimizer_tile=1024)):
             e.set_tuning(**t)
             got = _out(e, b, k, B, n)
             assert got[0] == want[0], t
