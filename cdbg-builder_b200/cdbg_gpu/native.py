@@ -106,7 +106,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("batch_occ", ctypes.c_uint64), ("minimizer_tile", ctypes.c_uint32),
                 ("heavy_colors", ctypes.c_uint32), ("table_slots_q", ctypes.c_uint32),
                 ("union_lists", ctypes.c_uint32), ("table_group_mb", ctypes.c_uint32),
-                ("radix_bits", ctypes.c_uint32)]
+                ("radix_bits", ctypes.c_uint32), ("gpu_inflate", ctypes.c_uint32)]
 
 
 class ServerParams(ctypes.Structure):
@@ -164,6 +164,9 @@ SIGNATURES = {
                                             ctypes.c_char_p, c_u64p]),
     "cdbg_gpu_sort_pairs_u64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_uint64]),
+    "cdbg_gpu_gunzip": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_u64p, ctypes.c_uint32,
+                                       ctypes.POINTER(ctypes.c_void_p), c_u64p, c_u64p,
+                                       ctypes.POINTER(ctypes.c_uint32)]),
     "cdbg_gpu_phase2": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Phase2Args),
                                        ctypes.POINTER(Phase2Stats)]),
     "cdbg_gpu_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeqBatch),
@@ -320,10 +323,11 @@ class Engine:
         return a.value, b.value
 
     def set_tuning(self, batch_occ=0, minimizer_tile=0, heavy_colors=0, table_slots_q=0, union_lists=0,
-                   table_group_mb=0, radix_bits=0):
+                   table_group_mb=0, radix_bits=0, gpu_inflate=0):
         _check(lib().cdbg_engine_set_tuning(self._h, ctypes.byref(Tuning(batch_occ, minimizer_tile, heavy_colors,
                                                                          table_slots_q, union_lists,
-                                                                         table_group_mb, radix_bits))))
+                                                                         table_group_mb, radix_bits,
+                                                                         gpu_inflate))))
 
     def tuning(self):
         t = Tuning()
@@ -383,6 +387,23 @@ class Engine:
     def sort_pairs_u64(self, keys_ptr, vals_ptr, n):
         """Stable in-place sort of n device (u64 key, u32 value) pairs by key."""
         _check(lib().cdbg_gpu_sort_pairs_u64(self._h, keys_ptr, vals_ptr, n))
+
+    def gunzip(self, streams, caps):
+        """Device gzip decoder on byte strings `streams` (out_caps `caps`):
+        [(status, bytes)] per stream."""
+        n = len(streams)
+        bufs = [ctypes.create_string_buffer(max(int(c), 1)) for c in caps]
+        keep = [ctypes.create_string_buffer(bytes(x), len(x)) if len(x) else ctypes.create_string_buffer(1)
+                for x in streams]
+        sp = (ctypes.c_void_p * max(n, 1))(*[ctypes.cast(b, ctypes.c_void_p) for b in keep])
+        op = (ctypes.c_void_p * max(n, 1))(*[ctypes.cast(b, ctypes.c_void_p) for b in bufs])
+        lens = np.array([len(x) for x in streams] + [0], dtype=np.uint64)
+        capa = np.array(list(caps) + [0], dtype=np.uint64)
+        olen = np.zeros(n + 1, dtype=np.uint64)
+        st = (ctypes.c_uint32 * max(n, 1))()
+        _check(lib().cdbg_gpu_gunzip(self._h, sp, lens.ctypes.data_as(c_u64p), n, op, capa.ctypes.data_as(c_u64p),
+                                     olen.ctypes.data_as(c_u64p), st))
+        return [(int(st[i]), bufs[i].raw[:int(olen[i])] if st[i] == 0 else b"") for i in range(n)]
 
     def dump_supers(self, batch, k, m, num_buckets, path):
         n = ctypes.c_uint64()

@@ -20,6 +20,7 @@
 #include "../host/io.hpp"
 #include "cdbg_gpu.h"
 #include "engine.cuh"
+#include "inflate.cuh"
 #include "phase1.cuh"
 #include "phase2.cuh"
 #include "primitives.cuh"
@@ -416,6 +417,58 @@ int cdbg_engine_kernel_stats(cdbg_engine* e, char* names, uint64_t names_cap, do
         ++i;
     }
     return (int)e->prof.totals.size();
+}
+
+int cdbg_gpu_gunzip(cdbg_engine* e, const uint8_t* const* streams, const uint64_t* lens, uint32_t n,
+                    uint8_t* const* outs, const uint64_t* out_caps, uint64_t* out_lens, uint32_t* status) {
+    if (!e || (n && (!streams || !lens || !outs || !out_caps || !out_lens || !status))) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    call_scope scope_(e);
+    try {
+        CDBG_CUDA(cudaSetDevice(e->device));
+        cudaStream_t st = e->st;
+        std::vector<uint64_t> meta(4 * (size_t)n + 1, 0);
+        uint64_t ti = 0, to = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            meta[i] = ti;
+            meta[n + i] = lens[i];
+            meta[2 * (size_t)n + i] = to;
+            meta[3 * (size_t)n + 1 + i] = out_caps[i];
+            ti += lens[i];
+            to += (out_caps[i] + 15) & ~uint64_t(15);
+        }
+        meta[3 * (size_t)n] = to;
+        std::vector<uint8_t> hin(ti + 64, 0), gz(n, 1);
+        for (uint32_t i = 0; i < n; ++i)
+            if (lens[i]) std::memcpy(hin.data() + meta[i], streams[i], lens[i]);
+        auto mk = e->A.mark();
+        uint8_t* d_in = e->A.alloc<uint8_t>(ti + 64);
+        uint8_t* d_out = e->A.alloc<uint8_t>(to + 64);
+        uint64_t* d_meta = e->A.alloc<uint64_t>(meta.size());
+        uint8_t* d_gz = e->A.alloc<uint8_t>(n + 1);
+        uint64_t* d_olen = e->A.alloc<uint64_t>(n + 1);
+        uint32_t* d_st = e->A.alloc<uint32_t>(n + 1);
+        CDBG_CUDA(cudaMemcpyAsync(d_in, hin.data(), hin.size(), cudaMemcpyHostToDevice, st));
+        CDBG_CUDA(cudaMemcpyAsync(d_meta, meta.data(), 8 * meta.size(), cudaMemcpyHostToDevice, st));
+        CDBG_CUDA(cudaMemcpyAsync(d_gz, gz.data(), n, cudaMemcpyHostToDevice, st));
+        cdbg::stream_set ss{d_in, d_meta, d_meta + n, d_gz, d_out, d_meta + 2 * (size_t)n,
+                            d_meta + 3 * (size_t)n + 1, d_olen, d_st, n};
+        cdbg::inflate_streams(ss, st);
+        CDBG_CUDA(cudaMemcpyAsync(out_lens, d_olen, 8ull * n, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaMemcpyAsync(status, d_st, 4ull * n, cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        for (uint32_t i = 0; i < n; ++i)
+            if (status[i] == cdbg::STREAM_OK && out_lens[i])
+                CDBG_CUDA(cudaMemcpyAsync(outs[i], d_out + meta[2 * (size_t)n + i], out_lens[i],
+                                          cudaMemcpyDeviceToHost, st));
+        CDBG_CUDA(cudaStreamSynchronize(st));
+        e->A.release(mk);
+        return 0;
+    } catch (std::exception const& ex) {
+        return fail(ex);
+    }
 }
 
 int cdbg_gpu_sort_pairs_u64(cdbg_engine* e, uint64_t* keys, uint32_t* vals, uint64_t n) {
@@ -906,9 +959,128 @@ void phase1_pipelined(cdbg_engine* e, cdbg_seq_batch const* b, uint32_t k, uint3
 // single pass produces.  The buffers are sized from the files' inflated-size
 // hints; returns false (nothing launched that matters) when a file inflates
 // to more than its hint says, and the caller reads the files whole instead.
+// Phase 1 from the files with the device reader: the files' bytes as stored
+// go to the device; one warp per gzip file inflates it into the file's region
+// of HBM (inflate_streams), the FASTA records are cut in place
+// (fasta_compact), and the regions -- one sequence per file, records
+// separated by a byte that is not a base -- go through build_runs and
+// find_supers like the host reader's sequences, with the same runs.
+// Returns false, with nothing kept, when the files do not suit it (no gzip
+// file, or, with gpu_inflate = 0, one file holding so much of the input that
+// a warp per file is slower than the host threads) or when a stream goes
+// back to the host reader.
+bool phase1_device_reader(cdbg_engine* e, std::vector<std::string> const& files, uint32_t threads, uint32_t k,
+                          uint32_t m, uint32_t B, cdbg::run_table& rt_all, cdbg::super_list& sl_all, uint64_t* h2d,
+                          uint64_t* input_bytes, uint32_t color_base, bool packed, uint64_t* seq_bytes) {
+    if (e->tune.gpu_inflate == 2) return false;
+    const size_t nf = files.size();
+    if (nf == 0 || nf >= (1u << 31)) return false;
+    std::vector<cdbg::io::file_probe> pr;
+    cdbg::io::probe_files(files, threads, pr);
+    std::vector<uint64_t> ioff(nf + 1, 0), ooff(nf + 1, 0), ocap(nf);
+    std::vector<uint8_t> gz(nf);
+    uint64_t max_out = 0;
+    bool any_gz = false;
+    for (size_t i = 0; i < nf; ++i) {
+        ioff[i + 1] = ioff[i] + pr[i].size;
+        ocap[i] = pr[i].gz ? pr[i].hint : pr[i].size;
+        ooff[i + 1] = ooff[i] + ((ocap[i] + 15) & ~uint64_t(15));
+        gz[i] = pr[i].gz ? 1 : 0;
+        any_gz |= pr[i].gz;
+        max_out = std::max(max_out, ocap[i]);
+    }
+    const uint64_t tot_in = ioff[nf], tot_out = ooff[nf];
+    if (!any_gz) return false;
+    // a warp inflates a few tens of MB/s, a host thread several times that:
+    // the device reader wins while no file holds more than about 1/(6T) of
+    // the input
+    if (e->tune.gpu_inflate == 0 && (double)max_out * 6.0 * threads > (double)tot_out) return false;
+    cudaStream_t st = e->st;
+    char* h = (char*)e->h_in.ensure(tot_in + 64);
+    cdbg::io::read_raw_files(files, threads, h, ioff.data());
+    auto ma = e->A.mark();
+    auto mp = e->P.mark();
+    uint8_t* d_in = e->A.alloc<uint8_t>(tot_in + 64);
+    uint8_t* d_out = e->A.alloc<uint8_t>(tot_out + 64);
+    // per-file arrays in one upload: in_off, in_len, out_off (nf + 1), out_cap
+    std::vector<uint64_t> meta(4 * nf + 1);
+    for (size_t i = 0; i < nf; ++i) {
+        meta[i] = ioff[i];
+        meta[nf + i] = pr[i].size;
+        meta[3 * nf + 1 + i] = ocap[i];
+    }
+    for (size_t i = 0; i <= nf; ++i) meta[2 * nf + i] = ooff[i];
+    uint64_t* d_meta = e->A.alloc<uint64_t>(meta.size());
+    uint8_t* d_gz = e->A.alloc<uint8_t>(nf);
+    uint64_t* d_olen = e->A.alloc<uint64_t>(nf);
+    uint64_t* d_sb = e->A.alloc<uint64_t>(nf);
+    uint32_t* d_status = e->A.alloc<uint32_t>(nf);
+    uint32_t* d_color = e->A.alloc<uint32_t>(nf);
+    std::vector<uint32_t> col(nf);
+    for (size_t i = 0; i < nf; ++i) col[i] = color_base + (uint32_t)i;
+    CDBG_CUDA(cudaMemcpyAsync(d_in, h, tot_in, cudaMemcpyHostToDevice, st));
+    CDBG_CUDA(cudaMemcpyAsync(d_meta, meta.data(), 8 * meta.size(), cudaMemcpyHostToDevice, st));
+    CDBG_CUDA(cudaMemcpyAsync(d_gz, gz.data(), nf, cudaMemcpyHostToDevice, st));
+    CDBG_CUDA(cudaMemcpyAsync(d_color, col.data(), 4 * nf, cudaMemcpyHostToDevice, st));
+    cdbg::stream_set ss{d_in,  d_meta,        d_meta + nf, d_gz,     d_out,
+                        d_meta + 2 * nf, d_meta + 3 * nf + 1, d_olen, d_status, (uint32_t)nf};
+    {
+        CDBG_PROF_BYTES("k_inflate", st, (double)tot_in + (double)tot_out);
+        cdbg::inflate_streams(ss, st);
+    }
+    {
+        CDBG_PROF_BYTES("k_fasta_compact", st, 2.0 * (double)tot_out);
+        cdbg::fasta_compact(ss, d_sb, st);
+    }
+    std::vector<uint32_t> status(nf);
+    std::vector<uint64_t> sb(nf);
+    CDBG_CUDA(cudaMemcpyAsync(status.data(), d_status, 4 * nf, cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaMemcpyAsync(sb.data(), d_sb, 8 * nf, cudaMemcpyDeviceToHost, st));
+    CDBG_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < nf; ++i)
+        if (status[i] != cdbg::STREAM_OK) {
+            e->A.release(ma);
+            e->P.release(mp);
+            return false;
+        }
+    cdbg::seq_input in;
+    in.ascii = d_out;
+    in.nbytes = tot_out;
+    in.seq_off = d_meta + 2 * nf;
+    in.seq_color = d_color;
+    in.num_seqs = (uint32_t)nf;
+    const uint64_t cap = tot_out / 32 + tot_out / std::max<uint32_t>(k, 1) + 128;
+    uint64_t* words = e->P.alloc<uint64_t>(cap);
+    cdbg::run_table rt;
+    cdbg::build_runs(in, k, e->A, st, rt, e->P, words, 0, cap);
+    if (rt.n == 0) {  // nothing to build from: the host reader's path handles it
+        e->A.release(ma);
+        e->P.release(mp);
+        return false;
+    }
+    sl_all = cdbg::super_list();
+    cdbg::find_supers(rt, k, m, B, e->A, st, sl_all, e->d_err, e->tune.minimizer_tile, packed);
+    rt_all = cdbg::run_table();
+    rt_all.words = words;
+    rt_all.nwords = rt.nwords;
+    rt_all.n_kmers = rt.n_kmers;
+    rt_all.n_bases = rt.n_bases;
+    if (h2d) *h2d += tot_in + 8 * meta.size() + 5 * nf;
+    if (input_bytes) *input_bytes = tot_in;
+    if (seq_bytes) {
+        uint64_t t = 0;
+        for (uint64_t v : sb) t += v;
+        *seq_bytes = t;
+    }
+    return true;
+}
+
 bool phase1_from_files(cdbg_engine* e, std::vector<std::string> const& files, uint32_t threads, uint32_t k,
                        uint32_t m, uint32_t B, cdbg::run_table& rt_all, cdbg::super_list& sl_all, uint64_t* h2d,
                        uint64_t* input_bytes, uint32_t color_base, bool packed, uint64_t* seq_bytes) {
+    if (phase1_device_reader(e, files, threads, k, m, B, rt_all, sl_all, h2d, input_bytes, color_base, packed,
+                             seq_bytes))
+        return true;
     cudaStream_t st = e->st;
     const size_t nf = files.size();
     uint64_t N = 0;
@@ -1364,6 +1536,10 @@ int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t) {
     if (v.radix_bits == 0) v.radix_bits = 8;
     if (v.radix_bits != 8 && v.radix_bits != 11) {
         g_last_error = "radix_bits must be 8 or 11";
+        return -1;
+    }
+    if (v.gpu_inflate > 2) {
+        g_last_error = "gpu_inflate must be 0, 1 or 2";
         return -1;
     }
     e->tune = v;

@@ -47,7 +47,7 @@ struct cdbg_engine {
     cdbg::phase2_state p2;
     uint32_t* d_err = nullptr;  // device error word (outside the arena)
     uint64_t mem_limit = 0;     // device memory cap of this engine (0 = none)
-    cdbg_tuning tune{0, 4096, 64, 8, 0, 0, 8};
+    cdbg_tuning tune{0, 4096, 64, 8, 0, 0, 8, 0};
     cdbg::record_set last_rs;  // records of the last in-memory build (in P)
     bool have_rs = false;
     // host copies of the last cdbg_gpu_build's outputs (outputs_to_host = 1)

@@ -232,26 +232,54 @@ void read_files(std::vector<std::string> const& files, size_t first, size_t coun
     }
 }
 
-uint64_t inflated_size_hint(std::string const& path) {
+file_probe probe_file(std::string const& path) {
     std::error_code ec;
     const uint64_t sz = std::filesystem::file_size(path, ec);
     if (ec) throw std::runtime_error("could not open input file: " + path);
     std::FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) throw std::runtime_error("could not open input file: " + path);
     unsigned char head[2] = {0, 0}, tail[4] = {0, 0, 0, 0};
-    const bool gz = std::fread(head, 1, 2, f) == 2 && head[0] == 0x1f && head[1] == 0x8b;
-    uint64_t v = sz;
-    if (gz && sz >= 18 && std::fseek(f, -4, SEEK_END) == 0 && std::fread(tail, 1, 4, f) == 4) {
+    file_probe p;
+    p.size = sz;
+    p.gz = std::fread(head, 1, 2, f) == 2 && head[0] == 0x1f && head[1] == 0x8b;
+    p.hint = sz;
+    if (p.gz && sz >= 18 && std::fseek(f, -4, SEEK_END) == 0 && std::fread(tail, 1, 4, f) == 4) {
         const uint64_t isize = (uint64_t)tail[0] | ((uint64_t)tail[1] << 8) | ((uint64_t)tail[2] << 16) |
                                ((uint64_t)tail[3] << 24);
         // the size field is mod 2^32: take the largest size congruent to it
         // that deflate's maximum ratio (1032:1) allows
         const uint64_t lim = sz * 1032;
-        v = isize;
+        uint64_t v = isize;
         while (v + (uint64_t(1) << 32) <= lim) v += uint64_t(1) << 32;
+        p.hint = v;
     }
     std::fclose(f);
-    return v;
+    return p;
+}
+
+uint64_t inflated_size_hint(std::string const& path) { return probe_file(path).hint; }
+
+void probe_files(std::vector<std::string> const& files, uint32_t threads, std::vector<file_probe>& out) {
+    out.assign(files.size(), file_probe());
+    parallel_for(files.size(), threads, [&](size_t i) { out[i] = probe_file(files[i]); });
+}
+
+void read_raw_files(std::vector<std::string> const& files, uint32_t threads, char* dst, uint64_t const* off) {
+    parallel_for(files.size(), threads, [&](size_t i) {
+        const int fd = ::open(files[i].c_str(), O_RDONLY);
+        if (fd < 0) throw std::runtime_error("could not open input file: " + files[i]);
+        uint64_t a = off[i];
+        const uint64_t b = off[i + 1];
+        while (a < b) {
+            const ssize_t r = ::read(fd, dst + a, (size_t)std::min<uint64_t>(b - a, 1ull << 30));
+            if (r <= 0) {
+                ::close(fd);
+                throw std::runtime_error("short read of input file: " + files[i]);
+            }
+            a += (uint64_t)r;
+        }
+        ::close(fd);
+    });
 }
 
 bool read_files_into(std::vector<std::string> const& files, size_t first, size_t count, uint32_t color_base,

@@ -40,6 +40,20 @@ void read_files(std::vector<std::string> const& files, size_t first, size_t coun
 // that size buffers from it check what they read.
 uint64_t inflated_size_hint(std::string const& path);
 
+// What the device reader needs to know about an input file before reading it:
+// its size on disk, whether it is gzip, and its inflated size hint.
+struct file_probe {
+    uint64_t size = 0;
+    bool gz = false;
+    uint64_t hint = 0;
+};
+file_probe probe_file(std::string const& path);
+void probe_files(std::vector<std::string> const& files, uint32_t threads, std::vector<file_probe>& out);
+
+// Reads files[i] whole (as stored on disk) into dst + off[i], in parallel;
+// off has files.size() + 1 entries, off[i + 1] - off[i] the file's size.
+void read_raw_files(std::vector<std::string> const& files, uint32_t threads, char* dst, uint64_t const* off);
+
 // read_files with the sequence bytes written to dst[0 .. cap) (out.seq stays
 // empty; out.off / out.color / out.input_bytes as read_files).  Returns false,
 // with nothing written past cap, when the sequences need more than cap bytes.

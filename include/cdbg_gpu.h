@@ -72,6 +72,16 @@ typedef struct cdbg_tuning {
                                   and probed while cache-resident (0, the
                                   default: one group per batch) */
     uint32_t radix_bits;       /* radix sort digit width: 8 or 11 (default 8) */
+    uint32_t gpu_inflate;      /* input files of cdbg_gpu_build_files and
+                                  cdbg_gpu_phase1 read by the device (one warp
+                                  inflates each gzip file, FASTA records are
+                                  cut on the device): 0 (default) when the
+                                  work spreads over many files, 1 whenever
+                                  the files are gzip, 2 never.  Streams the
+                                  device reader does not take (FASTQ, a
+                                  multi-member file over its size hint, data
+                                  it refuses) send the call to the host
+                                  reader; outputs are the same either way. */
 } cdbg_tuning;
 
 int cdbg_engine_set_tuning(cdbg_engine* e, const cdbg_tuning* t);
@@ -162,6 +172,15 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
  * emit_super_kmers (bucket_ingester.hpp:36-127). */
 int cdbg_gpu_dump_supers(cdbg_engine* e, const cdbg_seq_batch* b, uint32_t k, uint32_t m,
                          uint32_t num_buckets, const char* dump_path, uint64_t* n_supers);
+
+/* Test aid (no counterpart in the reference): the device gzip decoder of the
+ * device reader (gpu_inflate) on n gzip streams in host memory, inflated on
+ * the device in one launch, one warp per stream.  outs[i] (host, out_caps[i]
+ * bytes) receives stream i's bytes and out_lens[i] their count when
+ * status[i] is 0; status 1 = more than out_caps[i] bytes, 2 = not a stream
+ * the decoder accepts (the host reader's zlib then decides). */
+int cdbg_gpu_gunzip(cdbg_engine* e, const uint8_t* const* streams, const uint64_t* lens, uint32_t n,
+                    uint8_t* const* outs, const uint64_t* out_caps, uint64_t* out_lens, uint32_t* status);
 
 /* Stable sort of n device (key, value) pairs by the full 64-bit key, in place
  * on the engine's stream: the sort phase 1 uses to order super-k-mers by
