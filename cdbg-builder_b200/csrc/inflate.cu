@@ -16,8 +16,10 @@
 // never diverges; lanes split the table construction and copies.  Output goes
 // through a 4 KiB ring in shared memory, written to HBM in aligned 1 KiB
 // chunks; match sources closer than the ring come from it, farther ones from
-// HBM (already written).  Huffman codes of up to 10 bits decode with one
-// table lookup; longer codes fall back to a canonical decode by length.
+// HBM (already written).  A literal/length lookup of 11 bits yields up to
+// three literals at once (DNA's literal codes are 2-3 bits long), or one
+// length or end code; codes longer than the table fall back to a canonical
+// decode by length.
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -29,10 +31,11 @@ namespace cdbg {
 namespace {
 
 constexpr uint32_t FULL = 0xffffffffu;
-constexpr int IF_LB = 10;                // primary table index bits
+constexpr int LB_LIT = 11;               // literal/length table index bits
+constexpr int LB_DIST = 10;              // distance table index bits
 constexpr uint32_t IF_RING = 4096;       // shared-memory output window
 constexpr uint32_t IF_FLUSH = 1024;      // bytes per aligned write to HBM
-constexpr int IF_WARPS = 4;              // streams per CTA
+constexpr int IF_WARPS = 2;              // streams per CTA
 static_assert(IF_RING >= IF_FLUSH + 2 * 258, "match sources must be in the ring or already in HBM");
 
 // RFC 1951 3.2.5: length codes 257..285 and distance codes 0..29
@@ -58,8 +61,12 @@ struct code_aux {
 
 struct __align__(16) warp_state {
     uint8_t ring[IF_RING];
-    uint16_t lit[1 << IF_LB];   // (length << 9) | symbol, 0 = decode by length
-    uint16_t dist[1 << IF_LB];
+    // literal/length lookups: bits 0-3 bits consumed (0 = decode by length),
+    // bits 4-5 literals (1-3, bytes at bits 8, 16, 24; 0 = one non-literal
+    // symbol at bits 8-16)
+    uint32_t lit[1 << LB_LIT];
+    uint16_t lit1[1 << LB_LIT];  // one symbol per lookup: (length << 9) | symbol
+    uint16_t dist[1 << LB_DIST];
     code_aux la, da;
     uint32_t hist[16];
     uint8_t lens[320];
@@ -112,8 +119,8 @@ __device__ __forceinline__ uint32_t lanemask_lt_() {
 // over-subscribed set, and for an incomplete one unless it is a single code
 // of one bit or no code at all (with `strict`, for the code-length code, any
 // incomplete set) -- the sets zlib also refuses.  Warp-collective.
-__device__ bool build_code(uint8_t const* lens, int n, uint16_t* tab, code_aux& a, uint32_t* hist, int lane,
-                           bool strict) {
+__device__ bool build_code(uint8_t const* lens, int n, uint16_t* tab, int lb, code_aux& a, uint32_t* hist,
+                           int lane, bool strict) {
     if (lane < 16) hist[lane] = 0;
     __syncwarp();
     for (int s0 = 0; s0 < n; s0 += 32) {
@@ -144,7 +151,7 @@ __device__ bool build_code(uint8_t const* lens, int n, uint16_t* tab, code_aux& 
     }
     ok = __shfl_sync(FULL, ok, 0);
     if (!ok) return false;
-    for (int i = lane; i < (1 << IF_LB) / 2; i += 32) reinterpret_cast<uint32_t*>(tab)[i] = 0u;
+    for (int i = lane; i < (1 << lb) / 2; i += 32) reinterpret_cast<uint32_t*>(tab)[i] = 0u;
     if (lane < 16) hist[lane] = 0;
     __syncwarp();
     for (int s0 = 0; s0 < n; s0 += 32) {
@@ -157,10 +164,10 @@ __device__ bool build_code(uint8_t const* lens, int n, uint16_t* tab, code_aux& 
         if (l) {
             if (lane == __ffs(grp) - 1) hist[l] = before + __popc(grp);
             a.sym[a.base[l] + rank] = (uint16_t)s;
-            if (l <= (uint32_t)IF_LB) {
+            if (l <= (uint32_t)lb) {
                 const uint32_t rev = __brev(a.first[l] + rank) >> (32 - l);
                 const uint16_t e = (uint16_t)((l << 9) | (uint32_t)s);
-                for (uint32_t x = rev; x < (1u << IF_LB); x += 1u << l) tab[x] = e;
+                for (uint32_t x = rev; x < (1u << lb); x += 1u << l) tab[x] = e;
             }
         }
         __syncwarp();
@@ -168,29 +175,76 @@ __device__ bool build_code(uint8_t const* lens, int n, uint16_t* tab, code_aux& 
     return true;
 }
 
+// Canonical decode by length (codes longer than a table's index) of the
+// next bits `bb`: (bits used << 16) | symbol, or -1 for a bit string that is
+// no code.
+__device__ __noinline__ int decode_slow(uint64_t bb, code_aux const& a) {
+    uint32_t code = 0;
+    for (int len = 1; len < 16; ++len) {
+        code = (code << 1) | ((uint32_t)bb & 1u);
+        bb >>= 1;
+        const uint32_t off = code - a.first[len];
+        if (off < a.cnt[len]) return (len << 16) | a.sym[a.base[len] + off];
+    }
+    return -1;
+}
+
 // One symbol (at least 15 bits buffered); -1 for a bit string that is no code.
-__device__ __forceinline__ int decode_sym(bit_reader& br, uint16_t const* tab, code_aux const& a) {
-    const uint32_t e = tab[(uint32_t)br.bb & ((1u << IF_LB) - 1u)];
+__device__ __forceinline__ int decode_sym(bit_reader& br, uint16_t const* tab, int lb, code_aux const& a) {
+    const uint32_t e = tab[(uint32_t)br.bb & ((1u << lb) - 1u)];
     const uint32_t l = e >> 9;
     if (l) {
         br.drop(l);
         return (int)(e & 511u);
     }
-    uint32_t code = 0;
-    for (int len = 1; len < 16; ++len) {
-        code = (code << 1) | ((uint32_t)br.bb & 1u);
-        br.drop(1);
-        const uint32_t off = code - a.first[len];
-        if (off < a.cnt[len]) return a.sym[a.base[len] + off];
+    const int r = decode_slow(br.bb, a);
+    if (r < 0) return -1;
+    br.drop((uint32_t)r >> 16);
+    return r & 0xffff;
+}
+
+// The literal/length lookups from the one-symbol table: a literal whose code
+// leaves room in the index for the next code(s), when those are literals
+// too, yields two or three (the bits after a code are the index shifted
+// right by its length, upper bits zero, which select the same entry for any
+// code that fits).  Warp-collective.
+__device__ void pack_literals(warp_state& w, int lane) {
+    __syncwarp();
+    for (uint32_t x = (uint32_t)lane; x < (1u << LB_LIT); x += 32) {
+        const uint32_t e1 = w.lit1[x];
+        const uint32_t l1 = e1 >> 9, s1 = e1 & 511u;
+        uint32_t out = 0;
+        if (l1 && s1 >= 256) {
+            out = (s1 << 8) | l1;
+        } else if (l1) {
+            uint32_t tot = l1, cnt = 1;
+            out = s1 << 8;
+            const uint32_t e2 = w.lit1[x >> tot];
+            const uint32_t l2 = e2 >> 9, s2 = e2 & 511u;
+            if (l2 && s2 < 256 && tot + l2 <= (uint32_t)LB_LIT) {
+                out |= s2 << 16;
+                ++cnt;
+                tot += l2;
+                const uint32_t e3 = w.lit1[x >> tot];
+                const uint32_t l3 = e3 >> 9, s3 = e3 & 511u;
+                if (l3 && s3 < 256 && tot + l3 <= (uint32_t)LB_LIT) {
+                    out |= s3 << 24;
+                    ++cnt;
+                    tot += l3;
+                }
+            }
+            out |= (cnt << 4) | tot;
+        }
+        w.lit[x] = out;
     }
-    return -1;
+    __syncwarp();
 }
 
 struct out_state {
     uint8_t* o;      // region in HBM
-    uint64_t cap;
-    uint64_t op;     // bytes produced
-    uint64_t fp;     // bytes written to HBM (a multiple of IF_FLUSH)
+    uint32_t cap;    // (a stream of 4 GiB or more goes to the host reader)
+    uint32_t op;     // bytes produced
+    uint32_t fp;     // bytes written to HBM (a multiple of IF_FLUSH)
 };
 
 // Writes ring bytes [fp, fp + IF_FLUSH) to HBM (32 bytes per lane, aligned).
@@ -206,20 +260,23 @@ __device__ __forceinline__ void flush_chunk(warp_state& w, out_state& os, int la
 }
 
 // Copies L bytes from distance d back (d <= bytes produced in this member).
-// Lane i copies byte i of each 32-byte round: every source position is below
-// the copy's start or in an earlier round, and sources read before a round's
-// writes, so ring slots are never read after being overwritten.
+// Lane i copies byte i of each 32-byte round.  Every source position lies
+// before the copy (an overlapping copy, d < L, reads position op - d +
+// (i mod d): the period repeats), so no lane reads what this copy writes; a
+// ring slot read here is written here only when the write lands a whole ring
+// later (d + L > IF_RING), and then each round's writes wait for all reads.
 __device__ __forceinline__ void copy_match(warp_state& w, out_state& os, uint32_t d, uint32_t L, int lane) {
+    __syncwarp();  // the bytes stored before are visible to every lane
+    const bool wrap = d + L > IF_RING;
     for (uint32_t i0 = 0; i0 < L; i0 += 32) {
         const uint32_t i = i0 + (uint32_t)lane;
         uint8_t v = 0;
         if (i < L) {
-            const uint64_t s = os.op - d + (d < L ? i % d : i);
+            const uint32_t s = os.op - d + (d < L ? i % d : i);
             v = d <= IF_RING ? w.ring[s & (IF_RING - 1)] : os.o[s];
         }
-        __syncwarp();
+        if (wrap) __syncwarp();
         if (i < L) w.ring[(os.op + i) & (IF_RING - 1)] = v;
-        __syncwarp();
     }
     os.op += L;
 }
@@ -267,7 +324,8 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
     const uint32_t f = blockIdx.x * IF_WARPS + (uint32_t)wi;
     if (f >= s.n) return;  // whole warp
     warp_state& w = W[wi];
-    out_state os{s.out + s.out_off[f], s.out_cap[f], 0, 0};
+    const uint64_t cap64 = s.out_cap[f];
+    out_state os{s.out + s.out_off[f], (uint32_t)(cap64 < 0xfffff000ull ? cap64 : 0xfffff000ull), 0, 0};
     uint32_t st = STREAM_OK;
     if (!s.gz[f]) {
         // plain file: copied as is
@@ -277,7 +335,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
         } else {
             uint8_t const* src = s.in + s.in_off[f];
             for (uint64_t i = (uint64_t)lane; i < n; i += 32) os.o[i] = src[i];
-            os.op = n;
+            os.op = (uint32_t)n;
         }
         if (lane == 0) {
             s.out_len[f] = os.op;
@@ -291,7 +349,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
             st = STREAM_BAD;
             break;
         }
-        const uint64_t member0 = os.op;
+        const uint32_t member0 = os.op;
         bool last = false;
         while (!last && st == STREAM_OK) {  // blocks
             br.refill();
@@ -310,7 +368,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                     st = STREAM_BAD;
                     break;
                 }
-                if (os.op + len > os.cap) {
+                if ((uint64_t)os.op + len > os.cap) {
                     st = STREAM_OVERFLOW;
                     break;
                 }
@@ -347,8 +405,9 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                 for (int i = lane; i < 288 + 32; i += 32)
                     w.lens[i] = i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : i < 288 ? 8 : 5;
                 __syncwarp();
-                build_code(w.lens, 288, w.lit, w.la, w.hist, lane, false);
-                build_code(w.lens + 288, 32, w.dist, w.da, w.hist, lane, false);
+                build_code(w.lens, 288, w.lit1, LB_LIT, w.la, w.hist, lane, false);
+                build_code(w.lens + 288, 32, w.dist, LB_DIST, w.da, w.hist, lane, false);
+                pack_literals(w, lane);
             } else {
                 // dynamic codes (RFC 1951 3.2.7)
                 const uint32_t hlit = br.get(5) + 257, hdist = br.get(5) + 1, hclen = br.get(4) + 4;
@@ -364,7 +423,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                     if (lane == 0) w.lens[c_clen_order[i]] = (uint8_t)v;
                 }
                 __syncwarp();
-                if (!build_code(w.lens, 19, w.lit, w.la, w.hist, lane, true)) {
+                if (!build_code(w.lens, 19, w.lit1, LB_LIT, w.la, w.hist, lane, true)) {
                     st = STREAM_BAD;
                     break;
                 }
@@ -376,7 +435,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                         st = STREAM_BAD;
                         break;
                     }
-                    const int sym = decode_sym(br, w.lit, w.la);
+                    const int sym = decode_sym(br, w.lit1, LB_LIT, w.la);
                     if (sym < 0) {
                         st = STREAM_BAD;
                         break;
@@ -409,21 +468,44 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                 }
                 if (st != STREAM_OK) break;
                 __syncwarp();
-                if (w.lens[256] == 0 || !build_code(w.lens, (int)hlit, w.lit, w.la, w.hist, lane, false) ||
-                    !build_code(w.lens + hlit, (int)hdist, w.dist, w.da, w.hist, lane, false)) {
+                if (w.lens[256] == 0 || !build_code(w.lens, (int)hlit, w.lit1, LB_LIT, w.la, w.hist, lane, false) ||
+                    !build_code(w.lens + hlit, (int)hdist, w.dist, LB_DIST, w.da, w.hist, lane, false)) {
                     st = STREAM_BAD;
                     break;
                 }
+                pack_literals(w, lane);
             }
             // the block's symbols
             for (;;) {
                 if (os.op - os.fp >= IF_FLUSH) flush_chunk(w, os, lane);
-                br.refill();
-                if (br.overrun()) {
-                    st = STREAM_BAD;
-                    break;
+                if (br.nb <= 32) {
+                    br.refill();
+                    if (br.overrun()) {
+                        st = STREAM_BAD;
+                        break;
+                    }
                 }
-                int sym = decode_sym(br, w.lit, w.la);
+                const uint32_t e = w.lit[(uint32_t)br.bb & ((1u << LB_LIT) - 1u)];
+                const uint32_t cnt = (e >> 4) & 3u;
+                if (cnt) {  // one to three literals
+                    if ((uint64_t)os.op + cnt > os.cap) {
+                        st = STREAM_OVERFLOW;
+                        break;
+                    }
+                    if ((uint32_t)lane < cnt) w.ring[(os.op + lane) & (IF_RING - 1)] = (uint8_t)(e >> (8 + 8 * lane));
+                    os.op += cnt;
+                    br.drop(e & 15u);
+                    continue;
+                }
+                int sym;
+                if (e & 15u) {
+                    sym = (int)(e >> 8);
+                    br.drop(e & 15u);
+                } else {
+                    const int r = decode_slow(br.bb, w.la);
+                    sym = r < 0 ? -1 : (r & 0xffff);
+                    if (r >= 0) br.drop((uint32_t)r >> 16);
+                }
                 if (sym < 256) {
                     if (sym < 0) {
                         st = STREAM_BAD;
@@ -445,17 +527,17 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                 }
                 const uint32_t L = c_len_base[sym] + br.get(c_len_extra[sym]);
                 br.refill();
-                const int ds = decode_sym(br, w.dist, w.da);
+                const int ds = decode_sym(br, w.dist, LB_DIST, w.da);
                 if (ds < 0 || ds >= 30) {
                     st = STREAM_BAD;
                     break;
                 }
                 const uint32_t d = c_dist_base[ds] + br.get(c_dist_extra[ds]);
-                if ((uint64_t)d > os.op - member0) {
+                if (d > os.op - member0) {
                     st = STREAM_BAD;
                     break;
                 }
-                if (os.op + L > os.cap) {
+                if ((uint64_t)os.op + L > os.cap) {
                     st = STREAM_OVERFLOW;
                     break;
                 }
@@ -487,8 +569,8 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
     }
     __syncwarp();
     if (st == STREAM_OK) {
-        const uint64_t rest = os.op - os.fp;
-        for (uint64_t i = (uint64_t)lane; i < rest; i += 32) os.o[os.fp + i] = w.ring[(os.fp + i) & (IF_RING - 1)];
+        const uint32_t rest = os.op - os.fp;
+        for (uint32_t i = (uint32_t)lane; i < rest; i += 32) os.o[os.fp + i] = w.ring[(os.fp + i) & (IF_RING - 1)];
     }
     if (lane == 0) {
         s.out_len[f] = st == STREAM_OK ? os.op : 0;
