@@ -17,9 +17,10 @@
 // through a 4 KiB ring in shared memory, written to HBM in aligned 1 KiB
 // chunks; match sources closer than the ring come from it, farther ones from
 // HBM (already written).  A literal/length lookup of 11 bits yields up to
-// three literals at once (DNA's literal codes are 2-3 bits long), or one
-// length or end code; codes longer than the table fall back to a canonical
-// decode by length.
+// three literals at once, or a whole match length; a distance lookup of 11
+// bits a whole distance (gzip -1 writes DNA as matches of about 4 bytes at a
+// few hundred bytes' distance, whose codes and extra bits fit the indexes);
+// codes longer than the tables fall back to a canonical decode by length.
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -32,10 +33,10 @@ namespace {
 
 constexpr uint32_t FULL = 0xffffffffu;
 constexpr int LB_LIT = 11;               // literal/length table index bits
-constexpr int LB_DIST = 10;              // distance table index bits
+constexpr int LB_DIST = 11;              // distance table index bits
 constexpr uint32_t IF_RING = 4096;       // shared-memory output window
 constexpr uint32_t IF_FLUSH = 1024;      // bytes per aligned write to HBM
-constexpr int IF_WARPS = 2;              // streams per CTA
+constexpr int IF_WARPS = 1;              // streams per CTA
 static_assert(IF_RING >= IF_FLUSH + 2 * 258, "match sources must be in the ring or already in HBM");
 
 // RFC 1951 3.2.5: length codes 257..285 and distance codes 0..29
@@ -61,36 +62,48 @@ struct code_aux {
 
 struct __align__(16) warp_state {
     uint8_t ring[IF_RING];
-    // literal/length lookups: bits 0-3 bits consumed (0 = decode by length),
-    // bits 4-5 literals (1-3, bytes at bits 8, 16, 24; 0 = one non-literal
-    // symbol at bits 8-16)
+    // literal/length lookups (LB_LIT bits of input): bits 0-4 bits consumed,
+    // bits 5-7 kind: 1-3 literals (bytes at bits 8, 16, 24), K_LEN a match
+    // length (bits 8-16, extra bits that fit the index already added; bits
+    // 17-19 extra bits still to read), K_END end of block, K_BAD no valid
+    // symbol, 0 a code longer than the index (decode by length)
     uint32_t lit[1 << LB_LIT];
-    uint16_t lit1[1 << LB_LIT];  // one symbol per lookup: (length << 9) | symbol
-    uint16_t dist[1 << LB_DIST];
+    // distance lookups (LB_DIST bits): bits 0-4 bits consumed, bits 5-8
+    // extra bits still to read, bits 9-24 distance (folded extra added),
+    // bits 25-26 kind: 1 valid, 2 no valid distance, 0 decode by length
+    uint32_t dist[1 << LB_DIST];
+    uint16_t one[1 << LB_LIT];  // one symbol per lookup, (length << 9) | symbol
     code_aux la, da;
     uint32_t hist[16];
     uint8_t lens[320];
 };
 
+constexpr uint32_t K_LEN = 4, K_END = 5, K_BAD = 6;
+
 // Little-endian bit reader over the input (RFC 1951 3.1.1: bits from the
-// least significant end of each byte).  All lanes hold the same state.
+// least significant end of each byte).  All lanes hold the same state.  The
+// buffer above the `nb` valid bits holds either zeros or the input bits that
+// follow (a refill ORs the next eight bytes in place, so repeated bytes land
+// on identical bits); code that moves `ip` by hand clears it.
 struct bit_reader {
-    uint8_t const* in;
-    uint64_t ip;   // next byte to load
-    uint64_t end;  // end of this stream's bytes
-    uint64_t bb;   // bits not yet consumed, next bit at bit 0
-    uint32_t nb;   // number of them
-    // afterwards at least 32 bits are buffered (bytes past `end` read as
+    uint8_t const* in;  // 8-byte aligned, readable 32 bytes past `end`
+    uint64_t ip;        // byte of bit `nb` of the buffer
+    uint64_t end;       // end of this stream's bytes
+    uint64_t bb;
+    uint32_t nb;
+    // afterwards at least 56 bits are buffered (bytes past `end` read as
     // whatever follows; callers check ip against end)
     __device__ __forceinline__ void refill() {
-        if (nb <= 32) {
-            const uint64_t a = ip & ~uint64_t(3);
-            const uint32_t w0 = __ldg(reinterpret_cast<uint32_t const*>(in + a));
-            const uint32_t w1 = __ldg(reinterpret_cast<uint32_t const*>(in + a) + 1);
-            const uint32_t v = __funnelshift_r(w0, w1, (uint32_t)(ip & 3) * 8u);
-            bb |= (uint64_t)v << nb;
-            nb += 32;
-            ip += 4;
+        if (nb < 56) {
+            const uint64_t a = ip & ~uint64_t(7);
+            const uint32_t sh = (uint32_t)(ip & 7) * 8u;
+            const uint64_t w0 = __ldg(reinterpret_cast<unsigned long long const*>(in + a));
+            const uint64_t w1 = __ldg(reinterpret_cast<unsigned long long const*>(in + a) + 1);
+            const uint64_t v = sh ? (w0 >> sh) | (w1 << (64u - sh)) : w0;
+            bb |= v << nb;
+            const uint32_t take = (63u - nb) >> 3;
+            ip += take;
+            nb += 8u * take;
         }
     }
     __device__ __forceinline__ void drop(uint32_t n) {
@@ -107,6 +120,12 @@ struct bit_reader {
     // first byte not consumed (the buffer holds whole bytes after align())
     __device__ __forceinline__ uint64_t pos() const { return ip - nb / 8; }
     __device__ __forceinline__ void align() { drop(nb & 7u); }
+    // continue at byte position p (nothing buffered)
+    __device__ __forceinline__ void seek(uint64_t p) {
+        ip = p;
+        bb = 0;
+        nb = 0;
+    }
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt_() {
@@ -189,7 +208,8 @@ __device__ __noinline__ int decode_slow(uint64_t bb, code_aux const& a) {
     return -1;
 }
 
-// One symbol (at least 15 bits buffered); -1 for a bit string that is no code.
+// One symbol from a one-symbol table (at least 15 bits buffered); -1 for a
+// bit string that is no code.
 __device__ __forceinline__ int decode_sym(bit_reader& br, uint16_t const* tab, int lb, code_aux const& a) {
     const uint32_t e = tab[(uint32_t)br.bb & ((1u << lb) - 1u)];
     const uint32_t l = e >> 9;
@@ -203,29 +223,30 @@ __device__ __forceinline__ int decode_sym(bit_reader& br, uint16_t const* tab, i
     return r & 0xffff;
 }
 
-// The literal/length lookups from the one-symbol table: a literal whose code
-// leaves room in the index for the next code(s), when those are literals
-// too, yields two or three (the bits after a code are the index shifted
-// right by its length, upper bits zero, which select the same entry for any
-// code that fits).  Warp-collective.
-__device__ void pack_literals(warp_state& w, int lane) {
+// Literal/length lookups from the one-symbol table in w.one.  A literal whose
+// code leaves room in the index for the next code(s), when those are
+// literals too, yields two or three (the bits after a code are the index
+// shifted right by its length, upper bits zero, which select the same entry
+// for any code that fits); a length code whose extra bits fit in the index
+// comes with them added.  Warp-collective.
+__device__ void pack_litlen(warp_state& w, int lane) {
     __syncwarp();
     for (uint32_t x = (uint32_t)lane; x < (1u << LB_LIT); x += 32) {
-        const uint32_t e1 = w.lit1[x];
+        const uint32_t e1 = w.one[x];
         const uint32_t l1 = e1 >> 9, s1 = e1 & 511u;
         uint32_t out = 0;
-        if (l1 && s1 >= 256) {
-            out = (s1 << 8) | l1;
-        } else if (l1) {
+        if (l1 == 0) {
+            out = 0;
+        } else if (s1 < 256) {
             uint32_t tot = l1, cnt = 1;
             out = s1 << 8;
-            const uint32_t e2 = w.lit1[x >> tot];
+            const uint32_t e2 = w.one[x >> tot];
             const uint32_t l2 = e2 >> 9, s2 = e2 & 511u;
             if (l2 && s2 < 256 && tot + l2 <= (uint32_t)LB_LIT) {
                 out |= s2 << 16;
                 ++cnt;
                 tot += l2;
-                const uint32_t e3 = w.lit1[x >> tot];
+                const uint32_t e3 = w.one[x >> tot];
                 const uint32_t l3 = e3 >> 9, s3 = e3 & 511u;
                 if (l3 && s3 < 256 && tot + l3 <= (uint32_t)LB_LIT) {
                     out |= s3 << 24;
@@ -233,9 +254,46 @@ __device__ void pack_literals(warp_state& w, int lane) {
                     tot += l3;
                 }
             }
-            out |= (cnt << 4) | tot;
+            out |= (cnt << 5) | tot;
+        } else if (s1 == 256) {
+            out = (K_END << 5) | l1;
+        } else if (s1 <= 285) {
+            const uint32_t i = s1 - 257, ex = c_len_extra[i];
+            uint32_t len = c_len_base[i], c = l1, rem = ex;
+            if (l1 + ex <= (uint32_t)LB_LIT) {
+                len += (x >> l1) & ((1u << ex) - 1u);
+                c = l1 + ex;
+                rem = 0;
+            }
+            out = (rem << 17) | (len << 8) | (K_LEN << 5) | c;
+        } else {
+            out = (K_BAD << 5) | l1;
         }
         w.lit[x] = out;
+    }
+    __syncwarp();
+}
+
+// Distance lookups from the one-symbol table in w.one.  Warp-collective.
+__device__ void pack_dist(warp_state& w, int lane) {
+    __syncwarp();
+    for (uint32_t x = (uint32_t)lane; x < (1u << LB_DIST); x += 32) {
+        const uint32_t e1 = w.one[x];
+        const uint32_t l1 = e1 >> 9, s1 = e1 & 511u;
+        uint32_t out = 0;
+        if (l1 && s1 < 30) {
+            const uint32_t ex = c_dist_extra[s1];
+            uint32_t d = c_dist_base[s1], c = l1, rem = ex;
+            if (l1 + ex <= (uint32_t)LB_DIST) {
+                d += (x >> l1) & ((1u << ex) - 1u);
+                c = l1 + ex;
+                rem = 0;
+            }
+            out = (1u << 25) | (d << 9) | (rem << 5) | c;
+        } else if (l1) {
+            out = (2u << 25) | l1;
+        }
+        w.dist[x] = out;
     }
     __syncwarp();
 }
@@ -250,7 +308,7 @@ struct out_state {
 // Writes ring bytes [fp, fp + IF_FLUSH) to HBM (32 bytes per lane, aligned).
 __device__ __forceinline__ void flush_chunk(warp_state& w, out_state& os, int lane) {
     __syncwarp();
-    const uint32_t r = (uint32_t)(os.fp & (IF_RING - 1));
+    const uint32_t r = os.fp & (IF_RING - 1);
     uint4 const* src = reinterpret_cast<uint4 const*>(w.ring + r) + 2 * lane;
     uint4* dst = reinterpret_cast<uint4*>(os.o + os.fp) + 2 * lane;
     dst[0] = src[0];
@@ -265,18 +323,26 @@ __device__ __forceinline__ void flush_chunk(warp_state& w, out_state& os, int la
 // (i mod d): the period repeats), so no lane reads what this copy writes; a
 // ring slot read here is written here only when the write lands a whole ring
 // later (d + L > IF_RING), and then each round's writes wait for all reads.
+// The common case -- at most 32 bytes, no overlap, source in the ring -- is
+// one round.
 __device__ __forceinline__ void copy_match(warp_state& w, out_state& os, uint32_t d, uint32_t L, int lane) {
     __syncwarp();  // the bytes stored before are visible to every lane
+    const uint32_t i = (uint32_t)lane;
+    if (L <= 32 && d >= L && d + L <= IF_RING) {
+        if (i < L) w.ring[(os.op + i) & (IF_RING - 1)] = w.ring[(os.op - d + i) & (IF_RING - 1)];
+        os.op += L;
+        return;
+    }
     const bool wrap = d + L > IF_RING;
     for (uint32_t i0 = 0; i0 < L; i0 += 32) {
-        const uint32_t i = i0 + (uint32_t)lane;
+        const uint32_t j = i0 + i;
         uint8_t v = 0;
-        if (i < L) {
-            const uint32_t s = os.op - d + (d < L ? i % d : i);
-            v = d <= IF_RING ? w.ring[s & (IF_RING - 1)] : os.o[s];
+        if (j < L) {
+            const uint32_t src = os.op - d + (d < L ? j % d : j);
+            v = d <= IF_RING ? w.ring[src & (IF_RING - 1)] : os.o[src];
         }
         if (wrap) __syncwarp();
-        if (i < L) w.ring[(os.op + i) & (IF_RING - 1)] = v;
+        if (j < L) w.ring[(os.op + j) & (IF_RING - 1)] = v;
     }
     os.op += L;
 }
@@ -294,13 +360,9 @@ __device__ bool read_member_header(bit_reader& br) {
     br.get(8);
     br.get(8);  // XFL, OS
     if (flg & 4u) {  // FEXTRA
-        br.refill();
-        uint32_t xlen = br.get(16);
-        while (xlen > 0 && br.nb >= 8) {
-            br.get(8);
-            --xlen;
-        }
-        br.ip += xlen;  // nb is 0 here
+        const uint32_t xlen = br.get(16);
+        const uint64_t p = br.pos() + xlen;
+        br.seek(p);
         if (br.overrun()) return false;
     }
     for (uint32_t bit = 8; bit <= 16; bit <<= 1) {  // FNAME, FCOMMENT: zero-terminated
@@ -362,7 +424,6 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
             if (type == 0) {
                 // stored: LEN, NLEN at the next byte boundary, then LEN bytes
                 br.align();
-                br.refill();
                 const uint32_t len = br.get(16), nlen = br.get(16);
                 if ((len ^ 0xffffu) != nlen) {
                     st = STREAM_BAD;
@@ -372,27 +433,19 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                     st = STREAM_OVERFLOW;
                     break;
                 }
-                uint32_t left = len;
-                while (left > 0 && br.nb >= 8) {  // bytes already in the bit buffer
-                    if (os.op - os.fp >= IF_FLUSH) flush_chunk(w, os, lane);
-                    const uint32_t v = br.get(8);
-                    if (lane == 0) w.ring[os.op & (IF_RING - 1)] = (uint8_t)v;
-                    ++os.op;
-                    --left;
-                }
-                if (br.ip + left > br.end) {
+                const uint64_t p = br.pos();
+                if (p + len > br.end) {
                     st = STREAM_BAD;
                     break;
                 }
-                for (uint32_t i0 = 0; i0 < left; i0 += 32) {
+                for (uint32_t i0 = 0; i0 < len; i0 += 32) {
                     if (os.op - os.fp >= IF_FLUSH) flush_chunk(w, os, lane);
-                    const uint32_t i = i0 + (uint32_t)lane;
-                    const uint32_t n = min(32u, left - i0);
-                    if ((uint32_t)lane < n) w.ring[(os.op + lane) & (IF_RING - 1)] = br.in[br.ip + i];
+                    const uint32_t n = min(32u, len - i0);
+                    if ((uint32_t)lane < n) w.ring[(os.op + lane) & (IF_RING - 1)] = br.in[p + i0 + lane];
                     os.op += n;
                     __syncwarp();
                 }
-                br.ip += left;
+                br.seek(p + len);
                 continue;
             }
             if (type == 3) {
@@ -405,9 +458,10 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                 for (int i = lane; i < 288 + 32; i += 32)
                     w.lens[i] = i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : i < 288 ? 8 : 5;
                 __syncwarp();
-                build_code(w.lens, 288, w.lit1, LB_LIT, w.la, w.hist, lane, false);
-                build_code(w.lens + 288, 32, w.dist, LB_DIST, w.da, w.hist, lane, false);
-                pack_literals(w, lane);
+                build_code(w.lens, 288, w.one, LB_LIT, w.la, w.hist, lane, false);
+                pack_litlen(w, lane);
+                build_code(w.lens + 288, 32, w.one, LB_DIST, w.da, w.hist, lane, false);
+                pack_dist(w, lane);
             } else {
                 // dynamic codes (RFC 1951 3.2.7)
                 const uint32_t hlit = br.get(5) + 257, hdist = br.get(5) + 1, hclen = br.get(4) + 4;
@@ -423,7 +477,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                     if (lane == 0) w.lens[c_clen_order[i]] = (uint8_t)v;
                 }
                 __syncwarp();
-                if (!build_code(w.lens, 19, w.lit1, LB_LIT, w.la, w.hist, lane, true)) {
+                if (!build_code(w.lens, 19, w.one, LB_LIT, w.la, w.hist, lane, true)) {
                     st = STREAM_BAD;
                     break;
                 }
@@ -435,7 +489,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                         st = STREAM_BAD;
                         break;
                     }
-                    const int sym = decode_sym(br, w.lit1, LB_LIT, w.la);
+                    const int sym = decode_sym(br, w.one, LB_LIT, w.la);
                     if (sym < 0) {
                         st = STREAM_BAD;
                         break;
@@ -468,17 +522,22 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                 }
                 if (st != STREAM_OK) break;
                 __syncwarp();
-                if (w.lens[256] == 0 || !build_code(w.lens, (int)hlit, w.lit1, LB_LIT, w.la, w.hist, lane, false) ||
-                    !build_code(w.lens + hlit, (int)hdist, w.dist, LB_DIST, w.da, w.hist, lane, false)) {
+                if (w.lens[256] == 0 || !build_code(w.lens, (int)hlit, w.one, LB_LIT, w.la, w.hist, lane, false)) {
                     st = STREAM_BAD;
                     break;
                 }
-                pack_literals(w, lane);
+                pack_litlen(w, lane);
+                if (!build_code(w.lens + hlit, (int)hdist, w.one, LB_DIST, w.da, w.hist, lane, false)) {
+                    st = STREAM_BAD;
+                    break;
+                }
+                pack_dist(w, lane);
             }
-            // the block's symbols
+            // the block's symbols: after a refill at least 56 bits are
+            // buffered, enough for a whole match (15 + 5 + 15 + 13 bits)
             for (;;) {
                 if (os.op - os.fp >= IF_FLUSH) flush_chunk(w, os, lane);
-                if (br.nb <= 32) {
+                if (br.nb < 56) {
                     br.refill();
                     if (br.overrun()) {
                         st = STREAM_BAD;
@@ -486,53 +545,71 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
                     }
                 }
                 const uint32_t e = w.lit[(uint32_t)br.bb & ((1u << LB_LIT) - 1u)];
-                const uint32_t cnt = (e >> 4) & 3u;
-                if (cnt) {  // one to three literals
-                    if ((uint64_t)os.op + cnt > os.cap) {
+                const uint32_t kind = (e >> 5) & 7u;
+                if (kind - 1u < 3u) {  // one to three literals
+                    if ((uint64_t)os.op + kind > os.cap) {
                         st = STREAM_OVERFLOW;
                         break;
                     }
-                    if ((uint32_t)lane < cnt) w.ring[(os.op + lane) & (IF_RING - 1)] = (uint8_t)(e >> (8 + 8 * lane));
-                    os.op += cnt;
-                    br.drop(e & 15u);
+                    if ((uint32_t)lane < kind) w.ring[(os.op + lane) & (IF_RING - 1)] = (uint8_t)(e >> (8 + 8 * lane));
+                    os.op += kind;
+                    br.drop(e & 31u);
                     continue;
                 }
-                int sym;
-                if (e & 15u) {
-                    sym = (int)(e >> 8);
-                    br.drop(e & 15u);
+                uint32_t L;
+                if (kind == K_LEN) {
+                    br.drop(e & 31u);
+                    L = ((e >> 8) & 511u) + br.get((e >> 17) & 7u);
+                } else if (kind == K_END) {
+                    br.drop(e & 31u);
+                    break;
+                } else if (kind == K_BAD) {
+                    st = STREAM_BAD;
+                    break;
                 } else {
+                    // a code longer than the index
                     const int r = decode_slow(br.bb, w.la);
-                    sym = r < 0 ? -1 : (r & 0xffff);
-                    if (r >= 0) br.drop((uint32_t)r >> 16);
-                }
-                if (sym < 256) {
-                    if (sym < 0) {
+                    if (r < 0) {
                         st = STREAM_BAD;
                         break;
                     }
-                    if (os.op >= os.cap) {
-                        st = STREAM_OVERFLOW;
+                    br.drop((uint32_t)r >> 16);
+                    const uint32_t sym = (uint32_t)r & 0xffffu;
+                    if (sym < 256) {
+                        if (os.op >= os.cap) {
+                            st = STREAM_OVERFLOW;
+                            break;
+                        }
+                        if (lane == 0) w.ring[os.op & (IF_RING - 1)] = (uint8_t)sym;
+                        ++os.op;
+                        continue;
+                    }
+                    if (sym == 256) break;
+                    if (sym > 285) {
+                        st = STREAM_BAD;
                         break;
                     }
-                    if (lane == 0) w.ring[os.op & (IF_RING - 1)] = (uint8_t)sym;
-                    ++os.op;
-                    continue;
+                    L = c_len_base[sym - 257] + br.get(c_len_extra[sym - 257]);
                 }
-                if (sym == 256) break;
-                sym -= 257;
-                if (sym >= 29) {
+                const uint32_t de = w.dist[(uint32_t)br.bb & ((1u << LB_DIST) - 1u)];
+                const uint32_t dk = de >> 25;
+                uint32_t d;
+                if (dk == 1) {
+                    br.drop(de & 31u);
+                    d = ((de >> 9) & 0xffffu) + br.get((de >> 5) & 15u);
+                } else if (dk == 0) {
+                    const int r = decode_slow(br.bb, w.da);
+                    if (r < 0 || (r & 0xffff) >= 30) {
+                        st = STREAM_BAD;
+                        break;
+                    }
+                    br.drop((uint32_t)r >> 16);
+                    const uint32_t ds = (uint32_t)r & 0xffffu;
+                    d = c_dist_base[ds] + br.get(c_dist_extra[ds]);
+                } else {
                     st = STREAM_BAD;
                     break;
                 }
-                const uint32_t L = c_len_base[sym] + br.get(c_len_extra[sym]);
-                br.refill();
-                const int ds = decode_sym(br, w.dist, LB_DIST, w.da);
-                if (ds < 0 || ds >= 30) {
-                    st = STREAM_BAD;
-                    break;
-                }
-                const uint32_t d = c_dist_base[ds] + br.get(c_dist_extra[ds]);
                 if (d > os.op - member0) {
                     st = STREAM_BAD;
                     break;
@@ -552,7 +629,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
         br.get(16);
         br.refill();
         const uint32_t isize = br.get(16) | (br.get(16) << 16);
-        if (br.overrun() || isize != (uint32_t)(os.op - member0)) {
+        if (br.overrun() || isize != os.op - member0) {
             st = STREAM_BAD;
             break;
         }
@@ -563,9 +640,7 @@ __global__ void __launch_bounds__(IF_WARPS * 32) k_inflate(stream_set s) {
         }
         if (p == br.end) break;
         // another member follows (anything else fails its header check)
-        br.ip = p;
-        br.bb = 0;
-        br.nb = 0;
+        br.seek(p);
     }
     __syncwarp();
     if (st == STREAM_OK) {
