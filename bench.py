@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="pangenome")
     ap.add_argument("--genomes", type=int, default=0, help="override genome count (0 = workload's)")
+    ap.add_argument("--genome-scale", type=float, default=1.0,
+                    help="scale the workload's genome lengths (small cases for profiling; 1 = the workload)")
     ap.add_argument("--ref-slices", type=int, default=8,
                     help="reference CPU runs: 1/N of every genome per step (rotating over the N slices)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -250,9 +252,9 @@ class ReferenceSample:
     collection's divergence structure; step i runs slice i mod nslices, so
     consecutive steps cover the whole collection."""
 
-    def __init__(self, workload, n_genomes, nslices, threads, seed=1):
+    def __init__(self, workload, n_genomes, nslices, threads, seed=1, scale=1.0):
         from cdbg_gpu import synth
-        p, _, self.k, blog2 = synth.preset(workload, seed=seed)
+        p, _, self.k, blog2 = synth.preset(workload, seed=seed, scale=scale)
         self.B = 1 << blog2
         self.n, self.S, self.threads = n_genomes, nslices, threads
         self.seq, self.lens, self.per = synth.collection(p, n_genomes)
@@ -281,7 +283,7 @@ class ReferenceSample:
         shutil.rmtree(self.work, ignore_errors=True)
 
 
-def workload_name(n_genomes, k, B, workload="pangenome"):
+def workload_name(n_genomes, k, B, workload="pangenome", scale=1.0):
     from cdbg_gpu.native import best_m
     shape = {
         "pangenome": "%d genomes x 4.8 Mbp (0.1-2%% SNPs, 1-200 contigs)",
@@ -289,13 +291,14 @@ def workload_name(n_genomes, k, B, workload="pangenome"):
         "largek": "%d genomes x 4.8 Mbp + 2%% tandem repeats + 200 shared 1-5 kbp repeats each",
         "skewed": "%d genomes x 1-6 Mbp log-uniform, 10%% homopolymer/dinucleotide runs",
     }.get(workload, "%d genomes")
-    return "%s: %s, k=%d, m=%d, %d buckets" % (workload, shape % n_genomes, k, best_m(k), B)
+    name = "%s: %s, k=%d, m=%d, %d buckets" % (workload, shape % n_genomes, k, best_m(k), B)
+    return name if scale == 1.0 else name + ", genome lengths x%g" % scale
 
 
-def workload_config(workload, n_genomes, k, B, seq_bytes):
+def workload_config(workload, n_genomes, k, B, seq_bytes, scale=1.0):
     """The `config` both arms print (identical, so the lines compare)."""
     from cdbg_gpu.native import best_m
-    return {"workload": workload_name(n_genomes, k, B, workload), "genomes": n_genomes, "k": k, "m": best_m(k),
+    return {"workload": workload_name(n_genomes, k, B, workload, scale), "genomes": n_genomes, "k": k, "m": best_m(k),
             "buckets": B,
             "l2": ("inputs (%.1f GB) larger than L2" % (seq_bytes / 1e9)) if seq_bytes > 126e6 else
                   ("inputs (%.0f MB) smaller than L2, not flushed between steps" % (seq_bytes / 1e6))}
@@ -313,7 +316,7 @@ def reference_arm(a):
     _, n_genomes, k, blog2 = synth.preset(a.workload)
     if a.genomes:
         n_genomes = a.genomes
-    R = ReferenceSample(a.workload, n_genomes, a.ref_slices, threads)
+    R = ReferenceSample(a.workload, n_genomes, a.ref_slices, threads, scale=a.genome_scale)
     try:
         i = 0
         for _ in range(a.warmup):
@@ -327,7 +330,7 @@ def reference_arm(a):
             s_tot += s
             secs.append(s)
         sample = R.describe(km_tot // max(a.steps, 1))
-        cfg = workload_config(a.workload, n_genomes, k, R.B, R.seq.nbytes)
+        cfg = workload_config(a.workload, n_genomes, k, R.B, R.seq.nbytes, a.genome_scale)
     finally:
         R.close()
     v = km_tot / s_tot
@@ -359,7 +362,7 @@ def main_gpu(a):
         if world > 1:
             torch.distributed.barrier()
 
-    p, n_genomes, k, blog2 = synth.preset(a.workload, seed=1 + rank)
+    p, n_genomes, k, blog2 = synth.preset(a.workload, seed=1 + rank, scale=a.genome_scale)
     if a.genomes:
         n_genomes = a.genomes
     B = 1 << blog2
@@ -543,7 +546,7 @@ def main_gpu(a):
     # ---- CPU baseline (reference, bounded sample), rank 0 at N = 1
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(REF_P12):
-        R = ReferenceSample(a.workload, n_genomes, a.ref_slices, os.cpu_count() or 1)
+        R = ReferenceSample(a.workload, n_genomes, a.ref_slices, os.cpu_count() or 1, scale=a.genome_scale)
         try:
             km, s, det = R.run(0)
             cpu = {"value": km / s, "unit": "k-mers/s", "cores": os.cpu_count(), "kind": "reference",
@@ -556,7 +559,7 @@ def main_gpu(a):
     # (one thread: deterministic ids and order) on this build's bucket files
     check = None
     if rank == 0 and a.check:
-        R = ReferenceSample(a.workload, n_genomes, a.ref_slices, os.cpu_count() or 1)
+        R = ReferenceSample(a.workload, n_genomes, a.ref_slices, os.cpu_count() or 1, scale=a.genome_scale)
         try:
             lst, skm = R.slice(0)
             sfiles = [l.strip() for l in open(lst) if l.strip()]
@@ -585,7 +588,7 @@ def main_gpu(a):
         line = {"metric": "phase1+2 k-mers/s", "value": value, "unit": "k-mers/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64" if k <= 31 else "u128", "data": "synthetic",
-                "config": workload_config(a.workload, n_genomes, k, B, seq.nbytes),
+                "config": workload_config(a.workload, n_genomes, k, B, seq.nbytes, a.genome_scale),
                 "parallelism": "replicas%d" % world,
                 "workload_detail": {"kmers_per_step": int(job_kmers), "bases": int(seq.nbytes),
                                     "generate_s": gen_s, "tuning": eng.tuning()},

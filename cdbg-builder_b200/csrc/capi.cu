@@ -6,9 +6,11 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <deque>
 #include <functional>
 #include <mutex>
 #include <map>
+#include <memory>
 #include <cstdio>
 #include <cstring>
 #include <filesystem>
@@ -1296,6 +1298,18 @@ int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phas
         pp.union_bitmaps = e->tune.union_lists == 0;
         pp.group_bytes = e->tune.table_group_mb ? (uint64_t)e->tune.table_group_mb << 20 : ~0ull;
         pp.to_host = false;  // outputs accumulate in HBM
+        e->frag_sink.streamed = 0;
+        if (!p->outputs_to_host && e->frag_sink.fn && e->h_frag.p && e->h_frag.cap) {
+            // the caller writes each batch's fragments out while later batches
+            // run: stream them into the (already large enough, from earlier
+            // builds) pinned buffer and tell it
+            pp.frag_host = (uint8_t*)e->h_frag.p;
+            pp.frag_host_cap = e->h_frag.cap;
+            pp.copy_st = e->copy_st;
+            pp.copy_ev = e->copy_ev;
+            pp.on_frag = e->frag_sink.fn;
+            pp.on_frag_ctx = e->frag_sink.ctx;
+        }
         if (p->outputs_to_host && e->h_frag.p && e->h_frag.cap) {
             // stream each batch's fragments into the (already large enough,
             // from earlier builds) pinned buffer while phase 2 goes on
@@ -1313,6 +1327,7 @@ int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phas
         cdbg::phase2_result out;
         out.state = &e->p2;
         cdbg::run_phase2(rs, pp, e->A, e->st, e->d_err, out);
+        if (pp.on_frag) e->frag_sink.streamed = out.frag_host_copied;
         const uint64_t nwords = (out.nbits + 63) / 64;
         if (p->outputs_to_host) {
             const bool streamed = pp.frag_host && out.frag_host_copied == out.frag_nbytes;
@@ -1401,6 +1416,91 @@ int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_par
     return build_core(e, p, ph1, r, nullptr);
 }
 
+namespace {
+// Writes the fragment file while phase 2 runs: phase 2 streams each batch's
+// fragments to the engine's pinned buffer (engine.frag_sink) and this writer,
+// on its own thread, writes each range once its copy has completed.
+struct frag_file_writer {
+    struct item {
+        uint64_t off, n;
+        cudaEvent_t ev;
+    };
+    cdbg_engine* e;
+    cdbg::io::range_file file;
+    uint32_t threads;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<item> q;
+    std::vector<cudaEvent_t> events;
+    bool done = false;
+    std::exception_ptr err;
+    std::thread t;
+
+    frag_file_writer(cdbg_engine* en, std::string const& path, uint32_t th) : e(en), file(path), threads(th) {
+        t = std::thread([this] { run(); });
+    }
+    ~frag_file_writer() {
+        try {
+            drain();
+        } catch (...) {
+        }
+    }
+    // phase 2 queued fragment bytes [off, off + n) to the pinned buffer on the
+    // copy stream
+    static void hook(void* ctx, uint64_t off, uint64_t n) {
+        auto* w = static_cast<frag_file_writer*>(ctx);
+        cudaEvent_t ev;
+        CDBG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        {
+            std::lock_guard<std::mutex> lk(w->mu);
+            w->events.push_back(ev);
+        }
+        CDBG_CUDA(cudaEventRecord(ev, w->e->copy_st));
+        {
+            std::lock_guard<std::mutex> lk(w->mu);
+            w->q.push_back({off, n, ev});
+        }
+        w->cv.notify_one();
+    }
+    void run() {
+        cudaSetDevice(e->device);
+        for (;;) {
+            item it;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return done || !q.empty(); });
+                if (q.empty()) return;
+                it = q.front();
+                q.pop_front();
+            }
+            if (err) continue;
+            try {
+                CDBG_CUDA(cudaEventSynchronize(it.ev));
+                file.write(static_cast<uint8_t const*>(e->h_frag.p) + it.off, it.off, it.n, threads);
+            } catch (...) {
+                err = std::current_exception();
+            }
+        }
+    }
+    // every queued range written (before the pinned buffer may move)
+    void drain() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            done = true;
+        }
+        cv.notify_one();
+        if (t.joinable()) t.join();
+        for (auto ev : events) cudaEventDestroy(ev);
+        events.clear();
+        if (err) {
+            std::exception_ptr x = err;
+            err = nullptr;
+            std::rethrow_exception(x);
+        }
+    }
+};
+}  // namespace
+
 int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_build_result* r) {
     if (!e || !a || !r || (!a->files && a->num_files)) {
         g_last_error = "null argument";
@@ -1424,6 +1524,20 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             if (p.num_colors >= (1u << 28)) return false;
             return phase1_from_files(e, files, th, p.k, m, p.num_buckets, rt, sl, h2d, &inb);
         };
+        // the fragment file is written batch by batch while phase 2 runs
+        std::unique_ptr<frag_file_writer> fw;
+        if (a->frag_path) {
+            fw.reset(new frag_file_writer(e, a->frag_path, th));
+            e->frag_sink.fn = &frag_file_writer::hook;
+            e->frag_sink.ctx = fw.get();
+        }
+        struct unhook {
+            cdbg_engine* e;
+            ~unhook() {
+                e->frag_sink.fn = nullptr;
+                e->frag_sink.ctx = nullptr;
+            }
+        } unhook_{e};
         bool redo = false;
         int rc = build_core(e, &p, ph1, r, &redo);
         if (rc != 0) return rc;
@@ -1437,6 +1551,10 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             rc = cdbg_gpu_build(e, &b, &p, r);
             if (rc != 0) return rc;
         }
+        const uint64_t streamed = fw ? std::min<uint64_t>(e->frag_sink.streamed, r->frag_nbytes) : 0;
+        // the pinned fragment buffer may move below unless it holds them all:
+        // then the streamed ranges must be written first
+        if (fw && streamed < r->frag_nbytes) fw->drain();
         if (!p.outputs_to_host) {
             // outputs are in HBM: the frag bytes, color-set words and the
             // Elias-Fano encoding of the class offsets (made on the device)
@@ -1447,11 +1565,19 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             const uint64_t nwords = (r->class_bits + 63) / 64;
             if (a->color_sets_path)
                 cdbg::ef_encode(r->class_offsets, r->n_color_sets, r->class_bits, e->A, e->st, ef);
-            uint8_t* hf = (uint8_t*)e->h_frag.ensure(r->frag_nbytes + 8);
+            void* hf_before = e->h_frag.p;
+            // (a buffer that took every fragment stays where the writer reads it)
+            uint8_t* hf = fw && streamed == r->frag_nbytes && r->frag_nbytes
+                              ? (uint8_t*)e->h_frag.p
+                              : (uint8_t*)e->h_frag.ensure(r->frag_nbytes + 8);
+            // bytes of hf already holding the fragments (the streamed prefix,
+            // unless the buffer just moved)
+            const uint64_t have = (void*)hf == hf_before ? streamed : 0;
             uint64_t* hw = (uint64_t*)e->h_words.ensure(8 * nwords + 8);
             uint64_t* hl = (uint64_t*)e->h_offsets.ensure(8 * (ef.low_words + ef.high_words) + 16);
-            if (r->frag_nbytes)
-                CDBG_CUDA(cudaMemcpyAsync(hf, r->frag_bytes, r->frag_nbytes, cudaMemcpyDeviceToHost, e->st));
+            if (r->frag_nbytes > have)
+                CDBG_CUDA(cudaMemcpyAsync(hf + have, r->frag_bytes + have, r->frag_nbytes - have,
+                                          cudaMemcpyDeviceToHost, e->st));
             if (a->color_sets_path) {
                 if (nwords)
                     CDBG_CUDA(cudaMemcpyAsync(hw, r->class_words, 8 * nwords, cudaMemcpyDeviceToHost, e->st));
@@ -1474,7 +1600,16 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
                         cs_err = std::current_exception();
                     }
                 });
-            if (a->frag_path) cdbg::io::write_file_parallel(a->frag_path, hf, r->frag_nbytes, th);
+            if (fw) {
+                try {
+                    fw->drain();  // the streamed ranges are in the file
+                    fw->file.write(hf + streamed, streamed, r->frag_nbytes - streamed, th);
+                    fw->file.finish(r->frag_nbytes);
+                } catch (...) {
+                    if (cs_writer.joinable()) cs_writer.join();
+                    throw;
+                }
+            }
             if (cs_writer.joinable()) cs_writer.join();
             if (cs_err) std::rethrow_exception(cs_err);
             r->frag_bytes = hf;

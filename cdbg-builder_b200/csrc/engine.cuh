@@ -55,6 +55,14 @@ struct cdbg_engine {
     // inflated input sequences of cdbg_gpu_build_files, read while the
     // device works on the groups read before
     pinned_buffer h_in;
+    // set by cdbg_gpu_build_files while it writes the fragment file: phase 2
+    // streams each batch's fragments to h_frag and calls `fn` (when h_frag is
+    // already large enough); `streamed` receives the bytes so queued
+    struct frag_sink_hook {
+        void (*fn)(void*, uint64_t, uint64_t) = nullptr;
+        void* ctx = nullptr;
+        uint64_t streamed = 0;
+    } frag_sink;
     // decompressed bucket ranges of the drop-in phase 2 (one read while the
     // device processes the other)
     pinned_buffer h_bk[2];

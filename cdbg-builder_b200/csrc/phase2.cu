@@ -172,6 +172,19 @@ static_assert(sizeof(slot_t<uint64_t>) == 16, "slot layout");
 static_assert(sizeof(slot_t<u128>) == 32, "slot layout");
 constexpr uint64_t MAX_BATCH_RECORDS = (1ull << 28) - 2;  // owner field of `om`
 
+// First slot of key x in a table of `cap` slots (cap < 2^32): the key folded
+// to 64 bits, an odd-constant multiply, and its top 32 bits scaled to the
+// capacity.  Table positions decide no output (nodes are numbered by first
+// occurrence, not by slot), only probe lengths.
+__device__ __forceinline__ uint32_t slot_of(uint64_t x, uint32_t cap) {
+    const uint64_t h = (x ^ (x >> 31)) * 0x9e3779b97f4a7c15ULL;
+    return (uint32_t)(((h >> 32) * (uint64_t)cap) >> 32);
+}
+__device__ __forceinline__ uint32_t slot_of(u128 x, uint32_t cap) {
+    const uint64_t f = (uint64_t)x ^ ((uint64_t)(x >> 64) * 0xc2b2ae3d27d4eb4fULL);
+    return slot_of(f, cap);
+}
+
 // A 64-bit-key slot's key and (rank | om << 32) in one 16-byte load that
 // bypasses L1.
 __device__ __forceinline__ void slot_load(slot_t<uint64_t> const* e, uint64_t& key, uint64_t& ro) {
@@ -188,8 +201,9 @@ template <typename K>
 __device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off0, uint64_t off, uint64_t cap, K x,
                                                  uint64_t& ro) {
     const K EMPTY = kmer_ops<K>::empty();
-    uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
-    for (uint64_t i = 0; i < cap; ++i) {
+    const uint32_t cap32 = (uint32_t)cap;
+    uint32_t s = slot_of(x, cap32);
+    for (uint32_t i = 0; i < cap32; ++i) {
         slot_t<K>* e = &slots[off + s - off0];
         if constexpr (sizeof(K) == 8) {
             uint64_t cur, v;
@@ -212,7 +226,7 @@ __device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off0
                 return off + s;
             }
         }
-        if (++s == cap) s = 0;
+        s = s + 1 == cap32 ? 0u : s + 1;
     }
     return ~0ull;
 }
@@ -1587,27 +1601,31 @@ __global__ void k_node_cid(uint64_t D, uint32_t const* __restrict__ n_rec, uint3
 // Node index of k-mer x, NONE32 when absent.  The tables are read-only once
 // the nodes are numbered, so the probes go through the read-only path, and a
 // 64-bit-key slot's probe load brings its rank (the node index) along.
+// Probes from slot s on: node index of x, or NONE32.
 template <typename K>
-__device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb, K x) {
+__device__ __forceinline__ uint32_t node_probe(slot_t<K> const* t, uint32_t cap, uint32_t s, K x) {
     const K EMPTY = kmer_ops<K>::empty();
-    const uint64_t off = T.tab_off[tb] - T.off0, cap = T.tab_cap[tb];
-    uint64_t s = __umul64hi(kmer_ops<K>::hash(x), cap);
-    for (uint64_t i = 0; i < cap; ++i) {
-        slot_t<K> const* e = &T.slots[off + s];
+    for (uint32_t i = 0; i < cap; ++i) {
+        slot_t<K> const* e = &t[s];
         if constexpr (sizeof(K) == 8) {
             const ulonglong2 v = __ldg(reinterpret_cast<ulonglong2 const*>(e));
             if (v.x == x) return (uint32_t)v.y;
             if (v.x == EMPTY) return NONE32;
         } else {
             const ulonglong2 kv = __ldg(reinterpret_cast<ulonglong2 const*>(e));
-            const uint32_t rank = __ldg(&e->rank);
             const K cur = ((u128)kv.y << 64) | (u128)kv.x;
-            if (cur == x) return rank;
+            if (cur == x) return __ldg(&e->rank);
             if (cur == EMPTY) return NONE32;
         }
-        if (++s == cap) s = 0;
+        s = s + 1 == cap ? 0u : s + 1;
     }
     return NONE32;
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb, K x) {
+    const uint32_t cap = (uint32_t)T.tab_cap[tb];
+    return node_probe<K>(T.slots + (T.tab_off[tb] - T.off0), cap, slot_of(x, cap), x);
 }
 
 // Nodes [*nb, *ne) (one bucket group's, numbered on the device).
@@ -1623,6 +1641,8 @@ __global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* n
     const K msk = ops::mask(k);
     const K rev = ops::revcomp(can, k);
     const uint32_t tb = n_bucket[n] - T.b0;
+    const uint32_t cap = (uint32_t)T.tab_cap[tb];
+    slot_t<K> const* t = T.slots + (T.tab_off[tb] - T.off0);
     const uint32_t top = 2 * (k - 1);
     uint32_t out = 0;
     // appending nt to x prepends 3 - nt to revcomp(x): (rc(x) >> 2) | (3 - nt) << 2(k-1)
@@ -1631,10 +1651,12 @@ __global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* n
         const K hi = (K)(3u - nt) << top;
         const K f = ((can << 2) | (K)nt) & msk;
         const K fr = (rev >> 2) | hi;
-        if (node_lookup<K>(T, tb, f <= fr ? f : fr) != NONE32) out |= 1u << nt;
+        const K cf = f <= fr ? f : fr;
+        if (node_probe<K>(t, cap, slot_of(cf, cap), cf) != NONE32) out |= 1u << nt;
         const K r = ((rev << 2) | (K)nt) & msk;
         const K rr = (can >> 2) | hi;
-        if (node_lookup<K>(T, tb, r <= rr ? r : rr) != NONE32) out |= 1u << (4 + nt);
+        const K cr = r <= rr ? r : rr;
+        if (node_probe<K>(t, cap, slot_of(cr, cap), cr) != NONE32) out |= 1u << (4 + nt);
     }
     n_mask[n] = (uint8_t)out;
 }
@@ -2818,6 +2840,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
             CDBG_CUDA(cudaMemcpyAsync(p.frag_host + old_n, dfrag.p + old_n, fbytes, cudaMemcpyDeviceToHost,
                                       p.copy_st));
             out.frag_host_copied = dfrag.n;
+            if (p.on_frag) p.on_frag(p.on_frag_ctx, old_n, fbytes);
         }
     }
     if (!p.to_host && p.copy_st) {

@@ -101,6 +101,11 @@ struct phase2_params {
     // as they fit in `frag_host_cap` (nothing is streamed when null).
     uint8_t* frag_host = nullptr;
     uint64_t frag_host_cap = 0;
+    // called on the host right after a batch's fragment bytes [off, off + n)
+    // are queued to frag_host on copy_st (a consumer may write them out while
+    // later batches run)
+    void (*on_frag)(void* ctx, uint64_t off, uint64_t n) = nullptr;
+    void* on_frag_ctx = nullptr;
     // likewise the class dictionary's completed bit-vector words and class
     // offsets (capacities in entries)
     uint64_t* words_host = nullptr;

@@ -313,54 +313,64 @@ bool read_files_into(std::vector<std::string> const& files, size_t first, size_t
     return true;
 }
 
-void write_file_parallel(std::string const& path, uint8_t const* data, uint64_t n, uint32_t threads) {
-    const int fd = ::open(path.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0644);
-    if (fd < 0) throw std::runtime_error("cannot open output file: " + path + ": " + std::strerror(errno));
-    if (n == 0) {
-        ::close(fd);
-        return;
-    }
-    if (::ftruncate(fd, (off_t)n) != 0) {
-        ::close(fd);
-        throw std::runtime_error("cannot size output file: " + path + ": " + std::strerror(errno));
-    }
+range_file::range_file(std::string const& path) : m_path(path) {
+    m_fd = ::open(path.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0644);
+    if (m_fd < 0) throw std::runtime_error("cannot open output file: " + path + ": " + std::strerror(errno));
+    struct statfs fs;
+    constexpr long kTmpfsMagic = 0x01021994;
+    m_tmpfs = ::fstatfs(m_fd, &fs) == 0 && (long)fs.f_type == kTmpfsMagic;
+}
+
+range_file::~range_file() {
+    if (m_fd >= 0) ::close(m_fd);
+}
+
+void range_file::write(uint8_t const* data, uint64_t off, uint64_t n, uint32_t threads) {
+    if (n == 0) return;
     const uint64_t piece = std::max<uint64_t>(32ull << 20, (n + threads - 1) / std::max<uint32_t>(threads, 1));
     const size_t np = (size_t)((n + piece - 1) / piece);
     std::atomic<bool> bad{false};
-    // On a RAM-backed file system (tmpfs) writes to one file take the file's
-    // lock one call at a time, so parallel writes run as one; a shared
-    // mapping filled by several threads fills its pages in parallel.  On a
-    // disk file system the mapping is slower (its page faults and dirty-page
-    // accounting), and positional writes of disjoint ranges are used.  The
-    // space is reserved first (fallocate), so a full file system is an error
-    // here rather than a fault in the copy.
-    struct statfs fs;
-    constexpr long kTmpfsMagic = 0x01021994;
     void* map = MAP_FAILED;
-    if (::fstatfs(fd, &fs) == 0 && (long)fs.f_type == kTmpfsMagic && ::fallocate(fd, 0, 0, (off_t)n) == 0)
-        map = ::mmap(nullptr, (size_t)n, PROT_WRITE, MAP_SHARED, fd, 0);
+    const uint64_t pg = (uint64_t)::sysconf(_SC_PAGESIZE);
+    const uint64_t a = off & ~(pg - 1);
+    if (m_tmpfs && ::fallocate(m_fd, 0, (off_t)off, (off_t)n) == 0)
+        map = ::mmap(nullptr, (size_t)(off + n - a), PROT_WRITE, MAP_SHARED, m_fd, (off_t)a);
     if (map != MAP_FAILED) {
-        uint8_t* dst = (uint8_t*)map;
+        uint8_t* dst = (uint8_t*)map + (off - a);
         parallel_for(np, threads, [&](size_t i) {
-            const uint64_t a = i * piece, b = std::min<uint64_t>(n, a + piece);
-            std::memcpy(dst + a, data + a, (size_t)(b - a));
+            const uint64_t x = i * piece, y = std::min<uint64_t>(n, x + piece);
+            std::memcpy(dst + x, data + x, (size_t)(y - x));
         });
-        if (::munmap(map, (size_t)n) != 0) bad = true;
+        if (::munmap(map, (size_t)(off + n - a)) != 0) bad = true;
     } else {
         parallel_for(np, threads, [&](size_t i) {
-            uint64_t a = i * piece;
-            const uint64_t b = std::min<uint64_t>(n, a + piece);
-            while (a < b) {
-                const ssize_t w = ::pwrite(fd, data + a, (size_t)std::min<uint64_t>(b - a, 1ull << 30), (off_t)a);
+            uint64_t x = i * piece;
+            const uint64_t y = std::min<uint64_t>(n, x + piece);
+            while (x < y) {
+                const ssize_t w =
+                    ::pwrite(m_fd, data + x, (size_t)std::min<uint64_t>(y - x, 1ull << 30), (off_t)(off + x));
                 if (w <= 0) {
                     bad = true;
                     return;
                 }
-                a += (uint64_t)w;
+                x += (uint64_t)w;
             }
         });
     }
-    if (::close(fd) != 0 || bad) throw std::runtime_error("short write to " + path);
+    if (bad) throw std::runtime_error("short write to " + m_path);
+}
+
+void range_file::finish(uint64_t total) {
+    const int fd = m_fd;
+    m_fd = -1;
+    const bool ok = ::ftruncate(fd, (off_t)total) == 0;
+    if (::close(fd) != 0 || !ok) throw std::runtime_error("cannot finish output file " + m_path);
+}
+
+void write_file_parallel(std::string const& path, uint8_t const* data, uint64_t n, uint32_t threads) {
+    range_file f(path);
+    f.write(data, 0, n, threads);
+    f.finish(n);
 }
 
 // ---------------------------------------------------------------- buckets

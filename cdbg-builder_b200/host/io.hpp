@@ -60,9 +60,29 @@ void read_raw_files(std::vector<std::string> const& files, uint32_t threads, cha
 bool read_files_into(std::vector<std::string> const& files, size_t first, size_t count, uint32_t color_base,
                      uint32_t threads, char* dst, uint64_t cap, seq_batch& out);
 
-// Write n bytes to `path` with `threads` threads (positional writes of
-// disjoint ranges).
+// Write n bytes to `path` with `threads` threads (range_file).
 void write_file_parallel(std::string const& path, uint8_t const* data, uint64_t n, uint32_t threads);
+
+// An output file written range by range, in any order, each range by several
+// threads: on a RAM-backed file system (tmpfs), where writes to one file take
+// its lock one call at a time, through shared mappings of the range filled in
+// parallel (the space reserved first, so a full file system is an error, not
+// a fault); elsewhere by positional writes of disjoint pieces.
+class range_file {
+public:
+    explicit range_file(std::string const& path);
+    ~range_file();
+    range_file(range_file const&) = delete;
+    range_file& operator=(range_file const&) = delete;
+    void write(uint8_t const* data, uint64_t off, uint64_t n, uint32_t threads);
+    // sets the file's size and closes it
+    void finish(uint64_t total);
+
+private:
+    std::string m_path;
+    int m_fd = -1;
+    bool m_tmpfs = false;
+};
 
 // ---- bucket files (bucket_io.hpp:19-40) ------------------------------------
 // Append one LZ4 frame per non-empty bucket slice to open bucket files.
