@@ -478,7 +478,7 @@ def main_gpu(a):
                    # phase 1 here spans the host inflate/parse it overlaps with;
                    # the rest of the call after phase 2 is the output copies and writes
                    "last_call_ms": {"phase1_with_read": re2.ms_phase1, "phase2": re2.ms_phase2,
-                                    "total": re2.ms_total},
+                                    "outputs_after_phase2": re2.ms_outputs, "total": re2.ms_total},
                    "h2d_bytes_per_step": int(re2.h2d_bytes), "d2h_bytes_per_step": int(re2.d2h_bytes),
                    "path": "cdbg_gpu_build_files: %d gzip FASTA files (%.2f GB) -> frag_unitigs.bin (%.2f GB) + "
                            ".color_sets in %s, wall time per call" % (len(files), gz_bytes / 1e9,

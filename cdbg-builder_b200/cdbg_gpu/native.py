@@ -92,7 +92,7 @@ class BuildResult(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
                 ("n_bases", ctypes.c_uint64),
                 ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
-                ("ms_total", ctypes.c_double)]
+                ("ms_total", ctypes.c_double), ("ms_outputs", ctypes.c_double)]
 
 
 class Merged(ctypes.Structure):

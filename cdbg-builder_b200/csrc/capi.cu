@@ -1551,6 +1551,7 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             rc = cdbg_gpu_build(e, &b, &p, r);
             if (rc != 0) return rc;
         }
+        const auto t_built = std::chrono::steady_clock::now();
         const uint64_t streamed = fw ? std::min<uint64_t>(e->frag_sink.streamed, r->frag_nbytes) : 0;
         // the pinned fragment buffer may move below unless it holds them all:
         // then the streamed ranges must be written first
@@ -1618,7 +1619,9 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             e->A.reset();
         }
         (void)inb;
-        r->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        const auto t_end = std::chrono::steady_clock::now();
+        r->ms_outputs = std::chrono::duration<double, std::milli>(t_end - t_built).count();
+        r->ms_total = std::chrono::duration<double, std::milli>(t_end - t0).count();
         return 0;
     } catch (std::exception const& ex) {
         if (e) e->A.reset();

@@ -258,6 +258,8 @@ typedef struct cdbg_build_result {
     uint64_t h2d_bytes, d2h_bytes;
     uint64_t n_bases;            /* bases in ACGT runs >= k */
     double ms_phase1, ms_phase2, ms_total; /* device time (CUDA events) */
+    double ms_outputs;           /* cdbg_gpu_build_files: wall time after phase 2
+                                    (output copies and file writes left) */
 } cdbg_build_result;
 
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
