@@ -127,9 +127,6 @@ __host__ __device__ __forceinline__ uint64_t set_hash_final(uint64_t acc, uint64
 }
 
 // ------------------------------------------------------------------ tables
-__device__ __forceinline__ uint64_t key_cas(uint64_t* a, uint64_t cmp, uint64_t val) {
-    return (uint64_t)atomicCAS((unsigned long long*)a, (unsigned long long)cmp, (unsigned long long)val);
-}
 __device__ __forceinline__ u128 key_cas(u128* a, u128 cmp, u128 val) {
     uint64_t olo, ohi;
     const uint64_t clo = (uint64_t)cmp, chi = (uint64_t)(cmp >> 64);
@@ -213,7 +210,8 @@ __device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off0
                 return off + s;
             }
             if (cur == EMPTY) {
-                const K old = key_cas(&e->key, EMPTY, x);
+                const K old = (K)atomicCAS((unsigned long long*)&e->key, (unsigned long long)EMPTY,
+                                           (unsigned long long)x);
                 if (old == EMPTY || old == x) {
                     ro = v;
                     return off + s;
@@ -223,6 +221,43 @@ __device__ __forceinline__ uint64_t table_upsert(slot_t<K>* slots, uint64_t off0
             const K old = key_cas(&e->key, EMPTY, x);  // atomic 128-bit read-or-claim
             if (old == EMPTY || old == x) {
                 ro = *(volatile uint64_t const*)&e->rank;
+                return off + s;
+            }
+        }
+        s = s + 1 == cap32 ? 0u : s + 1;
+    }
+    return ~0ull;
+}
+
+// 64-bit-key tables: insert-or-find like table_upsert, but an empty slot is
+// claimed together with the payload a new k-mer gets -- its rank and om --
+// in one 128-bit compare-and-swap of the whole slot (key, rank, om), so the
+// occurrence that creates a k-mer needs no further atomics.  `claimed` tells
+// whether this call wrote the payload; otherwise `ro` is the slot's (rank |
+// om << 32) as read (the caller's updates as in table_upsert).
+__device__ __forceinline__ uint64_t table_claim(slot_t<uint64_t>* slots, uint64_t off0, uint64_t off, uint64_t cap,
+                                                uint64_t x, uint64_t payload, uint64_t& ro, bool& claimed) {
+    const uint64_t EMPTY = kmer_ops<uint64_t>::empty();
+    const uint32_t cap32 = (uint32_t)cap;
+    uint32_t s = slot_of(x, cap32);
+    claimed = false;
+    for (uint32_t i = 0; i < cap32; ++i) {
+        slot_t<uint64_t>* e = &slots[off + s - off0];
+        uint64_t cur, v;
+        slot_load(e, cur, v);
+        if (cur == x) {
+            ro = v;
+            return off + s;
+        }
+        if (cur == EMPTY) {
+            const u128 old = key_cas(reinterpret_cast<u128*>(e), ((u128)v << 64) | (u128)EMPTY,
+                                     ((u128)payload << 64) | (u128)x);
+            if ((uint64_t)old == EMPTY && (uint64_t)(old >> 64) == v) {
+                claimed = true;
+                return off + s;
+            }
+            if ((uint64_t)old == x) {
+                ro = (uint64_t)(old >> 64);
                 return off + s;
             }
         }
@@ -380,8 +415,19 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     const uint64_t rec = window_record(win, R.occ, R0, nrec, O0 + t);
     const occ_info<K> oi = decode_occ_r<K>(R, rec, O0 + t, k);
     const uint32_t tb = R.bucket[oi.r] - T.b0;
+    const uint32_t mo = oi.contrib | (oi.owned ? M_PRIMARY : 0u);
+    const uint32_t own = (uint32_t)(oi.r - R0 + 1) << 4;
     uint64_t ro = 0;
-    const uint64_t s = table_upsert<K>(T.slots, T.off0, T.tab_off[tb], T.tab_cap[tb], oi.can, ro);
+    bool claimed = false;
+    uint64_t s;
+    if constexpr (sizeof(K) == 8) {
+        // a new k-mer's slot: rank t, and om as the updates below would leave it
+        const uint32_t om0 = oi.owned ? (own | mo) : mo;
+        s = table_claim(T.slots, T.off0, T.tab_off[tb], T.tab_cap[tb], oi.can,
+                        (uint64_t)(uint32_t)t | ((uint64_t)om0 << 32), ro, claimed);
+    } else {
+        s = table_upsert<K>(T.slots, T.off0, T.tab_off[tb], T.tab_cap[tb], oi.can, ro);
+    }
     if (s == ~0ull) {
         set_error(err, ERR_TABLE_FULL);
         occ_slot[t] = NONE32;
@@ -389,7 +435,7 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     }
     // slot of this occurrence, bit 31 = owned (read by k_multi_pairs)
     occ_slot[t] = (uint32_t)s | (oi.owned ? 0x80000000u : 0u);
-    const uint32_t mo = oi.contrib | (oi.owned ? M_PRIMARY : 0u);
+    if (claimed) return;
     // rank and om as read while probing (never newer than the slot): the
     // reduction and the updates below stay correct, and a k-mer whose slot
     // already holds everything this occurrence adds costs no further access
@@ -402,7 +448,6 @@ __global__ void __launch_bounds__(256) k_insert(rec_view R, tables<K> T, uint64_
     }
     // owner: the first owning record, M_MULTI once a second one appears.
     // `om` only gains bits, so the loop ends after a few changes by others.
-    const uint32_t own = (uint32_t)(oi.r - R0 + 1) << 4;
     for (int it = 0;; ++it) {
         const uint32_t cur = old & ~0xfu;
         const uint32_t want = (cur == own || (old & M_MULTI)) ? (old | mo)
