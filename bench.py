@@ -667,8 +667,8 @@ def path_algorithmic_bytes(r, w, record_bytes):
 # DRAM bytes per algorithmic byte of kernels whose launch sites declare their
 # algorithmic bytes (one capture; the ratio carries to other sizes).
 TRAFFIC_RATIO = {
-    # first phase-1 pass at 40 genomes: 20,646,311 pairs, 495.5 MB algorithmic, 472.2 MB DRAM
-    "k_rs_downsweep": (472166144 / 495511464, "profiles/phase12_top_kernels_pangenome40.md"),
+    # first phase-1 pass at 40 genomes: 20,646,311 pairs, 495.5 MB algorithmic, 463.8 MB DRAM
+    "k_rs_onesweep": (463810560 / 495511464, "profiles/phase12_top_kernels_pangenome40.md"),
 }
 
 TRAFFIC_PER_UNIT = {
