@@ -1,6 +1,6 @@
-"""CPU: the C++ adapter printed in INTEGRATION.md compiles against the
-reference's headers and this project's header, and links against
-libcdbg_gpu.so (no GPU needed to link)."""
+"""CPU: the C++ adapter the repository's integration guide prints (its first
+C++ block) compiles against the reference's headers and this project's
+header, and links against libcdbg_gpu.so (no GPU needed to link)."""
 import os
 import re
 import shutil
