@@ -1674,11 +1674,14 @@ __device__ __forceinline__ uint32_t node_lookup(tables<K> const& T, uint32_t tb,
 }
 
 // Nodes [*nb, *ne) (one bucket group's, numbered on the device).
+// Also records, per side, the node of the neighbour when it is the side's
+// only one (link[2n] left, link[2n + 1] right, NONE32 otherwise): k_links
+// then needs no probe.
 template <typename K>
 __global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* nb, unsigned long long const* ne,
                                                      tables<K> T, K const* __restrict__ n_key,
                                                      uint32_t const* __restrict__ n_bucket, uint32_t k,
-                                                     uint8_t* __restrict__ n_mask) {
+                                                     uint8_t* __restrict__ n_mask, uint32_t* __restrict__ link) {
     const uint64_t n = *nb + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= *ne) return;
     typedef kmer_ops<K> ops;
@@ -1689,7 +1692,7 @@ __global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* n
     const uint32_t cap = (uint32_t)T.tab_cap[tb];
     slot_t<K> const* t = T.slots + (T.tab_off[tb] - T.off0);
     const uint32_t top = 2 * (k - 1);
-    uint32_t out = 0;
+    uint32_t out = 0, right = NONE32, left = NONE32;
     // appending nt to x prepends 3 - nt to revcomp(x): (rc(x) >> 2) | (3 - nt) << 2(k-1)
 #pragma unroll
     for (uint32_t nt = 0; nt < 4; ++nt) {
@@ -1697,20 +1700,31 @@ __global__ void __launch_bounds__(256, 8) k_ext_mask(unsigned long long const* n
         const K f = ((can << 2) | (K)nt) & msk;
         const K fr = (rev >> 2) | hi;
         const K cf = f <= fr ? f : fr;
-        if (node_probe<K>(t, cap, slot_of(cf, cap), cf) != NONE32) out |= 1u << nt;
+        const uint32_t a = node_probe<K>(t, cap, slot_of(cf, cap), cf);
+        if (a != NONE32) {
+            out |= 1u << nt;
+            right = a;
+        }
         const K r = ((rev << 2) | (K)nt) & msk;
         const K rr = (can >> 2) | hi;
         const K cr = r <= rr ? r : rr;
-        if (node_probe<K>(t, cap, slot_of(cr, cap), cr) != NONE32) out |= 1u << (4 + nt);
+        const uint32_t b = node_probe<K>(t, cap, slot_of(cr, cap), cr);
+        if (b != NONE32) {
+            out |= 1u << (4 + nt);
+            left = b;
+        }
     }
     n_mask[n] = (uint8_t)out;
+    link[2 * n] = __popc(out >> 4) == 1 ? left : NONE32;
+    link[2 * n + 1] = __popc(out & 0xfu) == 1 ? right : NONE32;
 }
 
 __device__ __forceinline__ uint32_t fwd_nib(uint32_t m, bool rc) { return (rc ? (m >> 4) : m) & 0xfu; }
 __device__ __forceinline__ uint32_t back_nib(uint32_t m, bool rc) { return (rc ? m : (m >> 4)) & 0xfu; }
 
 // link[2n] = L port, link[2n+1] = R port: (node << 1) | rc of the state
-// reached, NONE32 when the step is not clean.
+// reached, NONE32 when the step is not clean.  On entry link holds the
+// sides' only neighbours as k_ext_mask found them.
 template <typename K>
 __global__ void __launch_bounds__(256, 8) k_links(unsigned long long const* nb, unsigned long long const* ne,
                                                   tables<K> T, K const* __restrict__ n_key,
@@ -1722,7 +1736,6 @@ __global__ void __launch_bounds__(256, 8) k_links(unsigned long long const* nb, 
     typedef kmer_ops<K> ops;
     const K can = n_key[n];
     const uint32_t m = n_mask[n];
-    const uint32_t tb = n_bucket[n] - T.b0;
     const K msk = ops::mask(k);
     const uint32_t top = 2 * (k - 1);
     const uint32_t nibr = fwd_nib(m, false), nibl = back_nib(m, false);
@@ -1736,7 +1749,7 @@ __global__ void __launch_bounds__(256, 8) k_links(unsigned long long const* nb, 
             const K nf = ((can << 2) | (K)nt) & msk;
             const K nr = (rev >> 2) | ((K)(3u - nt) << top);
             const bool nrc = !(nf <= nr);
-            const uint32_t nn = node_lookup<K>(T, tb, nrc ? nr : nf);
+            const uint32_t nn = link[2 * n + 1];
             if (nn != NONE32 && __popc(back_nib(n_mask[nn], nrc)) == 1) lr = (nn << 1) | (nrc ? 1u : 0u);
         }
     }
@@ -1749,7 +1762,7 @@ __global__ void __launch_bounds__(256, 8) k_links(unsigned long long const* nb, 
             const K nr = (can >> 2) | ((K)(3u - nt) << top);
             const bool srcc = !(nf <= nr);
             const bool nrc = !srcc;
-            const uint32_t nn = node_lookup<K>(T, tb, srcc ? nr : nf);
+            const uint32_t nn = link[2 * n];
             if (nn != NONE32 && __popc(fwd_nib(n_mask[nn], nrc)) == 1) ll = (nn << 1) | (nrc ? 1u : 0u);
         }
     }
@@ -2442,7 +2455,7 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         CDBG_CHECK_LAUNCH();
         {
             CDBG_PROF("k_ext_mask", st);
-            k_ext_mask<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, TG, n_key, n_bucket, k, n_mask);
+            k_ext_mask<K><<<grid(tn, 256), 256, 0, st>>>(nbase, nnext, TG, n_key, n_bucket, k, n_mask, link);
         }
         CDBG_CHECK_LAUNCH();
         {
