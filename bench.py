@@ -623,7 +623,7 @@ def _per_unit(w):
         "k_insert": None,
         "k_multi_pairs": ("occ", 4 + 4),          # occurrence slot read + pair written
         "k_ext_mask": ("distinct", w + 4 + 1),    # key + bucket read, mask written
-        "k_links": ("distinct", w + 4 + 1 + 8),   # key + bucket + mask read, two links written
+        "k_links": ("distinct", w + 1 + 8 + 8),   # key + mask + recorded neighbours read, two links written
         "k_chain_paths": ("distinct", 8 + 1 + 1 + 4),  # links + flags + mask read, fragment element written
         "k_frag_write": ("frag_bytes", 1),        # fragment records written
     }

@@ -649,9 +649,21 @@ __global__ void __launch_bounds__(OCC_BLOCK)
         if (t < nocc) {
             const uint32_t v = occ_slot[t];
             if (v != NONE32 && (v & 0x80000000u)) {
-                const uint32_t n = slot_rank ? __ldg(slot_rank + (uint64_t)(v & 0x7fffffffu) * rank_stride)
-                                             : (v & 0x7fffffffu);
-                if (n_rec[n] == MULTI_TAG) {
+                uint32_t n;
+                bool multi;
+                if (slot_rank) {
+                    // the slot's node index and owner bits in one load: a
+                    // multi-record k-mer has both M_PRIMARY and M_MULTI (the
+                    // MULTI_TAG k_make_nodes writes to n_rec)
+                    const uint2 ro = __ldg(reinterpret_cast<uint2 const*>(
+                        slot_rank + (uint64_t)(v & 0x7fffffffu) * rank_stride));
+                    n = ro.x;
+                    multi = (ro.y & (M_PRIMARY | M_MULTI)) == (M_PRIMARY | M_MULTI);
+                } else {
+                    n = v & 0x7fffffffu;
+                    multi = n_rec[n] == MULTI_TAG;
+                }
+                if (multi) {
                     // the record lies between this occurrence block's first record
                     // and the next one's (a few dozen records): search only there
                     const uint64_t rlo = blk_rec[b];
