@@ -83,6 +83,66 @@ __global__ void k_seq_starts(uint64_t const* __restrict__ seq_off, uint32_t num_
 //   ends   = P & (~V | S)
 //   starts = V & (S | ~P)
 // (a full 32-byte chunk is read with two 16-byte loads when aligned).
+// Run boundaries at positions [p0, p0 + 32) as bit masks: E (a run ends at
+// p) and St (a run starts at p).
+__device__ __forceinline__ void ev_masks(uint8_t const* __restrict__ ascii, uint64_t nbytes,
+                                         uint32_t const* __restrict__ starts, uint64_t p0, uint32_t& E,
+                                         uint32_t& St) {
+    E = St = 0;
+    if (p0 > nbytes) return;
+    uint32_t V = 0;
+    if (p0 + 32 <= nbytes && ((reinterpret_cast<uintptr_t>(ascii) & 15) == 0)) {
+        const uint4 a = reinterpret_cast<uint4 const*>(ascii + p0)[0];
+        const uint4 b = reinterpret_cast<uint4 const*>(ascii + p0)[1];
+        const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 32; ++i) V |= byte_valid((w[i >> 2] >> (8 * (i & 3))) & 0xffu) << i;
+    } else {
+        const uint32_t n = (uint32_t)((nbytes - p0) < 32 ? (nbytes - p0) : 32);
+        for (uint32_t i = 0; i < n; ++i) V |= byte_valid(ascii[p0 + i]) << i;
+    }
+    // sequence starts in [p0, p0 + 32), and nbytes itself (bit i of word
+    // p0 / 32 of the boundary bitmap; p0 is a multiple of 32)
+    const uint32_t S = starts[p0 >> 5];
+    // validity of the byte before p0, whatever sequence it belongs to: a
+    // run of the previous sequence that ends exactly at p0 is closed here
+    const uint32_t pin = (p0 > 0) ? byte_valid(ascii[p0 - 1]) : 0u;
+    const uint32_t P = (V << 1) | pin;
+    E = P & (~V | S);
+    St = V & (S | ~P);
+    if (nbytes - p0 < 31) {  // positions past nbytes are not positions
+        const uint32_t keep = (2u << (uint32_t)(nbytes - p0)) - 1u;
+        E &= keep;
+        St &= keep;
+    }
+}
+
+__device__ __forceinline__ void ev_write(uint32_t E, uint32_t St, uint64_t p0, uint64_t o, uint64_t cap,
+                                         uint64_t* __restrict__ events) {
+    uint32_t m = E | St;
+    while (m) {
+        const uint32_t i = __ffs(m) - 1;
+        m &= m - 1;
+        const uint64_t p = p0 + i;
+        if ((E >> i) & 1u) {  // run end
+            if (o < cap) events[o] = p << 1;
+            ++o;
+        }
+        if ((St >> i) & 1u) {  // run start
+            if (o < cap) events[o] = (p << 1) | 1u;
+            ++o;
+        }
+    }
+}
+
+// Run boundary events over positions [0, nbytes]: (pos << 1) | 1 for a run
+// start, (pos << 1) for a run end.  Sequence starts (and nbytes) split runs.
+// Each thread owns 32 positions as bit masks: V = valid bases, S = sequence
+// starts, P = validity of the byte before each position; then
+//   ends   = P & (~V | S)
+//   starts = V & (S | ~P)
+// (a full 32-byte chunk is read with two 16-byte loads when aligned).
+// Two passes: the counts per tile, then (after their scan) the events.
 template <bool WRITE>
 __global__ void __launch_bounds__(EV_THREADS)
     k_run_events(uint8_t const* __restrict__ ascii, uint64_t nbytes, uint32_t const* __restrict__ starts,
@@ -91,34 +151,8 @@ __global__ void __launch_bounds__(EV_THREADS)
     static_assert(EV_PER_THREAD == 32, "one 32-bit mask per thread");
     __shared__ uint32_t sw[EV_THREADS / 32 + 1];
     const uint64_t p0 = (uint64_t)blockIdx.x * EV_TILE + (uint64_t)threadIdx.x * EV_PER_THREAD;
-    uint32_t E = 0, St = 0;
-    if (p0 <= nbytes) {
-        uint32_t V = 0;
-        if (p0 + 32 <= nbytes && ((reinterpret_cast<uintptr_t>(ascii) & 15) == 0)) {
-            const uint4 a = reinterpret_cast<uint4 const*>(ascii + p0)[0];
-            const uint4 b = reinterpret_cast<uint4 const*>(ascii + p0)[1];
-            const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-            for (int i = 0; i < 32; ++i) V |= byte_valid((w[i >> 2] >> (8 * (i & 3))) & 0xffu) << i;
-        } else {
-            const uint32_t n = (uint32_t)((nbytes - p0) < 32 ? (nbytes - p0) : 32);
-            for (uint32_t i = 0; i < n; ++i) V |= byte_valid(ascii[p0 + i]) << i;
-        }
-        // sequence starts in [p0, p0 + 32), and nbytes itself (bit i of word
-        // p0 / 32 of the boundary bitmap; p0 is a multiple of 32)
-        const uint32_t S = starts[p0 >> 5];
-        // validity of the byte before p0, whatever sequence it belongs to: a
-        // run of the previous sequence that ends exactly at p0 is closed here
-        const uint32_t pin = (p0 > 0) ? byte_valid(ascii[p0 - 1]) : 0u;
-        const uint32_t P = (V << 1) | pin;
-        E = P & (~V | S);
-        St = V & (S | ~P);
-        if (nbytes - p0 < 31) {  // positions past nbytes are not positions
-            const uint32_t keep = (2u << (uint32_t)(nbytes - p0)) - 1u;
-            E &= keep;
-            St &= keep;
-        }
-    }
+    uint32_t E, St;
+    ev_masks(ascii, nbytes, starts, p0, E, St);
     const uint32_t cnt = __popc(E) + __popc(St);
     uint32_t tot;
     const uint32_t ex = prim::block_exclusive_scan<uint32_t, EV_THREADS>(cnt, sw, tot);
@@ -126,15 +160,39 @@ __global__ void __launch_bounds__(EV_THREADS)
         if (threadIdx.x == 0) tile_count[blockIdx.x] = tot;
         return;
     }
-    uint64_t o = tile_off[blockIdx.x] + ex;
-    uint32_t m = E | St;
-    while (m) {
-        const uint32_t i = __ffs(m) - 1;
-        m &= m - 1;
-        const uint64_t p = p0 + i;
-        if ((E >> i) & 1u) events[o++] = p << 1;           // run end
-        if ((St >> i) & 1u) events[o++] = (p << 1) | 1u;   // run start
+    ev_write(E, St, p0, tile_off[blockIdx.x] + ex, ~0ull, events);
+}
+
+// The same in one pass: tiles take indices in launch order and find their
+// output offset by decoupled look-back; events past `cap` are counted, not
+// written, and the last tile stores the total in *total (the caller runs the
+// two passes when it exceeds cap).
+__global__ void __launch_bounds__(EV_THREADS)
+    k_run_events_1p(uint8_t const* __restrict__ ascii, uint64_t nbytes, uint32_t const* __restrict__ starts,
+                    uint64_t ntiles, uint32_t* tile_counter, unsigned long long* status,
+                    uint64_t* __restrict__ events, uint64_t cap, unsigned long long* total, uint32_t* err) {
+    __shared__ uint32_t sw[EV_THREADS / 32 + 1];
+    __shared__ uint64_t s_tile, s_excl;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    const uint64_t p0 = tile * EV_TILE + (uint64_t)threadIdx.x * EV_PER_THREAD;
+    uint32_t E, St;
+    ev_masks(ascii, nbytes, starts, p0, E, St);
+    const uint32_t cnt = __popc(E) + __popc(St);
+    uint32_t tot;
+    const uint32_t ex = prim::block_exclusive_scan<uint32_t, EV_THREADS>(cnt, sw, tot);
+    if (threadIdx.x < 32) {
+        uint64_t excl = 0;
+        const bool ok = prim::lookback_exclusive(status, tile, tot, excl);
+        if (threadIdx.x == 0) {
+            if (!ok) set_error(err, ERR_CHAIN_LIMIT);
+            s_excl = excl;
+            if (tile == ntiles - 1) *total = excl + tot;
+        }
     }
+    __syncthreads();
+    ev_write(E, St, p0, s_excl + ex, cap, events);
 }
 
 // Pair events into runs; keep[i] = len >= k.
@@ -252,11 +310,22 @@ __device__ __forceinline__ uint64_t mz_window(uint64_t const* sw, uint32_t x) {
     return s ? (lo >> s) | (hi << (64 - s)) : lo;
 }
 
-// Rolling-hash tables of one tile, filled by threads 0..31: stab[j][b] =
+// Rolling-hash tables of one tile, filled by threads 0..63: stab[j][b] =
 // [0] seed(b), [1] rol(seed(b), m), [2] ror(seed(b^3), 1), [3] rol(seed(b^3),
-// m-1), and tf/tr[(out << 2) | in] = one rolling step of base `out` leaving and
-// base `in` entering, forward and reverse-complement strand.
-__device__ __forceinline__ void mz_tables(uint64_t (*stab)[4], uint64_t* tf, uint64_t* tr, uint32_t m) {
+// m-1); tf/tr[(out << 2) | in] = one rolling step of base `out` leaving and
+// base `in` entering, forward and reverse-complement strand; and, for the
+// first m-mer of a chunk two bases at a time, p2f[x] = rol(seed(a), 1) ^
+// seed(b) and p2r[x] = rol(seed(b ^ 3), 1) ^ seed(a ^ 3) for the base pair x =
+// a | b << 2 (a first in the sequence).
+__device__ __forceinline__ void mz_tables(uint64_t (*stab)[4], uint64_t* tf, uint64_t* tr, uint64_t* p2f,
+                                          uint64_t* p2r, uint32_t m) {
+    if (threadIdx.x >= 32 && threadIdx.x < 64) {
+        const uint32_t x = threadIdx.x & 15, a = x & 3, b = x >> 2;
+        if (threadIdx.x < 48)
+            p2f[x] = rol64(nt_seed(a), 1) ^ nt_seed(b);
+        else
+            p2r[x] = rol64(nt_seed(b ^ 3u), 1) ^ nt_seed(a ^ 3u);
+    }
     if (threadIdx.x < 16) {
         const uint32_t b = threadIdx.x & 3, j = threadIdx.x >> 2;
         const uint64_t sb = nt_seed(b), sc = nt_seed(b ^ 3u);
@@ -276,17 +345,22 @@ __device__ __forceinline__ void mz_tables(uint64_t (*stab)[4], uint64_t* tf, uin
 // windows, so every extraction in the unrolled loop is a constant shift.
 template <int HC>
 __device__ __forceinline__ void mz_hash(uint64_t const* sw, uint64_t* sh, uint64_t const (*stab)[4],
-                                        uint64_t const* tf, uint64_t const* tr, uint32_t rel0, uint32_t nh,
-                                        uint32_t m) {
+                                        uint64_t const* tf, uint64_t const* tr, uint64_t const* p2f,
+                                        uint64_t const* p2r, uint32_t rel0, uint32_t nh, uint32_t m) {
     const uint32_t q0 = threadIdx.x * HC;
     if (q0 >= nh) return;
     const uint32_t cnt = min((uint32_t)HC, nh - q0);
     const uint32_t x0 = rel0 + q0;
     const uint64_t wout = mz_window(sw, x0);         // bases q0 .. q0 + 31
     const uint64_t win = mz_window(sw, x0 + m - 1);  // bases q0 + m - 1 .. + 31
+    // the first m-mer in Horner form, two bases per step
     uint64_t f = 0, rc = 0;
-    for (uint32_t i = 0; i < m; ++i) f = rol64(f, 1) ^ stab[0][(uint32_t)(wout >> (2 * i)) & 3u];
-    for (uint32_t i = m; i-- > 0;) rc = rol64(rc, 1) ^ stab[0][((uint32_t)(wout >> (2 * i)) & 3u) ^ 3u];
+    uint32_t i = 0;
+    for (; i + 1 < m; i += 2) f = rol64(f, 2) ^ p2f[(uint32_t)(wout >> (2 * i)) & 15u];
+    if (i < m) f = rol64(f, 1) ^ stab[0][(uint32_t)(wout >> (2 * i)) & 3u];
+    uint32_t j = m;
+    for (; j >= 2; j -= 2) rc = rol64(rc, 2) ^ p2r[(uint32_t)(wout >> (2 * (j - 2))) & 15u];
+    if (j == 1) rc = rol64(rc, 1) ^ stab[0][((uint32_t)wout & 3u) ^ 3u];
     sh[mz_pad(q0)] = f <= rc ? f : rc;
 #pragma unroll
     for (int j = 1; j < HC; ++j) {
@@ -325,11 +399,11 @@ __global__ void __launch_bounds__(MZ_THREADS)
     uint64_t* sh = mz_dyn + LY::WMAX;        // hashes, then prefix minima (padded index)
     uint64_t* smin = sh + LY::HPAD;          // suffix minima, then window minima
     __shared__ uint64_t stab[4][4];  // rotated ntHash seeds, by base
-    __shared__ uint64_t tf[16], tr[16];  // rolling terms by (out base, in base)
+    __shared__ uint64_t tf[16], tr[16], p2f[16], p2r[16];  // rolling terms by (out base, in base)
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint64_t s_tile, s_excl;
 
-    mz_tables(stab, tf, tr, m);
+    mz_tables(stab, tf, tr, p2f, p2r, m);
     uint64_t tile = blockIdx.x;
     if (MODE == 2) {
         if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -363,7 +437,7 @@ __global__ void __launch_bounds__(MZ_THREADS)
     }
     const uint32_t rel0 = (uint32_t)(pa - wa * 32);  // stream offset of base e0 in sw
     // canonical m-mer hashes h[0..nh) (h[q] = m-mer at base e0 + q)
-    mz_hash<HC>(sw, sh, stab, tf, tr, rel0, nh, m);
+    mz_hash<HC>(sw, sh, stab, tf, tr, p2f, p2r, rel0, nh, m);
     __syncthreads();
     // sliding minimum smin[q] = min h[q .. q + W - 1] by segments of W hashes
     // (van Herk / Gil-Werman): with suf[q] the minimum from q to the end of its
@@ -507,12 +581,12 @@ __global__ void __launch_bounds__(MZ_THREADS)
     uint64_t* sw = mz_dyn;
     uint64_t* sh = mz_dyn + LY::WMAX;
     __shared__ uint64_t stab[4][4];
-    __shared__ uint64_t tf[16], tr[16];
+    __shared__ uint64_t tf[16], tr[16], p2f[16], p2r[16];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint64_t s_tile, s_excl;
     __shared__ uint32_t s_run;
     __shared__ uint32_t sws[MZ_THREADS / 32 + 1];
-    mz_tables(stab, tf, tr, m);
+    mz_tables(stab, tf, tr, p2f, p2r, m);
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const uint64_t tile = s_tile;
@@ -538,7 +612,7 @@ __global__ void __launch_bounds__(MZ_THREADS)
         if (threadIdx.x == 0) atomicExch(&status[tile], (2ull << 62));  // unblock successors
         return;
     }
-    mz_hash<HC>(sw, sh, stab, tf, tr, (uint32_t)(pa - wa * 32), nh, m);
+    mz_hash<HC>(sw, sh, stab, tf, tr, p2f, p2r, (uint32_t)(pa - wa * 32), nh, m);
     __syncthreads();
     const uint32_t ncut = (uint32_t)(j1 - j0);
     const uint32_t c0 = threadIdx.x * MZR_C;       // first (k-1)-mer of this thread, from j0
@@ -986,22 +1060,51 @@ void build_runs(seq_input const& in, uint32_t k, dev_arena& A, cudaStream_t st, 
     CDBG_CUDA(cudaMemsetAsync(starts, 0, 4 * nsw, st));
     k_seq_starts<<<grid((uint64_t)in.num_seqs + 1, 256), 256, 0, st>>>(in.seq_off, in.num_seqs, starts);
     CDBG_CHECK_LAUNCH();
+    // one pass into room for a run every 64 bases (two events each); input
+    // with more runs than that takes the two passes
+    uint64_t ev_cap = in.nbytes / 32 + 1024;
+    uint64_t* ev = A.alloc<uint64_t>(ev_cap);
+    uint64_t nev = 0;
     {
-        CDBG_PROF("k_run_events", st);
-        k_run_events<false><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, starts, tcount, nullptr,
-                                                                     nullptr);
+        uint32_t* counter = A.alloc<uint32_t>(1);
+        unsigned long long* status = A.alloc<unsigned long long>(tiles);
+        unsigned long long* total = A.alloc<unsigned long long>(1);
+        uint32_t* lerr = A.alloc<uint32_t>(1);
+        CDBG_CUDA(cudaMemsetAsync(counter, 0, 4, st));
+        CDBG_CUDA(cudaMemsetAsync(status, 0, 8 * tiles, st));
+        CDBG_CUDA(cudaMemsetAsync(lerr, 0, 4, st));
+        {
+            CDBG_PROF("k_run_events", st);
+            k_run_events_1p<<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, starts, tiles, counter,
+                                                                   status, ev, ev_cap, total, lerr);
+        }
+        CDBG_CHECK_LAUNCH();
+        uint64_t got[2] = {0, 0};
+        read_small(&got[0], total, 8, st);
+        uint32_t le = 0;
+        read_small(&le, lerr, 4, st);
+        if (le) throw std::runtime_error("run events: look-back wait limit reached");
+        nev = got[0];
     }
-    CDBG_CHECK_LAUNCH();
-    prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, tiles, A, st, toff + tiles);
-    const uint64_t nev = read_dev(toff + tiles, st);
+    if (nev > ev_cap) {
+        {
+            CDBG_PROF("k_run_events", st);
+            k_run_events<false><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, starts, tcount,
+                                                                         nullptr, nullptr);
+        }
+        CDBG_CHECK_LAUNCH();
+        prim::exclusive_scan<uint32_t, uint64_t>(tcount, toff, tiles, A, st, toff + tiles);
+        nev = read_dev(toff + tiles, st);
+        ev = A.alloc<uint64_t>(nev);
+        {
+            CDBG_PROF("k_run_events", st);
+            k_run_events<true><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, starts, tcount, toff,
+                                                                        ev);
+        }
+        CDBG_CHECK_LAUNCH();
+    }
     const uint64_t nraw = nev / 2;
     if (nraw == 0) return;
-    uint64_t* ev = A.alloc<uint64_t>(nev);
-    {
-        CDBG_PROF("k_run_events", st);
-        k_run_events<true><<<(unsigned)tiles, EV_THREADS, 0, st>>>(in.ascii, in.nbytes, starts, tcount, toff, ev);
-    }
-    CDBG_CHECK_LAUNCH();
     uint64_t* src = A.alloc<uint64_t>(nraw);
     uint32_t* len = A.alloc<uint32_t>(nraw);
     uint32_t* color = A.alloc<uint32_t>(nraw);
