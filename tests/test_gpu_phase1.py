@@ -110,3 +110,29 @@ def test_sequence_boundaries_on_chunk_edges(engine, oracle, tmp_path):
         hs = native.HostSequences(files)
         engine.dump_supers(hs.batch, k, 0, 64, str(tmp_path / "g.bin"))
         assert filecmp.cmp(str(tmp_path / "o.bin"), str(tmp_path / "g.bin"), shallow=False), k
+
+
+def test_short_runs_take_the_two_pass_run_events(engine, oracle, tmp_path):
+    """Sequences broken by an N every 20-40 bases: more runs than one per 64
+    bases, so the one-pass run-boundary kernel's room overflows and the two
+    counting passes run instead; the super-k-mers still equal the oracle's."""
+    import numpy as np
+    rng = np.random.default_rng(17)
+    os.makedirs(tmp_path / "in")
+    names = []
+    for g in range(4):
+        s = rng.choice(np.frombuffer(b"ACGT", dtype=np.uint8), size=200_000)
+        gaps = np.cumsum(rng.integers(20, 41, size=10_000))
+        s[gaps[gaps < s.size]] = ord("N")
+        path = str(tmp_path / "in" / ("g%d.fa" % g))
+        with open(path, "wb") as f:
+            f.write(b">g\n" + s.tobytes() + b"\n")
+        names.append(path)
+    lst = str(tmp_path / "in" / "filenames.txt")
+    with open(lst, "w") as f:
+        f.write("".join(n + "\n" for n in names))
+    k, B = 21, 64
+    oracle.phase1(lst, k, B, dump=str(tmp_path / "o.bin"))
+    hs = native.HostSequences(names)
+    engine.dump_supers(hs.batch, k, 0, B, str(tmp_path / "g.bin"))
+    assert filecmp.cmp(str(tmp_path / "o.bin"), str(tmp_path / "g.bin"), shallow=False)
