@@ -1227,6 +1227,25 @@ __device__ __forceinline__ void encode_one(cand_set const& cs, uint64_t j, uint6
             return;
         }
     }
+    if (ENC && cs.list && N < sparse_t) {
+        // a sparse set held as an ascending list: its gap codes straight
+        // from the list, 32 at a time at offsets from a warp scan of their
+        // lengths (the codes the bitmap walk below would write)
+        if (lane == 0) put_delta(words, pos0, N);
+        uint64_t p = pos0 + hdr;
+        for (uint64_t base = 0; base < N; base += 32) {
+            const uint64_t i = base + lane;
+            const uint32_t v = i < N ? cs.list[i] : 0u;
+            uint32_t pv = __shfl_up_sync(0xffffffffu, v, 1);
+            if (lane == 0 && base) pv = cs.list[base - 1];
+            const uint64_t gap = i == 0 ? (uint64_t)v : (uint64_t)(v - pv - 1);
+            uint64_t total;
+            const uint64_t ex = warp_excl_scan64(i < N ? delta_bits(gap) : 0u, total);
+            if (i < N) put_delta(words, p + ex, gap);
+            p += total;
+        }
+        return;
+    }
     if (cs.bm) {
         for (uint32_t w = lane; w < nw; w += 32) bm[w] = cs.bm[w];
     } else {
