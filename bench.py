@@ -16,6 +16,11 @@ frag spill and the color classes.
             of each call.
   e2e_host  pinned host sequences in, host outputs out (cdbg_gpu_build).
 
+`--workload stitch-seed` times round 0 of the stitch instead
+(cdbg_gpu_stitch_seed over the pangenome build's frag_unitigs.bin, round-0
+files and closed unitigs written), in fragments/s, with the reference's own
+seed (oracle/_ref/ref_seed) on the same file as its CPU baseline.
+
 Max over ranks.  `--impl reference` times the reference's own phase 1 +
 phase 2 (oracle/_ref/ref_phase12: the builder's ingest_bucketed, close and
 process_buckets, built from the reference's sources) with all host cores on
@@ -78,6 +83,7 @@ def parse():
                     help="serving: requests of the stream the plain one-at-a-time path serves")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
     ap.add_argument("--serving-buckets", type=int, default=1024)
+    ap.add_argument("--seed-buckets", type=int, default=1024, help="stitch-seed: round-store buckets")
     return ap.parse_args()
 
 
@@ -823,10 +829,130 @@ def main_serving(a):
     return 0
 
 
+def main_seed(a):
+    """Round 0 of the stitch (cdbg_gpu_stitch_seed) over the frag_unitigs.bin of
+    the pangenome build: fragments/s, and the reference's own seed
+    (oracle/_ref/ref_seed, all host cores) on the same file beside it.  Rank 0
+    only (a per-GPU figure; the build's bench line carries the replicas)."""
+    import numpy as np
+    import torch
+    from cdbg_gpu import native, synth
+    rank, local, world = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    p, n_genomes, k, blog2 = synth.preset("pangenome", seed=1, scale=a.genome_scale)
+    if a.genomes:
+        n_genomes = a.genomes
+    B = a.seed_buckets
+    seq, lens, per = synth.collection(p, n_genomes)
+    off = np.zeros(len(lens) + 1, dtype=np.uint64)
+    off[1:] = np.cumsum(lens)
+    colors = np.repeat(np.arange(n_genomes, dtype=np.uint32), per)
+    eng = native.Engine(local)
+    h_seq = torch.from_numpy(seq).pin_memory()
+    h_off = torch.from_numpy(off.view(np.int64)).pin_memory()
+    h_col = torch.from_numpy(colors.view(np.int32)).pin_memory()
+    batch = native.SeqBatch(h_seq.data_ptr(), seq.nbytes, h_off.data_ptr(), h_col.data_ptr(), len(colors), 0)
+    r = eng.build(batch, k, 1 << blog2, n_genomes)
+    n_frag_bytes = r.frag_nbytes
+    frags = torch.empty(n_frag_bytes + 16, dtype=torch.uint8).pin_memory()
+    ctypes_memmove(frags.data_ptr(), r.frag_bytes, n_frag_bytes)
+    del h_seq, h_off, h_col, seq
+    eng.trim()
+    base = scratch_base(4 * n_frag_bytes + (8 << 30)) or tempfile.gettempdir()
+    work = tempfile.mkdtemp(prefix="cdbg_seed_", dir=base)
+    try:
+        rd, closed = os.path.join(work, "gpu"), os.path.join(work, "gpu_closed.bin")
+
+        def step():
+            return eng.stitch_seed((frags.data_ptr(), n_frag_bytes), k, rd, num_buckets=B, closed_path=closed)
+
+        for _ in range(max(a.warmup, 3)):
+            st = step()
+        clk = ClockSampler(local)
+        clk.start()
+        l0 = native.launch_count()
+        runs = [step() for _ in range(a.steps)]
+        launches = (native.launch_count() - l0) // max(1, a.steps)
+        clocks = clk.stop()
+        eng.profile(True)
+        step()
+        kstats = eng.kernel_stats()
+        eng.profile(False)
+        nf = runs[0]["fragments"]
+        ms_dev = statistics.mean(x["ms_device"] for x in runs)
+        ms_tot = statistics.mean(x["ms_total"] for x in runs)
+        st = runs[-1]
+        hbm, src = peaks()
+        seed_k = {kk: v for kk, v in kstats.items() if kk.startswith("k_seed")}
+        top = max(seed_k, key=lambda kk: seed_k[kk][0])
+        # algorithmic bytes of one launch of the top kernel
+        # (k_seed_info: every record byte read, its offset, 32 bytes of sizes,
+        # bucket and state written; k_seed_write: every record byte read, the
+        # tigs and closed unitigs written, 48 bytes of per-fragment offsets,
+        # sizes and state read)
+        if top == "k_seed_info":
+            alg = n_frag_bytes + 8 * (nf + 1) + 32 * nf
+        elif top == "k_seed_write":
+            alg = n_frag_bytes + st["round0_bytes"] + st["closed_nbytes"] + 48 * nf
+        else:
+            alg = None
+        top_ms = seed_k[top][0] / max(1, seed_k[top][1])
+        achieved = alg / (top_ms * 1e6) if alg else None
+        # the reference's seed on the same file, all host cores
+        ref = None
+        exe = os.path.join(ROOT, "oracle", "_ref", "ref_seed")
+        if not a.no_cpu_baseline and os.path.exists(exe):
+            fp = os.path.join(work, "frag_unitigs.bin")
+            frags[:n_frag_bytes].numpy().tofile(fp)
+            threads = os.cpu_count() or 1
+            out = subprocess.run([exe, fp, str(k), str(B), str(threads), os.path.join(work, "ref")],
+                                 capture_output=True, text=True, check=True).stdout
+            sec = float(re.search(r"seconds=([0-9.]+)", out).group(1))
+            ref = {"value": nf / sec, "unit": "fragments/s", "cores": threads, "kind": "reference",
+                   "sample": "the whole frag file (%d fragments, %.2f GB), one run, %d round-store buckets"
+                             % (nf, n_frag_bytes / 1e9, B), "seconds": sec}
+        line = {"metric": "stitch round-0 seed fragments/s", "value": nf / (ms_dev / 1e3), "unit": "fragments/s",
+                "n_gpus": 1, "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_dev,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                "config": {"workload": "stitch seed: the frag_unitigs.bin of the pangenome build (%d genomes x "
+                                       "~4.8 Mbp, k=%d), %d round-store buckets" % (n_genomes, k, B),
+                           "fragments": nf, "frag_bytes": n_frag_bytes, "routed": st["routed"],
+                           "closed_fragments": st["closed_fragments"], "closed_unitigs": st["closed_unitigs"],
+                           "round0_bytes": st["round0_bytes"], "round0_file_bytes": st["round0_file_bytes"],
+                           "l2": "inputs larger than L2 (%.1f GB of fragments)" % (n_frag_bytes / 1e9)},
+                "e2e": {"value": nf / (ms_tot / 1e3), "unit": "fragments/s", "ms_per_call": ms_tot,
+                        "ms_scan": statistics.mean(x["ms_scan"] for x in runs),
+                        "ms_device": ms_dev, "ms_files": statistics.mean(x["ms_files"] for x in runs),
+                        "h2d_bytes_per_step": n_frag_bytes, "d2h_bytes_per_step": st["round0_bytes"]
+                        + st["closed_nbytes"], "what": "host frag bytes in, round-0 files and closed-unitig file "
+                        "written (%s)" % ("tmpfs" if base == "/dev/shm" else "disk")},
+                "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm if achieved else None, "traffic": None,
+                             "peak_source": src, "ms_per_launch": top_ms},
+                "kernels_ms": {kk: v[0] for kk, v in seed_k.items()},
+                "cpu_baseline": ref, "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line))
+        if a.out:
+            with open(a.out, "w") as f:
+                f.write(json.dumps(line) + "\n")
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    return 0
+
+
+def ctypes_memmove(dst, src, n):
+    import ctypes
+    ctypes.memmove(dst, src, n)
+
+
 if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
         sys.exit(reference_arm(args))
     if args.workload == "serving":
         sys.exit(main_serving(args))
+    if args.workload == "stitch-seed":
+        sys.exit(main_seed(args))
     sys.exit(main_gpu(args))

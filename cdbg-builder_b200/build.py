@@ -24,7 +24,7 @@ OBJ = os.path.join(PKG, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CUDA_INC = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(NVCC))), "include")
-CU_SOURCES = ["phase1.cu", "phase2.cu", "inflate.cu", "capi.cu"]
+CU_SOURCES = ["phase1.cu", "phase2.cu", "inflate.cu", "seed.cu", "capi.cu"]
 HOST_SOURCES = ["io.cpp", "server.cpp", "shards.cpp"]
 # the reference checkout sits beside this repository unless the variable says otherwise
 REFERENCE = os.environ.get("CDBG_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))

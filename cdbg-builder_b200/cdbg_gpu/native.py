@@ -95,6 +95,22 @@ class BuildResult(ctypes.Structure):
                 ("ms_total", ctypes.c_double), ("ms_outputs", ctypes.c_double)]
 
 
+class SeedArgs(ctypes.Structure):
+    _fields_ = [("frags", ctypes.c_void_p), ("frag_nbytes", ctypes.c_uint64), ("k", ctypes.c_uint32),
+                ("num_buckets", ctypes.c_uint32), ("kmer_bits", ctypes.c_uint32),
+                ("host_threads", ctypes.c_uint32), ("chunk_bytes", ctypes.c_uint64),
+                ("round_dir", ctypes.c_char_p), ("closed_path", ctypes.c_char_p)]
+
+
+class SeedStats(ctypes.Structure):
+    _fields_ = [("fragments", ctypes.c_uint64), ("routed", ctypes.c_uint64),
+                ("closed_fragments", ctypes.c_uint64), ("closed_unitigs", ctypes.c_uint64),
+                ("routed_frag_bytes", ctypes.c_uint64), ("round0_bytes", ctypes.c_uint64), ("round0_file_bytes", ctypes.c_uint64),
+                ("closed", ctypes.c_void_p), ("closed_nbytes", ctypes.c_uint64), ("n_passes", ctypes.c_uint64),
+                ("ms_scan", ctypes.c_double), ("ms_device", ctypes.c_double), ("ms_files", ctypes.c_double),
+                ("ms_total", ctypes.c_double)]
+
+
 class Merged(ctypes.Structure):
     _fields_ = [("frag_bytes", ctypes.c_void_p), ("frag_nbytes", ctypes.c_uint64),
                 ("class_words", ctypes.c_void_p), ("class_bits", ctypes.c_uint64),
@@ -173,6 +189,10 @@ SIGNATURES = {
                                       ctypes.POINTER(BuildParams), ctypes.POINTER(BuildResult)]),
     "cdbg_gpu_build_files": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BuildFilesArgs),
                                             ctypes.POINTER(BuildResult)]),
+    "cdbg_gpu_stitch_seed": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SeedArgs),
+                                            ctypes.POINTER(SeedStats)]),
+    "cdbg_frag_record_offsets": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, c_u64p,
+                                                ctypes.c_uint64, c_u64p]),
     "cdbg_engine_set_memory_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "cdbg_engine_memory": (ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p]),
     "cdbg_engine_trim": (ctypes.c_int, [ctypes.c_void_p]),
@@ -453,12 +473,45 @@ class Engine:
         _check(lib().cdbg_gpu_build_files(self._h, ctypes.byref(a), ctypes.byref(r)))
         return r
 
+    def stitch_seed(self, frags, k, round_dir, num_buckets=1024, closed_path=None, kmer_bits=0, host_threads=0,
+                    chunk_bytes=0):
+        """cdbg_gpu_stitch_seed: round 0 of the stitch from frag_unitigs.bin
+        bytes (bytes, a buffer, or (address, nbytes) of host memory).  Returns
+        the stats as a dict; with no closed_path, 'closed' holds the closed
+        unitigs' frag records."""
+        if isinstance(frags, tuple):
+            addr, n = frags
+            keep = None
+        else:
+            keep = (ctypes.c_char * len(frags)).from_buffer_copy(frags) if len(frags) else None
+            addr, n = (ctypes.addressof(keep) if keep is not None else None), len(frags)
+        a = SeedArgs(addr, n, k, num_buckets, kmer_bits, host_threads, chunk_bytes, round_dir.encode(),
+                     closed_path.encode() if closed_path else None)
+        st = SeedStats()
+        _check(lib().cdbg_gpu_stitch_seed(self._h, ctypes.byref(a), ctypes.byref(st)))
+        out = {name: getattr(st, name) for name, _ in SeedStats._fields_ if name != "closed"}
+        if not closed_path:
+            out["closed"] = ctypes.string_at(st.closed, st.closed_nbytes) if st.closed_nbytes else b""
+        return out
+
     def build(self, batch, k, num_buckets, num_colors, m=0, batch_occ=0, outputs_to_host=True, buckets=None):
         lo, hi = buckets if buckets else (0, 0)
         p = BuildParams(k, m, num_buckets, num_colors, batch_occ, 1 if outputs_to_host else 0, lo, hi)
         r = BuildResult()
         _check(lib().cdbg_gpu_build(self._h, ctypes.byref(batch), ctypes.byref(p), ctypes.byref(r)))
         return r
+
+
+def frag_record_offsets(frags, host_threads=0):
+    """Record offsets of frag_unitigs.bin bytes (numpy uint64, records + 1)."""
+    import numpy as np
+    buf = (ctypes.c_char * len(frags)).from_buffer_copy(frags) if len(frags) else None
+    n = ctypes.c_uint64()
+    _check(lib().cdbg_frag_record_offsets(buf, len(frags), host_threads, None, 0, ctypes.byref(n)))
+    out = np.zeros(n.value + 1, dtype=np.uint64)
+    _check(lib().cdbg_frag_record_offsets(buf, len(frags), host_threads,
+                                          out.ctypes.data_as(c_u64p), len(out), ctypes.byref(n)))
+    return out
 
 
 def launch_count():

@@ -26,6 +26,7 @@
 #include "phase1.cuh"
 #include "phase2.cuh"
 #include "primitives.cuh"
+#include "seed.cuh"
 
 namespace {
 
@@ -1625,6 +1626,172 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
         return 0;
     } catch (std::exception const& ex) {
         if (e) e->A.reset();
+        return fail(ex);
+    }
+}
+
+int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stats* s) {
+    if (!e || !a || !s || (!a->frags && a->frag_nbytes) || !a->round_dir) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    call_scope scope_(e);
+    try {
+        using clk = std::chrono::steady_clock;
+        const auto t0 = clk::now();
+        CDBG_CUDA(cudaSetDevice(e->device));
+        *s = cdbg_seed_stats();
+        if (a->kmer_bits != 0 && a->kmer_bits != 64 && a->kmer_bits != 128)
+            throw std::runtime_error("kmer_bits must be 0, 64 or 128");
+        cdbg::seed_config c;
+        c.k = a->k;
+        c.num_buckets = a->num_buckets ? a->num_buckets : 1024;
+        c.wide = a->kmer_bits ? a->kmer_bits == 128 : a->k > 31;
+        if (c.k < 2 || c.k > (c.wide ? 63u : 32u)) throw std::runtime_error("k out of range for the k-mer width");
+        const uint32_t T = host_threads(a->host_threads);
+        e->A.reset();
+        // fragment bytes per device pass: a pass holds about 3x its bytes
+        // (fragments, tigs, closed unitigs, ~80 bytes per fragment)
+        uint64_t chunk = a->chunk_bytes;
+        if (!chunk) {
+            size_t fr = 0, tot = 0;
+            CDBG_CUDA(cudaMemGetInfo(&fr, &tot));
+            uint64_t avail = fr + e->A.cached_free();
+            if (e->mem_limit && e->mem_limit < avail) avail = e->mem_limit;
+            chunk = std::max<uint64_t>(avail / 4, 64ull << 20);
+        }
+        // One pass: the bytes go up on another thread while the records are
+        // found (the copy needs no record boundaries).
+        const bool one_pass = a->frag_nbytes <= chunk;
+        uint8_t* dF1 = nullptr;
+        cudaError_t up_err = cudaSuccess;
+        std::thread uploader;
+        if (one_pass && a->frag_nbytes) {
+            dF1 = e->A.alloc<uint8_t>(a->frag_nbytes + 16);
+            uploader = std::thread([&] {
+                up_err = cudaSetDevice(e->device);
+                if (up_err == cudaSuccess) up_err = cudaMemsetAsync(dF1 + a->frag_nbytes, 0, 16, e->st);
+                if (up_err == cudaSuccess)
+                    up_err = cudaMemcpyAsync(dF1, a->frags, a->frag_nbytes, cudaMemcpyHostToDevice, e->st);
+                if (up_err == cudaSuccess) up_err = cudaStreamSynchronize(e->st);
+            });
+        }
+        // record boundaries: the records are variable-length and back to back
+        std::vector<uint64_t>& off = e->h_rec_off;
+        try {
+            cdbg::io::frag_record_offsets(a->frags, a->frag_nbytes, off, T, &e->h_rec_parts);
+        } catch (...) {
+            if (uploader.joinable()) uploader.join();
+            throw;
+        }
+        if (uploader.joinable()) uploader.join();
+        CDBG_CUDA(up_err);
+        const uint64_t n = off.size() - 1;
+        s->fragments = n;
+        s->ms_scan = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        cdbg::io::round0_store store(a->round_dir, c.num_buckets);
+        std::FILE* cf = nullptr;
+        if (a->closed_path) {
+            cf = std::fopen(a->closed_path, "wb");
+            if (!cf) throw std::runtime_error(std::string("cannot open ") + a->closed_path);
+        }
+        std::unique_ptr<std::FILE, int (*)(std::FILE*)> cf_guard(cf, [](std::FILE* f) { return f ? std::fclose(f) : 0; });
+        e->h_closed.clear();
+        cudaEvent_t ev[2];
+        CDBG_CUDA(cudaEventCreate(&ev[0]));
+        CDBG_CUDA(cudaEventCreate(&ev[1]));
+        std::unique_ptr<cudaEvent_t, void (*)(cudaEvent_t*)> ev_guard(ev, [](cudaEvent_t* v) {
+            cudaEventDestroy(v[0]);
+            cudaEventDestroy(v[1]);
+        });
+        std::vector<uint64_t> loff, boff(c.num_buckets + 1);
+        for (uint64_t i0 = 0; i0 < n;) {
+            uint64_t i1 = i0 + 1;
+            while (i1 < n && off[i1 + 1] - off[i0] <= chunk) ++i1;
+            const uint64_t nc = i1 - i0, bytes = off[i1] - off[i0];
+            auto mk = e->A.mark();
+            uint8_t* dF = dF1;
+            if (!dF) {
+                dF = e->A.alloc<uint8_t>(bytes + 16);
+                CDBG_CUDA(cudaMemsetAsync(dF + bytes, 0, 16, e->st));
+                CDBG_CUDA(cudaMemcpyAsync(dF, a->frags + off[i0], bytes, cudaMemcpyHostToDevice, e->st));
+            }
+            uint64_t* dOff = e->A.alloc<uint64_t>(nc + 1);
+            if (i0 == 0 && i1 == n) {
+                CDBG_CUDA(cudaMemcpyAsync(dOff, off.data(), 8 * (nc + 1), cudaMemcpyHostToDevice, e->st));
+            } else {
+                loff.resize(nc + 1);
+                for (uint64_t i = 0; i <= nc; ++i) loff[i] = off[i0 + i] - off[i0];
+                CDBG_CUDA(cudaMemcpyAsync(dOff, loff.data(), 8 * (nc + 1), cudaMemcpyHostToDevice, e->st));
+            }
+            CDBG_CUDA(cudaEventRecord(ev[0], e->st));
+            cdbg::seed_device_out out;
+            cdbg::seed_fragments(dF, dOff, nc, c, e->A, e->st, e->d_err, out);
+            CDBG_CUDA(cudaEventRecord(ev[1], e->st));
+            uint8_t* ht = (uint8_t*)e->h_frag.ensure(out.tig_bytes + 16);
+            uint8_t* hc = (uint8_t*)e->h_words.ensure(out.closed_bytes + 16);
+            CDBG_CUDA(cudaMemcpyAsync(ht, out.tigs, out.tig_bytes, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(hc, out.closed, out.closed_bytes, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaMemcpyAsync(boff.data(), out.bucket_off, 8 * boff.size(), cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaStreamSynchronize(e->st));
+            float ms = 0;
+            CDBG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            s->ms_device += ms;
+            const auto tf = clk::now();
+            // the closed unitigs go out on their own thread while the frames compress
+            bool closed_ok = true;
+            std::thread closed_writer([&] {
+                if (cf)
+                    closed_ok = !out.closed_bytes || std::fwrite(hc, 1, out.closed_bytes, cf) == out.closed_bytes;
+                else
+                    e->h_closed.insert(e->h_closed.end(), hc, hc + out.closed_bytes);
+            });
+            try {
+                store.append(ht, boff.data(), T);
+            } catch (...) {
+                closed_writer.join();
+                throw;
+            }
+            closed_writer.join();
+            if (!closed_ok) throw std::runtime_error(std::string("short write to ") + a->closed_path);
+            s->ms_files += std::chrono::duration<double, std::milli>(clk::now() - tf).count();
+            s->routed += out.n_routed;
+            s->closed_fragments += out.n_closed;
+            s->closed_unitigs += out.n_pieces;
+            s->routed_frag_bytes += out.routed_record_bytes;
+            s->closed_nbytes += out.closed_bytes;
+            ++s->n_passes;
+            e->A.release(mk);
+            i0 = i1;
+        }
+        const auto tf = clk::now();
+        store.finish(T);
+        s->ms_files += std::chrono::duration<double, std::milli>(clk::now() - tf).count();
+        if (cf && std::fclose(cf_guard.release()) != 0)
+            throw std::runtime_error(std::string("close failed on ") + a->closed_path);
+        s->closed = cf ? nullptr : e->h_closed.data();
+        s->round0_bytes = store.raw_bytes();
+        s->round0_file_bytes = store.comp_bytes();
+        s->ms_total = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        return 0;
+    } catch (std::exception const& ex) {
+        return fail(ex);
+    }
+}
+
+int cdbg_frag_record_offsets(const uint8_t* frags, uint64_t frag_nbytes, uint32_t threads, uint64_t* offsets,
+                             uint64_t cap, uint64_t* n_records) {
+    if ((!frags && frag_nbytes) || !n_records || (!offsets && cap)) {
+        g_last_error = "null argument";
+        return -1;
+    }
+    try {
+        std::vector<uint64_t> off;
+        cdbg::io::frag_record_offsets(frags, frag_nbytes, off, host_threads(threads));
+        *n_records = off.size() - 1;
+        if (off.size() <= cap) std::memcpy(offsets, off.data(), 8 * off.size());
+        return 0;
+    } catch (std::exception const& ex) {
         return fail(ex);
     }
 }

@@ -433,6 +433,214 @@ void bucket_file_set::close() {
     }
 }
 
+// ---- stitch round store, round 0
+namespace {
+constexpr uint64_t ROUND_FRAME = 4ull << 20;  // round_store_file::FRAME_BUDGET (stitch_extmem.hpp:556)
+
+inline uint32_t get_u32(uint8_t const* p) {
+    uint32_t v;
+    std::memcpy(&v, p, 4);
+    return v;
+}
+}  // namespace
+
+round0_store::round0_store(std::string dir, uint32_t num_buckets)
+    : m_dir(std::move(dir)), m_B(num_buckets), m_files(num_buckets, nullptr), m_pend(num_buckets) {
+    std::filesystem::create_directories(m_dir);
+    // a round-0 file left from an earlier build would be read as input
+    for (uint32_t b = 0; b < m_B; ++b) std::remove(path(b).c_str());
+}
+
+round0_store::~round0_store() {
+    for (void* f : m_files)
+        if (f) std::fclose((std::FILE*)f);
+}
+
+std::string round0_store::path(uint32_t b) const {
+    return m_dir + "/stitch_r0_b" + std::to_string(b) + ".bin";
+}
+
+void round0_store::flush(uint32_t b, uint8_t const* data, uint64_t n, uint64_t& comp) {
+    if (n > LZ4_MAX_INPUT) throw std::runtime_error("stitch round frame too large for LZ4");
+    std::FILE* f = (std::FILE*)m_files[b];
+    if (!f) {
+        f = std::fopen(path(b).c_str(), "wb");
+        if (!f) throw std::runtime_error("cannot open stitch round file: " + path(b) + ": " + std::strerror(errno));
+        m_files[b] = f;
+    }
+    std::vector<char> out((size_t)LZ4_compressBound((int)n));
+    const int c = LZ4_compress_default((char const*)data, out.data(), (int)n, (int)out.size());
+    if (c <= 0) throw std::runtime_error("LZ4_compress_default failed on " + path(b));
+    const uint32_t u32 = (uint32_t)n, c32 = (uint32_t)c;
+    if (std::fwrite(&u32, 4, 1, f) != 1 || std::fwrite(&c32, 4, 1, f) != 1 ||
+        std::fwrite(out.data(), 1, (size_t)c, f) != (size_t)c)
+        throw std::runtime_error("short write to " + path(b));
+    comp += 8 + (uint64_t)c;
+}
+
+void round0_store::append(uint8_t const* tigs, uint64_t const* boff, uint32_t threads) {
+    std::vector<uint64_t> comp(m_B, 0);
+    parallel_for(m_B, threads, [&](size_t bi) {
+        const uint32_t b = (uint32_t)bi;
+        const uint64_t a = boff[b], e = boff[b + 1];
+        if (a == e) return;
+        std::vector<uint8_t>& pend = m_pend[b];
+        uint64_t seg = a, pos = a;
+        while (pos < e) {
+            // ext_tig_serialize layout: 13-byte head, runs, u32 seq_len, 2-bit bases
+            if (pos + 13 > e) throw std::runtime_error("truncated tig in round-0 output");
+            const uint64_t nruns = get_u32(tigs + pos + 9);
+            const uint64_t lp = pos + 13 + 12 * nruns;
+            if (lp + 4 > e) throw std::runtime_error("truncated tig in round-0 output");
+            pos = lp + 4 + ((uint64_t)get_u32(tigs + lp) + 3) / 4;
+            if (pos > e) throw std::runtime_error("truncated tig in round-0 output");
+            // emit() appends one tig, then flushes once the batch holds a frame
+            if (pend.size() + (pos - seg) >= ROUND_FRAME) {
+                if (pend.empty()) {
+                    flush(b, tigs + seg, pos - seg, comp[b]);
+                } else {
+                    pend.insert(pend.end(), tigs + seg, tigs + pos);
+                    flush(b, pend.data(), pend.size(), comp[b]);
+                    pend.clear();
+                }
+                seg = pos;
+            }
+        }
+        pend.insert(pend.end(), tigs + seg, tigs + e);
+    });
+    m_raw += boff[m_B] - boff[0];
+    for (uint64_t c : comp) m_comp += c;
+}
+
+void round0_store::finish(uint32_t threads) {
+    std::vector<uint64_t> comp(m_B, 0);
+    parallel_for(m_B, threads, [&](size_t bi) {
+        const uint32_t b = (uint32_t)bi;
+        std::vector<uint8_t>& pend = m_pend[b];
+        if (!pend.empty()) {
+            flush(b, pend.data(), pend.size(), comp[b]);
+            std::vector<uint8_t>().swap(pend);
+        }
+        std::FILE* f = (std::FILE*)m_files[b];
+        if (!f) return;
+        const uint32_t eof = 0;
+        if (std::fwrite(&eof, 4, 1, f) != 1) throw std::runtime_error("short write to " + path(b));
+        if (std::fclose(f) != 0) throw std::runtime_error("close failed on " + path(b));
+        m_files[b] = nullptr;
+        comp[b] += 4;
+    });
+    for (uint64_t c : comp) m_comp += c;
+}
+
+namespace {
+// The record at p: its end, or 0 when it runs past n.
+// [u8 open_flags][u32 nruns][nruns x 12][u32 seq_len][seq]
+inline uint64_t frag_record_end(uint8_t const* d, uint64_t n, uint64_t p) {
+    if (p + 5 > n) return 0;
+    const uint64_t lp = p + 5 + 12ull * get_u32(d + p + 1);
+    if (lp + 4 > n) return 0;
+    const uint64_t q = lp + 4 + get_u32(d + lp);
+    return q > n ? 0 : q;
+}
+
+// Could a record start at p?  Flags 0..3, a run count and length that stay in
+// the buffer, ACGT bases, and the same for the records after it (4 deep).
+bool plausible_start(uint8_t const* d, uint64_t n, uint64_t p) {
+    for (int depth = 0; depth < 4 && p < n; ++depth) {
+        if (d[p] > 3 || p + 5 > n || get_u32(d + p + 1) > (1u << 20)) return false;
+        const uint64_t q = frag_record_end(d, n, p);
+        if (!q) return false;
+        const uint64_t lp = p + 5 + 12ull * get_u32(d + p + 1);
+        const uint64_t s = lp + 4, e = std::min<uint64_t>(q, s + 16);
+        for (uint64_t x = s; x < e; ++x)
+            if (d[x] != 'A' && d[x] != 'C' && d[x] != 'G' && d[x] != 'T') return false;
+        p = q;
+    }
+    return true;
+}
+}  // namespace
+
+void frag_record_offsets(uint8_t const* d, uint64_t n, std::vector<uint64_t>& off, uint32_t threads,
+                         std::vector<std::vector<uint64_t>>* scratch) {
+    off.clear();
+    const uint64_t P = std::max<uint64_t>(1, std::min<uint64_t>(threads, n >> 20));
+    // Part t covers [c(t), c(t + 1)).  Part 0 starts at a record; every other
+    // part guesses its first record (plausible_start) and follows the chain
+    // to the first record at or past its end.  Chains that meet stay together
+    // (a record determines the next), so the merge takes a part's chain from
+    // where the true chain meets it and walks the true chain itself elsewhere.
+    auto c = [&](uint64_t t) { return n * t / P; };
+    struct part {
+        uint64_t start = 0, end = 0;
+        bool found = false, broken = false;
+        std::vector<uint64_t> recs;
+    };
+    std::vector<part> parts(P);
+    // the caller's vectors keep their pages from call to call
+    if (scratch) {
+        scratch->resize(std::max<size_t>(scratch->size(), P));
+        for (uint64_t t = 0; t < P; ++t) parts[t].recs.swap((*scratch)[t]);
+    }
+    struct give_back {
+        std::vector<part>& parts;
+        std::vector<std::vector<uint64_t>>* scratch;
+        ~give_back() {
+            if (scratch)
+                for (size_t t = 0; t < parts.size(); ++t) parts[t].recs.swap((*scratch)[t]);
+        }
+    } give_back_{parts, scratch};
+    parallel_for(P, (uint32_t)P, [&](size_t t) {
+        part& pt = parts[t];
+        uint64_t pos = c(t);
+        const uint64_t lim = c(t + 1);
+        if (t > 0) {
+            while (pos < lim && !plausible_start(d, n, pos)) ++pos;
+            if (pos >= lim) return;
+        }
+        pt.found = true;
+        pt.start = pos;
+        pt.recs.clear();
+        pt.recs.reserve((lim - pos) / 64 + 16);
+        while (pos < lim) {
+            const uint64_t q = frag_record_end(d, n, pos);
+            if (!q) {
+                pt.broken = true;
+                break;
+            }
+            pt.recs.push_back(pos);
+            pos = q;
+        }
+        pt.end = pos;
+    });
+    size_t guess = 1;
+    for (auto const& pt : parts) guess += pt.recs.size();
+    off.reserve(guess);
+    uint64_t e = 0;  // the next true record start
+    for (uint64_t t = 0; t < P; ++t) {
+        const uint64_t lim = c(t + 1);
+        if (e >= lim) continue;  // a record from an earlier part spans this one
+        part const& pt = parts[t];
+        size_t j = 0;
+        if (pt.found) j = std::lower_bound(pt.recs.begin(), pt.recs.end(), e) - pt.recs.begin();
+        while (e < lim) {
+            while (pt.found && j < pt.recs.size() && pt.recs[j] < e) ++j;
+            if (pt.found && j < pt.recs.size() && pt.recs[j] == e) {
+                // joined: the rest of this part's chain is true
+                off.insert(off.end(), pt.recs.begin() + j, pt.recs.end());
+                if (pt.broken) throw std::runtime_error("truncated fragment record");
+                e = pt.end;
+                break;
+            }
+            const uint64_t q = frag_record_end(d, n, e);
+            if (!q) throw std::runtime_error("truncated fragment record");
+            off.push_back(e);
+            e = q;
+        }
+    }
+    if (e != n) throw std::runtime_error("truncated fragment record");
+    off.push_back(n);
+}
+
 void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,
                        std::function<uint8_t*(uint64_t)> const& alloc, bucket_bytes& out,
                        bool delete_after) {

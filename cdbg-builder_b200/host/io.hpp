@@ -109,6 +109,43 @@ private:
     uint64_t m_comp = 0;
 };
 
+// ---- stitch round store, round 0 (stitch_extmem.hpp:471-600) --------------
+// <dir>/stitch_r0_b<b>.bin written as the reference's round_store_file writes
+// round 0: serialized tigs go to a per-bucket batch that is flushed as one
+// LZ4 frame [u32 raw][u32 compressed][bytes] as soon as it holds 4 MiB or
+// more, and at finish the rest is flushed and a [u32 0] end mark written.  A
+// bucket that received no tig has no file.
+class round0_store {
+public:
+    round0_store(std::string dir, uint32_t num_buckets);
+    ~round0_store();
+    round0_store(round0_store const&) = delete;
+    round0_store& operator=(round0_store const&) = delete;
+    std::string path(uint32_t b) const;
+    // tigs: serialized tigs, bucket by bucket; boff: num_buckets + 1 offsets.
+    // Successive calls append in order (the tigs of one call follow those of
+    // the calls before in every bucket).
+    void append(uint8_t const* tigs, uint64_t const* boff, uint32_t threads);
+    void finish(uint32_t threads);
+    uint64_t raw_bytes() const { return m_raw; }
+    uint64_t comp_bytes() const { return m_comp; }
+
+private:
+    void flush(uint32_t b, uint8_t const* data, uint64_t n, uint64_t& comp);
+    std::string m_dir;
+    uint32_t m_B;
+    std::vector<void*> m_files;
+    std::vector<std::vector<uint8_t>> m_pend;
+    uint64_t m_raw = 0, m_comp = 0;
+};
+
+// Byte offsets of the records of a frag_unitigs.bin buffer (n + 1 entries,
+// the last = n_bytes), found by `threads` threads; throws at a record that
+// runs past the end.  `scratch` (optional) holds the threads' lists between
+// calls, so their memory is reused.
+void frag_record_offsets(uint8_t const* data, uint64_t n_bytes, std::vector<uint64_t>& off, uint32_t threads,
+                         std::vector<std::vector<uint64_t>>* scratch = nullptr);
+
 // Decompressed contents of bucket files 0..B-1 back to back (buffer from
 // `alloc`), with `chunk_off` = byte offsets of frame starts (records never
 // straddle a frame) and `chunk_bucket` = the bucket of each chunk.

@@ -22,6 +22,11 @@
  *                       color-set merge (streaming_color_set_dict.hpp:148-182).
  *   cdbg_gpu_build   <- the two calls above back to back, in memory (no bucket
  *                       files): builder.hpp:180 + :269.
+ *   cdbg_gpu_stitch_seed <- detail::ext_seed_round0_raw_par(for_each_raw,
+ *                       frag_record_parse, k, store, sink, done, T), the
+ *                       round-0 half of stitch_unitigs_extmem_file_streaming
+ *                       (include/phase3_stitch/stitch_extmem.hpp:1013-1099,
+ *                       :1120-1129) with a round_store_file as the store.
  */
 #ifndef CDBG_GPU_H
 #define CDBG_GPU_H
@@ -312,6 +317,65 @@ int cdbg_merge_shards(uint32_t num_shards, const uint8_t* const* frag, const uin
                       const uint64_t* const* class_offsets, const uint64_t* n_classes, cdbg_merged* out);
 void cdbg_merged_free(cdbg_merged* m);
 const char* cdbg_merge_last_error(void);
+
+/* ---- round 0 of the phase-3 stitch ------------------------------------- */
+
+/* The frag-file seed of the stitch: every fragment of a frag_unitigs.bin
+ * (unitig_spill.hpp:491-522 records) becomes a round-0 tig in the round-store
+ * bucket of the canonical boundary k-mer it presents, or, when it has no open
+ * end, the monochromatic unitigs it splits into (stitch_extmem.hpp:930-944).
+ * Outputs:
+ *   round_dir/stitch_r0_b<b>.bin  the round store's round-0 files, byte for
+ *       byte as a one-thread reference seed writes them (tigs of a bucket in
+ *       fragment order, ext_tig_serialize layout, 4 MiB LZ4 frames, end
+ *       mark); earlier round-0 files of buckets [0, num_buckets) there are
+ *       removed first.  The reference's rounds continue from them:
+ *       round_store_file store(round_dir, num_buckets); store.advance();
+ *       ext_run_rounds(store, k, num_buckets, sink, done, T).
+ *   the closed fragments' unitigs as frag records, fragment order: what the
+ *       reference passes to `sink` during the seed (and counts in `done`),
+ *       written to closed_path, or, with closed_path NULL, left in host
+ *       memory owned by the engine (s->closed, valid until its next call).
+ * With many threads the reference appends a bucket's tigs in the order its
+ * workers finish; the rounds do not depend on that order (each tig's random
+ * state comes from its bases). */
+typedef struct cdbg_seed_args {
+    const uint8_t* frags;       /* frag_unitigs.bin contents, host memory */
+    uint64_t frag_nbytes;
+    uint32_t k;
+    uint32_t num_buckets;       /* round-store buckets; 0 = 1024 */
+    uint32_t kmer_bits;         /* width of the reference build's kmer_int_t: 64, 128
+                                   (CDBG_LARGE_K), or 0 = 64 for k <= 31, else 128 */
+    uint32_t host_threads;      /* 0 = all cores */
+    uint64_t chunk_bytes;       /* fragment bytes per device pass; 0 = auto */
+    const char* round_dir;
+    const char* closed_path;    /* may be NULL */
+} cdbg_seed_args;
+
+typedef struct cdbg_seed_stats {
+    uint64_t fragments, routed, closed_fragments, closed_unitigs;
+    uint64_t routed_frag_bytes; /* frag record bytes of the open fragments */
+    uint64_t round0_bytes;      /* serialized tigs (uncompressed) */
+    uint64_t round0_file_bytes; /* the round-0 files on disk */
+    const uint8_t* closed;      /* closed unitigs when closed_path is NULL */
+    uint64_t closed_nbytes;
+    uint64_t n_passes;
+    double ms_scan;             /* host: record offsets */
+    double ms_device;           /* device time of the seed kernels (CUDA events) */
+    double ms_files;            /* host: round-0 frames compressed and written, closed unitigs written */
+    double ms_total;            /* wall time of the call */
+} cdbg_seed_stats;
+
+int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stats* s);
+
+/* Byte offsets of the records of a frag_unitigs.bin buffer, found by several
+ * host threads (each guesses a record start in its share of the buffer and
+ * follows the records from there; the shares are joined where they meet the
+ * records followed from the buffer's start, so the result is exact).  Writes
+ * n_records + 1 offsets (the last = frag_nbytes) when cap allows.  Host only;
+ * fails on a record that runs past the end. */
+int cdbg_frag_record_offsets(const uint8_t* frags, uint64_t frag_nbytes, uint32_t host_threads, uint64_t* offsets,
+                             uint64_t cap, uint64_t* n_records);
 
 /* Serialized size of the bucket records of the engine's last cdbg_gpu_build
  * (the uncompressed bytes its bucket files would hold), counted on the device

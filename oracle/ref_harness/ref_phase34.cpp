@@ -6,6 +6,15 @@
 // in-process frag_unitig_writer / streaming_color_set_dict.
 //
 //   ref_phase34 <frag_file> <classes_file> <num_colors> <k> <threads> <out_basename> <tmp_dir>
+//               [<seed_closed_file>]
+//
+// With seed_closed_file, round 0 of the stitch comes from another
+// implementation: tmp_dir already holds the round-0 files stitch_r0_b<b>.bin
+// of 1024 round-store buckets, and seed_closed_file the closed fragments'
+// unitigs (frag records) that the seed would have passed to the sink.  They
+// go to the sink, the round store is advanced past round 0 and the
+// reference's doubling rounds (stitch_extmem.hpp:625, ext_run_rounds) run as
+// stitch_unitigs_extmem_file_streaming runs them after its seed (:1127-1128).
 //
 // classes_file: u64 count, then per class u32 n followed by n ascending u32
 // colors.  Every class is interned into a streaming_color_set_dict in file
@@ -50,8 +59,9 @@ static std::vector<std::vector<uint32_t>> read_classes(std::string const& path) 
 }
 
 int main(int argc, char** argv) {
-    if (argc != 8) {
-        std::fprintf(stderr, "usage: %s frag_file classes_file num_colors k threads out_basename tmp_dir\n",
+    if (argc != 8 && argc != 9) {
+        std::fprintf(stderr,
+                     "usage: %s frag_file classes_file num_colors k threads out_basename tmp_dir [seed_closed_file]\n",
                      argv[0]);
         return 2;
     }
@@ -98,8 +108,22 @@ int main(int argc, char** argv) {
             uint32_t len;
             while (rd.next_raw(rec, len)) fn(rec, len);
         };
-        cdbg::stitch_unitigs_extmem_file_streaming(for_each_raw, cdbg::frag_record_parse, k, tmp_dir,
-                                                   std::ref(uwriter), 1024, nullptr, T);
+        if (argc == 9) {
+            cdbg::frag_unitig_block_reader rd(argv[8]);
+            uint8_t const* rec;
+            uint32_t len;
+            while (rd.next_raw(rec, len)) {
+                cdbg::stitchable_unitig u;
+                cdbg::frag_record_parse(rec, len, u.open_flags, u.runs, u.seq);
+                uwriter(std::move(u));
+            }
+            cdbg::detail::round_store_file store(tmp_dir, 1024);
+            store.advance();
+            cdbg::detail::ext_run_rounds(store, k, 1024, std::ref(uwriter), nullptr, T);
+        } else {
+            cdbg::stitch_unitigs_extmem_file_streaming(for_each_raw, cdbg::frag_record_parse, k, tmp_dir,
+                                                       std::ref(uwriter), 1024, nullptr, T);
+        }
         const uint64_t num_unitigs = uwriter.total_unitigs();
         const uint64_t num_kmers = uwriter.total_seq_bytes() - num_unitigs * (uint64_t)(k - 1);
         cdbg::emit_fasta(uwriter, out, num_unitigs, 0.0);

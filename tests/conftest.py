@@ -107,3 +107,64 @@ def run_ref(args):
     r = subprocess.run(args, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     return r.stdout
+
+
+def read_round_file(path):
+    """Frames of a stitch round file ([u32 raw][u32 comp][bytes]... [u32 0]),
+    decompressed with the system LZ4 library: a list of raw frame bytes."""
+    import struct
+    L = ctypes.CDLL("liblz4.so.1")
+    L.LZ4_decompress_safe.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    data = open(path, "rb").read()
+    frames, p = [], 0
+    while True:
+        (u,) = struct.unpack_from("<I", data, p)
+        p += 4
+        if u == 0:
+            break
+        (c,) = struct.unpack_from("<I", data, p)
+        p += 4
+        dst = ctypes.create_string_buffer(u)
+        assert L.LZ4_decompress_safe(data[p:p + c], dst, c, u) == u, path
+        frames.append(dst.raw)
+        p += c
+    assert p == len(data), "bytes after the end mark in " + path
+    return frames
+
+
+def round0_files(d, num_buckets):
+    """{bucket: file bytes} of the stitch_r0_b<b>.bin files in d."""
+    out = {}
+    for b in range(num_buckets):
+        p = os.path.join(d, "stitch_r0_b%d.bin" % b)
+        if os.path.exists(p):
+            out[b] = open(p, "rb").read()
+    return out
+
+
+_ACGT = bytes(b"ACGT"[i & 3] for i in range(256))
+
+
+def synth_frags(seed, n, k, max_runs=4, max_m=20, p_foreign=0.2, p_closed=0.3):
+    """n random frag records (unitig_spill.hpp:491-522 layout) with the shapes
+    the seed branches on: closed and open (left, right, both) fragments, color
+    runs of several k-mers, COLOR_RUN_FOREIGN runs at the ends and inside,
+    closed fragments without runs.  Each sequence has sum(num_kmers) + k - 1
+    ACGT bases, and an open one at least k."""
+    import random
+    import struct
+    r = random.Random(seed)
+    out = bytearray()
+    for _ in range(n):
+        closed = r.random() < p_closed
+        of = 0 if closed else r.choice((1, 2, 3))
+        nr = r.randint(0 if closed else 1, max_runs)
+        runs = [((2 ** 64 - 1) if r.random() < p_foreign else r.randrange(1 << 20), r.randint(1, max_m))
+                for _ in range(nr)]
+        ln = sum(m for _, m in runs) + k - 1 if runs else k - 1
+        seq = r.randbytes(ln).translate(_ACGT)
+        out += struct.pack("<BI", of, nr)
+        for cid, m in runs:
+            out += struct.pack("<QI", cid, m)
+        out += struct.pack("<I", ln) + seq
+    return bytes(out)

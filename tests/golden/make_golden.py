@@ -15,8 +15,14 @@ their outputs as fixtures:
   <case>/frag_unitigs.bin  ref_phase2 over those bucket files, 1 thread
   <case>/out.color_sets    finalized color sets of the same run
   <case>/meta.json         k, m, num_buckets, num_colors, counts
+  <case>/seed_b64.pack     the reference's stitch round-0 files (ref_seed: its
+                           ext_seed_round0_raw_par, 1 thread, 64 round-store
+                           buckets) over frag_unitigs.bin, packed as
+                           [u64 size][file bytes] per bucket 0..63 (size 0: no file)
+  <case>/seed_closed.bin   the closed unitigs the same seed passed to its sink
 
-Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
+Usage: python tests/golden/make_golden.py [--seed-only]   (needs oracle/_ref built;
+--seed-only remakes the two seed fixtures from the existing frag_unitigs.bin)
 """
 import json
 import os
@@ -119,9 +125,42 @@ def make_case(name, spec):
     os.remove(abslist)
 
 
+SEED_BUCKETS = 64
+
+
+def make_seed(name, k):
+    d = os.path.join(HERE, name)
+    tmp = os.path.join(d, "_seed")
+    shutil.rmtree(tmp, ignore_errors=True)
+    run([os.path.join(REF, "ref_seed" + ("-largek" if k > 31 else "")), os.path.join(d, "frag_unitigs.bin"),
+         str(k), str(SEED_BUCKETS), "1", tmp])
+    with open(os.path.join(d, "seed_b%d.pack" % SEED_BUCKETS), "wb") as pk:
+        for b in range(SEED_BUCKETS):
+            f = os.path.join(tmp, "stitch_r0_b%d.bin" % b)
+            data = open(f, "rb").read() if os.path.exists(f) else b""
+            pk.write(struct.pack("<Q", len(data)) + data)
+    shutil.copy(os.path.join(tmp, "closed.bin"), os.path.join(d, "seed_closed.bin"))
+    shutil.rmtree(tmp)
+
+
+def unpack_seed(case_dir):
+    """{bucket: round-0 file bytes} of a case's seed fixture."""
+    data = open(os.path.join(case_dir, "seed_b%d.pack" % SEED_BUCKETS), "rb").read()
+    out, p = {}, 0
+    for b in range(SEED_BUCKETS):
+        (n,) = struct.unpack_from("<Q", data, p)
+        p += 8
+        if n:
+            out[b] = data[p:p + n]
+        p += n
+    return out
+
+
 if __name__ == "__main__":
     for name, spec in CASES.items():
-        make_case(name, spec)
+        if "--seed-only" not in sys.argv:
+            make_case(name, spec)
+        make_seed(name, spec[0])
         print("wrote", name)
 
 

@@ -24,6 +24,9 @@ int main(int argc, char**) {
     cdbg::streaming_color_set_dict d(4, "x.color_sets");
     cdbg::gpu::process_buckets(g, "tmp", 1024, 31, 4, "tmp/frag_unitigs.bin", d, false, 1);
     cdbg::gpu::build_in_memory(g, files, 31, 0, 1024, "tmp/frag_unitigs.bin", "x.color_sets", 1);
+    std::atomic<uint64_t> done{0};
+    cdbg::frag_unitig_writer sink("tmp/unitigs.bin");
+    cdbg::gpu::stitch_from_frag_file(g, "tmp/frag_unitigs.bin", 31, "tmp", std::ref(sink), 1024, &done, 1);
 }
 '''
 
