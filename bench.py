@@ -863,10 +863,17 @@ def main_seed(a):
     base = scratch_base(4 * n_frag_bytes + (8 << 30)) or tempfile.gettempdir()
     work = tempfile.mkdtemp(prefix="cdbg_seed_", dir=base)
     try:
-        rd, closed = os.path.join(work, "gpu"), os.path.join(work, "gpu_closed.bin")
+        calls = [0]
 
         def step():
-            return eng.stitch_seed((frags.data_ptr(), n_frag_bytes), k, rd, num_buckets=B, closed_path=closed)
+            # each call writes a fresh directory, as a build's stitch does; the
+            # files are removed after the call, outside its wall time
+            d = os.path.join(work, "gpu%d" % calls[0])
+            calls[0] += 1
+            r = eng.stitch_seed((frags.data_ptr(), n_frag_bytes), k, d, num_buckets=B,
+                                closed_path=os.path.join(d, "closed.bin"))
+            shutil.rmtree(d, ignore_errors=True)
+            return r
 
         for _ in range(max(a.warmup, 3)):
             st = step()

@@ -1677,16 +1677,20 @@ int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stat
             });
         }
         // record boundaries: the records are variable-length and back to back
-        std::vector<uint64_t>& off = e->h_rec_off;
+        // (into pinned memory the engine keeps: no page faults on later calls,
+        // and the upload is a direct copy)
+        uint64_t n = 0;
         try {
-            cdbg::io::frag_record_offsets(a->frags, a->frag_nbytes, off, T, &e->h_rec_parts);
+            n = cdbg::io::frag_record_offsets(
+                a->frags, a->frag_nbytes, T,
+                [&](uint64_t m) { return (uint64_t*)e->h_rec_off.ensure(8 * m); }, &e->h_rec_parts);
         } catch (...) {
             if (uploader.joinable()) uploader.join();
             throw;
         }
         if (uploader.joinable()) uploader.join();
         CDBG_CUDA(up_err);
-        const uint64_t n = off.size() - 1;
+        uint64_t const* off = (uint64_t const*)e->h_rec_off.p;
         s->fragments = n;
         s->ms_scan = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         cdbg::io::round0_store store(a->round_dir, c.num_buckets);
@@ -1718,7 +1722,7 @@ int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stat
             }
             uint64_t* dOff = e->A.alloc<uint64_t>(nc + 1);
             if (i0 == 0 && i1 == n) {
-                CDBG_CUDA(cudaMemcpyAsync(dOff, off.data(), 8 * (nc + 1), cudaMemcpyHostToDevice, e->st));
+                CDBG_CUDA(cudaMemcpyAsync(dOff, off, 8 * (nc + 1), cudaMemcpyHostToDevice, e->st));
             } else {
                 loff.resize(nc + 1);
                 for (uint64_t i = 0; i <= nc; ++i) loff[i] = off[i0 + i] - off[i0];
@@ -1728,31 +1732,57 @@ int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stat
             cdbg::seed_device_out out;
             cdbg::seed_fragments(dF, dOff, nc, c, e->A, e->st, e->d_err, out);
             CDBG_CUDA(cudaEventRecord(ev[1], e->st));
-            uint8_t* ht = (uint8_t*)e->h_frag.ensure(out.tig_bytes + 16);
-            uint8_t* hc = (uint8_t*)e->h_words.ensure(out.closed_bytes + 16);
-            CDBG_CUDA(cudaMemcpyAsync(ht, out.tigs, out.tig_bytes, cudaMemcpyDeviceToHost, e->st));
-            CDBG_CUDA(cudaMemcpyAsync(hc, out.closed, out.closed_bytes, cudaMemcpyDeviceToHost, e->st));
             CDBG_CUDA(cudaMemcpyAsync(boff.data(), out.bucket_off, 8 * boff.size(), cudaMemcpyDeviceToHost, e->st));
             CDBG_CUDA(cudaStreamSynchronize(e->st));
             float ms = 0;
             CDBG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
             s->ms_device += ms;
             const auto tf = clk::now();
-            // the closed unitigs go out on their own thread while the frames compress
+            // the tigs come back in bucket ranges of ~1/16 of their bytes: host
+            // threads compress and write one range while the next still copies;
+            // the closed unitigs follow and go out on their own thread
+            uint8_t* ht = (uint8_t*)e->h_frag.ensure(out.tig_bytes + 16);
+            uint8_t* hc = (uint8_t*)e->h_words.ensure(out.closed_bytes + 16);
+            std::vector<uint32_t> cut{0};
+            const uint64_t per = std::max<uint64_t>(64ull << 20, out.tig_bytes / 16);
+            for (uint32_t b = 1; b < c.num_buckets; ++b)
+                if (boff[b] - boff[cut.back()] >= per) cut.push_back(b);
+            cut.push_back(c.num_buckets);
+            std::vector<cudaEvent_t> rev(cut.size());  // ranges, then the closed unitigs
+            for (auto& x : rev) CDBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+            std::unique_ptr<std::vector<cudaEvent_t>, void (*)(std::vector<cudaEvent_t>*)> rev_guard(
+                &rev, [](std::vector<cudaEvent_t>* v) {
+                    for (auto x : *v) cudaEventDestroy(x);
+                });
+            for (size_t r = 0; r + 1 < cut.size(); ++r) {
+                const uint64_t lo = boff[cut[r]], hi = boff[cut[r + 1]];
+                if (hi > lo) CDBG_CUDA(cudaMemcpyAsync(ht + lo, out.tigs + lo, hi - lo, cudaMemcpyDeviceToHost, e->st));
+                CDBG_CUDA(cudaEventRecord(rev[r], e->st));
+            }
+            CDBG_CUDA(cudaMemcpyAsync(hc, out.closed, out.closed_bytes, cudaMemcpyDeviceToHost, e->st));
+            CDBG_CUDA(cudaEventRecord(rev.back(), e->st));
             bool closed_ok = true;
+            cudaError_t closed_err = cudaSuccess;
             std::thread closed_writer([&] {
+                closed_err = cudaSetDevice(e->device);
+                if (closed_err == cudaSuccess) closed_err = cudaEventSynchronize(rev.back());
+                if (closed_err != cudaSuccess) return;
                 if (cf)
                     closed_ok = !out.closed_bytes || std::fwrite(hc, 1, out.closed_bytes, cf) == out.closed_bytes;
                 else
                     e->h_closed.insert(e->h_closed.end(), hc, hc + out.closed_bytes);
             });
             try {
-                store.append(ht, boff.data(), T);
+                for (size_t r = 0; r + 1 < cut.size(); ++r) {
+                    CDBG_CUDA(cudaEventSynchronize(rev[r]));
+                    store.append_range(ht, boff.data(), cut[r], cut[r + 1], T);
+                }
             } catch (...) {
                 closed_writer.join();
                 throw;
             }
             closed_writer.join();
+            CDBG_CUDA(closed_err);
             if (!closed_ok) throw std::runtime_error(std::string("short write to ") + a->closed_path);
             s->ms_files += std::chrono::duration<double, std::milli>(clk::now() - tf).count();
             s->routed += out.n_routed;

@@ -67,7 +67,7 @@ struct cdbg_engine {
     // device processes the other)
     pinned_buffer h_bk[2];
     std::vector<uint8_t> h_closed;  // cdbg_gpu_stitch_seed: closed unitigs kept in memory
-    std::vector<uint64_t> h_rec_off;  // cdbg_gpu_stitch_seed: record offsets, reused between calls
+    pinned_buffer h_rec_off;  // cdbg_gpu_stitch_seed: record offsets, reused between calls
     std::vector<std::vector<uint64_t>> h_rec_parts;
     // mapped pinned page for the small reads the host waits on (counts, flags,
     // histograms): written by a kernel, so they never queue behind the output

@@ -34,6 +34,14 @@ namespace io {
 namespace {
 inline bool is_space(char c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
 
+// A compression output buffer per thread, kept between frames (a fresh
+// multi-MB buffer per frame costs its page faults every time).
+std::vector<char>& lz4_scratch(size_t n) {
+    thread_local std::vector<char> buf;
+    if (buf.size() < n) buf.resize(n);
+    return buf;
+}
+
 template <typename F>
 void parallel_for(size_t n, uint32_t threads, F&& f) {
     if (threads <= 1 || n <= 1) {
@@ -406,9 +414,8 @@ void bucket_file_set::append_frames_range(uint8_t const* raw, uint64_t const* bo
         if (a == e) return;
         if (e - a > (uint64_t)LZ4_MAX_INPUT) throw std::runtime_error("bucket slice too large for one LZ4 frame");
         std::FILE* f = (std::FILE*)m_files[b];
-        std::vector<char> out;
         const int src = (int)(e - a);
-        out.resize((size_t)LZ4_compressBound(src));
+        std::vector<char>& out = lz4_scratch((size_t)LZ4_compressBound(src));
         int c = LZ4_compress_default((char const*)raw + a, out.data(), src, (int)out.size());
         if (c <= 0) throw std::runtime_error("LZ4_compress_default failed on " + path((uint32_t)b));
         uint32_t u32 = (uint32_t)src, c32 = (uint32_t)c;
@@ -468,7 +475,7 @@ void round0_store::flush(uint32_t b, uint8_t const* data, uint64_t n, uint64_t& 
         if (!f) throw std::runtime_error("cannot open stitch round file: " + path(b) + ": " + std::strerror(errno));
         m_files[b] = f;
     }
-    std::vector<char> out((size_t)LZ4_compressBound((int)n));
+    std::vector<char>& out = lz4_scratch((size_t)LZ4_compressBound((int)n));
     const int c = LZ4_compress_default((char const*)data, out.data(), (int)n, (int)out.size());
     if (c <= 0) throw std::runtime_error("LZ4_compress_default failed on " + path(b));
     const uint32_t u32 = (uint32_t)n, c32 = (uint32_t)c;
@@ -479,9 +486,14 @@ void round0_store::flush(uint32_t b, uint8_t const* data, uint64_t n, uint64_t& 
 }
 
 void round0_store::append(uint8_t const* tigs, uint64_t const* boff, uint32_t threads) {
-    std::vector<uint64_t> comp(m_B, 0);
-    parallel_for(m_B, threads, [&](size_t bi) {
-        const uint32_t b = (uint32_t)bi;
+    append_range(tigs, boff, 0, m_B, threads);
+}
+
+void round0_store::append_range(uint8_t const* tigs, uint64_t const* boff, uint32_t b_lo, uint32_t b_hi,
+                                uint32_t threads) {
+    std::vector<uint64_t> comp(b_hi - b_lo, 0);
+    parallel_for(b_hi - b_lo, threads, [&](size_t bi) {
+        const uint32_t b = b_lo + (uint32_t)bi;
         const uint64_t a = boff[b], e = boff[b + 1];
         if (a == e) return;
         std::vector<uint8_t>& pend = m_pend[b];
@@ -497,10 +509,10 @@ void round0_store::append(uint8_t const* tigs, uint64_t const* boff, uint32_t th
             // emit() appends one tig, then flushes once the batch holds a frame
             if (pend.size() + (pos - seg) >= ROUND_FRAME) {
                 if (pend.empty()) {
-                    flush(b, tigs + seg, pos - seg, comp[b]);
+                    flush(b, tigs + seg, pos - seg, comp[bi]);
                 } else {
                     pend.insert(pend.end(), tigs + seg, tigs + pos);
-                    flush(b, pend.data(), pend.size(), comp[b]);
+                    flush(b, pend.data(), pend.size(), comp[bi]);
                     pend.clear();
                 }
                 seg = pos;
@@ -508,7 +520,7 @@ void round0_store::append(uint8_t const* tigs, uint64_t const* boff, uint32_t th
         }
         pend.insert(pend.end(), tigs + seg, tigs + e);
     });
-    m_raw += boff[m_B] - boff[0];
+    m_raw += boff[b_hi] - boff[b_lo];
     for (uint64_t c : comp) m_comp += c;
 }
 
@@ -560,9 +572,9 @@ bool plausible_start(uint8_t const* d, uint64_t n, uint64_t p) {
 }
 }  // namespace
 
-void frag_record_offsets(uint8_t const* d, uint64_t n, std::vector<uint64_t>& off, uint32_t threads,
-                         std::vector<std::vector<uint64_t>>* scratch) {
-    off.clear();
+uint64_t frag_record_offsets(uint8_t const* d, uint64_t n, uint32_t threads,
+                             std::function<uint64_t*(uint64_t)> const& alloc,
+                             std::vector<std::vector<uint64_t>>* scratch) {
     const uint64_t P = std::max<uint64_t>(1, std::min<uint64_t>(threads, n >> 20));
     // Part t covers [c(t), c(t + 1)).  Part 0 starts at a record; every other
     // part guesses its first record (plausible_start) and follows the chain
@@ -612,9 +624,14 @@ void frag_record_offsets(uint8_t const* d, uint64_t n, std::vector<uint64_t>& of
         }
         pt.end = pos;
     });
-    size_t guess = 1;
-    for (auto const& pt : parts) guess += pt.recs.size();
-    off.reserve(guess);
+    // The merge plan: per part, the records walked here (where the part's own
+    // chain was not yet joined) and then the part's chain from the join on.
+    struct seg {
+        std::vector<uint64_t> const* v;
+        size_t a, b;
+    };
+    std::vector<std::vector<uint64_t>> walked(P);
+    std::vector<seg> segs;
     uint64_t e = 0;  // the next true record start
     for (uint64_t t = 0; t < P; ++t) {
         const uint64_t lim = c(t + 1);
@@ -622,23 +639,44 @@ void frag_record_offsets(uint8_t const* d, uint64_t n, std::vector<uint64_t>& of
         part const& pt = parts[t];
         size_t j = 0;
         if (pt.found) j = std::lower_bound(pt.recs.begin(), pt.recs.end(), e) - pt.recs.begin();
+        bool joined = false;
         while (e < lim) {
             while (pt.found && j < pt.recs.size() && pt.recs[j] < e) ++j;
             if (pt.found && j < pt.recs.size() && pt.recs[j] == e) {
                 // joined: the rest of this part's chain is true
-                off.insert(off.end(), pt.recs.begin() + j, pt.recs.end());
                 if (pt.broken) throw std::runtime_error("truncated fragment record");
-                e = pt.end;
+                joined = true;
                 break;
             }
             const uint64_t q = frag_record_end(d, n, e);
             if (!q) throw std::runtime_error("truncated fragment record");
-            off.push_back(e);
+            walked[t].push_back(e);
             e = q;
+        }
+        if (!walked[t].empty()) segs.push_back({&walked[t], 0, walked[t].size()});
+        if (joined) {
+            segs.push_back({&pt.recs, j, pt.recs.size()});
+            e = pt.end;
         }
     }
     if (e != n) throw std::runtime_error("truncated fragment record");
-    off.push_back(n);
+    std::vector<uint64_t> at(segs.size() + 1, 0);
+    for (size_t i = 0; i < segs.size(); ++i) at[i + 1] = at[i] + (segs[i].b - segs[i].a);
+    const uint64_t nrec = at.back();
+    uint64_t* out = alloc(nrec + 1);
+    parallel_for(segs.size(), threads, [&](size_t i) {
+        if (segs[i].b > segs[i].a)
+            std::memcpy(out + at[i], segs[i].v->data() + segs[i].a, 8 * (segs[i].b - segs[i].a));
+    });
+    out[nrec] = n;
+    return nrec;
+}
+
+void frag_record_offsets(uint8_t const* d, uint64_t n, std::vector<uint64_t>& off, uint32_t threads) {
+    frag_record_offsets(d, n, threads, [&](uint64_t m) {
+        off.resize(m);
+        return off.data();
+    });
 }
 
 void read_bucket_files(std::string const& dir, uint32_t B, uint32_t threads,

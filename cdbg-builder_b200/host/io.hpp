@@ -126,6 +126,8 @@ public:
     // Successive calls append in order (the tigs of one call follow those of
     // the calls before in every bucket).
     void append(uint8_t const* tigs, uint64_t const* boff, uint32_t threads);
+    // The same for buckets [b_lo, b_hi) only (tigs + boff[b] is bucket b's).
+    void append_range(uint8_t const* tigs, uint64_t const* boff, uint32_t b_lo, uint32_t b_hi, uint32_t threads);
     void finish(uint32_t threads);
     uint64_t raw_bytes() const { return m_raw; }
     uint64_t comp_bytes() const { return m_comp; }
@@ -139,12 +141,16 @@ private:
     uint64_t m_raw = 0, m_comp = 0;
 };
 
-// Byte offsets of the records of a frag_unitigs.bin buffer (n + 1 entries,
-// the last = n_bytes), found by `threads` threads; throws at a record that
-// runs past the end.  `scratch` (optional) holds the threads' lists between
-// calls, so their memory is reused.
-void frag_record_offsets(uint8_t const* data, uint64_t n_bytes, std::vector<uint64_t>& off, uint32_t threads,
-                         std::vector<std::vector<uint64_t>>* scratch = nullptr);
+// Byte offsets of the records of a frag_unitigs.bin buffer, found by
+// `threads` threads: written to alloc(records + 1) (the last = n_bytes); the
+// number of records is returned.  Throws at a record that runs past the end.
+// `scratch` (optional) holds the threads' lists between calls, so their
+// memory is reused.
+uint64_t frag_record_offsets(uint8_t const* data, uint64_t n_bytes, uint32_t threads,
+                             std::function<uint64_t*(uint64_t)> const& alloc,
+                             std::vector<std::vector<uint64_t>>* scratch = nullptr);
+// The same into a vector.
+void frag_record_offsets(uint8_t const* data, uint64_t n_bytes, std::vector<uint64_t>& off, uint32_t threads);
 
 // Decompressed contents of bucket files 0..B-1 back to back (buffer from
 // `alloc`), with `chunk_off` = byte offsets of frame starts (records never
