@@ -78,7 +78,9 @@ class BuildFilesArgs(ctypes.Structure):
     _fields_ = [("files", ctypes.POINTER(ctypes.c_char_p)), ("num_files", ctypes.c_uint32),
                 ("k", ctypes.c_uint32), ("m", ctypes.c_uint32), ("num_buckets", ctypes.c_uint32),
                 ("host_threads", ctypes.c_uint32), ("batch_occ", ctypes.c_uint64),
-                ("frag_path", ctypes.c_char_p), ("color_sets_path", ctypes.c_char_p)]
+                ("frag_path", ctypes.c_char_p), ("color_sets_path", ctypes.c_char_p),
+                ("stitch_dir", ctypes.c_char_p), ("stitch_closed_path", ctypes.c_char_p),
+                ("stitch_buckets", ctypes.c_uint32), ("stitch_kmer_bits", ctypes.c_uint32)]
 
 
 class BuildResult(ctypes.Structure):
@@ -92,7 +94,8 @@ class BuildResult(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
                 ("n_bases", ctypes.c_uint64),
                 ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
-                ("ms_total", ctypes.c_double), ("ms_outputs", ctypes.c_double)]
+                ("ms_total", ctypes.c_double), ("ms_outputs", ctypes.c_double), ("ms_seed", ctypes.c_double),
+                ("seed_routed", ctypes.c_uint64), ("seed_closed_unitigs", ctypes.c_uint64)]
 
 
 class SeedArgs(ctypes.Structure):
@@ -462,13 +465,15 @@ class Engine:
         return buf.raw[:nbytes]
 
     def build_files(self, files, k, num_buckets, frag_path=None, color_sets_path=None, m=0, host_threads=0,
-                    batch_occ=0):
+                    batch_occ=0, stitch_dir=None, stitch_closed_path=None, stitch_buckets=0, stitch_kmer_bits=0):
         """cdbg_gpu_build_files: files in, frag_unitigs.bin / .color_sets out
-        (or, with no paths, outputs in host memory)."""
+        (or, with no paths, outputs in host memory); with stitch_dir, also the
+        stitch's round-0 files from the fragments in HBM."""
         arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
-        a = BuildFilesArgs(arr, len(files), k, m, num_buckets, host_threads, batch_occ,
-                           frag_path.encode() if frag_path else None,
-                           color_sets_path.encode() if color_sets_path else None)
+        enc = lambda x: x.encode() if x else None  # noqa: E731
+        a = BuildFilesArgs(arr, len(files), k, m, num_buckets, host_threads, batch_occ, enc(frag_path),
+                           enc(color_sets_path), enc(stitch_dir), enc(stitch_closed_path), stitch_buckets,
+                           stitch_kmer_bits)
         r = BuildResult()
         _check(lib().cdbg_gpu_build_files(self._h, ctypes.byref(a), ctypes.byref(r)))
         return r

@@ -1299,6 +1299,7 @@ int build_core(cdbg_engine* e, const cdbg_build_params* p, phase1_fn const& phas
         pp.union_bitmaps = e->tune.union_lists == 0;
         pp.group_bytes = e->tune.table_group_mb ? (uint64_t)e->tune.table_group_mb << 20 : ~0ull;
         pp.to_host = false;  // outputs accumulate in HBM
+        pp.keep_frag_offsets = e->keep_frag_offsets && !p->outputs_to_host;
         e->frag_sink.streamed = 0;
         if (!p->outputs_to_host && e->frag_sink.fn && e->h_frag.p && e->h_frag.cap) {
             // the caller writes each batch's fragments out while later batches
@@ -1502,6 +1503,10 @@ struct frag_file_writer {
 };
 }  // namespace
 
+static void seed_pass(cdbg_engine* e, uint8_t const* dF, uint64_t const* dOff, uint64_t nc, cdbg::seed_config const& c,
+                      cdbg::io::round0_store& store, std::FILE* cf, char const* closed_path, uint32_t T,
+                      cudaEvent_t* ev, cdbg_seed_stats* s);
+
 int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_build_result* r) {
     if (!e || !a || !r || (!a->files && a->num_files)) {
         g_last_error = "null argument";
@@ -1518,7 +1523,11 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
         p.num_buckets = a->num_buckets;
         p.num_colors = a->num_files;
         p.batch_occ = a->batch_occ;
-        p.outputs_to_host = a->frag_path || a->color_sets_path ? 0 : 1;
+        const bool seed = a->stitch_dir != nullptr;
+        if (a->stitch_kmer_bits != 0 && a->stitch_kmer_bits != 64 && a->stitch_kmer_bits != 128)
+            throw std::runtime_error("stitch_kmer_bits must be 0, 64 or 128");
+        // the round-0 seed reads the fragments where phase 2 leaves them, in HBM
+        p.outputs_to_host = a->frag_path || a->color_sets_path || seed ? 0 : 1;
         const uint32_t m = p.m ? p.m : best_m(p.k);
         uint64_t inb = 0;
         auto ph1 = [&](cdbg::run_table& rt, cdbg::super_list& sl, uint64_t* h2d) {
@@ -1532,11 +1541,13 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             e->frag_sink.fn = &frag_file_writer::hook;
             e->frag_sink.ctx = fw.get();
         }
+        e->keep_frag_offsets = seed;
         struct unhook {
             cdbg_engine* e;
             ~unhook() {
                 e->frag_sink.fn = nullptr;
                 e->frag_sink.ctx = nullptr;
+                e->keep_frag_offsets = false;
             }
         } unhook_{e};
         bool redo = false;
@@ -1568,18 +1579,30 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             if (a->color_sets_path)
                 cdbg::ef_encode(r->class_offsets, r->n_color_sets, r->class_bits, e->A, e->st, ef);
             void* hf_before = e->h_frag.p;
+            // the fragments come to the host unless only the seed reads them
+            const bool frag_out = !seed || a->frag_path;
             // (a buffer that took every fragment stays where the writer reads it)
-            uint8_t* hf = fw && streamed == r->frag_nbytes && r->frag_nbytes
+            uint8_t* hf = !frag_out ? nullptr
+                          : fw && streamed == r->frag_nbytes && r->frag_nbytes
                               ? (uint8_t*)e->h_frag.p
                               : (uint8_t*)e->h_frag.ensure(r->frag_nbytes + 8);
             // bytes of hf already holding the fragments (the streamed prefix,
             // unless the buffer just moved)
             const uint64_t have = (void*)hf == hf_before ? streamed : 0;
             uint64_t* hw = (uint64_t*)e->h_words.ensure(8 * nwords + 8);
-            uint64_t* hl = (uint64_t*)e->h_offsets.ensure(8 * (ef.low_words + ef.high_words) + 16);
-            if (r->frag_nbytes > have)
+            uint64_t* hl = (uint64_t*)e->h_offsets.ensure(
+                a->color_sets_path ? 8 * (ef.low_words + ef.high_words) + 16 : 8 * r->n_color_sets + 8);
+            if (frag_out && r->frag_nbytes > have)
                 CDBG_CUDA(cudaMemcpyAsync(hf + have, r->frag_bytes + have, r->frag_nbytes - have,
                                           cudaMemcpyDeviceToHost, e->st));
+            if (!a->color_sets_path) {
+                // no .color_sets file: the class words and offsets come back
+                if (nwords)
+                    CDBG_CUDA(cudaMemcpyAsync(hw, r->class_words, 8 * nwords, cudaMemcpyDeviceToHost, e->st));
+                if (r->n_color_sets)
+                    CDBG_CUDA(cudaMemcpyAsync(hl, r->class_offsets, 8 * r->n_color_sets, cudaMemcpyDeviceToHost,
+                                              e->st));
+            }
             if (a->color_sets_path) {
                 if (nwords)
                     CDBG_CUDA(cudaMemcpyAsync(hw, r->class_words, 8 * nwords, cudaMemcpyDeviceToHost, e->st));
@@ -1590,7 +1613,9 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
                                               cudaMemcpyDeviceToHost, e->st));
             }
             CDBG_CUDA(cudaStreamSynchronize(e->st));
-            r->d2h_bytes = r->frag_nbytes + (a->color_sets_path ? 8 * (nwords + ef.low_words + ef.high_words) : 0);
+            r->d2h_bytes = (frag_out ? r->frag_nbytes : 0) +
+                           (a->color_sets_path ? 8 * (nwords + ef.low_words + ef.high_words)
+                                               : 8 * (nwords + r->n_color_sets));
             std::thread cs_writer;
             std::exception_ptr cs_err;
             if (a->color_sets_path)
@@ -1616,8 +1641,47 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
             if (cs_err) std::rethrow_exception(cs_err);
             r->frag_bytes = hf;
             r->class_words = hw;
-            r->class_offsets = nullptr;  // in the file, Elias-Fano coded
+            r->class_offsets = a->color_sets_path ? nullptr : hl;  // else in the file, Elias-Fano coded
             e->A.reset();
+        }
+        if (seed) {
+            // round 0 of the stitch from the fragments and record offsets
+            // phase 2 left in HBM
+            call_scope scope_(e);
+            CDBG_CUDA(cudaSetDevice(e->device));
+            const auto ts = std::chrono::steady_clock::now();
+            cdbg::seed_config c;
+            c.k = p.k;
+            c.num_buckets = a->stitch_buckets ? a->stitch_buckets : 1024;
+            c.wide = a->stitch_kmer_bits ? a->stitch_kmer_bits == 128 : p.k > 31;
+            if (c.k > (c.wide ? 63u : 32u)) throw std::runtime_error("k out of range for the k-mer width");
+            const uint64_t n = r->n_fragments;
+            if (e->p2.frag_off.n != n || (n && !e->p2.frag_off.p))
+                throw std::runtime_error("the build kept no fragment record offsets");
+            uint64_t* dOff = n ? e->p2.frag_off.p : e->A.alloc<uint64_t>(1);  // room for n + 1 entries
+            const uint64_t end = r->frag_nbytes;
+            CDBG_CUDA(cudaMemcpyAsync(dOff + n, &end, 8, cudaMemcpyHostToDevice, e->st));
+            cdbg::io::round0_store store(a->stitch_dir, c.num_buckets);
+            const std::string cp = a->stitch_closed_path ? std::string(a->stitch_closed_path)
+                                                         : std::string(a->stitch_dir) + "/stitch_r0_closed.bin";
+            std::FILE* cf = std::fopen(cp.c_str(), "wb");
+            if (!cf) throw std::runtime_error("cannot open " + cp);
+            std::unique_ptr<std::FILE, int (*)(std::FILE*)> cf_guard(cf, [](std::FILE* f) { return std::fclose(f); });
+            cudaEvent_t ev[2];
+            CDBG_CUDA(cudaEventCreate(&ev[0]));
+            CDBG_CUDA(cudaEventCreate(&ev[1]));
+            std::unique_ptr<cudaEvent_t, void (*)(cudaEvent_t*)> ev_guard(ev, [](cudaEvent_t* v) {
+                cudaEventDestroy(v[0]);
+                cudaEventDestroy(v[1]);
+            });
+            cdbg_seed_stats ss{};
+            seed_pass(e, e->p2.frag.p, dOff, n, c, store, cf, cp.c_str(), th, ev, &ss);
+            store.finish(th);
+            if (std::fclose(cf_guard.release()) != 0) throw std::runtime_error("close failed on " + cp);
+            e->A.reset();
+            r->seed_routed = ss.routed;
+            r->seed_closed_unitigs = ss.closed_unitigs;
+            r->ms_seed = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();
         }
         (void)inb;
         const auto t_end = std::chrono::steady_clock::now();
@@ -1628,6 +1692,79 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
         if (e) e->A.reset();
         return fail(ex);
     }
+}
+
+// One device pass of the stitch's round-0 seed over n records at dF / dOff
+// (device): the tigs come back in bucket ranges of ~1/16 of their bytes and
+// host threads compress and write one range while the next still copies; the
+// closed unitigs follow and go to cf (or to e->h_closed) on their own thread.
+static void seed_pass(cdbg_engine* e, uint8_t const* dF, uint64_t const* dOff, uint64_t nc, cdbg::seed_config const& c,
+                      cdbg::io::round0_store& store, std::FILE* cf, char const* closed_path, uint32_t T,
+                      cudaEvent_t* ev, cdbg_seed_stats* s) {
+    std::vector<uint64_t> boff(c.num_buckets + 1);
+    CDBG_CUDA(cudaEventRecord(ev[0], e->st));
+    cdbg::seed_device_out out;
+    cdbg::seed_fragments(dF, dOff, nc, c, e->A, e->st, e->d_err, out);
+    CDBG_CUDA(cudaEventRecord(ev[1], e->st));
+    CDBG_CUDA(cudaMemcpyAsync(boff.data(), out.bucket_off, 8 * boff.size(), cudaMemcpyDeviceToHost, e->st));
+    CDBG_CUDA(cudaStreamSynchronize(e->st));
+    float ms = 0;
+    CDBG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    s->ms_device += ms;
+    const auto tf = std::chrono::steady_clock::now();
+    // the tigs come back in bucket ranges of ~1/16 of their bytes: host
+    // threads compress and write one range while the next still copies;
+    // the closed unitigs follow and go out on their own thread
+    uint8_t* ht = (uint8_t*)e->h_tigs.ensure(out.tig_bytes + 16);
+    uint8_t* hc = (uint8_t*)e->h_unitigs.ensure(out.closed_bytes + 16);
+    std::vector<uint32_t> cut{0};
+    const uint64_t per = std::max<uint64_t>(64ull << 20, out.tig_bytes / 16);
+    for (uint32_t b = 1; b < c.num_buckets; ++b)
+        if (boff[b] - boff[cut.back()] >= per) cut.push_back(b);
+    cut.push_back(c.num_buckets);
+    std::vector<cudaEvent_t> rev(cut.size());  // ranges, then the closed unitigs
+    for (auto& x : rev) CDBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    std::unique_ptr<std::vector<cudaEvent_t>, void (*)(std::vector<cudaEvent_t>*)> rev_guard(
+        &rev, [](std::vector<cudaEvent_t>* v) {
+            for (auto x : *v) cudaEventDestroy(x);
+        });
+    for (size_t r = 0; r + 1 < cut.size(); ++r) {
+        const uint64_t lo = boff[cut[r]], hi = boff[cut[r + 1]];
+        if (hi > lo) CDBG_CUDA(cudaMemcpyAsync(ht + lo, out.tigs + lo, hi - lo, cudaMemcpyDeviceToHost, e->st));
+        CDBG_CUDA(cudaEventRecord(rev[r], e->st));
+    }
+    CDBG_CUDA(cudaMemcpyAsync(hc, out.closed, out.closed_bytes, cudaMemcpyDeviceToHost, e->st));
+    CDBG_CUDA(cudaEventRecord(rev.back(), e->st));
+    bool closed_ok = true;
+    cudaError_t closed_err = cudaSuccess;
+    std::thread closed_writer([&] {
+        closed_err = cudaSetDevice(e->device);
+        if (closed_err == cudaSuccess) closed_err = cudaEventSynchronize(rev.back());
+        if (closed_err != cudaSuccess) return;
+        if (cf)
+            closed_ok = !out.closed_bytes || std::fwrite(hc, 1, out.closed_bytes, cf) == out.closed_bytes;
+        else
+            e->h_closed.insert(e->h_closed.end(), hc, hc + out.closed_bytes);
+    });
+    try {
+        for (size_t r = 0; r + 1 < cut.size(); ++r) {
+            CDBG_CUDA(cudaEventSynchronize(rev[r]));
+            store.append_range(ht, boff.data(), cut[r], cut[r + 1], T);
+        }
+    } catch (...) {
+        closed_writer.join();
+        throw;
+    }
+    closed_writer.join();
+    CDBG_CUDA(closed_err);
+    if (!closed_ok) throw std::runtime_error(std::string("short write to ") + closed_path);
+    s->ms_files += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tf).count();
+    s->routed += out.n_routed;
+    s->closed_fragments += out.n_closed;
+    s->closed_unitigs += out.n_pieces;
+    s->routed_frag_bytes += out.routed_record_bytes;
+    s->closed_nbytes += out.closed_bytes;
+    ++s->n_passes;
 }
 
 int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stats* s) {
@@ -1708,7 +1845,7 @@ int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stat
             cudaEventDestroy(v[0]);
             cudaEventDestroy(v[1]);
         });
-        std::vector<uint64_t> loff, boff(c.num_buckets + 1);
+        std::vector<uint64_t> loff;
         for (uint64_t i0 = 0; i0 < n;) {
             uint64_t i1 = i0 + 1;
             while (i1 < n && off[i1 + 1] - off[i0] <= chunk) ++i1;
@@ -1728,68 +1865,7 @@ int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stat
                 for (uint64_t i = 0; i <= nc; ++i) loff[i] = off[i0 + i] - off[i0];
                 CDBG_CUDA(cudaMemcpyAsync(dOff, loff.data(), 8 * (nc + 1), cudaMemcpyHostToDevice, e->st));
             }
-            CDBG_CUDA(cudaEventRecord(ev[0], e->st));
-            cdbg::seed_device_out out;
-            cdbg::seed_fragments(dF, dOff, nc, c, e->A, e->st, e->d_err, out);
-            CDBG_CUDA(cudaEventRecord(ev[1], e->st));
-            CDBG_CUDA(cudaMemcpyAsync(boff.data(), out.bucket_off, 8 * boff.size(), cudaMemcpyDeviceToHost, e->st));
-            CDBG_CUDA(cudaStreamSynchronize(e->st));
-            float ms = 0;
-            CDBG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-            s->ms_device += ms;
-            const auto tf = clk::now();
-            // the tigs come back in bucket ranges of ~1/16 of their bytes: host
-            // threads compress and write one range while the next still copies;
-            // the closed unitigs follow and go out on their own thread
-            uint8_t* ht = (uint8_t*)e->h_frag.ensure(out.tig_bytes + 16);
-            uint8_t* hc = (uint8_t*)e->h_words.ensure(out.closed_bytes + 16);
-            std::vector<uint32_t> cut{0};
-            const uint64_t per = std::max<uint64_t>(64ull << 20, out.tig_bytes / 16);
-            for (uint32_t b = 1; b < c.num_buckets; ++b)
-                if (boff[b] - boff[cut.back()] >= per) cut.push_back(b);
-            cut.push_back(c.num_buckets);
-            std::vector<cudaEvent_t> rev(cut.size());  // ranges, then the closed unitigs
-            for (auto& x : rev) CDBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
-            std::unique_ptr<std::vector<cudaEvent_t>, void (*)(std::vector<cudaEvent_t>*)> rev_guard(
-                &rev, [](std::vector<cudaEvent_t>* v) {
-                    for (auto x : *v) cudaEventDestroy(x);
-                });
-            for (size_t r = 0; r + 1 < cut.size(); ++r) {
-                const uint64_t lo = boff[cut[r]], hi = boff[cut[r + 1]];
-                if (hi > lo) CDBG_CUDA(cudaMemcpyAsync(ht + lo, out.tigs + lo, hi - lo, cudaMemcpyDeviceToHost, e->st));
-                CDBG_CUDA(cudaEventRecord(rev[r], e->st));
-            }
-            CDBG_CUDA(cudaMemcpyAsync(hc, out.closed, out.closed_bytes, cudaMemcpyDeviceToHost, e->st));
-            CDBG_CUDA(cudaEventRecord(rev.back(), e->st));
-            bool closed_ok = true;
-            cudaError_t closed_err = cudaSuccess;
-            std::thread closed_writer([&] {
-                closed_err = cudaSetDevice(e->device);
-                if (closed_err == cudaSuccess) closed_err = cudaEventSynchronize(rev.back());
-                if (closed_err != cudaSuccess) return;
-                if (cf)
-                    closed_ok = !out.closed_bytes || std::fwrite(hc, 1, out.closed_bytes, cf) == out.closed_bytes;
-                else
-                    e->h_closed.insert(e->h_closed.end(), hc, hc + out.closed_bytes);
-            });
-            try {
-                for (size_t r = 0; r + 1 < cut.size(); ++r) {
-                    CDBG_CUDA(cudaEventSynchronize(rev[r]));
-                    store.append_range(ht, boff.data(), cut[r], cut[r + 1], T);
-                }
-            } catch (...) {
-                closed_writer.join();
-                throw;
-            }
-            closed_writer.join();
-            CDBG_CUDA(closed_err);
-            if (!closed_ok) throw std::runtime_error(std::string("short write to ") + a->closed_path);
-            s->ms_files += std::chrono::duration<double, std::milli>(clk::now() - tf).count();
-            s->routed += out.n_routed;
-            s->closed_fragments += out.n_closed;
-            s->closed_unitigs += out.n_pieces;
-            s->routed_frag_bytes += out.routed_record_bytes;
-            s->closed_nbytes += out.closed_bytes;
+            seed_pass(e, dF, dOff, nc, c, store, cf, a->closed_path, T, ev, s);
             ++s->n_passes;
             e->A.release(mk);
             i0 = i1;

@@ -67,6 +67,8 @@ struct cdbg_engine {
     // device processes the other)
     pinned_buffer h_bk[2];
     std::vector<uint8_t> h_closed;  // cdbg_gpu_stitch_seed: closed unitigs kept in memory
+    pinned_buffer h_tigs, h_unitigs;  // stitch seed: tigs and closed unitigs on their way to the files
+    bool keep_frag_offsets = false;   // the next build keeps its fragment record offsets in p2.frag_off
     pinned_buffer h_rec_off;  // cdbg_gpu_stitch_seed: record offsets, reused between calls
     std::vector<std::vector<uint64_t>> h_rec_parts;
     // mapped pinned page for the small reads the host waits on (counts, flags,

@@ -2373,7 +2373,7 @@ template <typename K>
 void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, uint32_t b0, uint32_t b1,
                std::vector<uint64_t> const& bocc, dev_arena& A, cudaStream_t st, uint32_t* d_err,
                class_dict& dict, phase2_result& out, std::vector<uint64_t> const& hbstart, uint64_t* d_rhash,
-               dvec<uint8_t>& dfrag) {
+               dvec<uint8_t>& dfrag, dvec<uint64_t>& dfoff) {
     const uint32_t k = p.k, C = p.num_colors;
     const uint64_t R0 = hbstart[b0], R1 = hbstart[b1];
     const uint64_t nrec = R1 - R0;
@@ -2922,6 +2922,11 @@ void run_batch(record_set const& rs, rec_view const& R, phase2_params const& p, 
         dfrag.reserve(dfrag.n + fbytes + 8, st);
         CDBG_CUDA(cudaMemcpyAsync(dfrag.p + dfrag.n, fb, fbytes, cudaMemcpyDeviceToDevice, st));
         dfrag.n += fbytes;
+        if (p.keep_frag_offsets && nfr) {
+            dfoff.reserve(dfoff.n + nfr + 1, st);
+            add_offsets(foff, nfr, old_n, dfoff.p + dfoff.n, st);
+            dfoff.n += nfr;
+        }
         if (p.copy_st && p.frag_host && out.frag_host_copied == old_n && dfrag.n <= p.frag_host_cap && fbytes) {
             // this batch's fragments go to the host while the next batch runs
             CDBG_CUDA(cudaEventRecord(p.copy_ev, st));
@@ -3013,6 +3018,7 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
     }
     dvec<uint8_t>& dfrag = S.frag;
     dfrag.n = 0;
+    S.frag_off.n = 0;
     uint32_t b = 0;
     while (b < B) {
         const uint32_t s = b;
@@ -3025,7 +3031,7 @@ void run_all(record_set const& rs, phase2_params const& p, dev_arena& A, cudaStr
             recs += rb;
             ++b;
         }
-        run_batch<K>(rs, R, p, s, b, bocc, A, st, d_err, dict, out, hbstart, rhash, dfrag);
+        run_batch<K>(rs, R, p, s, b, bocc, A, st, d_err, dict, out, hbstart, rhash, dfrag, S.frag_off);
     }
     // outputs
     S.n = dict.n;

@@ -22,13 +22,14 @@ struct phase2_state {
     dvec<uint64_t> slot_hash;  // open-addressing table hash -> class
     dvec<uint32_t> slot_cid;
     dvec<uint8_t> frag;        // frag spill bytes (device-resident builds)
+    dvec<uint64_t> frag_off;   // their record offsets (phase2_params::keep_frag_offsets)
     // dictionary size, kept so that a later call can continue it
     uint64_t n = 0, nbits = 0, total_integers = 0, mask = 0;
     // Order later frees on `st` (after a stream switch).
     void set_stream(cudaStream_t st) {
         cls_hash.st_last = bit_off.st_last = words.st_last = slot_hash.st_last = st;
         slot_cid.st_last = st;
-        frag.st_last = st;
+        frag.st_last = frag_off.st_last = st;
     }
     void release() {
         cls_hash.release();
@@ -37,10 +38,11 @@ struct phase2_state {
         slot_hash.release();
         slot_cid.release();
         frag.release();
+        frag_off.release();
     }
     size_t bytes() const {
         return cls_hash.bytes() + bit_off.bytes() + words.bytes() + slot_hash.bytes() + slot_cid.bytes() +
-               frag.bytes();
+               frag.bytes() + frag_off.bytes();
     }
 };
 
@@ -106,6 +108,10 @@ struct phase2_params {
     // later batches run)
     void (*on_frag)(void* ctx, uint64_t off, uint64_t n) = nullptr;
     void* on_frag_ctx = nullptr;
+    // Device-resident mode: also keep the byte offset of every fragment
+    // record in phase2_state::frag_off (for a device pass over the records,
+    // such as the stitch's round-0 seed).
+    bool keep_frag_offsets = false;
     // likewise the class dictionary's completed bit-vector words and class
     // offsets (capacities in entries)
     uint64_t* words_host = nullptr;

@@ -265,6 +265,9 @@ typedef struct cdbg_build_result {
     double ms_phase1, ms_phase2, ms_total; /* device time (CUDA events) */
     double ms_outputs;           /* cdbg_gpu_build_files: wall time after phase 2
                                     (output copies and file writes left) */
+    double ms_seed;              /* cdbg_gpu_build_files with stitch_dir: wall time
+                                    of the round-0 seed (included in ms_outputs) */
+    uint64_t seed_routed, seed_closed_unitigs;
 } cdbg_build_result;
 
 int cdbg_gpu_build(cdbg_engine* e, const cdbg_seq_batch* b, const cdbg_build_params* p,
@@ -288,6 +291,15 @@ typedef struct cdbg_build_files_args {
     uint64_t batch_occ;            /* 0 = auto */
     const char* frag_path;         /* may be NULL */
     const char* color_sets_path;   /* may be NULL */
+    /* Round 0 of the stitch from the fragments while they are in HBM: what
+     * cdbg_gpu_stitch_seed writes from a frag file, without the file.  With
+     * stitch_dir set, the round-0 files go there and the closed unitigs to
+     * stitch_closed_path (NULL: stitch_dir/stitch_r0_closed.bin); frag_path may
+     * then be NULL (no frag file, and no fragments in the result). */
+    const char* stitch_dir;
+    const char* stitch_closed_path;
+    uint32_t stitch_buckets;       /* round-store buckets; 0 = 1024 */
+    uint32_t stitch_kmer_bits;     /* as cdbg_seed_args.kmer_bits */
 } cdbg_build_files_args;
 
 int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_build_result* r);

@@ -143,3 +143,35 @@ def test_gpu_seed_then_reference_rounds_equal_reference_build(engine, tmp_path, 
     run_ref([r34, frag_path, out + ".classes", "4", str(k), "1", out, out + "_tmp", closed])
     for ext in (".fa", ".color_sets", ".metadata.txt", ".u2c"):
         assert open(out + ext, "rb").read() == open(ref_out + ext, "rb").read(), ext
+
+
+@pytest.mark.parametrize("k", [31, 63])
+def test_build_files_seeds_round0_from_hbm(engine, tmp_path, k):
+    """cdbg_gpu_build_files with stitch_dir: round 0 seeded from the fragments
+    in HBM equals the reference's seed of the frag file the same call writes,
+    and the same without writing the frag file at all."""
+    from cdbg_gpu import formats, synth
+    extra = dict(tandem_frac=0.02, repeat_pool=3, repeat_min=300, repeat_max=800) if k > 31 else {}
+    p = synth.make_params(seed=70 + k, len_min=50000, len_max=90000, div_min=0.002, div_max=0.02, indels=5,
+                          contigs_min=1, contigs_max=4, lowcomp_frac=0.05, **extra)
+    lst = synth.write_fasta(p, 12, str(tmp_path / "in"), gzip_level=1)
+    files = [l.strip() for l in open(lst) if l.strip()]
+    fp, cs = str(tmp_path / "frag_unitigs.bin"), str(tmp_path / "out.color_sets")
+    d1 = str(tmp_path / "r1")
+    r = engine.build_files(files, k, 512, frag_path=fp, color_sets_path=cs, stitch_dir=d1, stitch_buckets=64)
+    frag = open(fp, "rb").read()
+    assert len(frag) == r.frag_nbytes and r.seed_routed > 0
+    ref_files, ref_closed = _ref_seed(frag, k, 64, str(tmp_path / "ref"))
+    assert round0_files(d1, 64) == ref_files
+    assert open(os.path.join(d1, "stitch_r0_closed.bin"), "rb").read() == ref_closed
+    # no frag file, no color-set file: the classes come back in host memory
+    d2 = str(tmp_path / "r2")
+    r2 = engine.build_files(files, k, 512, stitch_dir=d2, stitch_buckets=64,
+                            stitch_closed_path=str(tmp_path / "closed2.bin"))
+    assert round0_files(d2, 64) == ref_files
+    assert open(str(tmp_path / "closed2.bin"), "rb").read() == ref_closed
+    assert not r2.frag_bytes and r2.frag_nbytes == r.frag_nbytes
+    from cdbg_gpu import native
+    classes = formats.decode_classes(native.result_class_words(r2), native.result_class_offsets(r2), len(files))
+    _, _, _, ref_classes = formats.read_color_sets(cs)
+    assert classes == ref_classes
