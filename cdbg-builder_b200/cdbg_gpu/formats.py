@@ -28,7 +28,26 @@ def _lz4lib():
         _lz4 = ctypes.CDLL("liblz4.so.1")
         _lz4.LZ4_decompress_safe.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
         _lz4.LZ4_decompress_safe.restype = ctypes.c_int
+        _lz4.LZ4_compressBound.argtypes = [ctypes.c_int]
+        _lz4.LZ4_compressBound.restype = ctypes.c_int
+        _lz4.LZ4_compress_default.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        _lz4.LZ4_compress_default.restype = ctypes.c_int
     return _lz4
+
+
+def write_bucket_raw(path, raw):
+    """A bucket file (bucket_io.hpp:19-40 frames) holding `raw` record bytes
+    in one LZ4 frame, then the end mark."""
+    L = _lz4lib()
+    with open(path, "wb") as f:
+        if raw:
+            cap = L.LZ4_compressBound(len(raw))
+            dst = ctypes.create_string_buffer(cap)
+            c = L.LZ4_compress_default(bytes(raw), dst, len(raw), cap)
+            if c <= 0:
+                raise RuntimeError("LZ4_compress_default failed on " + path)
+            f.write(struct.pack("<II", len(raw), c) + dst.raw[:c])
+        f.write(struct.pack("<I", 0))
 
 
 def read_bucket_raw(path):

@@ -35,7 +35,7 @@ class Phase1Args(ctypes.Structure):
     _fields_ = [("files", ctypes.POINTER(ctypes.c_char_p)), ("num_files", ctypes.c_uint32),
                 ("k", ctypes.c_uint32), ("m", ctypes.c_uint32), ("num_buckets", ctypes.c_uint32),
                 ("tmp_dir", ctypes.c_char_p), ("host_threads", ctypes.c_uint32),
-                ("chunk_bytes", ctypes.c_uint64), ("bucket_unc_bytes", c_u64p)]
+                ("chunk_bytes", ctypes.c_uint64), ("bucket_unc_bytes", c_u64p), ("first_color", ctypes.c_uint32)]
 
 
 class Phase1Stats(ctypes.Structure):
@@ -96,6 +96,11 @@ class BuildResult(ctypes.Structure):
                 ("ms_phase1", ctypes.c_double), ("ms_phase2", ctypes.c_double),
                 ("ms_total", ctypes.c_double), ("ms_outputs", ctypes.c_double), ("ms_seed", ctypes.c_double),
                 ("seed_routed", ctypes.c_uint64), ("seed_closed_unitigs", ctypes.c_uint64)]
+
+
+class MergedRecords(ctypes.Structure):
+    _fields_ = [("bytes", ctypes.c_void_p), ("nbytes", ctypes.c_uint64), ("bucket_off", ctypes.c_void_p),
+                ("handle", ctypes.c_void_p)]
 
 
 class SeedArgs(ctypes.Structure):
@@ -217,6 +222,10 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_void_p), c_u64p,
                                          ctypes.POINTER(ctypes.c_void_p), c_u64p, ctypes.c_void_p]),
     "cdbg_merged_free": (None, [ctypes.c_void_p]),
+    "cdbg_merge_bucket_records": (ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
+                                                 ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, ctypes.c_uint32,
+                                                 ctypes.c_uint32, ctypes.POINTER(MergedRecords)]),
+    "cdbg_merged_records_free": (None, [ctypes.POINTER(MergedRecords)]),
     "cdbg_merge_last_error": (ctypes.c_char_p, []),
 }
 
@@ -434,11 +443,11 @@ class Engine:
                                           path.encode(), ctypes.byref(n)))
         return n.value
 
-    def phase1(self, files, k, num_buckets, tmp_dir, m=0, host_threads=0, chunk_bytes=0):
+    def phase1(self, files, k, num_buckets, tmp_dir, m=0, host_threads=0, chunk_bytes=0, first_color=0):
         arr = (ctypes.c_char_p * len(files))(*[f.encode() for f in files])
         unc = np.zeros(num_buckets, dtype=np.uint64)
         a = Phase1Args(arr, len(files), k, m, num_buckets, tmp_dir.encode(), host_threads,
-                       chunk_bytes, unc.ctypes.data_as(c_u64p))
+                       chunk_bytes, unc.ctypes.data_as(c_u64p), first_color)
         s = Phase1Stats()
         _check(lib().cdbg_gpu_phase1(self._h, ctypes.byref(a), ctypes.byref(s)))
         return s, unc

@@ -1,4 +1,4 @@
-"""Builds split by bucket range across ranks (one GPU per rank).
+"""Builds split across ranks (one GPU per rank).
 
 Phase 2 is bucket-local (the reference's algorithm.md:86-89: a bucket's
 graph, walk and color sets need no other bucket), so a build splits into
@@ -12,7 +12,16 @@ merged there (cdbg_merge_shards): identical sets are recognised by their
 encoded bits, new ones appended in order, and the fragments' ids rewritten.
 The result is byte for byte the single build's.
 
-The gather goes through torch.distributed (NCCL between GPUs, gloo on CPU)."""
+The gather goes through torch.distributed (NCCL between GPUs, gloo on CPU).
+
+Phase 1 can also be split, by input file: rank r reads only its consecutive
+slice of the files (file_range; colors stay global file indices) and runs
+phase 1 on it.  Every rank's bucket records then go to the rank that owns the
+bucket (exchange_bucket_records: one all-to-all of the record bytes in bucket
+order, whose bucket ranges are contiguous), and the owner merges the records
+all ranks made for a bucket into the records one phase 1 over all the files
+makes (merge_bucket_records, cdbg_merge_bucket_records) before its phase 2 of
+the range.  Nothing is read twice and no minimizer is computed twice."""
 import ctypes
 
 import numpy as np
@@ -79,3 +88,118 @@ def gather_merge(shard, rank, world, dst=0, group=None):
     if rank != dst:
         return None
     return merge_shards(got)
+
+
+def file_range(num_files, rank, world):
+    """Input files [lo, hi) that rank `rank` of `world` reads (colors lo..hi-1)."""
+    return num_files * rank // world, num_files * (rank + 1) // world
+
+
+def merge_bucket_records(sources, num_buckets, lo, hi):
+    """sources: [(record bytes, offsets of buckets lo..hi (hi - lo + 1))] of
+    several ranks' phase 1, in file order -> (bytes, offsets) of the records
+    one phase 1 over all their files makes for buckets [lo, hi)."""
+    L = native.lib()
+    n = len(sources)
+    bufs = [np.frombuffer(s[0], dtype=np.uint8) if len(s[0]) else np.zeros(1, dtype=np.uint8) for s in sources]
+    offs = [np.ascontiguousarray(s[1], dtype=np.uint64) for s in sources]
+    for o in offs:
+        if len(o) != hi - lo + 1:
+            raise ValueError("each source needs hi - lo + 1 offsets")
+    vp = ctypes.c_void_p * max(n, 1)
+    m = native.MergedRecords()
+    if L.cdbg_merge_bucket_records(n, vp(*[b.ctypes.data for b in bufs]), vp(*[o.ctypes.data for o in offs]),
+                                   num_buckets, lo, hi, ctypes.byref(m)) != 0:
+        raise RuntimeError(L.cdbg_merge_last_error().decode(errors="replace"))
+    try:
+        data = ctypes.string_at(m.bytes, m.nbytes) if m.nbytes else b""
+        off = np.ctypeslib.as_array(ctypes.cast(m.bucket_off, native.c_u64p), shape=(hi - lo + 1,)).copy()
+        return data, off
+    finally:
+        L.cdbg_merged_records_free(ctypes.byref(m))
+
+
+def exchange_bucket_records(raw, bucket_off, num_buckets, rank, world, group=None, device="cpu"):
+    """raw: this rank's phase-1 records of buckets 0..B-1 back to back,
+    bucket_off: their B + 1 offsets.  Sends every rank the records of its
+    bucket range (shard_range) and returns, for this rank's range, one
+    (bytes, offsets) per source rank, in rank order.  Every rank calls it (two
+    all-to-alls: the offsets, then the bytes; NCCL needs device="cuda")."""
+    import torch
+    import torch.distributed as dist
+    bucket_off = np.asarray(bucket_off, dtype=np.int64)
+    rng = [shard_range(num_buckets, q, world) for q in range(world)]
+    lo, hi = rng[rank]
+    if world == 1:
+        return [(bytes(raw), (bucket_off[lo:hi + 1] - bucket_off[lo]).astype(np.uint64))]
+    # per destination: its buckets' offsets, relative to the start of its bytes
+    off_send = np.concatenate([bucket_off[a:b + 1] - bucket_off[a] for a, b in rng])
+    off_in = [b - a + 1 for a, b in rng]
+    off_out = [hi - lo + 1] * world
+    t_off = torch.empty(sum(off_out), dtype=torch.int64, device=device)
+    dist.all_to_all_single(t_off, torch.from_numpy(off_send).to(device), off_out, off_in, group=group)
+    offs = t_off.cpu().numpy().reshape(world, hi - lo + 1)
+    byte_in = [int(bucket_off[b] - bucket_off[a]) for a, b in rng]
+    byte_out = [int(offs[s][-1]) for s in range(world)]
+    send = torch.from_numpy(np.frombuffer(raw, dtype=np.uint8).copy() if len(raw) else np.zeros(0, np.uint8))
+    t_bytes = torch.empty(sum(byte_out), dtype=torch.uint8, device=device)
+    dist.all_to_all_single(t_bytes, send.to(device), byte_out, byte_in, group=group)
+    got = t_bytes.cpu().numpy().tobytes()
+    out, p = [], 0
+    for s in range(world):
+        out.append((got[p:p + byte_out[s]], offs[s].astype(np.uint64)))
+        p += byte_out[s]
+    return out
+
+
+def read_bucket_dir(d, num_buckets):
+    """This rank's phase-1 bucket files (bucket_<b>.bin in d, a missing file an
+    empty bucket), decompressed: (record bytes of buckets 0..B-1, B + 1 offsets)."""
+    import os
+    from . import formats
+    parts, off = [], np.zeros(num_buckets + 1, dtype=np.uint64)
+    for b in range(num_buckets):
+        p = os.path.join(d, "bucket_%d.bin" % b)
+        raw = formats.read_bucket_raw(p) if os.path.exists(p) else b""
+        parts.append(raw)
+        off[b + 1] = off[b] + len(raw)
+    return b"".join(parts), off
+
+
+def write_bucket_dir(d, lo, data, off):
+    """Bucket files lo.. of merged records (one LZ4 frame each) in d."""
+    import os
+    from . import formats
+    os.makedirs(d, exist_ok=True)
+    for i in range(len(off) - 1):
+        formats.write_bucket_raw(os.path.join(d, "bucket_%d.bin" % (lo + i)), data[int(off[i]):int(off[i + 1])])
+
+
+def shard_from_phase2(frag_path, color_sets_path):
+    """(frag bytes, class words, class bits, class offsets) of a drop-in
+    phase 2's two files."""
+    from . import formats
+    frag = open(frag_path, "rb").read()
+    _, words, offs, _ = formats.read_color_sets(color_sets_path, decode=False)
+    bits = int(np.fromfile(color_sets_path, dtype=np.uint64, count=1, offset=12)[0])
+    return frag, np.asarray(words, dtype=np.uint64), bits, np.asarray(offs, dtype=np.uint64)
+
+
+def build_rank_by_files(engine, files, k, num_buckets, rank, world, work_dir, group=None, device="cuda", m=0):
+    """This rank's part of a build split by input file: the drop-in phase 1
+    of its slice of the files, the record exchange and merge, the drop-in
+    phase 2 of its bucket range.  Returns its shard for gather_merge.  Every
+    rank calls it (the exchange is a collective)."""
+    import os
+    f0, f1 = file_range(len(files), rank, world)
+    p1 = os.path.join(work_dir, "p1")
+    engine.phase1(files[f0:f1], k, num_buckets, p1, m=m, first_color=f0)
+    raw, off = read_bucket_dir(p1, num_buckets)
+    got = exchange_bucket_records(raw, off, num_buckets, rank, world, group=group, device=device)
+    lo, hi = shard_range(num_buckets, rank, world)
+    data, moff = merge_bucket_records(got, num_buckets, lo, hi)
+    md = os.path.join(work_dir, "merged")
+    write_bucket_dir(md, lo, data, moff)
+    frag, cs = os.path.join(work_dir, "frag_unitigs.bin"), os.path.join(work_dir, "out.color_sets")
+    engine.phase2(md, num_buckets, k, len(files), frag, cs)
+    return shard_from_phase2(frag, cs)

@@ -597,7 +597,8 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
         }
         std::vector<uint64_t> hint(files.size());
         for (size_t i = 0; i < files.size(); ++i) hint[i] = cdbg::io::inflated_size_hint(files[i]);
-        const bool packed = a->num_files < (1u << 28);
+        if ((uint64_t)a->first_color + a->num_files > 0xffffffffull) throw std::runtime_error("colors past 2^32");
+        const bool packed = (uint64_t)a->first_color + a->num_files < (1u << 28);
         double dev_s = 0;
         size_t f0 = 0;
         while (f0 < files.size()) {
@@ -618,13 +619,13 @@ int cdbg_gpu_phase1(cdbg_engine* e, const cdbg_phase1_args* a, cdbg_phase1_stats
             uint64_t inb = 0, nseq = 0;
             // the files are read on host threads while the device already
             // runs phase 1 on the ones read before
-            if (!phase1_from_files(e, cf, T, k, m, a->num_buckets, rt, sl, nullptr, &inb, (uint32_t)f0, packed,
+            if (!phase1_from_files(e, cf, T, k, m, a->num_buckets, rt, sl, nullptr, &inb, a->first_color + (uint32_t)f0, packed,
                                    &nseq)) {
                 // a file inflated past its size hint: read the chunk whole
                 e->A.reset();
                 e->P.reset();
                 cdbg::io::seq_batch hb;
-                cdbg::io::read_files(files, f0, f1 - f0, (uint32_t)f0, T, hb);
+                cdbg::io::read_files(files, f0, f1 - f0, a->first_color + (uint32_t)f0, T, hb);
                 inb = hb.input_bytes;
                 nseq = hb.seq.size();
                 cdbg_seq_batch b{hb.seq.data(), hb.seq.size(), hb.off.data(), hb.color.data(),

@@ -12,6 +12,7 @@
 // function of the set and the color count), so the merge deduplicates bit
 // strings, appends each new one to the global bit vector, and rewrites the
 // ids in the fragment records (unitig_spill.hpp:642-665 layout).
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -173,5 +174,175 @@ void cdbg_merged_free(cdbg_merged* m) {
 }
 
 const char* cdbg_merge_last_error(void) { return t_err.c_str(); }
+
+}  // extern "C"
+
+// ---- phase 1 split by input file ---------------------------------------------
+// Rank r reads its own slice of the input files (colors are global file
+// indices) and runs phase 1 on it; the records of every bucket then go to the
+// rank that owns the bucket, which merges the records all ranks made for it
+// into the records one phase 1 over all the files makes.  That phase 1 orders
+// a bucket's super-k-mer occurrences stably by the key (hash >> bb), in input
+// order between equal keys, and merges runs of consecutive occurrences with
+// equal key, length and bases (flags AND-ed, colors sorted unique).  Each
+// rank's records are that list over its own occurrences, and the ranks' files
+// are consecutive slices of the input, so the stable order of all the ranks'
+// records taken in rank order, merged the same way, is the one over all the
+// occurrences: merging runs of equal neighbours is the same whether done at
+// once or first within each rank's stretch.
+namespace {
+
+// The 64-bit key hash of a super-k-mer (length, then its 2-bit bases 32 at a
+// time, base i at bits 2(i%32) of word i/32, unused bits zero): the hash
+// phase 1 sorts by.
+uint64_t mix64_host(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+uint64_t super_hash_packed(uint8_t const* packed, uint32_t len) {
+    uint64_t h = mix64_host(0x51ed2701f3a5c2b9ULL ^ (uint64_t)len);
+    const uint64_t nb = ((uint64_t)len + 3) / 4;
+    for (uint64_t i = 0; i < nb; i += 8) {
+        uint64_t w = 0;
+        std::memcpy(&w, packed + i, (size_t)std::min<uint64_t>(8, nb - i));
+        h = mix64_host(h ^ w);
+    }
+    return h;
+}
+
+bool get_varint(uint8_t const* b, uint64_t end, uint64_t& p, uint64_t& v) {
+    v = 0;
+    for (uint32_t sh = 0; p < end && sh < 64; sh += 7) {
+        const uint8_t c = b[p++];
+        v |= (uint64_t)(c & 0x7f) << sh;
+        if (!(c & 0x80)) return true;
+    }
+    return false;
+}
+
+void put_varint(uint64_t v, std::vector<uint8_t>& out) {
+    while (v >= 0x80) {
+        out.push_back((uint8_t)(v | 0x80));
+        v >>= 7;
+    }
+    out.push_back((uint8_t)v);
+}
+
+// One serialized bucket record (super_kmer.hpp:105-143 layout: varint color
+// count, varint color gaps, varint (len << 4 | flags), 2-bit bases).
+struct rec_ref {
+    uint64_t key;
+    uint32_t len, flags;
+    uint8_t const* bases;
+    std::vector<uint32_t> colors;
+};
+
+void parse_records(uint8_t const* b, uint64_t n, uint32_t bb, std::vector<rec_ref>& out) {
+    uint64_t p = 0;
+    while (p < n) {
+        rec_ref r;
+        uint64_t nc, v;
+        if (!get_varint(b, n, p, nc)) throw std::runtime_error("malformed bucket record");
+        r.colors.resize(nc);
+        uint32_t prev = 0;
+        for (uint64_t c = 0; c < nc; ++c) {
+            if (!get_varint(b, n, p, v)) throw std::runtime_error("malformed bucket record");
+            prev += (uint32_t)v;
+            r.colors[c] = prev;
+        }
+        if (!get_varint(b, n, p, v)) throw std::runtime_error("malformed bucket record");
+        r.len = (uint32_t)(v >> 4);
+        r.flags = (uint32_t)(v & 0xf);
+        const uint64_t pb = ((uint64_t)r.len + 3) / 4;
+        if (p + pb > n) throw std::runtime_error("malformed bucket record");
+        r.bases = b + p;
+        p += pb;
+        const uint64_t h = super_hash_packed(r.bases, r.len);
+        r.key = bb ? (h >> bb) : h;
+        out.push_back(std::move(r));
+    }
+}
+
+struct merged_records_out {
+    std::vector<uint8_t> bytes;
+    std::vector<uint64_t> off;
+};
+
+}  // namespace
+
+extern "C" {
+
+int cdbg_merge_bucket_records(uint32_t num_sources, const uint8_t* const* src, const uint64_t* const* src_off,
+                              uint32_t num_buckets, uint32_t b_lo, uint32_t b_hi, cdbg_merged_records* out) {
+    try {
+        if (!out || (num_sources && (!src || !src_off))) throw std::runtime_error("null argument");
+        if (b_lo > b_hi || b_hi > num_buckets) throw std::runtime_error("bad bucket range");
+        uint32_t bb = 0;
+        while ((1ull << bb) < num_buckets) ++bb;
+        auto* m = new merged_records_out();
+        try {
+            const uint32_t nb = b_hi - b_lo;
+            m->off.assign(nb + 1, 0);
+            std::vector<rec_ref> recs;
+            std::vector<uint32_t> idx;
+            for (uint32_t i = 0; i < nb; ++i) {
+                recs.clear();
+                for (uint32_t s = 0; s < num_sources; ++s)
+                    parse_records(src[s] + src_off[s][i], src_off[s][i + 1] - src_off[s][i], bb, recs);
+                idx.resize(recs.size());
+                for (uint32_t j = 0; j < idx.size(); ++j) idx[j] = j;
+                std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return recs[a].key < recs[b].key; });
+                size_t j = 0;
+                while (j < idx.size()) {
+                    rec_ref const& a = recs[idx[j]];
+                    std::vector<uint32_t> colors = a.colors;
+                    uint32_t flags = a.flags;
+                    size_t t = j + 1;
+                    for (; t < idx.size(); ++t) {
+                        rec_ref const& c = recs[idx[t]];
+                        if (c.key != a.key || c.len != a.len ||
+                            std::memcmp(c.bases, a.bases, ((size_t)a.len + 3) / 4) != 0)
+                            break;
+                        flags &= c.flags;
+                        colors.insert(colors.end(), c.colors.begin(), c.colors.end());
+                    }
+                    if (t > j + 1) {
+                        std::sort(colors.begin(), colors.end());
+                        colors.erase(std::unique(colors.begin(), colors.end()), colors.end());
+                    }
+                    put_varint(colors.size(), m->bytes);
+                    uint32_t prev = 0;
+                    for (uint32_t c : colors) {
+                        put_varint(c - prev, m->bytes);
+                        prev = c;
+                    }
+                    put_varint(((uint64_t)a.len << 4) | flags, m->bytes);
+                    m->bytes.insert(m->bytes.end(), a.bases, a.bases + ((size_t)a.len + 3) / 4);
+                    j = t;
+                }
+                m->off[i + 1] = m->bytes.size();
+            }
+            out->bytes = m->bytes.data();
+            out->nbytes = m->bytes.size();
+            out->bucket_off = m->off.data();
+            out->handle = m;
+            return 0;
+        } catch (...) {
+            delete m;
+            throw;
+        }
+    } catch (std::exception const& ex) {
+        t_err = ex.what();
+        return -1;
+    }
+}
+
+void cdbg_merged_records_free(cdbg_merged_records* m) {
+    if (!m || !m->handle) return;
+    delete static_cast<merged_records_out*>(m->handle);
+    m->handle = nullptr;
+}
 
 }  // extern "C"

@@ -147,7 +147,7 @@ void cdbg_free_sequences(cdbg_seq_batch* b);
 /* ---- phase 1 ------------------------------------------------------------ */
 
 typedef struct cdbg_phase1_args {
-    const char* const* files; /* file i = color i (FASTA/FASTQ, optionally gzip) */
+    const char* const* files; /* file i = color first_color + i (FASTA/FASTQ, optionally gzip) */
     uint32_t num_files;
     uint32_t k;               /* <= 63 */
     uint32_t m;               /* 0 = compute_best_m(k) (minimizer.hpp:65) */
@@ -156,6 +156,8 @@ typedef struct cdbg_phase1_args {
     uint32_t host_threads;    /* inflate / parse / LZ4 threads (0 = all cores) */
     uint64_t chunk_bytes;     /* sequence bytes per device pass (0 = 8 GiB) */
     uint64_t* bucket_unc_bytes; /* out, num_buckets entries, may be NULL */
+    uint32_t first_color;     /* color of files[0]: one rank's slice of a collection
+                                 split by input file (0 for a whole build) */
 } cdbg_phase1_args;
 
 typedef struct cdbg_phase1_stats {
@@ -388,6 +390,28 @@ int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stat
  * fails on a record that runs past the end. */
 int cdbg_frag_record_offsets(const uint8_t* frags, uint64_t frag_nbytes, uint32_t host_threads, uint64_t* offsets,
                              uint64_t cap, uint64_t* n_records);
+
+/* Phase 1 split by input file: rank r runs phase 1 on its own consecutive
+ * slice of the input files (colors = global file indices) and sends each
+ * bucket's records to the rank that owns the bucket.  This merges, for the
+ * owner's buckets [b_lo, b_hi), the records all ranks made (source s's bucket
+ * b_lo + i is src[s][src_off[s][i] .. src_off[s][i + 1]), decompressed bucket
+ * file bytes, sources in file order) into the records one phase 1 over all
+ * the files makes: the super-k-mers stably ordered by their key, equal
+ * neighbours merged with flags AND-ed and colors united.  num_buckets is the
+ * whole build's B.  Host only; the result's buffers belong to the library
+ * until cdbg_merged_records_free; errors via cdbg_merge_last_error().  No
+ * counterpart in the reference, which builds in one process. */
+typedef struct cdbg_merged_records {
+    const uint8_t* bytes;        /* the records of the buckets back to back */
+    uint64_t nbytes;
+    const uint64_t* bucket_off;  /* b_hi - b_lo + 1 offsets into bytes */
+    void* handle;
+} cdbg_merged_records;
+
+int cdbg_merge_bucket_records(uint32_t num_sources, const uint8_t* const* src, const uint64_t* const* src_off,
+                              uint32_t num_buckets, uint32_t b_lo, uint32_t b_hi, cdbg_merged_records* out);
+void cdbg_merged_records_free(cdbg_merged_records* m);
 
 /* Serialized size of the bucket records of the engine's last cdbg_gpu_build
  * (the uncompressed bytes its bucket files would hold), counted on the device

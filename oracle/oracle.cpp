@@ -882,8 +882,18 @@ uint64_t oracle_super_hash(uint8_t const* b, uint32_t len) { return super_hash(b
 // Phase 1 over a filenames list: dumps every super-k-mer occurrence in the
 // layout of oracle/ref_harness/ref_phase1.cpp; when bucket_dir is non-null also
 // writes canonical bucket files bucket_<b>.bin (one LZ4 frame each).
+int oracle_phase1_from(char const* filelist, uint32_t first_color, uint32_t k, uint32_t m, uint32_t B,
+                       char const* dump_path, char const* bucket_dir, uint64_t* n_supers, uint64_t* n_kmers);
+
 int oracle_phase1(char const* filelist, uint32_t k, uint32_t m, uint32_t B, char const* dump_path,
                   char const* bucket_dir, uint64_t* n_supers, uint64_t* n_kmers) {
+    return oracle_phase1_from(filelist, 0, k, m, B, dump_path, bucket_dir, n_supers, n_kmers);
+}
+
+// Phase 1 with file i of the list read as color first_color + i (one rank's
+// slice of a collection split by input file).
+int oracle_phase1_from(char const* filelist, uint32_t first_color, uint32_t k, uint32_t m, uint32_t B,
+                       char const* dump_path, char const* bucket_dir, uint64_t* n_supers, uint64_t* n_kmers) {
     try {
         if (m == 0) m = best_m(k);
         auto files = read_list(filelist);
@@ -898,7 +908,7 @@ int oracle_phase1(char const* filelist, uint32_t k, uint32_t m, uint32_t B, char
                 for (size_t r = r0; r < runs.size(); ++r) {
                     size_t o0 = occ.size();
                     nk += runs[r].size() - k + 1;
-                    emit_supers(runs[r].data(), (uint32_t)runs[r].size(), k, m, B, c, occ);
+                    emit_supers(runs[r].data(), (uint32_t)runs[r].size(), k, m, B, first_color + c, occ);
                     for (size_t o = o0; o < occ.size(); ++o) occ_run.push_back((uint32_t)r);
                 }
             }
