@@ -226,6 +226,10 @@ SIGNATURES = {
                                                  ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, ctypes.c_uint32,
                                                  ctypes.c_uint32, ctypes.POINTER(MergedRecords)]),
     "cdbg_merged_records_free": (None, [ctypes.POINTER(MergedRecords)]),
+    "cdbg_class_strings": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    "cdbg_frag_remap_classes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                               ctypes.c_uint64]),
     "cdbg_merge_last_error": (ctypes.c_char_p, []),
 }
 

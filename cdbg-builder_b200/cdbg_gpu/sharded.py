@@ -203,3 +203,167 @@ def build_rank_by_files(engine, files, k, num_buckets, rank, world, work_dir, gr
     frag, cs = os.path.join(work_dir, "frag_unitigs.bin"), os.path.join(work_dir, "out.color_sets")
     engine.phase2(md, num_buckets, k, len(files), frag, cs)
     return shard_from_phase2(frag, cs)
+
+
+# ---- color-set interning across ranks -----------------------------------------
+# gather_merge interns every shard's classes on one rank.  intern_classes does
+# it hash-partitioned instead: the owner of a class (its hash mod the ranks)
+# learns every (rank, local id) that has it and which rank saw it first (the
+# lowest rank: buckets are split in rank order); each rank numbers the classes
+# it saw first in its own order, after the ranks before it (a prefix sum of
+# their counts), which is the single build's first-appearance order over
+# buckets 0..B-1; the owners pass those ids to the other holders, and every
+# rank rewrites its own fragments.  No rank holds more than its share of the
+# classes, and only the classes each rank saw first make up the .color_sets
+# bit vector.
+
+def _all_to_all_bytes(blobs, world, group=None, device="cpu"):
+    """blobs[q] goes to rank q; returns what every rank sent here, in rank order."""
+    import torch
+    import torch.distributed as dist
+    sizes = torch.tensor([len(b) for b in blobs], dtype=torch.int64, device=device)
+    got_sizes = torch.empty(world, dtype=torch.int64, device=device)
+    dist.all_to_all_single(got_sizes, sizes, group=group)
+    got_sizes = [int(x) for x in got_sizes.cpu().tolist()]
+    cat = b"".join(blobs)
+    send = torch.from_numpy(np.frombuffer(cat, dtype=np.uint8).copy() if cat else np.zeros(0, np.uint8))
+    recv = torch.empty(sum(got_sizes), dtype=torch.uint8, device=device)
+    dist.all_to_all_single(recv, send.to(device), got_sizes, [len(b) for b in blobs], group=group)
+    data = recv.cpu().numpy().tobytes()
+    out, p = [], 0
+    for n in got_sizes:
+        out.append(data[p:p + n])
+        p += n
+    return out
+
+
+def class_strings(words, class_bits, offsets):
+    """(hashes, strings, string offsets): each class's bits from bit 0 in whole
+    words and its 64-bit hash (cdbg_class_strings)."""
+    L = native.lib()
+    n = len(offsets)
+    w = np.ascontiguousarray(words, dtype=np.uint64) if len(words) else np.zeros(1, dtype=np.uint64)
+    o = np.ascontiguousarray(offsets, dtype=np.uint64) if n else np.zeros(1, dtype=np.uint64)
+    hashes = np.zeros(max(n, 1), dtype=np.uint64)
+    cap = int(class_bits) // 64 + n + 1
+    strings = np.zeros(cap, dtype=np.uint64)
+    soff = np.zeros(n + 1, dtype=np.uint64)
+    if L.cdbg_class_strings(w.ctypes.data, int(class_bits), o.ctypes.data, n, hashes.ctypes.data,
+                            strings.ctypes.data, cap, soff.ctypes.data) != 0:
+        raise RuntimeError(L.cdbg_merge_last_error().decode(errors="replace"))
+    return hashes[:n], strings, soff
+
+
+def remap_frag(frag, mapping):
+    """frag bytes with their color-set ids rewritten through `mapping`."""
+    L = native.lib()
+    buf = bytearray(frag)
+    m = np.ascontiguousarray(mapping, dtype=np.uint64) if len(mapping) else np.zeros(1, dtype=np.uint64)
+    cb = (ctypes.c_char * len(buf)).from_buffer(buf) if buf else None
+    if L.cdbg_frag_remap_classes(ctypes.addressof(cb) if cb is not None else None, len(buf), m.ctypes.data,
+                                 len(mapping)) != 0:
+        raise RuntimeError(L.cdbg_merge_last_error().decode(errors="replace"))
+    return bytes(buf)
+
+
+def intern_classes(shard, rank, world, group=None, device="cpu"):
+    """shard: (frag bytes, class words, class bits, class offsets) of this
+    rank's bucket range, ranks in bucket order.  Returns (frag bytes with the
+    whole build's color-set ids, the bit strings of the classes this rank saw
+    first as (words, bits), their lengths in bits, the whole-build id of the
+    first of them).  Every rank calls it (a collective)."""
+    import pickle
+    import torch
+    import torch.distributed as dist
+    frag, words, bits, offs = shard
+    n = len(offs)
+    hashes, strings, soff = class_strings(words, bits, offs)
+    lens = [int(offs[c + 1] if c + 1 < n else bits) - int(offs[c]) for c in range(n)]
+
+    def key(c):
+        return lens[c], strings[int(soff[c]):int(soff[c + 1])].tobytes()
+
+    # 1. every class to its owner
+    out = [[] for _ in range(world)]
+    for c in range(n):
+        ln, s = key(c)
+        out[int(hashes[c]) % world].append((c, ln, s))
+    got = [pickle.loads(b) for b in _all_to_all_bytes([pickle.dumps(x) for x in out], world, group, device)]
+    # 2. the owner finds each class's first holder and tells every holder
+    first = {}
+    for src in range(world):  # rank order: the first holder is the lowest rank
+        for c, ln, s in got[src]:
+            first.setdefault((ln, s), (src, c))
+    reply = [[(c, first[(ln, s)]) for c, ln, s in got[src]] for src in range(world)]
+    back = [pickle.loads(b) for b in _all_to_all_bytes([pickle.dumps(x) for x in reply], world, group, device)]
+    firsts = [None] * n
+    for part in back:
+        for c, f in part:
+            firsts[c] = f
+    new = [c for c in range(n) if firsts[c] == (rank, c)]
+    # 3. ids: the classes this rank saw first, after those of the ranks before it
+    counts = [0] * world
+    dist.all_gather_object(counts, len(new), group=group)
+    base = sum(counts[:rank])
+    gid = np.full(n, np.iinfo(np.uint64).max, dtype=np.uint64)
+    for i, c in enumerate(new):
+        gid[c] = base + i
+    # 4. the owners pass the new ids to every holder
+    tell = [[] for _ in range(world)]
+    for c in new:
+        tell[int(hashes[c]) % world].append((c, int(gid[c])))
+    learned = [pickle.loads(b) for b in _all_to_all_bytes([pickle.dumps(x) for x in tell], world, group, device)]
+    first_gid = {}
+    for src in range(world):
+        for c, g in learned[src]:
+            first_gid[(src, c)] = g
+    answer = [[(c, first_gid[first[(ln, s)]]) for c, ln, s in got[src]] for src in range(world)]
+    final = [pickle.loads(b) for b in _all_to_all_bytes([pickle.dumps(x) for x in answer], world, group, device)]
+    for part in final:
+        for c, g in part:
+            gid[c] = g
+    # 5. this rank's fragments and its classes' bits
+    seg = _concat_bits([(strings[int(soff[c]):int(soff[c + 1])], lens[c]) for c in new])
+    return remap_frag(frag, gid), seg, [lens[c] for c in new], base
+
+
+def _concat_bits(parts):
+    """[(words from bit 0, nbits)] -> (words, nbits) of the bit strings back to back."""
+    total = sum(int(nb) for _, nb in parts)
+    out = np.zeros((total + 63) // 64 + 1, dtype=np.uint64)
+    pos = 0
+    for w, nb in parts:
+        nb = int(nb)
+        if nb == 0:
+            continue
+        nw = (nb + 63) // 64
+        w = np.array(w[:nw], dtype=np.uint64)
+        if nb % 64:
+            w[-1] &= np.uint64((1 << (nb % 64)) - 1)
+        i, s = pos // 64, pos % 64
+        if s == 0:
+            out[i:i + nw] |= w
+        else:
+            out[i:i + nw] |= w << np.uint64(s)
+            out[i + 1:i + nw + 1] |= w >> np.uint64(64 - s)
+        pos += nb
+    return out[:(total + 63) // 64], total
+
+
+def assemble(interned, rank, world, dst=0, group=None):
+    """The whole build's (frag bytes, class words, class offsets, class bits)
+    on rank `dst` (None elsewhere) from every rank's intern_classes result:
+    the fragments and the class bit strings back to back in rank order, the
+    class offsets from the strings' lengths."""
+    import torch.distributed as dist
+    got = [None] * world if rank == dst else None
+    dist.gather_object(interned, got, dst=dst, group=group)
+    if rank != dst:
+        return None
+    frag = b"".join(g[0] for g in got)
+    words, bits = _concat_bits([g[1] for g in got])
+    lens = [ln for g in got for ln in g[2]]
+    offsets = np.zeros(len(lens), dtype=np.uint64)
+    if lens:
+        offsets[1:] = np.cumsum(np.asarray(lens[:-1], dtype=np.uint64))
+    return frag, words, offsets, bits

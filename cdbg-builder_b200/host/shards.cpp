@@ -339,6 +339,59 @@ int cdbg_merge_bucket_records(uint32_t num_sources, const uint8_t* const* src, c
     }
 }
 
+int cdbg_class_strings(const uint64_t* words, uint64_t class_bits, const uint64_t* offsets, uint64_t n,
+                       uint64_t* hashes, uint64_t* strings, uint64_t strings_cap, uint64_t* string_off) {
+    try {
+        if (n && (!words || !offsets || !hashes || !string_off)) throw std::runtime_error("null argument");
+        std::vector<uint64_t> key;
+        uint64_t at = 0;
+        string_off[0] = 0;
+        for (uint64_t c = 0; c < n; ++c) {
+            const uint64_t a = offsets[c], b = c + 1 < n ? offsets[c + 1] : class_bits;
+            if (b < a || b > class_bits) throw std::runtime_error("bad class offsets");
+            extract(words, a, b, key);
+            hashes[c] = hash_words(key, b - a);
+            if (at + key.size() > strings_cap) throw std::runtime_error("class strings buffer too small");
+            if (!key.empty()) std::memcpy(strings + at, key.data(), 8 * key.size());
+            at += key.size();
+            string_off[c + 1] = at;
+        }
+        return 0;
+    } catch (std::exception const& ex) {
+        t_err = ex.what();
+        return -1;
+    }
+}
+
+int cdbg_frag_remap_classes(uint8_t* frag, uint64_t n, const uint64_t* map, uint64_t nmap) {
+    try {
+        if (n && (!frag || (nmap && !map))) throw std::runtime_error("null argument");
+        uint64_t p = 0;
+        while (p < n) {
+            if (p + 5 > n) throw std::runtime_error("truncated fragment record");
+            uint32_t nr;
+            std::memcpy(&nr, frag + p + 1, 4);
+            const uint64_t runs_end = p + 5 + 12ull * nr;
+            if (runs_end + 4 > n) throw std::runtime_error("truncated fragment record");
+            uint32_t sl;
+            std::memcpy(&sl, frag + runs_end, 4);
+            if (runs_end + 4 + sl > n) throw std::runtime_error("truncated fragment record");
+            for (uint32_t r = 0; r < nr; ++r) {
+                uint64_t cid;
+                std::memcpy(&cid, frag + p + 5 + 12ull * r, 8);
+                if (cid == UINT64_MAX) continue;  // a foreign run keeps its marker
+                if (cid >= nmap) throw std::runtime_error("fragment color-set id out of range");
+                std::memcpy(frag + p + 5 + 12ull * r, map + cid, 8);
+            }
+            p = runs_end + 4 + sl;
+        }
+        return 0;
+    } catch (std::exception const& ex) {
+        t_err = ex.what();
+        return -1;
+    }
+}
+
 void cdbg_merged_records_free(cdbg_merged_records* m) {
     if (!m || !m->handle) return;
     delete static_cast<merged_records_out*>(m->handle);

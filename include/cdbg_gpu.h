@@ -413,6 +413,19 @@ int cdbg_merge_bucket_records(uint32_t num_sources, const uint8_t* const* src, c
                               uint32_t num_buckets, uint32_t b_lo, uint32_t b_hi, cdbg_merged_records* out);
 void cdbg_merged_records_free(cdbg_merged_records* m);
 
+/* Color-set interning across ranks (hash-partitioned, instead of merging all
+ * shards on one rank).  cdbg_class_strings: each of a shard's n classes (bits
+ * [offsets[c], offsets[c + 1]) of words, the last ending at class_bits)
+ * re-aligned to bit 0 in whole words, strings[string_off[c] ..
+ * string_off[c + 1]) (strings_cap >= class_bits / 64 + n words), and a 64-bit
+ * hash of it, hashes[c] (the owner rank is hash % ranks).
+ * cdbg_frag_remap_classes: the color-set ids of frag records rewritten in
+ * place through map[nmap] (foreign runs keep their marker).  Host only;
+ * errors via cdbg_merge_last_error().  No counterpart in the reference. */
+int cdbg_class_strings(const uint64_t* words, uint64_t class_bits, const uint64_t* offsets, uint64_t n,
+                       uint64_t* hashes, uint64_t* strings, uint64_t strings_cap, uint64_t* string_off);
+int cdbg_frag_remap_classes(uint8_t* frag, uint64_t n, const uint64_t* map, uint64_t nmap);
+
 /* Serialized size of the bucket records of the engine's last cdbg_gpu_build
  * (the uncompressed bytes its bucket files would hold), counted on the device
  * outside the build.  Valid until the engine's next call. */

@@ -129,3 +129,54 @@ def test_merge_of_any_split_is_the_single_build(tmp_path, world):
     # differently from the whole build
     if world > 1:
         assert any(len(s[3]) < len(want[3]) for s in shards)
+
+
+def _intern_worker(rank, world, port, d, out):
+    import sys
+    for p in (ROOT, os.path.join(ROOT, "cdbg-builder_b200"), os.path.join(ROOT, "tests")):
+        sys.path.insert(0, p)
+    import datetime
+    import torch.distributed as dist
+    from conftest import Oracle
+    from cdbg_gpu import sharded
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                           timeout=datetime.timedelta(seconds=60))
+    try:
+        orc = Oracle()
+        lst = os.path.join(d, "in", "filenames.txt")
+        rd = os.path.join(d, "rank%d" % rank)
+        os.makedirs(rd)
+        shard = _oracle_shard(orc, lst, rd, *sharded.shard_range(B, rank, world))
+        interned = sharded.intern_classes(shard, rank, world)
+        whole = sharded.assemble(interned, rank, world)
+        if rank == 0:
+            frag, w, o, bits = whole
+            out.put((frag, w.tobytes(), o.tobytes(), bits))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_hash_partitioned_interning_is_the_single_build(tmp_path, world):
+    """Color sets interned across ranks (owner = class hash mod ranks, ids by a
+    prefix sum over the ranks' first-seen classes, every rank rewriting its own
+    fragments) equal the single build byte for byte."""
+    if not os.path.exists(ORACLE_LIB):
+        pytest.skip("oracle not built")
+    from conftest import Oracle
+    d = str(tmp_path)
+    lst = _collection(d, seed=29)
+    want = _single(Oracle(), lst, os.path.join(d, "single"))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_intern_worker, args=(r, world, port, d, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    frag, w, o, bits = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert frag == want[0]
+    assert bits == want[2] and w == want[1].tobytes()
+    assert o == want[3].tobytes()
