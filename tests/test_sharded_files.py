@@ -4,7 +4,8 @@ the rank that owns the bucket (one all-to-all over torch.distributed, gloo,
 world size 2, two processes), which merges them into the records one phase 1
 over all the files makes, then runs phase 2 of its bucket range; the shards
 are gathered and merged on one rank.  The records and the final outputs equal
-the single build's byte for byte.
+the single build's byte for byte, merged on one rank or with the color sets
+interned across the ranks.
 
 Phase 1 and phase 2 of each rank are made here by the CPU oracle, in the
 places the GPU drop-in phases run on a rank's GPU; what is under test is the
@@ -87,11 +88,15 @@ def _worker(rank, world, port, d, out):
         sharded.write_bucket_dir(os.path.join(rd, "merged"), lo, data, moff)
         shard = _phase2_shard(Oracle(), os.path.join(rd, "merged"), os.path.join(rd, "out"))
         whole = sharded.gather_merge(shard, rank, world)
+        # the same shards interned across the ranks instead of on one
+        spread = sharded.assemble(sharded.intern_classes(shard, rank, world), rank, world)
         recs = (lo, data, moff.tobytes())
         allrecs = [None] * world if rank == 0 else None
         dist.gather_object(recs, allrecs, dst=0)
         if rank == 0:
             frag, w, o, bits = whole
+            assert spread[0] == frag and spread[1].tobytes() == w.tobytes()
+            assert spread[2].tobytes() == o.tobytes() and spread[3] == bits
             out.put((frag, w.tobytes(), o.tobytes(), bits, allrecs))
     finally:
         dist.destroy_process_group()
