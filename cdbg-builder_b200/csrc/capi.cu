@@ -1676,7 +1676,15 @@ int cdbg_gpu_build_files(cdbg_engine* e, const cdbg_build_files_args* a, cdbg_bu
                 cudaEventDestroy(v[1]);
             });
             cdbg_seed_stats ss{};
-            seed_pass(e, e->p2.frag.p, dOff, n, c, store, cf, cp.c_str(), th, ev, &ss);
+            // passes of at most 2^31 records (the kernels index records in 32
+            // bits); the offsets are absolute, so a pass is a slice of them
+            constexpr uint64_t PASS = 1ull << 31;
+            for (uint64_t i0 = 0; i0 < n || (n == 0 && i0 == 0); i0 += PASS) {
+                seed_pass(e, e->p2.frag.p, dOff + i0, std::min(PASS, n - i0), c, store, cf, cp.c_str(), th, ev,
+                          &ss);
+                e->A.reset();
+                if (n == 0) break;
+            }
             store.finish(th);
             if (std::fclose(cf_guard.release()) != 0) throw std::runtime_error("close failed on " + cp);
             e->A.reset();
