@@ -172,3 +172,29 @@ def test_merge_of_file_slices_is_the_single_phase1(tmp_path, slices):
             data, moff = sharded.merge_bucket_records(sources, B, lo, hi)
             assert data == raw[int(off[lo]):int(off[hi])]
             assert np.array_equal(moff, (off[lo:hi + 1] - off[lo]).astype(np.uint64))
+
+
+def test_merge_and_remap_reject_malformed_input():
+    """Truncated records, bad ranges and ids past the map are errors, not
+    wrong output."""
+    from cdbg_gpu import native, sharded
+    # one record: 1 color (7), len 5 flags 3, 2 bytes of bases
+    rec = bytes([1, 7, (5 << 4) | 3, 0x1b, 0x02])
+    data, off = sharded.merge_bucket_records([(rec, np.array([0, len(rec)], dtype=np.uint64))] * 2, 4, 1, 2)
+    assert data == rec and list(off) == [0, len(rec)]   # the same record twice merges into one
+    with pytest.raises(RuntimeError):
+        sharded.merge_bucket_records([(rec[:-1], np.array([0, len(rec) - 1], dtype=np.uint64))], 4, 1, 2)
+    with pytest.raises(RuntimeError):
+        sharded.merge_bucket_records([(rec, np.array([0, len(rec), len(rec)], dtype=np.uint64))], 4, 3, 5)
+    # a fragment with one run of color-set id 2
+    import struct
+    frag = struct.pack("<BI", 0, 1) + struct.pack("<QI", 2, 1) + struct.pack("<I", 31) + b"A" * 31
+    assert sharded.remap_frag(frag, [5, 6, 9])[5:13] == struct.pack("<Q", 9)
+    with pytest.raises(RuntimeError):
+        sharded.remap_frag(frag, [5, 6])
+    with pytest.raises(RuntimeError):
+        sharded.remap_frag(frag[:-1], [5, 6, 9])
+    h, strings, soff = sharded.class_strings(np.array([0b1011], dtype=np.uint64), 4, np.array([0, 3], dtype=np.uint64))
+    assert list(soff) == [0, 1, 2] and int(strings[0]) == 0b011 and int(strings[1]) == 0b1 and h[0] != h[1]
+    with pytest.raises(RuntimeError):
+        sharded.class_strings(np.array([0], dtype=np.uint64), 4, np.array([3, 1], dtype=np.uint64))
