@@ -1875,7 +1875,6 @@ int cdbg_gpu_stitch_seed(cdbg_engine* e, const cdbg_seed_args* a, cdbg_seed_stat
                 CDBG_CUDA(cudaMemcpyAsync(dOff, loff.data(), 8 * (nc + 1), cudaMemcpyHostToDevice, e->st));
             }
             seed_pass(e, dF, dOff, nc, c, store, cf, a->closed_path, T, ev, s);
-            ++s->n_passes;
             e->A.release(mk);
             i0 = i1;
         }
